@@ -1,0 +1,855 @@
+/*
+ * CPU restatement of tmol's LJ + LK pose scoring, used ONLY as a test oracle.
+ *
+ * This file is test infrastructure.  Nothing in the product links or calls
+ * it; tests, the smoke check and the benchmark's CPU-baseline leg load it
+ * through ctypes to check the CUDA path.
+ *
+ * It follows, function by function, the reference's CPU execution of the
+ * pose-score op (one thread per work group, work groups in index order), in
+ * the same floating-point operation order, so that the float build agrees
+ * with the compiled reference op to the last bit in most cases:
+ *
+ *   count-pair weight      tmol/score/ljlk/potentials/common.hh:14-22
+ *   LJ sigma rule          tmol/score/ljlk/potentials/common.hh:25-44
+ *   vdw / lj_score         tmol/score/ljlk/potentials/lj.hh:22-178
+ *   f_desolv / LK pair     tmol/score/ljlk/potentials/lk_isotropic.hh:23-236
+ *   LK isotropic score     tmol/score/ljlk/potentials/lk_isotropic.hh:239-361
+ *   Hermite splines        tmol/score/common/cubic_hermite_polynomial.hh:34-137
+ *   distance + gradient    tmol/score/common/geom.hh:20-40
+ *   block spheres          tmol/score/common/sphere_overlap.impl.hh:109-196
+ *   block neighbours       tmol/score/common/sphere_overlap.impl.hh:287-351
+ *   inter-block count pair tmol/score/common/count_pair.hh:162-207,
+ *                          tmol/score/ljlk/potentials/ljlk_pose_score.impl.hh:47-67
+ *   intra-block count pair ljlk_pose_score.impl.hh:115-134, 176-206
+ *   tile walk              tmol/score/common/tile_atom_pair_evaluation.hh:79-173, 358-505
+ *   whole-pose forward     ljlk_pose_score.impl.hh:953-1156
+ *   block-pair forward     ljlk_pose_score.impl.hh:803-951
+ *   block-pair backward    ljlk_pose_score.impl.hh:1160-1477
+ *
+ * Compile with -DORACLE_REAL=float (default) or -DORACLE_REAL=double and
+ * -ffp-contract=off (no fused multiply-add, as the reference's x86-64 build).
+ */
+
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#if defined(ORACLE_DOUBLE)
+#define ORACLE_REAL double
+#else
+#define ORACLE_REAL float
+#endif
+typedef ORACLE_REAL real;
+
+#define TILE 32
+#define MAX_N_CONN 4
+#define MAX_IMPORTANT_BOND_SEPARATION 4
+
+typedef struct {
+  real lj_radius, lj_wdepth, lk_dgfree, lk_lambda, lk_volume;
+  real is_donor, is_hydroxyl, is_polarh, is_acceptor, is_carbon_lk;
+} type_params_t;
+
+typedef struct {
+  real max_dis, lj_dlin_sigma_factor, lj_hbond_dis, lj_hbond_OH_donor_dis,
+      lj_hbond_hdis;
+} global_params_t;
+
+static real rsqrt_(real x) {
+#if defined(ORACLE_DOUBLE)
+  return sqrt(x);
+#else
+  return sqrtf(x);
+#endif
+}
+static real rexp_(real x) {
+#if defined(ORACLE_DOUBLE)
+  return exp(x);
+#else
+  return expf(x);
+#endif
+}
+static real rfloor_(real x) {
+#if defined(ORACLE_DOUBLE)
+  return floor(x);
+#else
+  return floorf(x);
+#endif
+}
+static real rmax_(real a, real b) { return a < b ? b : a; }
+static real rmin_(real a, real b) { return b < a ? b : a; }
+
+/* common.hh:14-22 */
+static real connectivity_weight(int bonded_path_length) {
+  if (bonded_path_length > 4) return (real)1.0;
+  if (bonded_path_length == 4) return (real)0.2;
+  return (real)0.0;
+}
+
+/* common.hh:25-44 */
+static real lj_sigma(const type_params_t* i, const type_params_t* j,
+                     const global_params_t* g) {
+  if ((i->is_donor != 0 && j->is_acceptor != 0) ||
+      (j->is_donor != 0 && i->is_acceptor != 0)) {
+    if ((i->is_donor != 0 && i->is_hydroxyl != 0) ||
+        (j->is_donor != 0 && j->is_hydroxyl != 0)) {
+      return g->lj_hbond_OH_donor_dis;
+    }
+    return g->lj_hbond_dis;
+  } else if ((i->is_polarh != 0 && j->is_acceptor != 0) ||
+             (j->is_polarh != 0 && i->is_acceptor != 0)) {
+    return g->lj_hbond_hdis;
+  }
+  return i->lj_radius + j->lj_radius;
+}
+
+/* cubic_hermite_polynomial.hh:48-63 */
+static real interpolate(real x, real x0, real p0, real dpdx0, real x1, real p1,
+                        real dpdx1) {
+  real t = (x - x0) / (x1 - x0);
+  real dp0 = dpdx0 * (x1 - x0);
+  real dp1 = dpdx1 * (x1 - x0);
+  return p0 + t * (dp0 + t * (-2 * dp0 - dp1 - 3 * p0 + 3 * p1 +
+                              t * (dp0 + dp1 + 2 * p0 - 2 * p1)));
+}
+
+/* cubic_hermite_polynomial.hh:83-102 */
+static void interpolate_V_dV(real x, real x0, real p0, real dpdx0, real x1,
+                             real p1, real dpdx1, real* V, real* dV) {
+  real t = (x - x0) / (x1 - x0);
+  real dp0 = dpdx0 * (x1 - x0);
+  real dp1 = dpdx1 * (x1 - x0);
+  real p = p0 + t * (dp0 + t * (-2 * dp0 - dp1 - 3 * p0 + 3 * p1 +
+                                t * (dp0 + dp1 + 2 * p0 - 2 * p1)));
+  real dp = dp0 + t * (-4 * dp0 - 2 * dp1 - 6 * p0 + 6 * p1 +
+                       t * (3 * dp0 + 3 * dp1 + 6 * p0 - 6 * p1));
+  *V = p;
+  *dV = dp / (x1 - x0);
+}
+
+/* cubic_hermite_polynomial.hh:104-113 */
+static real interpolate_to_zero(real x, real x0, real p0, real dpdx0, real x1) {
+  real t = (x - x0) / (x1 - x0);
+  real dp0 = dpdx0 * (x1 - x0);
+  return p0 + t * (dp0 + t * (-2 * dp0 - 3 * p0 + t * (dp0 + 2 * p0)));
+}
+
+/* cubic_hermite_polynomial.hh:127-137 */
+static void interpolate_to_zero_V_dV(real x, real x0, real p0, real dpdx0,
+                                     real x1, real* V, real* dV) {
+  real t = (x - x0) / (x1 - x0);
+  real dp0 = dpdx0 * (x1 - x0);
+  *V = p0 + t * (dp0 + t * (-2 * dp0 - 3 * p0 + t * (dp0 + 2 * p0)));
+  *dV = (dp0 + t * (-4 * dp0 - 6 * p0 + t * (3 * dp0 + 6 * p0))) / (x1 - x0);
+}
+
+/* lj.hh:32-36 */
+static real vdw_V(real dist, real sigma, real epsilon) {
+  real sd = (sigma / dist);
+  real sd2 = sd * sd;
+  real sd6 = sd2 * sd2 * sd2;
+  real sd12 = sd6 * sd6;
+  return epsilon * (sd12 - 2 * sd6);
+}
+
+/* lj.hh:38-47 */
+static void vdw_V_dV(real dist, real sigma, real epsilon, real* V, real* dV) {
+  real sd = (sigma / dist);
+  real sd2 = sd * sd;
+  real sd6 = sd2 * sd2 * sd2;
+  real sd12 = sd6 * sd6;
+  *V = epsilon * (sd12 - (real)2.0 * sd6);
+  *dV = epsilon * (((real)-12.0 * sd12 / dist) - ((real)-12.0 * sd6 / dist));
+}
+
+/* lj.hh:65-113 (energy only) */
+void oracle_lj_score_V(real dist, real bonded_path_length,
+                       const type_params_t* i, const type_params_t* j,
+                       const global_params_t* g, real out[2]) {
+  real cpoly_dmax = g->max_dis;
+  real spline_start = g->max_dis - (real)1.5;
+  real weight, Vatr, Vrep;
+  if (dist > cpoly_dmax) {
+    Vatr = 0;
+    Vrep = 0;
+    weight = 0;
+  } else {
+    real sigma = lj_sigma(i, j, g);
+    real epsilon = rsqrt_(i->lj_wdepth * j->lj_wdepth);
+    real d_lin = sigma * g->lj_dlin_sigma_factor;
+    real cpoly_dmin =
+        sigma > spline_start
+            ? (sigma > cpoly_dmax - (real)0.1 ? cpoly_dmax - (real)0.1 : sigma)
+            : spline_start;
+    weight = connectivity_weight((int)bonded_path_length);
+    if (dist > cpoly_dmin) {
+      real v0, dv0;
+      vdw_V_dV(cpoly_dmin, sigma, epsilon, &v0, &dv0);
+      Vatr = interpolate_to_zero(dist, cpoly_dmin, v0, dv0, cpoly_dmax);
+    } else if (dist > d_lin) {
+      Vatr = vdw_V(dist, sigma, epsilon);
+    } else {
+      real v0, dv0;
+      vdw_V_dV(d_lin, sigma, epsilon, &v0, &dv0);
+      Vatr = (v0 + dv0 * (dist - d_lin));
+    }
+    if (dist < sigma) {
+      Vrep = Vatr + epsilon;
+      Vatr = -epsilon;
+    } else {
+      Vrep = 0;
+    }
+  }
+  out[0] = weight * Vatr;
+  out[1] = weight * Vrep;
+}
+
+/* lj.hh:115-177: out = {Vatr, Vrep, dVatr/dd, dVrep/dd} */
+void oracle_lj_score_V_dV(real dist, real bonded_path_length,
+                          const type_params_t* i, const type_params_t* j,
+                          const global_params_t* g, real out[4]) {
+  real sigma = lj_sigma(i, j, g);
+  real weight = connectivity_weight((int)bonded_path_length);
+  real epsilon = rsqrt_(i->lj_wdepth * j->lj_wdepth);
+  real d_lin = sigma * g->lj_dlin_sigma_factor;
+  real cpoly_dmax = g->max_dis;
+  real cpoly_dmin = g->max_dis - (real)1.5;
+  if (sigma > cpoly_dmin) cpoly_dmin = sigma;
+  if (cpoly_dmin > cpoly_dmax - (real)0.1) cpoly_dmin = cpoly_dmax - (real)0.1;
+  real lj, dlj;
+  if (dist < d_lin) {
+    real v0, dv0;
+    vdw_V_dV(d_lin, sigma, epsilon, &v0, &dv0);
+    lj = v0 + dv0 * (dist - d_lin);
+    dlj = dv0;
+  } else if (dist < cpoly_dmin) {
+    vdw_V_dV(dist, sigma, epsilon, &lj, &dlj);
+  } else if (dist < cpoly_dmax) {
+    real v0, dv0;
+    vdw_V_dV(cpoly_dmin, sigma, epsilon, &v0, &dv0);
+    interpolate_to_zero_V_dV(dist, cpoly_dmin, v0, dv0, cpoly_dmax, &lj, &dlj);
+  } else {
+    lj = 0;
+    dlj = 0;
+  }
+  real Vatr, Vrep, dVatr, dVrep;
+  if (dist < sigma) {
+    Vatr = -epsilon;
+    Vrep = lj + epsilon;
+    dVatr = 0;
+    dVrep = dlj;
+  } else {
+    Vatr = lj;
+    Vrep = 0;
+    dVatr = dlj;
+    dVrep = 0;
+  }
+  out[0] = weight * Vatr;
+  out[1] = weight * Vrep;
+  out[2] = weight * dVatr;
+  out[3] = weight * dVrep;
+}
+
+static const real pi_pow1p5 = (real)5.56832799683f;
+
+/* lk_isotropic.hh:30-51 */
+static real f_desolv_V(real dist, real lj_radius_i, real lk_dgfree_i,
+                       real lk_lambda_i, real lk_volume_j) {
+  return (-lk_volume_j * lk_dgfree_i / (2 * pi_pow1p5 * lk_lambda_i) /
+          (dist * dist) *
+          rexp_(-(dist - lj_radius_i) * (dist - lj_radius_i) /
+                (lk_lambda_i * lk_lambda_i)));
+}
+
+/* lk_isotropic.hh:53-94 */
+static void f_desolv_V_dV(real dist, real lj_radius_i, real lk_dgfree_i,
+                          real lk_lambda_i, real lk_volume_j, real* V,
+                          real* dV) {
+  real exp_val = rexp_(-(dist - lj_radius_i) * (dist - lj_radius_i) /
+                       (lk_lambda_i * lk_lambda_i));
+  *V = (-lk_volume_j * lk_dgfree_i / (2 * pi_pow1p5 * lk_lambda_i) /
+        (dist * dist) * exp_val);
+  *dV = (-lk_volume_j * lk_dgfree_i / (2 * pi_pow1p5 * lk_lambda_i) * exp_val *
+         ((-2 / (dist * dist * dist)) +
+          (1 / (dist * dist) * -(2 * dist - 2 * lj_radius_i) /
+           (lk_lambda_i * lk_lambda_i))));
+}
+
+/* close-spline knots, lk_isotropic.hh:132-143 */
+static void lk_knots(real lj_sigma_ij, int is_cc_pair, real* d_min,
+                     real* close_dmin, real* close_dmax) {
+  real dm = (real)(lj_sigma_ij * .89);
+  if (is_cc_pair) dm = rmax_(dm, (real)4.2);
+  real n = rfloor_((real)20 * dm * dm);
+  *d_min = dm;
+  *close_dmin = rsqrt_(rmax_((real)0, n - 29) / 20);
+  *close_dmax = rsqrt_(rmin_(n + 21, (real)405) / 20);
+}
+
+/* lk_isotropic.hh:167-236 */
+static void lk_isotropic_pair_V_dV(real dist, real bonded_path_length,
+                                   real lj_sigma_ij, real lj_radius_i,
+                                   real lk_dgfree_i, real lk_lambda_i,
+                                   real lk_volume_j, real max_dis,
+                                   int is_cc_pair, real* V, real* dV) {
+  real d_min, close_dmin, close_dmax;
+  lk_knots(lj_sigma_ij, is_cc_pair, &d_min, &close_dmin, &close_dmax);
+  real far_dmax = max_dis;
+  real far_dmin = max_dis - (real)1.5;
+  real weight = connectivity_weight((int)bonded_path_length);
+  real lk, dlk;
+  if (dist < close_dmin) {
+    lk = f_desolv_V(d_min, lj_radius_i, lk_dgfree_i, lk_lambda_i, lk_volume_j);
+    dlk = 0;
+  } else if (dist < close_dmax) {
+    real v1, dv1;
+    f_desolv_V_dV(close_dmax, lj_radius_i, lk_dgfree_i, lk_lambda_i,
+                  lk_volume_j, &v1, &dv1);
+    interpolate_V_dV(
+        dist, close_dmin,
+        f_desolv_V(d_min, lj_radius_i, lk_dgfree_i, lk_lambda_i, lk_volume_j),
+        (real)0.0, close_dmax, v1, dv1, &lk, &dlk);
+  } else if (dist < far_dmin) {
+    f_desolv_V_dV(dist, lj_radius_i, lk_dgfree_i, lk_lambda_i, lk_volume_j,
+                  &lk, &dlk);
+  } else if (dist < far_dmax) {
+    real v0, dv0;
+    f_desolv_V_dV(far_dmin, lj_radius_i, lk_dgfree_i, lk_lambda_i, lk_volume_j,
+                  &v0, &dv0);
+    interpolate_to_zero_V_dV(dist, far_dmin, v0, dv0, far_dmax, &lk, &dlk);
+  } else {
+    lk = 0;
+    dlk = 0;
+  }
+  *V = weight * lk;
+  *dV = weight * dlk;
+}
+
+/* lk_isotropic.hh:248-326 (energy only) */
+real oracle_lk_score_V(real dist, real bonded_path_length,
+                       const type_params_t* i, const type_params_t* j,
+                       const global_params_t* g) {
+  real sigma = lj_sigma(i, j, g);
+  int is_cc = (i->is_carbon_lk != 0) && (j->is_carbon_lk != 0);
+  real d_min, close_dmin, close_dmax;
+  lk_knots(sigma, is_cc, &d_min, &close_dmin, &close_dmax);
+  real far_dmax = g->max_dis;
+  real far_dmin = g->max_dis - (real)1.5;
+  real weight = connectivity_weight((int)bonded_path_length);
+  real lk;
+  if (dist > far_dmax) {
+    lk = 0;
+  } else if (dist > far_dmin) {
+    real v0, dv0;
+    f_desolv_V_dV(far_dmin, i->lj_radius, i->lk_dgfree, i->lk_lambda,
+                  j->lk_volume, &v0, &dv0);
+    lk = interpolate_to_zero(dist, far_dmin, v0, dv0, far_dmax);
+    f_desolv_V_dV(far_dmin, j->lj_radius, j->lk_dgfree, j->lk_lambda,
+                  i->lk_volume, &v0, &dv0);
+    lk += interpolate_to_zero(dist, far_dmin, v0, dv0, far_dmax);
+  } else if (dist > close_dmax) {
+    lk = f_desolv_V(dist, i->lj_radius, i->lk_dgfree, i->lk_lambda,
+                    j->lk_volume) +
+         f_desolv_V(dist, j->lj_radius, j->lk_dgfree, j->lk_lambda,
+                    i->lk_volume);
+  } else if (dist > close_dmin) {
+    real v1, dv1;
+    f_desolv_V_dV(close_dmax, i->lj_radius, i->lk_dgfree, i->lk_lambda,
+                  j->lk_volume, &v1, &dv1);
+    lk = interpolate(dist, close_dmin,
+                     f_desolv_V(d_min, i->lj_radius, i->lk_dgfree, i->lk_lambda,
+                                j->lk_volume),
+                     (real)0.0, close_dmax, v1, dv1);
+    f_desolv_V_dV(close_dmax, j->lj_radius, j->lk_dgfree, j->lk_lambda,
+                  i->lk_volume, &v1, &dv1);
+    lk += interpolate(dist, close_dmin,
+                      f_desolv_V(d_min, j->lj_radius, j->lk_dgfree,
+                                 j->lk_lambda, i->lk_volume),
+                      (real)0.0, close_dmax, v1, dv1);
+  } else {
+    lk = f_desolv_V(d_min, i->lj_radius, i->lk_dgfree, i->lk_lambda,
+                    j->lk_volume) +
+         f_desolv_V(d_min, j->lj_radius, j->lk_dgfree, j->lk_lambda,
+                    i->lk_volume);
+  }
+  return weight * lk;
+}
+
+/* lk_isotropic.hh:328-361: out = {V, dV/dd} */
+void oracle_lk_score_V_dV(real dist, real bonded_path_length,
+                          const type_params_t* i, const type_params_t* j,
+                          const global_params_t* g, real out[2]) {
+  real sigma = lj_sigma(i, j, g);
+  int is_cc = (i->is_carbon_lk != 0) && (j->is_carbon_lk != 0);
+  real v1, d1, v2, d2;
+  lk_isotropic_pair_V_dV(dist, bonded_path_length, sigma, i->lj_radius,
+                         i->lk_dgfree, i->lk_lambda, j->lk_volume, g->max_dis,
+                         is_cc, &v1, &d1);
+  lk_isotropic_pair_V_dV(dist, bonded_path_length, sigma, j->lj_radius,
+                         j->lk_dgfree, j->lk_lambda, i->lk_volume, g->max_dis,
+                         is_cc, &v2, &d2);
+  out[0] = v1 + v2;
+  out[1] = d1 + d2;
+}
+
+/* ---------------------------------------------------------------------- */
+/* Pose scoring.                                                           */
+
+typedef struct {
+  /* inputs (row-major, int32 tables, `real` floats) */
+  const real* coords; /* [n_atoms][3] */
+  const int32_t* rot_coord_offset;      /* [n_rots] */
+  const int32_t* first_rot_block_type;  /* [P][B] */
+  const int32_t* block_ind_for_rot;     /* [n_rots] */
+  const int32_t* pose_ind_for_rot;      /* [n_rots] */
+  const int32_t* block_type_ind_for_rot;/* [n_rots] */
+  const int32_t* rot_offset_for_block;  /* [P][B] */
+  const int32_t* min_bondsep;           /* [P][B][B] */
+  const int32_t* inter_block_bondsep;   /* [P][B][B][C][C] */
+  const int32_t* bt_n_atoms;            /* [nbt] */
+  const int32_t* bt_n_heavy_in_tile;    /* [nbt][ntiles] */
+  const int32_t* bt_heavy_in_tile;      /* [nbt][32*ntiles] */
+  const int32_t* bt_atom_types;         /* [nbt][A] */
+  const int32_t* bt_n_conn;             /* [nbt] */
+  const int32_t* bt_conn_atom;          /* [nbt][C] */
+  const int32_t* bt_path_distance;      /* [nbt][A][A] */
+  const int32_t* bt_is_ligand;          /* [nbt] */
+  const real* type_params;              /* [T][10] */
+  const real* global_params;            /* [5] */
+  real max_dis;
+  int n_atoms, n_rots, P, B, nbt, A, C, ntiles, T;
+} oracle_inputs_t;
+
+typedef struct {
+  int pose, b1, b2, rot1, rot2, bt1, bt2, n1, n2, off1, off2;
+  int n_conn1, n_conn2, min_sep, striking;
+  unsigned char conn_ats1[MAX_N_CONN], conn_ats2[MAX_N_CONN];
+  unsigned char conn_seps[MAX_N_CONN * MAX_N_CONN];
+  int lig_pair;
+} pair_ctx_t;
+
+static const type_params_t* tparams(const oracle_inputs_t* in, int bt,
+                                    int atom) {
+  int t = in->bt_atom_types[bt * in->A + atom];
+  return (const type_params_t*)(in->type_params + 10 * (size_t)t);
+}
+
+/* count_pair.hh:162-207 + ljlk_pose_score.impl.hh:47-67 */
+static int inter_separation(const oracle_inputs_t* in, const pair_ctx_t* c,
+                            int a1, int a2) {
+  int sep = c->min_sep;
+  if (sep <= MAX_IMPORTANT_BOND_SEPARATION) {
+    sep = MAX_IMPORTANT_BOND_SEPARATION + 1;
+    for (int ii = 0; ii < c->n_conn1; ++ii) {
+      unsigned char pd1 = (unsigned char)in->bt_path_distance
+          [((size_t)c->bt1 * in->A + c->conn_ats1[ii]) * in->A + a1];
+      for (int jj = 0; jj < c->n_conn2; ++jj) {
+        int cs = c->conn_seps[ii * c->n_conn2 + jj];
+        unsigned char pd2 = (unsigned char)in->bt_path_distance
+            [((size_t)c->bt2 * in->A + c->conn_ats2[jj]) * in->A + a2];
+        int s = pd1 + cs + pd2;
+        if (s < sep) sep = s;
+      }
+    }
+  }
+  if (c->lig_pair && (sep == 3 || sep == 4)) sep = 5;
+  return sep;
+}
+
+static int intra_separation(const oracle_inputs_t* in, int bt, int a1,
+                            int a2) {
+  return in->bt_path_distance[((size_t)bt * in->A + a1) * in->A + a2];
+}
+
+/* geom.hh:20-40; Eigen's norm() sums the squares as x^2 + (y^2 + z^2) */
+static void dist_and_grad(const real* x1, const real* x2, real* d,
+                          real g1[3]) {
+  real dx = x1[0] - x2[0], dy = x1[1] - x2[1], dz = x1[2] - x2[2];
+  real V = rsqrt_(dx * dx + (dy * dy + dz * dz));
+  *d = V;
+  if (V != 0) {
+    g1[0] = dx / V;
+    g1[1] = dy / V;
+    g1[2] = dz / V;
+  } else {
+    g1[0] = g1[1] = g1[2] = 0;
+  }
+}
+
+static void acc3(real* dst, const real* g, real s) {
+  for (int k = 0; k < 3; ++k) {
+    real v = s * g[k];
+    if (v != 0) dst[k] += v;
+  }
+}
+static void acc3_neg(real* dst, const real* g, real s) {
+  for (int k = 0; k < 3; ++k) {
+    real v = s * -g[k];
+    if (v != 0) dst[k] += v;
+  }
+}
+
+/* Modes of the per-atom-pair evaluation. */
+enum { MODE_ENERGY = 0, MODE_ENERGY_AND_DERIVS = 1, MODE_WEIGHTED_DERIVS = 2 };
+
+typedef struct {
+  int mode;
+  real* dV;       /* MODE 1: [3][n_atoms][3]; MODE 2: [n_atoms][3] */
+  real w[3];      /* MODE 2 weights for atr, rep, lk */
+} eval_t;
+
+static void eval_lj(const oracle_inputs_t* in, const eval_t* ev, int bt1,
+                    int a1, int at1, int bt2, int a2, int at2, int sep,
+                    real* atr, real* rep) {
+  const global_params_t* g = (const global_params_t*)in->global_params;
+  const real* x1 = in->coords + 3 * (size_t)at1;
+  const real* x2 = in->coords + 3 * (size_t)at2;
+  const type_params_t* t1 = tparams(in, bt1, a1);
+  const type_params_t* t2 = tparams(in, bt2, a2);
+  if (ev->mode == MODE_ENERGY) {
+    real dx = x1[0] - x2[0], dy = x1[1] - x2[1], dz = x1[2] - x2[2];
+    real d = rsqrt_(dx * dx + (dy * dy + dz * dz));
+    real out[2];
+    oracle_lj_score_V(d, (real)sep, t1, t2, g, out);
+    *atr = out[0];
+    *rep = out[1];
+    return;
+  }
+  real d, gr[3];
+  dist_and_grad(x1, x2, &d, gr);
+  real o[4];
+  oracle_lj_score_V_dV(d, (real)sep, t1, t2, g, o);
+  if (ev->mode == MODE_ENERGY_AND_DERIVS) {
+    size_t N3 = 3 * (size_t)in->n_atoms;
+    /* ljlk.hh:629-664: atom 1 (atr, rep per component), then atom 2 */
+    for (int k = 0; k < 3; ++k) {
+      real va = o[2] * gr[k];
+      real vr = o[3] * gr[k];
+      if (va != 0) ev->dV[0 * N3 + 3 * (size_t)at1 + k] += va;
+      if (vr != 0) ev->dV[1 * N3 + 3 * (size_t)at1 + k] += vr;
+    }
+    for (int k = 0; k < 3; ++k) {
+      real va = o[2] * -gr[k];
+      real vr = o[3] * -gr[k];
+      if (va != 0) ev->dV[0 * N3 + 3 * (size_t)at2 + k] += va;
+      if (vr != 0) ev->dV[1 * N3 + 3 * (size_t)at2 + k] += vr;
+    }
+  } else {
+    /* ljlk.hh:531-594 */
+    for (int k = 0; k < 3; ++k) {
+      real va = ev->w[0] * o[2] * gr[k];
+      real vr = ev->w[1] * o[3] * gr[k];
+      if (va != 0) ev->dV[3 * (size_t)at1 + k] += va;
+      if (vr != 0) ev->dV[3 * (size_t)at1 + k] += vr;
+    }
+    for (int k = 0; k < 3; ++k) {
+      real va = ev->w[0] * o[2] * -gr[k];
+      real vr = ev->w[1] * o[3] * -gr[k];
+      if (va != 0) ev->dV[3 * (size_t)at2 + k] += va;
+      if (vr != 0) ev->dV[3 * (size_t)at2 + k] += vr;
+    }
+  }
+  *atr = o[0];
+  *rep = o[1];
+}
+
+static real eval_lk(const oracle_inputs_t* in, const eval_t* ev, int bt1,
+                    int a1, int at1, int bt2, int a2, int at2, int sep) {
+  const global_params_t* g = (const global_params_t*)in->global_params;
+  const real* x1 = in->coords + 3 * (size_t)at1;
+  const real* x2 = in->coords + 3 * (size_t)at2;
+  const type_params_t* t1 = tparams(in, bt1, a1);
+  const type_params_t* t2 = tparams(in, bt2, a2);
+  if (ev->mode == MODE_ENERGY) {
+    real dx = x1[0] - x2[0], dy = x1[1] - x2[1], dz = x1[2] - x2[2];
+    real d = rsqrt_(dx * dx + (dy * dy + dz * dz));
+    return oracle_lk_score_V(d, (real)sep, t1, t2, g);
+  }
+  real d, gr[3];
+  dist_and_grad(x1, x2, &d, gr);
+  real o[2];
+  oracle_lk_score_V_dV(d, (real)sep, t1, t2, g, o);
+  if (ev->mode == MODE_ENERGY_AND_DERIVS) {
+    size_t N3 = 3 * (size_t)in->n_atoms;
+    acc3(ev->dV + 2 * N3 + 3 * (size_t)at1, gr, o[1]);
+    acc3_neg(ev->dV + 2 * N3 + 3 * (size_t)at2, gr, o[1]);
+  } else {
+    acc3(ev->dV + 3 * (size_t)at1, gr, ev->w[2] * o[1]);
+    acc3_neg(ev->dV + 3 * (size_t)at2, gr, ev->w[2] * o[1]);
+  }
+  return o[0];
+}
+
+/* One work group of the pose kernel: all atom pairs of one block pair,
+ * walked tile by tile (tile_atom_pair_evaluation.hh:358-505).  Returns the
+ * three block-pair totals. */
+static void eval_block_pair(const oracle_inputs_t* in, const eval_t* ev,
+                            const pair_ctx_t* c, real tot[3]) {
+  real t_atr = 0, t_rep = 0, t_lk = 0;
+  int nt_tiles = in->ntiles;
+  if (c->b1 != c->b2) {
+    int n_it1 = (c->n1 - 1) / TILE + 1;
+    int n_it2 = (c->n2 - 1) / TILE + 1;
+    for (int i = 0; i < n_it1; ++i) {
+      int s1 = TILE * i;
+      int nr1 = c->n1 - s1 < TILE ? c->n1 - s1 : TILE;
+      int nh1 = in->bt_n_heavy_in_tile[c->bt1 * nt_tiles + i];
+      for (int j = 0; j < n_it2; ++j) {
+        int s2 = TILE * j;
+        int nr2 = c->n2 - s2 < TILE ? c->n2 - s2 : TILE;
+        int nh2 = in->bt_n_heavy_in_tile[c->bt2 * nt_tiles + j];
+        real la = 0, lr = 0, lk = 0;
+        for (int k = 0; k < nr1 * nr2; ++k) {
+          int a1 = s1 + k / nr2, a2 = s2 + k % nr2;
+          int sep = inter_separation(in, c, a1, a2);
+          real atr, rep;
+          eval_lj(in, ev, c->bt1, a1, c->off1 + a1, c->bt2, a2, c->off2 + a2,
+                  sep, &atr, &rep);
+          la += atr;
+          lr += rep;
+        }
+        t_atr += la;
+        t_rep += lr;
+        if (nh1 > 0 && nh2 > 0) {
+          for (int k = 0; k < nh1 * nh2; ++k) {
+            int h1 = k / nh2, h2 = k % nh2;
+            int a1 = s1 + in->bt_heavy_in_tile[c->bt1 * TILE * nt_tiles + s1 + h1];
+            int a2 = s2 + in->bt_heavy_in_tile[c->bt2 * TILE * nt_tiles + s2 + h2];
+            int sep = inter_separation(in, c, a1, a2);
+            lk += eval_lk(in, ev, c->bt1, a1, c->off1 + a1, c->bt2, a2,
+                          c->off2 + a2, sep);
+          }
+        }
+        t_lk += lk;
+      }
+    }
+  } else {
+    int n_it = (c->n1 - 1) / TILE + 1;
+    for (int i = 0; i < n_it; ++i) {
+      int s1 = TILE * i;
+      int nr1 = c->n1 - s1 < TILE ? c->n1 - s1 : TILE;
+      int nh1 = in->bt_n_heavy_in_tile[c->bt1 * nt_tiles + i];
+      for (int j = i; j < n_it; ++j) {
+        int s2 = TILE * j;
+        int nr2 = c->n1 - s2 < TILE ? c->n1 - s2 : TILE;
+        int nh2 = in->bt_n_heavy_in_tile[c->bt1 * nt_tiles + j];
+        real la = 0, lr = 0, lk = 0;
+        for (int k = 0; k < nr1 * nr2; ++k) {
+          int a1 = s1 + k / nr2, a2 = s2 + k % nr2;
+          if (a1 >= a2) continue;
+          int sep = intra_separation(in, c->bt1, a1, a2);
+          real atr, rep;
+          eval_lj(in, ev, c->bt1, a1, c->off1 + a1, c->bt1, a2, c->off1 + a2,
+                  sep, &atr, &rep);
+          la += atr;
+          lr += rep;
+        }
+        t_atr += la;
+        t_rep += lr;
+        if (nh1 > 0 && nh2 > 0) {
+          for (int k = 0; k < nh1 * nh2; ++k) {
+            int h1 = k / nh2, h2 = k % nh2;
+            if (h1 + s1 >= h2 + s2) continue;
+            int a1 = s1 + in->bt_heavy_in_tile[c->bt1 * TILE * nt_tiles + s1 + h1];
+            int a2 = s2 + in->bt_heavy_in_tile[c->bt1 * TILE * nt_tiles + s2 + h2];
+            int sep = intra_separation(in, c->bt1, a1, a2);
+            lk += eval_lk(in, ev, c->bt1, a1, c->off1 + a1, c->bt1, a2,
+                          c->off1 + a2, sep);
+          }
+        }
+        t_lk += lk;
+      }
+    }
+  }
+  tot[0] = t_atr;
+  tot[1] = t_rep;
+  tot[2] = t_lk;
+}
+
+/* sphere_overlap.impl.hh:109-196: per rotamer centroid + radius */
+static void compute_spheres(const oracle_inputs_t* in, real* spheres) {
+  for (size_t k = 0; k < (size_t)in->P * in->B * 4; ++k) spheres[k] = 0;
+  for (int r = 0; r < in->n_rots; ++r) {
+    int p = in->pose_ind_for_rot[r];
+    int b = in->block_ind_for_rot[r];
+    int bt = in->block_type_ind_for_rot[r];
+    int off = in->rot_coord_offset[r];
+    if (bt < 0) continue;
+    int n = in->bt_n_atoms[bt];
+    real c[3] = {0, 0, 0};
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k < 3; ++k) c[k] += in->coords[3 * (size_t)(off + i) + k];
+    for (int k = 0; k < 3; ++k) c[k] /= n;
+    real d2max = 0;
+    for (int i = 0; i < n; ++i) {
+      const real* x = in->coords + 3 * (size_t)(off + i);
+      real d2 = ((x[0] - c[0]) * (x[0] - c[0]) + (x[1] - c[1]) * (x[1] - c[1]) +
+                 (x[2] - c[2]) * (x[2] - c[2]));
+      if (d2 > d2max) d2max = d2;
+    }
+    real* s = spheres + 4 * ((size_t)p * in->B + b);
+    s[0] = c[0];
+    s[1] = c[1];
+    s[2] = c[2];
+    s[3] = rsqrt_(d2max);
+  }
+}
+
+/* sphere_overlap.impl.hh:287-351 */
+static void detect_neighbors(const oracle_inputs_t* in, const real* spheres,
+                             int32_t* nbr) {
+  int B = in->B;
+  memset(nbr, 0, sizeof(int32_t) * (size_t)in->P * B * B);
+  for (int p = 0; p < in->P; ++p)
+    for (int i = 0; i < B; ++i)
+      for (int j = i; j < B; ++j) {
+        if (in->first_rot_block_type[p * B + i] < 0) continue;
+        if (in->first_rot_block_type[p * B + j] < 0) continue;
+        const real* s1 = spheres + 4 * ((size_t)p * B + i);
+        const real* s2 = spheres + 4 * ((size_t)p * B + j);
+        real d2 = ((s1[0] - s2[0]) * (s1[0] - s2[0]) +
+                   (s1[1] - s2[1]) * (s1[1] - s2[1]) +
+                   (s1[2] - s2[2]) * (s1[2] - s2[2]));
+        real thr = s1[3] + s2[3] + in->max_dis;
+        if (d2 < thr * thr) nbr[((size_t)p * B + i) * B + j] = 1;
+      }
+}
+
+static int setup_pair(const oracle_inputs_t* in, int p, int b1, int b2,
+                      pair_ctx_t* c) {
+  int B = in->B;
+  c->pose = p;
+  c->b1 = b1;
+  c->b2 = b2;
+  c->rot1 = in->rot_offset_for_block[p * B + b1];
+  c->rot2 = in->rot_offset_for_block[p * B + b2];
+  if (c->rot1 < 0 || c->rot2 < 0) return 0;
+  c->bt1 = in->block_type_ind_for_rot[c->rot1];
+  c->bt2 = in->block_type_ind_for_rot[c->rot2];
+  if (c->bt1 < 0 || c->bt2 < 0) return 0;
+  c->n1 = in->bt_n_atoms[c->bt1];
+  c->n2 = in->bt_n_atoms[c->bt2];
+  c->off1 = in->rot_coord_offset[c->rot1];
+  c->off2 = in->rot_coord_offset[c->rot2];
+  c->n_conn1 = in->bt_n_conn[c->bt1];
+  c->n_conn2 = in->bt_n_conn[c->bt2];
+  c->min_sep = in->min_bondsep[((size_t)p * B + b1) * B + b2];
+  c->striking = c->min_sep <= MAX_IMPORTANT_BOND_SEPARATION;
+  c->lig_pair = in->bt_is_ligand[c->bt1] && in->bt_is_ligand[c->bt2];
+  if (c->striking) {
+    for (int k = 0; k < c->n_conn1; ++k)
+      c->conn_ats1[k] = (unsigned char)in->bt_conn_atom[c->bt1 * in->C + k];
+    for (int k = 0; k < c->n_conn2; ++k)
+      c->conn_ats2[k] = (unsigned char)in->bt_conn_atom[c->bt2 * in->C + k];
+    for (int k1 = 0; k1 < c->n_conn1; ++k1)
+      for (int k2 = 0; k2 < c->n_conn2; ++k2)
+        c->conn_seps[k1 * c->n_conn2 + k2] =
+            (unsigned char)in->inter_block_bondsep
+                [((((size_t)p * B + b1) * B + b2) * in->C + k1) * in->C + k2];
+  }
+  return 1;
+}
+
+/*
+ * The pose-score op forward (ljlk_pose_score.impl.hh:628-1158).
+ *   block_pair == 0: out_E[3][P] (whole pose); if out_dV != NULL, the
+ *     per-term gradients [3][n_atoms][3] are accumulated and energies use the
+ *     V_dV evaluators, as the reference does when coords require grad.
+ *   block_pair != 0: out_E[3][P][B][B], energies only.
+ *   out_nbr[P][B][B] receives the block-neighbour matrix.
+ */
+int oracle_ljlk_pose_scores(const oracle_inputs_t* in, int block_pair,
+                            real* out_E, real* out_dV, int32_t* out_nbr) {
+  int P = in->P, B = in->B;
+  real* spheres = (real*)malloc(sizeof(real) * 4 * (size_t)P * B + 16);
+  if (!spheres) return 1;
+  compute_spheres(in, spheres);
+  detect_neighbors(in, spheres, out_nbr);
+  free(spheres);
+  size_t n_out = block_pair ? (size_t)3 * P * B * B : (size_t)3 * P;
+  for (size_t k = 0; k < n_out; ++k) out_E[k] = 0;
+  eval_t ev;
+  ev.mode = (!block_pair && out_dV) ? MODE_ENERGY_AND_DERIVS : MODE_ENERGY;
+  ev.dV = out_dV;
+  if (out_dV && !block_pair)
+    for (size_t k = 0; k < (size_t)9 * in->n_atoms; ++k) out_dV[k] = 0;
+  for (int p = 0; p < P; ++p)
+    for (int b1 = 0; b1 < B; ++b1)
+      for (int b2 = b1; b2 < B; ++b2) {
+        if (out_nbr[((size_t)p * B + b1) * B + b2] == 0) continue;
+        pair_ctx_t c;
+        if (!setup_pair(in, p, b1, b2, &c)) continue;
+        real tot[3];
+        eval_block_pair(in, &ev, &c, tot);
+        for (int t = 0; t < 3; ++t) {
+          if (block_pair)
+            out_E[(((size_t)t * P + p) * B + b1) * B + b2] = tot[t];
+          else
+            out_E[(size_t)t * P + p] += tot[t];
+        }
+      }
+  return 0;
+}
+
+/*
+ * Recompute adjoint: dL/dx[n_atoms][3] = sum over neighbouring block pairs
+ * (b1 <= b2) of dTdV[t][p][b1][b2] * dE_t(b1, b2)/dx, as the reference's
+ * block-pair backward (ljlk_pose_score.impl.hh:1160-1477).  With
+ * per_pose_weights != 0, dTdV is [3][P] and applies to every block pair of
+ * the pose (the whole-pose adjoint).
+ */
+int oracle_ljlk_backward(const oracle_inputs_t* in, const int32_t* nbr,
+                         const real* dTdV, int per_pose_weights, real* out_dx) {
+  int P = in->P, B = in->B;
+  for (size_t k = 0; k < (size_t)3 * in->n_atoms; ++k) out_dx[k] = 0;
+  eval_t ev;
+  ev.mode = MODE_WEIGHTED_DERIVS;
+  ev.dV = out_dx;
+  for (int p = 0; p < P; ++p)
+    for (int b1 = 0; b1 < B; ++b1)
+      for (int b2 = b1; b2 < B; ++b2) {
+        if (nbr[((size_t)p * B + b1) * B + b2] == 0) continue;
+        pair_ctx_t c;
+        if (!setup_pair(in, p, b1, b2, &c)) continue;
+        for (int t = 0; t < 3; ++t)
+          ev.w[t] = per_pose_weights
+                        ? dTdV[(size_t)t * P + p]
+                        : dTdV[(((size_t)t * P + p) * B + b1) * B + b2];
+        real tot[3];
+        eval_block_pair(in, &ev, &c, tot);
+      }
+  return 0;
+}
+
+/* Number of atom pairs and heavy-atom pairs the neighbour list covers: the
+ * benchmark's unit of work (inter: n1*n2, intra: n(n-1)/2). */
+void oracle_count_pairs(const oracle_inputs_t* in, const int32_t* nbr,
+                        int64_t* atom_pairs, int64_t* heavy_pairs) {
+  int64_t ap = 0, hp = 0;
+  int P = in->P, B = in->B;
+  for (int p = 0; p < P; ++p)
+    for (int b1 = 0; b1 < B; ++b1)
+      for (int b2 = b1; b2 < B; ++b2) {
+        if (nbr[((size_t)p * B + b1) * B + b2] == 0) continue;
+        pair_ctx_t c;
+        if (!setup_pair(in, p, b1, b2, &c)) continue;
+        int h1 = 0, h2 = 0;
+        for (int t = 0; t < in->ntiles; ++t) {
+          h1 += in->bt_n_heavy_in_tile[c.bt1 * in->ntiles + t];
+          h2 += in->bt_n_heavy_in_tile[c.bt2 * in->ntiles + t];
+        }
+        if (b1 != b2) {
+          ap += (int64_t)c.n1 * c.n2;
+          hp += (int64_t)h1 * h2;
+        } else {
+          ap += (int64_t)c.n1 * (c.n1 - 1) / 2;
+          hp += (int64_t)h1 * (h1 - 1) / 2;
+        }
+      }
+  *atom_pairs = ap;
+  *heavy_pairs = hp;
+}
+
+int oracle_sizeof_real(void) { return (int)sizeof(real); }

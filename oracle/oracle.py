@@ -1,0 +1,255 @@
+"""ctypes front end of the C oracle (``oracle/ljlk_oracle.c``) and of the
+compiled reference op (``oracle/_ref``).
+
+Test infrastructure only: tests, ``__graft_entry__.smoke()`` and the
+benchmark's CPU-baseline leg import this module, as the checker.  The
+product never does.
+
+Arguments follow the reference op's order (``tmol/score/ljlk/potentials/
+compiled.ops.cpp:533-597``): ``coords`` then the 26-item tail that
+``tmol_b200.score.ljlk_energy_term.pose_score_args`` returns.
+"""
+
+import ctypes
+import os
+import subprocess
+
+import numpy
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIBS = {}
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def _lib(f64):
+    key = "f64" if f64 else "f32"
+    if key not in _LIBS:
+        path = os.path.join(HERE, f"liboracle_ljlk_{key}.so")
+        if not os.path.exists(path):
+            build()
+        lib = ctypes.CDLL(path)
+        _LIBS[key] = lib
+    return _LIBS[key]
+
+
+def _inputs_struct(real_t):
+    P = ctypes.POINTER
+    i32p = P(ctypes.c_int32)
+    rp = P(real_t)
+
+    class Inputs(ctypes.Structure):
+        _fields_ = [
+            ("coords", rp),
+            ("rot_coord_offset", i32p),
+            ("first_rot_block_type", i32p),
+            ("block_ind_for_rot", i32p),
+            ("pose_ind_for_rot", i32p),
+            ("block_type_ind_for_rot", i32p),
+            ("rot_offset_for_block", i32p),
+            ("min_bondsep", i32p),
+            ("inter_block_bondsep", i32p),
+            ("bt_n_atoms", i32p),
+            ("bt_n_heavy_in_tile", i32p),
+            ("bt_heavy_in_tile", i32p),
+            ("bt_atom_types", i32p),
+            ("bt_n_conn", i32p),
+            ("bt_conn_atom", i32p),
+            ("bt_path_distance", i32p),
+            ("bt_is_ligand", i32p),
+            ("type_params", rp),
+            ("global_params", rp),
+            ("max_dis", real_t),
+            ("n_atoms", ctypes.c_int),
+            ("n_rots", ctypes.c_int),
+            ("P", ctypes.c_int),
+            ("B", ctypes.c_int),
+            ("nbt", ctypes.c_int),
+            ("A", ctypes.c_int),
+            ("C", ctypes.c_int),
+            ("ntiles", ctypes.c_int),
+            ("T", ctypes.c_int),
+        ]
+
+    return Inputs
+
+
+class OracleCall:
+    """Holds contiguous numpy copies of one op call's inputs and the ctypes
+    struct pointing at them."""
+
+    def __init__(self, coords, args, f64=False):
+        self.f64 = f64
+        self.np_real = numpy.float64 if f64 else numpy.float32
+        real_t = ctypes.c_double if f64 else ctypes.c_float
+        self.real_t = real_t
+        (
+            rot_coord_offset,
+            _pose_ind_for_atom,
+            _first_rot_for_block,
+            first_rot_block_type,
+            block_ind_for_rot,
+            pose_ind_for_rot,
+            block_type_ind_for_rot,
+            _n_rots_for_pose,
+            _rot_offset_for_pose,
+            _n_rots_for_block,
+            rot_offset_for_block,
+            _max_n_rots_per_pose,
+            min_bondsep,
+            inter_block_bondsep,
+            bt_n_atoms,
+            bt_n_heavy_in_tile,
+            bt_heavy_in_tile,
+            bt_atom_types,
+            bt_n_conn,
+            bt_conn_atom,
+            bt_path_distance,
+            bt_is_ligand,
+            type_params,
+            global_params,
+            max_dis,
+        ) = args[:25]
+        self.keep = []
+
+        def i32(t):
+            a = numpy.ascontiguousarray(t.detach().cpu().numpy().astype(numpy.int32))
+            self.keep.append(a)
+            return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+
+        def rl(t):
+            a = numpy.ascontiguousarray(t.detach().cpu().numpy().astype(self.np_real))
+            self.keep.append(a)
+            return a.ctypes.data_as(ctypes.POINTER(real_t))
+
+        Inputs = _inputs_struct(real_t)
+        s = Inputs()
+        s.coords = rl(coords.reshape(-1, 3))
+        s.rot_coord_offset = i32(rot_coord_offset)
+        s.first_rot_block_type = i32(first_rot_block_type)
+        s.block_ind_for_rot = i32(block_ind_for_rot)
+        s.pose_ind_for_rot = i32(pose_ind_for_rot)
+        s.block_type_ind_for_rot = i32(block_type_ind_for_rot)
+        s.rot_offset_for_block = i32(rot_offset_for_block)
+        s.min_bondsep = i32(min_bondsep)
+        s.inter_block_bondsep = i32(inter_block_bondsep)
+        s.bt_n_atoms = i32(bt_n_atoms)
+        s.bt_n_heavy_in_tile = i32(bt_n_heavy_in_tile)
+        s.bt_heavy_in_tile = i32(bt_heavy_in_tile)
+        s.bt_atom_types = i32(bt_atom_types)
+        s.bt_n_conn = i32(bt_n_conn)
+        s.bt_conn_atom = i32(bt_conn_atom)
+        s.bt_path_distance = i32(bt_path_distance)
+        s.bt_is_ligand = i32(bt_is_ligand)
+        s.type_params = rl(type_params)
+        s.global_params = rl(global_params.reshape(-1))
+        s.max_dis = float(max_dis)
+        s.n_atoms = coords.reshape(-1, 3).shape[0]
+        s.n_rots = rot_coord_offset.shape[0]
+        s.P = first_rot_block_type.shape[0]
+        s.B = first_rot_block_type.shape[1]
+        s.nbt = bt_n_atoms.shape[0]
+        s.A = bt_atom_types.shape[1]
+        s.C = bt_conn_atom.shape[1]
+        s.ntiles = bt_n_heavy_in_tile.shape[1]
+        s.T = type_params.shape[0]
+        self.s = s
+        self.P, self.B, self.N = s.P, s.B, s.n_atoms
+
+    def _ptr(self, a):
+        return a.ctypes.data_as(ctypes.c_void_p)
+
+    def pose_scores(self, block_pair=False, require_gradient=False):
+        """Returns (E [3, P] or [3, P, B, B], dV [3, N, 3] or None, nbr [P, B, B])."""
+        lib = _lib(self.f64)
+        P, B, N = self.P, self.B, self.N
+        E = numpy.zeros((3, P, B, B) if block_pair else (3, P), dtype=self.np_real)
+        nbr = numpy.zeros((P, B, B), dtype=numpy.int32)
+        dV = numpy.zeros((3, N, 3), dtype=self.np_real) if (require_gradient and not block_pair) else None
+        rc = lib.oracle_ljlk_pose_scores(
+            ctypes.byref(self.s),
+            ctypes.c_int(int(block_pair)),
+            self._ptr(E),
+            self._ptr(dV) if dV is not None else ctypes.c_void_p(0),
+            self._ptr(nbr),
+        )
+        assert rc == 0
+        return E, dV, nbr
+
+    def backward(self, nbr, dTdV, per_pose_weights):
+        lib = _lib(self.f64)
+        w = numpy.ascontiguousarray(numpy.asarray(dTdV, dtype=self.np_real))
+        nb = numpy.ascontiguousarray(nbr.astype(numpy.int32))
+        out = numpy.zeros((self.N, 3), dtype=self.np_real)
+        rc = lib.oracle_ljlk_backward(
+            ctypes.byref(self.s), self._ptr(nb), self._ptr(w), ctypes.c_int(int(per_pose_weights)), self._ptr(out)
+        )
+        assert rc == 0
+        return out
+
+    def count_pairs(self, nbr):
+        lib = _lib(self.f64)
+        nb = numpy.ascontiguousarray(nbr.astype(numpy.int32))
+        ap = ctypes.c_int64()
+        hp = ctypes.c_int64()
+        lib.oracle_count_pairs(ctypes.byref(self.s), self._ptr(nb), ctypes.byref(ap), ctypes.byref(hp))
+        return ap.value, hp.value
+
+
+def potential(name, dist, sep, tp_i, tp_j, gp, f64=True):
+    """Scalar potentials: name in {lj_V, lj_V_dV, lk_V, lk_V_dV}."""
+    lib = _lib(f64)
+    npr = numpy.float64 if f64 else numpy.float32
+    real_t = ctypes.c_double if f64 else ctypes.c_float
+    ti = numpy.ascontiguousarray(numpy.asarray(tp_i, dtype=npr))
+    tj = numpy.ascontiguousarray(numpy.asarray(tp_j, dtype=npr))
+    g = numpy.ascontiguousarray(numpy.asarray(gp, dtype=npr).reshape(-1))
+    vp = ctypes.c_void_p
+    if name == "lk_V":
+        f = lib.oracle_lk_score_V
+        f.restype = real_t
+        return float(
+            f(real_t(dist), real_t(sep), vp(ti.ctypes.data), vp(tj.ctypes.data), vp(g.ctypes.data))
+        )
+    n_out = {"lj_V": 2, "lj_V_dV": 4, "lk_V_dV": 2}[name]
+    out = numpy.zeros(n_out, dtype=npr)
+    f = {
+        "lj_V": lib.oracle_lj_score_V,
+        "lj_V_dV": lib.oracle_lj_score_V_dV,
+        "lk_V_dV": lib.oracle_lk_score_V_dV,
+    }[name]
+    f(real_t(dist), real_t(sep), vp(ti.ctypes.data), vp(tj.ctypes.data), vp(g.ctypes.data), vp(out.ctypes.data))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# The compiled reference op (built by oracle/build_ref.py into oracle/_ref).
+
+REF_LIB = os.path.join(HERE, "_ref", "tmol_ljlk_ref.so")
+_ref_loaded = False
+
+
+def reference_available():
+    return os.path.exists(REF_LIB)
+
+
+def load_reference():
+    global _ref_loaded
+    if not _ref_loaded:
+        torch.ops.load_library(REF_LIB)
+        _ref_loaded = True
+    return torch.ops.tmol_ljlk.ljlk_pose_scores
+
+
+def reference_pose_scores(coords, args, require_gradient=True):
+    """Runs the reference CPU op: returns (E, dE/dx or None, nbr)."""
+    op = load_reference()
+    cpu_args = [a.cpu() if isinstance(a, torch.Tensor) else a for a in args]
+    c = coords.detach().cpu().reshape(-1, 3).clone()
+    if require_gradient:
+        c.requires_grad_(True)
+    E, nbr = op(c, *cpu_args)
+    return E, c, nbr
