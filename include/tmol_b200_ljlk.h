@@ -1,0 +1,170 @@
+/*
+ * tmol_b200_ljlk: B200 (sm_100a) LJ + LK pose scoring behind a C ABI.
+ *
+ * The inputs are the tensors of tmol's pose-score op
+ * ``torch.ops.tmol_ljlk.ljlk_pose_scores``
+ * (tmol/score/ljlk/potentials/compiled.ops.cpp:533-597, registered at :667-670),
+ * passed as device pointers with their sizes.  All integer tables are int32,
+ * row-major and contiguous; real tables are float32 (or float64 through the
+ * *_f64 entry points).
+ *
+ * Life cycle:
+ *   tmol_b200_ljlk_plan_create   once per PoseStack (reads the static tables,
+ *                                derives compact count-pair / parameter
+ *                                tables, allocates scratch; synchronises the
+ *                                stream once to validate indices)
+ *   tmol_b200_ljlk_forward       energies (whole-pose [3, P] or block-pair
+ *                                [3, P, B, B]) and, optionally, the dense
+ *                                block-neighbour matrix [P, B, B]
+ *   tmol_b200_ljlk_backward      recompute adjoint: dL/dcoords [N, 3] from
+ *                                dL/dE ([3, P] or [3, P, B, B])
+ *   tmol_b200_ljlk_plan_destroy
+ *
+ * forward/backward enqueue work on `stream`, allocate nothing and never
+ * synchronise; a plan owns scratch memory, so one plan must not be used by
+ * two streams at once.  Every function returns a tmol_b200_status code.
+ */
+#ifndef TMOL_B200_LJLK_H
+#define TMOL_B200_LJLK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  TMOL_B200_OK = 0,
+  TMOL_B200_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad flag */
+  TMOL_B200_ERR_SHAPE = 2,            /* inconsistent or unsupported sizes */
+  TMOL_B200_ERR_INDEX_RANGE = 3,      /* a table holds an out-of-range index */
+  TMOL_B200_ERR_CAPACITY = 4,         /* a fixed-capacity table overflowed */
+  TMOL_B200_ERR_CUDA = 5,             /* a CUDA runtime call failed */
+  TMOL_B200_ERR_DTYPE = 6             /* plan and call disagree on float width */
+} tmol_b200_status;
+
+/* Device pointers and sizes of the op's static arguments (everything but
+ * the coordinates and the output-mode flag).  Names and meanings follow the
+ * reference op (compiled.ops.cpp:33-60):
+ *   n_poses = P, max_n_blocks = B, n_rots = P * B (one rotamer per block),
+ *   n_block_types = nbt, max_n_block_atoms = A, max_n_conn = C,
+ *   max_n_tiles = ceil(A / 32), n_atom_types = T. */
+typedef struct {
+  int64_t n_atoms; /* rows of rot_coords */
+  int32_t n_poses, max_n_blocks, n_rots;
+  int32_t n_block_types, max_n_block_atoms, max_n_conn, max_n_tiles;
+  int32_t n_atom_types;
+
+  const int32_t* rot_coord_offset;       /* [n_rots] */
+  const int32_t* pose_ind_for_atom;      /* [n_atoms] (validated, unused) */
+  const int32_t* first_rot_for_block;    /* [P, B] */
+  const int32_t* first_rot_block_type;   /* [P, B], -1 = no block */
+  const int32_t* block_ind_for_rot;      /* [n_rots] */
+  const int32_t* pose_ind_for_rot;       /* [n_rots] */
+  const int32_t* block_type_ind_for_rot; /* [n_rots] */
+  const int32_t* n_rots_for_pose;        /* [P] */
+  const int32_t* rot_offset_for_pose;    /* [P] */
+  const int32_t* n_rots_for_block;       /* [P, B] */
+  const int32_t* rot_offset_for_block;   /* [P, B] */
+  int32_t max_n_rots_per_pose;
+
+  const int32_t* min_bondsep;         /* [P, B, B] */
+  const int32_t* inter_block_bondsep; /* [P, B, B, C, C] */
+  const int32_t* bt_n_atoms;          /* [nbt] */
+  const int32_t* bt_n_heavy_atoms_in_tile; /* [nbt, max_n_tiles] */
+  const int32_t* bt_heavy_atoms_in_tile;   /* [nbt, 32 * max_n_tiles] */
+  const int32_t* bt_atom_types;       /* [nbt, A] */
+  const int32_t* bt_n_conn;           /* [nbt] */
+  const int32_t* bt_conn_atom;        /* [nbt, C] */
+  const int32_t* bt_path_distance;    /* [nbt, A, A] */
+  const int32_t* bt_is_ligand_fragment; /* [nbt] */
+  const void* type_params;   /* [T, 10] float or double */
+  const void* global_params; /* [1, 5] float or double */
+  double max_dis;            /* neighbour-detection reach */
+} tmol_b200_ljlk_inputs;
+
+/* Launch shape of the scoring kernels; zeros select the built-in defaults.
+ *   rows_per_item   block rows (b1) per work item: a work item is
+ *                   (pose, [r0, r0 + rows_per_item)) against every b2 >= b1
+ *   warps_per_cta   warps per CTA; each warp evaluates one block pair at a time
+ *   ctas_per_sm     resident CTAs per SM of the persistent grid */
+typedef struct {
+  int32_t rows_per_item;
+  int32_t warps_per_cta;
+  int32_t ctas_per_sm;
+} tmol_b200_ljlk_launch;
+
+typedef struct tmol_b200_ljlk_plan tmol_b200_ljlk_plan;
+
+/* Replaces the per-call setup of LJLKPoseScoreDispatch::forward
+ * (tmol/score/ljlk/potentials/ljlk_pose_score.impl.hh:628-778): derives the
+ * compact tables once.  `real_bytes` is 4 (float32) or 8 (float64). */
+int tmol_b200_ljlk_plan_create(const tmol_b200_ljlk_inputs* inputs,
+                               int real_bytes,
+                               const tmol_b200_ljlk_launch* launch,
+                               void* stream, tmol_b200_ljlk_plan** plan_out);
+
+int tmol_b200_ljlk_plan_destroy(tmol_b200_ljlk_plan* plan);
+
+/* Changes the launch shape of an existing plan (autotuning). */
+int tmol_b200_ljlk_plan_set_launch(tmol_b200_ljlk_plan* plan,
+                                   const tmol_b200_ljlk_launch* launch);
+
+/* Replaces LJLKPoseScoreOp::forward / LJLKPoseScoreDispatch::forward
+ * (compiled.ops.cpp:33-155; ljlk_pose_score.impl.hh:628-1158):
+ *   coords         [n_atoms, 3] device
+ *   energies       [3, P] (block_pair == 0) or [3, P, B, B] (block_pair != 0);
+ *                  overwritten
+ *   block_neighbors [P, B, B] int32 or NULL; overwritten when given */
+int tmol_b200_ljlk_forward(tmol_b200_ljlk_plan* plan, const void* coords,
+                           int block_pair, void* energies,
+                           int32_t* block_neighbors, void* stream);
+
+/* Replaces LJLKPoseScoreOp::backward (compiled.ops.cpp:157-278) with a
+ * recompute adjoint (the reference's block-pair backward,
+ * ljlk_pose_score.impl.hh:1160-1477, generalised to per-pose weights):
+ *   dTdV       [3, P] (block_pair == 0) or [3, P, B, B] (block_pair != 0)
+ *   dcoords    [n_atoms, 3]; overwritten with sum_t dTdV_t * dE_t/dcoords */
+int tmol_b200_ljlk_backward(tmol_b200_ljlk_plan* plan, const void* coords,
+                            int block_pair, const void* dTdV, void* dcoords,
+                            void* stream);
+
+/* Energies and weighted gradient in one pass, the work of the reference's
+ * whole-pose forward when coords require grad (ljlk_pose_score.impl.hh:
+ * 953-1119) followed by its elementwise backward (compiled.ops.cpp:164-173):
+ *   weights    [3, P]: dL/dE per term and pose
+ *   energies   [3, P]; overwritten
+ *   dcoords    [n_atoms, 3]; overwritten with sum_t weights_t * dE_t/dcoords */
+int tmol_b200_ljlk_energy_and_gradient(tmol_b200_ljlk_plan* plan,
+                                       const void* coords, const void* weights,
+                                       void* energies, void* dcoords,
+                                       void* stream);
+
+/* Work counters of the last forward / energy_and_gradient call, the units of
+ * the throughput and roofline figures (synchronises the stream):
+ *   counts[0] neighbouring block pairs (incl. each block with itself)
+ *   counts[1] atom pairs they hold (inter: n1 * n2, intra: n (n - 1) / 2)
+ *   counts[2] heavy-atom pairs they hold (same rule)
+ *   counts[3] atom pairs closer than max_dis with non-zero count-pair weight
+ *   counts[4] heavy-atom pairs among counts[3] */
+int tmol_b200_ljlk_last_counts(tmol_b200_ljlk_plan* plan, void* stream,
+                               int64_t* counts);
+
+/* Kernel timing: while enabled, CUDA events bracket each scoring-kernel
+ * launch (up to 4096); profile_read sums their durations (synchronising). */
+int tmol_b200_ljlk_profile(tmol_b200_ljlk_plan* plan, int enable);
+int tmol_b200_ljlk_profile_read(tmol_b200_ljlk_plan* plan, double* total_ms,
+                                int32_t* n_launches);
+
+/* Sizes of the plan's device allocations in bytes. */
+int64_t tmol_b200_ljlk_plan_device_bytes(const tmol_b200_ljlk_plan* plan);
+
+/* Human-readable text of a status code. */
+const char* tmol_b200_status_string(int status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TMOL_B200_LJLK_H */

@@ -1,0 +1,91 @@
+"""Generate the golden fixtures under tests/golden from the reference itself.
+
+Run in a checkout that has the reference sources and the compiled reference
+op (``python oracle/build_ref.py``):
+
+    python tests/golden/make_golden.py /path/to/tmol
+
+Writes
+  ubq.npz            1ubq (tmol/tests/data/pdb/1ubq.pdb) as block-type names
+                     and coordinates in block-type atom order, the reference
+                     op's per-pose energies and gradient for it, and the
+                     reference test suite's stored whole-pose energies
+                     (tmol/tests/data/term_baselines/LJLKEnergyTerm/
+                     test_whole_pose_scoring_10.yaml)
+  ubq_blockpair.npz  reference op block-pair energies of 1ubq
+  synthetic.npz      reference op energies, gradient and neighbour matrix of
+                     a jagged batch of seeded synthetic poses (1, 2, 7, 33,
+                     100 residues), plus the sizes and seeds that rebuild it
+"""
+
+import os
+import sys
+
+import numpy
+import torch
+import yaml
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.abspath(os.path.join(HERE, "..", "..")))
+
+from oracle import oracle as O  # noqa: E402
+from tmol_b200.pose.builder import build_pose_stack  # noqa: E402
+from tmol_b200.pose.pdb import pose_from_pdb_text  # noqa: E402
+from tmol_b200.pose.synthetic import synthetic_pose_stack  # noqa: E402
+from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm, pose_score_args  # noqa: E402
+
+SYN_SIZES = [1, 2, 7, 33, 100]
+SYN_SEEDS = [11, 12, 13, 14, 15]
+
+
+def ref_scores(ps, term):
+    args = pose_score_args(ps, term)
+    coords = ps.coords.flatten(0, 1)
+    E, c, nbr = O.reference_pose_scores(coords, args, require_gradient=True)
+    E.sum().backward()
+    return E.detach().numpy(), c.grad.numpy(), nbr.numpy()
+
+
+def main(ref_root):
+    term = LJLKEnergyTerm()
+    with open(os.path.join(ref_root, "tmol/tests/data/pdb/1ubq.pdb")) as f:
+        topo, xyz = pose_from_pdb_text(f.read())
+    with open(
+        os.path.join(
+            ref_root,
+            "tmol/tests/data/term_baselines/LJLKEnergyTerm/test_whole_pose_scoring_10.yaml",
+        )
+    ) as f:
+        gold = yaml.safe_load(f)
+    gold_E = numpy.array([gold[f"term{t}"]["pose0"] for t in range(3)], dtype=numpy.float64)
+    ps = build_pose_stack([topo], [xyz])
+    E, g, nbr = ref_scores(ps, term)
+    numpy.savez_compressed(
+        os.path.join(HERE, "ubq.npz"),
+        block_type_names=numpy.array(topo.block_type_names),
+        coords=xyz.astype(numpy.float32),
+        ref_energies=E,
+        ref_grad=g,
+        ref_neighbors=nbr,
+        tmol_test_energies=gold_E,
+    )
+    args = pose_score_args(ps, term, block_pair=True)
+    Eb, _ = O.load_reference()(ps.coords.flatten(0, 1).clone(), *args)
+    numpy.savez_compressed(os.path.join(HERE, "ubq_blockpair.npz"), ref_block_pair_energies=Eb.numpy())
+
+    ps = synthetic_pose_stack(SYN_SIZES, SYN_SEEDS)
+    E, g, nbr = ref_scores(ps, term)
+    numpy.savez_compressed(
+        os.path.join(HERE, "synthetic.npz"),
+        sizes=numpy.array(SYN_SIZES),
+        seeds=numpy.array(SYN_SEEDS),
+        coords=ps.coords.numpy(),
+        ref_energies=E,
+        ref_grad=g,
+        ref_neighbors=nbr,
+    )
+    print("wrote fixtures to", HERE)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -1,0 +1,125 @@
+"""CUDA path vs the oracle and the reference's golden fixtures.
+
+Tolerances (the parity bar for this path):
+  per-pose energies   |dE| <= 1e-3 kcal/mol + 1e-5 * |E|
+  gradients           |dg| <= 1e-4 * |g| + 1e-4 * max|g| per component
+  neighbour matrix    bit-exact
+float64 runs are held to 1e-9 relative.
+"""
+
+import numpy
+import pytest
+import torch
+
+from oracle import oracle as O
+from tmol_b200.score.ljlk_energy_term import pose_score_args
+from tmol_b200.score.ljlk_op import LJLKPlan, ljlk_pose_scores, clear_plan_cache
+
+pytestmark = pytest.mark.gpu
+DEV = torch.device("cuda:0")
+
+
+def E_close(E, ref, rtol=1e-5, atol=1e-3):
+    numpy.testing.assert_allclose(E, ref, rtol=rtol, atol=atol)
+
+
+def g_close(g, ref, rtol=1e-4):
+    scale = numpy.abs(ref).max()
+    numpy.testing.assert_allclose(g, ref, rtol=rtol, atol=rtol * scale)
+
+
+def gpu_scores(ps, term, dtype=torch.float32, block_pair=False, grad_weights=None):
+    args = [a.to(DEV) if isinstance(a, torch.Tensor) else a for a in pose_score_args(ps, term, block_pair)]
+    coords = ps.coords.flatten(0, 1).to(DEV, dtype).requires_grad_(True)
+    args = [a.to(dtype) if isinstance(a, torch.Tensor) and a.is_floating_point() else a for a in args]
+    E, nbr = ljlk_pose_scores(coords, *args)
+    g = None
+    if grad_weights is not None:
+        (E * torch.as_tensor(grad_weights, device=DEV, dtype=dtype)).sum().backward()
+        g = coords.grad.detach().cpu().numpy()
+    return E.detach().cpu().numpy(), g, nbr.cpu().numpy()
+
+
+def test_ubq_against_reference_fixture(ubq_pose_stack, term, ubq_golden):
+    E, g, nbr = gpu_scores(ubq_pose_stack, term, grad_weights=numpy.ones((3, 1)))
+    E_close(E, ubq_golden["ref_energies"])
+    numpy.testing.assert_allclose(E[:, 0], ubq_golden["tmol_test_energies"], atol=1e-5, rtol=1e-3)
+    g_close(g, ubq_golden["ref_grad"])
+    assert numpy.array_equal(nbr, ubq_golden["ref_neighbors"])
+
+
+def test_synthetic_jagged_against_reference_fixture(synthetic_pose_stack_golden, term, synthetic_golden):
+    E, g, nbr = gpu_scores(synthetic_pose_stack_golden, term, grad_weights=numpy.ones((3, 1)))
+    E_close(E, synthetic_golden["ref_energies"])
+    g_close(g, synthetic_golden["ref_grad"])
+    assert numpy.array_equal(nbr, synthetic_golden["ref_neighbors"])
+
+
+@pytest.mark.parametrize("sizes,seed", [([150] * 8, 100), ([5, 80, 20, 1, 300, 47], 7)])
+def test_batches_against_oracle(term, sizes, seed):
+    from tmol_b200.pose.synthetic import synthetic_pose_stack
+
+    ps = synthetic_pose_stack(sizes, [seed + k for k in range(len(sizes))])
+    rng = numpy.random.default_rng(seed)
+    w = rng.uniform(0.2, 1.5, size=(3, len(sizes)))
+    E, g, nbr = gpu_scores(ps, term, grad_weights=w)
+    oc = O.OracleCall(ps.coords.flatten(0, 1), pose_score_args(ps, term))
+    Eo, dVo, nbro = oc.pose_scores(require_gradient=True)
+    E_close(E, Eo)
+    assert numpy.array_equal(nbr, nbro)
+    pose = ps.pose_ind_for_atom.numpy()
+    g_ref = (dVo * w[:, pose][:, :, None]).sum(0)
+    g_close(g, g_ref)
+
+
+def test_block_pair_mode_and_adjoint(synthetic_pose_stack_golden, term):
+    ps = synthetic_pose_stack_golden
+    P, B = ps.n_poses, ps.max_n_blocks
+    rng = numpy.random.default_rng(3)
+    w = rng.normal(size=(3, P, B, B))
+    E, g, nbr = gpu_scores(ps, term, block_pair=True, grad_weights=w)
+    oc = O.OracleCall(ps.coords.flatten(0, 1), pose_score_args(ps, term, True))
+    Eo, _, nbro = oc.pose_scores(block_pair=True)
+    E_close(E, Eo)
+    assert numpy.array_equal(nbr, nbro)
+    go = oc.backward(nbro, w.astype(numpy.float32), per_pose_weights=False)
+    g_close(g, go)
+
+
+def test_float64_path(synthetic_pose_stack_golden, term):
+    ps = synthetic_pose_stack_golden
+    E, g, nbr = gpu_scores(ps, term, dtype=torch.float64, grad_weights=numpy.ones((3, 1)))
+    oc = O.OracleCall(ps.coords.flatten(0, 1).double(), pose_score_args(ps, term), f64=True)
+    Eo, dVo, _ = oc.pose_scores(require_gradient=True)
+    E_close(E, Eo, rtol=1e-9, atol=1e-9)
+    g_close(g, dVo.sum(0), rtol=1e-9)
+
+
+def test_gradcheck_float64(term):
+    from tmol_b200.pose.synthetic import synthetic_pose_stack
+
+    ps = synthetic_pose_stack([4, 3], [21, 22])
+    args = [a.to(DEV) if isinstance(a, torch.Tensor) else a for a in pose_score_args(ps, term)]
+    args = [a.double() if isinstance(a, torch.Tensor) and a.is_floating_point() else a for a in args]
+    wt = torch.rand(3, 1, device=DEV, dtype=torch.float64)
+
+    def f(c):
+        E, _ = ljlk_pose_scores(c, *args)
+        return (wt * E).sum()
+
+    c = ps.coords.flatten(0, 1).to(DEV, torch.float64).requires_grad_(True)
+    assert torch.autograd.gradcheck(f, (c,), eps=1e-6, atol=1e-5, rtol=1e-3)
+
+
+def test_plan_errors_are_raised(ubq_pose_stack, term):
+    from tmol_b200.native import NativeError
+
+    args = [a.to(DEV) if isinstance(a, torch.Tensor) else a for a in pose_score_args(ubq_pose_stack, term)]
+    bad = list(args)
+    at = bad[17].clone()
+    at[0, 0] = 10_000  # atom type index past the type table
+    bad[17] = at
+    coords = ubq_pose_stack.coords.flatten(0, 1).to(DEV)
+    with pytest.raises(NativeError, match="index out of range"):
+        LJLKPlan(coords, bad[:-1])
+    clear_plan_cache()

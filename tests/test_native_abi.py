@@ -1,0 +1,66 @@
+"""The C-ABI library loads and exports every function include/ declares.
+
+No GPU work is done here: only host-side entry points are called."""
+
+import ctypes
+import os
+import re
+
+import pytest
+
+from tmol_b200 import native
+
+ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+
+
+def declared_functions():
+    names = []
+    inc = os.path.join(ROOT, "include")
+    for fn in sorted(os.listdir(inc)):
+        if not fn.endswith(".h"):
+            continue
+        text = open(os.path.join(inc, fn)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names += re.findall(r"\b(tmol_b200_\w+)\s*\(", text)
+    return sorted(set(names))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert "tmol_b200_ljlk_forward" in names and "tmol_b200_ljlk_backward" in names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = native.load()
+    for name in declared_functions():
+        assert hasattr(lib, name), name
+
+
+def test_binding_covers_header():
+    assert set(declared_functions()) <= set(native.SIGNATURES)
+
+
+def test_status_strings_and_argument_checks():
+    lib = native.load()
+    assert lib.tmol_b200_status_string(0) == b"ok"
+    assert b"index" in lib.tmol_b200_status_string(3)
+    out = ctypes.c_void_p()
+    # null inputs are rejected before any device work
+    assert lib.tmol_b200_ljlk_plan_create(None, 4, None, None, ctypes.byref(out)) == 1
+    s = native.Inputs()
+    assert lib.tmol_b200_ljlk_plan_create(ctypes.byref(s), 3, None, None, ctypes.byref(out)) == 6
+    s.max_n_conn = 5
+    assert lib.tmol_b200_ljlk_plan_create(ctypes.byref(s), 4, None, None, ctypes.byref(out)) == 2
+    assert lib.tmol_b200_ljlk_plan_destroy(None) == 1
+    assert lib.tmol_b200_ljlk_forward(None, None, 0, None, None, None) == 1
+    assert lib.tmol_b200_ljlk_plan_device_bytes(None) == -1
+
+
+def test_op_refuses_cpu_tensors(ubq_pose_stack, term):
+    import torch
+    from tmol_b200.score.ljlk_energy_term import pose_score_args
+    from tmol_b200.score.ljlk_op import ljlk_pose_scores
+
+    args = pose_score_args(ubq_pose_stack, term)
+    with pytest.raises(RuntimeError, match="CUDA"):
+        ljlk_pose_scores(ubq_pose_stack.coords.flatten(0, 1), *args)

@@ -1,0 +1,136 @@
+"""ctypes binding of the C ABI in ``include/tmol_b200_ljlk.h``.
+
+The shared library is built in-tree (``tmol_b200/lib``) by
+``tmol_b200.build``.  There is no fallback: importing this module without the
+library raises, and every entry point's status code is turned into an
+exception.
+"""
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libtmol_b200_ljlk.so")
+
+_i32p = ctypes.POINTER(ctypes.c_int32)
+
+
+class Inputs(ctypes.Structure):
+    """``tmol_b200_ljlk_inputs``."""
+
+    _fields_ = [
+        ("n_atoms", ctypes.c_int64),
+        ("n_poses", ctypes.c_int32),
+        ("max_n_blocks", ctypes.c_int32),
+        ("n_rots", ctypes.c_int32),
+        ("n_block_types", ctypes.c_int32),
+        ("max_n_block_atoms", ctypes.c_int32),
+        ("max_n_conn", ctypes.c_int32),
+        ("max_n_tiles", ctypes.c_int32),
+        ("n_atom_types", ctypes.c_int32),
+        ("rot_coord_offset", ctypes.c_void_p),
+        ("pose_ind_for_atom", ctypes.c_void_p),
+        ("first_rot_for_block", ctypes.c_void_p),
+        ("first_rot_block_type", ctypes.c_void_p),
+        ("block_ind_for_rot", ctypes.c_void_p),
+        ("pose_ind_for_rot", ctypes.c_void_p),
+        ("block_type_ind_for_rot", ctypes.c_void_p),
+        ("n_rots_for_pose", ctypes.c_void_p),
+        ("rot_offset_for_pose", ctypes.c_void_p),
+        ("n_rots_for_block", ctypes.c_void_p),
+        ("rot_offset_for_block", ctypes.c_void_p),
+        ("max_n_rots_per_pose", ctypes.c_int32),
+        ("min_bondsep", ctypes.c_void_p),
+        ("inter_block_bondsep", ctypes.c_void_p),
+        ("bt_n_atoms", ctypes.c_void_p),
+        ("bt_n_heavy_atoms_in_tile", ctypes.c_void_p),
+        ("bt_heavy_atoms_in_tile", ctypes.c_void_p),
+        ("bt_atom_types", ctypes.c_void_p),
+        ("bt_n_conn", ctypes.c_void_p),
+        ("bt_conn_atom", ctypes.c_void_p),
+        ("bt_path_distance", ctypes.c_void_p),
+        ("bt_is_ligand_fragment", ctypes.c_void_p),
+        ("type_params", ctypes.c_void_p),
+        ("global_params", ctypes.c_void_p),
+        ("max_dis", ctypes.c_double),
+    ]
+
+
+class Launch(ctypes.Structure):
+    """``tmol_b200_ljlk_launch``."""
+
+    _fields_ = [
+        ("rows_per_item", ctypes.c_int32),
+        ("warps_per_cta", ctypes.c_int32),
+        ("ctas_per_sm", ctypes.c_int32),
+    ]
+
+
+# Every symbol the header declares, with its ctypes signature.
+SIGNATURES = {
+    "tmol_b200_ljlk_plan_create": (
+        ctypes.c_int,
+        [ctypes.POINTER(Inputs), ctypes.c_int, ctypes.POINTER(Launch), ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)],
+    ),
+    "tmol_b200_ljlk_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "tmol_b200_ljlk_plan_set_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Launch)]),
+    "tmol_b200_ljlk_forward": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    ),
+    "tmol_b200_ljlk_backward": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    ),
+    "tmol_b200_ljlk_energy_and_gradient": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    ),
+    "tmol_b200_ljlk_last_counts": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)],
+    ),
+    "tmol_b200_ljlk_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "tmol_b200_ljlk_profile_read": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32)],
+    ),
+    "tmol_b200_ljlk_plan_device_bytes": (ctypes.c_int64, [ctypes.c_void_p]),
+    "tmol_b200_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+}
+
+_lib = None
+
+
+class NativeError(RuntimeError):
+    def __init__(self, func, status, text):
+        super().__init__(f"{func} failed with status {status}: {text}")
+        self.status = status
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"the tmol_b200 CUDA library is not built ({LIB_PATH} is missing); "
+                "run `python -m tmol_b200.build`"
+            )
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def check(func, status):
+    if status != 0:
+        text = load().tmol_b200_status_string(status).decode()
+        raise NativeError(func, status, text)
+
+
+def call(name, *args):
+    lib = load()
+    check(name, getattr(lib, name)(*args))

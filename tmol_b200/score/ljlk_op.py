@@ -1,0 +1,316 @@
+"""The LJ/LK pose-score op on B200, with tmol's argument list and outputs.
+
+``ljlk_pose_scores(coords, <26 static arguments>, output_block_pair_energies)``
+takes exactly the arguments of ``torch.ops.tmol_ljlk.ljlk_pose_scores``
+(``tmol/score/ljlk/potentials/compiled.ops.cpp:533-597``) and returns
+``(scores, block_neighbors)``: scores ``[3, P]`` (whole pose) or
+``[3, P, B, B]`` (block pairs), neighbours ``[P, B, B]`` int32.  Gradients
+flow to ``coords`` only, through a recompute adjoint kernel.
+
+The static arguments are turned into a device plan (compact count-pair and
+parameter tables) once and cached, keyed by the identity, shape and version
+of each static tensor.  All tensors must be on one CUDA device; there is no
+CPU path.
+"""
+
+import collections
+import ctypes
+
+import torch
+
+from .. import native
+
+N_STATIC = 26  # arguments after coords, before the output-mode flag
+
+
+class LJLKPlan:
+    """Owns one ``tmol_b200_ljlk_plan``."""
+
+    def __init__(self, coords_like, static_args, launch=None):
+        (
+            rot_coord_offset,
+            pose_ind_for_atom,
+            first_rot_for_block,
+            first_rot_block_type,
+            block_ind_for_rot,
+            pose_ind_for_rot,
+            block_type_ind_for_rot,
+            n_rots_for_pose,
+            rot_offset_for_pose,
+            n_rots_for_block,
+            rot_offset_for_block,
+            max_n_rots_per_pose,
+            min_bondsep,
+            inter_block_bondsep,
+            bt_n_atoms,
+            bt_n_heavy_in_tile,
+            bt_heavy_in_tile,
+            bt_atom_types,
+            bt_n_conn,
+            bt_conn_atom,
+            bt_path_distance,
+            bt_is_ligand,
+            type_params,
+            global_params,
+            max_dis,
+        ) = static_args
+        device = coords_like.device
+        if device.type != "cuda":
+            raise RuntimeError("tmol_b200 LJ/LK scoring runs on CUDA tensors only")
+        self.device = device
+        self.dtype = coords_like.dtype
+        if self.dtype not in (torch.float32, torch.float64):
+            raise TypeError(f"coordinates must be float32 or float64, got {self.dtype}")
+        ints = dict(
+            rot_coord_offset=rot_coord_offset,
+            pose_ind_for_atom=pose_ind_for_atom,
+            first_rot_for_block=first_rot_for_block,
+            first_rot_block_type=first_rot_block_type,
+            block_ind_for_rot=block_ind_for_rot,
+            pose_ind_for_rot=pose_ind_for_rot,
+            block_type_ind_for_rot=block_type_ind_for_rot,
+            n_rots_for_pose=n_rots_for_pose,
+            rot_offset_for_pose=rot_offset_for_pose,
+            n_rots_for_block=n_rots_for_block,
+            rot_offset_for_block=rot_offset_for_block,
+            min_bondsep=min_bondsep,
+            inter_block_bondsep=inter_block_bondsep,
+            bt_n_atoms=bt_n_atoms,
+            bt_n_heavy_atoms_in_tile=bt_n_heavy_in_tile,
+            bt_heavy_atoms_in_tile=bt_heavy_in_tile,
+            bt_atom_types=bt_atom_types,
+            bt_n_conn=bt_n_conn,
+            bt_conn_atom=bt_conn_atom,
+            bt_path_distance=bt_path_distance,
+            bt_is_ligand_fragment=bt_is_ligand,
+        )
+        keep = []
+        s = native.Inputs()
+        for name, t in ints.items():
+            if not isinstance(t, torch.Tensor):
+                raise TypeError(f"{name} must be a tensor")
+            if t.device != device:
+                raise RuntimeError(f"{name} is on {t.device}, coordinates on {device}")
+            t = t.to(torch.int32).contiguous()
+            keep.append(t)
+            setattr(s, name, t.data_ptr())
+        reals = {}
+        for name, t in (("type_params", type_params), ("global_params", global_params)):
+            if t.device != device:
+                raise RuntimeError(f"{name} is on {t.device}, coordinates on {device}")
+            t = t.to(self.dtype).contiguous()
+            keep.append(t)
+            reals[name] = t
+            setattr(s, name, t.data_ptr())
+        P, B = first_rot_for_block.shape
+        C = bt_conn_atom.shape[1]
+        if tuple(inter_block_bondsep.shape) != (P, B, B, C, C):
+            raise ValueError(
+                f"inter_block_bondsep has shape {tuple(inter_block_bondsep.shape)}, expected {(P, B, B, C, C)}"
+            )
+        if tuple(min_bondsep.shape) != (P, B, B):
+            raise ValueError(f"min_bondsep has shape {tuple(min_bondsep.shape)}, expected {(P, B, B)}")
+        if reals["type_params"].dim() != 2 or reals["type_params"].shape[1] != 10:
+            raise ValueError("type_params must be [n_types, 10]")
+        if reals["global_params"].numel() != 5:
+            raise ValueError("global_params must hold 5 values")
+        s.n_poses = P
+        s.max_n_blocks = B
+        s.n_rots = rot_coord_offset.shape[0]
+        s.n_block_types = bt_n_atoms.shape[0]
+        s.max_n_block_atoms = bt_atom_types.shape[1]
+        s.max_n_conn = C
+        s.max_n_tiles = bt_n_heavy_in_tile.shape[1]
+        s.n_atom_types = type_params.shape[0]
+        s.max_n_rots_per_pose = int(max_n_rots_per_pose)
+        s.max_dis = float(max_dis)
+        self.n_poses, self.max_n_blocks = P, B
+        self.n_atoms = pose_ind_for_atom.shape[0]
+        s.n_atoms = self.n_atoms
+        self.launch = native.Launch(*(launch or (0, 0, 0)))
+        ptr = ctypes.c_void_p()
+        with torch.cuda.device(device):
+            stream = torch.cuda.current_stream(device).cuda_stream
+            native.call(
+                "tmol_b200_ljlk_plan_create",
+                ctypes.byref(s),
+                4 if self.dtype == torch.float32 else 8,
+                ctypes.byref(self.launch),
+                ctypes.c_void_p(stream),
+                ctypes.byref(ptr),
+            )
+        self.ptr = ptr
+        del keep
+
+    def __del__(self):
+        ptr = getattr(self, "ptr", None)
+        if ptr is not None and ptr.value:
+            try:
+                native.load().tmol_b200_ljlk_plan_destroy(ptr)
+            except Exception:
+                pass
+            self.ptr = None
+
+    def set_launch(self, rows_per_item=0, warps_per_cta=0, ctas_per_sm=0):
+        self.launch = native.Launch(rows_per_item, warps_per_cta, ctas_per_sm)
+        native.call("tmol_b200_ljlk_plan_set_launch", self.ptr, ctypes.byref(self.launch))
+
+    def device_bytes(self):
+        return native.load().tmol_b200_ljlk_plan_device_bytes(self.ptr)
+
+    def _stream(self):
+        return ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def _check_coords(self, coords):
+        if coords.device != self.device or coords.dtype != self.dtype:
+            raise RuntimeError(
+                f"coordinates ({coords.device}, {coords.dtype}) do not match the plan "
+                f"({self.device}, {self.dtype})"
+            )
+        if coords.dim() != 2 or coords.shape[1] != 3 or coords.shape[0] != self.n_atoms:
+            raise ValueError(f"coordinates must be [{self.n_atoms}, 3], got {tuple(coords.shape)}")
+
+    def forward(self, coords, block_pair=False, want_neighbors=True, energies=None):
+        self._check_coords(coords)
+        coords = coords.contiguous()
+        P, B = self.n_poses, self.max_n_blocks
+        shape = (3, P, B, B) if block_pair else (3, P)
+        if energies is None:
+            energies = torch.empty(shape, dtype=self.dtype, device=self.device)
+        nbr = torch.empty((P, B, B), dtype=torch.int32, device=self.device) if want_neighbors else None
+        native.call(
+            "tmol_b200_ljlk_forward",
+            self.ptr,
+            ctypes.c_void_p(coords.data_ptr()),
+            int(block_pair),
+            ctypes.c_void_p(energies.data_ptr()),
+            ctypes.c_void_p(nbr.data_ptr() if nbr is not None else 0),
+            self._stream(),
+        )
+        return energies, nbr
+
+    def backward(self, coords, dTdV, block_pair=False, dcoords=None):
+        self._check_coords(coords)
+        coords = coords.contiguous()
+        dTdV = dTdV.to(self.dtype).contiguous()
+        if dcoords is None:
+            dcoords = torch.empty_like(coords)
+        native.call(
+            "tmol_b200_ljlk_backward",
+            self.ptr,
+            ctypes.c_void_p(coords.data_ptr()),
+            int(block_pair),
+            ctypes.c_void_p(dTdV.data_ptr()),
+            ctypes.c_void_p(dcoords.data_ptr()),
+            self._stream(),
+        )
+        return dcoords
+
+    def energy_and_gradient(self, coords, weights, energies=None, dcoords=None):
+        """Energies [3, P] and sum_t weights[t, pose] * dE_t/dcoords in one pass."""
+        self._check_coords(coords)
+        coords = coords.contiguous()
+        weights = weights.to(self.dtype).contiguous()
+        if tuple(weights.shape) != (3, self.n_poses):
+            raise ValueError(f"weights must be [3, {self.n_poses}]")
+        if energies is None:
+            energies = torch.empty((3, self.n_poses), dtype=self.dtype, device=self.device)
+        if dcoords is None:
+            dcoords = torch.empty_like(coords)
+        native.call(
+            "tmol_b200_ljlk_energy_and_gradient",
+            self.ptr,
+            ctypes.c_void_p(coords.data_ptr()),
+            ctypes.c_void_p(weights.data_ptr()),
+            ctypes.c_void_p(energies.data_ptr()),
+            ctypes.c_void_p(dcoords.data_ptr()),
+            self._stream(),
+        )
+        return energies, dcoords
+
+    COUNT_NAMES = ("block_pairs", "atom_pairs", "heavy_pairs", "atom_pairs_in_range", "heavy_pairs_in_range")
+
+    def last_counts(self):
+        """Work counters of the last forward / energy_and_gradient call."""
+        arr = (ctypes.c_int64 * 5)()
+        native.call("tmol_b200_ljlk_last_counts", self.ptr, self._stream(), arr)
+        return dict(zip(self.COUNT_NAMES, list(arr)))
+
+    def profile(self, enable=True):
+        native.call("tmol_b200_ljlk_profile", self.ptr, int(enable))
+
+    def profile_read(self):
+        """(total milliseconds, launches) of the scoring kernel since profile()."""
+        ms = ctypes.c_double()
+        n = ctypes.c_int32()
+        native.call("tmol_b200_ljlk_profile_read", self.ptr, ctypes.byref(ms), ctypes.byref(n))
+        return ms.value, n.value
+
+
+class _ScoreFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, coords, plan, block_pair, want_neighbors):
+        E, nbr = plan.forward(coords, block_pair, want_neighbors)
+        ctx.plan = plan
+        ctx.block_pair = block_pair
+        ctx.save_for_backward(coords)
+        if nbr is None:
+            nbr = torch.empty((0,), dtype=torch.int32, device=coords.device)
+        ctx.mark_non_differentiable(nbr)
+        return E, nbr
+
+    @staticmethod
+    def backward(ctx, dE, _dnbr):
+        (coords,) = ctx.saved_tensors
+        if dE is None:
+            return None, None, None, None
+        dx = ctx.plan.backward(coords, dE, ctx.block_pair)
+        return dx, None, None, None
+
+
+_PLAN_CACHE = collections.OrderedDict()
+_PLAN_CACHE_SIZE = 8
+
+
+def _plan_key(coords, static):
+    parts = [coords.device, coords.dtype]
+    for t in static:
+        if isinstance(t, torch.Tensor):
+            parts.append((t.data_ptr(), tuple(t.shape), t.dtype, t._version))
+        else:
+            parts.append(t)
+    return tuple(parts)
+
+
+def get_plan(coords, static):
+    key = _plan_key(coords, static)
+    entry = _PLAN_CACHE.get(key)
+    if entry is not None:
+        _PLAN_CACHE.move_to_end(key)
+        return entry[0]
+    plan = LJLKPlan(coords, static)
+    # the static tensors are held so that their addresses cannot be reused
+    # by other tensors while the key is cached
+    _PLAN_CACHE[key] = (plan, [t for t in static if isinstance(t, torch.Tensor)])
+    while len(_PLAN_CACHE) > _PLAN_CACHE_SIZE:
+        _PLAN_CACHE.popitem(last=False)
+    return plan
+
+
+def clear_plan_cache():
+    _PLAN_CACHE.clear()
+
+
+def ljlk_pose_scores(coords, *args, return_block_neighbors=True):
+    """Drop-in for ``torch.ops.tmol_ljlk.ljlk_pose_scores``."""
+    if len(args) != N_STATIC:
+        raise TypeError(f"ljlk_pose_scores takes coords + {N_STATIC} arguments, got {1 + len(args)}")
+    static = args[:-1]
+    block_pair = bool(args[-1])
+    plan = get_plan(coords, static)
+    return pose_scores_with_plan(coords, plan, block_pair, return_block_neighbors)
+
+
+def pose_scores_with_plan(coords, plan, block_pair=False, return_block_neighbors=False):
+    scores, nbr = _ScoreFn.apply(coords, plan, block_pair, return_block_neighbors)
+    return scores, (nbr if return_block_neighbors else None)
