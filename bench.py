@@ -1,0 +1,513 @@
+#!/usr/bin/env python
+"""LJ + LK energy + gradient throughput on B200 (tmol's LJLK pose scoring).
+
+Workload (one "step"): the uniform batch of 64 synthetic proteins x 150
+residues (seeded; residues uniform over the 20 canonical amino acids, ideal
+geometry from tmol's internal coordinates, 60% helix / 40% strand dihedrals,
+rotameric chis), float32; per step, the per-pose LJ-attractive, LJ-repulsive
+and LK energies and the gradient of their weighted sum with respect to every
+coordinate (weights 1.0 / 0.55 / 1.0, tmol's beta2016 weights).
+
+Arms:
+  (default)         the B200 path: one fused energy + gradient pass per step
+                    (sphere kernel + fused neighbour/atom-pair kernel),
+                    replayed as a CUDA graph; inputs resident in HBM.
+  --impl reference  tmol's own CPU implementation of the op (compiled from
+                    its sources into oracle/_ref), on all host cores: one
+                    process per core, each scoring a slice of the poses.
+
+Under torchrun each rank scores its own batch (independent seeds); the
+timing is the maximum over ranks (weak scaling, no collective on the data
+path).  Prints one JSON line (rank 0).
+"""
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+N_POSES = 64
+N_RES = 150
+TERM_WEIGHTS = (1.0, 0.55, 1.0)
+METRIC = "LJ+LK energy+grad poses/s (64x150-residue batch, 1 B200)"
+L2_FLUSH_BYTES = 256 << 20
+
+# Algorithmic FLOPs per unit (E + dE), counted on the restatement's most
+# populated branch (far cubic fade, 4.5-6 A); FMA = 2, div/sqrt/exp/floor = 1.
+F_PAIR_TEST = 8  # every atom pair of a neighbouring block pair: distance^2 test
+F_LJ = 64  # each pair inside max_dis with non-zero count-pair weight
+F_LK = 111  # each heavy-atom pair among those (both LK directions)
+
+
+def workload(rank):
+    from tmol_b200.pose.synthetic import synthetic_pose_stack
+
+    seeds = [rank * N_POSES + k for k in range(N_POSES)]
+    return synthetic_pose_stack([N_RES] * N_POSES, seeds)
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML while running."""
+
+    REASONS = {
+        "hw_slowdown": 0x8,
+        "hw_thermal_slowdown": 0x40,
+        "sw_thermal_slowdown": 0x20,
+        "sw_power_cap": 0x4,
+        "hw_power_brake_slowdown": 0x80,
+    }
+
+    def __init__(self, index):
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+                r = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for name, bit in self.REASONS.items():
+                    if r & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.002)
+
+    def __enter__(self):
+        if self.nv is not None:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self.nv is not None:
+            self.t.join()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unavailable"]}
+        return {
+            "sm_mhz": statistics.median(self.samples),
+            "sm_max_mhz": self.max_mhz,
+            "reasons": sorted(self.reasons),
+            "samples": len(self.samples),
+        }
+
+
+def dist_setup():
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.item()
+
+
+def sum_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return t.item()
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def cpu_reference_sample(ps, term, reps=3):
+    """tmol's CPU op (oracle/_ref, else the bit-exact C restatement) on the
+    whole batch, energies + gradient, single thread; best of `reps`."""
+    import torch
+
+    from oracle import oracle as O
+    from tmol_b200.score.ljlk_energy_term import pose_score_args
+
+    torch.set_num_threads(1)
+    args = pose_score_args(ps, term)
+    coords = ps.coords.flatten(0, 1)
+    if O.reference_available():
+        kind = "reference"
+
+        def run():
+            E, c, _ = O.reference_pose_scores(coords, args, require_gradient=True)
+            (torch.tensor(TERM_WEIGHTS)[:, None] * E).sum().backward()
+
+    else:
+        kind = "port"
+        oc = O.OracleCall(coords, args)
+
+        def run():
+            oc.pose_scores(require_gradient=True)
+
+    run()
+    best = float("inf")
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        run()
+        best = min(best, time.perf_counter() - t0)
+    return kind, best
+
+
+def _ref_worker(conn, slice_ps_args):
+    import torch
+
+    torch.set_num_threads(1)
+    from oracle import oracle as O
+
+    coords, args = slice_ps_args
+    op = O.load_reference() if O.reference_available() else None
+    oc = None if op is not None else O.OracleCall(coords, args)
+    w = torch.tensor(TERM_WEIGHTS)[:, None]
+    while True:
+        msg = conn.recv()
+        if msg is None:
+            break
+        t0 = time.perf_counter()
+        if op is not None:
+            c = coords.clone().requires_grad_(True)
+            E, _ = op(c, *args)
+            (w * E).sum().backward()
+        else:
+            oc.pose_scores(require_gradient=True)
+        conn.send(time.perf_counter() - t0)
+
+
+def run_reference(args, world, rank):
+    """tmol's CPU op on all host cores (one process per core)."""
+    import multiprocessing as mp
+
+    from oracle import oracle as O
+    from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm, pose_score_args
+
+    if rank != 0:
+        return 0
+    term = LJLKEnergyTerm()
+    ps = workload(0)
+    n_proc = min(os.cpu_count() or 1, N_POSES)
+    bounds = [round(k * N_POSES / n_proc) for k in range(n_proc + 1)]
+    ctx = mp.get_context("spawn")
+    workers = []
+    for k in range(n_proc):
+        sub = ps.slice_poses(bounds[k], bounds[k + 1])
+        a = pose_score_args(sub, term)
+        parent, child = ctx.Pipe()
+        pr = ctx.Process(target=_ref_worker, args=(child, (sub.coords.flatten(0, 1).clone(), a)))
+        pr.start()
+        workers.append((pr, parent))
+
+    def step():
+        t0 = time.perf_counter()
+        for _, c in workers:
+            c.send(1)
+        for _, c in workers:
+            c.recv()
+        return time.perf_counter() - t0
+
+    for _ in range(max(args.warmup, 1)):
+        step()
+    times = [step() for _ in range(args.steps)]
+    for pr, c in workers:
+        c.send(None)
+        pr.join()
+    t = sum(times)
+    value = N_POSES * args.steps / t
+    kind = "reference" if O.reference_available() else "port"
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": "poses/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * t / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded proteins, ideal geometry)",
+        "config": {
+            "workload": f"{N_POSES} poses x {N_RES} residues, energy + gradient",
+            "poses": N_POSES,
+            "residues_per_pose": N_RES,
+        },
+        "cpu_baseline": {
+            "value": value,
+            "unit": "poses/s",
+            "cores": n_proc,
+            "kind": kind,
+            "sample": f"the full {N_POSES}-pose batch per step, split over {n_proc} single-threaded processes",
+        },
+        "e2e": {"value": value, "unit": "poses/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def flops_per_step(counts):
+    return (
+        counts["atom_pairs"] * F_PAIR_TEST
+        + counts["atom_pairs_in_range"] * F_LJ
+        + counts["heavy_pairs_in_range"] * F_LK
+    )
+
+
+def load_traffic():
+    path = os.path.join(ROOT, "profiles", "ljlk_score_traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d.get("dram_bytes_per_launch")
+    except Exception:
+        return None
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def run_b200(args, world, rank, local):
+    import torch
+
+    from tmol_b200 import native
+    from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm, pose_score_args
+    from tmol_b200.score.ljlk_op import LJLKPlan
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    term = LJLKEnergyTerm()
+    ps_cpu = workload(rank)
+    static = [a.to(dev) if isinstance(a, torch.Tensor) else a for a in pose_score_args(ps_cpu, term)[:-1]]
+    coords = ps_cpu.coords.flatten(0, 1).to(dev).contiguous()
+    plan = LJLKPlan(coords, static)
+    P = ps_cpu.n_poses
+    weights = torch.tensor(TERM_WEIGHTS, device=dev, dtype=torch.float32)[:, None].expand(3, P).contiguous()
+    energies = torch.empty((3, P), device=dev)
+    dcoords = torch.empty_like(coords)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, device=dev, dtype=torch.float32)
+
+    def step():
+        plan.energy_and_gradient(coords, weights, energies, dcoords)
+
+    # warm-up (also validates the launch), autotuning of the launch shape and
+    # work order, then capture of one step as a graph
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    from tmol_b200.tune import autotune
+
+    launch_shape, _ = autotune(plan, step, use_cache=False)
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    counts = plan.last_counts()
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        step()
+        torch.cuda.synchronize()
+        with torch.cuda.graph(g, stream=s):
+            step()
+    torch.cuda.current_stream().wait_stream(s)
+    for _ in range(max(args.warmup, 3)):
+        g.replay()
+    torch.cuda.synchronize()
+
+    # timed region: K graph replays, L2 flushed before each (outside the events)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record()
+            g.replay()
+            ev[k][1].record()
+        torch.cuda.synchronize()
+    barrier(world)
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    ms_max = max_over_ranks(ms, world)
+    poses_total = sum_over_ranks(P * args.steps, world)
+    value = poses_total / (ms_max / 1e3)
+
+    # kernel-level timing of the scoring kernel (direct launches, events
+    # recorded by the library around each launch on the launching stream)
+    plan.profile(True)
+    for _ in range(args.steps):
+        flush.zero_()
+        step()
+    kern_ms, n_launch = plan.profile_read()
+    plan.profile(False)
+    kern_avg_ms = kern_ms / max(n_launch, 1)
+
+    # end to end through the public entry point with host buffers: pinned
+    # coordinates in, energies and gradient out, copies inside the timing
+    h_coords = coords.cpu().pin_memory()
+    h_E = torch.empty((3, P), pin_memory=True)
+    h_g = torch.empty(coords.shape, pin_memory=True)
+    d_in = torch.empty_like(coords)
+    e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for _ in range(2):
+        d_in.copy_(h_coords, non_blocking=True)
+        plan.energy_and_gradient(d_in, weights, energies, dcoords)
+        h_E.copy_(energies, non_blocking=True)
+        h_g.copy_(dcoords, non_blocking=True)
+    torch.cuda.synchronize()
+    barrier(world)
+    for k in range(args.steps):
+        flush.zero_()
+        e2e_ev[k][0].record()
+        d_in.copy_(h_coords, non_blocking=True)
+        plan.energy_and_gradient(d_in, weights, energies, dcoords)
+        h_E.copy_(energies, non_blocking=True)
+        h_g.copy_(dcoords, non_blocking=True)
+        e2e_ev[k][1].record()
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in e2e_ev), world)
+    e2e_value = poses_total / (e2e_ms / 1e3)
+    h2d = coords.numel() * 4
+    d2h = (3 * P + coords.numel()) * 4
+
+    fp32_peak = native.measure_fp32_peak_tflops(torch.cuda.current_stream().cuda_stream)
+    flops = flops_per_step(counts)
+    achieved = flops / (kern_avg_ms * 1e-3) / 1e12
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        kind, t_cpu = cpu_reference_sample(ps_cpu, term)
+        cpu = {
+            "value": N_POSES / t_cpu,
+            "unit": "poses/s",
+            "cores": 1,
+            "kind": kind,
+            "sample": f"the full {N_POSES}x{N_RES} batch, energies + gradient, best of 3, one thread",
+        }
+
+    if rank == 0:
+        peaks = measured_peaks()
+        traffic = load_traffic()
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "poses/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded proteins, ideal geometry)",
+            "config": {
+                "workload": f"{N_POSES} poses x {N_RES} residues, energy + gradient, weights {list(TERM_WEIGHTS)}",
+                "poses_per_gpu": N_POSES,
+                "residues_per_pose": N_RES,
+                "atoms_per_gpu": int(coords.shape[0]),
+                "l2": "flushed (256 MiB write) before every timed step",
+                "launch": "CUDA graph replay: 2 kernels per step",
+                "launch_shape": dict(zip(("items_per_ticket", "warps_per_cta", "ctas_per_sm", "candidates_per_item"), launch_shape)),
+                "parallelism": f"weak, {world} independent batch(es)",
+            },
+            "atom_pairs_per_s": counts["atom_pairs"] * args.steps * world / (ms_max / 1e3),
+            "work_per_step": counts,
+            "gpu_launches": 2 * args.steps,
+            "clocks": clk.summary(),
+            "roofline": {
+                "bound": "fp32",
+                "achieved": achieved,
+                "peak": fp32_peak,
+                "unit": "TFLOP/s",
+                "frac": achieved / fp32_peak,
+                "traffic": traffic,
+                "kernel": "score_kernel<float, GRAD> (fused neighbour + atom-pair energy and gradient)",
+                "kernel_ms": kern_avg_ms,
+                "flops_per_launch": flops,
+                "peak_source": "measured: FMA-loop probe over all SMs in this run (tmol_b200_measure_fp32_peak)",
+                "hbm_peak_gbs": peaks.get("hbm_gbs"),
+            },
+            "e2e": {
+                "value": e2e_value,
+                "unit": "poses/s",
+                "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h,
+            },
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    del g
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        return run_reference(args, world, rank)
+    world, rank, local = dist_setup()
+    return run_b200(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

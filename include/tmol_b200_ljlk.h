@@ -84,15 +84,17 @@ typedef struct {
   double max_dis;            /* neighbour-detection reach */
 } tmol_b200_ljlk_inputs;
 
-/* Launch shape of the scoring kernels; zeros select the built-in defaults.
- *   rows_per_item   block rows (b1) per work item: a work item is
- *                   (pose, [r0, r0 + rows_per_item)) against every b2 >= b1
- *   warps_per_cta   warps per CTA; each warp evaluates one block pair at a time
- *   ctas_per_sm     resident CTAs per SM of the persistent grid */
+/* Launch shape of the scoring kernel; zeros select the built-in defaults.
+ * A work item is (pose, block b1, a range of later blocks b2 >= b1).
+ *   rows_per_item        work items a warp takes per atomic ticket
+ *   warps_per_cta        warps per CTA (at most 8); every warp works alone
+ *   ctas_per_sm          resident CTAs per SM of the persistent grid
+ *   candidates_per_item  candidate blocks b2 per work item (at most 1024) */
 typedef struct {
   int32_t rows_per_item;
   int32_t warps_per_cta;
   int32_t ctas_per_sm;
+  int32_t candidates_per_item;
 } tmol_b200_ljlk_launch;
 
 typedef struct tmol_b200_ljlk_plan tmol_b200_ljlk_plan;
@@ -106,6 +108,12 @@ int tmol_b200_ljlk_plan_create(const tmol_b200_ljlk_inputs* inputs,
                                void* stream, tmol_b200_ljlk_plan** plan_out);
 
 int tmol_b200_ljlk_plan_destroy(tmol_b200_ljlk_plan* plan);
+
+/* Reorders the plan's work items longest-first by the cost each item took
+ * in the last scoring call (synchronises the stream).  Coordinates change
+ * little between calls in minimisation or trajectory replay, so the order
+ * keeps the tail of the next launches short. */
+int tmol_b200_ljlk_plan_rebalance(tmol_b200_ljlk_plan* plan, void* stream);
 
 /* Changes the launch shape of an existing plan (autotuning). */
 int tmol_b200_ljlk_plan_set_launch(tmol_b200_ljlk_plan* plan,
@@ -156,6 +164,12 @@ int tmol_b200_ljlk_last_counts(tmol_b200_ljlk_plan* plan, void* stream,
 int tmol_b200_ljlk_profile(tmol_b200_ljlk_plan* plan, int enable);
 int tmol_b200_ljlk_profile_read(tmol_b200_ljlk_plan* plan, double* total_ms,
                                 int32_t* n_launches);
+
+/* Measurement helper with no counterpart in the reference: times a
+ * register-resident FMA loop over every SM and returns the device's FP32
+ * throughput in TFLOP/s, the denominator of the scoring kernel's roofline.
+ * Allocates 4 bytes and synchronises the stream. */
+int tmol_b200_measure_fp32_peak(void* stream, double* tflops);
 
 /* Sizes of the plan's device allocations in bytes. */
 int64_t tmol_b200_ljlk_plan_device_bytes(const tmol_b200_ljlk_plan* plan);

@@ -123,3 +123,24 @@ def test_plan_errors_are_raised(ubq_pose_stack, term):
     with pytest.raises(NativeError, match="index out of range"):
         LJLKPlan(coords, bad[:-1])
     clear_plan_cache()
+
+
+@pytest.mark.parametrize("block_pair", [False, True])
+def test_exotic_blocks_against_oracle(term, block_pair):
+    from exotic_blocks import exotic_pose_stack
+
+    ps = exotic_pose_stack()
+    P, B = ps.n_poses, ps.max_n_blocks
+    rng = numpy.random.default_rng(5)
+    w = rng.normal(size=(3, P, B, B) if block_pair else (3, P))
+    E, g, nbr = gpu_scores(ps, term, block_pair=block_pair, grad_weights=w)
+    oc = O.OracleCall(ps.coords.flatten(0, 1), pose_score_args(ps, term, block_pair))
+    Eo, dVo, nbro = oc.pose_scores(block_pair=block_pair, require_gradient=not block_pair)
+    E_close(E, Eo)
+    assert numpy.array_equal(nbr, nbro)
+    if block_pair:
+        go = oc.backward(nbro, w.astype(numpy.float32), per_pose_weights=False)
+    else:
+        pose = ps.pose_ind_for_atom.numpy()
+        go = (dVo * w[:, pose][:, :, None]).sum(0)
+    g_close(g, go)

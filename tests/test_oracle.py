@@ -7,6 +7,9 @@ compared there with atol 1e-5, rtol 1e-3), and bit-exact agreement with the
 reference op's energies, gradients and neighbour matrix.
 """
 
+import os
+import sys
+
 import numpy
 import pytest
 import torch
@@ -153,3 +156,21 @@ def test_lk_known_answers(term, f64):
         numpy.testing.assert_allclose(
             O.potential("lk_V", d, 6, i, j, gp, f64), O.potential("lk_V_dV", d, 6, i, j, gp, f64)[0], rtol=1e-5
         )
+
+
+def test_exotic_blocks_oracle_matches_reference(term):
+    """Multi-tile blocks, three connections and ligand fragments: the oracle
+    against the compiled reference op (skipped where it is not built)."""
+    from exotic_blocks import exotic_pose_stack
+
+    if not O.reference_available():
+        pytest.skip("reference op not built")
+    ps = exotic_pose_stack()
+    assert ps.packed_block_types.max_n_conn == 3 and ps.packed_block_types.max_n_atoms > 32
+    args = pose_score_args(ps, term)
+    E, c, nbr = O.reference_pose_scores(ps.coords.flatten(0, 1), args)
+    E.sum().backward()
+    Eo, dVo, nbro = O.OracleCall(ps.coords.flatten(0, 1), args).pose_scores(require_gradient=True)
+    assert numpy.array_equal(E.detach().numpy(), Eo)
+    assert numpy.array_equal(dVo.sum(0), c.grad.numpy())
+    assert numpy.array_equal(nbr.numpy(), nbro)

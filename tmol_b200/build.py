@@ -46,6 +46,7 @@ def build(force=False, verbose=False, extra=()):
         + [
             "-O3",
             "-lineinfo",
+            "--use_fast_math",
             "-std=c++17",
             "-Xcompiler",
             "-fPIC",

@@ -5,27 +5,29 @@
 // Layout in HBM (per PoseStack, built once by tmol_b200_ljlk_plan_create):
 //   blk_bt[P*B], blk_off[P*B]      block type and first-atom offset per block
 //   pose_last[P]                   1 + index of each pose's last real block
-//   atom_params[nbt*A]             per block-type atom LJ/LK parameters + flags
+//   bt_tf[nbt*A]                   per block-type atom: compact atom type | heavy
+//   ljtab, lktab[ntp*ntp]          per atom-type-pair LJ / LK constants
 //   bt_pd[nbt][A][A] (u8)          intra-block bond separation
 //   bt_conn_pd[nbt][C][A] (u8)     bond separation from each connection atom
 //   cp_*[P*B][CP_CAP]              per block: the later blocks within
 //                                  count-pair reach (min bond separation <= 4)
 //                                  with their connection-pair separations;
 //                                  replaces the dense [P,B,B,C,C] tensor
-//   work[n_work] (int4)            (pose, first row, end row) work items
+//   work[n_work] (int4)            rows: (pose, b1) for every block slot up
+//                                  to each pose's last real block
 //   spheres[P*B][4]                centroid + radius, rebuilt every call
 //
-// Scoring (one persistent launch per call, after the sphere kernel):
-// CTAs take work items from an atomic ticket.  For item (p, [r0, r1)) the
-// CTA tests every candidate pair (b1 in [r0, r1), b2 in [b1, nb)) against the
-// bounding-sphere rule of tmol/score/common/sphere_overlap.impl.hh:287-351,
-// queues the hits in shared memory, and its warps evaluate the queued block
-// pairs, one block pair per warp: the two blocks' atoms (tiles of 32) are
-// staged in the warp's shared-memory slab and the warp strides over the atom
-// pairs.  Energies stay in registers for the whole item and are reduced once
-// per item (whole-pose) or once per block pair (block-pair output).  The
-// adjoint accumulates per-atom gradients in the slab with shared-memory
-// atomics and flushes each atom once per block pair to global memory.
+// Scoring (one persistent launch per call, after the sphere kernel): every
+// warp is an independent worker taking rows from an atomic ticket.  For row
+// (p, b1) it stages b1's atoms (a tile of 32) in its shared-memory slab,
+// tests b1 against all later blocks of the pose with the bounding-sphere rule
+// (32 candidates per ballot) and evaluates each neighbouring block pair at
+// once, in two phases: a screening pass over all atom pairs (distance and
+// count-pair weight) compacts the pairs that contribute into a per-warp
+// queue, split into LJ-only and heavy-atom (LJ + LK) pairs, and a dense pass
+// evaluates the queue with every lane busy.  Energies stay in registers for
+// the whole row; gradients accumulate in the slab (b1's across the whole
+// row) and are flushed to global memory once per block pair (b2) or row (b1).
 
 #include <cuda_runtime.h>
 
@@ -42,9 +44,8 @@ namespace tmol_b200 {
 constexpr int TILE = 32;
 constexpr int MAX_CONN = 4;
 constexpr int CP_CAP = 16;
-constexpr int QUEUE_CAP = 1024;
 constexpr int MAX_ROWS_PER_ITEM = 64;
-constexpr int MAX_WARPS = 16;
+constexpr int MAX_WARPS = 8;
 
 enum StatusBits : int {
   kStIndex = 1,
@@ -121,12 +122,12 @@ __global__ void plan_blocks_kernel(PlanBuildArgs a) {
   }
 }
 
-template <typename Real>
-__global__ void plan_block_types_kernel(PlanBuildArgs a,
-                                        AtomParams<Real>* atom_params) {
+// Per block-type atom: compact type index | heavy flag, byte copies of the
+// bond-separation tables, and index validation.
+__global__ void plan_block_types_kernel(PlanBuildArgs a, const int* type_map,
+                                        uint16_t* bt_tf) {
   const tmol_b200_ljlk_inputs& in = a.in;
   int nbt = in.n_block_types, A = in.max_n_block_atoms, C = in.max_n_conn;
-  const Real* tp = (const Real*)in.type_params;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nbt * A;
        i += gridDim.x * blockDim.x) {
     int bt = i / A, at = i - bt * A;
@@ -135,32 +136,20 @@ __global__ void plan_block_types_kernel(PlanBuildArgs a,
       if (at == 0) atomicOr(a.status, kStIndex);
       continue;
     }
-    AtomParams<Real> prm = {};
+    uint16_t tf = 0;
     if (at < n) {
       int t = in.bt_atom_types[i];
-      if (t < 0 || t >= in.n_atom_types) {
+      if (t < 0 || t >= in.n_atom_types || type_map[t] < 0) {
         atomicOr(a.status, kStIndex);
       } else {
-        const Real* r = tp + 10 * (int64_t)t;
-        prm.lj_radius = r[0];
-        prm.lj_wdepth = r[1];
-        prm.lk_dgfree = r[2];
-        prm.lk_lambda = r[3];
-        prm.lk_volume = r[4];
-        int f = 0;
-        if (r[5] != 0) f |= kDonor;
-        if (r[6] != 0) f |= kHydroxyl;
-        if (r[7] != 0) f |= kPolarH;
-        if (r[8] != 0) f |= kAcceptor;
-        if (r[9] != 0) f |= kCarbonLK;
-        prm.flags = f | a.bt_flags[i];
+        tf = (uint16_t)(type_map[t] | (a.bt_flags[i] == kHeavy ? 256 : 0));
       }
       for (int at2 = 0; at2 < A; ++at2) {
         int v = in.bt_path_distance[(int64_t)i * A + at2];
         a.bt_pd[(int64_t)i * A + at2] = (uint8_t)(v < 0 ? 0 : (v > 255 ? 255 : v));
       }
     }
-    atom_params[i] = prm;
+    bt_tf[i] = tf;
     int nc = in.bt_n_conn[bt];
     if (at == 0 && (nc < 0 || nc > C)) atomicOr(a.status, kStIndex);
     for (int c = 0; c < C; ++c) {
@@ -176,6 +165,35 @@ __global__ void plan_block_types_kernel(PlanBuildArgs a,
       }
       a.bt_conn_pd[((int64_t)bt * C + c) * A + at] = v;
     }
+  }
+}
+
+// Type-pair tables for every ordered pair of the compact atom types.
+template <typename Real>
+__global__ void plan_tables_kernel(const Real* type_params, const Real* gp,
+                                   const int* compact_types, int ntp,
+                                   LJRecord<Real>* ljtab, LKRecord<Real>* lktab) {
+  GlobalParams<Real> g = {gp[0], gp[1], gp[2], gp[3], gp[4]};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ntp * ntp;
+       i += gridDim.x * blockDim.x) {
+    AtomParams<Real> pr[2];
+    int ts[2] = {compact_types[i / ntp], compact_types[i % ntp]};
+    for (int k = 0; k < 2; ++k) {
+      const Real* r = type_params + 10 * (int64_t)ts[k];
+      pr[k].lj_radius = r[0];
+      pr[k].lj_wdepth = r[1];
+      pr[k].lk_dgfree = r[2];
+      pr[k].lk_lambda = r[3];
+      pr[k].lk_volume = r[4];
+      int f = 0;
+      if (r[5] != 0) f |= kDonor;
+      if (r[6] != 0) f |= kHydroxyl;
+      if (r[7] != 0) f |= kPolarH;
+      if (r[8] != 0) f |= kAcceptor;
+      if (r[9] != 0) f |= kCarbonLK;
+      pr[k].flags = f;
+    }
+    build_records(pr[0], pr[1], g, ljtab[i], lktab[i]);
   }
 }
 
@@ -255,7 +273,10 @@ struct ScoreArgs {
   const int* blk_bt;
   const int* blk_off;
   const int* pose_last;
-  const AtomParams<Real>* atom_params;
+  const uint16_t* bt_tf;  // per block-type atom: compact type | heavy << 8
+  const LJRecord<Real>* ljtab;
+  const LKRecord<Real>* lktab;
+  int ntp;  // compact atom types (tables are ntp x ntp)
   const uint8_t* bt_pd;
   const uint8_t* bt_conn_pd;
   const int* bt_n_atoms;
@@ -269,6 +290,7 @@ struct ScoreArgs {
   GlobalParams<Real> g;
   Real reach;
   const int4* work;
+  int* item_cost;  // measured cost of each work item (clock cycles / 16)
   int n_work;
   int P, B, A, C;
   Real* energies;
@@ -320,195 +342,60 @@ __global__ void spheres_kernel(ScoreArgs<Real> s) {
   }
 }
 
-template <typename Real>
-struct WarpSlab {
-  Real x[2][TILE], y[2][TILE], z[2][TILE];
-  AtomParams<Real> prm[2][TILE];
-  Real gx[2][TILE], gy[2][TILE], gz[2][TILE];
-  uint8_t cpd[2][MAX_CONN][TILE];
-  uint8_t seps[16];
+// ---------------------------------------------------------------------------
+// Per-warp shared-memory slab.
+//
+// Side 0 holds a tile (<= 32 atoms) of the row block b1; side 1 packs the
+// atoms of up to MAX_SLOTS neighbouring blocks b2 (at most M1 atoms), so that
+// one screening pass covers several block pairs with every lane busy.  The
+// pair queue collects the atom pairs that contribute (inside max_dis with a
+// non-zero count-pair weight): LJ-only pairs from the front, heavy-atom
+// (LJ + LK) pairs from the back.  An entry packs a1 (5 bits) | j (6 bits) |
+// count-pair-weight-0.2 flag (bit 11) | j-on-side-0 flag (bit 12).
+
+constexpr int M1 = 64;
+constexpr int MAX_SLOTS = 8;
+constexpr int QCAP = 512;
+constexpr int kTfHeavy = 256;
+
+enum SlotKind : int {
+  kSlotFar = 0,       // bond separation > 4 everywhere: weight 1
+  kSlotStriking = 1,  // count pair through the connection atoms
+  kSlotIntra = 2,     // another tile of block b1: intra-block separation table
 };
 
 template <typename Real>
-__device__ __forceinline__ void stage_tile(const ScoreArgs<Real>& s,
-                                           WarpSlab<Real>& w, int side, int bt,
-                                           int off, int start, int cnt,
-                                           int nconn, bool striking, int lane,
-                                           bool grad) {
-  if (lane < cnt) {
-    int at = start + lane;
-    const Real* c = s.coords + 3 * ((int64_t)off + at);
-    w.x[side][lane] = c[0];
-    w.y[side][lane] = c[1];
-    w.z[side][lane] = c[2];
-    w.prm[side][lane] = s.atom_params[(int64_t)bt * s.A + at];
-    if (striking) {
-      for (int k = 0; k < nconn; ++k)
-        w.cpd[side][k][lane] = s.bt_conn_pd[((int64_t)bt * s.C + k) * s.A + at];
-    }
-    if (grad) {
-      w.gx[side][lane] = 0;
-      w.gy[side][lane] = 0;
-      w.gz[side][lane] = 0;
-    }
-  }
-}
+struct Slab {
+  Real x0[TILE], y0[TILE], z0[TILE];
+  Real gx0[TILE], gy0[TILE], gz0[TILE];
+  uint32_t cpd0[TILE];  // bond separation to each connection atom, a byte each
+  uint16_t tf0[TILE];
+  Real x1[M1], y1[M1], z1[M1];
+  Real gx1[M1], gy1[M1], gz1[M1];
+  uint32_t cpd1[M1];
+  int gidx1[M1];  // global atom index
+  uint16_t tf1[M1];
+  uint8_t slot1[M1];   // slot of the packed atom
+  uint8_t local1[M1];  // atom index within its block
+  uint8_t seps[MAX_SLOTS][16];
+  int slot_kind[MAX_SLOTS], slot_nc[MAX_SLOTS], slot_lig[MAX_SLOTS];
+  Real slot_sph[MAX_SLOTS][4];  // bounding sphere of each slot's block
+  unsigned long long counts[8];
+  uint16_t queue[QCAP];
+};
 
-template <typename Real>
-__device__ __forceinline__ void flush_tile(const ScoreArgs<Real>& s,
-                                           WarpSlab<Real>& w, int side,
-                                           int off, int start, int cnt,
-                                           int lane) {
-  if (lane < cnt) {
-    Real* d = s.dcoords + 3 * ((int64_t)off + start + lane);
-    Real gx = w.gx[side][lane], gy = w.gy[side][lane], gz = w.gz[side][lane];
-    if (gx != 0) atomicAdd(d + 0, gx);
-    if (gy != 0) atomicAdd(d + 1, gy);
-    if (gz != 0) atomicAdd(d + 2, gz);
-  }
-}
+struct RowInfo {
+  int p, b1, i1, bt1, off1, n1, nc1, lig1;
+  int st1, c1;  // tile of b1 in side 0
+};
 
 // Per-warp work counters (units of the throughput and roofline figures):
 //   [0] block pairs, [1] atom pairs (inter n1*n2, intra n(n-1)/2),
 //   [2] heavy-atom pairs (same rule), [3] atom pairs inside max_dis with a
 //   non-zero count-pair weight, [4] heavy-atom pairs among those.
+// All are warp-uniform.
 constexpr int N_COUNTS = 5;
 
-struct WarpCounts {
-  long long c[N_COUNTS];
-};
-
-// All atom pairs of one block pair.  GRAD: accumulate sum_t wt[t] * dE_t/dx
-// into the slab (and the energies into acc); else add the energies to acc.
-template <typename Real, bool GRAD>
-__device__ void eval_block_pair(const ScoreArgs<Real>& s, WarpSlab<Real>& w,
-                                int p, int b1, int b2, int lane, Real acc[3],
-                                const Real wt[3], WarpCounts& cnt) {
-  int i1 = p * s.B + b1, i2 = p * s.B + b2;
-  int bt1 = s.blk_bt[i1], bt2 = s.blk_bt[i2];
-  int off1 = s.blk_off[i1], off2 = s.blk_off[i2];
-  int n1 = s.bt_n_atoms[bt1], n2 = s.bt_n_atoms[bt2];
-  bool intra = b1 == b2;
-  bool lig = s.bt_is_ligand[bt1] && s.bt_is_ligand[bt2];
-  int minsep = 6;
-  bool striking = false;
-  int nc1 = 0, nc2 = 0;
-  if (!intra) {
-    int ncp = s.cp_count[i1];
-    for (int k = 0; k < ncp; ++k) {
-      int e = i1 * CP_CAP + k;
-      if (s.cp_b2[e] == b2) {
-        minsep = s.cp_minsep[e];
-        striking = true;
-        if (lane < 16) w.seps[lane] = s.cp_seps[(int64_t)e * 16 + lane];
-        break;
-      }
-    }
-    if (striking) {
-      nc1 = s.bt_n_conn[bt1];
-      nc2 = s.bt_n_conn[bt2];
-    }
-  }
-  cnt.c[0] += 1;
-  cnt.c[1] += intra ? (long long)n1 * (n1 - 1) / 2 : (long long)n1 * n2;
-  const Real maxd2 = s.g.max_dis * s.g.max_dis;
-  long long h_all = 0;
-  int n_in = 0, n_in_heavy = 0;
-  int nt1 = (n1 + TILE - 1) / TILE, nt2 = (n2 + TILE - 1) / TILE;
-  for (int ti = 0; ti < nt1; ++ti) {
-    int st1 = ti * TILE;
-    int c1 = min(TILE, n1 - st1);
-    stage_tile(s, w, 0, bt1, off1, st1, c1, nc1, striking, lane, GRAD);
-    __syncwarp();
-    int h1 = __popc(__ballot_sync(0xffffffffu, lane < c1 && (w.prm[0][lane].flags & kHeavy)));
-    for (int tj = intra ? ti : 0; tj < nt2; ++tj) {
-      int st2 = tj * TILE;
-      int c2 = min(TILE, n2 - st2);
-      bool same = intra && ti == tj;
-      int side2 = same ? 0 : 1;
-      if (!same) stage_tile(s, w, 1, bt2, off2, st2, c2, nc2, striking, lane, GRAD);
-      __syncwarp();
-      int h2 = same ? h1
-                    : __popc(__ballot_sync(0xffffffffu,
-                                           lane < c2 && (w.prm[1][lane].flags & kHeavy)));
-      h_all += same ? (long long)h1 * (h1 - 1) / 2 : (long long)h1 * h2;
-      int npairs = c1 * c2;
-      for (int k = lane; k < npairs; k += 32) {
-        int a1 = k / c2;
-        int a2 = k - a1 * c2;
-        if (same && a1 >= a2) continue;
-        Real dx = w.x[0][a1] - w.x[side2][a2];
-        Real dy = w.y[0][a1] - w.y[side2][a2];
-        Real dz = w.z[0][a1] - w.z[side2][a2];
-        Real d2 = dx * dx + dy * dy + dz * dz;
-        if (!(d2 < maxd2)) continue;
-        int sep;
-        if (intra) {
-          sep = s.bt_pd[((int64_t)bt1 * s.A + st1 + a1) * s.A + st2 + a2];
-        } else if (striking) {
-          sep = 5;
-          for (int u = 0; u < nc1; ++u) {
-            int pd1 = w.cpd[0][u][a1];
-            for (int v = 0; v < nc2; ++v) {
-              int t = pd1 + w.seps[u * 4 + v] + w.cpd[1][v][a2];
-              sep = t < sep ? t : sep;
-            }
-          }
-        } else {
-          sep = minsep;
-        }
-        if (lig && (sep == 3 || sep == 4)) sep = 5;
-        Real wcp = connectivity_weight<Real>(sep);
-        if (wcp == Real(0)) continue;
-        Real d = sqrt(d2);
-        const AtomParams<Real>& pa = w.prm[0][a1];
-        const AtomParams<Real>& pb = w.prm[side2][a2];
-        LJPair<Real> q = lj_pair(pa, pb, s.g);
-        bool heavy = (pa.flags & kHeavy) && (pb.flags & kHeavy);
-        ++n_in;
-        n_in_heavy += heavy;
-        if (!GRAD) {
-          Real atr, rep;
-          lj_V(d, q, atr, rep);
-          acc[0] += wcp * atr;
-          acc[1] += wcp * rep;
-          if (heavy) acc[2] += wcp * lk_V(d, q.sigma, pa, pb, s.g.max_dis);
-        } else {
-          Real atr, rep, datr, drep;
-          lj_V_dV(d, q, atr, rep, datr, drep);
-          acc[0] += wcp * atr;
-          acc[1] += wcp * rep;
-          Real dE = wt[0] * datr + wt[1] * drep;
-          if (heavy) {
-            Real lk, dlk;
-            lk_V_dV(d, q.sigma, pa, pb, s.g.max_dis, lk, dlk);
-            acc[2] += wcp * lk;
-            dE += wt[2] * dlk;
-          }
-          dE *= wcp;
-          if (dE != Real(0) && d != Real(0)) {
-            Real f = dE / d;
-            Real fx = f * dx, fy = f * dy, fz = f * dz;
-            atomicAdd(&w.gx[0][a1], fx);
-            atomicAdd(&w.gy[0][a1], fy);
-            atomicAdd(&w.gz[0][a1], fz);
-            atomicAdd(&w.gx[side2][a2], -fx);
-            atomicAdd(&w.gy[side2][a2], -fy);
-            atomicAdd(&w.gz[side2][a2], -fz);
-          }
-        }
-      }
-      __syncwarp();
-      if (GRAD && !same) flush_tile(s, w, 1, off2, st2, c2, lane);
-      __syncwarp();
-    }
-    if (GRAD) flush_tile(s, w, 0, off1, st1, c1, lane);
-    __syncwarp();
-  }
-  cnt.c[2] += h_all;
-  cnt.c[3] += n_in;
-  cnt.c[4] += n_in_heavy;
-}
 
 template <typename Real>
 __device__ __forceinline__ Real warp_sum(Real v) {
@@ -516,129 +403,659 @@ __device__ __forceinline__ Real warp_sum(Real v) {
   return v;
 }
 
-// The fused per-item kernel.  GRAD selects the adjoint (which also yields
-// the energies when s.energies is set); BLOCK_PAIR selects per-block-pair
-// energies / weights instead of per-pose ones.
-template <typename Real, bool GRAD, bool BLOCK_PAIR>
-__global__ void __launch_bounds__(32 * MAX_WARPS)
-    score_kernel(ScoreArgs<Real> s, int rows_per_item) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int n_warps = blockDim.x >> 5;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  WarpSlab<Real>* slabs = reinterpret_cast<WarpSlab<Real>*>(smem_raw);
-  WarpSlab<Real>& w = slabs[warp];
-  int* queue = reinterpret_cast<int*>(slabs + n_warps);
-  __shared__ int s_item, s_qcount;
-  __shared__ int s_rowoff[MAX_ROWS_PER_ITEM + 1];
-  __shared__ Real s_red[3][MAX_WARPS];
-  __shared__ unsigned long long s_cnt[N_COUNTS];
-  if (threadIdx.x < N_COUNTS) s_cnt[threadIdx.x] = 0;
-  WarpCounts cnt = {};
-  const bool want_E = !GRAD || s.energies != nullptr;
+template <typename Real>
+__device__ __forceinline__ uint32_t load_cpd(const ScoreArgs<Real>& s, int bt,
+                                             int nconn, int at) {
+  uint32_t v = 0x06060606u;
+  for (int k = 0; k < nconn; ++k) {
+    uint32_t d = s.bt_conn_pd[((int64_t)bt * s.C + k) * s.A + at];
+    v = (v & ~(0xffu << (8 * k))) | (d << (8 * k));
+  }
+  return v;
+}
 
-  for (;;) {
-    __syncthreads();
-    if (threadIdx.x == 0) s_item = atomicAdd(s.ticket, 1);
-    __syncthreads();
-    int item = s_item;
-    if (item >= s.n_work) break;
-    int4 wi = s.work[item];
-    int p = wi.x, r0 = wi.y, r1 = wi.z;
-    int nb = s.pose_last[p];
-    int nrows = r1 - r0;
-    if (threadIdx.x == 0) {
-      int acc = 0;
-      for (int r = 0; r < nrows; ++r) {
-        s_rowoff[r] = acc;
-        acc += nb - (r0 + r);
+// Stage atoms [start, start + cnt) of block (bt, off) into side 0.
+template <typename Real>
+__device__ __forceinline__ void stage_side0(const ScoreArgs<Real>& s,
+                                            Slab<Real>& w, int bt, int off,
+                                            int start, int cnt, int nconn,
+                                            int lane) {
+  if (lane < cnt) {
+    int at = start + lane;
+    const Real* c = s.coords + 3 * ((int64_t)off + at);
+    w.x0[lane] = c[0];
+    w.y0[lane] = c[1];
+    w.z0[lane] = c[2];
+    w.tf0[lane] = s.bt_tf[(int64_t)bt * s.A + at];
+    w.cpd0[lane] = load_cpd(s, bt, nconn, at);
+    w.gx0[lane] = 0;
+    w.gy0[lane] = 0;
+    w.gz0[lane] = 0;
+  }
+}
+
+// Append the atoms of [start, start + cnt) of block (bt, off) that can reach
+// block b1 to side 1 at j0: an atom farther than r1 + max_dis from b1's
+// centroid is farther than max_dis from every b1 atom, and every term is zero
+// there.  Returns the number of atoms kept.
+template <typename Real>
+__device__ __forceinline__ int stage_side1(const ScoreArgs<Real>& s,
+                                           Slab<Real>& w, int j0, int slot,
+                                           int bt, int off, int start,
+                                           int cnt, int nconn, Real cx,
+                                           Real cy, Real cz, Real reach2,
+                                           int lane) {
+  bool keep = false;
+  Real x = 0, y = 0, z = 0;
+  int at = start + lane;
+  if (lane < cnt) {
+    const Real* c = s.coords + 3 * ((int64_t)off + at);
+    x = c[0];
+    y = c[1];
+    z = c[2];
+    Real dx = x - cx, dy = y - cy, dz = z - cz;
+    keep = dx * dx + dy * dy + dz * dz < reach2;
+  }
+  unsigned km = __ballot_sync(0xffffffffu, keep);
+  if (keep) {
+    int j = j0 + __popc(km & ((1u << lane) - 1));
+    w.x1[j] = x;
+    w.y1[j] = y;
+    w.z1[j] = z;
+    w.tf1[j] = s.bt_tf[(int64_t)bt * s.A + at];
+    w.cpd1[j] = load_cpd(s, bt, nconn, at);
+    w.gidx1[j] = off + at;
+    w.slot1[j] = (uint8_t)slot;
+    w.local1[j] = (uint8_t)at;
+    w.gx1[j] = 0;
+    w.gy1[j] = 0;
+    w.gz1[j] = 0;
+  }
+  return __popc(km);
+}
+
+template <typename Real>
+__device__ __forceinline__ void flush_side0(const ScoreArgs<Real>& s,
+                                            Slab<Real>& w, int off, int start,
+                                            int cnt, int lane) {
+  if (lane < cnt) {
+    Real* d = s.dcoords + 3 * ((int64_t)off + start + lane);
+    Real gx = w.gx0[lane], gy = w.gy0[lane], gz = w.gz0[lane];
+    if (gx != 0) atomicAdd(d + 0, gx);
+    if (gy != 0) atomicAdd(d + 1, gy);
+    if (gz != 0) atomicAdd(d + 2, gz);
+  }
+}
+
+template <typename Real>
+__device__ __forceinline__ void flush_side1(const ScoreArgs<Real>& s,
+                                            Slab<Real>& w, int m, int lane) {
+  for (int j = lane; j < m; j += 32) {
+    Real* d = s.dcoords + 3 * (int64_t)w.gidx1[j];
+    Real gx = w.gx1[j], gy = w.gy1[j], gz = w.gz1[j];
+    if (gx != 0) atomicAdd(d + 0, gx);
+    if (gy != 0) atomicAdd(d + 1, gy);
+    if (gz != 0) atomicAdd(d + 2, gz);
+  }
+}
+
+// What the out-of-line screening and evaluation functions need, by value.
+template <typename Real>
+struct EvalCtx {
+  const LJRecord<Real>* ljtab;
+  const LKRecord<Real>* lktab;
+  const uint8_t* pd;  // intra-block separations of b1, row st1 (tile start)
+  int ntp, A;
+  Real max_dis;
+  Real wt0, wt1, wt2;  // gradient weights of the three terms
+};
+
+template <typename Real>
+struct E3 {
+  Real atr, rep, lk;
+};
+
+__device__ __forceinline__ void cnt_add(unsigned long long* c, int k, long long v, int lane) {
+  if (lane == 0) c[k] += (unsigned long long)v;
+}
+
+// Dense evaluation of one queue (HEAVY: LJ + LK, else LJ only); returns the
+// lane's energy sums.  Entries come in screening order, so lanes sharing a1
+// are mostly contiguous: their a1 forces are summed with a segmented shuffle
+// reduction and added once per segment.
+template <typename Real, bool GRAD, bool HEAVY>
+__device__ __noinline__ E3<Real> eval_queue(EvalCtx<Real> c, Slab<Real>* wp,
+                                            int n, int lane) {
+  Slab<Real>& w = *wp;
+  E3<Real> acc = {0, 0, 0};
+  const Real dmax = c.max_dis;
+  const Real far_dmin = c.max_dis - Real(1.5);
+  for (int base = 0; base < n; base += 32) {
+    int i = base + lane;
+    bool act = i < n;
+    int e = act ? (int)w.queue[HEAVY ? QCAP - 1 - i : i] : 0;
+    int a1 = e & 31, j = (e >> 5) & 63;
+    bool to0 = (e >> 12) & 1;
+    Real wcp = (e >> 11) & 1 ? Real(0.2) : Real(1);
+    Real fx = 0, fy = 0, fz = 0;
+    if (act) {
+      Real x2 = to0 ? w.x0[j] : w.x1[j];
+      Real y2 = to0 ? w.y0[j] : w.y1[j];
+      Real z2 = to0 ? w.z0[j] : w.z1[j];
+      int t2 = (to0 ? w.tf0[j] : w.tf1[j]) & 0xff;
+      int t1 = w.tf0[a1] & 0xff;
+      Real dx = w.x0[a1] - x2;
+      Real dy = w.y0[a1] - y2;
+      Real dz = w.z0[a1] - z2;
+      Real d = sqrt(dx * dx + dy * dy + dz * dz);
+      int tp = t1 * c.ntp + t2;
+      LJRecord<Real> lr = c.ljtab[tp];
+      Real atr, rep, datr, drep;
+      lj_eval<Real, GRAD>(d, lr, dmax, atr, rep, datr, drep);
+      acc.atr += wcp * atr;
+      acc.rep += wcp * rep;
+      Real dE = c.wt0 * datr + c.wt1 * drep;
+      if (HEAVY) {
+        LKRecord<Real> kr = c.lktab[tp];
+        Real lk, dlk;
+        lk_eval<Real, GRAD>(d, kr, far_dmin, dmax, lk, dlk);
+        acc.lk += wcp * lk;
+        dE += c.wt2 * dlk;
       }
-      s_rowoff[nrows] = acc;
+      if (GRAD && d != Real(0)) {
+        Real f = wcp * dE / d;
+        fx = f * dx;
+        fy = f * dy;
+        fz = f * dz;
+      }
     }
-    Real acc[3] = {0, 0, 0};
-    Real wt[3] = {0, 0, 0};
-    if (GRAD && !BLOCK_PAIR) {
-      for (int t = 0; t < 3; ++t) wt[t] = s.dTdV[t * s.P + p];
-    }
-    __syncthreads();
-    int n_cand = s_rowoff[nrows];
-    for (int base = 0; base < n_cand; base += QUEUE_CAP) {
-      if (threadIdx.x == 0) s_qcount = 0;
-      __syncthreads();
-      int end = min(base + QUEUE_CAP, n_cand);
-      for (int c = base + threadIdx.x; c < end; c += blockDim.x) {
-        int r = 0;
-        while (r + 1 < nrows && s_rowoff[r + 1] <= c) ++r;
-        int b1 = r0 + r;
-        int b2 = b1 + (c - s_rowoff[r]);
-        int i1 = p * s.B + b1, i2 = p * s.B + b2;
-        bool hit = false;
-        if (s.blk_bt[i1] >= 0 && s.blk_bt[i2] >= 0) {
-          const Real* s1 = s.spheres + 4 * (int64_t)i1;
-          const Real* s2 = s.spheres + 4 * (int64_t)i2;
-          Real dx = sub_rn(s1[0], s2[0]);
-          Real dy = sub_rn(s1[1], s2[1]);
-          Real dz = sub_rn(s1[2], s2[2]);
-          Real d2 = add_rn(add_rn(mul_rn(dx, dx), mul_rn(dy, dy)), mul_rn(dz, dz));
-          Real thr = add_rn(add_rn(s1[3], s2[3]), s.reach);
-          hit = d2 < mul_rn(thr, thr);
-        }
-        if (s.nbr) s.nbr[(int64_t)i1 * s.B + b2] = hit ? 1 : 0;
-        if (hit) {
-          int slot = atomicAdd(&s_qcount, 1);
-          queue[slot] = b1 | (b2 << 16);
+    if (GRAD) {
+      // segments: maximal runs of lanes with equal a1; a run only merges
+      // lanes before the next segment head, so a1 values that recur later
+      // in the warp form separate segments
+      int key = act ? a1 : -1 - lane;
+      int kprev = __shfl_up_sync(0xffffffffu, key, 1);
+      bool head = lane == 0 || kprev != key;
+      unsigned heads = __ballot_sync(0xffffffffu, head);
+      unsigned after = heads & ~((2u << lane) - 1u);
+      int seg_end = after ? __ffs(after) - 1 : 32;
+      Real sx = fx, sy = fy, sz = fz;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        Real tx = __shfl_down_sync(0xffffffffu, sx, o);
+        Real ty = __shfl_down_sync(0xffffffffu, sy, o);
+        Real tz = __shfl_down_sync(0xffffffffu, sz, o);
+        if (lane + o < seg_end) {
+          sx += tx;
+          sy += ty;
+          sz += tz;
         }
       }
-      __syncthreads();
-      int nq = s_qcount;
-      for (int e = warp; e < nq; e += n_warps) {
-        int pk = queue[e];
-        int b1 = pk & 0xffff, b2 = pk >> 16;
-        if (BLOCK_PAIR) {
-          int64_t o = ((int64_t)p * s.B + b1) * s.B + b2;
-          int64_t stride = (int64_t)s.P * s.B * s.B;
-          if (GRAD) {
-            for (int t = 0; t < 3; ++t) wt[t] = s.dTdV[t * stride + o];
-          }
-          Real pacc[3] = {0, 0, 0};
-          eval_block_pair<Real, GRAD>(s, w, p, b1, b2, lane, pacc, wt, cnt);
-          if (want_E) {
-            for (int t = 0; t < 3; ++t) {
-              Real v = warp_sum(pacc[t]);
-              if (lane == 0) s.energies[t * stride + o] = v;
+      if (act && head && (sx != 0 || sy != 0 || sz != 0)) {
+        atomicAdd(&w.gx0[a1], sx);
+        atomicAdd(&w.gy0[a1], sy);
+        atomicAdd(&w.gz0[a1], sz);
+      }
+      if (act && (fx != 0 || fy != 0 || fz != 0)) {
+        Real* gx = to0 ? w.gx0 : w.gx1;
+        Real* gy = to0 ? w.gy0 : w.gy1;
+        Real* gz = to0 ? w.gz0 : w.gz1;
+        atomicAdd(&gx[j], -fx);
+        atomicAdd(&gy[j], -fy);
+        atomicAdd(&gz[j], -fz);
+      }
+    }
+  }
+  return acc;
+}
+
+template <typename Real, bool GRAD>
+__device__ __forceinline__ void drain_queue(const EvalCtx<Real>& c,
+                                            Slab<Real>* wp, int& nl, int& nh,
+                                            int lane, E3<Real>& acc) {
+  __syncwarp();
+  cnt_add(wp->counts, 3, nl + nh, lane);
+  cnt_add(wp->counts, 4, nh, lane);
+  if (nh) {
+    E3<Real> e = eval_queue<Real, GRAD, true>(c, wp, nh, lane);
+    acc.atr += e.atr;
+    acc.rep += e.rep;
+    acc.lk += e.lk;
+  }
+  if (nl) {
+    E3<Real> e = eval_queue<Real, GRAD, false>(c, wp, nl, lane);
+    acc.atr += e.atr;
+    acc.rep += e.rep;
+  }
+  __syncwarp();
+  nl = 0;
+  nh = 0;
+}
+
+__device__ __forceinline__ void queue_push(uint16_t* queue, bool in, bool hv,
+                                           int entry, int lane, int& nl,
+                                           int& nh) {
+  unsigned lt = (1u << lane) - 1;
+  unsigned mh = __ballot_sync(0xffffffffu, hv);
+  unsigned ml = __ballot_sync(0xffffffffu, in && !hv);
+  if ((mh | ml) == 0) return;
+  if (hv) queue[QCAP - 1 - (nh + __popc(mh & lt))] = (uint16_t)entry;
+  if (in && !hv) queue[nl + __popc(ml & lt)] = (uint16_t)entry;
+  nh += __popc(mh);
+  nl += __popc(ml);
+}
+
+// Pairs inside the side-0 tile of c1 atoms (a1 < a2), weights from the
+// intra-block separation table (ljlk_pose_score.impl.hh:115-134; the ligand
+// 3/4 -> 5 rule is already folded into that table and is not applied again).
+template <typename Real, bool GRAD>
+__device__ __noinline__ E3<Real> intra_tile(EvalCtx<Real> c, Slab<Real>* wp,
+                                            int st1, int c1, int lane) {
+  Slab<Real>& w = *wp;
+  E3<Real> acc = {0, 0, 0};
+  const Real maxd2 = c.max_dis * c.max_dis;
+  int nl = 0, nh = 0;
+  int npairs = c1 * c1;
+  int qq = TILE / c1, rr = TILE - qq * c1;
+  int a1 = lane / c1, a2 = lane - a1 * c1;
+  for (int base = 0; base < npairs; base += 32) {
+    bool in = false, hv = false;
+    int wbit = 0;
+    if (base + lane < npairs && a1 < a2) {
+      Real dx = w.x0[a1] - w.x0[a2];
+      Real dy = w.y0[a1] - w.y0[a2];
+      Real dz = w.z0[a1] - w.z0[a2];
+      Real d2 = dx * dx + dy * dy + dz * dz;
+      if (d2 < maxd2) {
+        int sep = c.pd[a1 * c.A + st1 + a2];
+        in = sep >= 4;
+        wbit = sep == 4;
+        hv = in && (w.tf0[a1] & w.tf0[a2] & kTfHeavy);
+      }
+    }
+    queue_push(w.queue, in, hv, a1 | (a2 << 5) | (wbit << 11) | (1 << 12), lane, nl, nh);
+    a1 += qq;
+    a2 += rr;
+    if (a2 >= c1) {
+      a2 -= c1;
+      a1 += 1;
+    }
+  }
+  drain_queue<Real, GRAD>(c, wp, nl, nh, lane, acc);
+  return acc;
+}
+
+// Screen side 0 (c1 atoms, nc1 connections) against the m packed side-1
+// atoms of `ns` slots, draining the queue whenever it could overflow.  Lanes
+// walk the packed atoms (32 per chunk); side-0 atoms are broadcast one per
+// step, skipping those farther than r_k + max_dis from every slot block's
+// centroid.  Returns the lane's energy sums.
+template <typename Real, bool GRAD>
+__device__ __noinline__ E3<Real> screen_slots(EvalCtx<Real> c, Slab<Real>* wp,
+                                              int c1, int nc1, int m, int ns,
+                                              int lane) {
+  Slab<Real>& w = *wp;
+  E3<Real> acc = {0, 0, 0};
+  const Real maxd2 = c.max_dis * c.max_dis;
+  bool act0 = false;
+  if (lane < c1) {
+    for (int k = 0; k < ns; ++k) {
+      Real dx = w.x0[lane] - w.slot_sph[k][0];
+      Real dy = w.y0[lane] - w.slot_sph[k][1];
+      Real dz = w.z0[lane] - w.slot_sph[k][2];
+      Real rr = w.slot_sph[k][3] + c.max_dis;
+      act0 |= dx * dx + dy * dy + dz * dz < rr * rr * Real(1.0001);
+    }
+  }
+  const unsigned rows = __ballot_sync(0xffffffffu, act0);
+  int nl = 0, nh = 0;
+  for (int cbase = 0; cbase < m; cbase += 32) {
+    int j = cbase + lane;
+    bool valid = j < m;
+    int jj = valid ? j : 0;
+    Real xj = w.x1[jj], yj = w.y1[jj], zj = w.z1[jj];
+    int heavy_j = valid ? (w.tf1[jj] & kTfHeavy) : 0;
+    int slot = w.slot1[jj];
+    int kind = w.slot_kind[slot];
+    int nc2 = w.slot_nc[slot];
+    bool lig = w.slot_lig[slot];
+    uint32_t cpdj = w.cpd1[jj];
+    const uint8_t* seps = w.seps[slot];
+    const uint8_t* pd = c.pd + w.local1[jj];
+    for (unsigned rm = rows; rm; rm &= rm - 1) {
+      int a1 = __ffs(rm) - 1;
+      Real dx = w.x0[a1] - xj;
+      Real dy = w.y0[a1] - yj;
+      Real dz = w.z0[a1] - zj;
+      Real d2 = dx * dx + dy * dy + dz * dz;
+      bool in = false, hv = false;
+      int wbit = 0;
+      if (valid && d2 < maxd2) {
+        int sep;
+        if (kind == kSlotFar) {
+          sep = 6;
+        } else if (kind == kSlotStriking) {
+          sep = 5;
+          uint32_t c0 = w.cpd0[a1];
+          for (int u = 0; u < nc1; ++u) {
+            int pd1 = (c0 >> (8 * u)) & 0xff;
+            for (int v = 0; v < nc2; ++v) {
+              int t = pd1 + seps[u * 4 + v] + ((cpdj >> (8 * v)) & 0xff);
+              sep = t < sep ? t : sep;
             }
           }
         } else {
-          eval_block_pair<Real, GRAD>(s, w, p, b1, b2, lane, acc, wt, cnt);
+          sep = pd[a1 * c.A];
+        }
+        if (lig && (sep == 3 || sep == 4)) sep = 5;
+        in = sep >= 4;
+        wbit = sep == 4;
+        hv = in && (heavy_j & w.tf0[a1]);
+      }
+      queue_push(w.queue, in, hv, a1 | (j << 5) | (wbit << 11), lane, nl, nh);
+      if (nl + nh > QCAP - 32) drain_queue<Real, GRAD>(c, wp, nl, nh, lane, acc);
+    }
+  }
+  drain_queue<Real, GRAD>(c, wp, nl, nh, lane, acc);
+  return acc;
+}
+
+// Count-pair lookup for (row block, b2): lanes hold the row's partner list.
+struct RowPartners {
+  int b2;      // this lane's partner block, or -1
+  int minsep;  // its minimum bond separation
+  int entry;   // its cp table entry
+};
+
+// Scores the staged slots against side 0 and flushes their gradients.
+template <typename Real, bool GRAD, bool BLOCK_PAIR>
+__device__ __forceinline__ void score_group(const ScoreArgs<Real>& s,
+                                            Slab<Real>& w, const EvalCtx<Real>& c,
+                                            const RowInfo& r, int& m, int& ns,
+                                            int lane, E3<Real>& acc,
+                                            int64_t pair_o, bool want_E) {
+  __syncwarp();
+  if (m > 0) {
+    E3<Real> e = screen_slots<Real, GRAD>(c, &w, r.c1, r.nc1, m, ns, lane);
+    if (GRAD) flush_side1(s, w, m, lane);
+    if (BLOCK_PAIR) {
+      if (want_E) {
+        const int64_t stride = (int64_t)s.P * s.B * s.B;
+        Real v0 = warp_sum(e.atr), v1 = warp_sum(e.rep), v2 = warp_sum(e.lk);
+        if (lane == 0) {
+          s.energies[pair_o] += v0;
+          s.energies[stride + pair_o] += v1;
+          s.energies[2 * stride + pair_o] += v2;
         }
       }
-      __syncthreads();
-    }
-    if (!BLOCK_PAIR && want_E) {
-      for (int t = 0; t < 3; ++t) {
-        Real v = warp_sum(acc[t]);
-        if (lane == 0) s_red[t][warp] = v;
-      }
-      __syncthreads();
-      if (threadIdx.x < 3) {
-        Real v = 0;
-        for (int k = 0; k < n_warps; ++k) v += s_red[threadIdx.x][k];
-        if (v != Real(0)) atomicAdd(&s.energies[threadIdx.x * s.P + p], v);
-      }
+    } else {
+      acc.atr += e.atr;
+      acc.rep += e.rep;
+      acc.lk += e.lk;
     }
   }
-  if (s.counts) {
-    // counters 0..2 are warp-uniform (lane 0 reports); 3..4 are per lane
-    for (int k = 0; k < N_COUNTS; ++k) {
-      long long v = cnt.c[k];
-      if (k >= 3) {
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncwarp();
+  m = 0;
+  ns = 0;
+}
+
+// The fused kernel.  A work item is (pose p, block b1, candidate range
+// [c0, c1) of later blocks b2 >= b1).  Every warp takes items from a global
+// ticket, tests b1 against each candidate with the bounding-sphere rule of
+// tmol/score/common/sphere_overlap.impl.hh:287-351 (32 per ballot) and
+// scores the hits: b1 with itself when b1 is in the range, the other
+// neighbours packed into side 1.  GRAD selects the adjoint (which also
+// yields the energies when s.energies is set); BLOCK_PAIR selects
+// per-block-pair energies / weights instead of per-pose ones (one block pair
+// per group).
+#ifndef TMOL_B200_FLOAT_MIN_CTAS
+#define TMOL_B200_FLOAT_MIN_CTAS 2
+#endif
+
+template <typename Real, bool GRAD, bool BLOCK_PAIR>
+__global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_CTAS : 1)
+    score_kernel(ScoreArgs<Real> s, int items_per_ticket) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  Slab<Real>& w = reinterpret_cast<Slab<Real>*>(smem_raw)[warp];
+  if (lane < N_COUNTS) w.counts[lane] = 0;
+  __syncwarp();
+  const bool want_E = !GRAD || s.energies != nullptr;
+  const int64_t stride = (int64_t)s.P * s.B * s.B;
+  const int max_slots = BLOCK_PAIR ? 1 : MAX_SLOTS;
+  const Real reach_atoms = s.g.max_dis;
+
+  for (;;) {
+    int t = 0;
+    if (lane == 0) t = atomicAdd(s.ticket, 1);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    int it0 = t * items_per_ticket;
+    if (it0 >= s.n_work) break;
+    int it1 = min(it0 + items_per_ticket, s.n_work);
+    for (int item = it0; item < it1; ++item) {
+      long long t_item = clock64();
+      int4 wi = s.work[item];
+      RowInfo r;
+      r.p = wi.x;
+      r.b1 = wi.y;
+      int cand0 = wi.z, cand1 = wi.w;
+      r.i1 = r.p * s.B + r.b1;
+      r.bt1 = s.blk_bt[r.i1];
+      if (r.bt1 < 0) continue;
+      r.off1 = s.blk_off[r.i1];
+      r.n1 = s.bt_n_atoms[r.bt1];
+      r.nc1 = s.bt_n_conn[r.bt1];
+      r.lig1 = s.bt_is_ligand[r.bt1];
+      E3<Real> acc = {0, 0, 0};
+      EvalCtx<Real> ec;
+      ec.ljtab = s.ljtab;
+      ec.lktab = s.lktab;
+      ec.ntp = s.ntp;
+      ec.A = s.A;
+      ec.max_dis = s.g.max_dis;
+      ec.wt0 = ec.wt1 = ec.wt2 = 0;
+      if (GRAD && !BLOCK_PAIR) {
+        ec.wt0 = s.dTdV[r.p];
+        ec.wt1 = s.dTdV[s.P + r.p];
+        ec.wt2 = s.dTdV[2 * s.P + r.p];
       }
-      if (lane == 0 && v) atomicAdd(&s_cnt[k], (unsigned long long)v);
+      const Real* sph1 = s.spheres + 4 * (int64_t)r.i1;
+      const Real c1x = sph1[0], c1y = sph1[1], c1z = sph1[2], rad1 = sph1[3];
+      const Real reach1 = rad1 + reach_atoms;
+      const Real reach1_2 = reach1 * reach1 * Real(1.0001);
+
+      // neighbour tests of the whole range first: one ballot mask per 32
+      // candidates, kept in registers (lane k holds the mask of batch k)
+      unsigned my_mask = 0;
+      int n_batches = (cand1 - cand0 + 31) / 32;
+      for (int bi = 0; bi < n_batches; ++bi) {
+        int b2 = cand0 + bi * 32 + lane;
+        bool hit = false;
+        if (b2 < cand1) {
+          int i2 = r.p * s.B + b2;
+          if (s.blk_bt[i2] >= 0) {
+            const Real* s2 = s.spheres + 4 * (int64_t)i2;
+            Real dx = sub_rn(c1x, s2[0]);
+            Real dy = sub_rn(c1y, s2[1]);
+            Real dz = sub_rn(c1z, s2[2]);
+            Real d2 = add_rn(add_rn(mul_rn(dx, dx), mul_rn(dy, dy)), mul_rn(dz, dz));
+            Real thr = add_rn(add_rn(rad1, s2[3]), s.reach);
+            hit = d2 < mul_rn(thr, thr);
+          }
+          if (s.nbr) s.nbr[(int64_t)r.i1 * s.B + b2] = hit ? 1 : 0;
+        }
+        unsigned mk = __ballot_sync(0xffffffffu, hit);
+        if (lane == bi) my_mask = mk;
+      }
+      bool any = __any_sync(0xffffffffu, my_mask != 0);
+      if (!any) {
+        if (s.item_cost && lane == 0)
+          s.item_cost[item] = (int)min((clock64() - t_item) >> 4, (long long)0x7fffffff);
+        continue;
+      }
+
+      // the row's count-pair partners, one per lane
+      RowPartners rp;
+      {
+        int ncp = s.cp_count[r.i1];
+        rp.b2 = -1;
+        rp.minsep = 6;
+        rp.entry = r.i1 * CP_CAP + lane;
+        if (lane < ncp) {
+          rp.b2 = s.cp_b2[rp.entry];
+          rp.minsep = s.cp_minsep[rp.entry];
+        }
+      }
+      int nt1 = (r.n1 + TILE - 1) / TILE;
+      for (int ti = 0; ti < nt1; ++ti) {
+        r.st1 = ti * TILE;
+        r.c1 = min(TILE, r.n1 - r.st1);
+        stage_side0(s, w, r.bt1, r.off1, r.st1, r.c1, r.nc1, lane);
+        ec.pd = s.bt_pd + ((int64_t)r.bt1 * s.A + r.st1) * s.A;
+        __syncwarp();
+        int h1 = __popc(__ballot_sync(0xffffffffu, lane < r.c1 && (w.tf0[lane] & kTfHeavy)));
+        int m = 0, ns = 0;
+        int64_t pair_o = 0;
+        for (int bi = 0; bi < n_batches; ++bi) {
+          unsigned mask = __shfl_sync(0xffffffffu, my_mask, bi);
+          while (mask) {
+            int k = __ffs(mask) - 1;
+            mask &= mask - 1;
+            int bb2 = cand0 + bi * 32 + k;
+            if (bb2 == r.b1) {
+              // b1 with itself: this tile with itself, then with b1's later tiles
+              score_group<Real, GRAD, BLOCK_PAIR>(s, w, ec, r, m, ns, lane, acc, pair_o, want_E);
+              pair_o = (int64_t)r.i1 * s.B + r.b1;
+              if (BLOCK_PAIR && GRAD) {
+                ec.wt0 = s.dTdV[pair_o];
+                ec.wt1 = s.dTdV[stride + pair_o];
+                ec.wt2 = s.dTdV[2 * stride + pair_o];
+              }
+              if (ti == 0) {
+                cnt_add(w.counts, 0, 1, lane);
+                cnt_add(w.counts, 1, (long long)r.n1 * (r.n1 - 1) / 2, lane);
+              }
+              cnt_add(w.counts, 2, (long long)h1 * (h1 - 1) / 2, lane);
+              {
+                E3<Real> e = intra_tile<Real, GRAD>(ec, &w, r.st1, r.c1, lane);
+                if (BLOCK_PAIR) {
+                  if (want_E) {
+                    Real v0 = warp_sum(e.atr), v1 = warp_sum(e.rep), v2 = warp_sum(e.lk);
+                    if (lane == 0) {
+                      s.energies[pair_o] += v0;
+                      s.energies[stride + pair_o] += v1;
+                      s.energies[2 * stride + pair_o] += v2;
+                    }
+                  }
+                } else {
+                  acc.atr += e.atr;
+                  acc.rep += e.rep;
+                  acc.lk += e.lk;
+                }
+              }
+              for (int tj = ti + 1; tj < nt1; ++tj) {
+                int st2 = tj * TILE, c2 = min(TILE, r.n1 - st2);
+                if (lane == 0) {
+                  w.slot_kind[0] = kSlotIntra;
+                  w.slot_nc[0] = 0;
+                  w.slot_lig[0] = 0;
+                  w.slot_sph[0][0] = c1x;
+                  w.slot_sph[0][1] = c1y;
+                  w.slot_sph[0][2] = c1z;
+                  w.slot_sph[0][3] = rad1;
+                }
+                int h2 = __popc(__ballot_sync(
+                    0xffffffffu, lane < c2 && (s.bt_tf[(int64_t)r.bt1 * s.A + st2 + lane] & kTfHeavy)));
+                cnt_add(w.counts, 2, (long long)h1 * h2, lane);
+                m = stage_side1(s, w, 0, 0, r.bt1, r.off1, st2, c2, 0, c1x, c1y, c1z, reach1_2, lane);
+                ns = 1;
+                score_group<Real, GRAD, BLOCK_PAIR>(s, w, ec, r, m, ns, lane, acc, pair_o, want_E);
+              }
+              continue;
+            }
+            int i2 = r.p * s.B + bb2;
+            int bt2 = s.blk_bt[i2];
+            int off2 = s.blk_off[i2];
+            int n2 = s.bt_n_atoms[bt2];
+            int nt2 = (n2 + TILE - 1) / TILE;
+            unsigned pm = __ballot_sync(0xffffffffu, rp.b2 == bb2);
+            int kind = kSlotFar, nc2 = 0, e = 0;
+            if (pm) {
+              int src = __ffs(pm) - 1;
+              int msep = __shfl_sync(0xffffffffu, rp.minsep, src);
+              e = __shfl_sync(0xffffffffu, rp.entry, src);
+              kind = msep <= 4 ? kSlotStriking : kSlotFar;
+            }
+            if (kind == kSlotStriking) nc2 = s.bt_n_conn[bt2];
+            int lig = r.lig1 && s.bt_is_ligand[bt2];
+            const Real* s2 = s.spheres + 4 * (int64_t)i2;
+            if (ti == 0) {
+              cnt_add(w.counts, 0, 1, lane);
+              cnt_add(w.counts, 1, (long long)r.n1 * n2, lane);
+            }
+            for (int tj = 0; tj < nt2; ++tj) {
+              int st2 = tj * TILE, c2 = min(TILE, n2 - st2);
+              int h2 = __popc(__ballot_sync(
+                  0xffffffffu, lane < c2 && (s.bt_tf[(int64_t)bt2 * s.A + st2 + lane] & kTfHeavy)));
+              cnt_add(w.counts, 2, (long long)h1 * h2, lane);
+              if (m + c2 > M1 || ns == max_slots)
+                score_group<Real, GRAD, BLOCK_PAIR>(s, w, ec, r, m, ns, lane, acc, pair_o, want_E);
+              if (lane == 0) {
+                w.slot_kind[ns] = kind;
+                w.slot_nc[ns] = nc2;
+                w.slot_lig[ns] = lig;
+              }
+              if (lane < 4) w.slot_sph[ns][lane] = s2[lane];
+              if (kind == kSlotStriking && lane < 16) w.seps[ns][lane] = s.cp_seps[(int64_t)e * 16 + lane];
+              int kept = stage_side1(s, w, m, ns, bt2, off2, st2, c2, nc2, c1x, c1y, c1z, reach1_2, lane);
+              if (kept > 0) {
+                m += kept;
+                ns += 1;
+              }
+              if (BLOCK_PAIR) {
+                pair_o = (int64_t)r.i1 * s.B + bb2;
+                if (GRAD) {
+                  ec.wt0 = s.dTdV[pair_o];
+                  ec.wt1 = s.dTdV[stride + pair_o];
+                  ec.wt2 = s.dTdV[2 * stride + pair_o];
+                }
+              }
+            }
+          }
+        }
+        score_group<Real, GRAD, BLOCK_PAIR>(s, w, ec, r, m, ns, lane, acc, pair_o, want_E);
+        if (GRAD) flush_side0(s, w, r.off1, r.st1, r.c1, lane);
+        __syncwarp();
+      }
+      if (!BLOCK_PAIR && want_E) {
+        Real v0 = warp_sum(acc.atr), v1 = warp_sum(acc.rep), v2 = warp_sum(acc.lk);
+        if (lane == 0) {
+          if (v0 != Real(0)) atomicAdd(&s.energies[r.p], v0);
+          if (v1 != Real(0)) atomicAdd(&s.energies[s.P + r.p], v1);
+          if (v2 != Real(0)) atomicAdd(&s.energies[2 * s.P + r.p], v2);
+        }
+      }
+      if (s.item_cost && lane == 0)
+        s.item_cost[item] = (int)min((clock64() - t_item) >> 4, (long long)0x7fffffff);
     }
-    __syncthreads();
-    if (threadIdx.x < N_COUNTS && s_cnt[threadIdx.x])
-      atomicAdd(&s.counts[threadIdx.x], s_cnt[threadIdx.x]);
   }
+  __syncwarp();
+  if (s.counts && lane < N_COUNTS && w.counts[lane])
+    atomicAdd(&s.counts[lane], w.counts[lane]);
+}
+
+// FP32 issue-rate probe: 8 independent FMA chains per thread, so that the
+// FMA pipe, not latency, bounds it.  2 FLOP per FMA.
+__global__ void fp32_peak_kernel(float* out, int iters, float a, float b) {
+  float x[8];
+  for (int k = 0; k < 8; ++k) x[k] = threadIdx.x * 1e-3f + k;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = fmaf(x[k], a, b);
+  }
+  float acc = 0;
+  for (int k = 0; k < 8; ++k) acc += x[k];
+  if (acc == 1234.5f) out[0] = acc;  // keeps the chains live
 }
 
 }  // namespace tmol_b200
@@ -657,7 +1074,12 @@ struct tmol_b200_ljlk_plan {
   int* blk_bt = nullptr;
   int* blk_off = nullptr;
   int* pose_last = nullptr;
-  void* atom_params = nullptr;
+  uint16_t* bt_tf = nullptr;
+  int* type_map = nullptr;
+  int* compact_types = nullptr;
+  void* ljtab = nullptr;
+  void* lktab = nullptr;
+  int ntp = 0;
   uint8_t* bt_pd = nullptr;
   uint8_t* bt_conn_pd = nullptr;
   int* bt_flags = nullptr;
@@ -669,6 +1091,7 @@ struct tmol_b200_ljlk_plan {
   int* cp_minsep = nullptr;
   uint8_t* cp_seps = nullptr;
   int4* work = nullptr;
+  int* item_cost = nullptr;
   int n_work = 0;
   void* spheres = nullptr;
   int* counters = nullptr;  // [0] ticket, [1] status
@@ -707,10 +1130,12 @@ int status_from_bits(int bits) {
 }
 
 void free_plan(tmol_b200_ljlk_plan* pl) {
-  void* ptrs[] = {pl->blk_bt,    pl->blk_off,    pl->pose_last,  pl->atom_params,
+  void* ptrs[] = {pl->blk_bt,    pl->blk_off,    pl->pose_last,  pl->bt_tf,
+                  pl->type_map,  pl->compact_types, pl->ljtab,   pl->lktab,
                   pl->bt_pd,     pl->bt_conn_pd, pl->bt_flags,   pl->bt_n_atoms,
                   pl->bt_n_conn, pl->bt_is_ligand, pl->cp_count, pl->cp_b2,
                   pl->cp_minsep, pl->cp_seps,    pl->work,       pl->spheres,
+                  pl->item_cost,
                   pl->counters,  pl->counts};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -719,16 +1144,18 @@ void free_plan(tmol_b200_ljlk_plan* pl) {
 }
 
 void default_launch(tmol_b200_ljlk_launch& l) {
-  if (l.rows_per_item <= 0) l.rows_per_item = 4;
+  if (l.rows_per_item <= 0) l.rows_per_item = 1;
   if (l.warps_per_cta <= 0) l.warps_per_cta = 8;
-  if (l.ctas_per_sm <= 0) l.ctas_per_sm = 4;
+  if (l.ctas_per_sm <= 0) l.ctas_per_sm = 2;
+  if (l.candidates_per_item <= 0) l.candidates_per_item = 64;
   l.rows_per_item = std::min(l.rows_per_item, MAX_ROWS_PER_ITEM);
   l.warps_per_cta = std::min(l.warps_per_cta, MAX_WARPS);
+  l.candidates_per_item = std::min(l.candidates_per_item, 32 * 32);
 }
 
 template <typename Real>
 cudaError_t set_smem_limits() {
-  int smem = (int)(MAX_WARPS * sizeof(WarpSlab<Real>) + QUEUE_CAP * sizeof(int));
+  int smem = (int)(MAX_WARPS * sizeof(Slab<Real>));
   cudaError_t e;
   if ((e = cudaFuncSetAttribute(score_kernel<Real, false, false>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
@@ -744,16 +1171,23 @@ cudaError_t set_smem_limits() {
 }
 
 int build_work(tmol_b200_ljlk_plan* pl, cudaStream_t st) {
+  // items (pose, b1, [c0, c1)): the later blocks of each row in ranges of
+  // CAND_CHUNK candidates
   std::vector<int4> work;
-  int R = pl->launch.rows_per_item;
   for (int p = 0; p < pl->P; ++p) {
     int nb = pl->host_pose_last[p];
-    for (int r = 0; r < nb; r += R) work.push_back(make_int4(p, r, std::min(nb, r + R), 0));
+    for (int r = 0; r < nb; ++r)
+      for (int c = r; c < nb; c += pl->launch.candidates_per_item)
+        work.push_back(make_int4(p, r, c, std::min(nb, c + pl->launch.candidates_per_item)));
   }
   if (pl->work) cudaFree(pl->work);
+  if (pl->item_cost) cudaFree(pl->item_cost);
   pl->work = nullptr;
+  pl->item_cost = nullptr;
   pl->n_work = (int)work.size();
   CK(cudaMalloc((void**)&pl->work, std::max<size_t>(work.size(), 1) * sizeof(int4)));
+  CK(cudaMalloc((void**)&pl->item_cost, std::max<size_t>(work.size(), 1) * sizeof(int)));
+  CK(cudaMemsetAsync(pl->item_cost, 0, std::max<size_t>(work.size(), 1) * sizeof(int), st));
   if (!work.empty())
     CK(cudaMemcpyAsync(pl->work, work.data(), work.size() * sizeof(int4),
                        cudaMemcpyHostToDevice, st));
@@ -768,7 +1202,10 @@ ScoreArgs<Real> score_args(tmol_b200_ljlk_plan* pl, const void* coords) {
   s.blk_bt = pl->blk_bt;
   s.blk_off = pl->blk_off;
   s.pose_last = pl->pose_last;
-  s.atom_params = (const AtomParams<Real>*)pl->atom_params;
+  s.bt_tf = pl->bt_tf;
+  s.ljtab = (const LJRecord<Real>*)pl->ljtab;
+  s.lktab = (const LKRecord<Real>*)pl->lktab;
+  s.ntp = pl->ntp;
   s.bt_pd = pl->bt_pd;
   s.bt_conn_pd = pl->bt_conn_pd;
   s.bt_n_atoms = pl->bt_n_atoms;
@@ -787,6 +1224,7 @@ ScoreArgs<Real> score_args(tmol_b200_ljlk_plan* pl, const void* coords) {
   s.g.lj_hbond_hdis = gp[4];
   s.reach = (Real)pl->reach;
   s.work = pl->work;
+  s.item_cost = pl->item_cost;
   s.n_work = pl->n_work;
   s.P = pl->P;
   s.B = pl->B;
@@ -807,9 +1245,11 @@ int launch_score(tmol_b200_ljlk_plan* pl, ScoreArgs<Real> s, cudaStream_t st) {
   CK(cudaMemsetAsync(pl->counters, 0, sizeof(int), st));
   if (pl->n_work == 0) return TMOL_B200_OK;
   int warps = pl->launch.warps_per_cta;
-  size_t smem = warps * sizeof(WarpSlab<Real>) + QUEUE_CAP * sizeof(int);
+  size_t smem = warps * sizeof(Slab<Real>);
   auto kern = score_kernel<Real, GRAD, BLOCK_PAIR>;
-  int grid = std::max(1, std::min(pl->n_work, pl->n_sm * pl->launch.ctas_per_sm));
+  int R = pl->launch.rows_per_item;
+  int n_tickets = (pl->n_work + R - 1) / R;
+  int grid = std::max(1, std::min((n_tickets + warps - 1) / warps, pl->n_sm * pl->launch.ctas_per_sm));
   bool prof = pl->profiling && 2 * (size_t)pl->prof_n + 1 < pl->prof_events.size();
   if (prof) CK(cudaEventRecord(pl->prof_events[2 * pl->prof_n], st));
   kern<<<grid, 32 * warps, smem, st>>>(s, pl->launch.rows_per_item);
@@ -915,7 +1355,7 @@ int tmol_b200_ljlk_plan_create(const tmol_b200_ljlk_inputs* in, int real_bytes,
   pl->T = T;
   pl->N = in->n_atoms;
   pl->reach = in->max_dis;
-  pl->launch = launch ? *launch : tmol_b200_ljlk_launch{0, 0, 0};
+  pl->launch = launch ? *launch : tmol_b200_ljlk_launch{0, 0, 0, 0};
   default_launch(pl->launch);
   int dev = 0;
   int rc = TMOL_B200_OK;
@@ -933,8 +1373,8 @@ int tmol_b200_ljlk_plan_create(const tmol_b200_ljlk_inputs* in, int real_bytes,
   PCK(dalloc(pl, &pl->blk_bt, PB));
   PCK(dalloc(pl, &pl->blk_off, PB));
   PCK(dalloc(pl, &pl->pose_last, P));
-  PCK(dalloc(pl, (unsigned char**)&pl->atom_params,
-             (size_t)nbt * A * (real_bytes == 4 ? sizeof(AtomParams<float>) : sizeof(AtomParams<double>))));
+  PCK(dalloc(pl, &pl->bt_tf, (size_t)nbt * A));
+  PCK(dalloc(pl, &pl->type_map, std::max(T, 1)));
   PCK(dalloc(pl, &pl->bt_pd, (size_t)nbt * A * A));
   PCK(dalloc(pl, &pl->bt_conn_pd, (size_t)nbt * C * A));
   PCK(dalloc(pl, &pl->bt_flags, (size_t)nbt * A));
@@ -981,12 +1421,6 @@ int tmol_b200_ljlk_plan_create(const tmol_b200_ljlk_inputs* in, int real_bytes,
     int gh = std::max(1, std::min(((nbt * nt * TILE) + 255) / 256, pl->n_sm * 8));
     plan_heavy_kernel<<<gh, 256, 0, st>>>(a);
     PCK(cudaGetLastError());
-    int gb = std::max(1, std::min(((nbt * A) + 255) / 256, pl->n_sm * 8));
-    if (real_bytes == 4)
-      plan_block_types_kernel<float><<<gb, 256, 0, st>>>(a, (AtomParams<float>*)pl->atom_params);
-    else
-      plan_block_types_kernel<double><<<gb, 256, 0, st>>>(a, (AtomParams<double>*)pl->atom_params);
-    PCK(cudaGetLastError());
   }
   if (PB > 0) {
     int gc = std::max(1, std::min<int>((int)((PB * 32 + 255) / 256), pl->n_sm * 16));
@@ -999,6 +1433,66 @@ int tmol_b200_ljlk_plan_create(const tmol_b200_ljlk_inputs* in, int real_bytes,
   if (P > 0)
     PCK(cudaMemcpyAsync(pl->host_pose_last.data(), pl->pose_last, sizeof(int) * P,
                         cudaMemcpyDeviceToHost, st));
+  // compact atom types: the types the block types use, in index order
+  std::vector<int> h_types((size_t)nbt * A), h_nat(std::max(nbt, 1));
+  if (nbt > 0) {
+    PCK(cudaMemcpyAsync(h_types.data(), in->bt_atom_types, sizeof(int) * h_types.size(),
+                        cudaMemcpyDeviceToHost, st));
+    PCK(cudaMemcpyAsync(h_nat.data(), in->bt_n_atoms, sizeof(int) * nbt, cudaMemcpyDeviceToHost, st));
+  }
+  PCK(cudaStreamSynchronize(st));
+  rc = status_from_bits(status_bits);
+  if (rc != TMOL_B200_OK) {
+    free_plan(pl);
+    return rc;
+  }
+  std::vector<int> type_map(std::max(T, 1), -1), compact;
+  for (int bt = 0; bt < nbt; ++bt) {
+    int n = std::min(std::max(h_nat[bt], 0), A);
+    for (int k = 0; k < n; ++k) {
+      int t = h_types[(size_t)bt * A + k];
+      if (t >= 0 && t < T) type_map[t] = 0;
+    }
+  }
+  for (int t = 0; t < T; ++t)
+    if (type_map[t] == 0) {
+      type_map[t] = (int)compact.size();
+      compact.push_back(t);
+    }
+  pl->ntp = (int)compact.size();
+  if (pl->ntp > 255) {
+    free_plan(pl);
+    return TMOL_B200_ERR_SHAPE;
+  }
+  size_t ntp2 = (size_t)std::max(pl->ntp, 1) * std::max(pl->ntp, 1);
+  PCK(dalloc(pl, &pl->compact_types, std::max(pl->ntp, 1)));
+  PCK(dalloc(pl, (unsigned char**)&pl->ljtab,
+             ntp2 * (real_bytes == 4 ? sizeof(LJRecord<float>) : sizeof(LJRecord<double>))));
+  PCK(dalloc(pl, (unsigned char**)&pl->lktab,
+             ntp2 * (real_bytes == 4 ? sizeof(LKRecord<float>) : sizeof(LKRecord<double>))));
+  PCK(cudaMemcpyAsync(pl->type_map, type_map.data(), sizeof(int) * std::max(T, 1),
+                      cudaMemcpyHostToDevice, st));
+  if (pl->ntp > 0)
+    PCK(cudaMemcpyAsync(pl->compact_types, compact.data(), sizeof(int) * pl->ntp,
+                        cudaMemcpyHostToDevice, st));
+  if (nbt > 0) {
+    int gb = std::max(1, std::min(((nbt * A) + 255) / 256, pl->n_sm * 8));
+    plan_block_types_kernel<<<gb, 256, 0, st>>>(a, pl->type_map, pl->bt_tf);
+    PCK(cudaGetLastError());
+  }
+  if (pl->ntp > 0) {
+    int gt = std::max(1, std::min((int)((ntp2 + 127) / 128), pl->n_sm * 8));
+    if (real_bytes == 4)
+      plan_tables_kernel<float><<<gt, 128, 0, st>>>(
+          (const float*)in->type_params, (const float*)in->global_params, pl->compact_types,
+          pl->ntp, (LJRecord<float>*)pl->ljtab, (LKRecord<float>*)pl->lktab);
+    else
+      plan_tables_kernel<double><<<gt, 128, 0, st>>>(
+          (const double*)in->type_params, (const double*)in->global_params, pl->compact_types,
+          pl->ntp, (LJRecord<double>*)pl->ljtab, (LKRecord<double>*)pl->lktab);
+    PCK(cudaGetLastError());
+  }
+  PCK(cudaMemcpyAsync(&status_bits, pl->counters + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
   PCK(cudaStreamSynchronize(st));
   rc = status_from_bits(status_bits);
   if (rc != TMOL_B200_OK) {
@@ -1010,7 +1504,7 @@ int tmol_b200_ljlk_plan_create(const tmol_b200_ljlk_inputs* in, int real_bytes,
     free_plan(pl);
     return rc;
   }
-  pl->device_bytes += (int64_t)std::max(pl->n_work, 1) * sizeof(int4);
+  pl->device_bytes += (int64_t)std::max(pl->n_work, 1) * (sizeof(int4) + sizeof(int));
 #undef PCK
   *plan_out = pl;
   return TMOL_B200_OK;
@@ -1025,13 +1519,10 @@ int tmol_b200_ljlk_plan_destroy(tmol_b200_ljlk_plan* plan) {
 int tmol_b200_ljlk_plan_set_launch(tmol_b200_ljlk_plan* plan,
                                    const tmol_b200_ljlk_launch* launch) {
   if (!plan || !launch) return TMOL_B200_ERR_INVALID_ARGUMENT;
-  int old_rows = plan->launch.rows_per_item;
+  int old_cpi = plan->launch.candidates_per_item;
   plan->launch = *launch;
   default_launch(plan->launch);
-  if (plan->launch.rows_per_item != old_rows) {
-    cudaStream_t st = 0;
-    return build_work(plan, st);
-  }
+  if (plan->launch.candidates_per_item != old_cpi) return build_work(plan, 0);
   return TMOL_B200_OK;
 }
 
@@ -1102,6 +1593,60 @@ int tmol_b200_ljlk_profile_read(tmol_b200_ljlk_plan* plan, double* total_ms,
   }
   *total_ms = tot;
   *n_launches = plan->prof_n;
+  return TMOL_B200_OK;
+}
+
+int tmol_b200_measure_fp32_peak(void* stream, double* tflops) {
+  if (!tflops) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  int dev = 0, n_sm = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+  float* out = nullptr;
+  CK(cudaMallocAsync((void**)&out, sizeof(float), st));
+  const int threads = 512, blocks = n_sm * 4, iters = 1 << 16;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  fp32_peak_kernel<<<blocks, threads, 0, st>>>(out, iters / 8, 0.999f, 1e-4f);
+  CK(cudaEventRecord(e0, st));
+  fp32_peak_kernel<<<blocks, threads, 0, st>>>(out, iters, 0.999f, 1e-4f);
+  CK(cudaEventRecord(e1, st));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CK(cudaFreeAsync(out, st));
+  CK(cudaStreamSynchronize(st));
+  double flops = 2.0 * 8.0 * (double)iters * threads * blocks;
+  *tflops = flops / (ms * 1e-3) / 1e12;
+  return TMOL_B200_OK;
+}
+
+int tmol_b200_ljlk_plan_rebalance(tmol_b200_ljlk_plan* plan, void* stream) {
+  if (!plan) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  int n = plan->n_work;
+  if (n == 0) return TMOL_B200_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  std::vector<int4> work(n);
+  std::vector<int> cost(n);
+  CK(cudaMemcpyAsync(work.data(), plan->work, sizeof(int4) * n, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(cost.data(), plan->item_cost, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  // longest items first, so that the last items any warp takes are short
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+  std::vector<int4> sorted(n);
+  std::vector<int> sorted_cost(n);
+  for (int i = 0; i < n; ++i) {
+    sorted[i] = work[order[i]];
+    sorted_cost[i] = cost[order[i]];
+  }
+  CK(cudaMemcpyAsync(plan->work, sorted.data(), sizeof(int4) * n, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(plan->item_cost, sorted_cost.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
+  CK(cudaStreamSynchronize(st));
   return TMOL_B200_OK;
 }
 

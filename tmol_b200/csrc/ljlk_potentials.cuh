@@ -328,3 +328,146 @@ __device__ __forceinline__ void lk_V_dV(Real dist, Real sigma,
 }
 
 }  // namespace tmol_b200
+
+namespace tmol_b200 {
+
+// ---------------------------------------------------------------------------
+// Type-pair tables.  Everything in the two potentials that depends only on
+// the two atom types (sigma, epsilon, region boundaries and the function
+// values and slopes at the spline knots) is computed once per plan for every
+// ordered pair of the atom types a PoseStack uses.  Per atom pair the kernels
+// then evaluate one region: the LJ linear extension, the 12-6 form or the
+// fade-out cubic; the LK flat value, the close cubic, the two Gaussians, or
+// the fade-out cubic.  LK splines of the two directions share their knots,
+// so the table stores the sums of both directions' knot values and one
+// cubic is evaluated for the pair.
+
+template <typename Real>
+struct LJRecord {  // 8 values
+  Real sigma, eps, d_lin, dmin;
+  Real lin_V, lin_dV;  // 12-6 value and slope at d_lin
+  Real spl_V, spl_dV;  // 12-6 value and slope at dmin (start of the fade)
+};
+
+template <typename Real>
+struct LKRecord {  // 16 values (13 used)
+  Real close_dmin, close_dmax;
+  Real flat_V;                // both directions at d_min
+  Real cmax_V, cmax_dV;       // both directions at close_dmax
+  Real fmin_V, fmin_dV;       // both directions at far_dmin
+  Real c_i, r_i, il2_i;       // i desolvated by j: c * exp(-(d-r)^2 * il2) / d^2
+  Real c_j, r_j, il2_j;       // j desolvated by i
+  Real pad0, pad1, pad2;
+};
+
+template <typename Real>
+__device__ __forceinline__ void build_records(const AtomParams<Real>& i,
+                                              const AtomParams<Real>& j,
+                                              const GlobalParams<Real>& g,
+                                              LJRecord<Real>& lj,
+                                              LKRecord<Real>& lk) {
+  LJPair<Real> q = lj_pair(i, j, g);
+  lj.sigma = q.sigma;
+  lj.eps = q.eps;
+  lj.d_lin = q.d_lin;
+  lj.dmin = q.dmin;
+  vdw_V_dV(q.d_lin, q.sigma, q.eps, lj.lin_V, lj.lin_dV);
+  vdw_V_dV(q.dmin, q.sigma, q.eps, lj.spl_V, lj.spl_dV);
+
+  bool cc = (i.flags & kCarbonLK) && (j.flags & kCarbonLK);
+  LKKnots<Real> k = lk_knots(q.sigma, cc, g.max_dis);
+  lk.close_dmin = k.close_dmin;
+  lk.close_dmax = k.close_dmax;
+  lk.flat_V = desolv_V(k.d_min, i.lj_radius, i.lk_dgfree, i.lk_lambda, j.lk_volume) +
+              desolv_V(k.d_min, j.lj_radius, j.lk_dgfree, j.lk_lambda, i.lk_volume);
+  Real v1, d1, v2, d2;
+  desolv_V_dV(k.close_dmax, i.lj_radius, i.lk_dgfree, i.lk_lambda, j.lk_volume, v1, d1);
+  desolv_V_dV(k.close_dmax, j.lj_radius, j.lk_dgfree, j.lk_lambda, i.lk_volume, v2, d2);
+  lk.cmax_V = v1 + v2;
+  lk.cmax_dV = d1 + d2;
+  desolv_V_dV(k.far_dmin, i.lj_radius, i.lk_dgfree, i.lk_lambda, j.lk_volume, v1, d1);
+  desolv_V_dV(k.far_dmin, j.lj_radius, j.lk_dgfree, j.lk_lambda, i.lk_volume, v2, d2);
+  lk.fmin_V = v1 + v2;
+  lk.fmin_dV = d1 + d2;
+  const Real pi_pow1p5 = Real(5.56832799683f);
+  lk.c_i = -j.lk_volume * i.lk_dgfree / (Real(2) * pi_pow1p5 * i.lk_lambda);
+  lk.r_i = i.lj_radius;
+  lk.il2_i = Real(1) / (i.lk_lambda * i.lk_lambda);
+  lk.c_j = -i.lk_volume * j.lk_dgfree / (Real(2) * pi_pow1p5 * j.lk_lambda);
+  lk.r_j = j.lj_radius;
+  lk.il2_j = Real(1) / (j.lk_lambda * j.lk_lambda);
+  lk.pad0 = lk.pad1 = lk.pad2 = Real(0);
+}
+
+// Unweighted LJ (atr, rep) and, with DERIV, their distance derivatives.
+template <typename Real, bool DERIV>
+__device__ __forceinline__ void lj_eval(Real d, const LJRecord<Real>& r,
+                                        Real dmax, Real& atr, Real& rep,
+                                        Real& datr, Real& drep) {
+  Real lj, dlj = 0;
+  if (d < r.d_lin) {
+    lj = r.lin_V + r.lin_dV * (d - r.d_lin);
+    dlj = r.lin_dV;
+  } else if (d < r.dmin) {
+    Real inv = Real(1) / d;
+    Real sd = r.sigma * inv;
+    Real sd2 = sd * sd;
+    Real sd6 = sd2 * sd2 * sd2;
+    Real sd12 = sd6 * sd6;
+    lj = r.eps * (sd12 - Real(2) * sd6);
+    if (DERIV) dlj = r.eps * (Real(12) * (sd6 - sd12)) * inv;
+  } else {
+    Real h = dmax - r.dmin;
+    Real t = (d - r.dmin) / h;
+    Real p0 = r.spl_V, dp0 = r.spl_dV * h;
+    lj = p0 + t * (dp0 + t * (-2 * dp0 - 3 * p0 + t * (dp0 + 2 * p0)));
+    if (DERIV) dlj = (dp0 + t * (-4 * dp0 - 6 * p0 + t * (3 * dp0 + 6 * p0))) / h;
+  }
+  if (d < r.sigma) {
+    atr = -r.eps;
+    rep = lj + r.eps;
+    datr = 0;
+    drep = dlj;
+  } else {
+    atr = lj;
+    rep = 0;
+    datr = dlj;
+    drep = 0;
+  }
+}
+
+// Unweighted LK (both directions) and, with DERIV, its distance derivative.
+template <typename Real, bool DERIV>
+__device__ __forceinline__ void lk_eval(Real d, const LKRecord<Real>& r,
+                                        Real far_dmin, Real far_dmax, Real& V,
+                                        Real& dV) {
+  dV = 0;
+  if (d < r.close_dmin) {
+    V = r.flat_V;
+  } else if (d < r.close_dmax) {
+    Real h = r.close_dmax - r.close_dmin;
+    Real t = (d - r.close_dmin) / h;
+    Real p0 = r.flat_V, p1 = r.cmax_V, dp1 = r.cmax_dV * h;
+    V = p0 + t * (t * (-dp1 - 3 * p0 + 3 * p1 + t * (dp1 + 2 * p0 - 2 * p1)));
+    if (DERIV) dV = (t * (-2 * dp1 - 6 * p0 + 6 * p1 + t * (3 * dp1 + 6 * p0 - 6 * p1))) / h;
+  } else if (d < far_dmin) {
+    Real inv_d2 = Real(1) / (d * d);
+    Real xi = d - r.r_i, xj = d - r.r_j;
+    Real ei = r.c_i * exp(-xi * xi * r.il2_i);
+    Real ej = r.c_j * exp(-xj * xj * r.il2_j);
+    V = (ei + ej) * inv_d2;
+    if (DERIV) {
+      Real inv_d = Real(1) / d;
+      dV = inv_d2 * (ei * (Real(-2) * inv_d - Real(2) * xi * r.il2_i) +
+                     ej * (Real(-2) * inv_d - Real(2) * xj * r.il2_j));
+    }
+  } else {
+    Real h = far_dmax - far_dmin;
+    Real t = (d - far_dmin) / h;
+    Real p0 = r.fmin_V, dp0 = r.fmin_dV * h;
+    V = p0 + t * (dp0 + t * (-2 * dp0 - 3 * p0 + t * (dp0 + 2 * p0)));
+    if (DERIV) dV = (dp0 + t * (-4 * dp0 - 6 * p0 + t * (3 * dp0 + 6 * p0))) / h;
+  }
+}
+
+}  // namespace tmol_b200

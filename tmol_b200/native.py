@@ -10,7 +10,7 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libtmol_b200_ljlk.so")
+LIB_PATH = os.environ.get("TMOL_B200_LIB") or os.path.join(HERE, "lib", "libtmol_b200_ljlk.so")
 
 _i32p = ctypes.POINTER(ctypes.c_int32)
 
@@ -63,6 +63,7 @@ class Launch(ctypes.Structure):
         ("rows_per_item", ctypes.c_int32),
         ("warps_per_cta", ctypes.c_int32),
         ("ctas_per_sm", ctypes.c_int32),
+        ("candidates_per_item", ctypes.c_int32),
     ]
 
 
@@ -74,6 +75,7 @@ SIGNATURES = {
     ),
     "tmol_b200_ljlk_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "tmol_b200_ljlk_plan_set_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Launch)]),
+    "tmol_b200_ljlk_plan_rebalance": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "tmol_b200_ljlk_forward": (
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
@@ -96,6 +98,7 @@ SIGNATURES = {
         [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32)],
     ),
     "tmol_b200_ljlk_plan_device_bytes": (ctypes.c_int64, [ctypes.c_void_p]),
+    "tmol_b200_measure_fp32_peak": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     "tmol_b200_status_string": (ctypes.c_char_p, [ctypes.c_int]),
 }
 
@@ -134,3 +137,10 @@ def check(func, status):
 def call(name, *args):
     lib = load()
     check(name, getattr(lib, name)(*args))
+
+
+def measure_fp32_peak_tflops(stream_handle=0):
+    """Device FP32 FMA throughput in TFLOP/s (see the C declaration)."""
+    v = ctypes.c_double()
+    call("tmol_b200_measure_fp32_peak", ctypes.c_void_p(stream_handle), ctypes.byref(v))
+    return v.value

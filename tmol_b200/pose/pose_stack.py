@@ -90,6 +90,18 @@ class PoseStack:
     def n_blocks_per_pose(self):
         return (self.block_type_ind >= 0).sum(dim=1)
 
+    def slice_poses(self, p0, p1):
+        """A PoseStack of poses [p0, p1) (same block and atom padding)."""
+        return PoseStack(
+            self.packed_block_types,
+            self.coords[p0:p1],
+            self.block_coord_offset[p0:p1],
+            self.inter_residue_connections[p0:p1],
+            self.inter_block_bondsep[p0:p1],
+            self.block_type_ind[p0:p1],
+            self.device,
+        )
+
     def to(self, device):
         device = torch.device(device)
         ps = PoseStack(

@@ -127,7 +127,7 @@ class LJLKPlan:
         self.n_poses, self.max_n_blocks = P, B
         self.n_atoms = pose_ind_for_atom.shape[0]
         s.n_atoms = self.n_atoms
-        self.launch = native.Launch(*(launch or (0, 0, 0)))
+        self.launch = native.Launch(*(launch or (0, 0, 0, 0)))
         ptr = ctypes.c_void_p()
         with torch.cuda.device(device):
             stream = torch.cuda.current_stream(device).cuda_stream
@@ -151,9 +151,18 @@ class LJLKPlan:
                 pass
             self.ptr = None
 
-    def set_launch(self, rows_per_item=0, warps_per_cta=0, ctas_per_sm=0):
-        self.launch = native.Launch(rows_per_item, warps_per_cta, ctas_per_sm)
+    def set_launch(self, rows_per_item=0, warps_per_cta=0, ctas_per_sm=0, candidates_per_item=0):
+        """Launch shape (0 = default); see tmol_b200_ljlk_launch."""
+        self.launch = native.Launch(rows_per_item, warps_per_cta, ctas_per_sm, candidates_per_item)
         native.call("tmol_b200_ljlk_plan_set_launch", self.ptr, ctypes.byref(self.launch))
+
+    def launch_tuple(self):
+        l = self.launch
+        return (l.rows_per_item, l.warps_per_cta, l.ctas_per_sm, l.candidates_per_item)
+
+    def rebalance(self):
+        """Order the work items longest-first by their cost in the last call."""
+        native.call("tmol_b200_ljlk_plan_rebalance", self.ptr, self._stream())
 
     def device_bytes(self):
         return native.load().tmol_b200_ljlk_plan_device_bytes(self.ptr)
