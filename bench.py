@@ -344,7 +344,13 @@ def run_b200(args, world, rank, local):
     torch.cuda.synchronize()
     from tmol_b200.tune import autotune
 
-    launch_shape, _ = autotune(plan, step, use_cache=False)
+    if args.launch:
+        launch_shape = tuple(int(v) for v in args.launch.split(","))
+        plan.set_launch(*launch_shape)
+        step()
+        plan.rebalance()
+    else:
+        launch_shape, _ = autotune(plan, step, use_cache=False)
     for _ in range(max(args.warmup, 3)):
         step()
     torch.cuda.synchronize()
@@ -500,6 +506,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument(
+        "--launch",
+        default="",
+        help="fixed launch shape items_per_ticket,warps_per_cta,ctas_per_sm,candidates_per_item "
+        "(default: autotune)",
+    )
     args = ap.parse_args()
     if args.impl == "reference":
         world = int(os.environ.get("WORLD_SIZE", "1"))

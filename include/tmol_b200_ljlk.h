@@ -174,6 +174,34 @@ int tmol_b200_measure_fp32_peak(void* stream, double* tflops);
 /* Sizes of the plan's device allocations in bytes. */
 int64_t tmol_b200_ljlk_plan_device_bytes(const tmol_b200_ljlk_plan* plan);
 
+/* Block-neighbour matrix without any device allocation.  No counterpart in
+ * the reference: it exists for callers that may not allocate GPU memory
+ * while running (code living inside a memory pool it does not own, or a
+ * loop that must never enter the allocator) but need the same bounding-
+ * sphere neighbour matrix as tmol_b200_ljlk_forward returns.
+ *   coords              [n_atoms, 3] float32, device
+ *   block_type          [n_poses * max_n_blocks] int32 (the op's
+ *                       first_rot_block_type; -1 or out of range = no block)
+ *   block_coord_offset  [n_poses * max_n_blocks] int32 (the op's
+ *                       rot_coord_offset: first atom of each block)
+ *   bt_n_atoms          [n_block_types] int32
+ *   block_neighbors     [n_poses, max_n_blocks, max_n_blocks] int32 out;
+ *                       every cell is written (1 iff b1 <= b2 are neighbours)
+ * Scratch (the block spheres) is a fixed array in the library's device
+ * memory: at most 262,144 blocks (n_poses * max_n_blocks), 4 MiB, kept by
+ * every GPU that loads the library until the process exits; larger inputs
+ * return TMOL_B200_ERR_CAPACITY before any GPU work.  The first call on a
+ * device looks up that array's device address (cudaGetSymbolAddress); make
+ * the first call on each device before any stream capture.  Every call
+ * shares the one array and overwrites it, so calls that overlap on the GPU
+ * (different streams, or different host threads on one device) race; order
+ * them on one stream.  Calls no cudaMalloc, cudaFree or allocating routine. */
+int tmol_b200_ljlk_block_neighbors_noalloc(
+    const float* coords, int64_t n_atoms, const int32_t* block_type,
+    const int32_t* block_coord_offset, const int32_t* bt_n_atoms,
+    int32_t n_block_types, int32_t n_poses, int32_t max_n_blocks,
+    double max_dis, int32_t* block_neighbors, void* stream);
+
 /* Human-readable text of a status code. */
 const char* tmol_b200_status_string(int status);
 

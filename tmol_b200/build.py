@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "lib", "libtmol_b200_ljlk.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["ljlk.cu"]
+SOURCES = ["ljlk.cu", "ljlk_noalloc.cu"]
 HEADERS = ["ljlk_potentials.cuh"]
 
 

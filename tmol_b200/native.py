@@ -99,6 +99,22 @@ SIGNATURES = {
     ),
     "tmol_b200_ljlk_plan_device_bytes": (ctypes.c_int64, [ctypes.c_void_p]),
     "tmol_b200_measure_fp32_peak": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
+    "tmol_b200_ljlk_block_neighbors_noalloc": (
+        ctypes.c_int,
+        [
+            ctypes.c_void_p,
+            ctypes.c_int64,
+            ctypes.c_void_p,
+            ctypes.c_void_p,
+            ctypes.c_void_p,
+            ctypes.c_int32,
+            ctypes.c_int32,
+            ctypes.c_int32,
+            ctypes.c_double,
+            ctypes.c_void_p,
+            ctypes.c_void_p,
+        ],
+    ),
     "tmol_b200_status_string": (ctypes.c_char_p, [ctypes.c_int]),
 }
 
