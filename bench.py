@@ -37,6 +37,11 @@ N_POSES = 64
 N_RES = 150
 TERM_WEIGHTS = (1.0, 0.55, 1.0)
 METRIC = "LJ+LK energy+grad poses/s (64x150-residue batch, 1 B200)"
+# the uneven batch: 256 poses, residue counts log-uniform in [20, 1000],
+# coordinates perturbed by N(0, 0.05 A) inside every replayed step
+UNEVEN_POSES = 256
+UNEVEN_SEED = 2
+PERTURB_SD = 0.05
 L2_FLUSH_BYTES = 256 << 20
 
 # Algorithmic FLOPs per unit (E + dE), counted on the restatement's most
@@ -46,11 +51,32 @@ F_LJ = 64  # each pair inside max_dis with non-zero count-pair weight
 F_LK = 111  # each heavy-atom pair among those (both LK directions)
 
 
-def workload(rank):
+def workload_sizes(name, rank):
+    import numpy
+
+    from tmol_b200.pose.synthetic import log_uniform_sizes
+
+    if name == "uniform64x150":
+        return [N_RES] * N_POSES, [rank * N_POSES + k for k in range(N_POSES)]
+    rng = numpy.random.default_rng(UNEVEN_SEED + 1000 * rank)
+    sizes = log_uniform_sizes(rng, UNEVEN_POSES, 20, 1000)
+    return sizes, [100000 * (rank + 1) + k for k in range(UNEVEN_POSES)]
+
+
+def workload(rank, name="uniform64x150", device="cpu"):
     from tmol_b200.pose.synthetic import synthetic_pose_stack
 
-    seeds = [rank * N_POSES + k for k in range(N_POSES)]
-    return synthetic_pose_stack([N_RES] * N_POSES, seeds)
+    sizes, seeds = workload_sizes(name, rank)
+    return synthetic_pose_stack(sizes, seeds, device=device)
+
+
+def workload_label(name):
+    if name == "uniform64x150":
+        return f"{N_POSES} poses x {N_RES} residues, energy + gradient, weights {list(TERM_WEIGHTS)}"
+    return (
+        f"{UNEVEN_POSES} poses, residues log-uniform in [20, 1000], energy + gradient, "
+        f"coordinates + N(0, {PERTURB_SD} A) each replayed step, weights {list(TERM_WEIGHTS)}"
+    )
 
 
 class ClockSampler:
@@ -192,16 +218,23 @@ def cpu_reference_sample(ps, term, reps=3):
     return kind, best
 
 
-def _ref_worker(conn, slice_ps_args):
+def _ref_worker(conn, sizes, seeds):
+    """One single-threaded process of the reference arm: builds its share of
+    the poses (same sizes and seeds as the GPU arm) and scores it on demand."""
     import torch
 
     torch.set_num_threads(1)
     from oracle import oracle as O
+    from tmol_b200.pose.synthetic import synthetic_pose_stack
+    from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm, pose_score_args
 
-    coords, args = slice_ps_args
+    ps = synthetic_pose_stack(sizes, seeds)
+    args = pose_score_args(ps, LJLKEnergyTerm())
+    coords = ps.coords.flatten(0, 1).clone()
     op = O.load_reference() if O.reference_available() else None
     oc = None if op is not None else O.OracleCall(coords, args)
     w = torch.tensor(TERM_WEIGHTS)[:, None]
+    conn.send("ready")
     while True:
         msg = conn.recv()
         if msg is None:
@@ -217,27 +250,35 @@ def _ref_worker(conn, slice_ps_args):
 
 
 def run_reference(args, world, rank):
-    """tmol's CPU op on all host cores (one process per core)."""
+    """tmol's CPU op on all host cores: one process per core, poses dealt
+    out longest-first so that every process gets a similar share."""
     import multiprocessing as mp
 
     from oracle import oracle as O
-    from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm, pose_score_args
 
     if rank != 0:
         return 0
-    term = LJLKEnergyTerm()
-    ps = workload(0)
-    n_proc = min(os.cpu_count() or 1, N_POSES)
-    bounds = [round(k * N_POSES / n_proc) for k in range(n_proc + 1)]
+    sizes, seeds = workload_sizes(args.workload, 0)
+    n_poses = len(sizes)
+    n_proc = min(os.cpu_count() or 1, n_poses)
+    shares = [[] for _ in range(n_proc)]
+    load = [0] * n_proc
+    for k in sorted(range(n_poses), key=lambda k: -sizes[k]):
+        q = load.index(min(load))
+        shares[q].append(k)
+        load[q] += sizes[k] * 16 * 20  # ~ atoms x neighbour atoms
     ctx = mp.get_context("spawn")
     workers = []
-    for k in range(n_proc):
-        sub = ps.slice_poses(bounds[k], bounds[k + 1])
-        a = pose_score_args(sub, term)
+    for share in shares:
         parent, child = ctx.Pipe()
-        pr = ctx.Process(target=_ref_worker, args=(child, (sub.coords.flatten(0, 1).clone(), a)))
+        pr = ctx.Process(
+            target=_ref_worker,
+            args=(child, [sizes[k] for k in share], [seeds[k] for k in share]),
+        )
         pr.start()
         workers.append((pr, parent))
+    for _, c in workers:
+        c.recv()
 
     def step():
         t0 = time.perf_counter()
@@ -254,7 +295,7 @@ def run_reference(args, world, rank):
         c.send(None)
         pr.join()
     t = sum(times)
-    value = N_POSES * args.steps / t
+    value = n_poses * args.steps / t
     kind = "reference" if O.reference_available() else "port"
     line = {
         "impl": "reference",
@@ -270,17 +311,13 @@ def run_reference(args, world, rank):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded proteins, ideal geometry)",
-        "config": {
-            "workload": f"{N_POSES} poses x {N_RES} residues, energy + gradient",
-            "poses": N_POSES,
-            "residues_per_pose": N_RES,
-        },
+        "config": {"workload": workload_label(args.workload), "poses": n_poses},
         "cpu_baseline": {
             "value": value,
             "unit": "poses/s",
             "cores": n_proc,
             "kind": kind,
-            "sample": f"the full {N_POSES}-pose batch per step, split over {n_proc} single-threaded processes",
+            "sample": f"the full {n_poses}-pose batch per step, dealt to {n_proc} single-threaded processes",
         },
         "e2e": {"value": value, "unit": "poses/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -314,6 +351,46 @@ def measured_peaks():
         return {}
 
 
+def cpu_baseline_for(name, ps_sizes_seeds, full_atom_pairs):
+    """The reference CPU op on one core, on a bounded sample of the workload
+    (the whole uniform batch; 16 seeded poses of the uneven batch, scaled to
+    the whole batch by atom pairs)."""
+    import numpy
+    import torch
+
+    from oracle import oracle as O
+    from tmol_b200.pose.synthetic import synthetic_pose_stack
+    from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm, pose_score_args
+
+    sizes, seeds = ps_sizes_seeds
+    term = LJLKEnergyTerm()
+    if name == "uniform64x150":
+        ps = synthetic_pose_stack(sizes, seeds)
+        kind, t = cpu_reference_sample(ps, term)
+        return {
+            "value": len(sizes) / t,
+            "unit": "poses/s",
+            "cores": 1,
+            "kind": kind,
+            "sample": f"the full {len(sizes)}x{N_RES} batch, energies + gradient, best of 3, one thread",
+        }
+    pick = numpy.random.default_rng(7).choice(len(sizes), 16, replace=False)
+    sub = synthetic_pose_stack([sizes[k] for k in pick], [seeds[k] for k in pick])
+    kind, t = cpu_reference_sample(sub, term, reps=1)
+    args = pose_score_args(sub, term)
+    _, _, nbr = O.OracleCall(sub.coords.flatten(0, 1), args).pose_scores()
+    ap_sample, _ = O.OracleCall(sub.coords.flatten(0, 1), args).count_pairs(nbr)
+    t_full = t * full_atom_pairs / max(ap_sample, 1)
+    return {
+        "value": len(sizes) / t_full,
+        "unit": "poses/s",
+        "cores": 1,
+        "kind": kind,
+        "sample": f"16 seeded poses of the batch ({ap_sample} atom pairs), one thread; "
+        f"extrapolated to the batch's {full_atom_pairs} atom pairs",
+    }
+
+
 def run_b200(args, world, rank, local):
     import torch
 
@@ -324,17 +401,28 @@ def run_b200(args, world, rank, local):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     term = LJLKEnergyTerm()
-    ps_cpu = workload(rank)
-    static = [a.to(dev) if isinstance(a, torch.Tensor) else a for a in pose_score_args(ps_cpu, term)[:-1]]
-    coords = ps_cpu.coords.flatten(0, 1).to(dev).contiguous()
+    sizes_seeds = workload_sizes(args.workload, rank)
+    ps = workload(rank, args.workload, device=dev)
+    static = [a.to(dev) if isinstance(a, torch.Tensor) else a for a in pose_score_args(ps, term)[:-1]]
+    coords = ps.coords.flatten(0, 1).to(dev).contiguous()
     plan = LJLKPlan(coords, static)
-    P = ps_cpu.n_poses
+    del static
+    P = ps.n_poses
+    n_residues = int((ps.block_type_ind >= 0).sum())
+    del ps
+    torch.cuda.empty_cache()
     weights = torch.tensor(TERM_WEIGHTS, device=dev, dtype=torch.float32)[:, None].expand(3, P).contiguous()
     energies = torch.empty((3, P), device=dev)
     dcoords = torch.empty_like(coords)
     flush = torch.empty(L2_FLUSH_BYTES // 4, device=dev, dtype=torch.float32)
+    perturb = args.workload == "uneven256"
+    base = coords.clone()
+    noise = torch.empty_like(coords)
 
     def step():
+        if perturb:
+            noise.normal_(0.0, PERTURB_SD)
+            torch.add(base, noise, out=coords)
         plan.energy_and_gradient(coords, weights, energies, dcoords)
 
     # warm-up (also validates the launch), autotuning of the launch shape and
@@ -430,20 +518,15 @@ def run_b200(args, world, rank, local):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        kind, t_cpu = cpu_reference_sample(ps_cpu, term)
-        cpu = {
-            "value": N_POSES / t_cpu,
-            "unit": "poses/s",
-            "cores": 1,
-            "kind": kind,
-            "sample": f"the full {N_POSES}x{N_RES} batch, energies + gradient, best of 3, one thread",
-        }
+        cpu = cpu_baseline_for(args.workload, sizes_seeds, counts["atom_pairs"])
 
     if rank == 0:
         peaks = measured_peaks()
         traffic = load_traffic()
         line = {
-            "metric": METRIC,
+            "metric": METRIC if args.workload == "uniform64x150" else METRIC.replace(
+                "64x150-residue batch", "256-pose uneven batch"
+            ),
             "value": value,
             "unit": "poses/s",
             "n_gpus": world,
@@ -456,13 +539,15 @@ def run_b200(args, world, rank, local):
             "dtype": "f32",
             "data": "synthetic (seeded proteins, ideal geometry)",
             "config": {
-                "workload": f"{N_POSES} poses x {N_RES} residues, energy + gradient, weights {list(TERM_WEIGHTS)}",
-                "poses_per_gpu": N_POSES,
-                "residues_per_pose": N_RES,
+                "workload": workload_label(args.workload),
+                "poses_per_gpu": P,
+                "residues_per_gpu": n_residues,
                 "atoms_per_gpu": int(coords.shape[0]),
                 "l2": "flushed (256 MiB write) before every timed step",
-                "launch": "CUDA graph replay: 2 kernels per step",
-                "launch_shape": dict(zip(("items_per_ticket", "warps_per_cta", "ctas_per_sm", "candidates_per_item"), launch_shape)),
+                "launch": "CUDA graph replay: 2 kernels per step" + (" + perturbation" if perturb else ""),
+                "launch_shape": dict(
+                    zip(("items_per_ticket", "warps_per_cta", "ctas_per_sm", "candidates_per_item"), launch_shape)
+                ),
                 "parallelism": f"weak, {world} independent batch(es)",
             },
             "atom_pairs_per_s": counts["atom_pairs"] * args.steps * world / (ms_max / 1e3),
@@ -475,7 +560,7 @@ def run_b200(args, world, rank, local):
                 "peak": fp32_peak,
                 "unit": "TFLOP/s",
                 "frac": achieved / fp32_peak,
-                "traffic": traffic,
+                "traffic": traffic if args.workload == "uniform64x150" else None,
                 "kernel": "score_kernel<float, GRAD> (fused neighbour + atom-pair energy and gradient)",
                 "kernel_ms": kern_avg_ms,
                 "flops_per_launch": flops,
@@ -505,6 +590,7 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="uniform64x150", choices=["uniform64x150", "uneven256"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument(
         "--launch",

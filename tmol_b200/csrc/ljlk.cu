@@ -303,42 +303,65 @@ struct ScoreArgs {
 
 // Bounding sphere per block: centroid (sum of atoms in order, then divided
 // by the atom count) and largest centroid distance, as
-// sphere_overlap.impl.hh:109-196 computes them on the CPU.
+// sphere_overlap.impl.hh:109-196 computes them on the CPU.  One warp per
+// block: lanes load 32 atoms at a time, lane 0 adds them in atom order
+// (shuffled to it one by one, no contraction) so that the sums are
+// bit-identical to the sequential CPU loop; the maximum is order-free.
 template <typename Real>
 __global__ void spheres_kernel(ScoreArgs<Real> s) {
-  int n_blocks = s.P * s.B;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_blocks;
-       i += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const int n_blocks = s.P * s.B;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n_blocks; i += warps) {
     int bt = s.blk_bt[i];
     Real* out = s.spheres + 4 * (int64_t)i;
     if (bt < 0) {
-      out[0] = out[1] = out[2] = out[3] = Real(0);
+      if (lane < 4) out[lane] = Real(0);
       continue;
     }
     int n = s.bt_n_atoms[bt];
     const Real* x = s.coords + 3 * (int64_t)s.blk_off[i];
     Real cx = 0, cy = 0, cz = 0;
-    for (int k = 0; k < n; ++k) {
-      cx = add_rn(cx, x[3 * k + 0]);
-      cy = add_rn(cy, x[3 * k + 1]);
-      cz = add_rn(cz, x[3 * k + 2]);
+    for (int base = 0; base < n; base += 32) {
+      int k = base + lane;
+      Real ax = 0, ay = 0, az = 0;
+      if (k < n) {
+        ax = x[3 * k + 0];
+        ay = x[3 * k + 1];
+        az = x[3 * k + 2];
+      }
+      int cnt = min(32, n - base);
+      for (int q = 0; q < cnt; ++q) {
+        Real vx = __shfl_sync(0xffffffffu, ax, q);
+        Real vy = __shfl_sync(0xffffffffu, ay, q);
+        Real vz = __shfl_sync(0xffffffffu, az, q);
+        cx = add_rn(cx, vx);
+        cy = add_rn(cy, vy);
+        cz = add_rn(cz, vz);
+      }
     }
     Real rn = Real(n);
     cx = div_rn(cx, rn);
     cy = div_rn(cy, rn);
     cz = div_rn(cz, rn);
     Real d2max = 0;
-    for (int k = 0; k < n; ++k) {
+    for (int k = lane; k < n; k += 32) {
       Real dx = sub_rn(x[3 * k + 0], cx);
       Real dy = sub_rn(x[3 * k + 1], cy);
       Real dz = sub_rn(x[3 * k + 2], cz);
       Real d2 = add_rn(add_rn(mul_rn(dx, dx), mul_rn(dy, dy)), mul_rn(dz, dz));
       if (d2 > d2max) d2max = d2;
     }
-    out[0] = cx;
-    out[1] = cy;
-    out[2] = cz;
-    out[3] = sqrt_rn(d2max);
+    for (int o = 16; o > 0; o >>= 1) {
+      Real v = __shfl_xor_sync(0xffffffffu, d2max, o);
+      d2max = v > d2max ? v : d2max;
+    }
+    if (lane == 0) {
+      out[0] = cx;
+      out[1] = cy;
+      out[2] = cz;
+      out[3] = sqrt_rn(d2max);
+    }
   }
 }
 
@@ -1239,7 +1262,7 @@ template <typename Real, bool GRAD, bool BLOCK_PAIR>
 int launch_score(tmol_b200_ljlk_plan* pl, ScoreArgs<Real> s, cudaStream_t st) {
   int n_blocks = pl->P * pl->B;
   int threads = 256;
-  int grid_s = std::max(1, std::min((n_blocks + threads - 1) / threads, pl->n_sm * 8));
+  int grid_s = std::max(1, std::min((n_blocks + 7) / 8, pl->n_sm * 16));
   spheres_kernel<Real><<<grid_s, threads, 0, st>>>(s);
   CK(cudaGetLastError());
   CK(cudaMemsetAsync(pl->counters, 0, sizeof(int), st));

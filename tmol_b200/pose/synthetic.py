@@ -64,10 +64,8 @@ def synthetic_pose_stack(
         cell = numpy.array([k % side, (k // side) % side, k // (side * side)], dtype=numpy.float64)
         c = coords[k]
         coords[k] = c - c.mean(axis=0) + spacing * cell
-    ps = build_pose_stack(topos, coords, pbt=pbt, device=torch.device("cpu"))
-    if torch.device(device) != torch.device("cpu"):
-        ps = ps.to(device)
-    return ps
+    # the dense bond-separation tensors are built directly on `device`
+    return build_pose_stack(topos, coords, pbt=pbt, device=torch.device(device))
 
 
 def log_uniform_sizes(rng, n, lo, hi):
