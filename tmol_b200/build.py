@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "lib", "libtmol_b200_ljlk.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["ljlk.cu", "ljlk_noalloc.cu"]
+SOURCES = ["ljlk.cu", "ljlk_noalloc.cu", "screen.cu"]
 HEADERS = ["ljlk_potentials.cuh"]
 
 
@@ -32,7 +32,8 @@ def _stale():
         return True
     t = os.path.getmtime(OUT)
     deps = [os.path.join(SRC, f) for f in SOURCES + HEADERS]
-    deps.append(os.path.join(HERE, "..", "include", "tmol_b200_ljlk.h"))
+    for h in ("tmol_b200_ljlk.h", "tmol_b200_screen.h"):
+        deps.append(os.path.join(HERE, "..", "include", h))
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 

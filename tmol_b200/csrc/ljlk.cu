@@ -37,6 +37,7 @@
 #include <vector>
 
 #include "../../include/tmol_b200_ljlk.h"
+#include "../../include/tmol_b200_screen.h"
 #include "ljlk_potentials.cuh"
 
 namespace tmol_b200 {
@@ -299,6 +300,10 @@ struct ScoreArgs {
   Real* dcoords;
   int* ticket;
   unsigned long long* counts;
+  // optional skip mask: bit b2 of row (p, b1) set = do not score the block
+  // pair (never honoured for b1 == b2 or count-pair partners)
+  const uint32_t* skip;
+  int skip_words;  // 32-bit words per row
 };
 
 // Bounding sphere per block: centroid (sum of atoms in order, then divided
@@ -887,6 +892,19 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
       const Real reach1 = rad1 + reach_atoms;
       const Real reach1_2 = reach1 * reach1 * Real(1.0001);
 
+      // the row's count-pair partners, one per lane
+      RowPartners rp;
+      const int ncp = s.cp_count[r.i1];
+      {
+        rp.b2 = -1;
+        rp.minsep = 6;
+        rp.entry = r.i1 * CP_CAP + lane;
+        if (lane < ncp) {
+          rp.b2 = s.cp_b2[rp.entry];
+          rp.minsep = s.cp_minsep[rp.entry];
+        }
+      }
+
       // neighbour tests of the whole range first: one ballot mask per 32
       // candidates, kept in registers (lane k holds the mask of batch k)
       unsigned my_mask = 0;
@@ -907,6 +925,15 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
           }
           if (s.nbr) s.nbr[(int64_t)r.i1 * s.B + b2] = hit ? 1 : 0;
         }
+        if (s.skip) {
+          // a screened-out pair is dropped unless it is b1 itself or one of
+          // b1's count-pair partners (bond separation <= 4)
+          bool drop = hit && b2 != r.b1 &&
+                      ((s.skip[(int64_t)r.i1 * s.skip_words + (b2 >> 5)] >> (b2 & 31)) & 1u);
+          for (int k = 0; k < ncp; ++k)
+            if (__shfl_sync(0xffffffffu, rp.b2, k) == b2) drop = false;
+          if (drop) hit = false;
+        }
         unsigned mk = __ballot_sync(0xffffffffu, hit);
         if (lane == bi) my_mask = mk;
       }
@@ -917,18 +944,6 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
         continue;
       }
 
-      // the row's count-pair partners, one per lane
-      RowPartners rp;
-      {
-        int ncp = s.cp_count[r.i1];
-        rp.b2 = -1;
-        rp.minsep = 6;
-        rp.entry = r.i1 * CP_CAP + lane;
-        if (lane < ncp) {
-          rp.b2 = s.cp_b2[rp.entry];
-          rp.minsep = s.cp_minsep[rp.entry];
-        }
-      }
       int nt1 = (r.n1 + TILE - 1) / TILE;
       for (int ti = 0; ti < nt1; ++ti) {
         r.st1 = ti * TILE;
@@ -1067,6 +1082,88 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
     atomicAdd(&s.counts[lane], w.counts[lane]);
 }
 
+// Block-pair screen candidates: every later block b2 of row (p, b1) that
+// passes the scoring kernel's sphere test (same arithmetic, so the same
+// pairs) and is not a count-pair partner (bond separation <= 4).  Appends
+// (row, b2), both block types and 8 features per pair in warp-aggregated
+// chunks; *count ends as the total, entries past `capacity` are not written.
+// Features (fp32): d/10, (d - r1 - r2)/6, r1/5, r2/5, log2(b2 - b1)/10,
+// (|a1 - a2| - d)/5, (|a1 - c2| - d)/5, (|a2 - c1| - d)/5, where c, r are
+// the block spheres, d = |c1 - c2| and a is a block's first atom.
+__global__ void screen_candidates_kernel(ScoreArgs<float> s, int capacity,
+                                         int32_t* pair_row, int32_t* pair_b2,
+                                         int32_t* pair_bt, float* feats,
+                                         int32_t* count) {
+  const int lane = threadIdx.x & 31;
+  const int n_rows = s.P * s.B;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n_rows; row += warps) {
+    const int bt1 = s.blk_bt[row];
+    if (bt1 < 0) continue;
+    const int p = row / s.B, b1 = row - p * s.B;
+    const int last = s.pose_last[p];
+    const float* sph1 = s.spheres + 4 * (int64_t)row;
+    const float c1x = sph1[0], c1y = sph1[1], c1z = sph1[2], rad1 = sph1[3];
+    const float* a1 = s.coords + 3 * (int64_t)s.blk_off[row];
+    const float a1x = a1[0], a1y = a1[1], a1z = a1[2];
+    const int ncp = s.cp_count[row];
+    const int my_cp = lane < ncp ? s.cp_b2[row * CP_CAP + lane] : -1;
+    for (int base = b1 + 1; base < last; base += 32) {
+      const int b2 = base + lane;
+      const int i2 = p * s.B + b2;
+      bool take = false;
+      int bt2 = -1;
+      if (b2 < last) {
+        bt2 = s.blk_bt[i2];
+        if (bt2 >= 0) {
+          const float* s2 = s.spheres + 4 * (int64_t)i2;
+          float dx = sub_rn(c1x, s2[0]);
+          float dy = sub_rn(c1y, s2[1]);
+          float dz = sub_rn(c1z, s2[2]);
+          float d2 = add_rn(add_rn(mul_rn(dx, dx), mul_rn(dy, dy)), mul_rn(dz, dz));
+          float thr = add_rn(add_rn(rad1, s2[3]), s.reach);
+          take = d2 < mul_rn(thr, thr);
+        }
+      }
+      for (int k = 0; k < ncp; ++k)
+        if (__shfl_sync(0xffffffffu, my_cp, k) == b2) take = false;
+      const unsigned m = __ballot_sync(0xffffffffu, take);
+      if (!m) continue;
+      int first = 0;
+      if (lane == 0) first = atomicAdd(count, __popc(m));
+      first = __shfl_sync(0xffffffffu, first, 0);
+      if (!take) continue;
+      const int idx = first + __popc(m & ((1u << lane) - 1u));
+      if (idx >= capacity) continue;
+      const float* s2 = s.spheres + 4 * (int64_t)i2;
+      const float* a2 = s.coords + 3 * (int64_t)s.blk_off[i2];
+      const float c2x = s2[0], c2y = s2[1], c2z = s2[2], rad2 = s2[3];
+      const float a2x = a2[0], a2y = a2[1], a2z = a2[2];
+      const float d = sqrtf((c1x - c2x) * (c1x - c2x) + (c1y - c2y) * (c1y - c2y) +
+                            (c1z - c2z) * (c1z - c2z));
+      const float daa = sqrtf((a1x - a2x) * (a1x - a2x) + (a1y - a2y) * (a1y - a2y) +
+                              (a1z - a2z) * (a1z - a2z));
+      const float dac = sqrtf((a1x - c2x) * (a1x - c2x) + (a1y - c2y) * (a1y - c2y) +
+                              (a1z - c2z) * (a1z - c2z));
+      const float dca = sqrtf((a2x - c1x) * (a2x - c1x) + (a2y - c1y) * (a2y - c1y) +
+                              (a2z - c1z) * (a2z - c1z));
+      float* f = feats + 8 * (int64_t)idx;
+      f[0] = d * 0.1f;
+      f[1] = (d - rad1 - rad2) * (1.0f / 6.0f);
+      f[2] = rad1 * 0.2f;
+      f[3] = rad2 * 0.2f;
+      f[4] = log2f((float)(b2 - b1)) * 0.1f;
+      f[5] = (daa - d) * 0.2f;
+      f[6] = (dac - d) * 0.2f;
+      f[7] = (dca - d) * 0.2f;
+      pair_row[idx] = row;
+      pair_b2[idx] = b2;
+      pair_bt[2 * idx] = bt1;
+      pair_bt[2 * idx + 1] = bt2;
+    }
+  }
+}
+
 // FP32 issue-rate probe: 8 independent FMA chains per thread, so that the
 // FMA pipe, not latency, bounds it.  2 FLOP per FMA.
 __global__ void fp32_peak_kernel(float* out, int iters, float a, float b) {
@@ -1128,6 +1225,8 @@ struct tmol_b200_ljlk_plan {
   int n_sm = 148;
   int64_t device_bytes = 0;
   std::vector<int> host_pose_last;
+  const uint32_t* skip = nullptr;  // caller-owned screen mask, or null
+  int skip_words = 0;
 };
 
 namespace {
@@ -1255,6 +1354,8 @@ ScoreArgs<Real> score_args(tmol_b200_ljlk_plan* pl, const void* coords) {
   s.C = pl->C;
   s.ticket = pl->counters;
   s.counts = pl->counts;
+  s.skip = pl->skip;
+  s.skip_words = pl->skip_words;
   return s;
 }
 
@@ -1670,6 +1771,41 @@ int tmol_b200_ljlk_plan_rebalance(tmol_b200_ljlk_plan* plan, void* stream) {
   CK(cudaMemcpyAsync(plan->work, sorted.data(), sizeof(int4) * n, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(plan->item_cost, sorted_cost.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
   CK(cudaStreamSynchronize(st));
+  return TMOL_B200_OK;
+}
+
+int tmol_b200_ljlk_plan_set_skip_mask(tmol_b200_ljlk_plan* plan,
+                                      const uint32_t* mask,
+                                      int32_t words_per_row) {
+  if (!plan) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  if (mask && words_per_row < (plan->B + 31) / 32) return TMOL_B200_ERR_SHAPE;
+  plan->skip = mask;
+  plan->skip_words = mask ? words_per_row : 0;
+  return TMOL_B200_OK;
+}
+
+int tmol_b200_ljlk_screen_candidates(tmol_b200_ljlk_plan* plan,
+                                     const void* coords, int32_t capacity,
+                                     int32_t* pair_row, int32_t* pair_b2,
+                                     int32_t* pair_bt, float* features,
+                                     int32_t* count, void* stream) {
+  if (!plan || !count || capacity < 0 || (!coords && plan->N > 0))
+    return TMOL_B200_ERR_INVALID_ARGUMENT;
+  if (capacity > 0 && (!pair_row || !pair_b2 || !pair_bt || !features))
+    return TMOL_B200_ERR_INVALID_ARGUMENT;
+  if (plan->real_bytes != 4) return TMOL_B200_ERR_DTYPE;
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(cudaMemsetAsync(count, 0, sizeof(int32_t), st));
+  const int n_blocks = plan->P * plan->B;
+  if (n_blocks == 0) return TMOL_B200_OK;
+  ScoreArgs<float> s = score_args<float>(plan, coords);
+  const int threads = 256;
+  const int grid = std::max(1, std::min((n_blocks + 7) / 8, plan->n_sm * 16));
+  spheres_kernel<float><<<grid, threads, 0, st>>>(s);
+  CK(cudaGetLastError());
+  screen_candidates_kernel<<<grid, threads, 0, st>>>(s, capacity, pair_row, pair_b2,
+                                                     pair_bt, features, count);
+  CK(cudaGetLastError());
   return TMOL_B200_OK;
 }
 

@@ -1,4 +1,5 @@
-"""ctypes binding of the C ABI in ``include/tmol_b200_ljlk.h``.
+"""ctypes binding of the C ABI in ``include/tmol_b200_ljlk.h`` and
+``include/tmol_b200_screen.h``.
 
 The shared library is built in-tree (``tmol_b200/lib``) by
 ``tmol_b200.build``.  There is no fallback: importing this module without the
@@ -68,6 +69,15 @@ class Launch(ctypes.Structure):
 
 
 # Every symbol the header declares, with its ctypes signature.
+_V, _I32, _I64, _F = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_float
+
+
+class ScreenWeights(ctypes.Structure):
+    """tmol_b200_screen_weights: device pointers of the screen MLP."""
+
+    _fields_ = [(n, ctypes.c_void_p) for n in ("w1", "w2", "w3", "w4", "b1", "b2", "b3", "b4", "emb")]
+
+
 SIGNATURES = {
     "tmol_b200_ljlk_plan_create": (
         ctypes.c_int,
@@ -116,6 +126,23 @@ SIGNATURES = {
         ],
     ),
     "tmol_b200_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    # learned block-pair screen (include/tmol_b200_screen.h)
+    "tmol_b200_ljlk_plan_set_skip_mask": (ctypes.c_int, [_V, _V, _I32]),
+    "tmol_b200_ljlk_screen_candidates": (ctypes.c_int, [_V, _V, _I32, _V, _V, _V, _V, _V, _V]),
+    "tmol_b200_screen_infer": (
+        ctypes.c_int,
+        [ctypes.POINTER(ScreenWeights), _V, _V, _V, _V, _V, _I32, _F, _V, _I32, _I64, _V, _V],
+    ),
+    "tmol_b200_screen_gemm": (
+        ctypes.c_int,
+        [_V, _I64, _I64, _V, _I64, _I64, _V, _I64, _V, _I64, _V, _I32, _I32, _I32, _I32, _I32, _I32, _V],
+    ),
+    "tmol_b200_screen_relu_backward": (ctypes.c_int, [_V, _V, _V, _V, _I64, _V]),
+    "tmol_b200_screen_col_sum": (ctypes.c_int, [_V, _I64, _I32, _V, _V]),
+    "tmol_b200_screen_pinball": (ctypes.c_int, [_V, _V, _I64, _F, _V, _V, _V, _V]),
+    "tmol_b200_screen_adam": (ctypes.c_int, [_V, _V, _V, _V, _V, _I64, _F, _F, _F, _F, _I32, _F, _V]),
+    "tmol_b200_screen_assemble_features": (ctypes.c_int, [_V, _V, _V, _I64, _V, _V]),
+    "tmol_b200_screen_embedding_backward": (ctypes.c_int, [_V, _V, _I64, _V, _V]),
 }
 
 _lib = None

@@ -33,18 +33,9 @@ def random_dihedrals(rng, n, extra_chi_sd=0.0):
     return phi, psi, omega, chis
 
 
-def synthetic_pose_stack(
-    n_res_per_pose,
-    seeds,
-    device=torch.device("cpu"),
-    extra_chi_sd=0.0,
-    spacing=1000.0,
-    pbt=None,
-):
-    """One pose per entry of ``n_res_per_pose``; pose k uses
-    ``numpy.random.default_rng(seeds[k])``.  Poses are translated onto a cubic
-    grid with ``spacing`` angstroms between neighbours so that no two overlap
-    (the scoring itself never couples poses)."""
+def synthetic_topologies_and_coords(n_res_per_pose, seeds, extra_chi_sd=0.0, spacing=1000.0, pbt=None):
+    """The host half of ``synthetic_pose_stack``: per-pose topologies and
+    ``[n_pose_atoms, 3]`` coordinates (numpy), already placed on the grid."""
     rts = ResidueTypeSet.get_default()
     pbt = pbt or default_packed_block_types(torch.device("cpu"))
     topos, phis, psis, omegas, chis = [], [], [], [], []
@@ -64,6 +55,22 @@ def synthetic_pose_stack(
         cell = numpy.array([k % side, (k // side) % side, k // (side * side)], dtype=numpy.float64)
         c = coords[k]
         coords[k] = c - c.mean(axis=0) + spacing * cell
+    return topos, coords
+
+
+def synthetic_pose_stack(
+    n_res_per_pose,
+    seeds,
+    device=torch.device("cpu"),
+    extra_chi_sd=0.0,
+    spacing=1000.0,
+    pbt=None,
+):
+    """One pose per entry of ``n_res_per_pose``; pose k uses
+    ``numpy.random.default_rng(seeds[k])``.  Poses are translated onto a cubic
+    grid with ``spacing`` angstroms between neighbours so that no two overlap
+    (the scoring itself never couples poses)."""
+    topos, coords = synthetic_topologies_and_coords(n_res_per_pose, seeds, extra_chi_sd, spacing, pbt)
     # the dense bond-separation tensors are built directly on `device`
     return build_pose_stack(topos, coords, pbt=pbt, device=torch.device(device))
 

@@ -245,6 +245,61 @@ class LJLKPlan:
         native.call("tmol_b200_ljlk_last_counts", self.ptr, self._stream(), arr)
         return dict(zip(self.COUNT_NAMES, list(arr)))
 
+    def skip_mask_words(self):
+        """32-bit words per (pose, block) row of a skip mask."""
+        return (self.max_n_blocks + 31) // 32
+
+    def set_skip_mask(self, mask):
+        """Install a block-pair skip mask (int32 [P * B, words], caller-owned,
+        kept alive by the plan) or remove it (None).  Bit b2 of row
+        (p, b1) set = later scoring calls leave block pair (b1, b2) out; the
+        diagonal and count-pair partners are always scored."""
+        if mask is None:
+            self._skip_mask = None
+            native.call("tmol_b200_ljlk_plan_set_skip_mask", self.ptr, None, 0)
+            return
+        if mask.device != self.device or mask.dtype != torch.int32 or not mask.is_contiguous():
+            raise ValueError("skip mask must be a contiguous int32 tensor on the plan's device")
+        if mask.dim() != 2 or mask.shape[0] != self.n_poses * self.max_n_blocks:
+            raise ValueError(f"skip mask must be [{self.n_poses * self.max_n_blocks}, words]")
+        self._skip_mask = mask
+        native.call(
+            "tmol_b200_ljlk_plan_set_skip_mask", self.ptr, ctypes.c_void_p(mask.data_ptr()), int(mask.shape[1])
+        )
+
+    def screen_candidates(self, coords, capacity, out=None):
+        """Block pairs b1 < b2 that pass the sphere test and are not
+        count-pair partners, with their screen features.  Returns a dict of
+        device tensors: row [cap] (p * B + b1), b2 [cap], bt [cap, 2],
+        features [cap, 8] and count [1] (total candidates, may exceed cap)."""
+        self._check_coords(coords)
+        if self.dtype != torch.float32:
+            raise TypeError("screen candidates need a float32 plan")
+        coords = coords.contiguous()
+        if out is None:
+            dev = self.device
+            out = dict(
+                row=torch.empty(capacity, dtype=torch.int32, device=dev),
+                b2=torch.empty(capacity, dtype=torch.int32, device=dev),
+                bt=torch.empty((capacity, 2), dtype=torch.int32, device=dev),
+                features=torch.empty((capacity, 8), dtype=torch.float32, device=dev),
+                count=torch.empty(1, dtype=torch.int32, device=dev),
+            )
+        capacity = out["row"].shape[0]
+        native.call(
+            "tmol_b200_ljlk_screen_candidates",
+            self.ptr,
+            ctypes.c_void_p(coords.data_ptr()),
+            int(capacity),
+            ctypes.c_void_p(out["row"].data_ptr()),
+            ctypes.c_void_p(out["b2"].data_ptr()),
+            ctypes.c_void_p(out["bt"].data_ptr()),
+            ctypes.c_void_p(out["features"].data_ptr()),
+            ctypes.c_void_p(out["count"].data_ptr()),
+            self._stream(),
+        )
+        return out
+
     def profile(self, enable=True):
         native.call("tmol_b200_ljlk_profile", self.ptr, int(enable))
 
