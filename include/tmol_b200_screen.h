@@ -11,11 +11,15 @@
  * per-row bit mask.  Intra-block pairs and count-pair partners (bond
  * separation <= 4) are never candidates and are never skipped.
  *
- * Candidate features (8 fp32 per pair), from the block spheres (centroid c,
- * radius r), d = |c1 - c2| and each block's first atom a:
+ * Candidate features (12 fp32 per pair), from the block spheres (centroid
+ * c, radius r), d = |c1 - c2|, each block's first atom a and its two
+ * sub-spheres u0 (atoms 0-3: N, CA, C, O of an amino acid) and u1 (the
+ * other atoms; u0 again for blocks of <= 4 atoms):
  *   d/10, (d - r1 - r2)/6, r1/5, r2/5, log2(b2 - b1)/10,
- *   (|a1 - a2| - d)/5, (|a1 - c2| - d)/5, (|a2 - c1| - d)/5
- * followed in the network input by the 12-value embeddings of both block
+ *   (|a1 - a2| - d)/5, (|a1 - c2| - d)/5, (|a2 - c1| - d)/5,
+ *   sub-sphere gaps (|u1_i - u2_j| - r - r)/6 for (i, j) = (0,0), (0,1),
+ *   (1,0), (1,1)
+ * followed in the network input by the 10-value embeddings of both block
  * types.
  *
  * All pointers are device pointers; every call enqueues work on `stream`
@@ -32,7 +36,7 @@ extern "C" {
 
 /* Network parameters (torch Linear layout: weight [out, in] row-major).
  *   w1 bf16 [128, 32], w2 bf16 [128, 128], w3 bf16 [128, 128], w4 bf16 [128]
- *   b1, b2, b3 fp32 [128], b4 fp32 [1], emb fp32 [n_block_types, 12] */
+ *   b1, b2, b3 fp32 [128], b4 fp32 [1], emb fp32 [n_block_types, 10] */
 typedef struct {
   const void* w1;
   const void* w2;
@@ -58,8 +62,8 @@ int tmol_b200_ljlk_plan_set_skip_mask(tmol_b200_ljlk_plan* plan,
 /* Screen candidates of the plan's PoseStack at `coords`: every block pair
  * b1 < b2 that passes the scoring kernel's sphere test and is not a
  * count-pair partner.  Writes pair_row[i] = p * B + b1, pair_b2[i] = b2,
- * pair_bt[2 i], pair_bt[2 i + 1] = the block types and features[8 i .. 8 i
- * + 7] for i < min(*count, capacity); *count (device) ends as the number of
+ * pair_bt[2 i], pair_bt[2 i + 1] = the block types and features[12 i ..
+ * 12 i + 11] for i < min(*count, capacity); *count (device) ends as the number of
  * candidates, which may exceed capacity.  float32 plans only. */
 int tmol_b200_ljlk_screen_candidates(tmol_b200_ljlk_plan* plan,
                                      const void* coords, int32_t capacity,
@@ -114,8 +118,8 @@ int tmol_b200_screen_adam(float* w, const float* grad, float* m, float* v,
                           float eps, int32_t step, float weight_decay,
                           void* stream);
 
-/* X [n, 32] bf16 = [features (8), emb[pair_bt[2 i]] (12),
- * emb[pair_bt[2 i + 1]] (12)]. */
+/* X [n, 32] bf16 = [features (12), emb[pair_bt[2 i]] (10),
+ * emb[pair_bt[2 i + 1]] (10)]. */
 int tmol_b200_screen_assemble_features(const float* features,
                                        const int32_t* pair_bt,
                                        const float* emb, int64_t n, void* X,

@@ -18,7 +18,7 @@ finite-difference check.
 
 import numpy
 
-N_IN, HID, EMB, N_SCAL = 32, 128, 12, 8
+N_IN, HID, EMB, N_SCAL = 32, 128, 10, 12
 
 
 def to_bf16(x):
@@ -102,34 +102,47 @@ def pinball(pred, y, tau):
     return loss, d
 
 
+def _sphere(x):
+    c = x.mean(0)
+    return c, numpy.sqrt(((x - c) ** 2).sum(1).max())
+
+
 def candidate_features(coords, block_type, block_offset, bt_n_atoms, nbr, min_bondsep, pose_index):
     """Candidates and features of one pose, as the candidate kernel defines
     them: pairs b1 < b2 with nbr[b1, b2] != 0 and min_bondsep > 4.
-    Returns (pairs [n, 2] sorted, features [n, 8] float64)."""
+    Returns (pairs [n, 2] sorted, features [n, 12] float64).  Sub-spheres:
+    atoms [0, 4) and [4, n) (the first part again when n <= 4)."""
     B = block_type.shape[0]
     cen = numpy.zeros((B, 3))
     rad = numpy.zeros(B)
     first = numpy.zeros((B, 3))
+    sub = numpy.zeros((B, 2, 4))
     for b in range(B):
         if block_type[b] < 0:
             continue
         x = numpy.asarray(coords[block_offset[b]:block_offset[b] + bt_n_atoms[block_type[b]]], numpy.float64)
-        cen[b] = x.mean(0)
-        rad[b] = numpy.sqrt(((x - cen[b]) ** 2).sum(1).max())
+        cen[b], rad[b] = _sphere(x)
         first[b] = x[0]
+        head = x[: min(4, len(x))]
+        tail = x[4:] if len(x) > 4 else head
+        for part, xs in enumerate((head, tail)):
+            c, r = _sphere(xs)
+            sub[b, part, :3] = c
+            sub[b, part, 3] = r
     b1, b2 = numpy.nonzero(numpy.triu(nbr, 1) & (min_bondsep > 4))
     d = numpy.linalg.norm(cen[b1] - cen[b2], axis=1)
-    feats = numpy.stack(
-        [
-            d / 10,
-            (d - rad[b1] - rad[b2]) / 6,
-            rad[b1] / 5,
-            rad[b2] / 5,
-            numpy.log2(numpy.maximum(b2 - b1, 1)) / 10,
-            (numpy.linalg.norm(first[b1] - first[b2], axis=1) - d) / 5,
-            (numpy.linalg.norm(first[b1] - cen[b2], axis=1) - d) / 5,
-            (numpy.linalg.norm(first[b2] - cen[b1], axis=1) - d) / 5,
-        ],
-        axis=1,
-    )
-    return numpy.stack([b1, b2], axis=1), feats
+    cols = [
+        d / 10,
+        (d - rad[b1] - rad[b2]) / 6,
+        rad[b1] / 5,
+        rad[b2] / 5,
+        numpy.log2(numpy.maximum(b2 - b1, 1)) / 10,
+        (numpy.linalg.norm(first[b1] - first[b2], axis=1) - d) / 5,
+        (numpy.linalg.norm(first[b1] - cen[b2], axis=1) - d) / 5,
+        (numpy.linalg.norm(first[b2] - cen[b1], axis=1) - d) / 5,
+    ]
+    for i in range(2):
+        for j in range(2):
+            u, v = sub[b1, i], sub[b2, j]
+            cols.append((numpy.linalg.norm(u[:, :3] - v[:, :3], axis=1) - u[:, 3] - v[:, 3]) / 6)
+    return numpy.stack([b1, b2], axis=1), numpy.stack(cols, axis=1)

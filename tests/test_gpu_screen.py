@@ -2,7 +2,8 @@
 
 - the BF16 tensor-core GEMM against an fp32 matmul of the same bf16 values;
 - candidate enumeration and features against the NumPy oracle (the
-  candidate set bit-exact, features to fp32 rounding);
+  candidate set bit-exact, features to fp32 rounding of coordinates that lie
+  up to ~1e3 A from the origin);
 - the skip mask's meaning: scoring with a mask equals the plain block-pair
   energies summed over the pairs left in (the diagonal and count-pair
   partners are never left out), and the gradient equals the C oracle's
@@ -109,7 +110,9 @@ def test_candidates_match_oracle(small):
         n_expected += len(pairs)
         for (b1, bb2), fe in zip(pairs, f):
             k = got[(p * B + int(b1), int(bb2))]
-            numpy.testing.assert_allclose(feats[k], fe, rtol=1e-4, atol=2e-5)
+            # poses sit up to ~1e3 A from the origin: fp32 centroids carry
+            # ~1e-4 A of rounding, features are distances / 5
+            numpy.testing.assert_allclose(feats[k], fe, rtol=1e-4, atol=1e-4)
             assert tuple(bt[k]) == (block_type[p, b1], block_type[p, bb2])
     assert n == n_expected
 
@@ -157,12 +160,13 @@ def test_skip_mask_leaves_out_exactly_the_masked_pairs(small):
     finally:
         plan.set_skip_mask(None)
     E3, _ = plan.forward(coords)
-    torch.testing.assert_close(E3, E0, rtol=0, atol=0)
+    # per-pose sums are accumulated atomically: equal up to summation order
+    torch.testing.assert_close(E3, E0, rtol=1e-6, atol=1e-6)
 
 
 def _random_rows(n, nbt, seed):
     g = torch.Generator(device=DEV).manual_seed(seed)
-    feats = torch.randn(n, 8, device=DEV, generator=g)
+    feats = torch.randn(n, 12, device=DEV, generator=g)
     bt = torch.randint(0, nbt, (n, 2), device=DEV, generator=g, dtype=torch.int32)
     return feats, bt
 

@@ -18,7 +18,7 @@ def random_params(rng, n_bt=7):
         "b3": rng.normal(0, 0.1, 128),
         "w4": rng.normal(0, (1 / 128) ** 0.5, (1, 128)),
         "b4": rng.normal(0, 0.1, 1),
-        "emb": rng.normal(0, 0.3, (n_bt, 12)),
+        "emb": rng.normal(0, 0.3, (n_bt, 10)),
     }
 
 
@@ -55,7 +55,7 @@ def test_mlp_backward_matches_finite_differences():
     rng = numpy.random.default_rng(1)
     params = random_params(rng)
     n = 40
-    feats = rng.normal(size=(n, 8))
+    feats = rng.normal(size=(n, 12))
     bt = rng.integers(0, 7, size=(n, 2))
     dpred = rng.normal(size=n)
     net = sm.MLP(params, bf16=False)
@@ -78,7 +78,7 @@ def test_mlp_backward_matches_finite_differences():
 def test_bf16_mode_is_close_to_float64():
     rng = numpy.random.default_rng(2)
     params = random_params(rng)
-    feats = rng.normal(size=(64, 8))
+    feats = rng.normal(size=(64, 12))
     bt = rng.integers(0, 7, size=(64, 2))
     p64 = sm.MLP(params, bf16=False).forward(feats, bt)
     p16 = sm.MLP(params, bf16=True).forward(feats, bt)

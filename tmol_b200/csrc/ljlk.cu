@@ -1082,18 +1082,68 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
     atomicAdd(&s.counts[lane], w.counts[lane]);
 }
 
+// Sub-spheres of every block for the screen's features: atoms [0, 4) (the
+// backbone N, CA, C, O of an amino acid) and atoms [4, n) (the rest; the
+// first part again when n <= 4), each as centroid + largest centroid
+// distance.  Plain fp32: these are network inputs, not neighbour tests.
+__global__ void sub_spheres_kernel(ScoreArgs<float> s, float* sub) {
+  const int n_blocks = s.P * s.B;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_blocks; i += gridDim.x * blockDim.x) {
+    float* out = sub + 8 * (int64_t)i;
+    const int bt = s.blk_bt[i];
+    if (bt < 0) {
+      for (int k = 0; k < 8; ++k) out[k] = 0.0f;
+      continue;
+    }
+    const int n = s.bt_n_atoms[bt];
+    const float* x = s.coords + 3 * (int64_t)s.blk_off[i];
+    for (int part = 0; part < 2; ++part) {
+      int a0 = 0, a1 = n < 4 ? n : 4;
+      if (part == 1 && n > 4) {
+        a0 = 4;
+        a1 = n;
+      }
+      float cx = 0, cy = 0, cz = 0;
+      for (int k = a0; k < a1; ++k) {
+        cx += x[3 * k];
+        cy += x[3 * k + 1];
+        cz += x[3 * k + 2];
+      }
+      const float inv = a1 > a0 ? 1.0f / (float)(a1 - a0) : 0.0f;
+      cx *= inv;
+      cy *= inv;
+      cz *= inv;
+      float r2 = 0;
+      for (int k = a0; k < a1; ++k) {
+        float dx = x[3 * k] - cx, dy = x[3 * k + 1] - cy, dz = x[3 * k + 2] - cz;
+        r2 = fmaxf(r2, dx * dx + dy * dy + dz * dz);
+      }
+      out[4 * part + 0] = cx;
+      out[4 * part + 1] = cy;
+      out[4 * part + 2] = cz;
+      out[4 * part + 3] = sqrtf(r2);
+    }
+  }
+}
+
+__device__ __forceinline__ float dist3(float ax, float ay, float az, float bx, float by, float bz) {
+  return sqrtf((ax - bx) * (ax - bx) + (ay - by) * (ay - by) + (az - bz) * (az - bz));
+}
+
 // Block-pair screen candidates: every later block b2 of row (p, b1) that
 // passes the scoring kernel's sphere test (same arithmetic, so the same
 // pairs) and is not a count-pair partner (bond separation <= 4).  Appends
-// (row, b2), both block types and 8 features per pair in warp-aggregated
+// (row, b2), both block types and 12 features per pair in warp-aggregated
 // chunks; *count ends as the total, entries past `capacity` are not written.
-// Features (fp32): d/10, (d - r1 - r2)/6, r1/5, r2/5, log2(b2 - b1)/10,
-// (|a1 - a2| - d)/5, (|a1 - c2| - d)/5, (|a2 - c1| - d)/5, where c, r are
-// the block spheres, d = |c1 - c2| and a is a block's first atom.
-__global__ void screen_candidates_kernel(ScoreArgs<float> s, int capacity,
-                                         int32_t* pair_row, int32_t* pair_b2,
-                                         int32_t* pair_bt, float* feats,
-                                         int32_t* count) {
+// Features (fp32), with c, r the block spheres, d = |c1 - c2|, a a block's
+// first atom and (u, v) the sub-spheres of sub_spheres_kernel:
+//   d/10, (d - r1 - r2)/6, r1/5, r2/5, log2(b2 - b1)/10,
+//   (|a1 - a2| - d)/5, (|a1 - c2| - d)/5, (|a2 - c1| - d)/5,
+//   then (|u1 - u2| - r_u1 - r_u2)/6 for (u1, u2) = (0,0), (0,1), (1,0), (1,1).
+__global__ void screen_candidates_kernel(ScoreArgs<float> s, const float* sub,
+                                         int capacity, int32_t* pair_row,
+                                         int32_t* pair_b2, int32_t* pair_bt,
+                                         float* feats, int32_t* count) {
   const int lane = threadIdx.x & 31;
   const int n_rows = s.P * s.B;
   const int warps = (gridDim.x * blockDim.x) >> 5;
@@ -1106,6 +1156,7 @@ __global__ void screen_candidates_kernel(ScoreArgs<float> s, int capacity,
     const float c1x = sph1[0], c1y = sph1[1], c1z = sph1[2], rad1 = sph1[3];
     const float* a1 = s.coords + 3 * (int64_t)s.blk_off[row];
     const float a1x = a1[0], a1y = a1[1], a1z = a1[2];
+    const float* u1 = sub + 8 * (int64_t)row;
     const int ncp = s.cp_count[row];
     const int my_cp = lane < ncp ? s.cp_b2[row * CP_CAP + lane] : -1;
     for (int base = b1 + 1; base < last; base += 32) {
@@ -1137,25 +1188,25 @@ __global__ void screen_candidates_kernel(ScoreArgs<float> s, int capacity,
       if (idx >= capacity) continue;
       const float* s2 = s.spheres + 4 * (int64_t)i2;
       const float* a2 = s.coords + 3 * (int64_t)s.blk_off[i2];
+      const float* u2 = sub + 8 * (int64_t)i2;
       const float c2x = s2[0], c2y = s2[1], c2z = s2[2], rad2 = s2[3];
       const float a2x = a2[0], a2y = a2[1], a2z = a2[2];
-      const float d = sqrtf((c1x - c2x) * (c1x - c2x) + (c1y - c2y) * (c1y - c2y) +
-                            (c1z - c2z) * (c1z - c2z));
-      const float daa = sqrtf((a1x - a2x) * (a1x - a2x) + (a1y - a2y) * (a1y - a2y) +
-                              (a1z - a2z) * (a1z - a2z));
-      const float dac = sqrtf((a1x - c2x) * (a1x - c2x) + (a1y - c2y) * (a1y - c2y) +
-                              (a1z - c2z) * (a1z - c2z));
-      const float dca = sqrtf((a2x - c1x) * (a2x - c1x) + (a2y - c1y) * (a2y - c1y) +
-                              (a2z - c1z) * (a2z - c1z));
-      float* f = feats + 8 * (int64_t)idx;
+      const float d = dist3(c1x, c1y, c1z, c2x, c2y, c2z);
+      float* f = feats + 12 * (int64_t)idx;
       f[0] = d * 0.1f;
       f[1] = (d - rad1 - rad2) * (1.0f / 6.0f);
       f[2] = rad1 * 0.2f;
       f[3] = rad2 * 0.2f;
       f[4] = log2f((float)(b2 - b1)) * 0.1f;
-      f[5] = (daa - d) * 0.2f;
-      f[6] = (dac - d) * 0.2f;
-      f[7] = (dca - d) * 0.2f;
+      f[5] = (dist3(a1x, a1y, a1z, a2x, a2y, a2z) - d) * 0.2f;
+      f[6] = (dist3(a1x, a1y, a1z, c2x, c2y, c2z) - d) * 0.2f;
+      f[7] = (dist3(a2x, a2y, a2z, c1x, c1y, c1z) - d) * 0.2f;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const float* x1 = u1 + 4 * (q >> 1);
+        const float* x2 = u2 + 4 * (q & 1);
+        f[8 + q] = (dist3(x1[0], x1[1], x1[2], x2[0], x2[1], x2[2]) - x1[3] - x2[3]) * (1.0f / 6.0f);
+      }
       pair_row[idx] = row;
       pair_b2[idx] = b2;
       pair_bt[2 * idx] = bt1;
@@ -1227,6 +1278,7 @@ struct tmol_b200_ljlk_plan {
   std::vector<int> host_pose_last;
   const uint32_t* skip = nullptr;  // caller-owned screen mask, or null
   int skip_words = 0;
+  float* sub_spheres = nullptr;  // screen features: [P*B][2][4] (float plans)
 };
 
 namespace {
@@ -1258,7 +1310,7 @@ void free_plan(tmol_b200_ljlk_plan* pl) {
                   pl->bt_n_conn, pl->bt_is_ligand, pl->cp_count, pl->cp_b2,
                   pl->cp_minsep, pl->cp_seps,    pl->work,       pl->spheres,
                   pl->item_cost,
-                  pl->counters,  pl->counts};
+                  pl->counters,  pl->counts,     pl->sub_spheres};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t e : pl->prof_events) cudaEventDestroy(e);
@@ -1510,6 +1562,7 @@ int tmol_b200_ljlk_plan_create(const tmol_b200_ljlk_inputs* in, int real_bytes,
   PCK(dalloc(pl, &pl->cp_minsep, PB * CP_CAP));
   PCK(dalloc(pl, &pl->cp_seps, PB * CP_CAP * 16));
   PCK(dalloc(pl, (unsigned char**)&pl->spheres, PB * 4 * real_bytes));
+  if (real_bytes == 4) PCK(dalloc(pl, &pl->sub_spheres, PB * 8));
   PCK(dalloc(pl, &pl->counters, 4));
   PCK(dalloc(pl, &pl->counts, N_COUNTS));
 
@@ -1803,8 +1856,11 @@ int tmol_b200_ljlk_screen_candidates(tmol_b200_ljlk_plan* plan,
   const int grid = std::max(1, std::min((n_blocks + 7) / 8, plan->n_sm * 16));
   spheres_kernel<float><<<grid, threads, 0, st>>>(s);
   CK(cudaGetLastError());
-  screen_candidates_kernel<<<grid, threads, 0, st>>>(s, capacity, pair_row, pair_b2,
-                                                     pair_bt, features, count);
+  const int grid_u = std::max(1, std::min((n_blocks + threads - 1) / threads, plan->n_sm * 8));
+  sub_spheres_kernel<<<grid_u, threads, 0, st>>>(s, plan->sub_spheres);
+  CK(cudaGetLastError());
+  screen_candidates_kernel<<<grid, threads, 0, st>>>(s, plan->sub_spheres, capacity, pair_row,
+                                                     pair_b2, pair_bt, features, count);
   CK(cudaGetLastError());
   return TMOL_B200_OK;
 }

@@ -4,9 +4,9 @@
 //
 // The MLP predicts an upper quantile of log10(|E_atr| + |E_rep| + |E_lk|)
 // of a neighbouring block pair from block-pair features (sphere gap,
-// centroid distance, radii, sequence separation, first-atom distances and
-// learned block-type embeddings); block pairs predicted below a threshold
-// are skipped.  Intra-block pairs and pairs within count-pair reach (bond
+// centroid distance, radii, sequence separation, first-atom distances,
+// sub-sphere gaps and learned block-type embeddings); block pairs predicted
+// below a threshold are skipped.  Intra-block pairs and pairs within count-pair reach (bond
 // separation <= 4) are never candidates, so the screen never changes the
 // count-pair structure.
 //
@@ -35,7 +35,7 @@ namespace screen {
 
 constexpr int BM = 64, BN = 64, BK = 32;
 constexpr int PAD = 8;
-constexpr int F_IN = 32, HID = 128, EMB = 12, N_SCAL = 8;
+constexpr int F_IN = 32, HID = 128, EMB = 10, N_SCAL = 12;
 
 struct GemmArgs {
   const __nv_bfloat16* A;
@@ -199,8 +199,8 @@ __global__ void adam_kernel(float* w, const float* grad, float* m, float* v,
   }
 }
 
-// Rows of X [N, 32] (bf16): 8 scalar features, then the embeddings of the
-// two block types (12 values each).
+// Rows of X [N, 32] (bf16): 12 scalar features, then the embeddings of the
+// two block types (10 values each).
 __global__ void assemble_features_kernel(const float* scal, const int32_t* bt,
                                          const float* emb, int64_t n,
                                          __nv_bfloat16* X) {
@@ -331,29 +331,25 @@ __global__ void __launch_bounds__(INF_WARPS * 32) infer_kernel(InferArgs g) {
   const int gid = lane >> 2, tig = lane & 3;
   for (int t = blockIdx.x * INF_WARPS + warp; t < n_tiles; t += gridDim.x * INF_WARPS) {
     const int r0 = t * 16;
-    // stage 16 input rows: lane handles row lane & 15, half lane >> 4
+    // stage 16 input rows: lane handles row lane & 15, columns
+    // [16 * (lane >> 4), 16 * (lane >> 4) + 16)
     {
-      const int rr = lane & 15, half = lane >> 4;
+      const int rr = lane & 15, c0 = (lane >> 4) * 16;
       const int row = r0 + rr;
       __nv_bfloat16* xr = sm.x[warp][rr];
       if (row < n) {
-        if (half == 0) {
-          const float* f = g.feats + (int64_t)row * N_SCAL;
+        const float* f = g.feats + (int64_t)row * N_SCAL;
+        const float* e1 = g.w.emb + (int64_t)g.pair_bt[2 * row] * EMB;
+        const float* e2 = g.w.emb + (int64_t)g.pair_bt[2 * row + 1] * EMB;
 #pragma unroll
-          for (int c = 0; c < N_SCAL; ++c) xr[c] = __float2bfloat16(f[c]);
-          const float* e1 = g.w.emb + (int64_t)g.pair_bt[2 * row] * EMB;
-#pragma unroll
-          for (int c = 0; c < 8; ++c) xr[N_SCAL + c] = __float2bfloat16(e1[c]);
-        } else {
-          const float* e1 = g.w.emb + (int64_t)g.pair_bt[2 * row] * EMB;
-#pragma unroll
-          for (int c = 8; c < EMB; ++c) xr[N_SCAL + c] = __float2bfloat16(e1[c]);
-          const float* e2 = g.w.emb + (int64_t)g.pair_bt[2 * row + 1] * EMB;
-#pragma unroll
-          for (int c = 0; c < EMB; ++c) xr[N_SCAL + EMB + c] = __float2bfloat16(e2[c]);
+        for (int k = 0; k < 16; ++k) {
+          const int c = c0 + k;
+          const float v = c < N_SCAL ? f[c] : (c < N_SCAL + EMB ? e1[c - N_SCAL] : e2[c - N_SCAL - EMB]);
+          xr[c] = __float2bfloat16(v);
         }
       } else {
-        for (int c = half * 16; c < half * 16 + 16; ++c) xr[c] = __float2bfloat16(0.0f);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) xr[c0 + k] = __float2bfloat16(0.0f);
       }
     }
     __syncwarp();

@@ -271,7 +271,7 @@ class LJLKPlan:
         """Block pairs b1 < b2 that pass the sphere test and are not
         count-pair partners, with their screen features.  Returns a dict of
         device tensors: row [cap] (p * B + b1), b2 [cap], bt [cap, 2],
-        features [cap, 8] and count [1] (total candidates, may exceed cap)."""
+        features [cap, 12] and count [1] (total candidates, may exceed cap)."""
         self._check_coords(coords)
         if self.dtype != torch.float32:
             raise TypeError("screen candidates need a float32 plan")
@@ -282,7 +282,7 @@ class LJLKPlan:
                 row=torch.empty(capacity, dtype=torch.int32, device=dev),
                 b2=torch.empty(capacity, dtype=torch.int32, device=dev),
                 bt=torch.empty((capacity, 2), dtype=torch.int32, device=dev),
-                features=torch.empty((capacity, 8), dtype=torch.float32, device=dev),
+                features=torch.empty((capacity, 12), dtype=torch.float32, device=dev),
                 count=torch.empty(1, dtype=torch.int32, device=dev),
             )
         capacity = out["row"].shape[0]

@@ -3,8 +3,8 @@ activations, fp32 accumulation, trained with a pinball (quantile) loss and
 Adam.  Every step runs on the library's own kernels; torch only holds the
 buffers.
 
-Input row (32 values): the 8 candidate features of
-``tmol_b200_ljlk_screen_candidates`` followed by the 12-value embeddings of
+Input row (32 values): the 12 candidate features of
+``tmol_b200_ljlk_screen_candidates`` followed by the 10-value embeddings of
 the two block types.
 """
 
@@ -16,7 +16,7 @@ import torch
 
 from .. import native
 
-N_IN, HID, EMB, N_SCAL = 32, 128, 12, 8
+N_IN, HID, EMB, N_SCAL = 32, 128, 10, 12
 PARAM_NAMES = ("w1", "b1", "w2", "b2", "w3", "b3", "w4", "b4", "emb")
 BF16_COPIES = ("w1", "w2", "w3", "w4")
 

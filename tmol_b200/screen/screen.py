@@ -51,7 +51,7 @@ class BlockPairScreen:
             row=torch.empty(self.capacity, dtype=torch.int32, device=dev),
             b2=torch.empty(self.capacity, dtype=torch.int32, device=dev),
             bt=torch.empty((self.capacity, 2), dtype=torch.int32, device=dev),
-            features=torch.empty((self.capacity, 8), dtype=torch.float32, device=dev),
+            features=torch.empty((self.capacity, 12), dtype=torch.float32, device=dev),
             count=torch.zeros(1, dtype=torch.int32, device=dev),
         )
         self.pred = None
