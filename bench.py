@@ -391,6 +391,79 @@ def cpu_baseline_for(name, ps_sizes_seeds, full_atom_pairs):
     }
 
 
+def time_replays(fn, steps, flush):
+    """Milliseconds of `steps` replays of fn captured as a CUDA graph, L2
+    flushed before each replay (outside the events)."""
+    import torch
+
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        fn()
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        fn()
+    for _ in range(3):
+        g.replay()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for k in range(steps):
+        flush.zero_()
+        ev[k][0].record()
+        g.replay()
+        ev[k][1].record()
+    torch.cuda.synchronize()
+    del g
+    return sum(a.elapsed_time(b) for a, b in ev)
+
+
+def measure_screen(plan, plan64, coords, weights, step, flush, steps, names, plain_ms):
+    """The learned block-pair screen on the same batch: the time of a step
+    with the screen rebuilt inside it and with the mask reused, the skipped
+    fraction and the per-pose |dE| it introduces (float64 plan, same mask)."""
+    import torch
+
+    from tmol_b200.screen import BlockPairScreen
+
+    screen = BlockPairScreen.trained(plan, names)
+    screen.update(coords)
+    torch.cuda.synchronize()
+    n_cand = screen.n_candidates()
+    n_skip = screen.n_skipped()
+    c64 = coords.double()
+    w64 = weights.double()
+    plan64.set_skip_mask(None)
+    E0, _ = plan64.energy_and_gradient(c64, w64)
+    E0 = E0.clone()
+    plan64.set_skip_mask(screen.mask)
+    E1, _ = plan64.energy_and_gradient(c64, w64)
+    plan64.set_skip_mask(None)
+    dE = (E1 - E0).abs()
+    tot = ((E1 - E0) * w64).sum(0).abs()
+    screen.attach()
+
+    def screened_step():
+        screen.update(coords)
+        step()
+
+    with_update = time_replays(screened_step, steps, flush) / steps
+    reused = time_replays(step, steps, flush) / steps
+    screen.detach()
+    return {
+        "threshold": screen.threshold,
+        "candidates": n_cand,
+        "skipped_block_pairs": n_skip,
+        "skipped_fraction": n_skip / max(n_cand, 1),
+        "max_abs_dE_per_pose_f64": float(max(dE.max().item(), tot.max().item())),
+        "ms_per_step_with_screen_update": with_update,
+        "ms_per_step_mask_reused": reused,
+        "ms_per_step_plain": plain_ms,
+        "speedup_with_update": plain_ms / with_update,
+        "speedup_mask_reused": plain_ms / reused,
+    }
+
+
 def run_b200(args, world, rank, local):
     import torch
 
@@ -406,6 +479,8 @@ def run_b200(args, world, rank, local):
     static = [a.to(dev) if isinstance(a, torch.Tensor) else a for a in pose_score_args(ps, term)[:-1]]
     coords = ps.coords.flatten(0, 1).to(dev).contiguous()
     plan = LJLKPlan(coords, static)
+    plan64 = None if args.no_screen else LJLKPlan(coords.double(), static)
+    bt_names = [bt.name for bt in ps.packed_block_types.active_block_types]
     del static
     P = ps.n_poses
     n_residues = int((ps.block_type_ind >= 0).sum())
@@ -512,6 +587,13 @@ def run_b200(args, world, rank, local):
     h2d = coords.numel() * 4
     d2h = (3 * P + coords.numel()) * 4
 
+    screened = None
+    if not args.no_screen:
+        screened = measure_screen(
+            plan, plan64, coords, weights, step, flush, args.steps, bt_names, ms_max / args.steps
+        )
+        del plan64
+
     fp32_peak = native.measure_fp32_peak_tflops(torch.cuda.current_stream().cuda_stream)
     flops = flops_per_step(counts)
     achieved = flops / (kern_avg_ms * 1e-3) / 1e12
@@ -574,6 +656,7 @@ def run_b200(args, world, rank, local):
                 "d2h_bytes_per_step": d2h,
             },
             "cpu_baseline": cpu,
+            "screened": screened,
         }
         print(json.dumps(line), flush=True)
     del g
@@ -592,6 +675,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="uniform64x150", choices=["uniform64x150", "uneven256"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-screen", action="store_true", help="skip the learned-screen measurement")
     ap.add_argument(
         "--launch",
         default="",

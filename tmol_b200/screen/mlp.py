@@ -73,6 +73,20 @@ class ScreenMLP:
             self.params[k].copy_(v.to(self.device))
         self.refresh_bf16()
 
+    @classmethod
+    def load(cls, path, device, block_type_names=None):
+        """A trained network from ``path`` (written by
+        ``tmol_b200.screen.train``) and its calibrated skip threshold.  With
+        ``block_type_names``, checks that the embedding rows follow the same
+        block-type order."""
+        st = dict(numpy.load(path, allow_pickle=False))
+        names = [str(v) for v in st["block_type_names"]]
+        if block_type_names is not None and list(block_type_names) != names:
+            raise ValueError("the screen's block-type order differs from the packed block types")
+        net = cls(len(names), device)
+        net.load_state_dict(st)
+        return net, float(st["threshold"])
+
     def weights_struct(self):
         w = native.ScreenWeights()
         for k in BF16_COPIES:

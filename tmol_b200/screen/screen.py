@@ -1,8 +1,14 @@
 """Candidate enumeration, labels and the skip-mask driver of the screen."""
 
+import os
+
 import torch
 
 from .mlp import ScreenMLP
+
+# the network trained by ``python -m tmol_b200.screen.train`` (2000 synthetic
+# poses, 14.1M labelled block pairs), with its calibrated threshold
+TRAINED_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "screen_weights.npz")
 
 # label: log10 of the pair's summed energy magnitude, floored at 1e-6
 LABEL_FLOOR = 1e-6
@@ -36,6 +42,12 @@ class BlockPairScreen:
     scoring call); ``attach()`` makes the plan's scoring calls honour the
     mask, ``detach()`` restores plain scoring.  Candidates beyond
     ``capacity`` are never skipped."""
+
+    @classmethod
+    def trained(cls, plan, block_type_names=None, capacity=None, path=TRAINED_WEIGHTS):
+        """The screen with the trained network shipped in the package."""
+        mlp, threshold = ScreenMLP.load(path, plan.device, block_type_names)
+        return cls(mlp, plan, threshold, capacity)
 
     def __init__(self, mlp: ScreenMLP, plan, threshold, capacity=None):
         self.mlp = mlp

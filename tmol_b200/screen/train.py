@@ -45,7 +45,6 @@ from .mlp import ScreenMLP
 from .screen import BlockPairScreen, block_pair_labels
 
 BETA2016 = (1.0, 0.55, 1.0)
-WEIGHTS_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "screen_weights.npz")
 
 
 def _host_chunk(job):
@@ -324,7 +323,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--out", required=True)
     ap.add_argument("--train-poses", type=int, default=2000)
-    ap.add_argument("--val-poses", type=int, default=16)
+    ap.add_argument("--val-poses", type=int, default=48)
     ap.add_argument("--val-residues", type=int, default=1000)
     ap.add_argument("--test-poses", type=int, default=16)
     ap.add_argument("--test-residues", type=int, default=1000)
