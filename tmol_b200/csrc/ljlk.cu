@@ -892,17 +892,11 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
       const Real reach1 = rad1 + reach_atoms;
       const Real reach1_2 = reach1 * reach1 * Real(1.0001);
 
-      // the row's count-pair partners, one per lane
-      RowPartners rp;
-      const int ncp = s.cp_count[r.i1];
-      {
-        rp.b2 = -1;
-        rp.minsep = 6;
-        rp.entry = r.i1 * CP_CAP + lane;
-        if (lane < ncp) {
-          rp.b2 = s.cp_b2[rp.entry];
-          rp.minsep = s.cp_minsep[rp.entry];
-        }
+      // with a skip mask: the row's count-pair partners, which it never skips
+      int skip_ncp = 0, skip_cp = -1;
+      if (s.skip) {
+        skip_ncp = s.cp_count[r.i1];
+        if (lane < skip_ncp) skip_cp = s.cp_b2[r.i1 * CP_CAP + lane];
       }
 
       // neighbour tests of the whole range first: one ballot mask per 32
@@ -930,8 +924,8 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
           // b1's count-pair partners (bond separation <= 4)
           bool drop = hit && b2 != r.b1 &&
                       ((s.skip[(int64_t)r.i1 * s.skip_words + (b2 >> 5)] >> (b2 & 31)) & 1u);
-          for (int k = 0; k < ncp; ++k)
-            if (__shfl_sync(0xffffffffu, rp.b2, k) == b2) drop = false;
+          for (int k = 0; k < skip_ncp; ++k)
+            if (__shfl_sync(0xffffffffu, skip_cp, k) == b2) drop = false;
           if (drop) hit = false;
         }
         unsigned mk = __ballot_sync(0xffffffffu, hit);
@@ -944,6 +938,18 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
         continue;
       }
 
+      // the row's count-pair partners, one per lane
+      RowPartners rp;
+      {
+        int ncp = s.cp_count[r.i1];
+        rp.b2 = -1;
+        rp.minsep = 6;
+        rp.entry = r.i1 * CP_CAP + lane;
+        if (lane < ncp) {
+          rp.b2 = s.cp_b2[rp.entry];
+          rp.minsep = s.cp_minsep[rp.entry];
+        }
+      }
       int nt1 = (r.n1 + TILE - 1) / TILE;
       for (int ti = 0; ti < nt1; ++ti) {
         r.st1 = ti * TILE;
