@@ -378,8 +378,11 @@ __global__ void spheres_kernel(ScoreArgs<Real> s) {
 // one screening pass covers several block pairs with every lane busy.  The
 // pair queue collects the atom pairs that contribute (inside max_dis with a
 // non-zero count-pair weight): LJ-only pairs from the front, heavy-atom
-// (LJ + LK) pairs from the back.  An entry packs a1 (5 bits) | j (6 bits) |
-// count-pair-weight-0.2 flag (bit 11) | j-on-side-0 flag (bit 12).
+// (LJ + LK) pairs from the back.  Both sides live in one atom array (side 0
+// at [0, TILE), side 1 at [TILE, TILE + M1)), each atom one 16-byte record
+// (x, y, z, type) so that a pair costs two vector loads; an entry packs
+// a1 (5 bits) | j in the atom array (7 bits) | count-pair-weight-0.2 flag
+// (bit 12).
 
 constexpr int M1 = 64;
 constexpr int MAX_SLOTS = 8;
@@ -392,17 +395,23 @@ enum SlotKind : int {
   kSlotIntra = 2,     // another tile of block b1: intra-block separation table
 };
 
+// One staged atom: coordinates and per block-type atom flags (compact atom
+// type | heavy << 8).
+template <typename Real>
+struct alignas(16) AtomRec {
+  Real x, y, z;
+  int tf;
+};
+
+constexpr int N_ATOMS = TILE + M1;
+
 template <typename Real>
 struct Slab {
-  Real x0[TILE], y0[TILE], z0[TILE];
-  Real gx0[TILE], gy0[TILE], gz0[TILE];
+  AtomRec<Real> at[N_ATOMS];            // side 0, then side 1
+  Real gx[N_ATOMS], gy[N_ATOMS], gz[N_ATOMS];  // gradient accumulators
   uint32_t cpd0[TILE];  // bond separation to each connection atom, a byte each
-  uint16_t tf0[TILE];
-  Real x1[M1], y1[M1], z1[M1];
-  Real gx1[M1], gy1[M1], gz1[M1];
   uint32_t cpd1[M1];
   int gidx1[M1];  // global atom index
-  uint16_t tf1[M1];
   uint8_t slot1[M1];   // slot of the packed atom
   uint8_t local1[M1];  // atom index within its block
   uint8_t seps[MAX_SLOTS][16];
@@ -451,14 +460,16 @@ __device__ __forceinline__ void stage_side0(const ScoreArgs<Real>& s,
   if (lane < cnt) {
     int at = start + lane;
     const Real* c = s.coords + 3 * ((int64_t)off + at);
-    w.x0[lane] = c[0];
-    w.y0[lane] = c[1];
-    w.z0[lane] = c[2];
-    w.tf0[lane] = s.bt_tf[(int64_t)bt * s.A + at];
+    AtomRec<Real> a;
+    a.x = c[0];
+    a.y = c[1];
+    a.z = c[2];
+    a.tf = s.bt_tf[(int64_t)bt * s.A + at];
+    w.at[lane] = a;
     w.cpd0[lane] = load_cpd(s, bt, nconn, at);
-    w.gx0[lane] = 0;
-    w.gy0[lane] = 0;
-    w.gz0[lane] = 0;
+    w.gx[lane] = 0;
+    w.gy[lane] = 0;
+    w.gz[lane] = 0;
   }
 }
 
@@ -487,17 +498,19 @@ __device__ __forceinline__ int stage_side1(const ScoreArgs<Real>& s,
   unsigned km = __ballot_sync(0xffffffffu, keep);
   if (keep) {
     int j = j0 + __popc(km & ((1u << lane) - 1));
-    w.x1[j] = x;
-    w.y1[j] = y;
-    w.z1[j] = z;
-    w.tf1[j] = s.bt_tf[(int64_t)bt * s.A + at];
+    AtomRec<Real> a;
+    a.x = x;
+    a.y = y;
+    a.z = z;
+    a.tf = s.bt_tf[(int64_t)bt * s.A + at];
+    w.at[TILE + j] = a;
     w.cpd1[j] = load_cpd(s, bt, nconn, at);
     w.gidx1[j] = off + at;
     w.slot1[j] = (uint8_t)slot;
     w.local1[j] = (uint8_t)at;
-    w.gx1[j] = 0;
-    w.gy1[j] = 0;
-    w.gz1[j] = 0;
+    w.gx[TILE + j] = 0;
+    w.gy[TILE + j] = 0;
+    w.gz[TILE + j] = 0;
   }
   return __popc(km);
 }
@@ -508,7 +521,7 @@ __device__ __forceinline__ void flush_side0(const ScoreArgs<Real>& s,
                                             int cnt, int lane) {
   if (lane < cnt) {
     Real* d = s.dcoords + 3 * ((int64_t)off + start + lane);
-    Real gx = w.gx0[lane], gy = w.gy0[lane], gz = w.gz0[lane];
+    Real gx = w.gx[lane], gy = w.gy[lane], gz = w.gz[lane];
     if (gx != 0) atomicAdd(d + 0, gx);
     if (gy != 0) atomicAdd(d + 1, gy);
     if (gz != 0) atomicAdd(d + 2, gz);
@@ -520,7 +533,7 @@ __device__ __forceinline__ void flush_side1(const ScoreArgs<Real>& s,
                                             Slab<Real>& w, int m, int lane) {
   for (int j = lane; j < m; j += 32) {
     Real* d = s.dcoords + 3 * (int64_t)w.gidx1[j];
-    Real gx = w.gx1[j], gy = w.gy1[j], gz = w.gz1[j];
+    Real gx = w.gx[TILE + j], gy = w.gy[TILE + j], gz = w.gz[TILE + j];
     if (gx != 0) atomicAdd(d + 0, gx);
     if (gy != 0) atomicAdd(d + 1, gy);
     if (gz != 0) atomicAdd(d + 2, gz);
@@ -562,19 +575,16 @@ __device__ __noinline__ E3<Real> eval_queue(EvalCtx<Real> c, Slab<Real>* wp,
     int i = base + lane;
     bool act = i < n;
     int e = act ? (int)w.queue[HEAVY ? QCAP - 1 - i : i] : 0;
-    int a1 = e & 31, j = (e >> 5) & 63;
-    bool to0 = (e >> 12) & 1;
-    Real wcp = (e >> 11) & 1 ? Real(0.2) : Real(1);
+    int a1 = e & 31, j = (e >> 5) & 127;
+    Real wcp = (e >> 12) & 1 ? Real(0.2) : Real(1);
     Real fx = 0, fy = 0, fz = 0;
     if (act) {
-      Real x2 = to0 ? w.x0[j] : w.x1[j];
-      Real y2 = to0 ? w.y0[j] : w.y1[j];
-      Real z2 = to0 ? w.z0[j] : w.z1[j];
-      int t2 = (to0 ? w.tf0[j] : w.tf1[j]) & 0xff;
-      int t1 = w.tf0[a1] & 0xff;
-      Real dx = w.x0[a1] - x2;
-      Real dy = w.y0[a1] - y2;
-      Real dz = w.z0[a1] - z2;
+      const AtomRec<Real> p1 = w.at[a1];
+      const AtomRec<Real> p2 = w.at[j];
+      int t1 = p1.tf & 0xff, t2 = p2.tf & 0xff;
+      Real dx = p1.x - p2.x;
+      Real dy = p1.y - p2.y;
+      Real dz = p1.z - p2.z;
       Real d = sqrt(dx * dx + dy * dy + dz * dz);
       int tp = t1 * c.ntp + t2;
       LJRecord<Real> lr = c.ljtab[tp];
@@ -620,17 +630,14 @@ __device__ __noinline__ E3<Real> eval_queue(EvalCtx<Real> c, Slab<Real>* wp,
         }
       }
       if (act && head && (sx != 0 || sy != 0 || sz != 0)) {
-        atomicAdd(&w.gx0[a1], sx);
-        atomicAdd(&w.gy0[a1], sy);
-        atomicAdd(&w.gz0[a1], sz);
+        atomicAdd(&w.gx[a1], sx);
+        atomicAdd(&w.gy[a1], sy);
+        atomicAdd(&w.gz[a1], sz);
       }
       if (act && (fx != 0 || fy != 0 || fz != 0)) {
-        Real* gx = to0 ? w.gx0 : w.gx1;
-        Real* gy = to0 ? w.gy0 : w.gy1;
-        Real* gz = to0 ? w.gz0 : w.gz1;
-        atomicAdd(&gx[j], -fx);
-        atomicAdd(&gy[j], -fy);
-        atomicAdd(&gz[j], -fz);
+        atomicAdd(&w.gx[j], -fx);
+        atomicAdd(&w.gy[j], -fy);
+        atomicAdd(&w.gz[j], -fz);
       }
     }
   }
@@ -690,18 +697,19 @@ __device__ __noinline__ E3<Real> intra_tile(EvalCtx<Real> c, Slab<Real>* wp,
     bool in = false, hv = false;
     int wbit = 0;
     if (base + lane < npairs && a1 < a2) {
-      Real dx = w.x0[a1] - w.x0[a2];
-      Real dy = w.y0[a1] - w.y0[a2];
-      Real dz = w.z0[a1] - w.z0[a2];
+      const AtomRec<Real> p1 = w.at[a1], p2 = w.at[a2];
+      Real dx = p1.x - p2.x;
+      Real dy = p1.y - p2.y;
+      Real dz = p1.z - p2.z;
       Real d2 = dx * dx + dy * dy + dz * dz;
       if (d2 < maxd2) {
         int sep = c.pd[a1 * c.A + st1 + a2];
         in = sep >= 4;
         wbit = sep == 4;
-        hv = in && (w.tf0[a1] & w.tf0[a2] & kTfHeavy);
+        hv = in && (p1.tf & p2.tf & kTfHeavy);
       }
     }
-    queue_push(w.queue, in, hv, a1 | (a2 << 5) | (wbit << 11) | (1 << 12), lane, nl, nh);
+    queue_push(w.queue, in, hv, a1 | (a2 << 5) | (wbit << 12), lane, nl, nh);
     a1 += qq;
     a2 += rr;
     if (a2 >= c1) {
@@ -727,10 +735,11 @@ __device__ __noinline__ E3<Real> screen_slots(EvalCtx<Real> c, Slab<Real>* wp,
   const Real maxd2 = c.max_dis * c.max_dis;
   bool act0 = false;
   if (lane < c1) {
+    const AtomRec<Real> p0 = w.at[lane];
     for (int k = 0; k < ns; ++k) {
-      Real dx = w.x0[lane] - w.slot_sph[k][0];
-      Real dy = w.y0[lane] - w.slot_sph[k][1];
-      Real dz = w.z0[lane] - w.slot_sph[k][2];
+      Real dx = p0.x - w.slot_sph[k][0];
+      Real dy = p0.y - w.slot_sph[k][1];
+      Real dz = p0.z - w.slot_sph[k][2];
       Real rr = w.slot_sph[k][3] + c.max_dis;
       act0 |= dx * dx + dy * dy + dz * dz < rr * rr * Real(1.0001);
     }
@@ -741,8 +750,9 @@ __device__ __noinline__ E3<Real> screen_slots(EvalCtx<Real> c, Slab<Real>* wp,
     int j = cbase + lane;
     bool valid = j < m;
     int jj = valid ? j : 0;
-    Real xj = w.x1[jj], yj = w.y1[jj], zj = w.z1[jj];
-    int heavy_j = valid ? (w.tf1[jj] & kTfHeavy) : 0;
+    const AtomRec<Real> pj = w.at[TILE + jj];
+    const Real xj = pj.x, yj = pj.y, zj = pj.z;
+    int heavy_j = valid ? (pj.tf & kTfHeavy) : 0;
     int slot = w.slot1[jj];
     int kind = w.slot_kind[slot];
     int nc2 = w.slot_nc[slot];
@@ -752,9 +762,10 @@ __device__ __noinline__ E3<Real> screen_slots(EvalCtx<Real> c, Slab<Real>* wp,
     const uint8_t* pd = c.pd + w.local1[jj];
     for (unsigned rm = rows; rm; rm &= rm - 1) {
       int a1 = __ffs(rm) - 1;
-      Real dx = w.x0[a1] - xj;
-      Real dy = w.y0[a1] - yj;
-      Real dz = w.z0[a1] - zj;
+      const AtomRec<Real> pa = w.at[a1];
+      Real dx = pa.x - xj;
+      Real dy = pa.y - yj;
+      Real dz = pa.z - zj;
       Real d2 = dx * dx + dy * dy + dz * dz;
       bool in = false, hv = false;
       int wbit = 0;
@@ -778,9 +789,9 @@ __device__ __noinline__ E3<Real> screen_slots(EvalCtx<Real> c, Slab<Real>* wp,
         if (lig && (sep == 3 || sep == 4)) sep = 5;
         in = sep >= 4;
         wbit = sep == 4;
-        hv = in && (heavy_j & w.tf0[a1]);
+        hv = in && (heavy_j & pa.tf);
       }
-      queue_push(w.queue, in, hv, a1 | (j << 5) | (wbit << 11), lane, nl, nh);
+      queue_push(w.queue, in, hv, a1 | ((TILE + j) << 5) | (wbit << 12), lane, nl, nh);
       if (nl + nh > QCAP - 32) drain_queue<Real, GRAD>(c, wp, nl, nh, lane, acc);
     }
   }
@@ -957,7 +968,7 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
         stage_side0(s, w, r.bt1, r.off1, r.st1, r.c1, r.nc1, lane);
         ec.pd = s.bt_pd + ((int64_t)r.bt1 * s.A + r.st1) * s.A;
         __syncwarp();
-        int h1 = __popc(__ballot_sync(0xffffffffu, lane < r.c1 && (w.tf0[lane] & kTfHeavy)));
+        int h1 = __popc(__ballot_sync(0xffffffffu, lane < r.c1 && (w.at[lane].tf & kTfHeavy)));
         int m = 0, ns = 0;
         int64_t pair_o = 0;
         for (int bi = 0; bi < n_batches; ++bi) {
