@@ -629,16 +629,37 @@ __device__ __noinline__ E3<Real> eval_queue(EvalCtx<Real> c, Slab<Real>* wp,
           sz += tz;
         }
       }
-      if (act && head && (sx != 0 || sy != 0 || sz != 0)) {
-        atomicAdd(&w.gx[a1], sx);
-        atomicAdd(&w.gy[a1], sy);
-        atomicAdd(&w.gz[a1], sz);
+      // segment heads and j targets: a lane whose address no other lane of
+      // this step touches adds without an atomic; lanes sharing an address
+      // (a1 recurring in two segments, j in two rows' entries) use atomics
+      const bool add0 = act && head;
+      const unsigned me = 1u << lane;
+      const unsigned p0 = __match_any_sync(0xffffffffu, add0 ? a1 : -1 - lane);
+      const unsigned p1 = __match_any_sync(0xffffffffu, act ? j : -1 - lane);
+      if (add0) {
+        if (p0 == me) {
+          w.gx[a1] += sx;
+          w.gy[a1] += sy;
+          w.gz[a1] += sz;
+        } else {
+          atomicAdd(&w.gx[a1], sx);
+          atomicAdd(&w.gy[a1], sy);
+          atomicAdd(&w.gz[a1], sz);
+        }
       }
-      if (act && (fx != 0 || fy != 0 || fz != 0)) {
-        atomicAdd(&w.gx[j], -fx);
-        atomicAdd(&w.gy[j], -fy);
-        atomicAdd(&w.gz[j], -fz);
+      __syncwarp();
+      if (act) {
+        if (p1 == me) {
+          w.gx[j] -= fx;
+          w.gy[j] -= fy;
+          w.gz[j] -= fz;
+        } else {
+          atomicAdd(&w.gx[j], -fx);
+          atomicAdd(&w.gy[j], -fy);
+          atomicAdd(&w.gz[j], -fz);
+        }
       }
+      __syncwarp();  // the next step's adds may touch the same atoms
     }
   }
   return acc;
@@ -747,50 +768,72 @@ __device__ __noinline__ E3<Real> screen_slots(EvalCtx<Real> c, Slab<Real>* wp,
   const unsigned rows = __ballot_sync(0xffffffffu, act0);
   int nl = 0, nh = 0;
   for (int cbase = 0; cbase < m; cbase += 32) {
-    int j = cbase + lane;
-    bool valid = j < m;
-    int jj = valid ? j : 0;
+    const int j = cbase + lane;
+    const bool valid = j < m;
+    const int jj = valid ? j : 0;
     const AtomRec<Real> pj = w.at[TILE + jj];
     const Real xj = pj.x, yj = pj.y, zj = pj.z;
-    int heavy_j = valid ? (pj.tf & kTfHeavy) : 0;
-    int slot = w.slot1[jj];
-    int kind = w.slot_kind[slot];
-    int nc2 = w.slot_nc[slot];
-    bool lig = w.slot_lig[slot];
-    uint32_t cpdj = w.cpd1[jj];
-    const uint8_t* seps = w.seps[slot];
-    const uint8_t* pd = c.pd + w.local1[jj];
-    for (unsigned rm = rows; rm; rm &= rm - 1) {
-      int a1 = __ffs(rm) - 1;
-      const AtomRec<Real> pa = w.at[a1];
-      Real dx = pa.x - xj;
-      Real dy = pa.y - yj;
-      Real dz = pa.z - zj;
-      Real d2 = dx * dx + dy * dy + dz * dz;
-      bool in = false, hv = false;
-      int wbit = 0;
-      if (valid && d2 < maxd2) {
-        int sep;
-        if (kind == kSlotFar) {
-          sep = 6;
-        } else if (kind == kSlotStriking) {
-          sep = 5;
-          uint32_t c0 = w.cpd0[a1];
-          for (int u = 0; u < nc1; ++u) {
-            int pd1 = (c0 >> (8 * u)) & 0xff;
+    const int heavy_j = valid ? (pj.tf & kTfHeavy) : 0;
+    const int slot = w.slot1[jj];
+    const int kind = w.slot_kind[slot];
+    // count-pair classes of this lane's pairs with the active rows, once per
+    // chunk: excl (separation < 4, weight 0) and w02 (separation 4, 0.2)
+    unsigned excl = 0, w02 = 0;
+    if (valid && kind != kSlotFar) {
+      const bool lig = w.slot_lig[slot];
+      if (kind == kSlotStriking) {
+        // separation through the connections: min over (u, v) of
+        // pd1[a1][u] + seps[u][v] + pd2[j][v], capped at 5; the minimum
+        // over v depends on this lane only
+        const int nc2 = w.slot_nc[slot];
+        const uint32_t cpdj = w.cpd1[jj];
+        const uint8_t* seps = w.seps[slot];
+        int best[MAX_CONN];
+#pragma unroll
+        for (int u = 0; u < MAX_CONN; ++u) {
+          best[u] = 255;
+          if (u < nc1)
             for (int v = 0; v < nc2; ++v) {
-              int t = pd1 + seps[u * 4 + v] + ((cpdj >> (8 * v)) & 0xff);
-              sep = t < sep ? t : sep;
+              const int t = seps[u * 4 + v] + ((cpdj >> (8 * v)) & 0xff);
+              best[u] = t < best[u] ? t : best[u];
             }
-          }
-        } else {
-          sep = pd[a1 * c.A];
         }
-        if (lig && (sep == 3 || sep == 4)) sep = 5;
-        in = sep >= 4;
-        wbit = sep == 4;
-        hv = in && (heavy_j & pa.tf);
+        for (unsigned rm = rows; rm; rm &= rm - 1) {
+          const int a1 = __ffs(rm) - 1;
+          const uint32_t c0 = w.cpd0[a1];
+          int sep = 5;
+#pragma unroll
+          for (int u = 0; u < MAX_CONN; ++u) {
+            const int t = (int)((c0 >> (8 * u)) & 0xff) + best[u];
+            sep = t < sep ? t : sep;
+          }
+          if (lig && (sep == 3 || sep == 4)) sep = 5;
+          excl |= (unsigned)(sep < 4) << a1;
+          w02 |= (unsigned)(sep == 4) << a1;
+        }
+      } else {
+        // another tile of block b1: the intra-block separation table
+        const uint8_t* pd = c.pd + w.local1[jj];
+        for (unsigned rm = rows; rm; rm &= rm - 1) {
+          const int a1 = __ffs(rm) - 1;
+          int sep = pd[a1 * c.A];
+          if (lig && (sep == 3 || sep == 4)) sep = 5;
+          excl |= (unsigned)(sep < 4) << a1;
+          w02 |= (unsigned)(sep == 4) << a1;
+        }
       }
+    }
+    const unsigned live = valid ? rows & ~excl : 0u;
+    for (unsigned rm = rows; rm; rm &= rm - 1) {
+      const int a1 = __ffs(rm) - 1;
+      const AtomRec<Real> pa = w.at[a1];
+      const Real dx = pa.x - xj;
+      const Real dy = pa.y - yj;
+      const Real dz = pa.z - zj;
+      const Real d2 = dx * dx + dy * dy + dz * dz;
+      const bool in = ((live >> a1) & 1u) && d2 < maxd2;
+      const bool hv = in && (heavy_j & pa.tf);
+      const int wbit = (w02 >> a1) & 1u;
       queue_push(w.queue, in, hv, a1 | ((TILE + j) << 5) | (wbit << 12), lane, nl, nh);
       if (nl + nh > QCAP - 32) drain_queue<Real, GRAD>(c, wp, nl, nh, lane, acc);
     }
