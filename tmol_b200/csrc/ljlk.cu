@@ -66,6 +66,11 @@ __device__ __forceinline__ float sqrt_rn(float a) { return __fsqrt_rn(a); }
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
+// 1 / sqrt(x) (x > 0): the hardware estimate in fp32, correctly rounded
+// operations in fp64
+__device__ __forceinline__ float inv_sqrt(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double inv_sqrt(double x) { return 1.0 / sqrt(x); }
 __device__ __forceinline__ double div_rn(double a, double b) { return __ddiv_rn(a, b); }
 __device__ __forceinline__ double sqrt_rn(double a) { return __dsqrt_rn(a); }
 
@@ -585,23 +590,27 @@ __device__ __noinline__ E3<Real> eval_queue(EvalCtx<Real> c, Slab<Real>* wp,
       Real dx = p1.x - p2.x;
       Real dy = p1.y - p2.y;
       Real dz = p1.z - p2.z;
-      Real d = sqrt(dx * dx + dy * dy + dz * dz);
+      const Real d2 = dx * dx + dy * dy + dz * dz;
+      // coincident atoms (d2 = 0) take the linear LJ and flat LK regions,
+      // which never use inv_d, and add no force
+      const Real inv_d = inv_sqrt(d2);
+      const Real d = d2 > Real(0) ? d2 * inv_d : Real(0);
       int tp = t1 * c.ntp + t2;
       LJRecord<Real> lr = c.ljtab[tp];
       Real atr, rep, datr, drep;
-      lj_eval<Real, GRAD>(d, lr, dmax, atr, rep, datr, drep);
+      lj_eval<Real, GRAD>(d, inv_d, lr, dmax, atr, rep, datr, drep);
       acc.atr += wcp * atr;
       acc.rep += wcp * rep;
       Real dE = c.wt0 * datr + c.wt1 * drep;
       if (HEAVY) {
         LKRecord<Real> kr = c.lktab[tp];
         Real lk, dlk;
-        lk_eval<Real, GRAD>(d, kr, far_dmin, dmax, lk, dlk);
+        lk_eval<Real, GRAD>(d, inv_d, kr, far_dmin, dmax, lk, dlk);
         acc.lk += wcp * lk;
         dE += c.wt2 * dlk;
       }
       if (GRAD && d != Real(0)) {
-        Real f = wcp * dE / d;
+        Real f = wcp * dE * inv_d;
         fx = f * dx;
         fy = f * dy;
         fz = f * dz;

@@ -399,9 +399,10 @@ __device__ __forceinline__ void build_records(const AtomParams<Real>& i,
   lk.pad0 = lk.pad1 = lk.pad2 = Real(0);
 }
 
-// Unweighted LJ (atr, rep) and, with DERIV, their distance derivatives.
+// Unweighted LJ (atr, rep) and, with DERIV, their distance derivatives;
+// inv = 1 / d.
 template <typename Real, bool DERIV>
-__device__ __forceinline__ void lj_eval(Real d, const LJRecord<Real>& r,
+__device__ __forceinline__ void lj_eval(Real d, Real inv, const LJRecord<Real>& r,
                                         Real dmax, Real& atr, Real& rep,
                                         Real& datr, Real& drep) {
   Real lj, dlj = 0;
@@ -409,7 +410,6 @@ __device__ __forceinline__ void lj_eval(Real d, const LJRecord<Real>& r,
     lj = r.lin_V + r.lin_dV * (d - r.d_lin);
     dlj = r.lin_dV;
   } else if (d < r.dmin) {
-    Real inv = Real(1) / d;
     Real sd = r.sigma * inv;
     Real sd2 = sd * sd;
     Real sd6 = sd2 * sd2 * sd2;
@@ -436,9 +436,10 @@ __device__ __forceinline__ void lj_eval(Real d, const LJRecord<Real>& r,
   }
 }
 
-// Unweighted LK (both directions) and, with DERIV, its distance derivative.
+// Unweighted LK (both directions) and, with DERIV, its distance
+// derivative; inv_d = 1 / d.
 template <typename Real, bool DERIV>
-__device__ __forceinline__ void lk_eval(Real d, const LKRecord<Real>& r,
+__device__ __forceinline__ void lk_eval(Real d, Real inv_d, const LKRecord<Real>& r,
                                         Real far_dmin, Real far_dmax, Real& V,
                                         Real& dV) {
   dV = 0;
@@ -451,13 +452,12 @@ __device__ __forceinline__ void lk_eval(Real d, const LKRecord<Real>& r,
     V = p0 + t * (t * (-dp1 - 3 * p0 + 3 * p1 + t * (dp1 + 2 * p0 - 2 * p1)));
     if (DERIV) dV = (t * (-2 * dp1 - 6 * p0 + 6 * p1 + t * (3 * dp1 + 6 * p0 - 6 * p1))) / h;
   } else if (d < far_dmin) {
-    Real inv_d2 = Real(1) / (d * d);
+    Real inv_d2 = inv_d * inv_d;
     Real xi = d - r.r_i, xj = d - r.r_j;
     Real ei = r.c_i * exp(-xi * xi * r.il2_i);
     Real ej = r.c_j * exp(-xj * xj * r.il2_j);
     V = (ei + ej) * inv_d2;
     if (DERIV) {
-      Real inv_d = Real(1) / d;
       dV = inv_d2 * (ei * (Real(-2) * inv_d - Real(2) * xi * r.il2_i) +
                      ej * (Real(-2) * inv_d - Real(2) * xj * r.il2_j));
     }
