@@ -420,6 +420,7 @@ typedef struct {
   const real* global_params;            /* [5] */
   real max_dis;
   int n_atoms, n_rots, P, B, nbt, A, C, ntiles, T;
+  const int32_t* n_rots_for_block;      /* [P][B] (rotamer scoring) */
 } oracle_inputs_t;
 
 typedef struct {
@@ -717,14 +718,16 @@ static void detect_neighbors(const oracle_inputs_t* in, const real* spheres,
       }
 }
 
-static int setup_pair(const oracle_inputs_t* in, int p, int b1, int b2,
-                      pair_ctx_t* c) {
+/* Context of one evaluation: rotamer rot1 of block b1 against rotamer rot2
+ * of block b2 of pose p (b1 == b2 means rot1 == rot2, intra-block). */
+static int setup_rot_pair(const oracle_inputs_t* in, int p, int b1, int b2,
+                          int rot1, int rot2, pair_ctx_t* c) {
   int B = in->B;
   c->pose = p;
   c->b1 = b1;
   c->b2 = b2;
-  c->rot1 = in->rot_offset_for_block[p * B + b1];
-  c->rot2 = in->rot_offset_for_block[p * B + b2];
+  c->rot1 = rot1;
+  c->rot2 = rot2;
   if (c->rot1 < 0 || c->rot2 < 0) return 0;
   c->bt1 = in->block_type_ind_for_rot[c->rot1];
   c->bt2 = in->block_type_ind_for_rot[c->rot2];
@@ -750,6 +753,14 @@ static int setup_pair(const oracle_inputs_t* in, int p, int b1, int b2,
                 [((((size_t)p * B + b1) * B + b2) * in->C + k1) * in->C + k2];
   }
   return 1;
+}
+
+/* The pose op: each block's first (only) rotamer. */
+static int setup_pair(const oracle_inputs_t* in, int p, int b1, int b2,
+                      pair_ctx_t* c) {
+  int B = in->B;
+  return setup_rot_pair(in, p, b1, b2, in->rot_offset_for_block[p * B + b1],
+                        in->rot_offset_for_block[p * B + b2], c);
 }
 
 /*
@@ -853,3 +864,189 @@ void oracle_count_pairs(const oracle_inputs_t* in, const int32_t* nbr,
 }
 
 int oracle_sizeof_real(void) { return (int)sizeof(real); }
+
+/* ---------------------------------------------------------------------- */
+/* Rotamer scoring (ljlk_pose_score.impl.hh:1479-2126).                    */
+
+/* compute_rot_spheres (sphere_overlap.impl.hh:23-107) with the CPU launch
+ * box (one thread): per rotamer, centroid of its atoms in order and the
+ * largest centroid distance. */
+static void rot_spheres(const oracle_inputs_t* in, real* rs) {
+  for (int r = 0; r < in->n_rots; ++r) {
+    real* s = rs + 4 * (size_t)r;
+    s[0] = s[1] = s[2] = s[3] = 0;
+    int bt = in->block_type_ind_for_rot[r];
+    if (bt < 0) continue;
+    int off = in->rot_coord_offset[r];
+    int n = in->bt_n_atoms[bt];
+    real c[3] = {0, 0, 0};
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k < 3; ++k) c[k] += in->coords[3 * (size_t)(off + i) + k];
+    for (int k = 0; k < 3; ++k) c[k] /= n;
+    real d2max = 0;
+    for (int i = 0; i < n; ++i) {
+      const real* x = in->coords + 3 * (size_t)(off + i);
+      real d2 = ((x[0] - c[0]) * (x[0] - c[0]) + (x[1] - c[1]) * (x[1] - c[1]) +
+                 (x[2] - c[2]) * (x[2] - c[2]));
+      if (d2 > d2max) d2max = d2;
+    }
+    s[0] = c[0];
+    s[1] = c[1];
+    s[2] = c[2];
+    s[3] = rsqrt_(d2max);
+  }
+}
+
+/* compute_block_spheres_from_rot_spheres (sphere_overlap.impl.hh:455-510):
+ * the mean of the block's rotamer centres and the largest centre distance
+ * plus rotamer radius. */
+static void block_spheres_from_rots(const oracle_inputs_t* in, const real* rs,
+                                    real* bs) {
+  for (int i = 0; i < in->P * in->B; ++i) {
+    real* s = bs + 4 * (size_t)i;
+    s[0] = s[1] = s[2] = s[3] = 0;
+    int n = in->n_rots_for_block[i];
+    int r0 = in->rot_offset_for_block[i];
+    if (n <= 0 || r0 < 0) continue;
+    real cx = 0, cy = 0, cz = 0;
+    for (int r = 0; r < n; ++r) {
+      cx += rs[4 * (size_t)(r0 + r) + 0];
+      cy += rs[4 * (size_t)(r0 + r) + 1];
+      cz += rs[4 * (size_t)(r0 + r) + 2];
+    }
+    cx /= n;
+    cy /= n;
+    cz /= n;
+    real rmax = 0;
+    for (int r = 0; r < n; ++r) {
+      const real* q = rs + 4 * (size_t)(r0 + r);
+      real dx = q[0] - cx, dy = q[1] - cy, dz = q[2] - cz;
+      real d = rsqrt_(dx * dx + dy * dy + dz * dz) + q[3];
+      if (d > rmax) rmax = d;
+    }
+    s[0] = cx;
+    s[1] = cy;
+    s[2] = cz;
+    s[3] = rmax;
+  }
+}
+
+/* Block neighbours of the rotamer op into nbr[P][B][B]; returns the number
+ * of rotamer pairs it dispatches (rot_neighbor_indices_from_block_neighbors,
+ * sphere_overlap.impl.hh:512-610): n_rots(b1) self pairs on the diagonal,
+ * n_rots(b1) * n_rots(b2) pairs off it. */
+int64_t oracle_ljlk_rotamer_count(const oracle_inputs_t* in, int32_t* nbr) {
+  int P = in->P, B = in->B;
+  real* rs = (real*)malloc(sizeof(real) * 4 * (size_t)(in->n_rots + 1));
+  real* bs = (real*)malloc(sizeof(real) * 4 * ((size_t)P * B + 1));
+  if (!rs || !bs) {
+    free(rs);
+    free(bs);
+    return -1;
+  }
+  rot_spheres(in, rs);
+  block_spheres_from_rots(in, rs, bs);
+  detect_neighbors(in, bs, nbr);
+  free(rs);
+  free(bs);
+  int64_t total = 0;
+  for (int p = 0; p < P; ++p)
+    for (int b1 = 0; b1 < B; ++b1)
+      for (int b2 = b1; b2 < B; ++b2) {
+        if (!nbr[((size_t)p * B + b1) * B + b2]) continue;
+        int64_t n1 = in->n_rots_for_block[p * B + b1];
+        int64_t n2 = in->n_rots_for_block[p * B + b2];
+        total += b1 == b2 ? n1 : n1 * n2;
+      }
+  return total;
+}
+
+/* Visit every dispatched rotamer pair in the reference's order (pose, b1,
+ * b2, rotamer of b1, rotamer of b2); fn(k, p, b1, b2, rot1, rot2). */
+typedef void (*rot_pair_fn)(const oracle_inputs_t*, int64_t, int, int, int, int,
+                            int, void*);
+static void for_rot_pairs(const oracle_inputs_t* in, const int32_t* nbr,
+                          rot_pair_fn fn, void* arg) {
+  int P = in->P, B = in->B;
+  int64_t k = 0;
+  for (int p = 0; p < P; ++p)
+    for (int b1 = 0; b1 < B; ++b1)
+      for (int b2 = b1; b2 < B; ++b2) {
+        if (!nbr[((size_t)p * B + b1) * B + b2]) continue;
+        int n1 = in->n_rots_for_block[p * B + b1];
+        int n2 = in->n_rots_for_block[p * B + b2];
+        int o1 = in->rot_offset_for_block[p * B + b1];
+        int o2 = in->rot_offset_for_block[p * B + b2];
+        if (o1 < 0 || o2 < 0) continue;
+        if (b1 == b2) {
+          for (int i = 0; i < n1; ++i) fn(in, k++, p, b1, b2, o1 + i, o1 + i, arg);
+        } else {
+          for (int i = 0; i < n1; ++i)
+            for (int j = 0; j < n2; ++j) fn(in, k++, p, b1, b2, o1 + i, o2 + j, arg);
+        }
+      }
+}
+
+typedef struct {
+  eval_t ev;
+  real* E;          /* [3][n] */
+  int32_t* idx;     /* [3][n] */
+  const real* dTdV; /* [3][n] */
+  int64_t n;
+} rot_job_t;
+
+static void rot_pair_energy(const oracle_inputs_t* in, int64_t k, int p, int b1,
+                            int b2, int rot1, int rot2, void* arg) {
+  rot_job_t* job = (rot_job_t*)arg;
+  job->idx[k] = p;
+  job->idx[job->n + k] = rot1;
+  job->idx[2 * job->n + k] = rot2;
+  real tot[3] = {0, 0, 0};
+  pair_ctx_t c;
+  if (setup_rot_pair(in, p, b1, b2, rot1, rot2, &c)) eval_block_pair(in, &job->ev, &c, tot);
+  for (int t = 0; t < 3; ++t) job->E[t * job->n + k] = tot[t];
+}
+
+static void rot_pair_adjoint(const oracle_inputs_t* in, int64_t k, int p, int b1,
+                             int b2, int rot1, int rot2, void* arg) {
+  rot_job_t* job = (rot_job_t*)arg;
+  pair_ctx_t c;
+  if (!setup_rot_pair(in, p, b1, b2, rot1, rot2, &c)) return;
+  for (int t = 0; t < 3; ++t) job->ev.w[t] = job->dTdV[t * job->n + k];
+  real tot[3];
+  eval_block_pair(in, &job->ev, &c, tot);
+}
+
+/*
+ * The rotamer-score op forward: out_E[3][n] energies of the n dispatched
+ * rotamer pairs and out_idx[3][n] their (pose, rot1, rot2), n from
+ * oracle_ljlk_rotamer_count (nbr as it returned).
+ */
+int oracle_ljlk_rotamer_scores(const oracle_inputs_t* in, const int32_t* nbr,
+                               int64_t n, real* out_E, int32_t* out_idx) {
+  rot_job_t job;
+  job.ev.mode = MODE_ENERGY;
+  job.ev.dV = NULL;
+  job.E = out_E;
+  job.idx = out_idx;
+  job.dTdV = NULL;
+  job.n = n;
+  for_rot_pairs(in, nbr, rot_pair_energy, &job);
+  return 0;
+}
+
+/* Its adjoint: out_dx[n_atoms][3] = sum_k sum_t dTdV[t][k] dE_t(pair k)/dx
+ * (ljlk_pose_score.impl.hh:1826-2126). */
+int oracle_ljlk_rotamer_backward(const oracle_inputs_t* in, const int32_t* nbr,
+                                 int64_t n, const real* dTdV, real* out_dx) {
+  for (size_t k = 0; k < (size_t)3 * in->n_atoms; ++k) out_dx[k] = 0;
+  rot_job_t job;
+  job.ev.mode = MODE_WEIGHTED_DERIVS;
+  job.ev.dV = out_dx;
+  job.E = NULL;
+  job.idx = NULL;
+  job.dTdV = dTdV;
+  job.n = n;
+  for_rot_pairs(in, nbr, rot_pair_adjoint, &job);
+  return 0;
+}

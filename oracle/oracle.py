@@ -32,6 +32,7 @@ def _lib(f64):
         if not os.path.exists(path):
             build()
         lib = ctypes.CDLL(path)
+        lib.oracle_ljlk_rotamer_count.restype = ctypes.c_int64
         _LIBS[key] = lib
     return _LIBS[key]
 
@@ -72,6 +73,7 @@ def _inputs_struct(real_t):
             ("C", ctypes.c_int),
             ("ntiles", ctypes.c_int),
             ("T", ctypes.c_int),
+            ("n_rots_for_block", i32p),
         ]
 
     return Inputs
@@ -96,7 +98,7 @@ class OracleCall:
             block_type_ind_for_rot,
             _n_rots_for_pose,
             _rot_offset_for_pose,
-            _n_rots_for_block,
+            n_rots_for_block,
             rot_offset_for_block,
             _max_n_rots_per_pose,
             min_bondsep,
@@ -144,6 +146,7 @@ class OracleCall:
         s.bt_conn_atom = i32(bt_conn_atom)
         s.bt_path_distance = i32(bt_path_distance)
         s.bt_is_ligand = i32(bt_is_ligand)
+        s.n_rots_for_block = i32(n_rots_for_block)
         s.type_params = rl(type_params)
         s.global_params = rl(global_params.reshape(-1))
         s.max_dis = float(max_dis)
@@ -187,6 +190,30 @@ class OracleCall:
         rc = lib.oracle_ljlk_backward(
             ctypes.byref(self.s), self._ptr(nb), self._ptr(w), ctypes.c_int(int(per_pose_weights)), self._ptr(out)
         )
+        assert rc == 0
+        return out
+
+    def rotamer_scores(self):
+        """The rotamer-score op: (E [3, n], indices [3, n] (pose, rot1, rot2),
+        block neighbours [P, B, B])."""
+        lib = _lib(self.f64)
+        nbr = numpy.zeros((self.P, self.B, self.B), dtype=numpy.int32)
+        n = lib.oracle_ljlk_rotamer_count(ctypes.byref(self.s), self._ptr(nbr))
+        assert n >= 0
+        E = numpy.zeros((3, n), dtype=self.np_real)
+        idx = numpy.zeros((3, n), dtype=numpy.int32)
+        rc = lib.oracle_ljlk_rotamer_scores(ctypes.byref(self.s), self._ptr(nbr), ctypes.c_int64(n),
+                                            self._ptr(E), self._ptr(idx))
+        assert rc == 0
+        return E, idx, nbr
+
+    def rotamer_backward(self, nbr, dTdV):
+        lib = _lib(self.f64)
+        w = numpy.ascontiguousarray(numpy.asarray(dTdV, dtype=self.np_real))
+        nb = numpy.ascontiguousarray(nbr.astype(numpy.int32))
+        out = numpy.zeros((self.N, 3), dtype=self.np_real)
+        rc = lib.oracle_ljlk_rotamer_backward(ctypes.byref(self.s), self._ptr(nb), ctypes.c_int64(w.shape[1]),
+                                              self._ptr(w), self._ptr(out))
         assert rc == 0
         return out
 
@@ -242,6 +269,19 @@ def load_reference():
         torch.ops.load_library(REF_LIB)
         _ref_loaded = True
     return torch.ops.tmol_ljlk.ljlk_pose_scores
+
+
+def reference_rotamer_scores(coords, args, require_gradient=True):
+    """Runs the reference CPU rotamer op: returns (scores [3, n], coords
+    tensor (with grad if requested), indices [3, n])."""
+    load_reference()
+    op = torch.ops.tmol_ljlk.ljlk_rotamer_scores
+    cpu_args = [a.cpu() if isinstance(a, torch.Tensor) else a for a in args]
+    c = coords.detach().cpu().reshape(-1, 3).clone()
+    if require_gradient:
+        c.requires_grad_(True)
+    E, idx = op(c, *cpu_args)
+    return E, c, idx
 
 
 def reference_pose_scores(coords, args, require_gradient=True):

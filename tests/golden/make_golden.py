@@ -16,6 +16,10 @@ Writes
   synthetic.npz      reference op energies, gradient and neighbour matrix of
                      a jagged batch of seeded synthetic poses (1, 2, 7, 33,
                      100 residues), plus the sizes and seeds that rebuild it
+  rotamers.npz       the reference rotamer-score op (ljlk_rotamer_scores) on
+                     a seeded rotamer set over a jagged batch of poses: the
+                     set itself, the rotamer-pair energies and dispatch
+                     indices, and the gradient of sum(w * E) for seeded w
 """
 
 import os
@@ -32,10 +36,19 @@ from oracle import oracle as O  # noqa: E402
 from tmol_b200.pose.builder import build_pose_stack  # noqa: E402
 from tmol_b200.pose.pdb import pose_from_pdb_text  # noqa: E402
 from tmol_b200.pose.synthetic import synthetic_pose_stack  # noqa: E402
-from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm, pose_score_args  # noqa: E402
+from tmol_b200.pose.rotamers import synthetic_rotamer_set  # noqa: E402
+from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm, pose_score_args, rotamer_score_args  # noqa: E402
 
 SYN_SIZES = [1, 2, 7, 33, 100]
 SYN_SEEDS = [11, 12, 13, 14, 15]
+ROT_SIZES = [12, 30, 1, 45]
+ROT_SEEDS = [21, 22, 23, 24]
+ROT_SET = dict(max_rots=4, mutate_fraction=0.25, seed=5, skip_fraction=0.1)
+ROT_FIELDS = (
+    "n_rots_for_pose", "rot_offset_for_pose", "n_rots_for_block", "rot_offset_for_block", "pose_for_rot",
+    "block_type_ind_for_rot", "block_ind_for_rot", "coord_offset_for_rot", "coords", "first_rot_block_type",
+    "pose_ind_for_atom",
+)
 
 
 def ref_scores(ps, term):
@@ -83,6 +96,24 @@ def main(ref_root):
         ref_energies=E,
         ref_grad=g,
         ref_neighbors=nbr,
+    )
+    ps = synthetic_pose_stack(ROT_SIZES, ROT_SEEDS)
+    rs = synthetic_rotamer_set(ps, **ROT_SET)
+    args = rotamer_score_args(ps, rs, term)
+    E, c, idx = O.reference_rotamer_scores(rs.coords, args, require_gradient=True)
+    w = torch.tensor(numpy.random.default_rng(7).normal(size=tuple(E.shape)), dtype=E.dtype)
+    (E * w).sum().backward()
+    numpy.savez_compressed(
+        os.path.join(HERE, "rotamers.npz"),
+        sizes=numpy.array(ROT_SIZES),
+        seeds=numpy.array(ROT_SEEDS),
+        pose_coords=ps.coords.numpy(),
+        max_n_rots_per_pose=numpy.array(rs.max_n_rots_per_pose),
+        **{f: getattr(rs, f).numpy() for f in ROT_FIELDS},
+        ref_energies=E.detach().numpy(),
+        ref_indices=idx.numpy(),
+        weights=w.numpy(),
+        ref_grad=c.grad.numpy(),
     )
     print("wrote fixtures to", HERE)
 

@@ -125,3 +125,31 @@ def pose_score_args(pose_stack, term, block_pair=False):
         pose_stack.max_n_rots_per_pose,
     ]
     return common + term.get_score_term_attributes(pose_stack) + [block_pair]
+
+
+def rotamer_score_args(pose_stack, rotamer_set, term):
+    """The rotamer-score op's argument list minus the coordinates, in the
+    order tmol's ``TermRotamerScoringModule`` passes it
+    (tmol/score/common/scoring_module.py:133-170; op at
+    ``compiled.ops.cpp:599-662``): the rotamer set's indexing, the pose's
+    term attributes, and ``output_block_pair_energies=True``."""
+
+    def i32(t):
+        return t if isinstance(t, int) else t.to(torch.int32)
+
+    rs = rotamer_set
+    common = [
+        i32(rs.coord_offset_for_rot),
+        i32(rs.pose_ind_for_atom),
+        i32(rs.rot_offset_for_block),
+        i32(rs.first_rot_block_type),
+        i32(rs.block_ind_for_rot),
+        i32(rs.pose_for_rot),
+        i32(rs.block_type_ind_for_rot),
+        i32(rs.n_rots_for_pose),
+        i32(rs.rot_offset_for_pose),
+        i32(rs.n_rots_for_block),
+        i32(rs.rot_offset_for_block),
+        int(rs.max_n_rots_per_pose),
+    ]
+    return common + term.get_score_term_attributes(pose_stack) + [True]
