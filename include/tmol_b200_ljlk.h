@@ -202,6 +202,58 @@ int tmol_b200_ljlk_block_neighbors_noalloc(
     int32_t n_block_types, int32_t n_poses, int32_t max_n_blocks,
     double max_dis, int32_t* block_neighbors, void* stream);
 
+/* ---- Rotamer scoring (tmol's ljlk_rotamer_scores, the packer's op) ----
+ *
+ * The inputs are those of torch.ops.tmol_ljlk.ljlk_rotamer_scores
+ * (compiled.ops.cpp:599-662): the same struct, where block (p, b) owns
+ * rotamers rot_offset_for_block[p, b] .. + n_rots_for_block[p, b] - 1
+ * (n_rots is the total; a block with no rotamers takes no part), each with
+ * its own block type and coordinates.  One call scores every rotamer pair
+ * of neighbouring blocks and every rotamer with itself:
+ *   count    -> number of pairs n and of work items (synchronises `stream`)
+ *   fill     -> indices [3, n] int32 (pose, rot1, rot2) in the reference's
+ *               order, and the work items [n_items, 4] int32
+ *   forward  -> energies [3, n]; backward -> dL/dcoords [n_atoms, 3] from
+ *               dL/dE [3, n]
+ * A rotamer plan only serves these calls (the pose entry points reject it). */
+
+/* Replaces the per-call set-up of LJLKRotamerScoreDispatch::forward
+ * (ljlk_pose_score.impl.hh:1479-1630): validates every rotamer table. */
+int tmol_b200_ljlk_rotamer_plan_create(const tmol_b200_ljlk_inputs* inputs,
+                                       int real_bytes,
+                                       const tmol_b200_ljlk_launch* launch,
+                                       void* stream,
+                                       tmol_b200_ljlk_plan** plan_out);
+
+/* Rotamer spheres, block spheres enclosing each block's rotamers and the
+ * block-neighbour rule, bit-exact with compute_rot_spheres,
+ * compute_block_spheres_from_rot_spheres and detect_block_neighbors
+ * (sphere_overlap.impl.hh:23-107, 455-510, 287-351), and the pair counts of
+ * rot_neighbor_indices_from_block_neighbors (:512-610). */
+int tmol_b200_ljlk_rotamer_count(tmol_b200_ljlk_plan* plan, const void* coords,
+                                  int64_t* n_pairs, int64_t* n_items,
+                                  void* stream);
+
+/* The dispatch indices of the last count (rot_neighbor_indices_from_block_
+ * neighbors, sphere_overlap.impl.hh:512-610) and the work items. */
+int tmol_b200_ljlk_rotamer_fill(tmol_b200_ljlk_plan* plan, int32_t* indices,
+                                int32_t* items, void* stream);
+
+/* Energies of the dispatched pairs: LJLKRotamerScoreOp::forward
+ * (compiled.ops.cpp:282-406, ljlk_pose_score.impl.hh:1632-1819). */
+int tmol_b200_ljlk_rotamer_forward(tmol_b200_ljlk_plan* plan,
+                                    const void* coords, const int32_t* items,
+                                    int64_t n_items, int64_t n_pairs,
+                                    void* energies, void* stream);
+
+/* Recompute adjoint: LJLKRotamerScoreOp::backward (compiled.ops.cpp:408-529,
+ * ljlk_pose_score.impl.hh:1826-2126). */
+int tmol_b200_ljlk_rotamer_backward(tmol_b200_ljlk_plan* plan,
+                                     const void* coords, const int32_t* items,
+                                     int64_t n_items, int64_t n_pairs,
+                                     const void* dTdV, void* dcoords,
+                                     void* stream);
+
 /* Human-readable text of a status code. */
 const char* tmol_b200_status_string(int status);
 

@@ -1,0 +1,132 @@
+"""GPU parity of rotamer scoring (tmol's ljlk_rotamer_scores).
+
+- against the reference op's outputs committed in tests/golden/rotamers.npz:
+  dispatch indices bit-exact, energies within 1e-5 relative / 1e-3 kcal/mol,
+  the gradient of sum(w * E) within 1e-4 of its largest component;
+- against the C oracle on larger seeded rotamer sets (mutations, blocks
+  without rotamers, up to 6 rotamers per block), in float32 and float64
+  (1e-9);
+- a rotamer set with exactly the native rotamer per block scores like the
+  pose op (the rotamer-pair energies add up to the whole-pose energies);
+- torch gradcheck in float64 through ``ljlk_rotamer_scores``, and the
+  rendered scoring module.
+"""
+
+import numpy
+import pytest
+import torch
+
+from oracle import oracle as O
+from tests.test_rotamer_oracle import fixture_case
+from tmol_b200 import native
+from tmol_b200.pose.rotamers import synthetic_rotamer_set
+from tmol_b200.pose.synthetic import synthetic_pose_stack
+from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm, pose_score_args, rotamer_score_args
+from tmol_b200.score.ljlk_op import LJLKPlan, ljlk_rotamer_scores
+
+pytestmark = pytest.mark.gpu
+DEV = torch.device("cuda:0")
+
+
+def E_close(E, ref, rtol=1e-5, atol=1e-3):
+    numpy.testing.assert_allclose(E, ref, rtol=rtol, atol=atol)
+
+
+def g_close(g, ref, rtol=1e-4):
+    scale = numpy.abs(ref).max()
+    numpy.testing.assert_allclose(g, ref, rtol=rtol, atol=rtol * scale)
+
+
+def gpu_args(ps, rs):
+    term = LJLKEnergyTerm(device=DEV)
+    return rotamer_score_args(ps, rs, term)
+
+
+def test_fixture_parity():
+    g, ps, rs = fixture_case(DEV)
+    args = gpu_args(ps, rs)
+    coords = rs.coords.clone().requires_grad_(True)
+    E, idx = ljlk_rotamer_scores(coords, *args)
+    assert numpy.array_equal(idx.cpu().numpy(), g["ref_indices"])
+    E_close(E.detach().cpu().numpy(), g["ref_energies"])
+    (E * torch.tensor(g["weights"], device=DEV)).sum().backward()
+    g_close(coords.grad.cpu().numpy(), g["ref_grad"])
+
+
+@pytest.mark.parametrize("sizes,seed,mut,skip", [([60, 120, 7], 41, 0.4, 0.1), ([200], 42, 0.0, 0.0)])
+def test_oracle_parity(sizes, seed, mut, skip):
+    ps = synthetic_pose_stack(sizes, [seed + k for k in range(len(sizes))], device=DEV, extra_chi_sd=15.0)
+    rs = synthetic_rotamer_set(ps, max_rots=6, mutate_fraction=mut, seed=seed, skip_fraction=skip)
+    args = gpu_args(ps, rs)
+    plan = LJLKPlan(rs.coords, args[:-1], rotamers=True)
+    idx, items = plan.rotamer_dispatch(rs.coords)
+    E = plan.rotamer_forward(rs.coords, items, idx.shape[1])
+    oc = O.OracleCall(rs.coords.cpu(), [a.cpu() if isinstance(a, torch.Tensor) else a for a in args])
+    Eo, idxo, nbr = oc.rotamer_scores()
+    assert numpy.array_equal(idx.cpu().numpy(), idxo)
+    E_close(E.cpu().numpy(), Eo)
+    w = torch.rand(E.shape, device=DEV, generator=torch.Generator(device=DEV).manual_seed(seed))
+    dx = plan.rotamer_backward(rs.coords, items, w)
+    g_close(dx.cpu().numpy(), oc.rotamer_backward(nbr, w.cpu().numpy()))
+
+
+def test_float64_matches_oracle():
+    ps = synthetic_pose_stack([50, 31], [51, 52], device=DEV, extra_chi_sd=15.0)
+    rs = synthetic_rotamer_set(ps, max_rots=4, mutate_fraction=0.3, seed=51)
+    args = gpu_args(ps, rs)
+    c64 = rs.coords.double()
+    plan = LJLKPlan(c64, args[:-1], rotamers=True)
+    idx, items = plan.rotamer_dispatch(c64)
+    E = plan.rotamer_forward(c64, items, idx.shape[1])
+    oc = O.OracleCall(c64.cpu(), [a.cpu() if isinstance(a, torch.Tensor) else a for a in args], f64=True)
+    Eo, idxo, nbr = oc.rotamer_scores()
+    assert numpy.array_equal(idx.cpu().numpy(), idxo)
+    E_close(E.cpu().numpy(), Eo, rtol=1e-9, atol=1e-9)
+    w = torch.rand(E.shape, device=DEV, dtype=torch.float64)
+    dx = plan.rotamer_backward(c64, items, w)
+    g_close(dx.cpu().numpy(), oc.rotamer_backward(nbr, w.cpu().numpy()), rtol=1e-9)
+
+
+def test_native_rotamers_reproduce_the_pose_op():
+    ps = synthetic_pose_stack([80, 35], [61, 62], device=DEV)
+    rs = synthetic_rotamer_set(ps, max_rots=1, seed=61)
+    term = LJLKEnergyTerm(device=DEV)
+    E_rot, idx = ljlk_rotamer_scores(rs.coords, *rotamer_score_args(ps, rs, term))
+    per_pose = torch.zeros((3, ps.n_poses), dtype=torch.float64, device=DEV)
+    per_pose.index_add_(1, idx[0].long(), E_rot.double())
+    coords = ps.coords.flatten(0, 1).contiguous()
+    plan = LJLKPlan(coords, pose_score_args(ps, term)[:-1])
+    E_pose, _ = plan.forward(coords, want_neighbors=False)
+    E_close(per_pose.cpu().numpy(), E_pose.double().cpu().numpy())
+
+
+def test_gradcheck_float64():
+    ps = synthetic_pose_stack([6, 4], [71, 72], device=DEV)
+    rs = synthetic_rotamer_set(ps, max_rots=3, mutate_fraction=0.5, seed=71)
+    args = gpu_args(ps, rs)
+    c = rs.coords.double().clone().requires_grad_(True)
+
+    def f(x):
+        return ljlk_rotamer_scores(x, *args)[0]
+
+    assert torch.autograd.gradcheck(f, (c,), eps=1e-6, atol=1e-5, rtol=1e-3)
+
+
+def test_rendered_module_and_plan_kinds():
+    g, ps, rs = fixture_case(DEV)
+    term = LJLKEnergyTerm(device=DEV)
+    mod = term.render_rotamer_scoring_module(ps, rs)
+    E, idx = mod(rs.coords)
+    assert numpy.array_equal(idx.cpu().numpy(), g["ref_indices"])
+    E_close(E.detach().cpu().numpy(), g["ref_energies"])
+    sparse = mod.forward_split(rs.coords)
+    assert sparse.shape == (3, ps.n_poses, rs.n_rotamers_total, rs.n_rotamers_total)
+    # a rotamer plan serves only the rotamer entry points, a pose plan only
+    # the pose ones
+    rplan = LJLKPlan(rs.coords, rotamer_score_args(ps, rs, term)[:-1], rotamers=True)
+    with pytest.raises(native.NativeError):
+        rplan.forward(rs.coords)
+    coords = ps.coords.flatten(0, 1).contiguous()
+    pplan = LJLKPlan(coords, pose_score_args(ps, term)[:-1])
+    with pytest.raises(native.NativeError):
+        pplan.rotamer_dispatch(coords)

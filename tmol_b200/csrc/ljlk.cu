@@ -90,6 +90,11 @@ struct PlanBuildArgs {
   int* cp_minsep;
   uint8_t* cp_seps;
   int* status;
+  int rotamers;  // rotamer plan: blocks may own any number of rotamers
+  int* rot_bt;   // rotamer plan: per-rotamer copies (validated)
+  int* rot_off;
+  int* rot_block;
+  int* rot_pose;
 };
 
 __global__ void plan_blocks_kernel(PlanBuildArgs a) {
@@ -101,6 +106,23 @@ __global__ void plan_blocks_kernel(PlanBuildArgs a) {
     int bt_first = in.first_rot_block_type[i];
     int rot = in.rot_offset_for_block[i];
     int bt = -1, off = 0;
+    if (a.rotamers) {
+      // a block without rotamers takes no part in rotamer scoring
+      const int nr = in.n_rots_for_block[i];
+      if (nr < 0) atomicOr(a.status, kStIndex);
+      if (nr <= 0) {
+        if (bt_first >= 0) atomicOr(a.status, kStShape);
+        a.blk_bt[i] = -1;
+        a.blk_off[i] = 0;
+        continue;
+      }
+      if (rot < 0 || (int64_t)rot + nr > in.n_rots) {
+        atomicOr(a.status, kStIndex);
+        a.blk_bt[i] = -1;
+        a.blk_off[i] = 0;
+        continue;
+      }
+    }
     if (rot < 0 || rot >= in.n_rots) {
       if (bt_first >= 0) atomicOr(a.status, kStIndex);
     } else {
@@ -125,6 +147,35 @@ __global__ void plan_blocks_kernel(PlanBuildArgs a) {
     a.blk_bt[i] = bt;
     a.blk_off[i] = off;
     if (bt >= 0) atomicMax(&a.pose_last[p], b + 1);
+  }
+}
+
+// Rotamer plan: per rotamer, its pose, block, block type and coordinates
+// must be in range and the rotamer must lie in its block's range.
+__global__ void plan_rotamers_kernel(PlanBuildArgs a) {
+  const tmol_b200_ljlk_inputs& in = a.in;
+  const int P = in.n_poses, B = in.max_n_blocks;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < in.n_rots; r += gridDim.x * blockDim.x) {
+    const int p = in.pose_ind_for_rot[r], b = in.block_ind_for_rot[r];
+    int bt = in.block_type_ind_for_rot[r];
+    const int off = in.rot_coord_offset[r];
+    if (p < 0 || p >= P || b < 0 || b >= B) {
+      atomicOr(a.status, kStIndex);
+    } else {
+      const int i = p * B + b;
+      const int r0 = in.rot_offset_for_block[i], nr = in.n_rots_for_block[i];
+      if (r < r0 || r >= r0 + nr) atomicOr(a.status, kStShape);
+    }
+    if (bt < 0 || bt >= in.n_block_types) {
+      atomicOr(a.status, kStIndex);
+      bt = 0;
+    } else if (off < 0 || (int64_t)off + in.bt_n_atoms[bt] > in.n_atoms) {
+      atomicOr(a.status, kStIndex);
+    }
+    a.rot_bt[r] = bt;
+    a.rot_off[r] = off < 0 ? 0 : off;
+    a.rot_block[r] = b < 0 || b >= B ? 0 : b;
+    a.rot_pose[r] = p < 0 || p >= P ? 0 : p;
   }
 }
 
@@ -318,61 +369,64 @@ struct ScoreArgs {
 // (shuffled to it one by one, no contraction) so that the sums are
 // bit-identical to the sequential CPU loop; the maximum is order-free.
 template <typename Real>
+__device__ __forceinline__ void warp_sphere(const Real* coords, const int* bt_n_atoms, int bt,
+                                            int off, int lane, Real* out) {
+  if (bt < 0) {
+    if (lane < 4) out[lane] = Real(0);
+    return;
+  }
+  int n = bt_n_atoms[bt];
+  const Real* x = coords + 3 * (int64_t)off;
+  Real cx = 0, cy = 0, cz = 0;
+  for (int base = 0; base < n; base += 32) {
+    int k = base + lane;
+    Real ax = 0, ay = 0, az = 0;
+    if (k < n) {
+      ax = x[3 * k + 0];
+      ay = x[3 * k + 1];
+      az = x[3 * k + 2];
+    }
+    int cnt = min(32, n - base);
+    for (int q = 0; q < cnt; ++q) {
+      Real vx = __shfl_sync(0xffffffffu, ax, q);
+      Real vy = __shfl_sync(0xffffffffu, ay, q);
+      Real vz = __shfl_sync(0xffffffffu, az, q);
+      cx = add_rn(cx, vx);
+      cy = add_rn(cy, vy);
+      cz = add_rn(cz, vz);
+    }
+  }
+  Real rn = Real(n);
+  cx = div_rn(cx, rn);
+  cy = div_rn(cy, rn);
+  cz = div_rn(cz, rn);
+  Real d2max = 0;
+  for (int k = lane; k < n; k += 32) {
+    Real dx = sub_rn(x[3 * k + 0], cx);
+    Real dy = sub_rn(x[3 * k + 1], cy);
+    Real dz = sub_rn(x[3 * k + 2], cz);
+    Real d2 = add_rn(add_rn(mul_rn(dx, dx), mul_rn(dy, dy)), mul_rn(dz, dz));
+    if (d2 > d2max) d2max = d2;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    Real v = __shfl_xor_sync(0xffffffffu, d2max, o);
+    d2max = v > d2max ? v : d2max;
+  }
+  if (lane == 0) {
+    out[0] = cx;
+    out[1] = cy;
+    out[2] = cz;
+    out[3] = sqrt_rn(d2max);
+  }
+}
+
+template <typename Real>
 __global__ void spheres_kernel(ScoreArgs<Real> s) {
   const int lane = threadIdx.x & 31;
   const int n_blocks = s.P * s.B;
   const int warps = (gridDim.x * blockDim.x) >> 5;
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n_blocks; i += warps) {
-    int bt = s.blk_bt[i];
-    Real* out = s.spheres + 4 * (int64_t)i;
-    if (bt < 0) {
-      if (lane < 4) out[lane] = Real(0);
-      continue;
-    }
-    int n = s.bt_n_atoms[bt];
-    const Real* x = s.coords + 3 * (int64_t)s.blk_off[i];
-    Real cx = 0, cy = 0, cz = 0;
-    for (int base = 0; base < n; base += 32) {
-      int k = base + lane;
-      Real ax = 0, ay = 0, az = 0;
-      if (k < n) {
-        ax = x[3 * k + 0];
-        ay = x[3 * k + 1];
-        az = x[3 * k + 2];
-      }
-      int cnt = min(32, n - base);
-      for (int q = 0; q < cnt; ++q) {
-        Real vx = __shfl_sync(0xffffffffu, ax, q);
-        Real vy = __shfl_sync(0xffffffffu, ay, q);
-        Real vz = __shfl_sync(0xffffffffu, az, q);
-        cx = add_rn(cx, vx);
-        cy = add_rn(cy, vy);
-        cz = add_rn(cz, vz);
-      }
-    }
-    Real rn = Real(n);
-    cx = div_rn(cx, rn);
-    cy = div_rn(cy, rn);
-    cz = div_rn(cz, rn);
-    Real d2max = 0;
-    for (int k = lane; k < n; k += 32) {
-      Real dx = sub_rn(x[3 * k + 0], cx);
-      Real dy = sub_rn(x[3 * k + 1], cy);
-      Real dz = sub_rn(x[3 * k + 2], cz);
-      Real d2 = add_rn(add_rn(mul_rn(dx, dx), mul_rn(dy, dy)), mul_rn(dz, dz));
-      if (d2 > d2max) d2max = d2;
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      Real v = __shfl_xor_sync(0xffffffffu, d2max, o);
-      d2max = v > d2max ? v : d2max;
-    }
-    if (lane == 0) {
-      out[0] = cx;
-      out[1] = cy;
-      out[2] = cz;
-      out[3] = sqrt_rn(d2max);
-    }
-  }
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n_blocks; i += warps)
+    warp_sphere(s.coords, s.bt_n_atoms, s.blk_bt[i], s.blk_off[i], lane, s.spheres + 4 * (int64_t)i);
 }
 
 // ---------------------------------------------------------------------------
@@ -1151,6 +1205,352 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
     atomicAdd(&s.counts[lane], w.counts[lane]);
 }
 
+// ---------------------------------------------------------------------------
+// Rotamer scoring (tmol's ljlk_rotamer_scores, ljlk_pose_score.impl.hh:
+// 1479-2126): every block owns a range of rotamers, each with its own block
+// type and coordinates; the energies of every rotamer pair of neighbouring
+// blocks (and of each rotamer with itself) are reported separately.
+
+// Rotamer indexing for the rotamer kernels.
+struct RotArgs {
+  const int* rot_bt;     // [R] block type of each rotamer
+  const int* rot_off;    // [R] first coordinate row
+  const int* rot_block;  // [R]
+  const int* rot_pose;   // [R]
+  const int* nrb;        // [P*B] rotamers per block
+  const int* rob;        // [P*B] first rotamer of each block
+  int R;
+  long long* row_pairs;  // [P*B] rotamer pairs per row (then their offsets)
+  long long* row_items;  // [P*B] work items per row (then their offsets)
+  int4* items;           // (rot1, first rot2, n rot2, first pair)
+  long long n_items;
+  int32_t* indices;      // [3, n_pairs] (pose, rot1, rot2)
+  long long n_pairs;
+};
+
+// Bounding sphere of each rotamer, as spheres_kernel (the reference's
+// compute_rot_spheres on the CPU, sphere_overlap.impl.hh:23-107).
+template <typename Real>
+__global__ void rot_spheres_kernel(ScoreArgs<Real> s, RotArgs ra, Real* rs) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < ra.R; r += warps)
+    warp_sphere(s.coords, s.bt_n_atoms, ra.rot_bt[r], ra.rot_off[r], lane, rs + 4 * (int64_t)r);
+}
+
+// Block spheres enclosing all rotamers of each block: the mean of the
+// rotamer centres and the largest centre distance plus rotamer radius
+// (compute_block_spheres_from_rot_spheres, sphere_overlap.impl.hh:455-510),
+// in the reference's order.
+template <typename Real>
+__global__ void block_spheres_from_rots_kernel(ScoreArgs<Real> s, RotArgs ra, const Real* rs) {
+  const int n_blocks = s.P * s.B;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_blocks; i += gridDim.x * blockDim.x) {
+    Real* out = s.spheres + 4 * (int64_t)i;
+    const int n = ra.nrb[i], r0 = ra.rob[i];
+    if (s.blk_bt[i] < 0 || n <= 0 || r0 < 0) {
+      out[0] = out[1] = out[2] = out[3] = Real(0);
+      continue;
+    }
+    Real cx = 0, cy = 0, cz = 0;
+    for (int r = 0; r < n; ++r) {
+      const Real* q = rs + 4 * (int64_t)(r0 + r);
+      cx = add_rn(cx, q[0]);
+      cy = add_rn(cy, q[1]);
+      cz = add_rn(cz, q[2]);
+    }
+    const Real rn = Real(n);
+    cx = div_rn(cx, rn);
+    cy = div_rn(cy, rn);
+    cz = div_rn(cz, rn);
+    Real rmax = 0;
+    for (int r = 0; r < n; ++r) {
+      const Real* q = rs + 4 * (int64_t)(r0 + r);
+      Real dx = sub_rn(q[0], cx), dy = sub_rn(q[1], cy), dz = sub_rn(q[2], cz);
+      Real d = add_rn(sqrt_rn(add_rn(add_rn(mul_rn(dx, dx), mul_rn(dy, dy)), mul_rn(dz, dz))), q[3]);
+      if (d > rmax) rmax = d;
+    }
+    out[0] = cx;
+    out[1] = cy;
+    out[2] = cz;
+    out[3] = rmax;
+  }
+}
+
+// The reference neighbour rule between blocks i1 and i2 (bit-exact).
+template <typename Real>
+__device__ __forceinline__ bool block_hit(const ScoreArgs<Real>& s, int i1, int i2) {
+  if (s.blk_bt[i2] < 0) return false;
+  const Real* s1 = s.spheres + 4 * (int64_t)i1;
+  const Real* s2 = s.spheres + 4 * (int64_t)i2;
+  Real dx = sub_rn(s1[0], s2[0]);
+  Real dy = sub_rn(s1[1], s2[1]);
+  Real dz = sub_rn(s1[2], s2[2]);
+  Real d2 = add_rn(add_rn(mul_rn(dx, dx), mul_rn(dy, dy)), mul_rn(dz, dz));
+  Real thr = add_rn(add_rn(s1[3], s2[3]), s.reach);
+  return d2 < mul_rn(thr, thr);
+}
+
+// Per row (p, b1): how many rotamer pairs and work items its neighbouring
+// blocks b2 >= b1 dispatch (n(b1) on the diagonal, n(b1) * n(b2) off it;
+// one item per rotamer of b1 and neighbour).
+template <typename Real>
+__global__ void rot_row_count_kernel(ScoreArgs<Real> s, RotArgs ra) {
+  const int lane = threadIdx.x & 31;
+  const int n_rows = s.P * s.B;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n_rows; row += warps) {
+    long long pairs = 0, items = 0;
+    if (s.blk_bt[row] >= 0) {
+      const int p = row / s.B, b1 = row - p * s.B;
+      const long long n1 = ra.nrb[row];
+      for (int b2 = b1 + lane; b2 < s.pose_last[p]; b2 += 32) {
+        const int i2 = p * s.B + b2;
+        if (!block_hit(s, row, i2)) continue;
+        pairs += b2 == b1 ? n1 : n1 * ra.nrb[i2];
+        items += n1;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
+      items += __shfl_xor_sync(0xffffffffu, items, o);
+    }
+    if (lane == 0) {
+      ra.row_pairs[row] = pairs;
+      ra.row_items[row] = items;
+    }
+  }
+}
+
+// Exclusive scans of a[0..n) and b[0..n) in place, totals into t[0], t[1];
+// one CTA of 1024 threads, each scanning a contiguous chunk.
+__global__ void __launch_bounds__(1024) scan2_kernel(long long* a, long long* b, int n,
+                                                     long long* t) {
+  __shared__ long long sa[1024], sb[1024];
+  const int tid = threadIdx.x;
+  const int chunk = (n + 1023) / 1024;
+  const int lo = min(n, tid * chunk), hi = min(n, lo + chunk);
+  long long va = 0, vb = 0;
+  for (int i = lo; i < hi; ++i) {
+    va += a[i];
+    vb += b[i];
+  }
+  sa[tid] = va;
+  sb[tid] = vb;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    long long xa = tid >= o ? sa[tid - o] : 0, xb = tid >= o ? sb[tid - o] : 0;
+    __syncthreads();
+    sa[tid] += xa;
+    sb[tid] += xb;
+    __syncthreads();
+  }
+  long long ra_ = sa[tid] - va, rb_ = sb[tid] - vb;
+  for (int i = lo; i < hi; ++i) {
+    const long long xa = a[i], xb = b[i];
+    a[i] = ra_;
+    b[i] = rb_;
+    ra_ += xa;
+    rb_ += xb;
+  }
+  if (tid == 1023) {
+    t[0] = sa[1023];
+    t[1] = sb[1023];
+  }
+}
+
+// Writes the dispatch indices (pose, rot1, rot2) in the reference's order
+// (pose, b1, b2, rotamer of b1, rotamer of b2) and the work items, row by
+// row from the scanned offsets.
+template <typename Real>
+__global__ void rot_row_fill_kernel(ScoreArgs<Real> s, RotArgs ra) {
+  const int lane = threadIdx.x & 31;
+  const int n_rows = s.P * s.B;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  const long long np = ra.n_pairs;
+  for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n_rows; row += warps) {
+    if (s.blk_bt[row] < 0) continue;
+    const int p = row / s.B, b1 = row - p * s.B;
+    const int n1 = ra.nrb[row], o1 = ra.rob[row];
+    long long pair_off = ra.row_pairs[row], item_off = ra.row_items[row];
+    for (int base = b1; base < s.pose_last[p]; base += 32) {
+      const int b2l = base + lane;
+      const bool hit = b2l < s.pose_last[p] && block_hit(s, row, p * s.B + b2l);
+      unsigned m = __ballot_sync(0xffffffffu, hit);
+      while (m) {
+        const int k = __ffs(m) - 1;
+        m &= m - 1;
+        const int b2 = base + k;
+        const int i2 = p * s.B + b2;
+        const bool diag = b2 == b1;
+        const int n2 = diag ? 1 : ra.nrb[i2];
+        const int o2 = ra.rob[i2];
+        for (int i = lane; i < n1; i += 32) {
+          const long long first = pair_off + (long long)i * n2;
+          if (item_off + i < ra.n_items)
+            ra.items[item_off + i] = make_int4(o1 + i, diag ? o1 + i : o2, n2, (int)first);
+        }
+        const long long cnt = (long long)n1 * n2;
+        for (long long q = lane; q < cnt; q += 32) {
+          const long long d = pair_off + q;
+          if (d >= np) break;
+          const int i = (int)(q / n2), j = (int)(q - (long long)i * n2);
+          ra.indices[d] = p;
+          ra.indices[np + d] = o1 + i;
+          ra.indices[2 * np + d] = diag ? o1 + i : o2 + j;
+        }
+        pair_off += cnt;
+        item_off += n1;
+      }
+    }
+  }
+}
+
+// Scoring of work items: rotamer rot1 (side 0, tile by tile) against the
+// rotamers rot2 of one neighbouring block (side 1, one rotamer tile per
+// group), or against itself on the diagonal.  Energies go to the item's
+// pairs (energies[t * n_pairs + d]; the warp owns them), the adjoint
+// weights come from dTdV[t * n_pairs + d].
+template <typename Real, bool GRAD>
+__global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_CTAS : 1)
+    rotamer_kernel(ScoreArgs<Real> s, RotArgs ra, const Real* rs) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  Slab<Real>& w = reinterpret_cast<Slab<Real>*>(smem_raw)[warp];
+  if (lane < N_COUNTS) w.counts[lane] = 0;
+  __syncwarp();
+  const long long np = ra.n_pairs;
+  const bool want_E = s.energies != nullptr;
+  const Real reach_atoms = s.g.max_dis;
+  for (;;) {
+    int it = 0;
+    if (lane == 0) it = atomicAdd(s.ticket, 1);
+    it = __shfl_sync(0xffffffffu, it, 0);
+    if (it >= ra.n_items) break;
+    const int4 item = ra.items[it];
+    const int rot1 = item.x, rot2_first = item.y, n_rot2 = item.z;
+    const long long pair_first = item.w;
+    RowInfo r;
+    r.p = ra.rot_pose[rot1];
+    r.b1 = ra.rot_block[rot1];
+    r.i1 = r.p * s.B + r.b1;
+    r.bt1 = ra.rot_bt[rot1];
+    r.off1 = ra.rot_off[rot1];
+    r.n1 = s.bt_n_atoms[r.bt1];
+    r.nc1 = s.bt_n_conn[r.bt1];
+    r.lig1 = s.bt_is_ligand[r.bt1];
+    EvalCtx<Real> ec;
+    ec.ljtab = s.ljtab;
+    ec.lktab = s.lktab;
+    ec.ntp = s.ntp;
+    ec.A = s.A;
+    ec.max_dis = s.g.max_dis;
+    ec.wt0 = ec.wt1 = ec.wt2 = 0;
+    const Real* sph1 = rs + 4 * (int64_t)rot1;
+    const Real c1x = sph1[0], c1y = sph1[1], c1z = sph1[2], rad1 = sph1[3];
+    const Real reach1 = rad1 + reach_atoms;
+    const Real reach1_2 = reach1 * reach1 * Real(1.0001);
+    const bool diag = rot2_first == rot1;
+    // block-level count pair of (b1, b2): kind and connection separations
+    int kind = kSlotFar, cp_entry = 0, b2 = diag ? r.b1 : ra.rot_block[rot2_first];
+    if (!diag) {
+      const int ncp = s.cp_count[r.i1];
+      const int e = r.i1 * CP_CAP + lane;
+      const bool match = lane < ncp && s.cp_b2[e] == b2;
+      const unsigned pm = __ballot_sync(0xffffffffu, match);
+      if (pm) {
+        const int src = __ffs(pm) - 1;
+        const int msep = __shfl_sync(0xffffffffu, lane < ncp ? s.cp_minsep[e] : 6, src);
+        cp_entry = r.i1 * CP_CAP + src;
+        kind = msep <= 4 ? kSlotStriking : kSlotFar;
+      }
+    }
+    const int nt1 = (r.n1 + TILE - 1) / TILE;
+    for (int ti = 0; ti < nt1; ++ti) {
+      r.st1 = ti * TILE;
+      r.c1 = min(TILE, r.n1 - r.st1);
+      stage_side0(s, w, r.bt1, r.off1, r.st1, r.c1, r.nc1, lane);
+      ec.pd = s.bt_pd + ((int64_t)r.bt1 * s.A + r.st1) * s.A;
+      __syncwarp();
+      for (int k = 0; k < n_rot2; ++k) {
+        const long long d = pair_first + k;
+        if (GRAD) {
+          ec.wt0 = s.dTdV[d];
+          ec.wt1 = s.dTdV[np + d];
+          ec.wt2 = s.dTdV[2 * np + d];
+        }
+        E3<Real> e = {0, 0, 0};
+        if (diag) {
+          // this tile with itself, then with the rotamer's later tiles
+          E3<Real> t = intra_tile<Real, GRAD>(ec, &w, r.st1, r.c1, lane);
+          e.atr += t.atr;
+          e.rep += t.rep;
+          e.lk += t.lk;
+          for (int tj = ti + 1; tj < nt1; ++tj) {
+            const int st2 = tj * TILE, c2 = min(TILE, r.n1 - st2);
+            if (lane == 0) {
+              w.slot_kind[0] = kSlotIntra;
+              w.slot_nc[0] = 0;
+              w.slot_lig[0] = 0;
+              w.slot_sph[0][0] = c1x;
+              w.slot_sph[0][1] = c1y;
+              w.slot_sph[0][2] = c1z;
+              w.slot_sph[0][3] = rad1;
+            }
+            const int m = stage_side1(s, w, 0, 0, r.bt1, r.off1, st2, c2, 0, c1x, c1y, c1z, reach1_2, lane);
+            __syncwarp();
+            if (m > 0) {
+              E3<Real> g = screen_slots<Real, GRAD>(ec, &w, r.c1, r.nc1, m, 1, lane);
+              if (GRAD) flush_side1(s, w, m, lane);
+              e.atr += g.atr;
+              e.rep += g.rep;
+              e.lk += g.lk;
+            }
+            __syncwarp();
+          }
+        } else {
+          const int rot2 = rot2_first + k;
+          const int bt2 = ra.rot_bt[rot2], off2 = ra.rot_off[rot2];
+          const int n2 = s.bt_n_atoms[bt2];
+          const int nc2 = kind == kSlotStriking ? s.bt_n_conn[bt2] : 0;
+          const int lig = r.lig1 && s.bt_is_ligand[bt2];
+          const Real* sph2 = rs + 4 * (int64_t)rot2;
+          for (int st2 = 0; st2 < n2; st2 += TILE) {
+            const int c2 = min(TILE, n2 - st2);
+            if (lane == 0) {
+              w.slot_kind[0] = kind;
+              w.slot_nc[0] = nc2;
+              w.slot_lig[0] = lig;
+            }
+            if (lane < 4) w.slot_sph[0][lane] = sph2[lane];
+            if (kind == kSlotStriking && lane < 16) w.seps[0][lane] = s.cp_seps[(int64_t)cp_entry * 16 + lane];
+            const int m = stage_side1(s, w, 0, 0, bt2, off2, st2, c2, nc2, c1x, c1y, c1z, reach1_2, lane);
+            __syncwarp();
+            if (m > 0) {
+              E3<Real> g = screen_slots<Real, GRAD>(ec, &w, r.c1, r.nc1, m, 1, lane);
+              if (GRAD) flush_side1(s, w, m, lane);
+              e.atr += g.atr;
+              e.rep += g.rep;
+              e.lk += g.lk;
+            }
+            __syncwarp();
+          }
+        }
+        if (want_E) {
+          const Real v0 = warp_sum(e.atr), v1 = warp_sum(e.rep), v2 = warp_sum(e.lk);
+          if (lane == 0) {
+            s.energies[d] += v0;
+            s.energies[np + d] += v1;
+            s.energies[2 * np + d] += v2;
+          }
+        }
+      }
+      if (GRAD) flush_side0(s, w, r.off1, r.st1, r.c1, lane);
+      __syncwarp();
+    }
+  }
+}
+
 // Sub-spheres of every block for the screen's features: atoms [0, 4) (the
 // backbone N, CA, C, O of an amino acid) and atoms [4, n) (the rest; the
 // first part again when n <= 4), each as centroid + largest centroid
@@ -1348,6 +1748,19 @@ struct tmol_b200_ljlk_plan {
   const uint32_t* skip = nullptr;  // caller-owned screen mask, or null
   int skip_words = 0;
   float* sub_spheres = nullptr;  // screen features: [P*B][2][4] (float plans)
+  // rotamer plans
+  bool rotamers = false;
+  int R = 0;
+  int* rot_bt = nullptr;
+  int* rot_off = nullptr;
+  int* rot_block = nullptr;
+  int* rot_pose = nullptr;
+  int* nrb = nullptr;  // rotamers per block [P*B]
+  int* rob = nullptr;  // first rotamer of each block [P*B]
+  void* rot_spheres = nullptr;   // [R][4] reals
+  long long* row_pairs = nullptr;  // [P*B] + 2 totals
+  long long* row_items = nullptr;  // [P*B]
+  long long n_pairs = -1, n_items = -1;  // of the last rotamer_count
 };
 
 namespace {
@@ -1379,7 +1792,9 @@ void free_plan(tmol_b200_ljlk_plan* pl) {
                   pl->bt_n_conn, pl->bt_is_ligand, pl->cp_count, pl->cp_b2,
                   pl->cp_minsep, pl->cp_seps,    pl->work,       pl->spheres,
                   pl->item_cost,
-                  pl->counters,  pl->counts,     pl->sub_spheres};
+                  pl->counters,  pl->counts,     pl->sub_spheres, pl->rot_bt,
+                  pl->rot_off,   pl->rot_block,  pl->rot_pose,    pl->nrb,
+                  pl->rob,       pl->rot_spheres, pl->row_pairs,  pl->row_items};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t e : pl->prof_events) cudaEventDestroy(e);
@@ -1407,6 +1822,12 @@ cudaError_t set_smem_limits() {
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
     return e;
   if ((e = cudaFuncSetAttribute(score_kernel<Real, true, false>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
+    return e;
+  if ((e = cudaFuncSetAttribute(rotamer_kernel<Real, false>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
+    return e;
+  if ((e = cudaFuncSetAttribute(rotamer_kernel<Real, true>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
     return e;
   return cudaFuncSetAttribute(score_kernel<Real, true, true>,
@@ -1546,6 +1967,104 @@ int energy_and_gradient_impl(tmol_b200_ljlk_plan* pl, const void* coords,
   return launch_score<Real, true, false>(pl, s, st);
 }
 
+RotArgs rot_args(tmol_b200_ljlk_plan* pl) {
+  RotArgs ra = {};
+  ra.rot_bt = pl->rot_bt;
+  ra.rot_off = pl->rot_off;
+  ra.rot_block = pl->rot_block;
+  ra.rot_pose = pl->rot_pose;
+  ra.nrb = pl->nrb;
+  ra.rob = pl->rob;
+  ra.R = pl->R;
+  ra.row_pairs = pl->row_pairs;
+  ra.row_items = pl->row_items;
+  return ra;
+}
+
+template <typename Real>
+int rotamer_count_impl(tmol_b200_ljlk_plan* pl, const void* coords, int64_t* n_pairs,
+                       int64_t* n_items, cudaStream_t st) {
+  ScoreArgs<Real> s = score_args<Real>(pl, coords);
+  RotArgs ra = rot_args(pl);
+  const int n_rows = pl->P * pl->B;
+  long long totals[2] = {0, 0};
+  if (n_rows > 0) {
+    if (pl->R > 0) {
+      int gr = std::max(1, std::min((pl->R + 7) / 8, pl->n_sm * 16));
+      rot_spheres_kernel<Real><<<gr, 256, 0, st>>>(s, ra, (Real*)pl->rot_spheres);
+      CK(cudaGetLastError());
+    }
+    int gb = std::max(1, std::min((n_rows + 255) / 256, pl->n_sm * 8));
+    block_spheres_from_rots_kernel<Real><<<gb, 256, 0, st>>>(s, ra, (const Real*)pl->rot_spheres);
+    CK(cudaGetLastError());
+    int gw = std::max(1, std::min((n_rows + 7) / 8, pl->n_sm * 16));
+    rot_row_count_kernel<Real><<<gw, 256, 0, st>>>(s, ra);
+    CK(cudaGetLastError());
+    scan2_kernel<<<1, 1024, 0, st>>>(pl->row_pairs, pl->row_items, n_rows, pl->row_pairs + n_rows);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(totals, pl->row_pairs + n_rows, sizeof(totals), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+  }
+  // pair indices are int32 in the op's output, and work items address pairs
+  // with an int
+  if (totals[0] >= ((long long)1 << 31) || totals[1] >= ((long long)1 << 31)) {
+    pl->n_pairs = pl->n_items = -1;
+    return TMOL_B200_ERR_CAPACITY;
+  }
+  pl->n_pairs = totals[0];
+  pl->n_items = totals[1];
+  *n_pairs = totals[0];
+  *n_items = totals[1];
+  return TMOL_B200_OK;
+}
+
+template <typename Real>
+int rotamer_fill_impl(tmol_b200_ljlk_plan* pl, int32_t* indices, int32_t* items, cudaStream_t st) {
+  ScoreArgs<Real> s = score_args<Real>(pl, nullptr);
+  RotArgs ra = rot_args(pl);
+  ra.items = (int4*)items;
+  ra.n_items = pl->n_items;
+  ra.indices = indices;
+  ra.n_pairs = pl->n_pairs;
+  const int n_rows = pl->P * pl->B;
+  if (n_rows == 0 || (pl->n_pairs == 0 && pl->n_items == 0)) return TMOL_B200_OK;
+  int gw = std::max(1, std::min((n_rows + 7) / 8, pl->n_sm * 16));
+  rot_row_fill_kernel<Real><<<gw, 256, 0, st>>>(s, ra);
+  CK(cudaGetLastError());
+  return TMOL_B200_OK;
+}
+
+template <typename Real, bool GRAD>
+int rotamer_score_impl(tmol_b200_ljlk_plan* pl, const void* coords, const int32_t* items,
+                       int64_t n_items, int64_t n_pairs, void* energies, const void* dTdV,
+                       void* dcoords, cudaStream_t st) {
+  ScoreArgs<Real> s = score_args<Real>(pl, coords);
+  RotArgs ra = rot_args(pl);
+  ra.items = (int4*)items;
+  ra.n_items = n_items;
+  ra.n_pairs = n_pairs;
+  s.energies = (Real*)energies;
+  s.dTdV = (const Real*)dTdV;
+  s.dcoords = (Real*)dcoords;
+  s.counts = nullptr;
+  if (energies) CK(cudaMemsetAsync(energies, 0, (size_t)3 * n_pairs * sizeof(Real), st));
+  if (dcoords) CK(cudaMemsetAsync(dcoords, 0, (size_t)pl->N * 3 * sizeof(Real), st));
+  if (n_items == 0) return TMOL_B200_OK;
+  if (pl->R > 0) {
+    int gr = std::max(1, std::min((pl->R + 7) / 8, pl->n_sm * 16));
+    rot_spheres_kernel<Real><<<gr, 256, 0, st>>>(s, ra, (Real*)pl->rot_spheres);
+    CK(cudaGetLastError());
+  }
+  CK(cudaMemsetAsync(pl->counters, 0, sizeof(int), st));
+  const int warps = pl->launch.warps_per_cta;
+  const size_t smem = warps * sizeof(Slab<Real>);
+  int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n_items + warps - 1) / warps,
+                                                         (int64_t)pl->n_sm * pl->launch.ctas_per_sm));
+  rotamer_kernel<Real, GRAD><<<grid, 32 * warps, smem, st>>>(s, ra, (const Real*)pl->rot_spheres);
+  CK(cudaGetLastError());
+  return TMOL_B200_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1563,9 +2082,13 @@ const char* tmol_b200_status_string(int status) {
   return "unknown status";
 }
 
-int tmol_b200_ljlk_plan_create(const tmol_b200_ljlk_inputs* in, int real_bytes,
-                               const tmol_b200_ljlk_launch* launch,
-                               void* stream, tmol_b200_ljlk_plan** plan_out) {
+}  // extern "C"
+
+namespace {
+
+int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
+                const tmol_b200_ljlk_launch* launch, void* stream, bool rotamers,
+                tmol_b200_ljlk_plan** plan_out) {
   if (!in || !plan_out) return TMOL_B200_ERR_INVALID_ARGUMENT;
   *plan_out = nullptr;
   if (real_bytes != 4 && real_bytes != 8) return TMOL_B200_ERR_DTYPE;
@@ -1574,7 +2097,9 @@ int tmol_b200_ljlk_plan_create(const tmol_b200_ljlk_inputs* in, int real_bytes,
   const int T = in->n_atom_types;
   if (P < 0 || B < 0 || nbt < 0 || A < 0 || C < 0 || T < 0 || in->n_atoms < 0)
     return TMOL_B200_ERR_SHAPE;
-  if (C > MAX_CONN || B >= 65536 || in->n_rots != P * B) return TMOL_B200_ERR_SHAPE;
+  if (C > MAX_CONN || B >= 65536) return TMOL_B200_ERR_SHAPE;
+  if (rotamers ? in->n_rots < 0 : in->n_rots != P * B) return TMOL_B200_ERR_SHAPE;
+  if (rotamers && P * B > 0 && !in->n_rots_for_block) return TMOL_B200_ERR_INVALID_ARGUMENT;
   if (nt * TILE < A) return TMOL_B200_ERR_SHAPE;
   if (in->n_atoms >= ((int64_t)1 << 31)) return TMOL_B200_ERR_SHAPE;
   const void* req[] = {in->rot_coord_offset, in->first_rot_block_type, in->block_ind_for_rot,
@@ -1658,6 +2183,35 @@ int tmol_b200_ljlk_plan_create(const tmol_b200_ljlk_inputs* in, int real_bytes,
   a.cp_minsep = pl->cp_minsep;
   a.cp_seps = pl->cp_seps;
   a.status = pl->counters + 1;
+  a.rotamers = rotamers ? 1 : 0;
+  a.rot_bt = a.rot_off = a.rot_block = a.rot_pose = nullptr;
+  if (rotamers) {
+    const int R = in->n_rots;
+    pl->rotamers = true;
+    pl->R = R;
+    PCK(dalloc(pl, &pl->rot_bt, R));
+    PCK(dalloc(pl, &pl->rot_off, R));
+    PCK(dalloc(pl, &pl->rot_block, R));
+    PCK(dalloc(pl, &pl->rot_pose, R));
+    PCK(dalloc(pl, &pl->nrb, PB));
+    PCK(dalloc(pl, &pl->rob, PB));
+    PCK(dalloc(pl, (unsigned char**)&pl->rot_spheres, (size_t)R * 4 * real_bytes));
+    PCK(dalloc(pl, &pl->row_pairs, PB + 2));
+    PCK(dalloc(pl, &pl->row_items, PB));
+    if (PB > 0) {
+      PCK(cudaMemcpyAsync(pl->nrb, in->n_rots_for_block, sizeof(int) * PB, cudaMemcpyDeviceToDevice, st));
+      PCK(cudaMemcpyAsync(pl->rob, in->rot_offset_for_block, sizeof(int) * PB, cudaMemcpyDeviceToDevice, st));
+    }
+    a.rot_bt = pl->rot_bt;
+    a.rot_off = pl->rot_off;
+    a.rot_block = pl->rot_block;
+    a.rot_pose = pl->rot_pose;
+    if (R > 0) {
+      int gr = std::max(1, std::min((R + 255) / 256, pl->n_sm * 8));
+      plan_rotamers_kernel<<<gr, 256, 0, st>>>(a);
+      PCK(cudaGetLastError());
+    }
+  }
   int g = std::max(1, std::min<int>((int)((PB + 255) / 256), pl->n_sm * 8));
   if (PB > 0) {
     plan_blocks_kernel<<<g, 256, 0, st>>>(a);
@@ -1745,7 +2299,7 @@ int tmol_b200_ljlk_plan_create(const tmol_b200_ljlk_inputs* in, int real_bytes,
     free_plan(pl);
     return rc;
   }
-  rc = build_work(pl, st);
+  rc = rotamers ? TMOL_B200_OK : build_work(pl, st);
   if (rc != TMOL_B200_OK) {
     free_plan(pl);
     return rc;
@@ -1754,6 +2308,22 @@ int tmol_b200_ljlk_plan_create(const tmol_b200_ljlk_inputs* in, int real_bytes,
 #undef PCK
   *plan_out = pl;
   return TMOL_B200_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tmol_b200_ljlk_plan_create(const tmol_b200_ljlk_inputs* in, int real_bytes,
+                               const tmol_b200_ljlk_launch* launch,
+                               void* stream, tmol_b200_ljlk_plan** plan_out) {
+  return create_plan(in, real_bytes, launch, stream, false, plan_out);
+}
+
+int tmol_b200_ljlk_rotamer_plan_create(const tmol_b200_ljlk_inputs* in, int real_bytes,
+                                       const tmol_b200_ljlk_launch* launch,
+                                       void* stream, tmol_b200_ljlk_plan** plan_out) {
+  return create_plan(in, real_bytes, launch, stream, true, plan_out);
 }
 
 int tmol_b200_ljlk_plan_destroy(tmol_b200_ljlk_plan* plan) {
@@ -1775,7 +2345,8 @@ int tmol_b200_ljlk_plan_set_launch(tmol_b200_ljlk_plan* plan,
 int tmol_b200_ljlk_forward(tmol_b200_ljlk_plan* plan, const void* coords,
                            int block_pair, void* energies,
                            int32_t* block_neighbors, void* stream) {
-  if (!plan || !energies || (!coords && plan->N > 0)) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  if (!plan || !energies || (!coords && plan->N > 0) || plan->rotamers)
+    return TMOL_B200_ERR_INVALID_ARGUMENT;
   cudaStream_t st = (cudaStream_t)stream;
   if (plan->real_bytes == 4)
     return forward_impl<float>(plan, coords, block_pair, energies, block_neighbors, st);
@@ -1785,7 +2356,7 @@ int tmol_b200_ljlk_forward(tmol_b200_ljlk_plan* plan, const void* coords,
 int tmol_b200_ljlk_backward(tmol_b200_ljlk_plan* plan, const void* coords,
                             int block_pair, const void* dTdV, void* dcoords,
                             void* stream) {
-  if (!plan || !dTdV || !dcoords || (!coords && plan->N > 0))
+  if (!plan || !dTdV || !dcoords || (!coords && plan->N > 0) || plan->rotamers)
     return TMOL_B200_ERR_INVALID_ARGUMENT;
   cudaStream_t st = (cudaStream_t)stream;
   if (plan->real_bytes == 4)
@@ -1797,7 +2368,7 @@ int tmol_b200_ljlk_energy_and_gradient(tmol_b200_ljlk_plan* plan,
                                        const void* coords, const void* weights,
                                        void* energies, void* dcoords,
                                        void* stream) {
-  if (!plan || !weights || !energies || !dcoords || (!coords && plan->N > 0))
+  if (!plan || !weights || !energies || !dcoords || (!coords && plan->N > 0) || plan->rotamers)
     return TMOL_B200_ERR_INVALID_ARGUMENT;
   cudaStream_t st = (cudaStream_t)stream;
   if (plan->real_bytes == 4)
@@ -1932,6 +2503,55 @@ int tmol_b200_ljlk_screen_candidates(tmol_b200_ljlk_plan* plan,
                                                      pair_b2, pair_bt, features, count);
   CK(cudaGetLastError());
   return TMOL_B200_OK;
+}
+
+int tmol_b200_ljlk_rotamer_count(tmol_b200_ljlk_plan* plan, const void* coords,
+                                  int64_t* n_pairs, int64_t* n_items, void* stream) {
+  if (!plan || !plan->rotamers || !n_pairs || !n_items || (!coords && plan->N > 0))
+    return TMOL_B200_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->real_bytes == 4) return rotamer_count_impl<float>(plan, coords, n_pairs, n_items, st);
+  return rotamer_count_impl<double>(plan, coords, n_pairs, n_items, st);
+}
+
+int tmol_b200_ljlk_rotamer_fill(tmol_b200_ljlk_plan* plan, int32_t* indices, int32_t* items,
+                                void* stream) {
+  if (!plan || !plan->rotamers || plan->n_pairs < 0) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  if ((plan->n_pairs > 0 && !indices) || (plan->n_items > 0 && !items))
+    return TMOL_B200_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->real_bytes == 4) return rotamer_fill_impl<float>(plan, indices, items, st);
+  return rotamer_fill_impl<double>(plan, indices, items, st);
+}
+
+int tmol_b200_ljlk_rotamer_forward(tmol_b200_ljlk_plan* plan, const void* coords,
+                                    const int32_t* items, int64_t n_items, int64_t n_pairs,
+                                    void* energies, void* stream) {
+  if (!plan || !plan->rotamers || !energies || n_items < 0 || n_pairs < 0 ||
+      (n_items > 0 && !items) || (!coords && plan->N > 0))
+    return TMOL_B200_ERR_INVALID_ARGUMENT;
+  if (n_items >= ((int64_t)1 << 31) || n_pairs >= ((int64_t)1 << 31)) return TMOL_B200_ERR_CAPACITY;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->real_bytes == 4)
+    return rotamer_score_impl<float, false>(plan, coords, items, n_items, n_pairs, energies, nullptr,
+                                            nullptr, st);
+  return rotamer_score_impl<double, false>(plan, coords, items, n_items, n_pairs, energies, nullptr,
+                                           nullptr, st);
+}
+
+int tmol_b200_ljlk_rotamer_backward(tmol_b200_ljlk_plan* plan, const void* coords,
+                                     const int32_t* items, int64_t n_items, int64_t n_pairs,
+                                     const void* dTdV, void* dcoords, void* stream) {
+  if (!plan || !plan->rotamers || !dTdV || !dcoords || n_items < 0 || n_pairs < 0 ||
+      (n_items > 0 && !items) || (!coords && plan->N > 0))
+    return TMOL_B200_ERR_INVALID_ARGUMENT;
+  if (n_items >= ((int64_t)1 << 31) || n_pairs >= ((int64_t)1 << 31)) return TMOL_B200_ERR_CAPACITY;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->real_bytes == 4)
+    return rotamer_score_impl<float, true>(plan, coords, items, n_items, n_pairs, nullptr, dTdV,
+                                           dcoords, st);
+  return rotamer_score_impl<double, true>(plan, coords, items, n_items, n_pairs, nullptr, dTdV,
+                                          dcoords, st);
 }
 
 int64_t tmol_b200_ljlk_plan_device_bytes(const tmol_b200_ljlk_plan* plan) {

@@ -126,6 +126,17 @@ SIGNATURES = {
         ],
     ),
     "tmol_b200_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    # rotamer scoring
+    "tmol_b200_ljlk_rotamer_plan_create": (
+        ctypes.c_int,
+        [ctypes.POINTER(Inputs), ctypes.c_int, ctypes.POINTER(Launch), ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)],
+    ),
+    "tmol_b200_ljlk_rotamer_count": (
+        ctypes.c_int, [_V, _V, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64), _V]
+    ),
+    "tmol_b200_ljlk_rotamer_fill": (ctypes.c_int, [_V, _V, _V, _V]),
+    "tmol_b200_ljlk_rotamer_forward": (ctypes.c_int, [_V, _V, _V, _I64, _I64, _V, _V]),
+    "tmol_b200_ljlk_rotamer_backward": (ctypes.c_int, [_V, _V, _V, _I64, _I64, _V, _V, _V]),
     # learned block-pair screen (include/tmol_b200_screen.h)
     "tmol_b200_ljlk_plan_set_skip_mask": (ctypes.c_int, [_V, _V, _I32]),
     "tmol_b200_ljlk_screen_candidates": (ctypes.c_int, [_V, _V, _I32, _V, _V, _V, _V, _V, _V]),

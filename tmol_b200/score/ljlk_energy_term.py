@@ -14,7 +14,7 @@ import torch
 from ..chem.restypes import ChemicalDatabase
 from .ljlk_params import global_params_tensor, type_params_tensor
 from .score_types import ScoreType
-from .scoring_module import TermBlockPairScoringModule, TermWholePoseScoringModule
+from .scoring_module import TermBlockPairScoringModule, TermRotamerScoringModule, TermWholePoseScoringModule
 
 
 class LJLKEnergyTerm:
@@ -70,6 +70,21 @@ class LJLKEnergyTerm:
         from .ljlk_op import ljlk_pose_scores
 
         return ljlk_pose_scores
+
+    def get_rotamer_score_term_function(self):
+        from .ljlk_op import ljlk_rotamer_scores
+
+        return ljlk_rotamer_scores
+
+    def render_rotamer_scoring_module(self, pose_stack, rotamer_set):
+        """tmol ``energy_term.py:132-147``: the rotamer-pair scoring module
+        over ``rotamer_set`` (see ``tmol_b200.pose.rotamers``)."""
+        return TermRotamerScoringModule(
+            self.class_name(),
+            rotamer_set,
+            self.get_score_term_attributes(pose_stack),
+            self.get_rotamer_score_term_function(),
+        )
 
     def get_score_term_attributes(self, pose_stack):
         self.setup_poses(pose_stack)

@@ -24,9 +24,11 @@ N_STATIC = 26  # arguments after coords, before the output-mode flag
 
 
 class LJLKPlan:
-    """Owns one ``tmol_b200_ljlk_plan``."""
+    """Owns one ``tmol_b200_ljlk_plan``: of the pose op (one rotamer per
+    block) or, with ``rotamers=True``, of the rotamer op (any number of
+    rotamers per block)."""
 
-    def __init__(self, coords_like, static_args, launch=None):
+    def __init__(self, coords_like, static_args, launch=None, rotamers=False):
         (
             rot_coord_offset,
             pose_ind_for_atom,
@@ -128,11 +130,12 @@ class LJLKPlan:
         self.n_atoms = pose_ind_for_atom.shape[0]
         s.n_atoms = self.n_atoms
         self.launch = native.Launch(*(launch or (0, 0, 0, 0)))
+        self.rotamers = bool(rotamers)
         ptr = ctypes.c_void_p()
         with torch.cuda.device(device):
             stream = torch.cuda.current_stream(device).cuda_stream
             native.call(
-                "tmol_b200_ljlk_plan_create",
+                "tmol_b200_ljlk_rotamer_plan_create" if rotamers else "tmol_b200_ljlk_plan_create",
                 ctypes.byref(s),
                 4 if self.dtype == torch.float32 else 8,
                 ctypes.byref(self.launch),
@@ -245,6 +248,52 @@ class LJLKPlan:
         native.call("tmol_b200_ljlk_last_counts", self.ptr, self._stream(), arr)
         return dict(zip(self.COUNT_NAMES, list(arr)))
 
+    # -- rotamer plans ----------------------------------------------------
+
+    def rotamer_dispatch(self, coords):
+        """The rotamer pairs the op scores at ``coords``: (indices [3, n]
+        int32 (pose, rot1, rot2), work items [n_items, 4] int32).
+        Synchronises the current stream once (the counts size the output)."""
+        self._check_coords(coords)
+        coords = coords.contiguous()
+        n_pairs, n_items = ctypes.c_int64(), ctypes.c_int64()
+        native.call(
+            "tmol_b200_ljlk_rotamer_count", self.ptr, ctypes.c_void_p(coords.data_ptr()),
+            ctypes.byref(n_pairs), ctypes.byref(n_items), self._stream(),
+        )
+        indices = torch.empty((3, n_pairs.value), dtype=torch.int32, device=self.device)
+        items = torch.empty((n_items.value, 4), dtype=torch.int32, device=self.device)
+        native.call(
+            "tmol_b200_ljlk_rotamer_fill", self.ptr, ctypes.c_void_p(indices.data_ptr() if n_pairs.value else 0),
+            ctypes.c_void_p(items.data_ptr() if n_items.value else 0), self._stream(),
+        )
+        return indices, items
+
+    def rotamer_forward(self, coords, items, n_pairs):
+        """Energies [3, n_pairs] of the dispatched rotamer pairs."""
+        self._check_coords(coords)
+        coords = coords.contiguous()
+        energies = torch.empty((3, n_pairs), dtype=self.dtype, device=self.device)
+        native.call(
+            "tmol_b200_ljlk_rotamer_forward", self.ptr, ctypes.c_void_p(coords.data_ptr()),
+            ctypes.c_void_p(items.data_ptr() if items.numel() else 0), items.shape[0], n_pairs,
+            ctypes.c_void_p(energies.data_ptr()), self._stream(),
+        )
+        return energies
+
+    def rotamer_backward(self, coords, items, dTdV):
+        """dL/dcoords from dL/dE [3, n_pairs]."""
+        self._check_coords(coords)
+        coords = coords.contiguous()
+        dTdV = dTdV.to(self.dtype).contiguous()
+        dcoords = torch.empty_like(coords)
+        native.call(
+            "tmol_b200_ljlk_rotamer_backward", self.ptr, ctypes.c_void_p(coords.data_ptr()),
+            ctypes.c_void_p(items.data_ptr() if items.numel() else 0), items.shape[0], dTdV.shape[1],
+            ctypes.c_void_p(dTdV.data_ptr()), ctypes.c_void_p(dcoords.data_ptr()), self._stream(),
+        )
+        return dcoords
+
     def skip_mask_words(self):
         """32-bit words per (pose, block) row of a skip mask."""
         return (self.max_n_blocks + 31) // 32
@@ -346,13 +395,13 @@ def _plan_key(coords, static):
     return tuple(parts)
 
 
-def get_plan(coords, static):
-    key = _plan_key(coords, static)
+def get_plan(coords, static, rotamers=False):
+    key = (rotamers,) + _plan_key(coords, static)
     entry = _PLAN_CACHE.get(key)
     if entry is not None:
         _PLAN_CACHE.move_to_end(key)
         return entry[0]
-    plan = LJLKPlan(coords, static)
+    plan = LJLKPlan(coords, static, rotamers=rotamers)
     # the static tensors are held so that their addresses cannot be reused
     # by other tensors while the key is cached
     _PLAN_CACHE[key] = (plan, [t for t in static if isinstance(t, torch.Tensor)])
@@ -378,3 +427,39 @@ def ljlk_pose_scores(coords, *args, return_block_neighbors=True):
 def pose_scores_with_plan(coords, plan, block_pair=False, return_block_neighbors=False):
     scores, nbr = _ScoreFn.apply(coords, plan, block_pair, return_block_neighbors)
     return scores, (nbr if return_block_neighbors else None)
+
+
+class _RotamerScoreFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, coords, plan):
+        indices, items = plan.rotamer_dispatch(coords)
+        energies = plan.rotamer_forward(coords, items, indices.shape[1])
+        ctx.plan = plan
+        ctx.save_for_backward(coords, items)
+        ctx.mark_non_differentiable(indices)
+        return energies, indices
+
+    @staticmethod
+    def backward(ctx, dE, _dindices):
+        coords, items = ctx.saved_tensors
+        if dE is None:
+            return None, None
+        return ctx.plan.rotamer_backward(coords, items, dE), None
+
+
+def ljlk_rotamer_scores(coords, *args):
+    """Drop-in for ``torch.ops.tmol_ljlk.ljlk_rotamer_scores``
+    (``tmol/score/ljlk/potentials/compiled.ops.cpp:599-662``): the rotamer
+    set's coordinates and the op's 26 further arguments (the last,
+    ``output_block_pair_energies``, must be True as tmol's rotamer scoring
+    module passes it).  Returns ``(scores [3, n], indices [3, n])``: the
+    energies of every rotamer pair of neighbouring blocks and of every
+    rotamer with itself, and their (pose, rot1, rot2); gradients flow to
+    ``coords``."""
+    if len(args) != N_STATIC:
+        raise TypeError(f"ljlk_rotamer_scores takes coords and {N_STATIC} further arguments")
+    static, block_pair = args[:-1], args[-1]
+    if not block_pair:
+        raise ValueError("rotamer scoring reports rotamer-pair energies (output_block_pair_energies=True)")
+    plan = get_plan(coords.reshape(-1, 3), static, rotamers=True)
+    return _RotamerScoreFn.apply(coords.reshape(-1, 3), plan)
