@@ -43,6 +43,12 @@ UNEVEN_POSES = 256
 UNEVEN_SEED = 2
 PERTURB_SD = 0.05
 L2_FLUSH_BYTES = 256 << 20
+# the rotamer workload: 16 poses x 150 residues, every block with 1..31
+# rotamers (the native one first; chis resampled, a quarter mutated)
+ROT_POSES = 16
+ROT_RES = 150
+ROT_SET = dict(max_rots=31, mutate_fraction=0.25, seed=9)
+ROT_METRIC = "LJ+LK rotamer-pair energies/s (16 poses x 150 residues, 1-31 rotamers per block, 1 B200)"
 
 # Algorithmic FLOPs per unit (E + dE), counted on the restatement's most
 # populated branch (far cubic fade, 4.5-6 A); FMA = 2, div/sqrt/exp/floor = 1.
@@ -68,6 +74,18 @@ def workload(rank, name="uniform64x150", device="cpu"):
 
     sizes, seeds = workload_sizes(name, rank)
     return synthetic_pose_stack(sizes, seeds, device=device)
+
+
+def rotamer_workload(rank, device, sizes=None, seeds=None):
+    from tmol_b200.pose.rotamers import synthetic_rotamer_set
+    from tmol_b200.pose.synthetic import synthetic_pose_stack
+
+    if sizes is None:
+        sizes = [ROT_RES] * ROT_POSES
+        seeds = [7000 + rank * ROT_POSES + k for k in range(ROT_POSES)]
+    ps = synthetic_pose_stack(sizes, seeds, device=device)
+    rs = synthetic_rotamer_set(ps, pose_seeds=seeds, **ROT_SET)
+    return ps, rs, sizes, seeds
 
 
 def workload_label(name):
@@ -249,6 +267,29 @@ def _ref_worker(conn, sizes, seeds):
         conn.send(time.perf_counter() - t0)
 
 
+def _ref_rot_worker(conn, sizes, seeds):
+    """One single-threaded process of the rotamer reference arm."""
+    import torch
+
+    torch.set_num_threads(1)
+    from oracle import oracle as O
+    from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm, rotamer_score_args
+
+    ps, rs, _, _ = rotamer_workload(0, "cpu", sizes, seeds)
+    args = rotamer_score_args(ps, rs, LJLKEnergyTerm())
+    conn.send("ready")
+    while True:
+        msg = conn.recv()
+        if msg is None:
+            break
+        t0 = time.perf_counter()
+        if O.reference_available():
+            O.reference_rotamer_scores(rs.coords, args, require_gradient=False)
+        else:
+            O.OracleCall(rs.coords, args).rotamer_scores()
+        conn.send(time.perf_counter() - t0)
+
+
 def run_reference(args, world, rank):
     """tmol's CPU op on all host cores: one process per core, poses dealt
     out longest-first so that every process gets a similar share."""
@@ -258,6 +299,8 @@ def run_reference(args, world, rank):
 
     if rank != 0:
         return 0
+    if args.workload == "rotamers16x150":
+        return run_reference_rotamers(args)
     sizes, seeds = workload_sizes(args.workload, 0)
     n_poses = len(sizes)
     n_proc = min(os.cpu_count() or 1, n_poses)
@@ -323,6 +366,232 @@ def run_reference(args, world, rank):
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def run_reference_rotamers(args):
+    """tmol's CPU rotamer op, one process per pose (energies of every
+    rotamer pair, as the packer asks for them)."""
+    import multiprocessing as mp
+
+    from oracle import oracle as O
+
+    sizes = [ROT_RES] * ROT_POSES
+    seeds = [7000 + k for k in range(ROT_POSES)]
+    n_proc = min(os.cpu_count() or 1, ROT_POSES)
+    shares = [list(range(q, ROT_POSES, n_proc)) for q in range(n_proc)]
+    ctx = mp.get_context("spawn")
+    workers = []
+    for share in shares:
+        parent, child = ctx.Pipe()
+        pr = ctx.Process(target=_ref_rot_worker, args=(child, [sizes[k] for k in share], [seeds[k] for k in share]))
+        pr.start()
+        workers.append((pr, parent))
+    for _, c in workers:
+        c.recv()
+
+    def step():
+        t0 = time.perf_counter()
+        for _, c in workers:
+            c.send(1)
+        for _, c in workers:
+            c.recv()
+        return time.perf_counter() - t0
+
+    for _ in range(max(args.warmup, 1)):
+        step()
+    times = [step() for _ in range(args.steps)]
+    for pr, c in workers:
+        c.send(None)
+        pr.join()
+    # the same batch's pair count, for the unit
+    import torch
+
+    from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm, rotamer_score_args
+
+    ps, rs, _, _ = rotamer_workload(0, "cpu", sizes, seeds)
+    n_pairs = O.OracleCall(rs.coords, rotamer_score_args(ps, rs, LJLKEnergyTerm())).rotamer_scores()[0].shape[1]
+    t = sum(times)
+    value = n_pairs * args.steps / t
+    kind = "reference" if O.reference_available() else "port"
+    line = {
+        "impl": "reference",
+        "metric": ROT_METRIC,
+        "value": value,
+        "unit": "rotamer pairs/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * t / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded proteins and rotamers, ideal geometry)",
+        "config": {"workload": "16 poses x 150 residues, 1-31 rotamers per block, energies", "rotamer_pairs": n_pairs},
+        "cpu_baseline": {
+            "value": value,
+            "unit": "rotamer pairs/s",
+            "cores": n_proc,
+            "kind": kind,
+            "sample": f"the full 16-pose batch per step, one pose per single-threaded process ({n_proc} processes)",
+        },
+        "e2e": {"value": value, "unit": "rotamer pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    del torch
+    return 0
+
+
+def run_rotamers(args, world, rank, local):
+    """Rotamer scoring (tmol's ljlk_rotamer_scores): per step the op's full
+    call, dispatch (rotamer and block spheres, neighbour blocks, pair list:
+    one host synchronisation to size the output) and the energies of every
+    rotamer pair of neighbouring blocks."""
+    import torch
+
+    from tmol_b200 import native
+    from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm, rotamer_score_args
+    from tmol_b200.score.ljlk_op import LJLKPlan
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    ps, rs, sizes, seeds = rotamer_workload(rank, dev)
+    rargs = rotamer_score_args(ps, rs, LJLKEnergyTerm(device=dev))
+    coords = rs.coords.contiguous()
+    plan = LJLKPlan(coords, rargs[:-1], rotamers=True, launch=(1, 8, 2, 32))
+    flush = torch.empty(L2_FLUSH_BYTES // 4, device=dev, dtype=torch.float32)
+
+    def op():
+        idx, items = plan.rotamer_dispatch(coords)
+        return plan.rotamer_forward(coords, items, idx.shape[1]), idx, items
+
+    for _ in range(max(args.warmup, 3)):
+        E, idx, items = op()
+    torch.cuda.synchronize()
+    n_pairs = idx.shape[1]
+    counts = plan.last_counts()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record()
+            op()
+            ev[k][1].record()
+        torch.cuda.synchronize()
+    barrier(world)
+    ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), world)
+    value = sum_over_ranks(n_pairs * args.steps, world) / (ms / 1e3)
+    # energies alone (a fixed pair list, as a packer reuses it): graph replays
+    energies = torch.empty((3, n_pairs), device=dev)
+
+    def energies_only():
+        native.call(
+            "tmol_b200_ljlk_rotamer_forward", plan.ptr, ctypes_ptr(coords), ctypes_ptr(items), items.shape[0],
+            n_pairs, ctypes_ptr(energies), plan._stream(),
+        )
+
+    e_ms = time_replays(energies_only, args.steps, flush) / args.steps
+    # end to end: host coordinates in, energies and pair indices out
+    h_coords = coords.cpu().pin_memory()
+    d_in = torch.empty_like(coords)
+    e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    d2h = 0
+    for k in range(args.steps):
+        flush.zero_()
+        e2e_ev[k][0].record()
+        d_in.copy_(h_coords, non_blocking=True)
+        idx2, items2 = plan.rotamer_dispatch(d_in)
+        E2 = plan.rotamer_forward(d_in, items2, idx2.shape[1])
+        hE, hI = E2.cpu(), idx2.cpu()
+        d2h = hE.numel() * 4 + hI.numel() * 4
+        e2e_ev[k][1].record()
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in e2e_ev), world)
+    fp32_peak = native.measure_fp32_peak_tflops(torch.cuda.current_stream().cuda_stream)
+    flops = counts["atom_pairs"] * F_PAIR_TEST + counts["atom_pairs_in_range"] * F_LJ + counts["heavy_pairs_in_range"] * F_LK
+    achieved = flops / (e_ms * 1e-3) / 1e12
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        ps0, rs0, _, _ = rotamer_workload(0, "cpu", sizes[:1], seeds[:1])
+        a0 = rotamer_score_args(ps0, rs0, LJLKEnergyTerm())
+        torch.set_num_threads(1)
+        best = float("inf")
+        for _ in range(2):
+            t0 = time.perf_counter()
+            if O.reference_available():
+                E0, _, _ = O.reference_rotamer_scores(rs0.coords, a0, require_gradient=False)
+            else:
+                E0 = torch.tensor(O.OracleCall(rs0.coords, a0).rotamer_scores()[0])
+            best = min(best, time.perf_counter() - t0)
+        cpu = {
+            "value": E0.shape[1] / best,
+            "unit": "rotamer pairs/s",
+            "cores": 1,
+            "kind": "reference" if O.reference_available() else "port",
+            "sample": "pose 0 of the batch (all its rotamer pairs), one thread, best of 2",
+        }
+    if rank == 0:
+        line = {
+            "metric": ROT_METRIC,
+            "value": value,
+            "unit": "rotamer pairs/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded proteins and rotamers, ideal geometry)",
+            "config": {
+                "workload": "16 poses x 150 residues, 1-31 rotamers per block, energies of every rotamer pair",
+                "rotamers": int(rs.n_rotamers_total),
+                "rotamer_pairs": n_pairs,
+                "l2": "flushed (256 MiB write) before every timed step",
+                "parallelism": f"weak, {world} independent batch(es)",
+            },
+            "atom_pairs_per_s": counts["atom_pairs"] * args.steps * world / (ms / 1e3),
+            "energies_only_ms_per_step": e_ms,
+            "work_per_step": counts,
+            "gpu_launches": 7 * args.steps,
+            "clocks": clk.summary(),
+            "roofline": {
+                "bound": "fp32",
+                "achieved": achieved,
+                "peak": fp32_peak,
+                "unit": "TFLOP/s",
+                "frac": achieved / fp32_peak,
+                "traffic": None,
+                "kernel": "rotamer_kernel<float, energies> (+ rotamer spheres), timed as graph replays",
+                "kernel_ms": e_ms,
+                "flops_per_launch": flops,
+                "peak_source": "measured: FMA-loop probe over all SMs in this run (tmol_b200_measure_fp32_peak)",
+            },
+            "e2e": {
+                "value": sum_over_ranks(n_pairs * args.steps, world) / (e2e_ms / 1e3),
+                "unit": "rotamer pairs/s",
+                "h2d_bytes_per_step": coords.numel() * 4,
+                "d2h_bytes_per_step": d2h,
+            },
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+def ctypes_ptr(t):
+    import ctypes
+
+    return ctypes.c_void_p(t.data_ptr())
 
 
 def flops_per_step(counts):
@@ -673,7 +942,7 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="uniform64x150", choices=["uniform64x150", "uneven256"])
+    ap.add_argument("--workload", default="uniform64x150", choices=["uniform64x150", "uneven256", "rotamers16x150"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-screen", action="store_true", help="skip the learned-screen measurement")
     ap.add_argument(
@@ -688,6 +957,8 @@ def main():
         rank = int(os.environ.get("RANK", "0"))
         return run_reference(args, world, rank)
     world, rank, local = dist_setup()
+    if args.workload == "rotamers16x150":
+        return run_rotamers(args, world, rank, local)
     return run_b200(args, world, rank, local)
 
 

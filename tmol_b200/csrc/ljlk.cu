@@ -1480,6 +1480,11 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
           ec.wt2 = s.dTdV[2 * np + d];
         }
         E3<Real> e = {0, 0, 0};
+        if (ti == 0) {
+          const long long n2a = diag ? 0 : s.bt_n_atoms[ra.rot_bt[rot2_first + k]];
+          cnt_add(w.counts, 0, 1, lane);
+          cnt_add(w.counts, 1, diag ? (long long)r.n1 * (r.n1 - 1) / 2 : (long long)r.n1 * n2a, lane);
+        }
         if (diag) {
           // this tile with itself, then with the rotamer's later tiles
           E3<Real> t = intra_tile<Real, GRAD>(ec, &w, r.st1, r.c1, lane);
@@ -1549,6 +1554,9 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
       __syncwarp();
     }
   }
+  __syncwarp();
+  if (s.counts && lane < N_COUNTS && w.counts[lane])
+    atomicAdd(&s.counts[lane], w.counts[lane]);
 }
 
 // Sub-spheres of every block for the screen's features: atoms [0, 4) (the
@@ -2046,7 +2054,8 @@ int rotamer_score_impl(tmol_b200_ljlk_plan* pl, const void* coords, const int32_
   s.energies = (Real*)energies;
   s.dTdV = (const Real*)dTdV;
   s.dcoords = (Real*)dcoords;
-  s.counts = nullptr;
+  s.counts = GRAD ? nullptr : pl->counts;
+  if (!GRAD) CK(cudaMemsetAsync(pl->counts, 0, N_COUNTS * sizeof(unsigned long long), st));
   if (energies) CK(cudaMemsetAsync(energies, 0, (size_t)3 * n_pairs * sizeof(Real), st));
   if (dcoords) CK(cudaMemsetAsync(dcoords, 0, (size_t)pl->N * 3 * sizeof(Real), st));
   if (n_items == 0) return TMOL_B200_OK;

@@ -88,11 +88,14 @@ def rotamer_set_from_arrays(block_ind_for_rot, pose_for_rot, bt_for_rot, rot_coo
 
 
 def synthetic_rotamer_set(pose_stack, max_rots=4, mutate_fraction=0.25, seed=0, chi_sd=10.0,
-                          skip_fraction=0.0):
+                          skip_fraction=0.0, pose_seeds=None):
     """Seeded rotamers for every block of ``pose_stack`` (a single-chain
     PoseStack from ``tmol_b200.pose``): 1..max_rots per block, the native
     placement first.  With ``skip_fraction``, that fraction of blocks gets
-    no rotamers at all (a block absent from the packing problem)."""
+    no rotamers at all (a block absent from the packing problem).  One
+    random stream serves the whole stack, or, with ``pose_seeds``, pose p
+    has its own (seeded by ``(seed, pose_seeds[p])``), so that any subset of
+    poses gets the same rotamers as the whole batch."""
     rng = numpy.random.default_rng(seed)
     pbt = pose_stack.packed_block_types
     bts = pbt.active_block_types
@@ -101,7 +104,10 @@ def synthetic_rotamer_set(pose_stack, max_rots=4, mutate_fraction=0.25, seed=0, 
     offs = pose_stack.block_coord_offset.detach().cpu().numpy()
     P, B = bti.shape
     block_ind, pose_for, bt_for, rot_xyz = [], [], [], []
+    builds = {}  # block-type name -> [(rotamer index, frame, chis)]; built per type at once
     for p in range(P):
+        if pose_seeds is not None:
+            rng = numpy.random.default_rng([seed, int(pose_seeds[p])])
         for b in range(B):
             if bti[p, b] < 0 or rng.random() < skip_fraction:
                 continue
@@ -113,14 +119,14 @@ def synthetic_rotamer_set(pose_stack, max_rots=4, mutate_fraction=0.25, seed=0, 
             bt_for.append(int(bti[p, b]))
             rot_xyz.append(native)
             ia = bt.atom_index
-            n_pos, ca_pos, c_pos = (native[ia[a]][None] for a in ("N", "CA", "C"))
-            down = up = None
+            n_pos, ca_pos, c_pos = (native[ia[a]] for a in ("N", "CA", "C"))
+            down, up = n_pos, c_pos
             if b > 0 and bti[p, b - 1] >= 0:
                 prev = bts[bti[p, b - 1]]
-                down = X[p, offs[p, b - 1] + prev.atom_index["C"]][None]
+                down = X[p, offs[p, b - 1] + prev.atom_index["C"]]
             if b + 1 < B and bti[p, b + 1] >= 0:
                 nxt = bts[bti[p, b + 1]]
-                up = X[p, offs[p, b + 1] + nxt.atom_index["N"]][None]
+                up = X[p, offs[p, b + 1] + nxt.atom_index["N"]]
             for _ in range(n - 1):
                 rbt = bt
                 if rng.random() < mutate_fraction:
@@ -129,13 +135,16 @@ def synthetic_rotamer_set(pose_stack, max_rots=4, mutate_fraction=0.25, seed=0, 
                     cand = [t for t in base if _variant_suffix(t.name) == _variant_suffix(bt.name)]
                     if cand:
                         rbt = cand[0]
-                chis = rng.choice([-60.0, 60.0, 180.0], size=(1, 4)) + rng.normal(0.0, chi_sd, (1, 4))
-                xyz = build_residue_coords(
-                    rbt, n_pos, ca_pos, c_pos,
-                    down if down is not None else n_pos, up if up is not None else c_pos, chis,
-                )[0]
+                chis = rng.choice([-60.0, 60.0, 180.0], size=4) + rng.normal(0.0, chi_sd, 4)
+                builds.setdefault(rbt.name, []).append((len(rot_xyz), (n_pos, ca_pos, c_pos, down, up), chis))
                 block_ind.append(b)
                 pose_for.append(p)
                 bt_for.append(pbt.bt_index[rbt.name])
-                rot_xyz.append(xyz)
+                rot_xyz.append(None)
+    for name, specs in builds.items():
+        frames = [numpy.stack([f[k] for _, f, _ in specs]) for k in range(5)]
+        chis = numpy.stack([c for _, _, c in specs])
+        xyz = build_residue_coords(bts[pbt.bt_index[name]], *frames, chis)
+        for (r, _, _), x in zip(specs, xyz):
+            rot_xyz[r] = x
     return rotamer_set_from_arrays(block_ind, pose_for, bt_for, rot_xyz, P, B, pose_stack.device)

@@ -109,7 +109,9 @@ class TermRotamerScoringModule(torch.nn.Module):
         scores, indices = self.forward(coords)
         return torch.stack(
             [
-                torch.sparse_coo_tensor(indices, scores[t], size=(self.n_poses, self.n_rots, self.n_rots))
+                torch.sparse_coo_tensor(
+                    indices, scores[t], size=(self.n_poses, self.n_rots, self.n_rots), check_invariants=True
+                )
                 for t in range(scores.shape[0])
             ]
         )
