@@ -144,3 +144,38 @@ def test_exotic_blocks_against_oracle(term, block_pair):
         pose = ps.pose_ind_for_atom.numpy()
         go = (dVo * w[:, pose][:, :, None]).sum(0)
     g_close(g, go)
+
+
+def test_coincident_atoms_and_an_empty_pose(synthetic_pose_stack_golden, term):
+    """Two atoms of different blocks on the same point (d = 0: the linear LJ
+    and flat LK regions, no force) and a pose whose blocks are all absent
+    (no energy, no gradient), against the oracle."""
+    ps = synthetic_pose_stack_golden
+    args = list(pose_score_args(ps, term))
+    coords = ps.coords.clone()
+    offs = ps.block_coord_offset
+    coords[4, offs[4, 30]] = coords[4, offs[4, 10]]
+    coords[4, offs[4, 31] + 2] = coords[4, offs[4, 12] + 3]
+    # pose 1: every block absent
+    first_bt = args[3].clone()
+    first_bt[1] = -1
+    bt_for_rot = args[6].clone().view(ps.n_poses, -1)
+    bt_for_rot[1] = -1
+    args[3] = first_bt
+    args[6] = bt_for_rot.reshape(-1)
+    flat = coords.flatten(0, 1)
+    oc = O.OracleCall(flat, args)
+    Eo, dVo, nbro = oc.pose_scores(require_gradient=True)
+    gpu_args = [a.to(DEV) if isinstance(a, torch.Tensor) else a for a in args]
+    c = flat.to(DEV).requires_grad_(True)
+    E, nbr = ljlk_pose_scores(c, *gpu_args)
+    w = torch.tensor([1.0, 0.55, 1.0], device=DEV)[:, None]
+    (E * w).sum().backward()
+    E_close(E.detach().cpu().numpy(), Eo)
+    assert numpy.array_equal(nbr.cpu().numpy(), nbro)
+    assert (E[:, 1] == 0).all() and nbr[1].sum() == 0
+    go = (dVo * numpy.array([1.0, 0.55, 1.0])[:, None, None]).sum(0)
+    g_close(c.grad.cpu().numpy(), go)
+    pose1 = (ps.pose_ind_for_atom == 1).numpy()
+    assert (c.grad.cpu().numpy()[pose1] == 0).all()
+    clear_plan_cache()

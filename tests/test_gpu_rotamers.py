@@ -9,7 +9,9 @@
 - a rotamer set with exactly the native rotamer per block scores like the
   pose op (the rotamer-pair energies add up to the whole-pose energies);
 - torch gradcheck in float64 through ``ljlk_rotamer_scores``, and the
-  rendered scoring module.
+  rendered scoring module;
+- rotamers of blocks with several tiles, three connections and ligand
+  fragments against the oracle.
 """
 
 import numpy
@@ -130,3 +132,46 @@ def test_rendered_module_and_plan_kinds():
     pplan = LJLKPlan(coords, pose_score_args(ps, term)[:-1])
     with pytest.raises(native.NativeError):
         pplan.rotamer_dispatch(coords)
+
+
+def test_exotic_block_rotamers_against_oracle():
+    """Rotamers of blocks with more than 32 atoms, three connections and
+    ligand fragments (copies of each native block moved by N(0, 0.4 A))."""
+    import sys
+    import os
+
+    sys.path.insert(0, os.path.dirname(__file__))
+    from exotic_blocks import exotic_pose_stack
+    from tmol_b200.pose.rotamers import rotamer_set_from_arrays
+
+    ps = exotic_pose_stack(seed=3)
+    rng = numpy.random.default_rng(8)
+    X = ps.coords.numpy()
+    bti = ps.block_type_ind.numpy()
+    offs = ps.block_coord_offset.numpy()
+    pbt = ps.packed_block_types
+    block_ind, pose_for, bt_for, xyz = [], [], [], []
+    for p in range(ps.n_poses):
+        for b in range(ps.max_n_blocks):
+            if bti[p, b] < 0:
+                continue
+            n = pbt.active_block_types[bti[p, b]].n_atoms
+            native = X[p, offs[p, b]:offs[p, b] + n]
+            for k in range(int(rng.integers(1, 4))):
+                block_ind.append(b)
+                pose_for.append(p)
+                bt_for.append(int(bti[p, b]))
+                xyz.append(native if k == 0 else native + rng.normal(scale=0.4, size=native.shape))
+    rs = rotamer_set_from_arrays(block_ind, pose_for, bt_for, xyz, ps.n_poses, ps.max_n_blocks, "cpu")
+    term = LJLKEnergyTerm()
+    args = rotamer_score_args(ps, rs, term)
+    oc = O.OracleCall(rs.coords, args)
+    Eo, idxo, nbr = oc.rotamer_scores()
+    gargs = [a.to(DEV) if isinstance(a, torch.Tensor) else a for a in args]
+    c = rs.coords.to(DEV).requires_grad_(True)
+    E, idx = ljlk_rotamer_scores(c, *gargs)
+    assert numpy.array_equal(idx.cpu().numpy(), idxo)
+    E_close(E.detach().cpu().numpy(), Eo)
+    w = rng.normal(size=Eo.shape).astype(numpy.float32)
+    (E * torch.tensor(w, device=DEV)).sum().backward()
+    g_close(c.grad.cpu().numpy(), oc.rotamer_backward(nbr, w))
