@@ -1516,10 +1516,15 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
         } else {
           const int rot2 = rot2_first + k;
           const int bt2 = ra.rot_bt[rot2], off2 = ra.rot_off[rot2];
-          const int n2 = s.bt_n_atoms[bt2];
           const int nc2 = kind == kSlotStriking ? s.bt_n_conn[bt2] : 0;
           const int lig = r.lig1 && s.bt_is_ligand[bt2];
           const Real* sph2 = rs + 4 * (int64_t)rot2;
+          // every atom of rot2 lies within its radius of its centre: when the
+          // spheres are farther apart than both radii plus the reach, the
+          // atom cull would drop them all, so the pair is left at zero
+          const Real sx = sph2[0] - c1x, sy = sph2[1] - c1y, sz = sph2[2] - c1z;
+          const Real lim = reach1 + sph2[3];
+          const int n2 = sx * sx + sy * sy + sz * sz < lim * lim * Real(1.0001) ? s.bt_n_atoms[bt2] : 0;
           for (int st2 = 0; st2 < n2; st2 += TILE) {
             const int c2 = min(TILE, n2 - st2);
             if (lane == 0) {
