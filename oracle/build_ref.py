@@ -4,11 +4,14 @@ sources, for use as a test oracle and as the timed CPU baseline.
 This is test infrastructure: only tests, the smoke check and the benchmark's
 CPU-baseline leg use what it builds.
 
-The op is two translation units of the reference,
+The LJ/LK op is two translation units of the reference,
 ``tmol/score/ljlk/potentials/compiled.ops.cpp`` (the ``torch::autograd``
-wrapper registering ``torch.ops.tmol_ljlk.ljlk_pose_scores``) and
+wrapper registering ``torch.ops.tmol_ljlk.ljlk_pose_scores`` and
+``ljlk_rotamer_scores``) and
 ``tmol/score/ljlk/potentials/ljlk_pose_score.cpu.cpp`` (the CPU instantiation
-of the pose-score dispatch), plus header-only code under ``tmol/`` and the
+of the dispatch); the elec op (``torch.ops.tmol_elec.elec_pose_scores``) is
+the two matching files under ``tmol/score/elec/potentials``.  Both use
+header-only code under ``tmol/`` and the
 vendored Eigen / moderngpu headers in ``tmol/extern``.  They are compiled in
 place with g++ -O3 through torch's extension builder (no reference build
 system is run); the shared library lands in ``oracle/_ref/``.
@@ -24,35 +27,43 @@ REF_DEFAULT = "/root/reference"
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 LIB_NAME = "tmol_ljlk_ref"
+ELEC_LIB_NAME = "tmol_elec_ref"
 
 
 def lib_path():
     return os.path.join(OUT, LIB_NAME + ".so")
 
 
+def elec_lib_path():
+    return os.path.join(OUT, "elec", ELEC_LIB_NAME + ".so")
+
+
 def build(ref=REF_DEFAULT, verbose=False):
     from torch.utils.cpp_extension import load
 
-    src = os.path.join(ref, "tmol", "score", "ljlk", "potentials")
-    if not os.path.isdir(src):
-        raise FileNotFoundError(f"reference sources not found under {src}")
-    os.makedirs(OUT, exist_ok=True)
     t0 = time.time()
-    load(
-        name=LIB_NAME,
-        sources=[
-            os.path.join(src, "compiled.ops.cpp"),
-            os.path.join(src, "ljlk_pose_score.cpu.cpp"),
-        ],
-        extra_include_paths=[ref, os.path.join(ref, "tmol", "extern")],
-        extra_cflags=["-O3", "-w"],
-        is_python_module=False,
-        build_directory=OUT,
-        verbose=verbose,
-    )
+    # each op in its own build directory: both have a compiled.ops.cpp
+    for name, sub, srcs, out in (
+        (LIB_NAME, "ljlk", ["compiled.ops.cpp", "ljlk_pose_score.cpu.cpp"], OUT),
+        (ELEC_LIB_NAME, "elec", ["compiled.ops.cpp", "elec_pose_score.cpu.cpp"], os.path.join(OUT, "elec")),
+    ):
+        src = os.path.join(ref, "tmol", "score", sub, "potentials")
+        if not os.path.isdir(src):
+            raise FileNotFoundError(f"reference sources not found under {src}")
+        os.makedirs(out, exist_ok=True)
+        load(
+            name=name,
+            sources=[os.path.join(src, f) for f in srcs],
+            extra_include_paths=[ref, os.path.join(ref, "tmol", "extern")],
+            extra_cflags=["-O3", "-w"],
+            is_python_module=False,
+            build_directory=out,
+            verbose=verbose,
+        )
     return time.time() - t0
 
 
 if __name__ == "__main__":
     ref = sys.argv[1] if len(sys.argv) > 1 else REF_DEFAULT
-    print(f"built {lib_path()} in {build(ref, verbose=True):.1f}s")
+    t = build(ref, verbose=True)
+    print(f"built {lib_path()} and {elec_lib_path()} in {t:.1f}s")

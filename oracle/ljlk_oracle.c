@@ -421,6 +421,14 @@ typedef struct {
   real max_dis;
   int n_atoms, n_rots, P, B, nbt, A, C, ntiles, T;
   const int32_t* n_rots_for_block;      /* [P][B] (rotamer scoring) */
+  /* the elec term (term == 1): per block-type atom partial charges, path
+   * distances to each atom's count-pair representative (conn-atom lookups;
+   * bt_path_distance then holds the representative-to-representative
+   * table), and the sigmoidal-dielectric parameters */
+  int term;
+  const real* bt_charge;                /* [nbt][A] */
+  const int32_t* bt_pd_inter;           /* [nbt][A][A] */
+  float elec_D, elec_D0, elec_S, elec_min_dis, elec_max_dis;
 } oracle_inputs_t;
 
 typedef struct {
@@ -441,14 +449,15 @@ static const type_params_t* tparams(const oracle_inputs_t* in, int bt,
 static int inter_separation(const oracle_inputs_t* in, const pair_ctx_t* c,
                             int a1, int a2) {
   int sep = c->min_sep;
+  const int32_t* pd = in->bt_pd_inter ? in->bt_pd_inter : in->bt_path_distance;
   if (sep <= MAX_IMPORTANT_BOND_SEPARATION) {
     sep = MAX_IMPORTANT_BOND_SEPARATION + 1;
     for (int ii = 0; ii < c->n_conn1; ++ii) {
-      unsigned char pd1 = (unsigned char)in->bt_path_distance
+      unsigned char pd1 = (unsigned char)pd
           [((size_t)c->bt1 * in->A + c->conn_ats1[ii]) * in->A + a1];
       for (int jj = 0; jj < c->n_conn2; ++jj) {
         int cs = c->conn_seps[ii * c->n_conn2 + jj];
-        unsigned char pd2 = (unsigned char)in->bt_path_distance
+        unsigned char pd2 = (unsigned char)pd
             [((size_t)c->bt2 * in->A + c->conn_ats2[jj]) * in->A + a2];
         int s = pd1 + cs + pd2;
         if (s < sep) sep = s;
@@ -583,6 +592,106 @@ static real eval_lk(const oracle_inputs_t* in, const eval_t* ev, int bt1,
   return o[0];
 }
 
+/* ---------------------------------------------------------------------- */
+/* The elec term (tmol/score/elec/potentials/potentials.hh:32-215): a      */
+/* sigmoidal distance-dependent dielectric Coulomb energy, flat below       */
+/* min_dis - 0.25, cubic fades over [min_dis - 0.25, min_dis + 0.25] and    */
+/* [max_dis - 1, max_dis].  The parameters are floats and the literals      */
+/* doubles, as in the reference, so intermediate values are promoted the    */
+/* same way before the result is rounded to `real`.                         */
+
+static real elec_eps(real dist, float D, float D0, float S) {
+  return (real)(D - 0.5 * (D - D0) * (2 + 2 * dist * S + dist * dist * S * S) *
+                        rexp_(-dist * S));
+}
+
+static real elec_deps_ddist(real dist, float D, float D0, float S) {
+  return (real)(0.5 * (D - D0) * dist * dist * S * S * S * rexp_(-dist * S));
+}
+
+/* elec_delec_ddist (potentials.hh:50-127) when dE != NULL, else elec
+ * (:129-205). */
+static real elec_pair(const oracle_inputs_t* in, real dist, real e_i, real e_j,
+                      real bonded_path_length, real* dE) {
+  const float D = in->elec_D, D0 = in->elec_D0, S = in->elec_S;
+  const float min_dis = in->elec_min_dis, max_dis = in->elec_max_dis;
+  real low_poly_start = min_dis - 0.25;
+  real low_poly_end = min_dis + 0.25;
+  real hi_poly_start = max_dis - 1.0;
+  real hi_poly_end = max_dis;
+  real weight = connectivity_weight(bonded_path_length);
+  real C1 = 322.0637;
+  real C2 = C1 / (max_dis * elec_eps(max_dis, D, D0, S));
+  real eiej = e_i * e_j;
+  real E = 0, dE_ = 0;
+  if (dE) *dE = 0;
+  if (eiej == 0) return 0;
+  if (dist < low_poly_start) {
+    real min_dis_score = C1 / (min_dis * elec_eps(min_dis, D, D0, S)) - C2;
+    E = eiej * min_dis_score;
+    dE_ = 0;
+  } else if (dist < low_poly_end) {
+    real min_dis_score = C1 / (min_dis * elec_eps(min_dis, D, D0, S)) - C2;
+    real eps_elec = elec_eps(low_poly_end, D, D0, S);
+    real deps_elec_d_dist = elec_deps_ddist(low_poly_end, D, D0, S);
+    real dmax_elec = eiej * (C1 / (low_poly_end * eps_elec) - C2);
+    real dmax_elec_d_dist = -C1 * eiej * (eps_elec + low_poly_end * deps_elec_d_dist) /
+                            (low_poly_end * low_poly_end * eps_elec * eps_elec);
+    if (dE) {
+      interpolate_V_dV(dist, low_poly_start, eiej * min_dis_score, 0.0, low_poly_end,
+                       dmax_elec, dmax_elec_d_dist, &E, &dE_);
+    } else {
+      E = interpolate(dist, low_poly_start, eiej * min_dis_score, 0.0, low_poly_end,
+                      dmax_elec, dmax_elec_d_dist);
+    }
+  } else if (dist < hi_poly_start) {
+    real eps_elec = elec_eps(dist, D, D0, S);
+    real deps_elec_d_dist = elec_deps_ddist(dist, D, D0, S);
+    E = eiej * (C1 / (dist * eps_elec) - C2);
+    dE_ = -C1 * eiej * (eps_elec + dist * deps_elec_d_dist) /
+          (dist * dist * eps_elec * eps_elec);
+  } else if (dist < hi_poly_end) {
+    real eps_elec = elec_eps(hi_poly_start, D, D0, S);
+    real deps_elec_d_dist = elec_deps_ddist(hi_poly_start, D, D0, S);
+    real dmin_elec = eiej * (C1 / (hi_poly_start * eps_elec) - C2);
+    real dmin_elec_d_dist = -C1 * eiej * (eps_elec + hi_poly_start * deps_elec_d_dist) /
+                            (hi_poly_start * hi_poly_start * eps_elec * eps_elec);
+    if (dE) {
+      interpolate_to_zero_V_dV(dist, hi_poly_start, dmin_elec, dmin_elec_d_dist,
+                               hi_poly_end, &E, &dE_);
+    } else {
+      E = interpolate_to_zero(dist, hi_poly_start, dmin_elec, dmin_elec_d_dist, hi_poly_end);
+    }
+  }
+  if (dE) *dE = weight * dE_;
+  return weight * E;
+}
+
+/* elec_atom_energy / _derivs / _energy_and_derivs_full (elec.hh:405-545) */
+static real eval_elec(const oracle_inputs_t* in, const eval_t* ev, int bt1, int a1,
+                      int at1, int bt2, int a2, int at2, int sep) {
+  const real* x1 = in->coords + 3 * (size_t)at1;
+  const real* x2 = in->coords + 3 * (size_t)at2;
+  const real q1 = in->bt_charge[(size_t)bt1 * in->A + a1];
+  const real q2 = in->bt_charge[(size_t)bt2 * in->A + a2];
+  if (ev->mode == MODE_ENERGY) {
+    real dx = x1[0] - x2[0], dy = x1[1] - x2[1], dz = x1[2] - x2[2];
+    real d = rsqrt_(dx * dx + (dy * dy + dz * dz));
+    return elec_pair(in, d, q1, q2, (real)sep, NULL);
+  }
+  real d, gr[3], dE;
+  dist_and_grad(x1, x2, &d, gr);
+  real E = elec_pair(in, d, q1, q2, (real)sep, &dE);
+  if (ev->mode == MODE_ENERGY_AND_DERIVS) {
+    acc3(ev->dV + 3 * (size_t)at1, gr, dE);
+    acc3_neg(ev->dV + 3 * (size_t)at2, gr, dE);
+  } else {
+    acc3(ev->dV + 3 * (size_t)at1, gr, ev->w[0] * dE);
+    acc3_neg(ev->dV + 3 * (size_t)at2, gr, ev->w[0] * dE);
+  }
+  return E;
+}
+
 /* One work group of the pose kernel: all atom pairs of one block pair,
  * walked tile by tile (tile_atom_pair_evaluation.hh:358-505).  Returns the
  * three block-pair totals. */
@@ -596,24 +705,27 @@ static void eval_block_pair(const oracle_inputs_t* in, const eval_t* ev,
     for (int i = 0; i < n_it1; ++i) {
       int s1 = TILE * i;
       int nr1 = c->n1 - s1 < TILE ? c->n1 - s1 : TILE;
-      int nh1 = in->bt_n_heavy_in_tile[c->bt1 * nt_tiles + i];
+      int nh1 = in->term == 0 ? in->bt_n_heavy_in_tile[c->bt1 * nt_tiles + i] : 0;
       for (int j = 0; j < n_it2; ++j) {
         int s2 = TILE * j;
         int nr2 = c->n2 - s2 < TILE ? c->n2 - s2 : TILE;
-        int nh2 = in->bt_n_heavy_in_tile[c->bt2 * nt_tiles + j];
+        int nh2 = in->term == 0 ? in->bt_n_heavy_in_tile[c->bt2 * nt_tiles + j] : 0;
         real la = 0, lr = 0, lk = 0;
         for (int k = 0; k < nr1 * nr2; ++k) {
           int a1 = s1 + k / nr2, a2 = s2 + k % nr2;
           int sep = inter_separation(in, c, a1, a2);
-          real atr, rep;
-          eval_lj(in, ev, c->bt1, a1, c->off1 + a1, c->bt2, a2, c->off2 + a2,
-                  sep, &atr, &rep);
+          real atr, rep = 0;
+          if (in->term == 1)
+            atr = eval_elec(in, ev, c->bt1, a1, c->off1 + a1, c->bt2, a2, c->off2 + a2, sep);
+          else
+            eval_lj(in, ev, c->bt1, a1, c->off1 + a1, c->bt2, a2, c->off2 + a2,
+                    sep, &atr, &rep);
           la += atr;
           lr += rep;
         }
         t_atr += la;
         t_rep += lr;
-        if (nh1 > 0 && nh2 > 0) {
+        if (in->term == 0 && nh1 > 0 && nh2 > 0) {
           for (int k = 0; k < nh1 * nh2; ++k) {
             int h1 = k / nh2, h2 = k % nh2;
             int a1 = s1 + in->bt_heavy_in_tile[c->bt1 * TILE * nt_tiles + s1 + h1];
@@ -631,25 +743,28 @@ static void eval_block_pair(const oracle_inputs_t* in, const eval_t* ev,
     for (int i = 0; i < n_it; ++i) {
       int s1 = TILE * i;
       int nr1 = c->n1 - s1 < TILE ? c->n1 - s1 : TILE;
-      int nh1 = in->bt_n_heavy_in_tile[c->bt1 * nt_tiles + i];
+      int nh1 = in->term == 0 ? in->bt_n_heavy_in_tile[c->bt1 * nt_tiles + i] : 0;
       for (int j = i; j < n_it; ++j) {
         int s2 = TILE * j;
         int nr2 = c->n1 - s2 < TILE ? c->n1 - s2 : TILE;
-        int nh2 = in->bt_n_heavy_in_tile[c->bt1 * nt_tiles + j];
+        int nh2 = in->term == 0 ? in->bt_n_heavy_in_tile[c->bt1 * nt_tiles + j] : 0;
         real la = 0, lr = 0, lk = 0;
         for (int k = 0; k < nr1 * nr2; ++k) {
           int a1 = s1 + k / nr2, a2 = s2 + k % nr2;
           if (a1 >= a2) continue;
           int sep = intra_separation(in, c->bt1, a1, a2);
-          real atr, rep;
-          eval_lj(in, ev, c->bt1, a1, c->off1 + a1, c->bt1, a2, c->off1 + a2,
-                  sep, &atr, &rep);
+          real atr, rep = 0;
+          if (in->term == 1)
+            atr = eval_elec(in, ev, c->bt1, a1, c->off1 + a1, c->bt1, a2, c->off1 + a2, sep);
+          else
+            eval_lj(in, ev, c->bt1, a1, c->off1 + a1, c->bt1, a2, c->off1 + a2,
+                    sep, &atr, &rep);
           la += atr;
           lr += rep;
         }
         t_atr += la;
         t_rep += lr;
-        if (nh1 > 0 && nh2 > 0) {
+        if (in->term == 0 && nh1 > 0 && nh2 > 0) {
           for (int k = 0; k < nh1 * nh2; ++k) {
             int h1 = k / nh2, h2 = k % nh2;
             if (h1 + s1 >= h2 + s2) continue;
@@ -847,7 +962,7 @@ void oracle_count_pairs(const oracle_inputs_t* in, const int32_t* nbr,
         pair_ctx_t c;
         if (!setup_pair(in, p, b1, b2, &c)) continue;
         int h1 = 0, h2 = 0;
-        for (int t = 0; t < in->ntiles; ++t) {
+        for (int t = 0; in->term == 0 && t < in->ntiles; ++t) {
           h1 += in->bt_n_heavy_in_tile[c.bt1 * in->ntiles + t];
           h2 += in->bt_n_heavy_in_tile[c.bt2 * in->ntiles + t];
         }

@@ -74,6 +74,14 @@ def _inputs_struct(real_t):
             ("ntiles", ctypes.c_int),
             ("T", ctypes.c_int),
             ("n_rots_for_block", i32p),
+            ("term", ctypes.c_int),
+            ("bt_charge", rp),
+            ("bt_pd_inter", i32p),
+            ("elec_D", ctypes.c_float),
+            ("elec_D0", ctypes.c_float),
+            ("elec_S", ctypes.c_float),
+            ("elec_min_dis", ctypes.c_float),
+            ("elec_max_dis", ctypes.c_float),
         ]
 
     return Inputs
@@ -81,10 +89,20 @@ def _inputs_struct(real_t):
 
 class OracleCall:
     """Holds contiguous numpy copies of one op call's inputs and the ctypes
-    struct pointing at them."""
+    struct pointing at them.  ``term="elec"`` takes the elec op's argument
+    list (``tmol/score/elec/potentials/compiled.ops.cpp:28-59``) instead of
+    the LJ/LK op's; energies then come back as [1, ...]."""
 
-    def __init__(self, coords, args, f64=False):
+    def __init__(self, coords, args, f64=False, term="ljlk"):
         self.f64 = f64
+        self.term = term
+        if term == "elec":
+            (min_bondsep, ibb, bt_n_atoms, bt_charge, bt_n_conn, bt_conn_atom, inter_rpd, intra_rpd,
+             bt_is_ligand, elec_global, max_dis) = args[12:23]
+            args = list(args[:12]) + [
+                min_bondsep, ibb, bt_n_atoms, None, None, None, bt_n_conn, bt_conn_atom, intra_rpd,
+                bt_is_ligand, None, None, max_dis,
+            ]
         self.np_real = numpy.float64 if f64 else numpy.float32
         real_t = ctypes.c_double if f64 else ctypes.c_float
         self.real_t = real_t
@@ -118,11 +136,15 @@ class OracleCall:
         self.keep = []
 
         def i32(t):
+            if t is None:
+                return None
             a = numpy.ascontiguousarray(t.detach().cpu().numpy().astype(numpy.int32))
             self.keep.append(a)
             return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
 
         def rl(t):
+            if t is None:
+                return None
             a = numpy.ascontiguousarray(t.detach().cpu().numpy().astype(self.np_real))
             self.keep.append(a)
             return a.ctypes.data_as(ctypes.POINTER(real_t))
@@ -148,17 +170,23 @@ class OracleCall:
         s.bt_is_ligand = i32(bt_is_ligand)
         s.n_rots_for_block = i32(n_rots_for_block)
         s.type_params = rl(type_params)
-        s.global_params = rl(global_params.reshape(-1))
+        s.global_params = rl(global_params.reshape(-1) if global_params is not None else None)
         s.max_dis = float(max_dis)
+        if term == "elec":
+            g = elec_global.detach().cpu().reshape(-1).to(torch.float32).numpy()
+            s.term = 1
+            s.bt_charge = rl(bt_charge)
+            s.bt_pd_inter = i32(inter_rpd)
+            s.elec_D, s.elec_D0, s.elec_S, s.elec_min_dis, s.elec_max_dis = (float(v) for v in g)
         s.n_atoms = coords.reshape(-1, 3).shape[0]
         s.n_rots = rot_coord_offset.shape[0]
         s.P = first_rot_block_type.shape[0]
         s.B = first_rot_block_type.shape[1]
         s.nbt = bt_n_atoms.shape[0]
-        s.A = bt_atom_types.shape[1]
+        s.A = (bt_charge if term == "elec" else bt_atom_types).shape[1]
         s.C = bt_conn_atom.shape[1]
-        s.ntiles = bt_n_heavy_in_tile.shape[1]
-        s.T = type_params.shape[0]
+        s.ntiles = 0 if term == "elec" else bt_n_heavy_in_tile.shape[1]
+        s.T = 0 if term == "elec" else type_params.shape[0]
         self.s = s
         self.P, self.B, self.N = s.P, s.B, s.n_atoms
 
@@ -282,6 +310,30 @@ def reference_rotamer_scores(coords, args, require_gradient=True):
         c.requires_grad_(True)
     E, idx = op(c, *cpu_args)
     return E, c, idx
+
+
+ELEC_REF_LIB = os.path.join(HERE, "_ref", "elec", "tmol_elec_ref.so")
+_elec_loaded = False
+
+
+def reference_elec_available():
+    return os.path.exists(ELEC_REF_LIB)
+
+
+def reference_elec_pose_scores(coords, args, require_gradient=True):
+    """Runs the reference CPU elec op: returns (E [1, P] or [1, P, B, B],
+    coords tensor (with grad if requested), block neighbours)."""
+    global _elec_loaded
+    if not _elec_loaded:
+        torch.ops.load_library(ELEC_REF_LIB)
+        _elec_loaded = True
+    op = torch.ops.tmol_elec.elec_pose_scores
+    cpu_args = [a.cpu() if isinstance(a, torch.Tensor) else a for a in args]
+    c = coords.detach().cpu().reshape(-1, 3).clone()
+    if require_gradient:
+        c.requires_grad_(True)
+    E, nbr = op(c, *cpu_args)
+    return E, c, nbr
 
 
 def reference_pose_scores(coords, args, require_gradient=True):

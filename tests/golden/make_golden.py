@@ -16,6 +16,9 @@ Writes
   synthetic.npz      reference op energies, gradient and neighbour matrix of
                      a jagged batch of seeded synthetic poses (1, 2, 7, 33,
                      100 residues), plus the sizes and seeds that rebuild it
+  elec.npz           the reference elec op (elec_pose_scores) on 1ubq and on
+                     a jagged synthetic batch: per-pose energies, gradient,
+                     neighbour matrix and block-pair energies
   rotamers.npz       the reference rotamer-score op (ljlk_rotamer_scores) on
                      a seeded rotamer set over a jagged batch of poses: the
                      set itself, the rotamer-pair energies and dispatch
@@ -37,10 +40,13 @@ from tmol_b200.pose.builder import build_pose_stack  # noqa: E402
 from tmol_b200.pose.pdb import pose_from_pdb_text  # noqa: E402
 from tmol_b200.pose.synthetic import synthetic_pose_stack  # noqa: E402
 from tmol_b200.pose.rotamers import synthetic_rotamer_set  # noqa: E402
+from tmol_b200.score.elec_energy_term import ElecEnergyTerm, elec_pose_score_args  # noqa: E402
 from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm, pose_score_args, rotamer_score_args  # noqa: E402
 
 SYN_SIZES = [1, 2, 7, 33, 100]
 SYN_SEEDS = [11, 12, 13, 14, 15]
+ELEC_SIZES = [40, 3, 17, 120]
+ELEC_SEEDS = [31, 32, 33, 34]
 ROT_SIZES = [12, 30, 1, 45]
 ROT_SEEDS = [21, 22, 23, 24]
 ROT_SET = dict(max_rots=4, mutate_fraction=0.25, seed=5, skip_fraction=0.1)
@@ -97,6 +103,23 @@ def main(ref_root):
         ref_grad=g,
         ref_neighbors=nbr,
     )
+    eterm = ElecEnergyTerm()
+    out = {}
+    for tag, eps_ in (("ubq", build_pose_stack([topo], [xyz])), ("syn", synthetic_pose_stack(ELEC_SIZES, ELEC_SEEDS))):
+        coords = eps_.coords.flatten(0, 1)
+        E, c, nbr = O.reference_elec_pose_scores(coords, elec_pose_score_args(eps_, eterm), require_gradient=True)
+        E.sum().backward()
+        Eb, _, _ = O.reference_elec_pose_scores(coords, elec_pose_score_args(eps_, eterm, True), require_gradient=False)
+        out.update({
+            f"{tag}_energies": E.detach().numpy(),
+            f"{tag}_grad": c.grad.numpy(),
+            f"{tag}_neighbors": nbr.numpy(),
+            f"{tag}_block_pair": Eb.detach().numpy(),
+        })
+    numpy.savez_compressed(
+        os.path.join(HERE, "elec.npz"), sizes=numpy.array(ELEC_SIZES), seeds=numpy.array(ELEC_SEEDS), **out
+    )
+
     ps = synthetic_pose_stack(ROT_SIZES, ROT_SEEDS)
     rs = synthetic_rotamer_set(ps, **ROT_SET)
     args = rotamer_score_args(ps, rs, term)

@@ -1,0 +1,80 @@
+"""The C oracle's elec term against the reference elec op: bit for bit
+against the committed fixture (1ubq and a jagged synthetic batch: per-pose
+energies, gradient, neighbour matrix, block-pair energies), against the
+live compiled op where it is present, and the partial-charge and count-pair
+representative tables against tmol's rules."""
+
+import numpy
+import pytest
+import torch
+
+from oracle import oracle as O
+from tests.conftest import load_golden
+from tmol_b200.pose.synthetic import synthetic_pose_stack
+from tmol_b200.score.elec_energy_term import ElecEnergyTerm, ElecParams, elec_pose_score_args
+
+
+@pytest.fixture(scope="module")
+def eterm():
+    return ElecEnergyTerm()
+
+
+def cases(ubq_pose_stack):
+    g = load_golden("elec.npz")
+    return g, [("ubq", ubq_pose_stack), ("syn", synthetic_pose_stack(list(g["sizes"]), list(g["seeds"])))]
+
+
+def test_oracle_matches_reference_fixture(ubq_pose_stack, eterm):
+    g, pss = cases(ubq_pose_stack)
+    for tag, ps in pss:
+        coords = ps.coords.flatten(0, 1)
+        oc = O.OracleCall(coords, elec_pose_score_args(ps, eterm), term="elec")
+        E, dV, nbr = oc.pose_scores(require_gradient=True)
+        assert numpy.array_equal(E[:1], g[f"{tag}_energies"]), tag
+        assert numpy.array_equal(dV[0], g[f"{tag}_grad"]), tag
+        assert numpy.array_equal(nbr, g[f"{tag}_neighbors"]), tag
+        Eb, _, _ = oc.pose_scores(block_pair=True)
+        assert numpy.array_equal(Eb[:1], g[f"{tag}_block_pair"]), tag
+
+
+@pytest.mark.skipif(not O.reference_elec_available(), reason="compiled reference elec op not built")
+@pytest.mark.parametrize("f64", [False, True])
+def test_oracle_matches_reference_op(eterm, f64):
+    ps = synthetic_pose_stack([60, 25], [41, 42], extra_chi_sd=20.0)
+    args = elec_pose_score_args(ps, eterm)
+    dt = torch.float64 if f64 else torch.float32
+    coords = ps.coords.flatten(0, 1).to(dt)
+    args64 = [a.to(dt) if isinstance(a, torch.Tensor) and a.is_floating_point() else a for a in args]
+    E_ref, c, nbr_ref = O.reference_elec_pose_scores(coords, args64)
+    E_ref.sum().backward()
+    oc = O.OracleCall(coords, args, f64=f64, term="elec")
+    E, dV, nbr = oc.pose_scores(require_gradient=True)
+    assert numpy.array_equal(E[:1], E_ref.detach().numpy())
+    assert numpy.array_equal(dV[0], c.grad.numpy())
+    assert numpy.array_equal(nbr, nbr_ref.numpy())
+    w = numpy.random.default_rng(3).normal(size=(3,) + E.shape[1:])
+    w[1:] = 0
+    dx = oc.backward(nbr, w, per_pose_weights=True)
+    ref = dV[0] * w[0, ps.pose_ind_for_atom.numpy()][:, None]
+    # the same terms summed in another order
+    numpy.testing.assert_allclose(dx, ref, rtol=1e-5, atol=1e-5 * numpy.abs(ref).max())
+
+
+def test_charge_and_representative_tables(eterm):
+    from tmol_b200.chem.restypes import ResidueTypeSet
+
+    rts = ResidueTypeSet.get_default()
+    p = ElecParams()
+    # variants take their own charges, falling back to the unpatched entry
+    ala_n = rts.types["ALA:nterm"]
+    q = dict(zip(ala_n.atom_names, p.partial_charges_for_block(ala_n)))
+    assert q["N"] == pytest.approx(-0.10440) and q["CB"] == pytest.approx(-0.36465)
+    # a hydrogen's representative is its heavy atom: the pair distances use
+    # the heavy atom's path distances
+    ala = rts.types["ALA"]
+    rep = p.representative_mapping(ala)
+    assert rep[ala.atom_index["N"]] == ala.atom_index["H"]
+    charge, inter, intra = eterm.block_type_tables(ala)
+    pd = numpy.asarray(ala.path_distance)
+    assert (inter == pd[:, rep]).all() and (intra == pd[rep][:, rep]).all()
+    assert abs(charge.sum()) < 1e-4  # neutral residue

@@ -15,9 +15,14 @@ pose builder use:
 * the canonical L-amino-acid residue types plus HIS_D;
 * the LJ/LK global parameters.
 
+The elec term's parameters (``database/default/scoring/elec.yaml``: the
+sigmoidal-dielectric global parameters, per residue / variant / atom partial
+charges and the count-pair representative atoms, in file order, since later
+representative lines override earlier ones) go to a second file.
+
 Usage::
 
-    python -m tmol_b200.chem.extract_db <tmol/database/default> <out.json>
+    python -m tmol_b200.chem.extract_db <tmol/database/default> <out.json> [<elec_out.json>]
 """
 
 import json
@@ -135,12 +140,40 @@ def extract(db_root):
     )
 
 
+def extract_elec(db_root):
+    with open(f"{db_root}/scoring/elec.yaml") as f:
+        elec = yaml.safe_load(f)
+
+    def res_var(tag):
+        parts = tag.split(":")
+        return parts[0], (parts[1] if len(parts) > 1 else "")
+
+    charges = []
+    for x in elec["atom_charge_parameters"]:
+        res, var = res_var(x["res"])
+        charges.append([res, var, x["atom"], float(x["charge"])])
+    cp_reps = []
+    for x in elec["atom_cp_reps_parameters"]:
+        res, var = res_var(x["res"])
+        cp_reps.append([res, var, x["atm_outer"], x["atm_inner"]])
+    return dict(
+        source="tmol parameter database (scoring/elec.yaml)",
+        global_params={k: float(v) for k, v in elec["global_parameters"].items()},
+        partial_charges=charges,
+        cp_reps=cp_reps,
+    )
+
+
 def main(argv):
     db_root, out = argv[1], argv[2]
     data = extract(db_root)
     with open(out, "w") as f:
         json.dump(data, f, indent=0, sort_keys=False)
         f.write("\n")
+    if len(argv) > 3:
+        with open(argv[3], "w") as f:
+            json.dump(extract_elec(db_root), f, indent=0, sort_keys=False)
+            f.write("\n")
 
 
 if __name__ == "__main__":
