@@ -605,6 +605,15 @@ static real elec_eps(real dist, float D, float D0, float S) {
                         rexp_(-dist * S));
 }
 
+/* eps called with a float distance (min_dis, max_dis): the reference's
+ * template deduces Real = float from that argument, so these values are
+ * float in both precisions of the op (and so are their products with
+ * min_dis / max_dis). */
+static float elec_eps_f(float dist, float D, float D0, float S) {
+  return (float)(D - 0.5 * (D - D0) * (2 + 2 * dist * S + dist * dist * S * S) *
+                         expf(-dist * S));
+}
+
 static real elec_deps_ddist(real dist, float D, float D0, float S) {
   return (real)(0.5 * (D - D0) * dist * dist * S * S * S * rexp_(-dist * S));
 }
@@ -621,17 +630,17 @@ static real elec_pair(const oracle_inputs_t* in, real dist, real e_i, real e_j,
   real hi_poly_end = max_dis;
   real weight = connectivity_weight(bonded_path_length);
   real C1 = 322.0637;
-  real C2 = C1 / (max_dis * elec_eps(max_dis, D, D0, S));
+  real C2 = C1 / (max_dis * elec_eps_f(max_dis, D, D0, S));
   real eiej = e_i * e_j;
   real E = 0, dE_ = 0;
   if (dE) *dE = 0;
   if (eiej == 0) return 0;
   if (dist < low_poly_start) {
-    real min_dis_score = C1 / (min_dis * elec_eps(min_dis, D, D0, S)) - C2;
+    real min_dis_score = C1 / (min_dis * elec_eps_f(min_dis, D, D0, S)) - C2;
     E = eiej * min_dis_score;
     dE_ = 0;
   } else if (dist < low_poly_end) {
-    real min_dis_score = C1 / (min_dis * elec_eps(min_dis, D, D0, S)) - C2;
+    real min_dis_score = C1 / (min_dis * elec_eps_f(min_dis, D, D0, S)) - C2;
     real eps_elec = elec_eps(low_poly_end, D, D0, S);
     real deps_elec_d_dist = elec_deps_ddist(low_poly_end, D, D0, S);
     real dmax_elec = eiej * (C1 / (low_poly_end * eps_elec) - C2);

@@ -49,9 +49,16 @@ def test_oracle_matches_reference_op(eterm, f64):
     E_ref.sum().backward()
     oc = O.OracleCall(coords, args, f64=f64, term="elec")
     E, dV, nbr = oc.pose_scores(require_gradient=True)
-    assert numpy.array_equal(E[:1], E_ref.detach().numpy())
-    assert numpy.array_equal(dV[0], c.grad.numpy())
     assert numpy.array_equal(nbr, nbr_ref.numpy())
+    if not f64:
+        assert numpy.array_equal(E[:1], E_ref.detach().numpy())
+        assert numpy.array_equal(dV[0], c.grad.numpy())
+    else:
+        # float64: the same operations, the last bit of some pair energies
+        # differs (the reference compiler's evaluation of the dielectric)
+        numpy.testing.assert_allclose(E[:1], E_ref.detach().numpy(), rtol=1e-13, atol=0)
+        g_ref = c.grad.numpy()
+        numpy.testing.assert_allclose(dV[0], g_ref, rtol=1e-12, atol=1e-12 * numpy.abs(g_ref).max())
     w = numpy.random.default_rng(3).normal(size=(3,) + E.shape[1:])
     w[1:] = 0
     dx = oc.backward(nbr, w, per_pose_weights=True)
