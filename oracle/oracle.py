@@ -336,6 +336,22 @@ def reference_elec_pose_scores(coords, args, require_gradient=True):
     return E, c, nbr
 
 
+def reference_elec_rotamer_scores(coords, args, require_gradient=True):
+    """Runs the reference CPU elec rotamer op: returns (scores [1, n], coords
+    tensor (with grad if requested), indices [3, n])."""
+    global _elec_loaded
+    if not _elec_loaded:
+        torch.ops.load_library(ELEC_REF_LIB)
+        _elec_loaded = True
+    op = torch.ops.tmol_elec.elec_rotamer_scores
+    cpu_args = [a.cpu() if isinstance(a, torch.Tensor) else a for a in args]
+    c = coords.detach().cpu().reshape(-1, 3).clone()
+    if require_gradient:
+        c.requires_grad_(True)
+    E, idx = op(c, *cpu_args)
+    return E, c, idx
+
+
 def reference_pose_scores(coords, args, require_gradient=True):
     """Runs the reference CPU op: returns (E, dE/dx or None, nbr)."""
     op = load_reference()

@@ -18,7 +18,10 @@ Writes
                      100 residues), plus the sizes and seeds that rebuild it
   elec.npz           the reference elec op (elec_pose_scores) on 1ubq and on
                      a jagged synthetic batch: per-pose energies, gradient,
-                     neighbour matrix and block-pair energies
+                     neighbour matrix and block-pair energies; and the
+                     reference elec rotamer op (elec_rotamer_scores) on the
+                     rotamer set of rotamers.npz (energies, indices, the
+                     gradient of sum(w * E) for seeded w)
   rotamers.npz       the reference rotamer-score op (ljlk_rotamer_scores) on
                      a seeded rotamer set over a jagged batch of poses: the
                      set itself, the rotamer-pair energies and dispatch
@@ -40,7 +43,11 @@ from tmol_b200.pose.builder import build_pose_stack  # noqa: E402
 from tmol_b200.pose.pdb import pose_from_pdb_text  # noqa: E402
 from tmol_b200.pose.synthetic import synthetic_pose_stack  # noqa: E402
 from tmol_b200.pose.rotamers import synthetic_rotamer_set  # noqa: E402
-from tmol_b200.score.elec_energy_term import ElecEnergyTerm, elec_pose_score_args  # noqa: E402
+from tmol_b200.score.elec_energy_term import (  # noqa: E402
+    ElecEnergyTerm,
+    elec_pose_score_args,
+    elec_rotamer_score_args,
+)
 from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm, pose_score_args, rotamer_score_args  # noqa: E402
 
 SYN_SIZES = [1, 2, 7, 33, 100]
@@ -116,12 +123,21 @@ def main(ref_root):
             f"{tag}_neighbors": nbr.numpy(),
             f"{tag}_block_pair": Eb.detach().numpy(),
         })
+    ps = synthetic_pose_stack(ROT_SIZES, ROT_SEEDS)
+    rs = synthetic_rotamer_set(ps, **ROT_SET)
+    E, c, idx = O.reference_elec_rotamer_scores(rs.coords, elec_rotamer_score_args(ps, rs, eterm))
+    w = torch.tensor(numpy.random.default_rng(9).normal(size=tuple(E.shape)), dtype=E.dtype)
+    (E * w).sum().backward()
+    out.update({
+        "rot_energies": E.detach().numpy(),
+        "rot_indices": idx.numpy(),
+        "rot_weights": w.numpy(),
+        "rot_grad": c.grad.numpy(),
+    })
     numpy.savez_compressed(
         os.path.join(HERE, "elec.npz"), sizes=numpy.array(ELEC_SIZES), seeds=numpy.array(ELEC_SEEDS), **out
     )
 
-    ps = synthetic_pose_stack(ROT_SIZES, ROT_SEEDS)
-    rs = synthetic_rotamer_set(ps, **ROT_SET)
     args = rotamer_score_args(ps, rs, term)
     E, c, idx = O.reference_rotamer_scores(rs.coords, args, require_gradient=True)
     w = torch.tensor(numpy.random.default_rng(7).normal(size=tuple(E.shape)), dtype=E.dtype)

@@ -85,3 +85,20 @@ def test_charge_and_representative_tables(eterm):
     pd = numpy.asarray(ala.path_distance)
     assert (inter == pd[:, rep]).all() and (intra == pd[rep][:, rep]).all()
     assert abs(charge.sum()) < 1e-4  # neutral residue
+
+
+def test_oracle_rotamer_scores_match_reference_fixture(eterm):
+    """Elec rotamer scoring (elec_rotamer_scores) on the rotamer set of
+    rotamers.npz: dispatch, energies and the gradient of sum(w * E)."""
+    from tests.test_rotamer_oracle import fixture_case
+    from tmol_b200.score.elec_energy_term import elec_rotamer_score_args
+
+    g = load_golden("elec.npz")
+    _, ps, rs = fixture_case()
+    oc = O.OracleCall(rs.coords, elec_rotamer_score_args(ps, rs, eterm), term="elec")
+    E, idx, nbr = oc.rotamer_scores()
+    assert numpy.array_equal(idx, g["rot_indices"])
+    assert numpy.array_equal(E[:1], g["rot_energies"])
+    w = numpy.zeros((3, E.shape[1]), dtype=numpy.float32)
+    w[0] = g["rot_weights"][0]
+    assert numpy.array_equal(oc.rotamer_backward(nbr, w), g["rot_grad"])

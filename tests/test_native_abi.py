@@ -54,6 +54,15 @@ def test_status_strings_and_argument_checks():
     assert lib.tmol_b200_ljlk_plan_destroy(None) == 1
     assert lib.tmol_b200_ljlk_forward(None, None, 0, None, None, None) == 1
     assert lib.tmol_b200_ljlk_plan_device_bytes(None) == -1
+    # the elec entry points check their arguments the same way
+    assert lib.tmol_b200_elec_plan_create(None, 4, None, None, ctypes.byref(out)) == 1
+    e = native.ElecInputs()
+    assert lib.tmol_b200_elec_plan_create(ctypes.byref(e), 3, None, None, ctypes.byref(out)) == 6
+    e.max_n_conn = 5
+    assert lib.tmol_b200_elec_plan_create(ctypes.byref(e), 4, None, None, ctypes.byref(out)) == 2
+    assert lib.tmol_b200_elec_plan_destroy(None) == 1
+    assert lib.tmol_b200_elec_forward(None, None, 0, None, None, None) == 1
+    assert lib.tmol_b200_elec_rotamer_fill(None, None, None, None) == 1
 
 
 def test_op_refuses_cpu_tensors(ubq_pose_stack, term):

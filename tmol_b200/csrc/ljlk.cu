@@ -36,8 +36,10 @@
 #include <cstring>
 #include <vector>
 
+#include "../../include/tmol_b200_elec.h"
 #include "../../include/tmol_b200_ljlk.h"
 #include "../../include/tmol_b200_screen.h"
+#include "elec_potentials.cuh"
 #include "ljlk_potentials.cuh"
 
 namespace tmol_b200 {
@@ -47,6 +49,14 @@ constexpr int MAX_CONN = 4;
 constexpr int CP_CAP = 16;
 constexpr int MAX_ROWS_PER_ITEM = 64;
 constexpr int MAX_WARPS = 8;
+
+// The energy term a plan scores: LJ + LK (fa_ljatr, fa_ljrep, fa_lk) or
+// elec (fa_elec).  Both share the neighbour detection, count-pair tables,
+// staging and screening; they differ in the per-atom record (atom type and
+// heavy flag, or partial charge) and the pair potential.
+enum TermKind : int { kTermLJLK = 0, kTermElec = 1 };
+
+__host__ __device__ constexpr int n_terms(int term) { return term == kTermElec ? 1 : 3; }
 
 enum StatusBits : int {
   kStIndex = 1,
@@ -95,6 +105,10 @@ struct PlanBuildArgs {
   int* rot_off;
   int* rot_block;
   int* rot_pose;
+  int term;
+  // elec: bond separations from each connection atom come from the
+  // representative table (the intra-block table is in.bt_path_distance)
+  const int32_t* bt_inter_pd;
 };
 
 __global__ void plan_blocks_kernel(PlanBuildArgs a) {
@@ -195,11 +209,13 @@ __global__ void plan_block_types_kernel(PlanBuildArgs a, const int* type_map,
     }
     uint16_t tf = 0;
     if (at < n) {
-      int t = in.bt_atom_types[i];
-      if (t < 0 || t >= in.n_atom_types || type_map[t] < 0) {
-        atomicOr(a.status, kStIndex);
-      } else {
-        tf = (uint16_t)(type_map[t] | (a.bt_flags[i] == kHeavy ? 256 : 0));
+      if (a.term == kTermLJLK) {
+        int t = in.bt_atom_types[i];
+        if (t < 0 || t >= in.n_atom_types || type_map[t] < 0) {
+          atomicOr(a.status, kStIndex);
+        } else {
+          tf = (uint16_t)(type_map[t] | (a.bt_flags[i] == kHeavy ? 256 : 0));
+        }
       }
       for (int at2 = 0; at2 < A; ++at2) {
         int v = in.bt_path_distance[(int64_t)i * A + at2];
@@ -207,6 +223,7 @@ __global__ void plan_block_types_kernel(PlanBuildArgs a, const int* type_map,
       }
     }
     bt_tf[i] = tf;
+    const int32_t* cpd_src = a.bt_inter_pd ? a.bt_inter_pd : in.bt_path_distance;
     int nc = in.bt_n_conn[bt];
     if (at == 0 && (nc < 0 || nc > C)) atomicOr(a.status, kStIndex);
     for (int c = 0; c < C; ++c) {
@@ -216,7 +233,7 @@ __global__ void plan_block_types_kernel(PlanBuildArgs a, const int* type_map,
         if (ca < 0 || ca >= n) {
           atomicOr(a.status, kStIndex);
         } else {
-          int d = in.bt_path_distance[((int64_t)bt * A + ca) * A + at];
+          int d = cpd_src[((int64_t)bt * A + ca) * A + at];
           v = (uint8_t)(d < 0 ? 0 : (d > 255 ? 255 : d));
         }
       }
@@ -360,6 +377,10 @@ struct ScoreArgs {
   // pair (never honoured for b1 == b2 or count-pair partners)
   const uint32_t* skip;
   int skip_words;  // 32-bit words per row
+  // elec plans: partial charge per block-type atom [nbt * A] and the
+  // potential's per-unit-charge constants (ElecK layout)
+  const Real* bt_q;
+  const Real* elec_k;
 };
 
 // Bounding sphere per block: centroid (sum of atoms in order, then divided
@@ -454,12 +475,15 @@ enum SlotKind : int {
   kSlotIntra = 2,     // another tile of block b1: intra-block separation table
 };
 
-// One staged atom: coordinates and per block-type atom flags (compact atom
-// type | heavy << 8).
+// One staged atom: coordinates and either per block-type atom flags
+// (LJ/LK: compact atom type | heavy << 8) or the partial charge (elec).
 template <typename Real>
 struct alignas(16) AtomRec {
   Real x, y, z;
-  int tf;
+  union {
+    int tf;
+    Real q;
+  };
 };
 
 constexpr int N_ATOMS = TILE + M1;
@@ -511,7 +535,7 @@ __device__ __forceinline__ uint32_t load_cpd(const ScoreArgs<Real>& s, int bt,
 }
 
 // Stage atoms [start, start + cnt) of block (bt, off) into side 0.
-template <typename Real>
+template <typename Real, int TERM = kTermLJLK>
 __device__ __forceinline__ void stage_side0(const ScoreArgs<Real>& s,
                                             Slab<Real>& w, int bt, int off,
                                             int start, int cnt, int nconn,
@@ -523,7 +547,10 @@ __device__ __forceinline__ void stage_side0(const ScoreArgs<Real>& s,
     a.x = c[0];
     a.y = c[1];
     a.z = c[2];
-    a.tf = s.bt_tf[(int64_t)bt * s.A + at];
+    if (TERM == kTermElec)
+      a.q = s.bt_q[(int64_t)bt * s.A + at];
+    else
+      a.tf = s.bt_tf[(int64_t)bt * s.A + at];
     w.at[lane] = a;
     w.cpd0[lane] = load_cpd(s, bt, nconn, at);
     w.gx[lane] = 0;
@@ -536,7 +563,7 @@ __device__ __forceinline__ void stage_side0(const ScoreArgs<Real>& s,
 // block b1 to side 1 at j0: an atom farther than r1 + max_dis from b1's
 // centroid is farther than max_dis from every b1 atom, and every term is zero
 // there.  Returns the number of atoms kept.
-template <typename Real>
+template <typename Real, int TERM = kTermLJLK>
 __device__ __forceinline__ int stage_side1(const ScoreArgs<Real>& s,
                                            Slab<Real>& w, int j0, int slot,
                                            int bt, int off, int start,
@@ -561,7 +588,10 @@ __device__ __forceinline__ int stage_side1(const ScoreArgs<Real>& s,
     a.x = x;
     a.y = y;
     a.z = z;
-    a.tf = s.bt_tf[(int64_t)bt * s.A + at];
+    if (TERM == kTermElec)
+      a.q = s.bt_q[(int64_t)bt * s.A + at];
+    else
+      a.tf = s.bt_tf[(int64_t)bt * s.A + at];
     w.at[TILE + j] = a;
     w.cpd1[j] = load_cpd(s, bt, nconn, at);
     w.gidx1[j] = off + at;
@@ -607,7 +637,8 @@ struct EvalCtx {
   const uint8_t* pd;  // intra-block separations of b1, row st1 (tile start)
   int ntp, A;
   Real max_dis;
-  Real wt0, wt1, wt2;  // gradient weights of the three terms
+  Real wt0, wt1, wt2;  // gradient weights of the three terms (elec: wt0)
+  const Real* elec_k;  // elec plans: ElecK constants
 };
 
 template <typename Real>
@@ -619,17 +650,20 @@ __device__ __forceinline__ void cnt_add(unsigned long long* c, int k, long long 
   if (lane == 0) c[k] += (unsigned long long)v;
 }
 
-// Dense evaluation of one queue (HEAVY: LJ + LK, else LJ only); returns the
-// lane's energy sums.  Entries come in screening order, so lanes sharing a1
-// are mostly contiguous: their a1 forces are summed with a segmented shuffle
-// reduction and added once per segment.
-template <typename Real, bool GRAD, bool HEAVY>
+// Dense evaluation of one queue (HEAVY: LJ + LK, else LJ only; elec: the
+// elec energy in .atr); returns the lane's energy sums.  Entries come in
+// screening order, so lanes sharing a1 are mostly contiguous: their a1
+// forces are summed with a segmented shuffle reduction and added once per
+// segment.
+template <typename Real, bool GRAD, bool HEAVY, int TERM = kTermLJLK>
 __device__ __noinline__ E3<Real> eval_queue(EvalCtx<Real> c, Slab<Real>* wp,
                                             int n, int lane) {
   Slab<Real>& w = *wp;
   E3<Real> acc = {0, 0, 0};
   const Real dmax = c.max_dis;
   const Real far_dmin = c.max_dis - Real(1.5);
+  ElecK<Real> K;
+  if (TERM == kTermElec) K = load_elec_k(c.elec_k);
   for (int base = 0; base < n; base += 32) {
     int i = base + lane;
     bool act = i < n;
@@ -637,7 +671,27 @@ __device__ __noinline__ E3<Real> eval_queue(EvalCtx<Real> c, Slab<Real>* wp,
     int a1 = e & 31, j = (e >> 5) & 127;
     Real wcp = (e >> 12) & 1 ? Real(0.2) : Real(1);
     Real fx = 0, fy = 0, fz = 0;
-    if (act) {
+    if (act && TERM == kTermElec) {
+      const AtomRec<Real> p1 = w.at[a1];
+      const AtomRec<Real> p2 = w.at[j];
+      const Real dx = p1.x - p2.x;
+      const Real dy = p1.y - p2.y;
+      const Real dz = p1.z - p2.z;
+      const Real d2 = dx * dx + dy * dy + dz * dz;
+      // coincident atoms take the flat region and add no force
+      const Real inv_d = inv_sqrt(d2);
+      const Real d = d2 > Real(0) ? d2 * inv_d : Real(0);
+      Real f, df = 0;
+      elec_eval<Real, GRAD>(d, K, f, df);
+      const Real wq = wcp * p1.q * p2.q;
+      acc.atr += wq * f;
+      if (GRAD && d != Real(0)) {
+        const Real g = wq * c.wt0 * df * inv_d;
+        fx = g * dx;
+        fy = g * dy;
+        fz = g * dz;
+      }
+    } else if (act) {
       const AtomRec<Real> p1 = w.at[a1];
       const AtomRec<Real> p2 = w.at[j];
       int t1 = p1.tf & 0xff, t2 = p2.tf & 0xff;
@@ -728,21 +782,21 @@ __device__ __noinline__ E3<Real> eval_queue(EvalCtx<Real> c, Slab<Real>* wp,
   return acc;
 }
 
-template <typename Real, bool GRAD>
+template <typename Real, bool GRAD, int TERM = kTermLJLK>
 __device__ __forceinline__ void drain_queue(const EvalCtx<Real>& c,
                                             Slab<Real>* wp, int& nl, int& nh,
                                             int lane, E3<Real>& acc) {
   __syncwarp();
   cnt_add(wp->counts, 3, nl + nh, lane);
   cnt_add(wp->counts, 4, nh, lane);
-  if (nh) {
+  if (TERM == kTermLJLK && nh) {
     E3<Real> e = eval_queue<Real, GRAD, true>(c, wp, nh, lane);
     acc.atr += e.atr;
     acc.rep += e.rep;
     acc.lk += e.lk;
   }
   if (nl) {
-    E3<Real> e = eval_queue<Real, GRAD, false>(c, wp, nl, lane);
+    E3<Real> e = eval_queue<Real, GRAD, false, TERM>(c, wp, nl, lane);
     acc.atr += e.atr;
     acc.rep += e.rep;
   }
@@ -767,7 +821,7 @@ __device__ __forceinline__ void queue_push(uint16_t* queue, bool in, bool hv,
 // Pairs inside the side-0 tile of c1 atoms (a1 < a2), weights from the
 // intra-block separation table (ljlk_pose_score.impl.hh:115-134; the ligand
 // 3/4 -> 5 rule is already folded into that table and is not applied again).
-template <typename Real, bool GRAD>
+template <typename Real, bool GRAD, int TERM = kTermLJLK>
 __device__ __noinline__ E3<Real> intra_tile(EvalCtx<Real> c, Slab<Real>* wp,
                                             int st1, int c1, int lane) {
   Slab<Real>& w = *wp;
@@ -790,7 +844,7 @@ __device__ __noinline__ E3<Real> intra_tile(EvalCtx<Real> c, Slab<Real>* wp,
         int sep = c.pd[a1 * c.A + st1 + a2];
         in = sep >= 4;
         wbit = sep == 4;
-        hv = in && (p1.tf & p2.tf & kTfHeavy);
+        hv = TERM == kTermLJLK && in && (p1.tf & p2.tf & kTfHeavy);
       }
     }
     queue_push(w.queue, in, hv, a1 | (a2 << 5) | (wbit << 12), lane, nl, nh);
@@ -801,7 +855,7 @@ __device__ __noinline__ E3<Real> intra_tile(EvalCtx<Real> c, Slab<Real>* wp,
       a1 += 1;
     }
   }
-  drain_queue<Real, GRAD>(c, wp, nl, nh, lane, acc);
+  drain_queue<Real, GRAD, TERM>(c, wp, nl, nh, lane, acc);
   return acc;
 }
 
@@ -810,7 +864,7 @@ __device__ __noinline__ E3<Real> intra_tile(EvalCtx<Real> c, Slab<Real>* wp,
 // walk the packed atoms (32 per chunk); side-0 atoms are broadcast one per
 // step, skipping those farther than r_k + max_dis from every slot block's
 // centroid.  Returns the lane's energy sums.
-template <typename Real, bool GRAD>
+template <typename Real, bool GRAD, int TERM = kTermLJLK>
 __device__ __noinline__ E3<Real> screen_slots(EvalCtx<Real> c, Slab<Real>* wp,
                                               int c1, int nc1, int m, int ns,
                                               int lane) {
@@ -836,7 +890,7 @@ __device__ __noinline__ E3<Real> screen_slots(EvalCtx<Real> c, Slab<Real>* wp,
     const int jj = valid ? j : 0;
     const AtomRec<Real> pj = w.at[TILE + jj];
     const Real xj = pj.x, yj = pj.y, zj = pj.z;
-    const int heavy_j = valid ? (pj.tf & kTfHeavy) : 0;
+    const int heavy_j = TERM == kTermLJLK && valid ? (pj.tf & kTfHeavy) : 0;
     const int slot = w.slot1[jj];
     const int kind = w.slot_kind[slot];
     // count-pair classes of this lane's pairs with the active rows, once per
@@ -895,13 +949,13 @@ __device__ __noinline__ E3<Real> screen_slots(EvalCtx<Real> c, Slab<Real>* wp,
       const Real dz = pa.z - zj;
       const Real d2 = dx * dx + dy * dy + dz * dz;
       const bool in = ((live >> a1) & 1u) && d2 < maxd2;
-      const bool hv = in && (heavy_j & pa.tf);
+      const bool hv = TERM == kTermLJLK && in && (heavy_j & pa.tf);
       const int wbit = (w02 >> a1) & 1u;
       queue_push(w.queue, in, hv, a1 | ((TILE + j) << 5) | (wbit << 12), lane, nl, nh);
-      if (nl + nh > QCAP - 32) drain_queue<Real, GRAD>(c, wp, nl, nh, lane, acc);
+      if (nl + nh > QCAP - 32) drain_queue<Real, GRAD, TERM>(c, wp, nl, nh, lane, acc);
     }
   }
-  drain_queue<Real, GRAD>(c, wp, nl, nh, lane, acc);
+  drain_queue<Real, GRAD, TERM>(c, wp, nl, nh, lane, acc);
   return acc;
 }
 
@@ -912,8 +966,26 @@ struct RowPartners {
   int entry;   // its cp table entry
 };
 
+// Adds a warp's block-pair energies to entry `o` of the [n_terms, stride]
+// output (the warp owns the entry).
+template <typename Real, int TERM>
+__device__ __forceinline__ void add_pair_energies(Real* out, int64_t stride, int64_t o,
+                                                  const E3<Real>& e, int lane) {
+  const Real v0 = warp_sum(e.atr);
+  if (TERM == kTermElec) {
+    if (lane == 0) out[o] += v0;
+    return;
+  }
+  const Real v1 = warp_sum(e.rep), v2 = warp_sum(e.lk);
+  if (lane == 0) {
+    out[o] += v0;
+    out[stride + o] += v1;
+    out[2 * stride + o] += v2;
+  }
+}
+
 // Scores the staged slots against side 0 and flushes their gradients.
-template <typename Real, bool GRAD, bool BLOCK_PAIR>
+template <typename Real, bool GRAD, bool BLOCK_PAIR, int TERM>
 __device__ __forceinline__ void score_group(const ScoreArgs<Real>& s,
                                             Slab<Real>& w, const EvalCtx<Real>& c,
                                             const RowInfo& r, int& m, int& ns,
@@ -921,18 +993,10 @@ __device__ __forceinline__ void score_group(const ScoreArgs<Real>& s,
                                             int64_t pair_o, bool want_E) {
   __syncwarp();
   if (m > 0) {
-    E3<Real> e = screen_slots<Real, GRAD>(c, &w, r.c1, r.nc1, m, ns, lane);
+    E3<Real> e = screen_slots<Real, GRAD, TERM>(c, &w, r.c1, r.nc1, m, ns, lane);
     if (GRAD) flush_side1(s, w, m, lane);
     if (BLOCK_PAIR) {
-      if (want_E) {
-        const int64_t stride = (int64_t)s.P * s.B * s.B;
-        Real v0 = warp_sum(e.atr), v1 = warp_sum(e.rep), v2 = warp_sum(e.lk);
-        if (lane == 0) {
-          s.energies[pair_o] += v0;
-          s.energies[stride + pair_o] += v1;
-          s.energies[2 * stride + pair_o] += v2;
-        }
-      }
+      if (want_E) add_pair_energies<Real, TERM>(s.energies, (int64_t)s.P * s.B * s.B, pair_o, e, lane);
     } else {
       acc.atr += e.atr;
       acc.rep += e.rep;
@@ -957,7 +1021,7 @@ __device__ __forceinline__ void score_group(const ScoreArgs<Real>& s,
 #define TMOL_B200_FLOAT_MIN_CTAS 2
 #endif
 
-template <typename Real, bool GRAD, bool BLOCK_PAIR>
+template <typename Real, bool GRAD, bool BLOCK_PAIR, int TERM>
 __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_CTAS : 1)
     score_kernel(ScoreArgs<Real> s, int items_per_ticket) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -998,11 +1062,14 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
       ec.ntp = s.ntp;
       ec.A = s.A;
       ec.max_dis = s.g.max_dis;
+      ec.elec_k = s.elec_k;
       ec.wt0 = ec.wt1 = ec.wt2 = 0;
       if (GRAD && !BLOCK_PAIR) {
         ec.wt0 = s.dTdV[r.p];
-        ec.wt1 = s.dTdV[s.P + r.p];
-        ec.wt2 = s.dTdV[2 * s.P + r.p];
+        if (TERM == kTermLJLK) {
+          ec.wt1 = s.dTdV[s.P + r.p];
+          ec.wt2 = s.dTdV[2 * s.P + r.p];
+        }
       }
       const Real* sph1 = s.spheres + 4 * (int64_t)r.i1;
       const Real c1x = sph1[0], c1y = sph1[1], c1z = sph1[2], rad1 = sph1[3];
@@ -1071,10 +1138,12 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
       for (int ti = 0; ti < nt1; ++ti) {
         r.st1 = ti * TILE;
         r.c1 = min(TILE, r.n1 - r.st1);
-        stage_side0(s, w, r.bt1, r.off1, r.st1, r.c1, r.nc1, lane);
+        stage_side0<Real, TERM>(s, w, r.bt1, r.off1, r.st1, r.c1, r.nc1, lane);
         ec.pd = s.bt_pd + ((int64_t)r.bt1 * s.A + r.st1) * s.A;
         __syncwarp();
-        int h1 = __popc(__ballot_sync(0xffffffffu, lane < r.c1 && (w.at[lane].tf & kTfHeavy)));
+        int h1 = TERM == kTermLJLK
+                     ? __popc(__ballot_sync(0xffffffffu, lane < r.c1 && (w.at[lane].tf & kTfHeavy)))
+                     : 0;
         int m = 0, ns = 0;
         int64_t pair_o = 0;
         for (int bi = 0; bi < n_batches; ++bi) {
@@ -1085,12 +1154,14 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
             int bb2 = cand0 + bi * 32 + k;
             if (bb2 == r.b1) {
               // b1 with itself: this tile with itself, then with b1's later tiles
-              score_group<Real, GRAD, BLOCK_PAIR>(s, w, ec, r, m, ns, lane, acc, pair_o, want_E);
+              score_group<Real, GRAD, BLOCK_PAIR, TERM>(s, w, ec, r, m, ns, lane, acc, pair_o, want_E);
               pair_o = (int64_t)r.i1 * s.B + r.b1;
               if (BLOCK_PAIR && GRAD) {
                 ec.wt0 = s.dTdV[pair_o];
-                ec.wt1 = s.dTdV[stride + pair_o];
-                ec.wt2 = s.dTdV[2 * stride + pair_o];
+                if (TERM == kTermLJLK) {
+                  ec.wt1 = s.dTdV[stride + pair_o];
+                  ec.wt2 = s.dTdV[2 * stride + pair_o];
+                }
               }
               if (ti == 0) {
                 cnt_add(w.counts, 0, 1, lane);
@@ -1098,16 +1169,9 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
               }
               cnt_add(w.counts, 2, (long long)h1 * (h1 - 1) / 2, lane);
               {
-                E3<Real> e = intra_tile<Real, GRAD>(ec, &w, r.st1, r.c1, lane);
+                E3<Real> e = intra_tile<Real, GRAD, TERM>(ec, &w, r.st1, r.c1, lane);
                 if (BLOCK_PAIR) {
-                  if (want_E) {
-                    Real v0 = warp_sum(e.atr), v1 = warp_sum(e.rep), v2 = warp_sum(e.lk);
-                    if (lane == 0) {
-                      s.energies[pair_o] += v0;
-                      s.energies[stride + pair_o] += v1;
-                      s.energies[2 * stride + pair_o] += v2;
-                    }
-                  }
+                  if (want_E) add_pair_energies<Real, TERM>(s.energies, stride, pair_o, e, lane);
                 } else {
                   acc.atr += e.atr;
                   acc.rep += e.rep;
@@ -1125,12 +1189,13 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
                   w.slot_sph[0][2] = c1z;
                   w.slot_sph[0][3] = rad1;
                 }
-                int h2 = __popc(__ballot_sync(
-                    0xffffffffu, lane < c2 && (s.bt_tf[(int64_t)r.bt1 * s.A + st2 + lane] & kTfHeavy)));
+                int h2 = TERM == kTermLJLK ? __popc(__ballot_sync(0xffffffffu,
+                                                                  lane < c2 && (s.bt_tf[(int64_t)r.bt1 * s.A + st2 + lane] & kTfHeavy)))
+                                           : 0;
                 cnt_add(w.counts, 2, (long long)h1 * h2, lane);
-                m = stage_side1(s, w, 0, 0, r.bt1, r.off1, st2, c2, 0, c1x, c1y, c1z, reach1_2, lane);
+                m = stage_side1<Real, TERM>(s, w, 0, 0, r.bt1, r.off1, st2, c2, 0, c1x, c1y, c1z, reach1_2, lane);
                 ns = 1;
-                score_group<Real, GRAD, BLOCK_PAIR>(s, w, ec, r, m, ns, lane, acc, pair_o, want_E);
+                score_group<Real, GRAD, BLOCK_PAIR, TERM>(s, w, ec, r, m, ns, lane, acc, pair_o, want_E);
               }
               continue;
             }
@@ -1156,11 +1221,12 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
             }
             for (int tj = 0; tj < nt2; ++tj) {
               int st2 = tj * TILE, c2 = min(TILE, n2 - st2);
-              int h2 = __popc(__ballot_sync(
-                  0xffffffffu, lane < c2 && (s.bt_tf[(int64_t)bt2 * s.A + st2 + lane] & kTfHeavy)));
+              int h2 = TERM == kTermLJLK ? __popc(__ballot_sync(0xffffffffu,
+                                                                lane < c2 && (s.bt_tf[(int64_t)bt2 * s.A + st2 + lane] & kTfHeavy)))
+                                         : 0;
               cnt_add(w.counts, 2, (long long)h1 * h2, lane);
               if (m + c2 > M1 || ns == max_slots)
-                score_group<Real, GRAD, BLOCK_PAIR>(s, w, ec, r, m, ns, lane, acc, pair_o, want_E);
+                score_group<Real, GRAD, BLOCK_PAIR, TERM>(s, w, ec, r, m, ns, lane, acc, pair_o, want_E);
               if (lane == 0) {
                 w.slot_kind[ns] = kind;
                 w.slot_nc[ns] = nc2;
@@ -1168,7 +1234,7 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
               }
               if (lane < 4) w.slot_sph[ns][lane] = s2[lane];
               if (kind == kSlotStriking && lane < 16) w.seps[ns][lane] = s.cp_seps[(int64_t)e * 16 + lane];
-              int kept = stage_side1(s, w, m, ns, bt2, off2, st2, c2, nc2, c1x, c1y, c1z, reach1_2, lane);
+              int kept = stage_side1<Real, TERM>(s, w, m, ns, bt2, off2, st2, c2, nc2, c1x, c1y, c1z, reach1_2, lane);
               if (kept > 0) {
                 m += kept;
                 ns += 1;
@@ -1177,19 +1243,23 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
                 pair_o = (int64_t)r.i1 * s.B + bb2;
                 if (GRAD) {
                   ec.wt0 = s.dTdV[pair_o];
-                  ec.wt1 = s.dTdV[stride + pair_o];
-                  ec.wt2 = s.dTdV[2 * stride + pair_o];
+                  if (TERM == kTermLJLK) {
+                    ec.wt1 = s.dTdV[stride + pair_o];
+                    ec.wt2 = s.dTdV[2 * stride + pair_o];
+                  }
                 }
               }
             }
           }
         }
-        score_group<Real, GRAD, BLOCK_PAIR>(s, w, ec, r, m, ns, lane, acc, pair_o, want_E);
+        score_group<Real, GRAD, BLOCK_PAIR, TERM>(s, w, ec, r, m, ns, lane, acc, pair_o, want_E);
         if (GRAD) flush_side0(s, w, r.off1, r.st1, r.c1, lane);
         __syncwarp();
       }
       if (!BLOCK_PAIR && want_E) {
-        Real v0 = warp_sum(acc.atr), v1 = warp_sum(acc.rep), v2 = warp_sum(acc.lk);
+        Real v0 = warp_sum(acc.atr);
+        Real v1 = TERM == kTermLJLK ? warp_sum(acc.rep) : Real(0);
+        Real v2 = TERM == kTermLJLK ? warp_sum(acc.lk) : Real(0);
         if (lane == 0) {
           if (v0 != Real(0)) atomicAdd(&s.energies[r.p], v0);
           if (v1 != Real(0)) atomicAdd(&s.energies[s.P + r.p], v1);
@@ -1411,7 +1481,7 @@ __global__ void rot_row_fill_kernel(ScoreArgs<Real> s, RotArgs ra) {
 // group), or against itself on the diagonal.  Energies go to the item's
 // pairs (energies[t * n_pairs + d]; the warp owns them), the adjoint
 // weights come from dTdV[t * n_pairs + d].
-template <typename Real, bool GRAD>
+template <typename Real, bool GRAD, int TERM>
 __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_CTAS : 1)
     rotamer_kernel(ScoreArgs<Real> s, RotArgs ra, const Real* rs) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1445,6 +1515,7 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
     ec.ntp = s.ntp;
     ec.A = s.A;
     ec.max_dis = s.g.max_dis;
+    ec.elec_k = s.elec_k;
     ec.wt0 = ec.wt1 = ec.wt2 = 0;
     const Real* sph1 = rs + 4 * (int64_t)rot1;
     const Real c1x = sph1[0], c1y = sph1[1], c1z = sph1[2], rad1 = sph1[3];
@@ -1469,15 +1540,17 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
     for (int ti = 0; ti < nt1; ++ti) {
       r.st1 = ti * TILE;
       r.c1 = min(TILE, r.n1 - r.st1);
-      stage_side0(s, w, r.bt1, r.off1, r.st1, r.c1, r.nc1, lane);
+      stage_side0<Real, TERM>(s, w, r.bt1, r.off1, r.st1, r.c1, r.nc1, lane);
       ec.pd = s.bt_pd + ((int64_t)r.bt1 * s.A + r.st1) * s.A;
       __syncwarp();
       for (int k = 0; k < n_rot2; ++k) {
         const long long d = pair_first + k;
         if (GRAD) {
           ec.wt0 = s.dTdV[d];
-          ec.wt1 = s.dTdV[np + d];
-          ec.wt2 = s.dTdV[2 * np + d];
+          if (TERM == kTermLJLK) {
+            ec.wt1 = s.dTdV[np + d];
+            ec.wt2 = s.dTdV[2 * np + d];
+          }
         }
         E3<Real> e = {0, 0, 0};
         if (ti == 0) {
@@ -1487,7 +1560,7 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
         }
         if (diag) {
           // this tile with itself, then with the rotamer's later tiles
-          E3<Real> t = intra_tile<Real, GRAD>(ec, &w, r.st1, r.c1, lane);
+          E3<Real> t = intra_tile<Real, GRAD, TERM>(ec, &w, r.st1, r.c1, lane);
           e.atr += t.atr;
           e.rep += t.rep;
           e.lk += t.lk;
@@ -1502,10 +1575,10 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
               w.slot_sph[0][2] = c1z;
               w.slot_sph[0][3] = rad1;
             }
-            const int m = stage_side1(s, w, 0, 0, r.bt1, r.off1, st2, c2, 0, c1x, c1y, c1z, reach1_2, lane);
+            const int m = stage_side1<Real, TERM>(s, w, 0, 0, r.bt1, r.off1, st2, c2, 0, c1x, c1y, c1z, reach1_2, lane);
             __syncwarp();
             if (m > 0) {
-              E3<Real> g = screen_slots<Real, GRAD>(ec, &w, r.c1, r.nc1, m, 1, lane);
+              E3<Real> g = screen_slots<Real, GRAD, TERM>(ec, &w, r.c1, r.nc1, m, 1, lane);
               if (GRAD) flush_side1(s, w, m, lane);
               e.atr += g.atr;
               e.rep += g.rep;
@@ -1534,10 +1607,10 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
             }
             if (lane < 4) w.slot_sph[0][lane] = sph2[lane];
             if (kind == kSlotStriking && lane < 16) w.seps[0][lane] = s.cp_seps[(int64_t)cp_entry * 16 + lane];
-            const int m = stage_side1(s, w, 0, 0, bt2, off2, st2, c2, nc2, c1x, c1y, c1z, reach1_2, lane);
+            const int m = stage_side1<Real, TERM>(s, w, 0, 0, bt2, off2, st2, c2, nc2, c1x, c1y, c1z, reach1_2, lane);
             __syncwarp();
             if (m > 0) {
-              E3<Real> g = screen_slots<Real, GRAD>(ec, &w, r.c1, r.nc1, m, 1, lane);
+              E3<Real> g = screen_slots<Real, GRAD, TERM>(ec, &w, r.c1, r.nc1, m, 1, lane);
               if (GRAD) flush_side1(s, w, m, lane);
               e.atr += g.atr;
               e.rep += g.rep;
@@ -1546,14 +1619,7 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
             __syncwarp();
           }
         }
-        if (want_E) {
-          const Real v0 = warp_sum(e.atr), v1 = warp_sum(e.rep), v2 = warp_sum(e.lk);
-          if (lane == 0) {
-            s.energies[d] += v0;
-            s.energies[np + d] += v1;
-            s.energies[2 * np + d] += v2;
-          }
-        }
+        if (want_E) add_pair_energies<Real, TERM>(s.energies, np, d, e, lane);
       }
       if (GRAD) flush_side0(s, w, r.off1, r.st1, r.c1, lane);
       __syncwarp();
@@ -1720,6 +1786,10 @@ using namespace tmol_b200;
 
 struct tmol_b200_ljlk_plan {
   int real_bytes;
+  int term = kTermLJLK;
+  void* bt_q = nullptr;    // elec: partial charges [nbt * A] reals
+  void* elec_k = nullptr;  // elec: ElecK constants [N_ELEC_K] reals
+  unsigned char elec_k_host[N_ELEC_K * sizeof(double)];
   tmol_b200_ljlk_inputs dims;  // sizes only; pointers are not kept
   int P, B, nbt, A, C, ntiles, T;
   int64_t N;
@@ -1807,7 +1877,8 @@ void free_plan(tmol_b200_ljlk_plan* pl) {
                   pl->item_cost,
                   pl->counters,  pl->counts,     pl->sub_spheres, pl->rot_bt,
                   pl->rot_off,   pl->rot_block,  pl->rot_pose,    pl->nrb,
-                  pl->rob,       pl->rot_spheres, pl->row_pairs,  pl->row_items};
+                  pl->rob,       pl->rot_spheres, pl->row_pairs,  pl->row_items,
+                  pl->bt_q,      pl->elec_k};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t e : pl->prof_events) cudaEventDestroy(e);
@@ -1824,27 +1895,23 @@ void default_launch(tmol_b200_ljlk_launch& l) {
   l.candidates_per_item = std::min(l.candidates_per_item, 32 * 32);
 }
 
+template <typename Real, int TERM>
+cudaError_t set_smem_limits_term() {
+  const int smem = (int)(MAX_WARPS * sizeof(Slab<Real>));
+  const void* kernels[] = {
+      (const void*)score_kernel<Real, false, false, TERM>, (const void*)score_kernel<Real, false, true, TERM>,
+      (const void*)score_kernel<Real, true, false, TERM>,  (const void*)score_kernel<Real, true, true, TERM>,
+      (const void*)rotamer_kernel<Real, false, TERM>,      (const void*)rotamer_kernel<Real, true, TERM>};
+  for (const void* k : kernels) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 template <typename Real>
-cudaError_t set_smem_limits() {
-  int smem = (int)(MAX_WARPS * sizeof(Slab<Real>));
-  cudaError_t e;
-  if ((e = cudaFuncSetAttribute(score_kernel<Real, false, false>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
-    return e;
-  if ((e = cudaFuncSetAttribute(score_kernel<Real, false, true>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
-    return e;
-  if ((e = cudaFuncSetAttribute(score_kernel<Real, true, false>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
-    return e;
-  if ((e = cudaFuncSetAttribute(rotamer_kernel<Real, false>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
-    return e;
-  if ((e = cudaFuncSetAttribute(rotamer_kernel<Real, true>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
-    return e;
-  return cudaFuncSetAttribute(score_kernel<Real, true, true>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+cudaError_t set_smem_limits(int term) {
+  return term == kTermElec ? set_smem_limits_term<Real, kTermElec>() : set_smem_limits_term<Real, kTermLJLK>();
 }
 
 int build_work(tmol_b200_ljlk_plan* pl, cudaStream_t st) {
@@ -1894,11 +1961,18 @@ ScoreArgs<Real> score_args(tmol_b200_ljlk_plan* pl, const void* coords) {
   s.cp_seps = pl->cp_seps;
   s.spheres = (Real*)pl->spheres;
   const Real* gp = (const Real*)pl->global_params;
-  s.g.max_dis = gp[0];
-  s.g.lj_dlin_sigma_factor = gp[1];
-  s.g.lj_hbond_dis = gp[2];
-  s.g.lj_hbond_OH_donor_dis = gp[3];
-  s.g.lj_hbond_hdis = gp[4];
+  if (pl->term == kTermElec) {
+    // elec global parameters: D, D0, S, min_dis, max_dis
+    s.g.max_dis = gp[4];
+    s.bt_q = (const Real*)pl->bt_q;
+    s.elec_k = (const Real*)pl->elec_k;
+  } else {
+    s.g.max_dis = gp[0];
+    s.g.lj_dlin_sigma_factor = gp[1];
+    s.g.lj_hbond_dis = gp[2];
+    s.g.lj_hbond_OH_donor_dis = gp[3];
+    s.g.lj_hbond_hdis = gp[4];
+  }
   s.reach = (Real)pl->reach;
   s.work = pl->work;
   s.item_cost = pl->item_cost;
@@ -1925,7 +1999,8 @@ int launch_score(tmol_b200_ljlk_plan* pl, ScoreArgs<Real> s, cudaStream_t st) {
   if (pl->n_work == 0) return TMOL_B200_OK;
   int warps = pl->launch.warps_per_cta;
   size_t smem = warps * sizeof(Slab<Real>);
-  auto kern = score_kernel<Real, GRAD, BLOCK_PAIR>;
+  auto kern = pl->term == kTermElec ? score_kernel<Real, GRAD, BLOCK_PAIR, kTermElec>
+                                    : score_kernel<Real, GRAD, BLOCK_PAIR, kTermLJLK>;
   int R = pl->launch.rows_per_item;
   int n_tickets = (pl->n_work + R - 1) / R;
   int grid = std::max(1, std::min((n_tickets + warps - 1) / warps, pl->n_sm * pl->launch.ctas_per_sm));
@@ -1946,7 +2021,8 @@ int forward_impl(tmol_b200_ljlk_plan* pl, const void* coords, int block_pair,
   ScoreArgs<Real> s = score_args<Real>(pl, coords);
   s.energies = (Real*)energies;
   s.nbr = nbr;
-  size_t n_e = block_pair ? (size_t)3 * pl->P * pl->B * pl->B : (size_t)3 * pl->P;
+  const size_t nt = n_terms(pl->term);
+  size_t n_e = block_pair ? nt * pl->P * pl->B * pl->B : nt * pl->P;
   CK(cudaMemsetAsync(energies, 0, n_e * sizeof(Real), st));
   if (nbr) CK(cudaMemsetAsync(nbr, 0, (size_t)pl->P * pl->B * pl->B * sizeof(int32_t), st));
   CK(cudaMemsetAsync(pl->counts, 0, N_COUNTS * sizeof(unsigned long long), st));
@@ -1975,7 +2051,7 @@ int energy_and_gradient_impl(tmol_b200_ljlk_plan* pl, const void* coords,
   s.dcoords = (Real*)dcoords;
   s.energies = (Real*)energies;
   CK(cudaMemsetAsync(dcoords, 0, (size_t)pl->N * 3 * sizeof(Real), st));
-  CK(cudaMemsetAsync(energies, 0, (size_t)3 * pl->P * sizeof(Real), st));
+  CK(cudaMemsetAsync(energies, 0, (size_t)n_terms(pl->term) * pl->P * sizeof(Real), st));
   CK(cudaMemsetAsync(pl->counts, 0, N_COUNTS * sizeof(unsigned long long), st));
   return launch_score<Real, true, false>(pl, s, st);
 }
@@ -2061,7 +2137,7 @@ int rotamer_score_impl(tmol_b200_ljlk_plan* pl, const void* coords, const int32_
   s.dcoords = (Real*)dcoords;
   s.counts = GRAD ? nullptr : pl->counts;
   if (!GRAD) CK(cudaMemsetAsync(pl->counts, 0, N_COUNTS * sizeof(unsigned long long), st));
-  if (energies) CK(cudaMemsetAsync(energies, 0, (size_t)3 * n_pairs * sizeof(Real), st));
+  if (energies) CK(cudaMemsetAsync(energies, 0, (size_t)n_terms(pl->term) * n_pairs * sizeof(Real), st));
   if (dcoords) CK(cudaMemsetAsync(dcoords, 0, (size_t)pl->N * 3 * sizeof(Real), st));
   if (n_items == 0) return TMOL_B200_OK;
   if (pl->R > 0) {
@@ -2074,7 +2150,10 @@ int rotamer_score_impl(tmol_b200_ljlk_plan* pl, const void* coords, const int32_
   const size_t smem = warps * sizeof(Slab<Real>);
   int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n_items + warps - 1) / warps,
                                                          (int64_t)pl->n_sm * pl->launch.ctas_per_sm));
-  rotamer_kernel<Real, GRAD><<<grid, 32 * warps, smem, st>>>(s, ra, (const Real*)pl->rot_spheres);
+  if (pl->term == kTermElec)
+    rotamer_kernel<Real, GRAD, kTermElec><<<grid, 32 * warps, smem, st>>>(s, ra, (const Real*)pl->rot_spheres);
+  else
+    rotamer_kernel<Real, GRAD, kTermLJLK><<<grid, 32 * warps, smem, st>>>(s, ra, (const Real*)pl->rot_spheres);
   CK(cudaGetLastError());
   return TMOL_B200_OK;
 }
@@ -2100,10 +2179,18 @@ const char* tmol_b200_status_string(int status) {
 
 namespace {
 
+// What an elec plan needs beyond the shared inputs (whose bt_path_distance
+// is then the intra-block representative table).
+struct ElecExtra {
+  const void* partial_charge;      // [nbt, A] reals
+  const int32_t* inter_repr_pd;    // [nbt, A, A]
+};
+
 int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
                 const tmol_b200_ljlk_launch* launch, void* stream, bool rotamers,
-                tmol_b200_ljlk_plan** plan_out) {
+                tmol_b200_ljlk_plan** plan_out, const ElecExtra* elec = nullptr) {
   if (!in || !plan_out) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  const int term = elec ? kTermElec : kTermLJLK;
   *plan_out = nullptr;
   if (real_bytes != 4 && real_bytes != 8) return TMOL_B200_ERR_DTYPE;
   const int P = in->n_poses, B = in->max_n_blocks, nbt = in->n_block_types;
@@ -2119,16 +2206,28 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
   const void* req[] = {in->rot_coord_offset, in->first_rot_block_type, in->block_ind_for_rot,
                        in->pose_ind_for_rot, in->block_type_ind_for_rot, in->rot_offset_for_block,
                        in->min_bondsep, in->inter_block_bondsep, in->bt_n_atoms,
-                       in->bt_n_heavy_atoms_in_tile, in->bt_heavy_atoms_in_tile, in->bt_atom_types,
                        in->bt_n_conn, in->bt_conn_atom, in->bt_path_distance,
-                       in->bt_is_ligand_fragment, in->type_params, in->global_params};
-  if (P * B > 0 && nbt > 0)
+                       in->bt_is_ligand_fragment, in->global_params};
+  const void* req_ljlk[] = {in->bt_n_heavy_atoms_in_tile, in->bt_heavy_atoms_in_tile, in->bt_atom_types,
+                            in->type_params};
+  const void* req_elec[] = {elec ? elec->partial_charge : nullptr, elec ? elec->inter_repr_pd : nullptr};
+  if (P * B > 0 && nbt > 0) {
     for (const void* r : req)
       if (!r) return TMOL_B200_ERR_INVALID_ARGUMENT;
+    if (term == kTermLJLK) {
+      for (const void* r : req_ljlk)
+        if (!r) return TMOL_B200_ERR_INVALID_ARGUMENT;
+    } else {
+      for (const void* r : req_elec)
+        if (!r) return TMOL_B200_ERR_INVALID_ARGUMENT;
+    }
+  }
+  if (!in->global_params) return TMOL_B200_ERR_INVALID_ARGUMENT;
 
   cudaStream_t st = (cudaStream_t)stream;
   auto* pl = new tmol_b200_ljlk_plan();
   pl->real_bytes = real_bytes;
+  pl->term = term;
   pl->dims = *in;
   pl->P = P;
   pl->B = B;
@@ -2152,7 +2251,7 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
   } while (0)
   PCK(cudaGetDevice(&dev));
   PCK(cudaDeviceGetAttribute(&pl->n_sm, cudaDevAttrMultiProcessorCount, dev));
-  PCK(real_bytes == 4 ? set_smem_limits<float>() : set_smem_limits<double>());
+  PCK(real_bytes == 4 ? set_smem_limits<float>(term) : set_smem_limits<double>(term));
   const int64_t PB = (int64_t)P * B;
   PCK(dalloc(pl, &pl->blk_bt, PB));
   PCK(dalloc(pl, &pl->blk_off, PB));
@@ -2173,6 +2272,13 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
   if (real_bytes == 4) PCK(dalloc(pl, &pl->sub_spheres, PB * 8));
   PCK(dalloc(pl, &pl->counters, 4));
   PCK(dalloc(pl, &pl->counts, N_COUNTS));
+  if (term == kTermElec) {
+    PCK(dalloc(pl, (unsigned char**)&pl->bt_q, (size_t)nbt * A * real_bytes));
+    PCK(dalloc(pl, (unsigned char**)&pl->elec_k, (size_t)N_ELEC_K * real_bytes));
+    if (nbt > 0 && A > 0)
+      PCK(cudaMemcpyAsync(pl->bt_q, elec->partial_charge, (size_t)nbt * A * real_bytes,
+                          cudaMemcpyDeviceToDevice, st));
+  }
 
   PCK(cudaMemsetAsync(pl->pose_last, 0, sizeof(int) * std::max(P, 1), st));
   PCK(cudaMemsetAsync(pl->counters, 0, sizeof(int) * 4, st));
@@ -2197,6 +2303,8 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
   a.cp_minsep = pl->cp_minsep;
   a.cp_seps = pl->cp_seps;
   a.status = pl->counters + 1;
+  a.term = term;
+  a.bt_inter_pd = elec ? elec->inter_repr_pd : nullptr;
   a.rotamers = rotamers ? 1 : 0;
   a.rot_bt = a.rot_off = a.rot_block = a.rot_pose = nullptr;
   if (rotamers) {
@@ -2231,7 +2339,7 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
     plan_blocks_kernel<<<g, 256, 0, st>>>(a);
     PCK(cudaGetLastError());
   }
-  if (nbt > 0) {
+  if (nbt > 0 && term == kTermLJLK) {
     int gh = std::max(1, std::min(((nbt * nt * TILE) + 255) / 256, pl->n_sm * 8));
     plan_heavy_kernel<<<gh, 256, 0, st>>>(a);
     PCK(cudaGetLastError());
@@ -2248,10 +2356,11 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
     PCK(cudaMemcpyAsync(pl->host_pose_last.data(), pl->pose_last, sizeof(int) * P,
                         cudaMemcpyDeviceToHost, st));
   // compact atom types: the types the block types use, in index order
-  std::vector<int> h_types((size_t)nbt * A), h_nat(std::max(nbt, 1));
+  std::vector<int> h_types(term == kTermLJLK ? (size_t)nbt * A : 0), h_nat(std::max(nbt, 1));
   if (nbt > 0) {
-    PCK(cudaMemcpyAsync(h_types.data(), in->bt_atom_types, sizeof(int) * h_types.size(),
-                        cudaMemcpyDeviceToHost, st));
+    if (term == kTermLJLK)
+      PCK(cudaMemcpyAsync(h_types.data(), in->bt_atom_types, sizeof(int) * h_types.size(),
+                          cudaMemcpyDeviceToHost, st));
     PCK(cudaMemcpyAsync(h_nat.data(), in->bt_n_atoms, sizeof(int) * nbt, cudaMemcpyDeviceToHost, st));
   }
   PCK(cudaStreamSynchronize(st));
@@ -2261,7 +2370,7 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
     return rc;
   }
   std::vector<int> type_map(std::max(T, 1), -1), compact;
-  for (int bt = 0; bt < nbt; ++bt) {
+  for (int bt = 0; term == kTermLJLK && bt < nbt; ++bt) {
     int n = std::min(std::max(h_nat[bt], 0), A);
     for (int k = 0; k < n; ++k) {
       int t = h_types[(size_t)bt * A + k];
@@ -2294,6 +2403,24 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
     plan_block_types_kernel<<<gb, 256, 0, st>>>(a, pl->type_map, pl->bt_tf);
     PCK(cudaGetLastError());
   }
+  if (term == kTermElec) {
+    // the potential's constants from the five global parameters, which the
+    // reference passes to the potential as floats
+    double k[N_ELEC_K];
+    float gpf[5];
+    for (int i = 0; i < 5; ++i)
+      gpf[i] = real_bytes == 4 ? ((const float*)pl->global_params)[i]
+                               : (float)((const double*)pl->global_params)[i];
+    elec_constants(gpf[0], gpf[1], gpf[2], gpf[3], gpf[4], k);
+    for (int i = 0; i < N_ELEC_K; ++i) {
+      if (real_bytes == 4)
+        ((float*)pl->elec_k_host)[i] = (float)k[i];
+      else
+        ((double*)pl->elec_k_host)[i] = k[i];
+    }
+    PCK(cudaMemcpyAsync(pl->elec_k, pl->elec_k_host, (size_t)N_ELEC_K * real_bytes, cudaMemcpyHostToDevice,
+                        st));
+  }
   if (pl->ntp > 0) {
     int gt = std::max(1, std::min((int)((ntp2 + 127) / 128), pl->n_sm * 8));
     if (real_bytes == 4)
@@ -2322,6 +2449,131 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
 #undef PCK
   *plan_out = pl;
   return TMOL_B200_OK;
+}
+
+tmol_b200_ljlk_inputs shared_inputs(const tmol_b200_elec_inputs* e) {
+  tmol_b200_ljlk_inputs in = {};
+  in.n_atoms = e->n_atoms;
+  in.n_poses = e->n_poses;
+  in.max_n_blocks = e->max_n_blocks;
+  in.n_rots = e->n_rots;
+  in.n_block_types = e->n_block_types;
+  in.max_n_block_atoms = e->max_n_block_atoms;
+  in.max_n_conn = e->max_n_conn;
+  in.max_n_tiles = (e->max_n_block_atoms + TILE - 1) / TILE;
+  in.n_atom_types = 0;
+  in.rot_coord_offset = e->rot_coord_offset;
+  in.pose_ind_for_atom = e->pose_ind_for_atom;
+  in.first_rot_for_block = e->first_rot_for_block;
+  in.first_rot_block_type = e->first_rot_block_type;
+  in.block_ind_for_rot = e->block_ind_for_rot;
+  in.pose_ind_for_rot = e->pose_ind_for_rot;
+  in.block_type_ind_for_rot = e->block_type_ind_for_rot;
+  in.n_rots_for_pose = e->n_rots_for_pose;
+  in.rot_offset_for_pose = e->rot_offset_for_pose;
+  in.n_rots_for_block = e->n_rots_for_block;
+  in.rot_offset_for_block = e->rot_offset_for_block;
+  in.max_n_rots_per_pose = e->max_n_rots_per_pose;
+  in.min_bondsep = e->min_bondsep;
+  in.inter_block_bondsep = e->inter_block_bondsep;
+  in.bt_n_atoms = e->bt_n_atoms;
+  in.bt_n_conn = e->bt_n_conn;
+  in.bt_conn_atom = e->bt_conn_atom;
+  in.bt_path_distance = e->bt_intra_repr_path_distance;
+  in.bt_is_ligand_fragment = e->bt_is_ligand_fragment;
+  in.global_params = e->global_params;
+  in.max_dis = e->max_dis;
+  return in;
+}
+
+int create_elec_plan(const tmol_b200_elec_inputs* e, int real_bytes, const tmol_b200_ljlk_launch* launch,
+                     void* stream, bool rotamers, tmol_b200_ljlk_plan** plan_out) {
+  if (!e || !plan_out) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  const tmol_b200_ljlk_inputs in = shared_inputs(e);
+  const ElecExtra x = {e->bt_partial_charge, e->bt_inter_repr_path_distance};
+  return create_plan(&in, real_bytes, launch, stream, rotamers, plan_out, &x);
+}
+
+bool pose_plan_of(const tmol_b200_ljlk_plan* plan, int term) {
+  return plan && !plan->rotamers && plan->term == term;
+}
+
+bool rotamer_plan_of(const tmol_b200_ljlk_plan* plan, int term) {
+  return plan && plan->rotamers && plan->term == term;
+}
+
+int pose_forward(tmol_b200_ljlk_plan* plan, int term, const void* coords, int block_pair, void* energies,
+                 int32_t* block_neighbors, void* stream) {
+  if (!pose_plan_of(plan, term) || !energies || (!coords && plan->N > 0))
+    return TMOL_B200_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->real_bytes == 4)
+    return forward_impl<float>(plan, coords, block_pair, energies, block_neighbors, st);
+  return forward_impl<double>(plan, coords, block_pair, energies, block_neighbors, st);
+}
+
+int pose_backward(tmol_b200_ljlk_plan* plan, int term, const void* coords, int block_pair, const void* dTdV,
+                  void* dcoords, void* stream) {
+  if (!pose_plan_of(plan, term) || !dTdV || !dcoords || (!coords && plan->N > 0))
+    return TMOL_B200_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->real_bytes == 4)
+    return backward_impl<float>(plan, coords, block_pair, dTdV, dcoords, st);
+  return backward_impl<double>(plan, coords, block_pair, dTdV, dcoords, st);
+}
+
+int pose_energy_and_gradient(tmol_b200_ljlk_plan* plan, int term, const void* coords, const void* weights,
+                             void* energies, void* dcoords, void* stream) {
+  if (!pose_plan_of(plan, term) || !weights || !energies || !dcoords || (!coords && plan->N > 0))
+    return TMOL_B200_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->real_bytes == 4)
+    return energy_and_gradient_impl<float>(plan, coords, weights, energies, dcoords, st);
+  return energy_and_gradient_impl<double>(plan, coords, weights, energies, dcoords, st);
+}
+
+int rotamer_count(tmol_b200_ljlk_plan* plan, int term, const void* coords, int64_t* n_pairs,
+                  int64_t* n_items, void* stream) {
+  if (!rotamer_plan_of(plan, term) || !n_pairs || !n_items || (!coords && plan->N > 0))
+    return TMOL_B200_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->real_bytes == 4) return rotamer_count_impl<float>(plan, coords, n_pairs, n_items, st);
+  return rotamer_count_impl<double>(plan, coords, n_pairs, n_items, st);
+}
+
+int rotamer_fill(tmol_b200_ljlk_plan* plan, int term, int32_t* indices, int32_t* items, void* stream) {
+  if (!rotamer_plan_of(plan, term) || plan->n_pairs < 0) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  if ((plan->n_pairs > 0 && !indices) || (plan->n_items > 0 && !items))
+    return TMOL_B200_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->real_bytes == 4) return rotamer_fill_impl<float>(plan, indices, items, st);
+  return rotamer_fill_impl<double>(plan, indices, items, st);
+}
+
+int rotamer_forward(tmol_b200_ljlk_plan* plan, int term, const void* coords, const int32_t* items,
+                    int64_t n_items, int64_t n_pairs, void* energies, void* stream) {
+  if (!rotamer_plan_of(plan, term) || !energies || n_items < 0 || n_pairs < 0 || (n_items > 0 && !items) ||
+      (!coords && plan->N > 0))
+    return TMOL_B200_ERR_INVALID_ARGUMENT;
+  if (n_items >= ((int64_t)1 << 31) || n_pairs >= ((int64_t)1 << 31)) return TMOL_B200_ERR_CAPACITY;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->real_bytes == 4)
+    return rotamer_score_impl<float, false>(plan, coords, items, n_items, n_pairs, energies, nullptr, nullptr,
+                                            st);
+  return rotamer_score_impl<double, false>(plan, coords, items, n_items, n_pairs, energies, nullptr, nullptr,
+                                           st);
+}
+
+int rotamer_backward(tmol_b200_ljlk_plan* plan, int term, const void* coords, const int32_t* items,
+                     int64_t n_items, int64_t n_pairs, const void* dTdV, void* dcoords, void* stream) {
+  if (!rotamer_plan_of(plan, term) || !dTdV || !dcoords || n_items < 0 || n_pairs < 0 ||
+      (n_items > 0 && !items) || (!coords && plan->N > 0))
+    return TMOL_B200_ERR_INVALID_ARGUMENT;
+  if (n_items >= ((int64_t)1 << 31) || n_pairs >= ((int64_t)1 << 31)) return TMOL_B200_ERR_CAPACITY;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->real_bytes == 4)
+    return rotamer_score_impl<float, true>(plan, coords, items, n_items, n_pairs, nullptr, dTdV, dcoords, st);
+  return rotamer_score_impl<double, true>(plan, coords, items, n_items, n_pairs, nullptr, dTdV, dcoords, st);
 }
 
 }  // namespace
@@ -2359,35 +2611,20 @@ int tmol_b200_ljlk_plan_set_launch(tmol_b200_ljlk_plan* plan,
 int tmol_b200_ljlk_forward(tmol_b200_ljlk_plan* plan, const void* coords,
                            int block_pair, void* energies,
                            int32_t* block_neighbors, void* stream) {
-  if (!plan || !energies || (!coords && plan->N > 0) || plan->rotamers)
-    return TMOL_B200_ERR_INVALID_ARGUMENT;
-  cudaStream_t st = (cudaStream_t)stream;
-  if (plan->real_bytes == 4)
-    return forward_impl<float>(plan, coords, block_pair, energies, block_neighbors, st);
-  return forward_impl<double>(plan, coords, block_pair, energies, block_neighbors, st);
+  return pose_forward(plan, kTermLJLK, coords, block_pair, energies, block_neighbors, stream);
 }
 
 int tmol_b200_ljlk_backward(tmol_b200_ljlk_plan* plan, const void* coords,
                             int block_pair, const void* dTdV, void* dcoords,
                             void* stream) {
-  if (!plan || !dTdV || !dcoords || (!coords && plan->N > 0) || plan->rotamers)
-    return TMOL_B200_ERR_INVALID_ARGUMENT;
-  cudaStream_t st = (cudaStream_t)stream;
-  if (plan->real_bytes == 4)
-    return backward_impl<float>(plan, coords, block_pair, dTdV, dcoords, st);
-  return backward_impl<double>(plan, coords, block_pair, dTdV, dcoords, st);
+  return pose_backward(plan, kTermLJLK, coords, block_pair, dTdV, dcoords, stream);
 }
 
 int tmol_b200_ljlk_energy_and_gradient(tmol_b200_ljlk_plan* plan,
                                        const void* coords, const void* weights,
                                        void* energies, void* dcoords,
                                        void* stream) {
-  if (!plan || !weights || !energies || !dcoords || (!coords && plan->N > 0) || plan->rotamers)
-    return TMOL_B200_ERR_INVALID_ARGUMENT;
-  cudaStream_t st = (cudaStream_t)stream;
-  if (plan->real_bytes == 4)
-    return energy_and_gradient_impl<float>(plan, coords, weights, energies, dcoords, st);
-  return energy_and_gradient_impl<double>(plan, coords, weights, energies, dcoords, st);
+  return pose_energy_and_gradient(plan, kTermLJLK, coords, weights, energies, dcoords, stream);
 }
 
 int tmol_b200_ljlk_last_counts(tmol_b200_ljlk_plan* plan, void* stream,
@@ -2521,51 +2758,83 @@ int tmol_b200_ljlk_screen_candidates(tmol_b200_ljlk_plan* plan,
 
 int tmol_b200_ljlk_rotamer_count(tmol_b200_ljlk_plan* plan, const void* coords,
                                   int64_t* n_pairs, int64_t* n_items, void* stream) {
-  if (!plan || !plan->rotamers || !n_pairs || !n_items || (!coords && plan->N > 0))
-    return TMOL_B200_ERR_INVALID_ARGUMENT;
-  cudaStream_t st = (cudaStream_t)stream;
-  if (plan->real_bytes == 4) return rotamer_count_impl<float>(plan, coords, n_pairs, n_items, st);
-  return rotamer_count_impl<double>(plan, coords, n_pairs, n_items, st);
+  return rotamer_count(plan, kTermLJLK, coords, n_pairs, n_items, stream);
 }
 
 int tmol_b200_ljlk_rotamer_fill(tmol_b200_ljlk_plan* plan, int32_t* indices, int32_t* items,
                                 void* stream) {
-  if (!plan || !plan->rotamers || plan->n_pairs < 0) return TMOL_B200_ERR_INVALID_ARGUMENT;
-  if ((plan->n_pairs > 0 && !indices) || (plan->n_items > 0 && !items))
-    return TMOL_B200_ERR_INVALID_ARGUMENT;
-  cudaStream_t st = (cudaStream_t)stream;
-  if (plan->real_bytes == 4) return rotamer_fill_impl<float>(plan, indices, items, st);
-  return rotamer_fill_impl<double>(plan, indices, items, st);
+  return rotamer_fill(plan, kTermLJLK, indices, items, stream);
 }
 
 int tmol_b200_ljlk_rotamer_forward(tmol_b200_ljlk_plan* plan, const void* coords,
                                     const int32_t* items, int64_t n_items, int64_t n_pairs,
                                     void* energies, void* stream) {
-  if (!plan || !plan->rotamers || !energies || n_items < 0 || n_pairs < 0 ||
-      (n_items > 0 && !items) || (!coords && plan->N > 0))
-    return TMOL_B200_ERR_INVALID_ARGUMENT;
-  if (n_items >= ((int64_t)1 << 31) || n_pairs >= ((int64_t)1 << 31)) return TMOL_B200_ERR_CAPACITY;
-  cudaStream_t st = (cudaStream_t)stream;
-  if (plan->real_bytes == 4)
-    return rotamer_score_impl<float, false>(plan, coords, items, n_items, n_pairs, energies, nullptr,
-                                            nullptr, st);
-  return rotamer_score_impl<double, false>(plan, coords, items, n_items, n_pairs, energies, nullptr,
-                                           nullptr, st);
+  return rotamer_forward(plan, kTermLJLK, coords, items, n_items, n_pairs, energies, stream);
 }
 
 int tmol_b200_ljlk_rotamer_backward(tmol_b200_ljlk_plan* plan, const void* coords,
                                      const int32_t* items, int64_t n_items, int64_t n_pairs,
                                      const void* dTdV, void* dcoords, void* stream) {
-  if (!plan || !plan->rotamers || !dTdV || !dcoords || n_items < 0 || n_pairs < 0 ||
-      (n_items > 0 && !items) || (!coords && plan->N > 0))
-    return TMOL_B200_ERR_INVALID_ARGUMENT;
-  if (n_items >= ((int64_t)1 << 31) || n_pairs >= ((int64_t)1 << 31)) return TMOL_B200_ERR_CAPACITY;
-  cudaStream_t st = (cudaStream_t)stream;
-  if (plan->real_bytes == 4)
-    return rotamer_score_impl<float, true>(plan, coords, items, n_items, n_pairs, nullptr, dTdV,
-                                           dcoords, st);
-  return rotamer_score_impl<double, true>(plan, coords, items, n_items, n_pairs, nullptr, dTdV,
-                                          dcoords, st);
+  return rotamer_backward(plan, kTermLJLK, coords, items, n_items, n_pairs, dTdV, dcoords, stream);
+}
+
+// ---------------------------------------------------------------------------
+// elec entry points (include/tmol_b200_elec.h)
+
+int tmol_b200_elec_plan_create(const tmol_b200_elec_inputs* in, int real_bytes,
+                               const tmol_b200_ljlk_launch* launch, void* stream,
+                               tmol_b200_elec_plan** plan_out) {
+  return create_elec_plan(in, real_bytes, launch, stream, false, plan_out);
+}
+
+int tmol_b200_elec_rotamer_plan_create(const tmol_b200_elec_inputs* in, int real_bytes,
+                                       const tmol_b200_ljlk_launch* launch, void* stream,
+                                       tmol_b200_elec_plan** plan_out) {
+  return create_elec_plan(in, real_bytes, launch, stream, true, plan_out);
+}
+
+int tmol_b200_elec_plan_destroy(tmol_b200_elec_plan* plan) {
+  if (!plan || plan->term != kTermElec) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  free_plan(plan);
+  return TMOL_B200_OK;
+}
+
+int tmol_b200_elec_forward(tmol_b200_elec_plan* plan, const void* coords, int block_pair,
+                           void* energies, int32_t* block_neighbors, void* stream) {
+  return pose_forward(plan, kTermElec, coords, block_pair, energies, block_neighbors, stream);
+}
+
+int tmol_b200_elec_backward(tmol_b200_elec_plan* plan, const void* coords, int block_pair,
+                            const void* dTdV, void* dcoords, void* stream) {
+  return pose_backward(plan, kTermElec, coords, block_pair, dTdV, dcoords, stream);
+}
+
+int tmol_b200_elec_energy_and_gradient(tmol_b200_elec_plan* plan, const void* coords,
+                                       const void* weights, void* energies, void* dcoords,
+                                       void* stream) {
+  return pose_energy_and_gradient(plan, kTermElec, coords, weights, energies, dcoords, stream);
+}
+
+int tmol_b200_elec_rotamer_count(tmol_b200_elec_plan* plan, const void* coords,
+                                 int64_t* n_pairs, int64_t* n_items, void* stream) {
+  return rotamer_count(plan, kTermElec, coords, n_pairs, n_items, stream);
+}
+
+int tmol_b200_elec_rotamer_fill(tmol_b200_elec_plan* plan, int32_t* indices, int32_t* items,
+                                void* stream) {
+  return rotamer_fill(plan, kTermElec, indices, items, stream);
+}
+
+int tmol_b200_elec_rotamer_forward(tmol_b200_elec_plan* plan, const void* coords,
+                                   const int32_t* items, int64_t n_items, int64_t n_pairs,
+                                   void* energies, void* stream) {
+  return rotamer_forward(plan, kTermElec, coords, items, n_items, n_pairs, energies, stream);
+}
+
+int tmol_b200_elec_rotamer_backward(tmol_b200_elec_plan* plan, const void* coords,
+                                    const int32_t* items, int64_t n_items, int64_t n_pairs,
+                                    const void* dTdV, void* dcoords, void* stream) {
+  return rotamer_backward(plan, kTermElec, coords, items, n_items, n_pairs, dTdV, dcoords, stream);
 }
 
 int64_t tmol_b200_ljlk_plan_device_bytes(const tmol_b200_ljlk_plan* plan) {

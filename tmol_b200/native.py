@@ -1,5 +1,5 @@
-"""ctypes binding of the C ABI in ``include/tmol_b200_ljlk.h`` and
-``include/tmol_b200_screen.h``.
+"""ctypes binding of the C ABI in ``include/tmol_b200_ljlk.h``,
+``include/tmol_b200_elec.h`` and ``include/tmol_b200_screen.h``.
 
 The shared library is built in-tree (``tmol_b200/lib``) by
 ``tmol_b200.build``.  There is no fallback: importing this module without the
@@ -52,6 +52,43 @@ class Inputs(ctypes.Structure):
         ("bt_path_distance", ctypes.c_void_p),
         ("bt_is_ligand_fragment", ctypes.c_void_p),
         ("type_params", ctypes.c_void_p),
+        ("global_params", ctypes.c_void_p),
+        ("max_dis", ctypes.c_double),
+    ]
+
+
+class ElecInputs(ctypes.Structure):
+    """``tmol_b200_elec_inputs``."""
+
+    _fields_ = [
+        ("n_atoms", ctypes.c_int64),
+        ("n_poses", ctypes.c_int32),
+        ("max_n_blocks", ctypes.c_int32),
+        ("n_rots", ctypes.c_int32),
+        ("n_block_types", ctypes.c_int32),
+        ("max_n_block_atoms", ctypes.c_int32),
+        ("max_n_conn", ctypes.c_int32),
+        ("rot_coord_offset", ctypes.c_void_p),
+        ("pose_ind_for_atom", ctypes.c_void_p),
+        ("first_rot_for_block", ctypes.c_void_p),
+        ("first_rot_block_type", ctypes.c_void_p),
+        ("block_ind_for_rot", ctypes.c_void_p),
+        ("pose_ind_for_rot", ctypes.c_void_p),
+        ("block_type_ind_for_rot", ctypes.c_void_p),
+        ("n_rots_for_pose", ctypes.c_void_p),
+        ("rot_offset_for_pose", ctypes.c_void_p),
+        ("n_rots_for_block", ctypes.c_void_p),
+        ("rot_offset_for_block", ctypes.c_void_p),
+        ("max_n_rots_per_pose", ctypes.c_int32),
+        ("min_bondsep", ctypes.c_void_p),
+        ("inter_block_bondsep", ctypes.c_void_p),
+        ("bt_n_atoms", ctypes.c_void_p),
+        ("bt_partial_charge", ctypes.c_void_p),
+        ("bt_n_conn", ctypes.c_void_p),
+        ("bt_conn_atom", ctypes.c_void_p),
+        ("bt_inter_repr_path_distance", ctypes.c_void_p),
+        ("bt_intra_repr_path_distance", ctypes.c_void_p),
+        ("bt_is_ligand_fragment", ctypes.c_void_p),
         ("global_params", ctypes.c_void_p),
         ("max_dis", ctypes.c_double),
     ]
@@ -137,6 +174,25 @@ SIGNATURES = {
     "tmol_b200_ljlk_rotamer_fill": (ctypes.c_int, [_V, _V, _V, _V]),
     "tmol_b200_ljlk_rotamer_forward": (ctypes.c_int, [_V, _V, _V, _I64, _I64, _V, _V]),
     "tmol_b200_ljlk_rotamer_backward": (ctypes.c_int, [_V, _V, _V, _I64, _I64, _V, _V, _V]),
+    # elec (include/tmol_b200_elec.h)
+    "tmol_b200_elec_plan_create": (
+        ctypes.c_int,
+        [ctypes.POINTER(ElecInputs), ctypes.c_int, ctypes.POINTER(Launch), _V, ctypes.POINTER(ctypes.c_void_p)],
+    ),
+    "tmol_b200_elec_rotamer_plan_create": (
+        ctypes.c_int,
+        [ctypes.POINTER(ElecInputs), ctypes.c_int, ctypes.POINTER(Launch), _V, ctypes.POINTER(ctypes.c_void_p)],
+    ),
+    "tmol_b200_elec_plan_destroy": (ctypes.c_int, [_V]),
+    "tmol_b200_elec_forward": (ctypes.c_int, [_V, _V, ctypes.c_int, _V, _V, _V]),
+    "tmol_b200_elec_backward": (ctypes.c_int, [_V, _V, ctypes.c_int, _V, _V, _V]),
+    "tmol_b200_elec_energy_and_gradient": (ctypes.c_int, [_V, _V, _V, _V, _V, _V]),
+    "tmol_b200_elec_rotamer_count": (
+        ctypes.c_int, [_V, _V, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64), _V]
+    ),
+    "tmol_b200_elec_rotamer_fill": (ctypes.c_int, [_V, _V, _V, _V]),
+    "tmol_b200_elec_rotamer_forward": (ctypes.c_int, [_V, _V, _V, _I64, _I64, _V, _V]),
+    "tmol_b200_elec_rotamer_backward": (ctypes.c_int, [_V, _V, _V, _I64, _I64, _V, _V, _V]),
     # learned block-pair screen (include/tmol_b200_screen.h)
     "tmol_b200_ljlk_plan_set_skip_mask": (ctypes.c_int, [_V, _V, _I32]),
     "tmol_b200_ljlk_screen_candidates": (ctypes.c_int, [_V, _V, _I32, _V, _V, _V, _V, _V, _V]),

@@ -7,10 +7,10 @@ residue name, the block's variants in order, then the unpatched entry) and
 the count-pair *representative* path distances: ``inter[a, b]`` is the number
 of bonds between atom a and the representative of atom b, and ``intra[a, b]``
 the number between the representatives of a and b, with 3 and 4 read as 5
-in non-polymer blocks (full weight for 1-4 pairs in ligands).  Its op,
-``elec_pose_scores`` (``tmol_b200.score.elec_op``), takes the same leading
-PoseStack arguments as the LJ/LK op and returns one energy per pose (or per
-block pair).
+in non-polymer blocks (full weight for 1-4 pairs in ligands).  Its ops,
+``elec_pose_scores`` and ``elec_rotamer_scores`` (``tmol_b200.score.elec_op``),
+take the same leading PoseStack (or rotamer-set) arguments as the LJ/LK ops
+and return one energy per pose, block pair or rotamer pair.
 """
 
 import json
@@ -191,6 +191,21 @@ class ElecEnergyTerm:
             self.get_pose_score_term_function(),
         )
 
+    def get_rotamer_score_term_function(self):
+        from .elec_op import elec_rotamer_scores
+
+        return elec_rotamer_scores
+
+    def render_rotamer_scoring_module(self, pose_stack, rotamer_set):
+        """tmol ``energy_term.py:132-147``: the rotamer-pair scoring module
+        over ``rotamer_set``."""
+        from .scoring_module import TermRotamerScoringModule
+
+        return TermRotamerScoringModule(
+            self.class_name(), rotamer_set, self.get_score_term_attributes(pose_stack),
+            self.get_rotamer_score_term_function(),
+        )
+
 
 def elec_pose_score_args(pose_stack, term, block_pair=False):
     """The elec op's argument list minus the coordinates (tmol
@@ -210,3 +225,13 @@ def elec_pose_score_args(pose_stack, term, block_pair=False):
         pose_stack.max_n_rots_per_pose,
     ]
     return common + term.get_score_term_attributes(pose_stack) + [block_pair]
+
+
+def elec_rotamer_score_args(pose_stack, rotamer_set, term):
+    """The elec rotamer op's argument list minus the coordinates: the rotamer
+    set's indexing (as ``TermRotamerScoringModule`` passes it,
+    tmol/score/common/scoring_module.py:133-170), the pose's term
+    attributes and ``output_block_pair_energies=True``."""
+    from .ljlk_energy_term import rotamer_score_args
+
+    return rotamer_score_args(pose_stack, rotamer_set, term)

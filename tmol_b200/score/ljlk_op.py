@@ -28,6 +28,10 @@ class LJLKPlan:
     block) or, with ``rotamers=True``, of the rotamer op (any number of
     rotamers per block)."""
 
+    N_TERMS = 3  # fa_ljatr, fa_ljrep, fa_lk
+    ABI = "tmol_b200_ljlk"  # prefix of the scoring entry points
+    NAME = "LJ/LK"
+
     def __init__(self, coords_like, static_args, launch=None, rotamers=False):
         (
             rot_coord_offset,
@@ -56,13 +60,7 @@ class LJLKPlan:
             global_params,
             max_dis,
         ) = static_args
-        device = coords_like.device
-        if device.type != "cuda":
-            raise RuntimeError("tmol_b200 LJ/LK scoring runs on CUDA tensors only")
-        self.device = device
-        self.dtype = coords_like.dtype
-        if self.dtype not in (torch.float32, torch.float64):
-            raise TypeError(f"coordinates must be float32 or float64, got {self.dtype}")
+        device = self._set_device(coords_like)
         ints = dict(
             rot_coord_offset=rot_coord_offset,
             pose_ind_for_atom=pose_ind_for_atom,
@@ -129,21 +127,35 @@ class LJLKPlan:
         self.n_poses, self.max_n_blocks = P, B
         self.n_atoms = pose_ind_for_atom.shape[0]
         s.n_atoms = self.n_atoms
+        self._create(s, launch, rotamers)
+        del keep
+
+    def _set_device(self, coords_like):
+        device = coords_like.device
+        if device.type != "cuda":
+            raise RuntimeError(f"tmol_b200 {self.NAME} scoring runs on CUDA tensors only")
+        self.device = device
+        self.dtype = coords_like.dtype
+        if self.dtype not in (torch.float32, torch.float64):
+            raise TypeError(f"coordinates must be float32 or float64, got {self.dtype}")
+        return device
+
+    def _create(self, inputs, launch, rotamers):
+        """Calls the plan-create entry point on the filled inputs struct."""
         self.launch = native.Launch(*(launch or (0, 0, 0, 0)))
         self.rotamers = bool(rotamers)
         ptr = ctypes.c_void_p()
-        with torch.cuda.device(device):
-            stream = torch.cuda.current_stream(device).cuda_stream
+        with torch.cuda.device(self.device):
+            stream = torch.cuda.current_stream(self.device).cuda_stream
             native.call(
-                "tmol_b200_ljlk_rotamer_plan_create" if rotamers else "tmol_b200_ljlk_plan_create",
-                ctypes.byref(s),
+                f"{self.ABI}_rotamer_plan_create" if rotamers else f"{self.ABI}_plan_create",
+                ctypes.byref(inputs),
                 4 if self.dtype == torch.float32 else 8,
                 ctypes.byref(self.launch),
                 ctypes.c_void_p(stream),
                 ctypes.byref(ptr),
             )
         self.ptr = ptr
-        del keep
 
     def __del__(self):
         ptr = getattr(self, "ptr", None)
@@ -186,12 +198,12 @@ class LJLKPlan:
         self._check_coords(coords)
         coords = coords.contiguous()
         P, B = self.n_poses, self.max_n_blocks
-        shape = (3, P, B, B) if block_pair else (3, P)
+        shape = (self.N_TERMS, P, B, B) if block_pair else (self.N_TERMS, P)
         if energies is None:
             energies = torch.empty(shape, dtype=self.dtype, device=self.device)
         nbr = torch.empty((P, B, B), dtype=torch.int32, device=self.device) if want_neighbors else None
         native.call(
-            "tmol_b200_ljlk_forward",
+            f"{self.ABI}_forward",
             self.ptr,
             ctypes.c_void_p(coords.data_ptr()),
             int(block_pair),
@@ -208,7 +220,7 @@ class LJLKPlan:
         if dcoords is None:
             dcoords = torch.empty_like(coords)
         native.call(
-            "tmol_b200_ljlk_backward",
+            f"{self.ABI}_backward",
             self.ptr,
             ctypes.c_void_p(coords.data_ptr()),
             int(block_pair),
@@ -219,18 +231,19 @@ class LJLKPlan:
         return dcoords
 
     def energy_and_gradient(self, coords, weights, energies=None, dcoords=None):
-        """Energies [3, P] and sum_t weights[t, pose] * dE_t/dcoords in one pass."""
+        """Energies [n_terms, P] and sum_t weights[t, pose] * dE_t/dcoords in
+        one pass."""
         self._check_coords(coords)
         coords = coords.contiguous()
         weights = weights.to(self.dtype).contiguous()
-        if tuple(weights.shape) != (3, self.n_poses):
-            raise ValueError(f"weights must be [3, {self.n_poses}]")
+        if tuple(weights.shape) != (self.N_TERMS, self.n_poses):
+            raise ValueError(f"weights must be [{self.N_TERMS}, {self.n_poses}]")
         if energies is None:
-            energies = torch.empty((3, self.n_poses), dtype=self.dtype, device=self.device)
+            energies = torch.empty((self.N_TERMS, self.n_poses), dtype=self.dtype, device=self.device)
         if dcoords is None:
             dcoords = torch.empty_like(coords)
         native.call(
-            "tmol_b200_ljlk_energy_and_gradient",
+            f"{self.ABI}_energy_and_gradient",
             self.ptr,
             ctypes.c_void_p(coords.data_ptr()),
             ctypes.c_void_p(weights.data_ptr()),
@@ -258,37 +271,37 @@ class LJLKPlan:
         coords = coords.contiguous()
         n_pairs, n_items = ctypes.c_int64(), ctypes.c_int64()
         native.call(
-            "tmol_b200_ljlk_rotamer_count", self.ptr, ctypes.c_void_p(coords.data_ptr()),
+            f"{self.ABI}_rotamer_count", self.ptr, ctypes.c_void_p(coords.data_ptr()),
             ctypes.byref(n_pairs), ctypes.byref(n_items), self._stream(),
         )
         indices = torch.empty((3, n_pairs.value), dtype=torch.int32, device=self.device)
         items = torch.empty((n_items.value, 4), dtype=torch.int32, device=self.device)
         native.call(
-            "tmol_b200_ljlk_rotamer_fill", self.ptr, ctypes.c_void_p(indices.data_ptr() if n_pairs.value else 0),
+            f"{self.ABI}_rotamer_fill", self.ptr, ctypes.c_void_p(indices.data_ptr() if n_pairs.value else 0),
             ctypes.c_void_p(items.data_ptr() if n_items.value else 0), self._stream(),
         )
         return indices, items
 
     def rotamer_forward(self, coords, items, n_pairs):
-        """Energies [3, n_pairs] of the dispatched rotamer pairs."""
+        """Energies [n_terms, n_pairs] of the dispatched rotamer pairs."""
         self._check_coords(coords)
         coords = coords.contiguous()
-        energies = torch.empty((3, n_pairs), dtype=self.dtype, device=self.device)
+        energies = torch.empty((self.N_TERMS, n_pairs), dtype=self.dtype, device=self.device)
         native.call(
-            "tmol_b200_ljlk_rotamer_forward", self.ptr, ctypes.c_void_p(coords.data_ptr()),
+            f"{self.ABI}_rotamer_forward", self.ptr, ctypes.c_void_p(coords.data_ptr()),
             ctypes.c_void_p(items.data_ptr() if items.numel() else 0), items.shape[0], n_pairs,
             ctypes.c_void_p(energies.data_ptr()), self._stream(),
         )
         return energies
 
     def rotamer_backward(self, coords, items, dTdV):
-        """dL/dcoords from dL/dE [3, n_pairs]."""
+        """dL/dcoords from dL/dE [n_terms, n_pairs]."""
         self._check_coords(coords)
         coords = coords.contiguous()
         dTdV = dTdV.to(self.dtype).contiguous()
         dcoords = torch.empty_like(coords)
         native.call(
-            "tmol_b200_ljlk_rotamer_backward", self.ptr, ctypes.c_void_p(coords.data_ptr()),
+            f"{self.ABI}_rotamer_backward", self.ptr, ctypes.c_void_p(coords.data_ptr()),
             ctypes.c_void_p(items.data_ptr() if items.numel() else 0), items.shape[0], dTdV.shape[1],
             ctypes.c_void_p(dTdV.data_ptr()), ctypes.c_void_p(dcoords.data_ptr()), self._stream(),
         )
@@ -395,13 +408,14 @@ def _plan_key(coords, static):
     return tuple(parts)
 
 
-def get_plan(coords, static, rotamers=False):
-    key = (rotamers,) + _plan_key(coords, static)
+def get_plan(coords, static, rotamers=False, plan_class=None):
+    plan_class = plan_class or LJLKPlan
+    key = (plan_class, rotamers) + _plan_key(coords, static)
     entry = _PLAN_CACHE.get(key)
     if entry is not None:
         _PLAN_CACHE.move_to_end(key)
         return entry[0]
-    plan = LJLKPlan(coords, static, rotamers=rotamers)
+    plan = plan_class(coords, static, rotamers=rotamers)
     # the static tensors are held so that their addresses cannot be reused
     # by other tensors while the key is cached
     _PLAN_CACHE[key] = (plan, [t for t in static if isinstance(t, torch.Tensor)])
