@@ -16,6 +16,11 @@ Arms:
                     its sources into oracle/_ref), on all host cores: one
                     process per core, each scoring a slice of the poses.
 
+Other workloads (--workload): the uneven 256-pose batch, rotamer-pair
+scoring (rotamers16x150) and the elec term on the uniform batch
+(elec64x150: per-pose fa_elec and the gradient of its sum).  The default
+line also carries an "elec" summary measured on the same batch.
+
 Under torchrun each rank scores its own batch (independent seeds); the
 timing is the maximum over ranks (weak scaling, no collective on the data
 path).  Prints one JSON line (rank 0).
@@ -49,12 +54,18 @@ ROT_POSES = 16
 ROT_RES = 150
 ROT_SET = dict(max_rots=31, mutate_fraction=0.25, seed=9)
 ROT_METRIC = "LJ+LK rotamer-pair energies/s (16 poses x 150 residues, 1-31 rotamers per block, 1 B200)"
+ELEC_METRIC = "elec energy+grad poses/s (64x150-residue batch, 1 B200)"
 
 # Algorithmic FLOPs per unit (E + dE), counted on the restatement's most
 # populated branch (far cubic fade, 4.5-6 A); FMA = 2, div/sqrt/exp/floor = 1.
 F_PAIR_TEST = 8  # every atom pair of a neighbouring block pair: distance^2 test
 F_LJ = 64  # each pair inside max_dis with non-zero count-pair weight
 F_LK = 111  # each heavy-atom pair among those (both LK directions)
+# elec: each pair inside max_dis with non-zero count-pair weight, counted on
+# the restatement's Coulomb branch (1.85-4.5 A, the most populated):
+# distance and unit vector 12, eps 14, deps 10, E 4, dE 8, weights 2,
+# energy sum 1, gradient on both atoms 9, charge product 1
+F_ELEC = 61
 
 
 def workload_sizes(name, rank):
@@ -62,7 +73,7 @@ def workload_sizes(name, rank):
 
     from tmol_b200.pose.synthetic import log_uniform_sizes
 
-    if name == "uniform64x150":
+    if name in ("uniform64x150", "elec64x150"):
         return [N_RES] * N_POSES, [rank * N_POSES + k for k in range(N_POSES)]
     rng = numpy.random.default_rng(UNEVEN_SEED + 1000 * rank)
     sizes = log_uniform_sizes(rng, UNEVEN_POSES, 20, 1000)
@@ -89,6 +100,8 @@ def rotamer_workload(rank, device, sizes=None, seeds=None):
 
 
 def workload_label(name):
+    if name == "elec64x150":
+        return f"{N_POSES} poses x {N_RES} residues, fa_elec energy + gradient"
     if name == "uniform64x150":
         return f"{N_POSES} poses x {N_RES} residues, energy + gradient, weights {list(TERM_WEIGHTS)}"
     return (
@@ -236,22 +249,36 @@ def cpu_reference_sample(ps, term, reps=3):
     return kind, best
 
 
-def _ref_worker(conn, sizes, seeds):
+def _ref_worker(conn, sizes, seeds, elec=False):
     """One single-threaded process of the reference arm: builds its share of
-    the poses (same sizes and seeds as the GPU arm) and scores it on demand."""
+    the poses (same sizes and seeds as the GPU arm) and scores it on demand
+    (LJ/LK, or elec with `elec`)."""
     import torch
 
     torch.set_num_threads(1)
     from oracle import oracle as O
     from tmol_b200.pose.synthetic import synthetic_pose_stack
-    from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm, pose_score_args
 
     ps = synthetic_pose_stack(sizes, seeds)
-    args = pose_score_args(ps, LJLKEnergyTerm())
     coords = ps.coords.flatten(0, 1).clone()
-    op = O.load_reference() if O.reference_available() else None
-    oc = None if op is not None else O.OracleCall(coords, args)
-    w = torch.tensor(TERM_WEIGHTS)[:, None]
+    if elec:
+        from tmol_b200.score.elec_energy_term import ElecEnergyTerm, elec_pose_score_args
+
+        args = elec_pose_score_args(ps, ElecEnergyTerm())
+        if O.reference_elec_available():
+            O.reference_elec_pose_scores(coords, args)  # loads the op library
+            op = torch.ops.tmol_elec.elec_pose_scores
+        else:
+            op = None
+        oc = None if op is not None else O.OracleCall(coords, args, term="elec")
+        w = torch.ones((1, 1))
+    else:
+        from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm, pose_score_args
+
+        args = pose_score_args(ps, LJLKEnergyTerm())
+        op = O.load_reference() if O.reference_available() else None
+        oc = None if op is not None else O.OracleCall(coords, args)
+        w = torch.tensor(TERM_WEIGHTS)[:, None]
     conn.send("ready")
     while True:
         msg = conn.recv()
@@ -301,6 +328,7 @@ def run_reference(args, world, rank):
         return 0
     if args.workload == "rotamers16x150":
         return run_reference_rotamers(args)
+    elec = args.workload == "elec64x150"
     sizes, seeds = workload_sizes(args.workload, 0)
     n_poses = len(sizes)
     n_proc = min(os.cpu_count() or 1, n_poses)
@@ -316,7 +344,7 @@ def run_reference(args, world, rank):
         parent, child = ctx.Pipe()
         pr = ctx.Process(
             target=_ref_worker,
-            args=(child, [sizes[k] for k in share], [seeds[k] for k in share]),
+            args=(child, [sizes[k] for k in share], [seeds[k] for k in share], elec),
         )
         pr.start()
         workers.append((pr, parent))
@@ -339,10 +367,13 @@ def run_reference(args, world, rank):
         pr.join()
     t = sum(times)
     value = n_poses * args.steps / t
-    kind = "reference" if O.reference_available() else "port"
+    if elec:
+        kind = "reference" if O.reference_elec_available() else "port"
+    else:
+        kind = "reference" if O.reference_available() else "port"
     line = {
         "impl": "reference",
-        "metric": METRIC,
+        "metric": ELEC_METRIC if elec else METRIC,
         "value": value,
         "unit": "poses/s",
         "n_gpus": args.gpus,
@@ -733,6 +764,234 @@ def measure_screen(plan, plan64, coords, weights, step, flush, steps, names, pla
     }
 
 
+def elec_plan_for(ps, coords, launch_shape=None):
+    """An elec plan of the batch (float32), on the launch shape given."""
+    import torch
+
+    from tmol_b200.score.elec_energy_term import ElecEnergyTerm, elec_pose_score_args
+    from tmol_b200.score.elec_op import ElecPlan
+
+    dev = coords.device
+    static = [a.to(dev) if isinstance(a, torch.Tensor) else a for a in elec_pose_score_args(ps, ElecEnergyTerm())[:-1]]
+    plan = ElecPlan(coords, static)
+    if launch_shape:
+        plan.set_launch(*launch_shape)
+    return plan
+
+
+def measure_elec(plan, coords, flush, steps):
+    """elec energy + gradient on the batch: graph-replayed step time (L2
+    flushed before each), the scoring kernel's average launch time and its
+    FP32 figures."""
+    import torch
+
+    P = plan.n_poses
+    w = torch.ones((1, P), device=coords.device)
+    E = torch.empty((1, P), device=coords.device)
+    dx = torch.empty_like(coords)
+
+    def step():
+        plan.energy_and_gradient(coords, w, E, dx)
+
+    step()
+    plan.rebalance()
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    counts = plan.last_counts()
+    ms = time_replays(step, steps, flush) / steps
+    plan.profile(True)
+    for _ in range(steps):
+        flush.zero_()
+        step()
+    kern_ms, n_launch = plan.profile_read()
+    plan.profile(False)
+    kern = kern_ms / max(n_launch, 1)
+    flops = counts["atom_pairs"] * F_PAIR_TEST + counts["atom_pairs_in_range"] * F_ELEC
+    return {
+        "ms_per_step": ms,
+        "poses_per_s": P / (ms / 1e3),
+        "kernel_ms": kern,
+        "flops_per_launch": flops,
+        "achieved_tflops": flops / (kern * 1e-3) / 1e12,
+        "work_per_step": {k: counts[k] for k in ("block_pairs", "atom_pairs", "atom_pairs_in_range")},
+    }, step
+
+
+def cpu_elec_sample(ps, reps=3):
+    """tmol's CPU elec op (oracle/_ref/elec, else the C restatement) on the
+    whole batch, energies + gradient, single thread; best of `reps`."""
+    import torch
+
+    from oracle import oracle as O
+    from tmol_b200.score.elec_energy_term import ElecEnergyTerm, elec_pose_score_args
+
+    torch.set_num_threads(1)
+    args = elec_pose_score_args(ps, ElecEnergyTerm())
+    coords = ps.coords.flatten(0, 1)
+    if O.reference_elec_available():
+        kind = "reference"
+
+        def run():
+            E, c, _ = O.reference_elec_pose_scores(coords, args, require_gradient=True)
+            E.sum().backward()
+
+    else:
+        kind = "port"
+        oc = O.OracleCall(coords, args, term="elec")
+
+        def run():
+            oc.pose_scores(require_gradient=True)
+
+    run()
+    best = float("inf")
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        run()
+        best = min(best, time.perf_counter() - t0)
+    return kind, best
+
+
+def run_elec(args, world, rank, local):
+    """The elec term on the uniform batch: per-pose fa_elec and the gradient
+    of its sum, one fused pass per step, replayed as a CUDA graph."""
+    import torch
+
+    from tmol_b200 import native
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    sizes, seeds = workload_sizes("uniform64x150", rank)
+    ps = workload(rank, "uniform64x150", device=dev)
+    coords = ps.coords.flatten(0, 1).to(dev).contiguous()
+    launch = tuple(int(v) for v in args.launch.split(",")) if args.launch else (1, 8, 2, 64)
+    plan = elec_plan_for(ps, coords, launch)
+    P = ps.n_poses
+    del ps
+    flush = torch.empty(L2_FLUSH_BYTES // 4, device=dev, dtype=torch.float32)
+    # warm-up: W graph replays (and the work order from one call's costs)
+    m, step = measure_elec(plan, coords, flush, max(args.warmup, 3))
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        step()
+        torch.cuda.synchronize()
+        with torch.cuda.graph(g, stream=s):
+            step()
+    torch.cuda.current_stream().wait_stream(s)
+    for _ in range(max(args.warmup, 3)):
+        g.replay()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record()
+            g.replay()
+            ev[k][1].record()
+        torch.cuda.synchronize()
+    barrier(world)
+    ms_max = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), world)
+    poses_total = sum_over_ranks(P * args.steps, world)
+    value = poses_total / (ms_max / 1e3)
+    m, _ = measure_elec(plan, coords, flush, args.steps)
+
+    # end to end with host buffers: pinned coordinates in, energies and
+    # gradient out
+    w = torch.ones((1, P), device=dev)
+    E = torch.empty((1, P), device=dev)
+    dx = torch.empty_like(coords)
+    h_coords = coords.cpu().pin_memory()
+    h_E = torch.empty((1, P), pin_memory=True)
+    h_g = torch.empty(coords.shape, pin_memory=True)
+    d_in = torch.empty_like(coords)
+    e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier(world)
+    for k in range(args.steps):
+        flush.zero_()
+        e2e_ev[k][0].record()
+        d_in.copy_(h_coords, non_blocking=True)
+        plan.energy_and_gradient(d_in, w, E, dx)
+        h_E.copy_(E, non_blocking=True)
+        h_g.copy_(dx, non_blocking=True)
+        e2e_ev[k][1].record()
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in e2e_ev), world)
+
+    fp32_peak = native.measure_fp32_peak_tflops(torch.cuda.current_stream().cuda_stream)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from tmol_b200.pose.synthetic import synthetic_pose_stack
+
+        kind, t = cpu_elec_sample(synthetic_pose_stack(sizes, seeds))
+        cpu = {
+            "value": len(sizes) / t,
+            "unit": "poses/s",
+            "cores": 1,
+            "kind": kind,
+            "sample": f"the full {len(sizes)}x{N_RES} batch, elec energies + gradient, best of 3, one thread",
+        }
+    if rank == 0:
+        line = {
+            "metric": ELEC_METRIC,
+            "value": value,
+            "unit": "poses/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded proteins, ideal geometry)",
+            "config": {
+                "workload": f"{N_POSES} poses x {N_RES} residues, fa_elec energy + gradient",
+                "poses_per_gpu": P,
+                "atoms_per_gpu": int(coords.shape[0]),
+                "l2": "flushed (256 MiB write) before every timed step",
+                "launch": "CUDA graph replay: 2 kernels per step",
+                "launch_shape": dict(
+                    zip(("items_per_ticket", "warps_per_cta", "ctas_per_sm", "candidates_per_item"), launch)
+                ),
+                "parallelism": f"weak, {world} independent batch(es)",
+            },
+            "work_per_step": m["work_per_step"],
+            "gpu_launches": 2 * args.steps,
+            "clocks": clk.summary(),
+            "roofline": {
+                "bound": "fp32",
+                "achieved": m["achieved_tflops"],
+                "peak": fp32_peak,
+                "unit": "TFLOP/s",
+                "frac": m["achieved_tflops"] / fp32_peak,
+                "traffic": None,
+                "kernel": "score_kernel<float, GRAD, elec> (fused neighbour + atom-pair energy and gradient)",
+                "kernel_ms": m["kernel_ms"],
+                "flops_per_launch": m["flops_per_launch"],
+                "peak_source": "measured: FMA-loop probe over all SMs in this run (tmol_b200_measure_fp32_peak)",
+            },
+            "e2e": {
+                "value": poses_total / (e2e_ms / 1e3),
+                "unit": "poses/s",
+                "h2d_bytes_per_step": coords.numel() * 4,
+                "d2h_bytes_per_step": (P + coords.numel()) * 4,
+            },
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    del g
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
 def run_b200(args, world, rank, local):
     import torch
 
@@ -749,6 +1008,7 @@ def run_b200(args, world, rank, local):
     coords = ps.coords.flatten(0, 1).to(dev).contiguous()
     plan = LJLKPlan(coords, static)
     plan64 = None if args.no_screen else LJLKPlan(coords.double(), static)
+    eplan = None if args.no_elec else elec_plan_for(ps, coords)
     bt_names = [bt.name for bt in ps.packed_block_types.active_block_types]
     del static
     P = ps.n_poses
@@ -864,6 +1124,15 @@ def run_b200(args, world, rank, local):
         del plan64
 
     fp32_peak = native.measure_fp32_peak_tflops(torch.cuda.current_stream().cuda_stream)
+    elec = None
+    if eplan is not None:
+        # the elec term on the same batch and launch shape (its own workload
+        # line: --workload elec64x150)
+        eplan.set_launch(*launch_shape)
+        elec, _ = measure_elec(eplan, coords, flush, args.steps)
+        elec["roofline_frac"] = elec["achieved_tflops"] / fp32_peak
+        elec["metric"] = ELEC_METRIC
+        del eplan
     flops = flops_per_step(counts)
     achieved = flops / (kern_avg_ms * 1e-3) / 1e12
 
@@ -926,6 +1195,7 @@ def run_b200(args, world, rank, local):
             },
             "cpu_baseline": cpu,
             "screened": screened,
+            "elec": elec,
         }
         print(json.dumps(line), flush=True)
     del g
@@ -942,9 +1212,12 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="uniform64x150", choices=["uniform64x150", "uneven256", "rotamers16x150"])
+    ap.add_argument(
+        "--workload", default="uniform64x150", choices=["uniform64x150", "uneven256", "rotamers16x150", "elec64x150"]
+    )
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-screen", action="store_true", help="skip the learned-screen measurement")
+    ap.add_argument("--no-elec", action="store_true", help="skip the elec summary of the default line")
     ap.add_argument(
         "--launch",
         default="",
@@ -959,6 +1232,8 @@ def main():
     world, rank, local = dist_setup()
     if args.workload == "rotamers16x150":
         return run_rotamers(args, world, rank, local)
+    if args.workload == "elec64x150":
+        return run_elec(args, world, rank, local)
     return run_b200(args, world, rank, local)
 
 

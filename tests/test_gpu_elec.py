@@ -128,8 +128,9 @@ def test_block_pair_backward_and_energy_and_gradient(eterm):
     E1, dx1 = plan.energy_and_gradient(coords, wp)
     E0, _ = plan.forward(coords, want_neighbors=False)
     dx0 = plan.backward(coords, wp)
-    E_close(E1.cpu().numpy(), E0.cpu().numpy(), rtol=1e-6, atol=1e-6)
-    g_close(dx1.cpu().numpy(), dx0.cpu().numpy(), rtol=1e-6)
+    # the same pair terms, summed by atomics in another order
+    E_close(E1.cpu().numpy(), E0.cpu().numpy(), rtol=1e-5, atol=1e-5)
+    g_close(dx1.cpu().numpy(), dx0.cpu().numpy(), rtol=1e-5)
 
 
 def test_gradcheck_float64(eterm):
@@ -140,7 +141,9 @@ def test_gradcheck_float64(eterm):
     def f(x):
         return elec_pose_scores(x, *args)[0]
 
-    assert torch.autograd.gradcheck(f, (c,), eps=1e-6, atol=1e-5, rtol=1e-3)
+    # gradient atomics add in a run-dependent order: repeated backward
+    # passes agree to rounding, not bit for bit
+    assert torch.autograd.gradcheck(f, (c,), eps=1e-6, atol=1e-5, rtol=1e-3, nondet_tol=1e-10)
 
 
 def test_exotic_blocks_against_oracle(eterm):

@@ -632,13 +632,15 @@ __device__ __forceinline__ void flush_side1(const ScoreArgs<Real>& s,
 // What the out-of-line screening and evaluation functions need, by value.
 template <typename Real>
 struct EvalCtx {
-  const LJRecord<Real>* ljtab;
+  union {
+    const LJRecord<Real>* ljtab;  // LJ/LK
+    const Real* elec_k;           // elec: ElecK constants
+  };
   const LKRecord<Real>* lktab;
   const uint8_t* pd;  // intra-block separations of b1, row st1 (tile start)
   int ntp, A;
   Real max_dis;
   Real wt0, wt1, wt2;  // gradient weights of the three terms (elec: wt0)
-  const Real* elec_k;  // elec plans: ElecK constants
 };
 
 template <typename Real>
@@ -1057,12 +1059,14 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
       r.lig1 = s.bt_is_ligand[r.bt1];
       E3<Real> acc = {0, 0, 0};
       EvalCtx<Real> ec;
-      ec.ljtab = s.ljtab;
+      if (TERM == kTermElec)
+        ec.elec_k = s.elec_k;
+      else
+        ec.ljtab = s.ljtab;
       ec.lktab = s.lktab;
       ec.ntp = s.ntp;
       ec.A = s.A;
       ec.max_dis = s.g.max_dis;
-      ec.elec_k = s.elec_k;
       ec.wt0 = ec.wt1 = ec.wt2 = 0;
       if (GRAD && !BLOCK_PAIR) {
         ec.wt0 = s.dTdV[r.p];
@@ -1510,12 +1514,14 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
     r.nc1 = s.bt_n_conn[r.bt1];
     r.lig1 = s.bt_is_ligand[r.bt1];
     EvalCtx<Real> ec;
-    ec.ljtab = s.ljtab;
+    if (TERM == kTermElec)
+      ec.elec_k = s.elec_k;
+    else
+      ec.ljtab = s.ljtab;
     ec.lktab = s.lktab;
     ec.ntp = s.ntp;
     ec.A = s.A;
     ec.max_dis = s.g.max_dis;
-    ec.elec_k = s.elec_k;
     ec.wt0 = ec.wt1 = ec.wt2 = 0;
     const Real* sph1 = rs + 4 * (int64_t)rot1;
     const Real c1x = sph1[0], c1y = sph1[1], c1z = sph1[2], rad1 = sph1[3];
