@@ -864,12 +864,22 @@ def run_elec(args, world, rank, local):
     sizes, seeds = workload_sizes("uniform64x150", rank)
     ps = workload(rank, "uniform64x150", device=dev)
     coords = ps.coords.flatten(0, 1).to(dev).contiguous()
-    launch = tuple(int(v) for v in args.launch.split(",")) if args.launch else (1, 8, 2, 64)
-    plan = elec_plan_for(ps, coords, launch)
+    plan = elec_plan_for(ps, coords)
     P = ps.n_poses
     del ps
     flush = torch.empty(L2_FLUSH_BYTES // 4, device=dev, dtype=torch.float32)
-    # warm-up: W graph replays (and the work order from one call's costs)
+    # warm-up: W graph replays (and the work order from one call's costs),
+    # then the launch shape: given, or autotuned as the LJ/LK arm does
+    m, step = measure_elec(plan, coords, flush, max(args.warmup, 3))
+    if args.launch:
+        launch = tuple(int(v) for v in args.launch.split(","))
+        plan.set_launch(*launch)
+        step()
+        plan.rebalance()
+    else:
+        from tmol_b200.tune import autotune
+
+        launch, _ = autotune(plan, step, use_cache=False)
     m, step = measure_elec(plan, coords, flush, max(args.warmup, 3))
     g = torch.cuda.CUDAGraph()
     s = torch.cuda.Stream()

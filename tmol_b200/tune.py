@@ -33,7 +33,8 @@ def _cache_path():
 
 def signature(plan, mean_block_atoms):
     name = torch.cuda.get_device_name(plan.device)
-    return f"{name}|P={plan.n_poses}|B={plan.max_n_blocks}|atoms/block={mean_block_atoms:.0f}|{plan.dtype}"
+    term = getattr(plan, "NAME", "LJ/LK")
+    return f"{name}|{term}|P={plan.n_poses}|B={plan.max_n_blocks}|atoms/block={mean_block_atoms:.0f}|{plan.dtype}"
 
 
 def _load_cache():
