@@ -10,7 +10,10 @@ wrapper registering ``torch.ops.tmol_ljlk.ljlk_pose_scores`` and
 ``ljlk_rotamer_scores``) and
 ``tmol/score/ljlk/potentials/ljlk_pose_score.cpu.cpp`` (the CPU instantiation
 of the dispatch); the elec op (``torch.ops.tmol_elec.elec_pose_scores``) is
-the two matching files under ``tmol/score/elec/potentials``.  Both use
+the two matching files under ``tmol/score/elec/potentials``; the stacked
+all-pairs-shortest-paths op (``torch.ops.tmol_apsp.apsp_op``, the PoseStack
+builder's bond-separation step) is ``tmol/pose/compiled/apsp_vestibule.ops.cpp``
+with ``apsp.cpu.cpp``.  All use
 header-only code under ``tmol/`` and the
 vendored Eigen / moderngpu headers in ``tmol/extern``.  They are compiled in
 place with g++ -O3 through torch's extension builder (no reference build
@@ -28,6 +31,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 LIB_NAME = "tmol_ljlk_ref"
 ELEC_LIB_NAME = "tmol_elec_ref"
+APSP_LIB_NAME = "tmol_apsp_ref"
 
 
 def lib_path():
@@ -38,16 +42,26 @@ def elec_lib_path():
     return os.path.join(OUT, "elec", ELEC_LIB_NAME + ".so")
 
 
+def apsp_lib_path():
+    return os.path.join(OUT, "apsp", APSP_LIB_NAME + ".so")
+
+
 def build(ref=REF_DEFAULT, verbose=False):
     from torch.utils.cpp_extension import load
 
     t0 = time.time()
     # each op in its own build directory: both have a compiled.ops.cpp
     for name, sub, srcs, out in (
-        (LIB_NAME, "ljlk", ["compiled.ops.cpp", "ljlk_pose_score.cpu.cpp"], OUT),
-        (ELEC_LIB_NAME, "elec", ["compiled.ops.cpp", "elec_pose_score.cpu.cpp"], os.path.join(OUT, "elec")),
+        (LIB_NAME, "score/ljlk/potentials", ["compiled.ops.cpp", "ljlk_pose_score.cpu.cpp"], OUT),
+        (
+            ELEC_LIB_NAME,
+            "score/elec/potentials",
+            ["compiled.ops.cpp", "elec_pose_score.cpu.cpp"],
+            os.path.join(OUT, "elec"),
+        ),
+        (APSP_LIB_NAME, "pose/compiled", ["apsp_vestibule.ops.cpp", "apsp.cpu.cpp"], os.path.join(OUT, "apsp")),
     ):
-        src = os.path.join(ref, "tmol", "score", sub, "potentials")
+        src = os.path.join(ref, "tmol", *sub.split("/"))
         if not os.path.isdir(src):
             raise FileNotFoundError(f"reference sources not found under {src}")
         os.makedirs(out, exist_ok=True)
@@ -66,4 +80,4 @@ def build(ref=REF_DEFAULT, verbose=False):
 if __name__ == "__main__":
     ref = sys.argv[1] if len(sys.argv) > 1 else REF_DEFAULT
     t = build(ref, verbose=True)
-    print(f"built {lib_path()} and {elec_lib_path()} in {t:.1f}s")
+    print(f"built {lib_path()}, {elec_lib_path()} and {apsp_lib_path()} in {t:.1f}s")

@@ -361,3 +361,73 @@ def reference_pose_scores(coords, args, require_gradient=True):
         c.requires_grad_(True)
     E, nbr = op(c, *cpu_args)
     return E, c, nbr
+
+
+# ---------------------------------------------------------------------------
+# PoseStack bond separation (oracle/apsp_oracle.c) and the reference's
+# stacked all-pairs-shortest-paths op (oracle/_ref/apsp)
+
+
+def _apsp_lib():
+    if "apsp" not in _LIBS:
+        path = os.path.join(HERE, "liboracle_apsp.so")
+        if not os.path.exists(path):
+            build()
+        _LIBS["apsp"] = ctypes.CDLL(path)
+    return _LIBS["apsp"]
+
+
+def _np_i32(a):
+    if isinstance(a, torch.Tensor):
+        a = a.detach().cpu().numpy()
+    return numpy.ascontiguousarray(numpy.asarray(a, dtype=numpy.int32))
+
+
+def apsp_stacked(weights, cutoff=-1):
+    """tmol's stacked_apsp on a copy of int32 weights [G, N, N] (-1 = no
+    edge): cutoff -1 = Floyd-Warshall, else distances capped at the cutoff."""
+    w = _np_i32(weights).copy()
+    G, N = w.shape[0], w.shape[1]
+    rc = _apsp_lib().oracle_apsp_stacked(
+        w.ctypes.data_as(ctypes.c_void_p), ctypes.c_int(G), ctypes.c_int(N), ctypes.c_int(int(cutoff))
+    )
+    assert rc == 0
+    return w
+
+
+def pose_bondsep(block_type_ind, inter_residue_connections, bt_n_conn, bt_conn_sep):
+    """inter_block_bondsep [P, B, B, C, C] and min_bondsep [P, B, B] of a
+    PoseStack from its connectivity, as tmol's builder computes them."""
+    bti = _np_i32(block_type_ind)
+    irc = _np_i32(inter_residue_connections)
+    nc = _np_i32(bt_n_conn)
+    cs = _np_i32(bt_conn_sep)
+    P, B = bti.shape
+    C = cs.shape[1]
+    ibb = numpy.empty((P, B, B, C, C), dtype=numpy.int32)
+    mb = numpy.empty((P, B, B), dtype=numpy.int32)
+    rc = _apsp_lib().oracle_pose_bondsep(
+        ctypes.c_int(P), ctypes.c_int(B), ctypes.c_int(C), ctypes.c_int(nc.shape[0]),
+        bti.ctypes.data_as(ctypes.c_void_p), irc.ctypes.data_as(ctypes.c_void_p),
+        nc.ctypes.data_as(ctypes.c_void_p), cs.ctypes.data_as(ctypes.c_void_p),
+        ibb.ctypes.data_as(ctypes.c_void_p), mb.ctypes.data_as(ctypes.c_void_p),
+    )
+    assert rc == 0, rc
+    return ibb, mb
+
+
+APSP_REF_LIB = os.path.join(HERE, "_ref", "apsp", "tmol_apsp_ref.so")
+
+
+def reference_apsp_available():
+    return os.path.exists(APSP_REF_LIB)
+
+
+def reference_apsp(weights, cutoff=-1):
+    """The reference's CPU stacked_apsp op on a copy of weights."""
+    if "apsp_ref" not in _LIBS:
+        torch.ops.load_library(APSP_REF_LIB)
+        _LIBS["apsp_ref"] = True
+    w = torch.as_tensor(_np_i32(weights)).clone()
+    torch.ops.tmol_apsp.apsp_op(w, int(cutoff))
+    return w.numpy()

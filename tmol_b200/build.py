@@ -16,8 +16,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "lib", "libtmol_b200_ljlk.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["ljlk.cu", "ljlk_noalloc.cu", "screen.cu"]
-HEADERS = ["ljlk_potentials.cuh", "elec_potentials.cuh"]
+SOURCES = ["ljlk.cu", "ljlk_noalloc.cu", "screen.cu", "bondsep.cu"]
+HEADERS = ["ljlk_potentials.cuh", "elec_potentials.cuh", "bondsep.cuh"]
 
 
 def nvcc_path():
@@ -32,7 +32,7 @@ def _stale():
         return True
     t = os.path.getmtime(OUT)
     deps = [os.path.join(SRC, f) for f in SOURCES + HEADERS]
-    for h in ("tmol_b200_ljlk.h", "tmol_b200_screen.h", "tmol_b200_elec.h"):
+    for h in ("tmol_b200_ljlk.h", "tmol_b200_screen.h", "tmol_b200_elec.h", "tmol_b200_pose.h"):
         deps.append(os.path.join(HERE, "..", "include", h))
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 

@@ -38,7 +38,9 @@
 
 #include "../../include/tmol_b200_elec.h"
 #include "../../include/tmol_b200_ljlk.h"
+#include "../../include/tmol_b200_pose.h"
 #include "../../include/tmol_b200_screen.h"
+#include "bondsep.cuh"
 #include "elec_potentials.cuh"
 #include "ljlk_potentials.cuh"
 
@@ -109,6 +111,10 @@ struct PlanBuildArgs {
   // elec: bond separations from each connection atom come from the
   // representative table (the intra-block table is in.bt_path_distance)
   const int32_t* bt_inter_pd;
+  // plans built from the pose's connectivity instead of the dense
+  // min_bondsep / inter_block_bondsep tensors
+  int use_conn;
+  PoseConn conn;
 };
 
 __global__ void plan_blocks_kernel(PlanBuildArgs a) {
@@ -335,6 +341,73 @@ __global__ void plan_count_pair_kernel(PlanBuildArgs a) {
       }
     }
     if (lane == 0) a.cp_count[row] = cnt < CP_CAP ? cnt : CP_CAP;
+  }
+}
+
+// The same partner table from the pose's connectivity, without the dense
+// tensors: one thread per row (pose, b1) runs the bounded search from each of
+// b1's connection points (bondsep.cuh) and keeps the later blocks whose
+// minimum separation is <= 4, in increasing b2, with their connection-pair
+// separations (6 where unreached).
+constexpr int CONN_ROW_CAP = 48;  // distinct later blocks within the cap
+
+__global__ void plan_count_pair_conn_kernel(PlanBuildArgs a) {
+  const int P = a.in.n_poses, B = a.in.max_n_blocks;
+  const PoseConn& g = a.conn;
+  int reach[BONDSEP_MAX_REACH], dist[BONDSEP_MAX_REACH];
+  int part_b2[CONN_ROW_CAP], part_min[CONN_ROW_CAP];
+  uint8_t part_sep[CONN_ROW_CAP][16];
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < P * B; row += gridDim.x * blockDim.x) {
+    const int p = row / B, b1 = row - p * B;
+    int cnt = 0;
+    if (a.blk_bt[row] >= 0) {
+      const int nc = block_n_conn(g, p, b1);
+      if (nc < 0 || nc > MAX_CONN) atomicOr(a.status, kStIndex);
+      int n_part = 0, st = 0;
+      for (int c1 = 0; c1 < nc && c1 < MAX_CONN; ++c1) {
+        const int n = bounded_paths(g, p, b1, c1, reach, dist, st);
+        for (int k = 0; k < n; ++k) {
+          const int b2 = reach[k] >> 3, c2 = reach[k] & 7;
+          if (b2 <= b1) continue;
+          int q = 0;
+          while (q < n_part && part_b2[q] != b2) ++q;
+          if (q == n_part) {
+            if (n_part == CONN_ROW_CAP) {
+              st |= kBsCapacity;
+              continue;
+            }
+            part_b2[q] = b2;
+            part_min[q] = MAX_SIG_SEP;
+            for (int e = 0; e < 16; ++e) part_sep[q][e] = MAX_SIG_SEP;
+            ++n_part;
+          }
+          if (c2 < MAX_CONN) part_sep[q][c1 * 4 + c2] = (uint8_t)dist[k];
+          part_min[q] = min(part_min[q], dist[k]);
+        }
+      }
+      if (st & kBsIndex) atomicOr(a.status, kStIndex);
+      if (st & kBsShape) atomicOr(a.status, kStShape);
+      if (st & kBsCapacity) atomicOr(a.status, kStCapacity);
+      // partners in increasing b2 (the dense route's order)
+      for (;;) {
+        int best = -1;
+        for (int q = 0; q < n_part; ++q)
+          if (part_min[q] <= 4 && a.blk_bt[p * B + part_b2[q]] >= 0 && (best < 0 || part_b2[q] < part_b2[best]))
+            best = q;
+        if (best < 0) break;
+        if (cnt < CP_CAP) {
+          const int64_t e = (int64_t)row * CP_CAP + cnt;
+          a.cp_b2[e] = part_b2[best];
+          a.cp_minsep[e] = part_min[best];
+          for (int k = 0; k < 16; ++k) a.cp_seps[e * 16 + k] = part_sep[best][k];
+        } else {
+          atomicOr(a.status, kStCapacity);
+        }
+        ++cnt;
+        part_min[best] = MAX_SIG_SEP + 1;  // taken
+      }
+    }
+    a.cp_count[row] = cnt < CP_CAP ? cnt : CP_CAP;
   }
 }
 
@@ -2194,7 +2267,8 @@ struct ElecExtra {
 
 int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
                 const tmol_b200_ljlk_launch* launch, void* stream, bool rotamers,
-                tmol_b200_ljlk_plan** plan_out, const ElecExtra* elec = nullptr) {
+                tmol_b200_ljlk_plan** plan_out, const ElecExtra* elec = nullptr,
+                const tmol_b200_pose_connectivity* conn = nullptr) {
   if (!in || !plan_out) return TMOL_B200_ERR_INVALID_ARGUMENT;
   const int term = elec ? kTermElec : kTermLJLK;
   *plan_out = nullptr;
@@ -2209,10 +2283,26 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
   if (rotamers && P * B > 0 && !in->n_rots_for_block) return TMOL_B200_ERR_INVALID_ARGUMENT;
   if (nt * TILE < A) return TMOL_B200_ERR_SHAPE;
   if (in->n_atoms >= ((int64_t)1 << 31)) return TMOL_B200_ERR_SHAPE;
+  // with the pose's connectivity, the dense bond-separation tensors are not
+  // read (and may be null)
+  const void* dense_cp[] = {in->min_bondsep, in->inter_block_bondsep};
+  const void* conn_req[] = {conn ? conn->block_type_ind : nullptr, conn ? conn->inter_residue_connections : nullptr,
+                            conn ? conn->bt_n_conn : nullptr, conn ? conn->bt_conn_sep : nullptr};
+  if (conn && (conn->n_poses != P || conn->max_n_blocks != B || conn->n_block_types != nbt ||
+               conn->max_n_conn != C))
+    return TMOL_B200_ERR_SHAPE;
+  if (P * B > 0) {
+    if (conn) {
+      for (const void* r : conn_req)
+        if (!r) return TMOL_B200_ERR_INVALID_ARGUMENT;
+    } else {
+      for (const void* r : dense_cp)
+        if (!r) return TMOL_B200_ERR_INVALID_ARGUMENT;
+    }
+  }
   const void* req[] = {in->rot_coord_offset, in->first_rot_block_type, in->block_ind_for_rot,
                        in->pose_ind_for_rot, in->block_type_ind_for_rot, in->rot_offset_for_block,
-                       in->min_bondsep, in->inter_block_bondsep, in->bt_n_atoms,
-                       in->bt_n_conn, in->bt_conn_atom, in->bt_path_distance,
+                       in->bt_n_atoms, in->bt_n_conn, in->bt_conn_atom, in->bt_path_distance,
                        in->bt_is_ligand_fragment, in->global_params};
   const void* req_ljlk[] = {in->bt_n_heavy_atoms_in_tile, in->bt_heavy_atoms_in_tile, in->bt_atom_types,
                             in->type_params};
@@ -2311,6 +2401,8 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
   a.status = pl->counters + 1;
   a.term = term;
   a.bt_inter_pd = elec ? elec->inter_repr_pd : nullptr;
+  a.use_conn = conn ? 1 : 0;
+  a.conn = conn ? pose_conn(*conn) : PoseConn{};
   a.rotamers = rotamers ? 1 : 0;
   a.rot_bt = a.rot_off = a.rot_block = a.rot_pose = nullptr;
   if (rotamers) {
@@ -2350,7 +2442,11 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
     plan_heavy_kernel<<<gh, 256, 0, st>>>(a);
     PCK(cudaGetLastError());
   }
-  if (PB > 0) {
+  if (PB > 0 && conn) {
+    int gc = std::max(1, std::min<int>((int)((PB + 127) / 128), pl->n_sm * 16));
+    plan_count_pair_conn_kernel<<<gc, 128, 0, st>>>(a);
+    PCK(cudaGetLastError());
+  } else if (PB > 0) {
     int gc = std::max(1, std::min<int>((int)((PB * 32 + 255) / 256), pl->n_sm * 16));
     plan_count_pair_kernel<<<gc, 256, 0, st>>>(a);
     PCK(cudaGetLastError());
@@ -2493,11 +2589,12 @@ tmol_b200_ljlk_inputs shared_inputs(const tmol_b200_elec_inputs* e) {
 }
 
 int create_elec_plan(const tmol_b200_elec_inputs* e, int real_bytes, const tmol_b200_ljlk_launch* launch,
-                     void* stream, bool rotamers, tmol_b200_ljlk_plan** plan_out) {
+                     void* stream, bool rotamers, tmol_b200_ljlk_plan** plan_out,
+                     const tmol_b200_pose_connectivity* conn = nullptr) {
   if (!e || !plan_out) return TMOL_B200_ERR_INVALID_ARGUMENT;
   const tmol_b200_ljlk_inputs in = shared_inputs(e);
   const ElecExtra x = {e->bt_partial_charge, e->bt_inter_repr_path_distance};
-  return create_plan(&in, real_bytes, launch, stream, rotamers, plan_out, &x);
+  return create_plan(&in, real_bytes, launch, stream, rotamers, plan_out, &x, conn);
 }
 
 bool pose_plan_of(const tmol_b200_ljlk_plan* plan, int term) {
@@ -2596,6 +2693,22 @@ int tmol_b200_ljlk_rotamer_plan_create(const tmol_b200_ljlk_inputs* in, int real
                                        const tmol_b200_ljlk_launch* launch,
                                        void* stream, tmol_b200_ljlk_plan** plan_out) {
   return create_plan(in, real_bytes, launch, stream, true, plan_out);
+}
+
+int tmol_b200_ljlk_plan_create_from_connectivity(const tmol_b200_ljlk_inputs* in,
+                                                 const tmol_b200_pose_connectivity* conn, int real_bytes,
+                                                 const tmol_b200_ljlk_launch* launch, void* stream,
+                                                 int rotamers, tmol_b200_ljlk_plan** plan_out) {
+  if (!conn) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  return create_plan(in, real_bytes, launch, stream, rotamers != 0, plan_out, nullptr, conn);
+}
+
+int tmol_b200_elec_plan_create_from_connectivity(const tmol_b200_elec_inputs* in,
+                                                 const tmol_b200_pose_connectivity* conn, int real_bytes,
+                                                 const tmol_b200_ljlk_launch* launch, void* stream,
+                                                 int rotamers, tmol_b200_elec_plan** plan_out) {
+  if (!conn) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  return create_elec_plan(in, real_bytes, launch, stream, rotamers != 0, plan_out, conn);
 }
 
 int tmol_b200_ljlk_plan_destroy(tmol_b200_ljlk_plan* plan) {

@@ -1,5 +1,6 @@
 """ctypes binding of the C ABI in ``include/tmol_b200_ljlk.h``,
-``include/tmol_b200_elec.h`` and ``include/tmol_b200_screen.h``.
+``include/tmol_b200_elec.h``, ``include/tmol_b200_pose.h`` and
+``include/tmol_b200_screen.h``.
 
 The shared library is built in-tree (``tmol_b200/lib``) by
 ``tmol_b200.build``.  There is no fallback: importing this module without the
@@ -91,6 +92,21 @@ class ElecInputs(ctypes.Structure):
         ("bt_is_ligand_fragment", ctypes.c_void_p),
         ("global_params", ctypes.c_void_p),
         ("max_dis", ctypes.c_double),
+    ]
+
+
+class PoseConnectivity(ctypes.Structure):
+    """``tmol_b200_pose_connectivity``."""
+
+    _fields_ = [
+        ("n_poses", ctypes.c_int32),
+        ("max_n_blocks", ctypes.c_int32),
+        ("n_block_types", ctypes.c_int32),
+        ("max_n_conn", ctypes.c_int32),
+        ("block_type_ind", ctypes.c_void_p),
+        ("inter_residue_connections", ctypes.c_void_p),
+        ("bt_n_conn", ctypes.c_void_p),
+        ("bt_conn_sep", ctypes.c_void_p),
     ]
 
 
@@ -193,6 +209,23 @@ SIGNATURES = {
     "tmol_b200_elec_rotamer_fill": (ctypes.c_int, [_V, _V, _V, _V]),
     "tmol_b200_elec_rotamer_forward": (ctypes.c_int, [_V, _V, _V, _I64, _I64, _V, _V]),
     "tmol_b200_elec_rotamer_backward": (ctypes.c_int, [_V, _V, _V, _I64, _I64, _V, _V, _V]),
+    # PoseStack construction (include/tmol_b200_pose.h)
+    "tmol_b200_pose_bondsep": (ctypes.c_int, [ctypes.POINTER(PoseConnectivity), _V, _V, _V]),
+    "tmol_b200_apsp_stacked": (ctypes.c_int, [_V, _I32, _I32, _I32, _V]),
+    "tmol_b200_ljlk_plan_create_from_connectivity": (
+        ctypes.c_int,
+        [
+            ctypes.POINTER(Inputs), ctypes.POINTER(PoseConnectivity), ctypes.c_int, ctypes.POINTER(Launch), _V,
+            ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+        ],
+    ),
+    "tmol_b200_elec_plan_create_from_connectivity": (
+        ctypes.c_int,
+        [
+            ctypes.POINTER(ElecInputs), ctypes.POINTER(PoseConnectivity), ctypes.c_int, ctypes.POINTER(Launch), _V,
+            ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+        ],
+    ),
     # learned block-pair screen (include/tmol_b200_screen.h)
     "tmol_b200_ljlk_plan_set_skip_mask": (ctypes.c_int, [_V, _V, _I32]),
     "tmol_b200_ljlk_screen_candidates": (ctypes.c_int, [_V, _V, _I32, _V, _V, _V, _V, _V, _V]),

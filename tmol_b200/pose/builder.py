@@ -14,8 +14,10 @@ The connectivity rules follow tmol's ``PoseStackBuilder.from_block_type_names``
    give ``inter_block_bondsep[p, b1, b2, c1, c2]`` (``:1271-1343``), 6 where
    a connection slot does not exist.
 
-The shortest paths here come from a capped Dijkstra per source node rather
-than tmol's all-pairs kernel; the integers are the same.
+The shortest paths come from a bounded search per connection point rather
+than tmol's all-pairs pass over a dense matrix; the integers are the same.
+On a CUDA device the search runs on the GPU (``tmol_b200.pose.bondsep``,
+one thread per connection point); on the host, a capped Dijkstra in Python.
 """
 
 import heapq
@@ -137,12 +139,22 @@ def build_pose_stack(topologies, coords_list=None, pbt=None, device=torch.device
         offsets[p, nb:] = pose_n_atoms[p]
     max_atoms = int(pose_n_atoms.max())
 
-    ibb = torch.full((P, B, B, C, C), MAX_SIG_BOND_SEPARATION, dtype=torch.int32, device=device)
-    for p, topo in enumerate(topologies):
-        ent = interblock_bondsep_entries(topo, pbt)
-        if ent:
-            e = torch.tensor(ent, dtype=torch.int64, device=device)
-            ibb[p, e[:, 0], e[:, 2], e[:, 1], e[:, 3]] = e[:, 4].to(torch.int32)
+    if torch.device(device).type == "cuda":
+        from .bondsep import bondsep_from_connectivity
+
+        ibb, _ = bondsep_from_connectivity(
+            torch.tensor(bt_ind, device=device),
+            torch.tensor(irc, device=device),
+            pbt.n_conn,
+            pbt.conn_at_intrablock_bond_sep,
+        )
+    else:
+        ibb = torch.full((P, B, B, C, C), MAX_SIG_BOND_SEPARATION, dtype=torch.int32, device=device)
+        for p, topo in enumerate(topologies):
+            ent = interblock_bondsep_entries(topo, pbt)
+            if ent:
+                e = torch.tensor(ent, dtype=torch.int64, device=device)
+                ibb[p, e[:, 0], e[:, 2], e[:, 1], e[:, 3]] = e[:, 4].to(torch.int32)
 
     coords = torch.zeros((P, max_atoms, 3), dtype=torch.float32)
     if coords_list is not None:

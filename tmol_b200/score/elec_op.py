@@ -30,7 +30,7 @@ class ElecPlan(LJLKPlan):
     ABI = "tmol_b200_elec"
     NAME = "elec"
 
-    def __init__(self, coords_like, static_args, launch=None, rotamers=False):
+    def __init__(self, coords_like, static_args, launch=None, rotamers=False, connectivity=None):
         (
             rot_coord_offset,
             pose_ind_for_atom,
@@ -79,6 +79,12 @@ class ElecPlan(LJLKPlan):
             bt_is_ligand_fragment=bt_is_ligand,
         )
         keep = []
+        if connectivity is not None:
+            # count-pair tables from the connectivity: the dense bond
+            # separation tensors are not needed
+            for name in ("min_bondsep", "inter_block_bondsep"):
+                if ints[name] is None:
+                    del ints[name]
         s = native.ElecInputs()
         for name, t in ints.items():
             if not isinstance(t, torch.Tensor):
@@ -97,11 +103,11 @@ class ElecPlan(LJLKPlan):
         P, B = first_rot_for_block.shape
         C = bt_conn_atom.shape[1]
         nbt, A = bt_partial_charge.shape
-        if tuple(inter_block_bondsep.shape) != (P, B, B, C, C):
+        if inter_block_bondsep is not None and tuple(inter_block_bondsep.shape) != (P, B, B, C, C):
             raise ValueError(
                 f"inter_block_bondsep has shape {tuple(inter_block_bondsep.shape)}, expected {(P, B, B, C, C)}"
             )
-        if tuple(min_bondsep.shape) != (P, B, B):
+        if min_bondsep is not None and tuple(min_bondsep.shape) != (P, B, B):
             raise ValueError(f"min_bondsep has shape {tuple(min_bondsep.shape)}, expected {(P, B, B)}")
         for name, t in (("inter", bt_inter_repr_path_distance), ("intra", bt_intra_repr_path_distance)):
             if tuple(t.shape) != (nbt, A, A):
@@ -119,7 +125,7 @@ class ElecPlan(LJLKPlan):
         self.n_poses, self.max_n_blocks = P, B
         self.n_atoms = pose_ind_for_atom.shape[0]
         s.n_atoms = self.n_atoms
-        self._create(s, launch, rotamers)
+        self._create(s, launch, rotamers, connectivity)
         del keep
 
     def set_skip_mask(self, mask):

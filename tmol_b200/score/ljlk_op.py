@@ -32,7 +32,7 @@ class LJLKPlan:
     ABI = "tmol_b200_ljlk"  # prefix of the scoring entry points
     NAME = "LJ/LK"
 
-    def __init__(self, coords_like, static_args, launch=None, rotamers=False):
+    def __init__(self, coords_like, static_args, launch=None, rotamers=False, connectivity=None):
         (
             rot_coord_offset,
             pose_ind_for_atom,
@@ -85,6 +85,12 @@ class LJLKPlan:
             bt_is_ligand_fragment=bt_is_ligand,
         )
         keep = []
+        if connectivity is not None:
+            # count-pair tables from the connectivity: the dense bond
+            # separation tensors are not needed
+            for name in ("min_bondsep", "inter_block_bondsep"):
+                if ints[name] is None:
+                    del ints[name]
         s = native.Inputs()
         for name, t in ints.items():
             if not isinstance(t, torch.Tensor):
@@ -104,11 +110,11 @@ class LJLKPlan:
             setattr(s, name, t.data_ptr())
         P, B = first_rot_for_block.shape
         C = bt_conn_atom.shape[1]
-        if tuple(inter_block_bondsep.shape) != (P, B, B, C, C):
+        if inter_block_bondsep is not None and tuple(inter_block_bondsep.shape) != (P, B, B, C, C):
             raise ValueError(
                 f"inter_block_bondsep has shape {tuple(inter_block_bondsep.shape)}, expected {(P, B, B, C, C)}"
             )
-        if tuple(min_bondsep.shape) != (P, B, B):
+        if min_bondsep is not None and tuple(min_bondsep.shape) != (P, B, B):
             raise ValueError(f"min_bondsep has shape {tuple(min_bondsep.shape)}, expected {(P, B, B)}")
         if reals["type_params"].dim() != 2 or reals["type_params"].shape[1] != 10:
             raise ValueError("type_params must be [n_types, 10]")
@@ -127,7 +133,7 @@ class LJLKPlan:
         self.n_poses, self.max_n_blocks = P, B
         self.n_atoms = pose_ind_for_atom.shape[0]
         s.n_atoms = self.n_atoms
-        self._create(s, launch, rotamers)
+        self._create(s, launch, rotamers, connectivity)
         del keep
 
     def _set_device(self, coords_like):
@@ -140,21 +146,44 @@ class LJLKPlan:
             raise TypeError(f"coordinates must be float32 or float64, got {self.dtype}")
         return device
 
-    def _create(self, inputs, launch, rotamers):
-        """Calls the plan-create entry point on the filled inputs struct."""
+    def _create(self, inputs, launch, rotamers, connectivity=None):
+        """Calls the plan-create entry point on the filled inputs struct;
+        with ``connectivity`` (a PoseStack, or the tuple (block_type_ind,
+        inter_residue_connections, bt_n_conn, bt_conn_sep)) the count-pair
+        tables are built from it (include/tmol_b200_pose.h)."""
         self.launch = native.Launch(*(launch or (0, 0, 0, 0)))
         self.rotamers = bool(rotamers)
         ptr = ctypes.c_void_p()
+        real_bytes = 4 if self.dtype == torch.float32 else 8
         with torch.cuda.device(self.device):
             stream = torch.cuda.current_stream(self.device).cuda_stream
-            native.call(
-                f"{self.ABI}_rotamer_plan_create" if rotamers else f"{self.ABI}_plan_create",
-                ctypes.byref(inputs),
-                4 if self.dtype == torch.float32 else 8,
-                ctypes.byref(self.launch),
-                ctypes.c_void_p(stream),
-                ctypes.byref(ptr),
-            )
+            if connectivity is None:
+                native.call(
+                    f"{self.ABI}_rotamer_plan_create" if rotamers else f"{self.ABI}_plan_create",
+                    ctypes.byref(inputs),
+                    real_bytes,
+                    ctypes.byref(self.launch),
+                    ctypes.c_void_p(stream),
+                    ctypes.byref(ptr),
+                )
+            else:
+                from ..pose.bondsep import connectivity as conn_struct, pose_connectivity
+
+                if isinstance(connectivity, tuple):
+                    cs, conn_keep = conn_struct(*connectivity)
+                else:
+                    cs, conn_keep = pose_connectivity(connectivity)
+                native.call(
+                    f"{self.ABI}_plan_create_from_connectivity",
+                    ctypes.byref(inputs),
+                    ctypes.byref(cs),
+                    real_bytes,
+                    ctypes.byref(self.launch),
+                    ctypes.c_void_p(stream),
+                    int(bool(rotamers)),
+                    ctypes.byref(ptr),
+                )
+                del conn_keep
         self.ptr = ptr
 
     def __del__(self):
