@@ -17,9 +17,11 @@ Arms:
                     process per core, each scoring a slice of the poses.
 
 Other workloads (--workload): the uneven 256-pose batch, rotamer-pair
-scoring (rotamers16x150) and the elec term on the uniform batch
-(elec64x150: per-pose fa_elec and the gradient of its sum).  The default
-line also carries an "elec" summary measured on the same batch.
+scoring (rotamers16x150), the elec term on the uniform batch (elec64x150:
+per-pose fa_elec and the gradient of its sum) and PoseStack bond separation
+(bondsep256: inter_block_bondsep and min_bondsep of the uneven batch from its
+connectivity).  The default line also carries an "elec" summary measured on
+the same batch.
 
 Under torchrun each rank scores its own batch (independent seeds); the
 timing is the maximum over ranks (weak scaling, no collective on the data
@@ -55,6 +57,7 @@ ROT_RES = 150
 ROT_SET = dict(max_rots=31, mutate_fraction=0.25, seed=9)
 ROT_METRIC = "LJ+LK rotamer-pair energies/s (16 poses x 150 residues, 1-31 rotamers per block, 1 B200)"
 ELEC_METRIC = "elec energy+grad poses/s (64x150-residue batch, 1 B200)"
+BONDSEP_METRIC = "inter-block bond separation poses/s (256-pose uneven batch, dense [P,B,B,C,C] + min, 1 B200)"
 
 # Algorithmic FLOPs per unit (E + dE), counted on the restatement's most
 # populated branch (far cubic fade, 4.5-6 A); FMA = 2, div/sqrt/exp/floor = 1.
@@ -328,6 +331,8 @@ def run_reference(args, world, rank):
         return 0
     if args.workload == "rotamers16x150":
         return run_reference_rotamers(args)
+    if args.workload == "bondsep256":
+        return run_reference_bondsep(args)
     elec = args.workload == "elec64x150"
     sizes, seeds = workload_sizes(args.workload, 0)
     n_poses = len(sizes)
@@ -1002,6 +1007,293 @@ def run_elec(args, world, rank, local):
     return 0
 
 
+def _bondsep_port_worker(conn, sizes, seeds):
+    """One single-threaded process of the bond-separation CPU arm: the C
+    restatement of the reference route (connection-point matrix, shortest
+    paths with cutoff 6, scatter), one pose at a time."""
+    from oracle import oracle as O
+    from tmol_b200.pose.synthetic import synthetic_topologies_and_coords
+    from tmol_b200.pose.builder import build_pose_stack
+
+    stacks = []
+    for sz, sd in zip(sizes, seeds):
+        topos, _ = synthetic_topologies_and_coords([sz], [sd], with_coords=False)
+        stacks.append(build_pose_stack(topos))
+    conn.send("ready")
+    while True:
+        msg = conn.recv()
+        if msg is None:
+            break
+        t0 = time.perf_counter()
+        for ps in stacks:
+            pbt = ps.packed_block_types
+            O.pose_bondsep(ps.block_type_ind, ps.inter_residue_connections, pbt.n_conn, pbt.conn_at_intrablock_bond_sep)
+        conn.send(time.perf_counter() - t0)
+
+
+def bondsep_cpu_sample(sizes, seeds, n=16):
+    """The C restatement of the reference route on one core, on n seeded
+    poses of the batch (each as its own stack), scaled to the batch by pose
+    count; seconds per batch."""
+    import numpy
+
+    from oracle import oracle as O
+    from tmol_b200.pose.builder import build_pose_stack
+    from tmol_b200.pose.synthetic import synthetic_topologies_and_coords
+
+    pick = numpy.random.default_rng(7).choice(len(sizes), n, replace=False)
+    stacks = []
+    for k in pick:
+        topos, _ = synthetic_topologies_and_coords([sizes[k]], [seeds[k]], with_coords=False)
+        stacks.append(build_pose_stack(topos))
+    best = float("inf")
+    for _ in range(3):
+        t0 = time.perf_counter()
+        for ps in stacks:
+            pbt = ps.packed_block_types
+            O.pose_bondsep(ps.block_type_ind, ps.inter_residue_connections, pbt.n_conn, pbt.conn_at_intrablock_bond_sep)
+        best = min(best, time.perf_counter() - t0)
+    return best * len(sizes) / n, [int(sizes[k]) for k in pick]
+
+
+def run_bondsep(args, world, rank, local):
+    """PoseStack bond separation on the GPU: the dense inter_block_bondsep
+    [P, B, B, C, C] and min_bondsep [P, B, B] of the uneven batch from its
+    connectivity, per step one call of tmol_b200_pose_bondsep (it validates
+    the connectivity and synchronises once).  Also: scoring-plan creation
+    from the connectivity (no dense tensors) against creation from them."""
+    import ctypes
+
+    import torch
+
+    from tmol_b200 import native
+    from tmol_b200.pose.bondsep import pose_connectivity
+    from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm, pose_score_args
+    from tmol_b200.score.ljlk_op import LJLKPlan
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    sizes, seeds = workload_sizes("uneven256", rank)
+    ps = workload(rank, "uneven256", device=dev)
+    P, B, C = ps.n_poses, ps.max_n_blocks, ps.packed_block_types.max_n_conn
+    cs, keep = pose_connectivity(ps)
+    ibb = torch.empty((P, B, B, C, C), dtype=torch.int32, device=dev)
+    mb = torch.empty((P, B, B), dtype=torch.int32, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, device=dev, dtype=torch.float32)
+    stream = torch.cuda.current_stream(dev)
+
+    def step(dense=True):
+        native.call(
+            "tmol_b200_pose_bondsep", ctypes.byref(cs), ctypes.c_void_p(ibb.data_ptr() if dense else 0),
+            ctypes.c_void_p(mb.data_ptr()), ctypes.c_void_p(stream.cuda_stream),
+        )
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier(world)
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record()
+            step()
+            ev[k][1].record()
+        torch.cuda.synchronize()
+    barrier(world)
+    ms_max = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), world)
+    value = sum_over_ranks(P * args.steps, world) / (ms_max / 1e3)
+    ms_step = ms_max / args.steps
+    # min_bondsep alone (the compact output)
+    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.zero_()
+        ev2[k][0].record()
+        step(dense=False)
+        ev2[k][1].record()
+    torch.cuda.synchronize()
+    ms_min_only = sum(a.elapsed_time(b) for a, b in ev2) / args.steps
+    assert torch.equal(ibb, ps.inter_block_bondsep)
+
+    # algorithmic bytes: the dense outputs written once, the connectivity
+    # read once (int32)
+    n_conn_pts = int(torch.where(ps.block_type_ind >= 0, ps.packed_block_types.n_conn[ps.block_type_ind.clamp(min=0).long()], 0).sum())
+    out_bytes = (ibb.numel() + mb.numel()) * 4
+    in_bytes = (ps.block_type_ind.numel() + ps.inter_residue_connections.numel()) * 4
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs")
+    achieved = (out_bytes + in_bytes) / (ms_step * 1e-3) / 1e9
+
+    # plan creation: from the dense tensors vs from the connectivity
+    term = LJLKEnergyTerm(device=dev)
+    static = [a.to(dev) if isinstance(a, torch.Tensor) else a for a in pose_score_args(ps, term)[:-1]]
+    coords = ps.coords.flatten(0, 1).contiguous()
+    sparse_static = [None if i in (12, 13) else a for i, a in enumerate(static)]
+    times = {}
+    for name, kw, st in (("dense", {}, static), ("connectivity", {"connectivity": ps}, sparse_static)):
+        LJLKPlan(coords, st, **kw)  # warm
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(3):
+            LJLKPlan(coords, st, **kw)
+        torch.cuda.synchronize()
+        times[name] = (time.perf_counter() - t0) / 3 * 1e3
+
+    # end to end: connectivity from pinned host memory, min_bondsep back
+    h_bt = ps.block_type_ind.cpu().pin_memory()
+    h_irc = ps.inter_residue_connections.cpu().pin_memory()
+    h_mb = torch.empty(mb.shape, dtype=torch.int32, pin_memory=True)
+    d_bt = torch.empty_like(ps.block_type_ind)
+    d_irc = torch.empty_like(ps.inter_residue_connections)
+    cs2 = native.PoseConnectivity(P, B, cs.n_block_types, C, d_bt.data_ptr(), d_irc.data_ptr(), cs.bt_n_conn,
+                                  cs.bt_conn_sep)
+    e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.zero_()
+        e2e_ev[k][0].record()
+        d_bt.copy_(h_bt, non_blocking=True)
+        d_irc.copy_(h_irc, non_blocking=True)
+        native.call("tmol_b200_pose_bondsep", ctypes.byref(cs2), ctypes.c_void_p(ibb.data_ptr()),
+                    ctypes.c_void_p(mb.data_ptr()), ctypes.c_void_p(stream.cuda_stream))
+        h_mb.copy_(mb, non_blocking=True)
+        e2e_ev[k][1].record()
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in e2e_ev), world)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        t_batch, picked = bondsep_cpu_sample(sizes, seeds)
+        cpu = {
+            "value": len(sizes) / t_batch,
+            "unit": "poses/s",
+            "cores": 1,
+            "kind": "port",
+            "sample": f"16 seeded poses of the batch ({sum(picked)} residues), each as its own stack, "
+            "C restatement of the reference route (bit-exact with the compiled reference apsp op), "
+            "best of 3, one thread; scaled to the batch by pose count",
+        }
+    if rank == 0:
+        line = {
+            "metric": BONDSEP_METRIC,
+            "value": value,
+            "unit": "poses/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_step,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "int32",
+            "data": "synthetic (seeded single-chain proteins)",
+            "config": {
+                "workload": f"{P} poses, residues log-uniform in [20, 1000], B = {B}, C = {C}, "
+                f"{n_conn_pts} connection points",
+                "l2": "flushed (256 MiB write) before every timed step; outputs far larger than L2",
+                "parallelism": f"weak, {world} independent batch(es)",
+            },
+            "gpu_launches": 3 * args.steps,
+            "clocks": clk.summary(),
+            "roofline": {
+                "bound": "hbm",
+                "achieved": achieved,
+                "peak": hbm,
+                "unit": "GB/s",
+                "frac": achieved / hbm if hbm else None,
+                "traffic": None,
+                "kernel": "fill_i32_kernel (x2) + bondsep_sources_kernel, one call incl. its status read-back",
+                "bytes_per_step": out_bytes + in_bytes,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)",
+            },
+            "min_bondsep_only_ms": ms_min_only,
+            "plan_create_ms": times,
+            "dense_tensor_bytes_avoided": int(ps.inter_block_bondsep.numel() * 4 + mb.numel() * 4),
+            "e2e": {
+                "value": sum_over_ranks(P * args.steps, world) / (e2e_ms / 1e3),
+                "unit": "poses/s",
+                "h2d_bytes_per_step": in_bytes,
+                "d2h_bytes_per_step": mb.numel() * 4,
+            },
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    del keep
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+def run_reference_bondsep(args):
+    """The C restatement of the reference route on all host cores: one
+    process per core, poses dealt out longest-first."""
+    import multiprocessing as mp
+
+    sizes, seeds = workload_sizes("uneven256", 0)
+    n_poses = len(sizes)
+    n_proc = min(os.cpu_count() or 1, n_poses)
+    shares = [[] for _ in range(n_proc)]
+    load = [0] * n_proc
+    for k in sorted(range(n_poses), key=lambda k: -sizes[k]):
+        q = load.index(min(load))
+        shares[q].append(k)
+        load[q] += sizes[k] ** 2
+    ctx = mp.get_context("spawn")
+    workers = []
+    for share in shares:
+        parent, child = ctx.Pipe()
+        pr = ctx.Process(target=_bondsep_port_worker, args=(child, [sizes[k] for k in share], [seeds[k] for k in share]))
+        pr.start()
+        workers.append((pr, parent))
+    for _, c in workers:
+        c.recv()
+
+    def step():
+        t0 = time.perf_counter()
+        for _, c in workers:
+            c.send(1)
+        for _, c in workers:
+            c.recv()
+        return time.perf_counter() - t0
+
+    for _ in range(max(args.warmup, 1)):
+        step()
+    times = [step() for _ in range(args.steps)]
+    for pr, c in workers:
+        c.send(None)
+        pr.join()
+    t = sum(times)
+    value = n_poses * args.steps / t
+    line = {
+        "impl": "reference",
+        "metric": BONDSEP_METRIC,
+        "value": value,
+        "unit": "poses/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * t / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "int32",
+        "data": "synthetic (seeded single-chain proteins)",
+        "config": {"workload": f"{n_poses} poses, residues log-uniform in [20, 1000]"},
+        "cpu_baseline": {
+            "value": value,
+            "unit": "poses/s",
+            "cores": n_proc,
+            "kind": "port",
+            "sample": f"the full {n_poses}-pose batch per step, each pose as its own stack, dealt to {n_proc} "
+            "single-threaded processes (C restatement of the reference route)",
+        },
+        "e2e": {"value": value, "unit": "poses/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_b200(args, world, rank, local):
     import torch
 
@@ -1223,7 +1515,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument(
-        "--workload", default="uniform64x150", choices=["uniform64x150", "uneven256", "rotamers16x150", "elec64x150"]
+        "--workload",
+        default="uniform64x150",
+        choices=["uniform64x150", "uneven256", "rotamers16x150", "elec64x150", "bondsep256"],
     )
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-screen", action="store_true", help="skip the learned-screen measurement")
@@ -1244,6 +1538,8 @@ def main():
         return run_rotamers(args, world, rank, local)
     if args.workload == "elec64x150":
         return run_elec(args, world, rank, local)
+    if args.workload == "bondsep256":
+        return run_bondsep(args, world, rank, local)
     return run_b200(args, world, rank, local)
 
 

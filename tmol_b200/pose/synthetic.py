@@ -33,9 +33,11 @@ def random_dihedrals(rng, n, extra_chi_sd=0.0):
     return phi, psi, omega, chis
 
 
-def synthetic_topologies_and_coords(n_res_per_pose, seeds, extra_chi_sd=0.0, spacing=1000.0, pbt=None):
+def synthetic_topologies_and_coords(n_res_per_pose, seeds, extra_chi_sd=0.0, spacing=1000.0, pbt=None,
+                                    with_coords=True):
     """The host half of ``synthetic_pose_stack``: per-pose topologies and
-    ``[n_pose_atoms, 3]`` coordinates (numpy), already placed on the grid."""
+    ``[n_pose_atoms, 3]`` coordinates (numpy), already placed on the grid
+    (None without ``with_coords``: the sequences only)."""
     rts = ResidueTypeSet.get_default()
     pbt = pbt or default_packed_block_types(torch.device("cpu"))
     topos, phis, psis, omegas, chis = [], [], [], [], []
@@ -48,6 +50,8 @@ def synthetic_topologies_and_coords(n_res_per_pose, seeds, extra_chi_sd=0.0, spa
         psis.append(ps)
         omegas.append(om)
         chis.append(ch)
+    if not with_coords:
+        return topos, None
     coords = build_chain_coords(pbt, topos, phis, psis, omegas, chis)
     P = len(topos)
     side = max(1, int(numpy.ceil(P ** (1.0 / 3.0))))
