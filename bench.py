@@ -1059,8 +1059,8 @@ def bondsep_cpu_sample(sizes, seeds, n=16):
 def run_bondsep(args, world, rank, local):
     """PoseStack bond separation on the GPU: the dense inter_block_bondsep
     [P, B, B, C, C] and min_bondsep [P, B, B] of the uneven batch from its
-    connectivity, per step one call of tmol_b200_pose_bondsep (it validates
-    the connectivity and synchronises once).  Also: scoring-plan creation
+    connectivity, per step one call of tmol_b200_pose_bondsep (three
+    kernels and a status word; its status is read after the timed steps).  Also: scoring-plan creation
     from the connectivity (no dense tensors) against creation from them."""
     import ctypes
 
@@ -1079,13 +1079,14 @@ def run_bondsep(args, world, rank, local):
     cs, keep = pose_connectivity(ps)
     ibb = torch.empty((P, B, B, C, C), dtype=torch.int32, device=dev)
     mb = torch.empty((P, B, B), dtype=torch.int32, device=dev)
+    status = torch.empty(1, dtype=torch.int32, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, device=dev, dtype=torch.float32)
     stream = torch.cuda.current_stream(dev)
 
     def step(dense=True):
         native.call(
             "tmol_b200_pose_bondsep", ctypes.byref(cs), ctypes.c_void_p(ibb.data_ptr() if dense else 0),
-            ctypes.c_void_p(mb.data_ptr()), ctypes.c_void_p(stream.cuda_stream),
+            ctypes.c_void_p(mb.data_ptr()), ctypes.c_void_p(status.data_ptr()), ctypes.c_void_p(stream.cuda_stream),
         )
 
     for _ in range(max(args.warmup, 3)):
@@ -1113,6 +1114,8 @@ def run_bondsep(args, world, rank, local):
         ev2[k][1].record()
     torch.cuda.synchronize()
     ms_min_only = sum(a.elapsed_time(b) for a, b in ev2) / args.steps
+    native.check("tmol_b200_pose_bondsep", int(status.item()))
+    step()
     assert torch.equal(ibb, ps.inter_block_bondsep)
 
     # algorithmic bytes: the dense outputs written once, the connectivity
@@ -1154,7 +1157,8 @@ def run_bondsep(args, world, rank, local):
         d_bt.copy_(h_bt, non_blocking=True)
         d_irc.copy_(h_irc, non_blocking=True)
         native.call("tmol_b200_pose_bondsep", ctypes.byref(cs2), ctypes.c_void_p(ibb.data_ptr()),
-                    ctypes.c_void_p(mb.data_ptr()), ctypes.c_void_p(stream.cuda_stream))
+                    ctypes.c_void_p(mb.data_ptr()), ctypes.c_void_p(status.data_ptr()),
+                    ctypes.c_void_p(stream.cuda_stream))
         h_mb.copy_(mb, non_blocking=True)
         e2e_ev[k][1].record()
     torch.cuda.synchronize()
@@ -1192,7 +1196,7 @@ def run_bondsep(args, world, rank, local):
                 "l2": "flushed (256 MiB write) before every timed step; outputs far larger than L2",
                 "parallelism": f"weak, {world} independent batch(es)",
             },
-            "gpu_launches": 3 * args.steps,
+            "gpu_launches": 4 * args.steps,
             "clocks": clk.summary(),
             "roofline": {
                 "bound": "hbm",
@@ -1201,7 +1205,7 @@ def run_bondsep(args, world, rank, local):
                 "unit": "GB/s",
                 "frac": achieved / hbm if hbm else None,
                 "traffic": None,
-                "kernel": "fill_i32_kernel (x2) + bondsep_sources_kernel, one call incl. its status read-back",
+                "kernel": "fill_i32_kernel (x2) + bondsep_sources_kernel + status, one call",
                 "bytes_per_step": out_bytes + in_bytes,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)",
             },

@@ -46,10 +46,18 @@ typedef struct {
  *                       (6 where a slot does not exist); overwritten
  *   min_bondsep         [P, B, B] or NULL: the minimum over (c1, c2);
  *                       overwritten
- * Validates the connectivity (indices in range, every bond recorded in both
- * directions) and synchronises the stream once. */
+ *   status              one int32 on the device, required: set, once the
+ *                       enqueued work has run, to TMOL_B200_OK or to the
+ *                       error the connectivity shows (TMOL_B200_ERR_INDEX_RANGE
+ *                       for an index out of range, TMOL_B200_ERR_SHAPE for a
+ *                       bond recorded in one direction only,
+ *                       TMOL_B200_ERR_CAPACITY for more than 64 connection
+ *                       points within 5 bonds of one); the outputs are
+ *                       meaningful only when it reads TMOL_B200_OK
+ * Enqueued on `stream`; allocates nothing, does not synchronise.  The return
+ * value reports invalid arguments and launch failures only. */
 int tmol_b200_pose_bondsep(const tmol_b200_pose_connectivity* conn, int32_t* inter_block_bondsep,
-                           int32_t* min_bondsep, void* stream);
+                           int32_t* min_bondsep, int32_t* status, void* stream);
 
 /* Replaces tmol's stacked_apsp / tmol_apsp::apsp_op
  * (tmol/pose/compiled/apsp_ops.py:16-33, apsp.cuda.cu, apsp.cpu.cpp), in place

@@ -69,6 +69,15 @@ __global__ void bondsep_sources_kernel(PoseConn g, int32_t* ibb, int32_t* minsep
   }
 }
 
+// status bits -> a tmol_b200_status code, in the plan builders' priority
+__global__ void bondsep_status_kernel(int* status) {
+  const int b = *status;
+  *status = (b & kBsIndex) ? TMOL_B200_ERR_INDEX_RANGE
+            : (b & kBsShape) ? TMOL_B200_ERR_SHAPE
+            : (b & kBsCapacity) ? TMOL_B200_ERR_CAPACITY
+                                : TMOL_B200_OK;
+}
+
 // ---------------------------------------------------------------------------
 // stacked all-pairs shortest paths
 
@@ -206,8 +215,8 @@ using namespace tmol_b200;
 extern "C" {
 
 int tmol_b200_pose_bondsep(const tmol_b200_pose_connectivity* conn, int32_t* inter_block_bondsep,
-                           int32_t* min_bondsep, void* stream) {
-  if (!conn) return TMOL_B200_ERR_INVALID_ARGUMENT;
+                           int32_t* min_bondsep, int32_t* status, void* stream) {
+  if (!conn || !status) return TMOL_B200_ERR_INVALID_ARGUMENT;
   const tmol_b200_pose_connectivity& c = *conn;
   if (c.n_poses < 0 || c.max_n_blocks < 0 || c.n_block_types < 0 || c.max_n_conn < 1 || c.max_n_conn > 8)
     return TMOL_B200_ERR_SHAPE;
@@ -221,6 +230,7 @@ int tmol_b200_pose_bondsep(const tmol_b200_pose_connectivity* conn, int32_t* int
   int dev = 0, n_sm = 148;
   BS_CK(cudaGetDevice(&dev));
   BS_CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+  BS_CK(cudaMemsetAsync(status, 0, sizeof(int32_t), st));
   const int fill_grid = n_sm * 8;
   if (inter_block_bondsep && n_ibb > 0) {
     fill_i32_kernel<<<fill_grid, 256, 0, st>>>(inter_block_bondsep, n_ibb, MAX_SIG_SEP);
@@ -231,26 +241,12 @@ int tmol_b200_pose_bondsep(const tmol_b200_pose_connectivity* conn, int32_t* int
     BS_CK(cudaGetLastError());
   }
   if (PB == 0) return TMOL_B200_OK;
-  int* d_status = nullptr;
-  BS_CK(cudaMallocAsync((void**)&d_status, sizeof(int), st));
-  int rc = TMOL_B200_OK;
-  if (cudaMemsetAsync(d_status, 0, sizeof(int), st) != cudaSuccess) rc = TMOL_B200_ERR_CUDA;
   const int64_t n_src = PB * c.max_n_conn;
-  if (rc == TMOL_B200_OK) {
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n_src + 127) / 128, (int64_t)n_sm * 16));
-    bondsep_sources_kernel<<<grid, 128, 0, st>>>(pose_conn(c), inter_block_bondsep, min_bondsep, d_status);
-    if (cudaGetLastError() != cudaSuccess) rc = TMOL_B200_ERR_CUDA;
-  }
-  int h_status = 0;
-  if (rc == TMOL_B200_OK &&
-      cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess)
-    rc = TMOL_B200_ERR_CUDA;
-  if (cudaFreeAsync(d_status, st) != cudaSuccess) rc = TMOL_B200_ERR_CUDA;
-  if (cudaStreamSynchronize(st) != cudaSuccess) rc = TMOL_B200_ERR_CUDA;
-  if (rc != TMOL_B200_OK) return rc;
-  if (h_status & kBsIndex) return TMOL_B200_ERR_INDEX_RANGE;
-  if (h_status & kBsShape) return TMOL_B200_ERR_SHAPE;
-  if (h_status & kBsCapacity) return TMOL_B200_ERR_CAPACITY;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n_src + 127) / 128, (int64_t)n_sm * 16));
+  bondsep_sources_kernel<<<grid, 128, 0, st>>>(pose_conn(c), inter_block_bondsep, min_bondsep, status);
+  BS_CK(cudaGetLastError());
+  bondsep_status_kernel<<<1, 1, 0, st>>>(status);
+  BS_CK(cudaGetLastError());
   return TMOL_B200_OK;
 }
 

@@ -210,7 +210,7 @@ SIGNATURES = {
     "tmol_b200_elec_rotamer_forward": (ctypes.c_int, [_V, _V, _V, _I64, _I64, _V, _V]),
     "tmol_b200_elec_rotamer_backward": (ctypes.c_int, [_V, _V, _V, _I64, _I64, _V, _V, _V]),
     # PoseStack construction (include/tmol_b200_pose.h)
-    "tmol_b200_pose_bondsep": (ctypes.c_int, [ctypes.POINTER(PoseConnectivity), _V, _V, _V]),
+    "tmol_b200_pose_bondsep": (ctypes.c_int, [ctypes.POINTER(PoseConnectivity), _V, _V, _V, _V]),
     "tmol_b200_apsp_stacked": (ctypes.c_int, [_V, _I32, _I32, _I32, _V]),
     "tmol_b200_ljlk_plan_create_from_connectivity": (
         ctypes.c_int,

@@ -51,13 +51,22 @@ def pose_connectivity(pose_stack):
     )
 
 
-def bondsep_from_connectivity(block_type_ind, inter_residue_connections, bt_n_conn, bt_conn_sep, dense=True):
-    """(inter_block_bondsep or None, min_bondsep)."""
+def bondsep_from_connectivity(block_type_ind, inter_residue_connections, bt_n_conn, bt_conn_sep, dense=True,
+                              check=True, out=None):
+    """(inter_block_bondsep or None, min_bondsep).  With ``check`` the
+    device status is read (one synchronisation) and a bad connectivity
+    raises ``NativeError``; without, the status tensor is returned third
+    for the caller to read.  ``out`` = (ibb or None, min_bondsep, status)
+    reuses buffers."""
     s, keep = connectivity(block_type_ind, inter_residue_connections, bt_n_conn, bt_conn_sep)
     device = block_type_ind.device
     P, B, C = s.n_poses, s.max_n_blocks, s.max_n_conn
-    ibb = torch.empty((P, B, B, C, C), dtype=torch.int32, device=device) if dense else None
-    mb = torch.empty((P, B, B), dtype=torch.int32, device=device)
+    if out is None:
+        ibb = torch.empty((P, B, B, C, C), dtype=torch.int32, device=device) if dense else None
+        mb = torch.empty((P, B, B), dtype=torch.int32, device=device)
+        status = torch.empty(1, dtype=torch.int32, device=device)
+    else:
+        ibb, mb, status = out
     with torch.cuda.device(device):
         stream = torch.cuda.current_stream(device).cuda_stream
         native.call(
@@ -65,9 +74,13 @@ def bondsep_from_connectivity(block_type_ind, inter_residue_connections, bt_n_co
             ctypes.byref(s),
             ctypes.c_void_p(ibb.data_ptr() if ibb is not None else 0),
             ctypes.c_void_p(mb.data_ptr()),
+            ctypes.c_void_p(status.data_ptr()),
             ctypes.c_void_p(stream),
         )
     del keep
+    if not check:
+        return ibb, mb, status
+    native.check("tmol_b200_pose_bondsep", int(status.item()))
     return ibb, mb
 
 
