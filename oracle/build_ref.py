@@ -13,7 +13,10 @@ of the dispatch); the elec op (``torch.ops.tmol_elec.elec_pose_scores``) is
 the two matching files under ``tmol/score/elec/potentials``; the stacked
 all-pairs-shortest-paths op (``torch.ops.tmol_apsp.apsp_op``, the PoseStack
 builder's bond-separation step) is ``tmol/pose/compiled/apsp_vestibule.ops.cpp``
-with ``apsp.cpu.cpp``.  All use
+with ``apsp.cpu.cpp``; the LK-ball ops (``torch.ops.tmol_lk_ball``: water
+generation and pose / rotamer scores) are ``tmol/score/lk_ball/potentials/
+compiled.ops.cpp`` with ``lk_ball_pose_score.cpu.cpp`` and
+``gen_pose_waters.cpu.cpp``.  All use
 header-only code under ``tmol/`` and the
 vendored Eigen / moderngpu headers in ``tmol/extern``.  They are compiled in
 place with g++ -O3 through torch's extension builder (no reference build
@@ -32,6 +35,7 @@ OUT = os.path.join(HERE, "_ref")
 LIB_NAME = "tmol_ljlk_ref"
 ELEC_LIB_NAME = "tmol_elec_ref"
 APSP_LIB_NAME = "tmol_apsp_ref"
+LKBALL_LIB_NAME = "tmol_lk_ball_ref"
 
 
 def lib_path():
@@ -44,6 +48,10 @@ def elec_lib_path():
 
 def apsp_lib_path():
     return os.path.join(OUT, "apsp", APSP_LIB_NAME + ".so")
+
+
+def lk_ball_lib_path():
+    return os.path.join(OUT, "lk_ball", LKBALL_LIB_NAME + ".so")
 
 
 def build(ref=REF_DEFAULT, verbose=False):
@@ -60,6 +68,12 @@ def build(ref=REF_DEFAULT, verbose=False):
             os.path.join(OUT, "elec"),
         ),
         (APSP_LIB_NAME, "pose/compiled", ["apsp_vestibule.ops.cpp", "apsp.cpu.cpp"], os.path.join(OUT, "apsp")),
+        (
+            LKBALL_LIB_NAME,
+            "score/lk_ball/potentials",
+            ["compiled.ops.cpp", "lk_ball_pose_score.cpu.cpp", "gen_pose_waters.cpu.cpp"],
+            os.path.join(OUT, "lk_ball"),
+        ),
     ):
         src = os.path.join(ref, "tmol", *sub.split("/"))
         if not os.path.isdir(src):
@@ -80,4 +94,4 @@ def build(ref=REF_DEFAULT, verbose=False):
 if __name__ == "__main__":
     ref = sys.argv[1] if len(sys.argv) > 1 else REF_DEFAULT
     t = build(ref, verbose=True)
-    print(f"built {lib_path()}, {elec_lib_path()} and {apsp_lib_path()} in {t:.1f}s")
+    print(f"built {lib_path()}, {elec_lib_path()}, {apsp_lib_path()} and {lk_ball_lib_path()} in {t:.1f}s")

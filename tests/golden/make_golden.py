@@ -18,7 +18,10 @@ Writes
                      100 residues), plus the sizes and seeds that rebuild it
   elec.npz           the reference elec op (elec_pose_scores) on 1ubq and on
                      a jagged synthetic batch: per-pose energies, gradient,
-                     neighbour matrix and block-pair energies; and the
+                     neighbour matrix and block-pair energies, plus the
+                     reference test suite's stored 1ubq elec energy
+                     (tmol/tests/data/term_baselines/ElecEnergyTerm/
+                     test_whole_pose_scoring_10.yaml); and the
                      reference elec rotamer op (elec_rotamer_scores) on the
                      rotamer set of rotamers.npz (energies, indices, the
                      gradient of sum(w * E) for seeded w)
@@ -111,7 +114,11 @@ def main(ref_root):
         ref_neighbors=nbr,
     )
     eterm = ElecEnergyTerm()
-    out = {}
+    with open(
+        os.path.join(ref_root, "tmol/tests/data/term_baselines/ElecEnergyTerm/test_whole_pose_scoring_10.yaml")
+    ) as f:
+        elec_gold = yaml.safe_load(f)
+    out = {"ubq_tmol_test_energy": numpy.array([elec_gold["term0"]["pose0"]], dtype=numpy.float64)}
     for tag, eps_ in (("ubq", build_pose_stack([topo], [xyz])), ("syn", synthetic_pose_stack(ELEC_SIZES, ELEC_SEEDS))):
         coords = eps_.coords.flatten(0, 1)
         E, c, nbr = O.reference_elec_pose_scores(coords, elec_pose_score_args(eps_, eterm), require_gradient=True)

@@ -102,3 +102,14 @@ def test_oracle_rotamer_scores_match_reference_fixture(eterm):
     w = numpy.zeros((3, E.shape[1]), dtype=numpy.float32)
     w[0] = g["rot_weights"][0]
     assert numpy.array_equal(oc.rotamer_backward(nbr, w), g["rot_grad"])
+
+
+def test_oracle_reproduces_the_reference_suites_stored_energy(ubq_pose_stack, eterm):
+    """1ubq elec energy stored by tmol's own test suite
+    (tmol/tests/data/term_baselines/ElecEnergyTerm/test_whole_pose_scoring_10.yaml;
+    that test's tolerance is atol 1e-5, rtol 1e-3): pins this package's charge
+    and count-pair representative tables."""
+    g = load_golden("elec.npz")
+    oc = O.OracleCall(ubq_pose_stack.coords.flatten(0, 1), elec_pose_score_args(ubq_pose_stack, eterm), term="elec")
+    E, _, _ = oc.pose_scores()
+    numpy.testing.assert_allclose(E[0, 0], g["ubq_tmol_test_energy"][0], rtol=1e-6, atol=1e-5)

@@ -74,6 +74,9 @@ def test_fixture_parity(ubq_pose_stack, eterm):
         E, grad, nbr = gpu_scores(ps, eterm, weights=numpy.ones((1, 1)))
         assert E.shape == (1, ps.n_poses)
         E_close(E, g[f"{tag}_energies"])
+        if tag == "ubq":
+            # tmol's own stored 1ubq elec energy, at that test's tolerance
+            numpy.testing.assert_allclose(E[0, 0], g["ubq_tmol_test_energy"][0], atol=1e-5, rtol=1e-3)
         g_close(grad, g[f"{tag}_grad"])
         assert numpy.array_equal(nbr, g[f"{tag}_neighbors"]), tag
         Eb, _, _ = gpu_scores(ps, eterm, block_pair=True)
