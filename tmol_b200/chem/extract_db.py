@@ -13,7 +13,12 @@ pose builder use:
   the order ``chemical.yaml`` lists them, joined with its ``ljlk.yaml`` row
   (``tmol/score/ljlk/params.py:99-163`` performs the same join);
 * the canonical L-amino-acid residue types plus HIS_D;
-* the LJ/LK global parameters.
+* the LJ/LK global parameters, and the LK-ball water-placement ones
+  (``lkb_water_*``; angles converted to radians as tmol's unit parser does);
+* the hbond donor and acceptor atom types (``database/default/scoring/
+  hbond.yaml``: which atom types donate or accept, as the LK-ball term builds
+  waters on them) and each atom type's acceptor hybridization
+  (``chemical.yaml``).
 
 The elec term's parameters (``database/default/scoring/elec.yaml``: the
 sigmoidal-dielectric global parameters, per residue / variant / atom partial
@@ -53,6 +58,8 @@ def extract(db_root):
         chem = yaml.safe_load(f)
     with open(f"{db_root}/scoring/ljlk.yaml") as f:
         ljlk = yaml.safe_load(f)
+    with open(f"{db_root}/scoring/hbond.yaml") as f:
+        hbond = yaml.safe_load(f)
 
     elements = {e["name"]: e["atomic_number"] for e in chem["element_types"]}
     ljlk_rows = {r["name"]: r for r in ljlk["atom_type_parameters"]}
@@ -73,6 +80,7 @@ def extract(db_root):
                 is_acceptor=bool(at.get("is_acceptor", False)),
                 is_hydroxyl=bool(at.get("is_hydroxyl", False)),
                 is_polarh=bool(at.get("is_polarh", False)),
+                acceptor_hybridization=at.get("acceptor_hybridization"),
                 lj_radius=params[0],
                 lj_wdepth=params[1],
                 lk_dgfree=params[2],
@@ -132,11 +140,19 @@ def extract(db_root):
             "lk_min_dis2sigma",
         )
     }
+    lkball = {"lkb_water_dist": float(gp["lkb_water_dist"])}
+    for k in ("lkb_water_angle_sp2", "lkb_water_angle_sp3", "lkb_water_angle_ring"):
+        lkball[k] = math.radians(_deg(gp[k]))
+    for k in ("lkb_water_tors_sp2", "lkb_water_tors_sp3", "lkb_water_tors_ring"):
+        lkball[k] = [math.radians(_deg(v)) for v in gp[k]]
     return dict(
-        source="tmol parameter database (chemical.yaml + scoring/ljlk.yaml)",
+        source="tmol parameter database (chemical.yaml + scoring/ljlk.yaml + scoring/hbond.yaml)",
         atom_types=atom_types,
         residues=residues,
         ljlk_global_params=global_params,
+        lkball_global_params=lkball,
+        hbond_donor_atom_types=[x["d"] for x in hbond["donor_atom_types"]],
+        hbond_acceptor_atom_types=[x["a"] for x in hbond["acceptor_atom_types"]],
     )
 
 

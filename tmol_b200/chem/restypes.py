@@ -45,6 +45,9 @@ class ChemicalDatabase:
         self.atom_type_index = {a["name"]: i for i, a in enumerate(self.atom_types)}
         self.residues = {r["name"]: r for r in data["residues"]}
         self.ljlk_global_params = data["ljlk_global_params"]
+        self.lkball_global_params = data.get("lkball_global_params", {})
+        self.hbond_donor_atom_types = data.get("hbond_donor_atom_types", [])
+        self.hbond_acceptor_atom_types = data.get("hbond_acceptor_atom_types", [])
 
     @classmethod
     def get_default(cls):

@@ -1,0 +1,141 @@
+"""LKBallEnergyTerm: the LK-ball solvation term (lk_ball_iso, lk_ball,
+lk_bridge, lk_bridge_uncpl), with tmol's argument lists
+(``tmol/score/lk_ball/lk_ball_energy_term.py:17-369``).
+
+Scoring is two ops: water generation (``gen_pose_waters``: up to four
+waters per polar atom, built from the polar atom and its bonded
+neighbours) and the pose score over polar-atom / heavy-atom pairs of
+neighbouring blocks, reading the waters (``lk_ball_pose_score``).  This
+module assembles their arguments from a PoseStack; the block-type tables
+come from ``tmol_b200.chem.lkball_tables``, the global parameters from the
+LJ/LK ones (``max_dis``, the hbond distances) and the LK-ball water
+geometry in tmol's ``ljlk.yaml``.
+"""
+
+import torch
+
+from ..chem.lkball_tables import packed_lkball_tables
+from .score_types import ScoreType
+
+
+class LKBallEnergyTerm:
+    def __init__(self, device=torch.device("cpu")):
+        self.device = torch.device(device)
+
+    @classmethod
+    def class_name(cls):
+        return "LKBall"
+
+    @classmethod
+    def score_types(cls):
+        return [ScoreType.lk_ball_iso, ScoreType.lk_ball, ScoreType.lk_bridge, ScoreType.lk_bridge_uncpl]
+
+    def n_bodies(self):
+        return 2
+
+    def setup_poses(self, pose_stack):
+        if not hasattr(pose_stack, "min_block_bondsep"):
+            mbs, _ = torch.min(pose_stack.inter_block_bondsep, dim=4)
+            mbs, _ = torch.min(mbs, dim=3)
+            pose_stack.min_block_bondsep = mbs.contiguous()
+
+    @staticmethod
+    def _gp(pbt):
+        return pbt.db.ljlk_global_params, pbt.db.lkball_global_params
+
+    def water_gen_global_params(self, pbt, device):
+        """[1, 4] (water distance, sp2 / sp3 / ring angles) and the three
+        torsion lists, float32 as tmol's resolver holds them."""
+        _, lkb = self._gp(pbt)
+        gp = torch.tensor(
+            [[lkb["lkb_water_dist"], lkb["lkb_water_angle_sp2"], lkb["lkb_water_angle_sp3"],
+              lkb["lkb_water_angle_ring"]]],
+            dtype=torch.float32,
+            device=device,
+        )
+        tors = [
+            torch.tensor(lkb[k], dtype=torch.float32, device=device)
+            for k in ("lkb_water_tors_sp2", "lkb_water_tors_sp3", "lkb_water_tors_ring")
+        ]
+        return gp, tors
+
+    def score_global_params(self, pbt, device):
+        """[1, 5]: hbond distance, OH-donor distance, H distance, water
+        distance, max_dis (tmol lk_ball_energy_term.py:32-47)."""
+        lj, lkb = self._gp(pbt)
+        return torch.tensor(
+            [[lj["lj_hbond_dis"], lj["lj_hbond_OH_donor_dis"], lj["lj_hbond_hdis"], lkb["lkb_water_dist"],
+              lj["max_dis"]]],
+            dtype=torch.float32,
+            device=device,
+        )
+
+
+def _common(pose_stack):
+    return [
+        pose_stack.rot_coord_offset,
+        pose_stack.pose_ind_for_atom,
+        pose_stack.first_rot_for_block,
+        pose_stack.block_type_ind,
+        pose_stack.block_ind_for_rot,
+        pose_stack.pose_ind_for_rot,
+        pose_stack.block_type_ind_for_rot,
+        pose_stack.n_rots_for_pose,
+        pose_stack.rot_offset_for_pose,
+        pose_stack.n_rots_for_block,
+        pose_stack.rot_offset_for_block,
+        pose_stack.max_n_rots_per_pose,
+    ]
+
+
+def water_gen_args(pose_stack, term):
+    """gen_pose_waters' argument list minus the coordinates
+    (tmol lk_ball_energy_term.py:245-270, compiled.ops.cpp:28-64)."""
+    pbt = pose_stack.packed_block_types
+    t = packed_lkball_tables(pbt)
+    gp, tors = term.water_gen_global_params(pbt, pose_stack.device)
+    return _common(pose_stack) + [
+        pose_stack.inter_residue_connections,
+        pbt.n_atoms,
+        pbt.n_conn,
+        pbt.conn_atom,
+        t["n_all_bonds"],
+        t["all_bonds"],
+        t["atom_all_bond_ranges"],
+        t["tile_n_donH"],
+        t["tile_n_acc"],
+        t["tile_donH_inds"],
+        t["tile_donH_hvy_inds"],
+        t["tile_which_donH_of_donH_hvy"],
+        t["tile_acc_inds"],
+        t["tile_acceptor_hybridization"],
+        t["tile_acceptor_n_attached_H"],
+        t["is_hydrogen"],
+        gp,
+        *tors,
+    ]
+
+
+def score_args(pose_stack, term, water_coords, block_pair=False):
+    """lk_ball_pose_score's argument list minus the coordinates
+    (tmol lk_ball_energy_term.py:275-300)."""
+    term.setup_poses(pose_stack)
+    pbt = pose_stack.packed_block_types
+    t = packed_lkball_tables(pbt)
+    return _common(pose_stack) + [
+        pose_stack.inter_residue_connections,
+        pose_stack.min_block_bondsep,
+        pose_stack.inter_block_bondsep,
+        pbt.n_atoms,
+        pbt.n_conn,
+        pbt.conn_atom,
+        t["tile_n_polar_atoms"],
+        t["tile_n_occluder_atoms"],
+        t["tile_pol_occ_inds"],
+        t["tile_lk_ball_params"],
+        t["bond_separation"],
+        term.score_global_params(pbt, pose_stack.device),
+        float(torch.tensor(pbt.db.ljlk_global_params["max_dis"], dtype=torch.float32).item()),
+        water_coords,
+        block_pair,
+    ]
