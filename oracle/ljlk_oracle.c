@@ -1174,3 +1174,640 @@ int oracle_ljlk_rotamer_backward(const oracle_inputs_t* in, const int32_t* nbr,
   for_rot_pairs(in, nbr, rot_pair_adjoint, &job);
   return 0;
 }
+
+/* ====================================================================== */
+/* LK-ball (tmol/score/lk_ball/potentials): waters built on polar atoms    */
+/* (water.hh:330-601, gen_pose_waters.impl.hh:30-250, acceptor bases       */
+/* hbond/identification.hh:27-160, bond walk bonded_atom.hh:157-270) and   */
+/* the four-term pair potential (lk_ball.hh:34-540) over polar / occluder  */
+/* pairs of neighbouring blocks (lk_ball.hh:1270-1360,                     */
+/* lk_ball_pose_score.impl.hh:330-540).  Shared inputs come in             */
+/* oracle_inputs_t: bt_path_distance is the plain bond separation and      */
+/* bt_is_ligand all zero (LK-ball has no ligand count-pair rule).  Sums    */
+/* run in pair order, not the reference's tile order, so results agree to */
+/* rounding, not bit for bit.                                              */
+
+#define LKB_NW 4
+#define LKB_NP 9
+
+typedef struct {
+  const int32_t* irc;          /* [P][B][C][2] */
+  const int32_t* all_bonds;    /* [nbt][NB][3] */
+  const int32_t* bond_ranges;  /* [nbt][A][2] */
+  int NB, NT;
+  const int32_t* tile_n_donH;  /* [nbt][NT] */
+  const int32_t* tile_n_acc;
+  const int32_t* tile_donH_inds; /* [nbt][NT][32] */
+  const int32_t* tile_donH_hvy;
+  const int32_t* tile_which_donH;
+  const int32_t* tile_acc_inds;
+  const int32_t* tile_acc_hyb;
+  const int32_t* tile_acc_nH;
+  const int32_t* is_hydrogen;  /* [nbt][A] */
+  const int32_t* tile_n_polar; /* [nbt][NT] */
+  const int32_t* tile_n_occ;
+  const int32_t* tile_pol_occ; /* [nbt][NT][32] */
+  const real* tile_params;     /* [nbt][NT][32][9] */
+  real water_dist, ang_sp2, ang_sp3, ang_ring;
+  const real* tors_sp2;
+  const real* tors_sp3;
+  const real* tors_ring;
+  int n_sp2, n_sp3, n_ring;
+  real hbond_dis, hbond_OH_donor_dis, hbond_hdis, max_dis;
+} lkb_inputs_t;
+
+typedef struct {
+  int block, bt, atom;
+} bcat_t;
+
+static int bcat_eq(bcat_t a, bcat_t b) { return a.block == b.block && a.bt == b.bt && a.atom == b.atom; }
+
+/* the k-th bonded neighbour of (block, bt, atom) in pose p: an intra-block
+ * bond, or across connection c to the partner's connection atom; an
+ * unresolved connection gives atom -1 */
+static bcat_t lkb_bonded(const oracle_inputs_t* in, const lkb_inputs_t* k, int p, bcat_t x, int bidx) {
+  const int32_t* e = k->all_bonds + ((size_t)x.bt * k->NB + bidx) * 3;
+  bcat_t r = {x.block, x.bt, e[1]};
+  if (e[1] >= 0) return r;
+  const int32_t* t = k->irc + (((size_t)p * in->B + x.block) * in->C + e[2]) * 2;
+  if (t[1] < 0) {
+    r.block = r.bt = r.atom = -1;
+    return r;
+  }
+  r.block = t[0];
+  r.bt = in->first_rot_block_type[(size_t)p * in->B + t[0]];
+  r.atom = in->bt_conn_atom[(size_t)r.bt * in->C + t[1]];
+  return r;
+}
+
+static int lkb_is_h(const lkb_inputs_t* k, const oracle_inputs_t* in, bcat_t x) {
+  return x.atom >= 0 && k->is_hydrogen[(size_t)x.bt * in->A + x.atom];
+}
+
+static void lkb_range(const oracle_inputs_t* in, const lkb_inputs_t* k, bcat_t x, int* lo, int* hi) {
+  const int32_t* r = k->bond_ranges + ((size_t)x.bt * in->A + x.atom) * 2;
+  *lo = r[0];
+  *hi = r[1];
+}
+
+/* identification.hh:35-148; hyb 1 sp2, 2 sp3, 3 ring.  Returns 0 when the
+ * water frame is undefined (no base, or B0 == B). */
+static int lkb_acc_bases(const oracle_inputs_t* in, const lkb_inputs_t* k, int p, bcat_t A, int hyb, bcat_t* B,
+                         bcat_t* B0) {
+  bcat_t none = {-1, -1, -1};
+  int lo, hi;
+  *B = none;
+  *B0 = none;
+  if (hyb < 1 || hyb > 3) return 0;
+  lkb_range(in, k, A, &lo, &hi);
+  for (int i = lo; i < hi; ++i) {
+    bcat_t o = lkb_bonded(in, k, p, A, i);
+    if (o.atom >= 0 && !lkb_is_h(k, in, o)) {
+      *B = o;
+      break;
+    }
+  }
+  if (hyb == 1) {
+    if (B->atom < 0) return 0;
+    int lo2, hi2;
+    lkb_range(in, k, *B, &lo2, &hi2);
+    for (int i = lo2; i < hi2; ++i) {
+      bcat_t o = lkb_bonded(in, k, p, *B, i);
+      if (o.atom < 0) continue;
+      if (B->block != A.block && o.block == A.block) continue;
+      if (!bcat_eq(o, A)) {
+        *B0 = o;
+        break;
+      }
+    }
+    if (B0->atom < 0) return 0;
+  } else if (hyb == 2) {
+    for (int i = lo; i < hi; ++i) {
+      bcat_t o = lkb_bonded(in, k, p, A, i);
+      if (o.atom >= 0 && !bcat_eq(o, *B) && lkb_is_h(k, in, o)) {
+        *B0 = o;
+        break;
+      }
+    }
+    if (B0->atom < 0)
+      for (int i = lo; i < hi; ++i) {
+        bcat_t o = lkb_bonded(in, k, p, A, i);
+        if (o.atom >= 0 && !bcat_eq(o, *B)) {
+          *B0 = o;
+          break;
+        }
+      }
+    if (B0->atom < 0) *B0 = *B;
+  } else {
+    if (B->atom < 0) return 0;
+    for (int i = lo; i < hi; ++i) {
+      bcat_t o = lkb_bonded(in, k, p, A, i);
+      if (o.atom >= 0 && !bcat_eq(o, *B) && !lkb_is_h(k, in, o)) {
+        *B0 = o;
+        break;
+      }
+    }
+    if (B0->atom < 0) return 0;
+  }
+  if (B->atom < 0 || bcat_eq(*B0, *B)) return 0;
+  return 1;
+}
+
+static size_t lkb_atom_row(const oracle_inputs_t* in, int p, bcat_t x) {
+  int rot = in->rot_offset_for_block[(size_t)p * in->B + x.block];
+  return (size_t)in->rot_coord_offset[rot] + x.atom;
+}
+
+static void v3_load(const real* c, size_t row, real v[3]) {
+  v[0] = c[3 * row];
+  v[1] = c[3 * row + 1];
+  v[2] = c[3 * row + 2];
+}
+static real v3_dot(const real* a, const real* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+static void v3_cross(const real* a, const real* b, real* o) {
+  o[0] = a[1] * b[2] - a[2] * b[1];
+  o[1] = a[2] * b[0] - a[0] * b[2];
+  o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+/* gen_coord.hh:40-74: the point at `dist` from A, angle(W, A, B) = angle,
+ * torsion(W, A, B, C) = torsion.  M = [e0, e1, e2] with e0 = (A - B) / |A - B|,
+ * e2 = e0 x (C - B) normalised, e1 = e2 x e0. */
+typedef struct {
+  real e0[3], e1[3], e2[3], u[3], c[3], nd, nu, v[3];
+} frame_t;
+
+static void lkb_frame(const real* A, const real* Bp, const real* C, real dist, real angle, real tor, frame_t* f) {
+  const real pi = (real)3.14159265358979323846;
+  real d[3];
+  for (int i = 0; i < 3; ++i) {
+    d[i] = A[i] - Bp[i];
+    f->c[i] = C[i] - Bp[i];
+  }
+  f->nd = rsqrt_(v3_dot(d, d));
+  for (int i = 0; i < 3; ++i) f->e0[i] = d[i] / f->nd;
+  v3_cross(f->e0, f->c, f->u);
+  f->nu = rsqrt_(v3_dot(f->u, f->u));
+  if (f->nu == 0) {
+    real alt[3] = {1, 0, 0};
+    if (f->e0[0] == 1 || f->e0[0] == -1) {
+      alt[0] = 0;
+      alt[1] = 1;
+    }
+    v3_cross(f->e0, alt, f->u);
+    f->nu = rsqrt_(v3_dot(f->u, f->u));
+  }
+  for (int i = 0; i < 3; ++i) f->e2[i] = f->u[i] / f->nu;
+  v3_cross(f->e2, f->e0, f->e1);
+  real sa = (real)sin(pi - angle), ca = (real)cos(pi - angle);
+  f->v[0] = dist * ca;
+  f->v[1] = dist * sa * (real)cos(tor);
+  f->v[2] = dist * sa * (real)sin(tor);
+}
+
+static void lkb_build(const real* A, const frame_t* f, real* W) {
+  for (int i = 0; i < 3; ++i) W[i] = A[i] + f->v[0] * f->e0[i] + f->v[1] * f->e1[i] + f->v[2] * f->e2[i];
+}
+
+/* vector-Jacobian product of lkb_build: gA, gB, gC += d(g . W)/d(A, B, C) */
+static void lkb_build_vjp(const frame_t* f, const real* g, real* gA, real* gB, real* gC) {
+  real ge0[3], ge1[3], ge2[3], t[3], gu[3], gd[3];
+  for (int i = 0; i < 3; ++i) {
+    gA[i] += g[i];
+    ge0[i] = f->v[0] * g[i];
+    ge1[i] = f->v[1] * g[i];
+    ge2[i] = f->v[2] * g[i];
+  }
+  /* e1 = e2 x e0 */
+  v3_cross(f->e0, ge1, t);
+  for (int i = 0; i < 3; ++i) ge2[i] += t[i];
+  v3_cross(ge1, f->e2, t);
+  for (int i = 0; i < 3; ++i) ge0[i] += t[i];
+  /* e2 = u / |u| */
+  real s = v3_dot(f->e2, ge2);
+  for (int i = 0; i < 3; ++i) gu[i] = (ge2[i] - f->e2[i] * s) / f->nu;
+  /* u = e0 x c */
+  v3_cross(f->c, gu, t);
+  for (int i = 0; i < 3; ++i) ge0[i] += t[i];
+  real gc[3];
+  v3_cross(gu, f->e0, gc);
+  /* e0 = (A - B) / |A - B| */
+  s = v3_dot(f->e0, ge0);
+  for (int i = 0; i < 3; ++i) gd[i] = (ge0[i] - f->e0[i] * s) / f->nd;
+  for (int i = 0; i < 3; ++i) {
+    gA[i] += gd[i];
+    gB[i] -= gd[i] + gc[i];
+    gC[i] += gc[i];
+  }
+}
+
+/* one water site: its atoms and how it is built */
+typedef struct {
+  int kind;  /* 0 none, 1 donor (D, H), 2 acceptor (A, B, B0) */
+  int hyb;
+  size_t rowA, rowB, rowB0; /* donor: rowA = D, rowB = H */
+  real tor, ang;
+} lkb_site_t;
+
+/* the site of water slot `w` of pose-atom (p, b, atom), or kind 0 */
+static void lkb_sites_for_block(const oracle_inputs_t* in, const lkb_inputs_t* k, int p, int b,
+                                lkb_site_t* sites /* [n_atoms][4] */) {
+  int bt = in->first_rot_block_type[(size_t)p * in->B + b];
+  int n = in->bt_n_atoms[bt];
+  for (int i = 0; i < n * LKB_NW; ++i) sites[i].kind = 0;
+  for (int t = 0; t < k->NT; ++t) {
+    size_t tb = ((size_t)bt * k->NT + t);
+    for (int q = 0; q < k->tile_n_donH[tb]; ++q) {
+      int H = t * TILE + k->tile_donH_inds[tb * TILE + q];
+      int D = k->tile_donH_hvy[tb * TILE + q];
+      int which = k->tile_which_donH[tb * TILE + q];
+      bcat_t dh = {b, bt, D}, hh = {b, bt, H};
+      lkb_site_t* s = &sites[D * LKB_NW + which];
+      s->kind = 1;
+      s->rowA = lkb_atom_row(in, p, dh);
+      s->rowB = lkb_atom_row(in, p, hh);
+    }
+    for (int q = 0; q < k->tile_n_acc[tb]; ++q) {
+      int Aat = t * TILE + k->tile_acc_inds[tb * TILE + q];
+      int hyb = k->tile_acc_hyb[tb * TILE + q];
+      int nH = k->tile_acc_nH[tb * TILE + q];
+      bcat_t A = {b, bt, Aat}, Bb, B0;
+      if (!lkb_acc_bases(in, k, p, A, hyb, &Bb, &B0)) continue;
+      const real* tors = hyb == 1 ? k->tors_sp2 : hyb == 2 ? k->tors_sp3 : k->tors_ring;
+      int nt = hyb == 1 ? k->n_sp2 : hyb == 2 ? k->n_sp3 : k->n_ring;
+      real ang = hyb == 1 ? k->ang_sp2 : hyb == 2 ? k->ang_sp3 : k->ang_ring;
+      for (int w = 0; w < LKB_NW && w < nt; ++w) {
+        if (w + nH >= LKB_NW) break;
+        lkb_site_t* s = &sites[Aat * LKB_NW + w + nH];
+        s->kind = 2;
+        s->hyb = hyb;
+        s->rowA = lkb_atom_row(in, p, A);
+        s->rowB = lkb_atom_row(in, p, Bb);
+        s->rowB0 = lkb_atom_row(in, p, B0);
+        s->tor = tors[w];
+        s->ang = ang;
+      }
+    }
+  }
+}
+
+static void lkb_site_water(const oracle_inputs_t* in, const lkb_inputs_t* k, const lkb_site_t* s, real* W,
+                           frame_t* f) {
+  real A[3], Bv[3], B0v[3];
+  v3_load(in->coords, s->rowA, A);
+  v3_load(in->coords, s->rowB, Bv);
+  if (s->kind == 1) {
+    /* water.hh:42-44: D + dist * (H - D) / |H - D| */
+    real h[3] = {Bv[0] - A[0], Bv[1] - A[1], Bv[2] - A[2]};
+    real nh = rsqrt_(v3_dot(h, h));
+    for (int i = 0; i < 3; ++i) W[i] = A[i] + k->water_dist * (h[i] / nh);
+    return;
+  }
+  v3_load(in->coords, s->rowB0, B0v);
+  if (s->hyb == 3)
+    for (int i = 0; i < 3; ++i) Bv[i] = (Bv[i] + B0v[i]) / 2;
+  lkb_frame(A, Bv, B0v, k->water_dist, s->ang, s->tor, f);
+  lkb_build(A, f, W);
+}
+
+/* gen_pose_waters: W [n_atoms][4][3], NAN where no water is built */
+int oracle_lkb_waters(const oracle_inputs_t* in, const lkb_inputs_t* k, real* W) {
+  for (size_t i = 0; i < (size_t)in->n_atoms * LKB_NW * 3; ++i) W[i] = (real)NAN;
+  lkb_site_t* sites = (lkb_site_t*)malloc(sizeof(lkb_site_t) * (size_t)in->A * LKB_NW);
+  if (!sites) return 2;
+  for (int p = 0; p < in->P; ++p)
+    for (int b = 0; b < in->B; ++b) {
+      int bt = in->first_rot_block_type[(size_t)p * in->B + b];
+      if (bt < 0) continue;
+      lkb_sites_for_block(in, k, p, b, sites);
+      int rot = in->rot_offset_for_block[(size_t)p * in->B + b];
+      size_t off = in->rot_coord_offset[rot];
+      for (int a = 0; a < in->bt_n_atoms[bt]; ++a)
+        for (int w = 0; w < LKB_NW; ++w) {
+          frame_t f;
+          if (sites[a * LKB_NW + w].kind)
+            lkb_site_water(in, k, &sites[a * LKB_NW + w], W + ((off + a) * LKB_NW + w) * 3, &f);
+        }
+    }
+  free(sites);
+  return 0;
+}
+
+/* lk_ball.hh:34-39 */
+static const real lkb_overlap_gap = (real)0.5, lkb_overlap_width = (real)2.6;
+#define LKB_ANGLE_OVERLAP ((real)2.8 * lkb_overlap_width)
+static const real lkb_ramp_width = (real)3.709;
+static real sq_(real v) { return v * v; }
+
+/* lk_fraction (lk_ball.hh:42-124): value and d/dJ, d/dWI */
+static real lkb_fraction(const real* WI, const real* J, real lj_radius_j, real* dJ, real* dWI) {
+  real d2_low = sq_((real)1.4 + lj_radius_j) - lkb_ramp_width;
+  if (d2_low < 0) d2_low = 0;
+  real wsum = 0, gJ[3] = {0, 0, 0}, gW[LKB_NW * 3] = {0};
+  for (int w = 0; w < LKB_NW; ++w) {
+    real dl[3] = {J[0] - WI[3 * w], J[1] - WI[3 * w + 1], J[2] - WI[3 * w + 2]};
+    real d2 = v3_dot(dl, dl) - d2_low;
+    if (isnan(d2)) continue;
+    real e = rexp_(-d2);
+    wsum += e;
+    for (int i = 0; i < 3; ++i) {
+      gJ[i] += 2 * e * dl[i];
+      gW[3 * w + i] = -2 * e * dl[i];
+    }
+  }
+  if (wsum != 0)
+    for (int i = 0; i < 3; ++i) {
+      gJ[i] /= wsum;
+      for (int w = 0; w < LKB_NW; ++w) gW[3 * w + i] /= wsum;
+    }
+  real x = -(real)log(wsum);
+  real frac = 0, df = 0;
+  if (x < 0)
+    frac = 1;
+  else if (x < lkb_ramp_width)
+    frac = sq_(1 - sq_(x / lkb_ramp_width));
+  if (x > 0 && x < lkb_ramp_width)
+    df = -4 * x * (sq_(lkb_ramp_width) - sq_(x)) / sq_(sq_(lkb_ramp_width));
+  if (dJ)
+    for (int i = 0; i < 3; ++i) dJ[i] = gJ[i] * df;
+  if (dWI)
+    for (int i = 0; i < LKB_NW * 3; ++i) dWI[i] = gW[i] * df;
+  return frac;
+}
+
+/* lk_bridge_fraction (lk_ball.hh:126-277) */
+static real lkb_bridge(const real* I, const real* J, const real* WI, const real* WJ, real water_dist, real* dI,
+                       real* dJ, real* dWI, real* dWJ) {
+  real wsum = 0, gWI[LKB_NW * 3] = {0}, gWJ[LKB_NW * 3] = {0};
+  for (int a = 0; a < LKB_NW; ++a)
+    for (int c = 0; c < LKB_NW; ++c) {
+      real dl[3] = {WI[3 * a] - WJ[3 * c], WI[3 * a + 1] - WJ[3 * c + 1], WI[3 * a + 2] - WJ[3 * c + 2]};
+      real d2 = v3_dot(dl, dl) - lkb_overlap_gap;
+      if (isnan(d2)) continue;
+      real e = rexp_(-d2);
+      for (int i = 0; i < 3; ++i) {
+        gWI[3 * a + i] += 2 * e * dl[i];
+        gWJ[3 * c + i] -= 2 * e * dl[i];
+      }
+      wsum += e;
+    }
+  if (wsum != 0)
+    for (int i = 0; i < LKB_NW * 3; ++i) {
+      gWI[i] /= wsum;
+      gWJ[i] /= wsum;
+    }
+  real x = -(real)log(wsum);
+  real ofrac, dof;
+  if (x > lkb_overlap_width) {
+    ofrac = 0;
+    dof = 0;
+  } else if (x > 0) {
+    ofrac = sq_(1 - sq_(x / lkb_overlap_width));
+    dof = -4 * x * (sq_(lkb_overlap_width) - sq_(x)) / sq_(sq_(lkb_overlap_width));
+  } else {
+    ofrac = 1;
+    dof = 0;
+  }
+  real target = (real)(8.0 / 3.0) * sq_(water_dist);
+  real dIJ[3] = {I[0] - J[0], I[1] - J[1], I[2] - J[2]};
+  real base = v3_dot(dIJ, dIJ) - target;
+  real afrac, daf;
+  real ab = base < 0 ? -base : base;
+  if (ab > LKB_ANGLE_OVERLAP) {
+    afrac = 0;
+    daf = 0;
+  } else if (ab > 0) {
+    afrac = sq_(1 - sq_(base / LKB_ANGLE_OVERLAP));
+    daf = -4 * base * (sq_(LKB_ANGLE_OVERLAP) - sq_(base)) / sq_(sq_(LKB_ANGLE_OVERLAP));
+  } else {
+    afrac = 1;
+    daf = 0;
+  }
+  if (dI)
+    for (int i = 0; i < 3; ++i) {
+      dI[i] = ofrac * daf * 2 * dIJ[i];
+      dJ[i] = -ofrac * daf * 2 * dIJ[i];
+    }
+  if (dWI)
+    for (int i = 0; i < LKB_NW * 3; ++i) {
+      dWI[i] = afrac * dof * gWI[i];
+      dWJ[i] = afrac * dof * gWJ[i];
+    }
+  return ofrac * afrac;
+}
+
+typedef struct {
+  real lj_radius, lk_dgfree, lk_lambda, lk_volume, is_donor, is_hydroxyl, is_polarh, is_acceptor, is_carbon_lk;
+} lkb_params_t;
+
+/* ljlk common.hh:25-44 with LK-ball's atom parameters */
+static real lkb_sigma(const lkb_params_t* i, const lkb_params_t* j, const lkb_inputs_t* k) {
+  if ((i->is_donor != 0 && j->is_acceptor != 0) || (j->is_donor != 0 && i->is_acceptor != 0)) {
+    if ((i->is_donor != 0 && i->is_hydroxyl != 0) || (j->is_donor != 0 && j->is_hydroxyl != 0))
+      return k->hbond_OH_donor_dis;
+    return k->hbond_dis;
+  } else if ((i->is_polarh != 0 && j->is_acceptor != 0) || (j->is_polarh != 0 && i->is_acceptor != 0)) {
+    return k->hbond_hdis;
+  }
+  return i->lj_radius + j->lj_radius;
+}
+
+/* lk_ball_score (lk_ball.hh:335-500) for polar I (waters WI) against
+ * occluder J (waters WJ): E[4]; with g (dL/dE[4]) the adjoint adds to
+ * gI, gJ, gWI, gWJ */
+static void lkb_pair(const real* I, const real* J, const real* WI, const real* WJ, int sep, const lkb_params_t* pi,
+                     const lkb_params_t* pj, const lkb_inputs_t* k, real* E, const real* g, real* gI, real* gJ,
+                     real* gWI, real* gWJ) {
+  E[0] = E[1] = E[2] = E[3] = 0;
+  if (sep <= 3) return;
+  real dv[3] = {I[0] - J[0], I[1] - J[1], I[2] - J[2]};
+  real dist = rsqrt_(v3_dot(dv, dv));
+  if (dist >= k->max_dis) return;
+  if (isnan(WI[0])) return;
+  real sigma = lkb_sigma(pi, pj, k);
+  real iso, diso;
+  lk_isotropic_pair_V_dV(dist, (real)sep, sigma, pi->lj_radius, pi->lk_dgfree, pi->lk_lambda, pj->lk_volume,
+                         k->max_dis, pi->is_carbon_lk != 0 && pj->is_carbon_lk != 0, &iso, &diso);
+  real fdJ[3], fdWI[LKB_NW * 3];
+  real fdes = lkb_fraction(WI, J, pj->lj_radius, fdJ, fdWI);
+  real bdI[3] = {0, 0, 0}, bdJ[3] = {0, 0, 0}, bdWI[LKB_NW * 3] = {0}, bdWJ[LKB_NW * 3] = {0};
+  real fov = 0;
+  if (pj->is_donor != 0 || pj->is_acceptor != 0) fov = lkb_bridge(I, J, WI, WJ, k->water_dist, bdI, bdJ, bdWI, bdWJ);
+  E[0] = iso;
+  E[1] = iso * fdes;
+  E[2] = iso * fov;
+  E[3] = fov / 2;
+  if (!g) return;
+  /* unit vector of the distance, zero at coincidence (geom.hh:20-40) */
+  real u[3] = {0, 0, 0};
+  if (dist != 0)
+    for (int i = 0; i < 3; ++i) u[i] = dv[i] / dist;
+  real giso = g[0] + g[1] * fdes + g[2] * fov;
+  for (int i = 0; i < 3; ++i) {
+    gI[i] += giso * diso * u[i] + g[2] * iso * bdI[i] + g[3] * bdI[i] / 2;
+    gJ[i] += -giso * diso * u[i] + g[1] * iso * fdJ[i] + g[2] * iso * bdJ[i] + g[3] * bdJ[i] / 2;
+  }
+  for (int i = 0; i < LKB_NW * 3; ++i) {
+    gWI[i] += g[1] * iso * fdWI[i] + g[2] * iso * bdWI[i] + g[3] * bdWI[i] / 2;
+    gWJ[i] += g[2] * iso * bdWJ[i] + g[3] * bdWJ[i] / 2;
+  }
+}
+
+/* polar / occluder lists of one block (all tiles): block-type atom index
+ * and parameters */
+static int lkb_lists(const oracle_inputs_t* in, const lkb_inputs_t* k, int bt, int* pol, int* occ, int* n_pol,
+                     const real** ppar, const real** opar) {
+  int np = 0, no = 0;
+  for (int t = 0; t < k->NT; ++t) {
+    size_t tb = (size_t)bt * k->NT + t;
+    int npt = k->tile_n_polar[tb], nott = k->tile_n_occ[tb];
+    for (int q = 0; q < nott; ++q) {
+      int a = t * TILE + k->tile_pol_occ[tb * TILE + q];
+      const real* par = k->tile_params + (tb * TILE + q) * LKB_NP;
+      if (q < npt) {
+        pol[np] = a;
+        ppar[np++] = par;
+      }
+      occ[no] = a;
+      opar[no++] = par;
+    }
+  }
+  *n_pol = np;
+  return no;
+}
+
+/* lk_ball_pose_score, whole-pose: E [4][P]; with wts [4][P] the gradient of
+ * sum_t wts[t][p] E[t][p] w.r.t. the coordinates (through the waters) goes
+ * to dx [n_atoms][3]; nbr [P][B][B] gets the block-neighbour matrix. */
+int oracle_lkb_pose_scores(const oracle_inputs_t* in, const lkb_inputs_t* k, const real* W, real* E,
+                           const real* wts, real* dx, int32_t* nbr) {
+  const int P = in->P, B = in->B, A = in->A;
+  real* spheres = (real*)malloc(sizeof(real) * 4 * ((size_t)P * B + 1));
+  int* pol1 = (int*)malloc(sizeof(int) * 4 * (size_t)(A + 1));
+  const real** par1 = (const real**)malloc(sizeof(real*) * 4 * (size_t)(A + 1));
+  real* gW = dx ? (real*)calloc((size_t)in->n_atoms * LKB_NW * 3 + 1, sizeof(real)) : NULL;
+  if (!spheres || !pol1 || !par1 || (dx && !gW)) return 2;
+  int *occ1 = pol1 + (A + 1), *pol2 = pol1 + 2 * (A + 1), *occ2 = pol1 + 3 * (A + 1);
+  const real **opar1 = par1 + (A + 1), **ppar2 = par1 + 2 * (A + 1), **opar2 = par1 + 3 * (A + 1);
+  compute_spheres(in, spheres);
+  detect_neighbors(in, spheres, nbr);
+  for (size_t i = 0; i < (size_t)4 * P; ++i) E[i] = 0;
+  if (dx)
+    for (size_t i = 0; i < (size_t)in->n_atoms * 3; ++i) dx[i] = 0;
+  for (int p = 0; p < P; ++p)
+    for (int b1 = 0; b1 < B; ++b1)
+      for (int b2 = b1; b2 < B; ++b2) {
+        if (!nbr[((size_t)p * B + b1) * B + b2]) continue;
+        pair_ctx_t c;
+        if (!setup_pair(in, p, b1, b2, &c)) continue;
+        int np1, np2;
+        int no1 = lkb_lists(in, k, c.bt1, pol1, occ1, &np1, par1, opar1);
+        int no2 = lkb_lists(in, k, c.bt2, pol2, occ2, &np2, ppar2, opar2);
+        real g4[4];
+        const real* gp = NULL;
+        if (dx) {
+          for (int t = 0; t < 4; ++t) g4[t] = wts[(size_t)t * P + p];
+          gp = g4;
+        }
+        /* (polar of side s, occluder of the other side) */
+        for (int side = 0; side < 2; ++side) {
+          if (b1 == b2 && side == 1) break;
+          const int* pol = side ? pol2 : pol1;
+          const real** ppar = side ? ppar2 : par1;
+          int npol = side ? np2 : np1;
+          const int* occ = (b1 == b2) ? occ1 : (side ? occ1 : occ2);
+          const real** opar = (b1 == b2) ? opar1 : (side ? opar1 : opar2);
+          int nocc = (b1 == b2) ? no1 : (side ? no1 : no2);
+          int offp = side ? c.off2 : c.off1, offo = (b1 == b2) ? c.off1 : (side ? c.off1 : c.off2);
+          for (int x = 0; x < npol; ++x)
+            for (int y = 0; y < nocc; ++y) {
+              int ap = pol[x], ao = occ[y];
+              if (b1 == b2 && ap == ao) continue;
+              int sep;
+              if (b1 == b2)
+                sep = in->bt_path_distance[((size_t)c.bt1 * A + ap) * A + ao];
+              else
+                sep = side ? inter_separation(in, &c, ao, ap) : inter_separation(in, &c, ap, ao);
+              size_t rp = (size_t)offp + ap, ro = (size_t)offo + ao;
+              real I[3], J[3], e[4];
+              v3_load(in->coords, rp, I);
+              v3_load(in->coords, ro, J);
+              lkb_params_t pi, pj;
+              memcpy(&pi, ppar[x], sizeof(pi));
+              memcpy(&pj, opar[y], sizeof(pj));
+              real gI[3] = {0, 0, 0}, gJ[3] = {0, 0, 0}, gWI[LKB_NW * 3] = {0}, gWJ[LKB_NW * 3] = {0};
+              lkb_pair(I, J, W + rp * LKB_NW * 3, W + ro * LKB_NW * 3, sep, &pi, &pj, k, e, gp, gI, gJ, gWI,
+                       gWJ);
+              for (int t = 0; t < 4; ++t) E[(size_t)t * P + p] += e[t];
+              if (dx) {
+                for (int i = 0; i < 3; ++i) {
+                  dx[3 * rp + i] += gI[i];
+                  dx[3 * ro + i] += gJ[i];
+                }
+                for (int i = 0; i < LKB_NW * 3; ++i) {
+                  gW[rp * LKB_NW * 3 + i] += gWI[i];
+                  gW[ro * LKB_NW * 3 + i] += gWJ[i];
+                }
+              }
+            }
+        }
+      }
+  if (dx) {
+    /* the waters' adjoint onto the atoms that place them (water.hh:412-600) */
+    lkb_site_t* sites = (lkb_site_t*)malloc(sizeof(lkb_site_t) * (size_t)A * LKB_NW);
+    for (int p = 0; p < P && sites; ++p)
+      for (int b = 0; b < B; ++b) {
+        int bt = in->first_rot_block_type[(size_t)p * B + b];
+        if (bt < 0) continue;
+        lkb_sites_for_block(in, k, p, b, sites);
+        int rot = in->rot_offset_for_block[(size_t)p * B + b];
+        size_t off = in->rot_coord_offset[rot];
+        for (int a = 0; a < in->bt_n_atoms[bt]; ++a)
+          for (int w = 0; w < LKB_NW; ++w) {
+            const lkb_site_t* s = &sites[a * LKB_NW + w];
+            if (!s->kind) continue;
+            const real* g = gW + ((off + a) * LKB_NW + w) * 3;
+            if (g[0] == 0 && g[1] == 0 && g[2] == 0) continue;
+            real Av[3], Bv[3];
+            v3_load(in->coords, s->rowA, Av);
+            v3_load(in->coords, s->rowB, Bv);
+            if (s->kind == 1) {
+              real h[3] = {Bv[0] - Av[0], Bv[1] - Av[1], Bv[2] - Av[2]};
+              real nh = rsqrt_(v3_dot(h, h));
+              real n[3] = {h[0] / nh, h[1] / nh, h[2] / nh};
+              real gn[3] = {k->water_dist * g[0], k->water_dist * g[1], k->water_dist * g[2]};
+              real sdot = v3_dot(n, gn);
+              for (int i = 0; i < 3; ++i) {
+                real gh = (gn[i] - n[i] * sdot) / nh;
+                dx[3 * s->rowA + i] += g[i] - gh;
+                dx[3 * s->rowB + i] += gh;
+              }
+              continue;
+            }
+            real B0v[3], Bm[3];
+            v3_load(in->coords, s->rowB0, B0v);
+            for (int i = 0; i < 3; ++i) Bm[i] = s->hyb == 3 ? (Bv[i] + B0v[i]) / 2 : Bv[i];
+            frame_t f;
+            lkb_frame(Av, Bm, B0v, k->water_dist, s->ang, s->tor, &f);
+            real gA[3] = {0, 0, 0}, gB[3] = {0, 0, 0}, gC[3] = {0, 0, 0};
+            lkb_build_vjp(&f, g, gA, gB, gC);
+            for (int i = 0; i < 3; ++i) {
+              dx[3 * s->rowA + i] += gA[i];
+              if (s->hyb == 3) {
+                dx[3 * s->rowB + i] += gB[i] / 2;
+                dx[3 * s->rowB0 + i] += gB[i] / 2;
+              } else {
+                dx[3 * s->rowB + i] += gB[i];
+              }
+              dx[3 * s->rowB0 + i] += gC[i];
+            }
+          }
+      }
+    free(sites);
+  }
+  free(spheres);
+  free(pol1);
+  free(par1);
+  free(gW);
+  return 0;
+}

@@ -93,9 +93,21 @@ class OracleCall:
     list (``tmol/score/elec/potentials/compiled.ops.cpp:28-59``) instead of
     the LJ/LK op's; energies then come back as [1, ...]."""
 
-    def __init__(self, coords, args, f64=False, term="ljlk"):
+    def __init__(self, coords, args, f64=False, term="ljlk", lkb_water_args=None):
         self.f64 = f64
         self.term = term
+        if term == "lkball":
+            # LK-ball: the score op's arguments (tmol_b200.score.lkball_energy_term.score_args)
+            # for the shared tables; the water-generation ones for the rest
+            (irc, min_bondsep, ibb, bt_n_atoms, bt_n_conn, bt_conn_atom, t_npol, t_nocc, t_polocc, t_params,
+             bond_sep, lkb_global, max_dis) = args[12:25]
+            nbt = bt_n_atoms.shape[0]
+            lkb_tables = (irc, t_npol, t_nocc, t_polocc, t_params, lkb_global)
+            args = list(args[:12]) + [
+                min_bondsep, ibb, bt_n_atoms, None, None, None, bt_n_conn, bt_conn_atom, bond_sep,
+                torch.zeros(nbt, dtype=torch.int32), None, None, max_dis,
+            ]
+            lkb_A = bond_sep.shape[1]
         if term == "elec":
             (min_bondsep, ibb, bt_n_atoms, bt_charge, bt_n_conn, bt_conn_atom, inter_rpd, intra_rpd,
              bt_is_ligand, elec_global, max_dis) = args[12:23]
@@ -183,12 +195,84 @@ class OracleCall:
         s.P = first_rot_block_type.shape[0]
         s.B = first_rot_block_type.shape[1]
         s.nbt = bt_n_atoms.shape[0]
-        s.A = (bt_charge if term == "elec" else bt_atom_types).shape[1]
+        if term == "lkball":
+            s.A = lkb_A
+        else:
+            s.A = (bt_charge if term == "elec" else bt_atom_types).shape[1]
         s.C = bt_conn_atom.shape[1]
-        s.ntiles = 0 if term == "elec" else bt_n_heavy_in_tile.shape[1]
-        s.T = 0 if term == "elec" else type_params.shape[0]
+        s.ntiles = 0 if term in ("elec", "lkball") else bt_n_heavy_in_tile.shape[1]
+        s.T = 0 if term in ("elec", "lkball") else type_params.shape[0]
         self.s = s
         self.P, self.B, self.N = s.P, s.B, s.n_atoms
+        if term == "lkball":
+            self.k = self._lkb_struct(lkb_tables, lkb_water_args, i32, rl, real_t)
+
+    def _lkb_struct(self, tables, wg, i32, rl, real_t):
+        irc, t_npol, t_nocc, t_polocc, t_params, lkb_global = tables
+        (_irc, _nat, _nconn, _catom, _n_all, all_bonds, ranges, t_ndonH, t_nacc, t_donH, t_donH_hvy, t_which,
+         t_acc, t_hyb, t_nH, is_h, wg_gp, tors_sp2, tors_sp3, tors_ring) = wg[12:32]
+        P = ctypes.POINTER
+        i32p = P(ctypes.c_int32)
+        rp = P(real_t)
+
+        class LKB(ctypes.Structure):
+            _fields_ = (
+                [("irc", i32p), ("all_bonds", i32p), ("bond_ranges", i32p), ("NB", ctypes.c_int), ("NT", ctypes.c_int)]
+                + [(n, i32p) for n in ("tile_n_donH", "tile_n_acc", "tile_donH_inds", "tile_donH_hvy",
+                                       "tile_which_donH", "tile_acc_inds", "tile_acc_hyb", "tile_acc_nH",
+                                       "is_hydrogen", "tile_n_polar", "tile_n_occ", "tile_pol_occ")]
+                + [("tile_params", rp)]
+                + [(n, real_t) for n in ("water_dist", "ang_sp2", "ang_sp3", "ang_ring")]
+                + [("tors_sp2", rp), ("tors_sp3", rp), ("tors_ring", rp)]
+                + [(n, ctypes.c_int) for n in ("n_sp2", "n_sp3", "n_ring")]
+                + [(n, real_t) for n in ("hbond_dis", "hbond_OH_donor_dis", "hbond_hdis", "max_dis")]
+            )
+
+        k = LKB()
+        k.irc = i32(irc)
+        k.all_bonds = i32(all_bonds)
+        k.bond_ranges = i32(ranges)
+        k.NB = all_bonds.shape[1]
+        k.NT = t_npol.shape[1]
+        for name, t in (("tile_n_donH", t_ndonH), ("tile_n_acc", t_nacc), ("tile_donH_inds", t_donH),
+                        ("tile_donH_hvy", t_donH_hvy), ("tile_which_donH", t_which), ("tile_acc_inds", t_acc),
+                        ("tile_acc_hyb", t_hyb), ("tile_acc_nH", t_nH), ("is_hydrogen", is_h),
+                        ("tile_n_polar", t_npol), ("tile_n_occ", t_nocc), ("tile_pol_occ", t_polocc)):
+            setattr(k, name, i32(t))
+        k.tile_params = rl(t_params)
+        g = wg_gp.detach().cpu().reshape(-1).to(torch.float64).numpy()
+        k.water_dist, k.ang_sp2, k.ang_sp3, k.ang_ring = (float(v) for v in g[:4])
+        k.tors_sp2, k.tors_sp3, k.tors_ring = rl(tors_sp2), rl(tors_sp3), rl(tors_ring)
+        k.n_sp2, k.n_sp3, k.n_ring = tors_sp2.numel(), tors_sp3.numel(), tors_ring.numel()
+        sg = lkb_global.detach().cpu().reshape(-1).to(torch.float64).numpy()
+        k.hbond_dis, k.hbond_OH_donor_dis, k.hbond_hdis, k.max_dis = float(sg[0]), float(sg[1]), float(sg[2]), float(sg[4])
+        return k
+
+    def lkb_waters(self):
+        """gen_pose_waters: [N, 4, 3] (NaN where no water)."""
+        W = numpy.empty((self.N, 4, 3), dtype=self.np_real)
+        rc = _lib(self.f64).oracle_lkb_waters(ctypes.byref(self.s), ctypes.byref(self.k), self._ptr(W))
+        assert rc == 0
+        return W
+
+    def lkb_scores(self, W, weights=None):
+        """(E [4, P], d(sum weights * E)/dcoords [N, 3] or None, neighbours)."""
+        E = numpy.zeros((4, self.P), dtype=self.np_real)
+        nbr = numpy.zeros((self.P, self.B, self.B), dtype=numpy.int32)
+        W = numpy.ascontiguousarray(W, dtype=self.np_real)
+        dx = None
+        wp = ctypes.c_void_p(0)
+        if weights is not None:
+            w = numpy.ascontiguousarray(numpy.asarray(weights, dtype=self.np_real).reshape(4, self.P))
+            self.keep.append(w)
+            wp = self._ptr(w)
+            dx = numpy.zeros((self.N, 3), dtype=self.np_real)
+        rc = _lib(self.f64).oracle_lkb_pose_scores(
+            ctypes.byref(self.s), ctypes.byref(self.k), self._ptr(W), self._ptr(E), wp,
+            self._ptr(dx) if dx is not None else ctypes.c_void_p(0), self._ptr(nbr),
+        )
+        assert rc == 0
+        return E, dx, nbr
 
     def _ptr(self, a):
         return a.ctypes.data_as(ctypes.c_void_p)
@@ -350,6 +434,32 @@ def reference_elec_rotamer_scores(coords, args, require_gradient=True):
         c.requires_grad_(True)
     E, idx = op(c, *cpu_args)
     return E, c, idx
+
+
+LKBALL_REF_LIB = os.path.join(HERE, "_ref", "lk_ball", "tmol_lk_ball_ref.so")
+
+
+def reference_lkball_available():
+    return os.path.exists(LKBALL_REF_LIB)
+
+
+def reference_lkball(coords, water_args, score_args, require_gradient=True):
+    """The reference CPU LK-ball ops: waters from gen_pose_waters, then
+    lk_ball_pose_score on them; returns (E [4, P], waters, coords tensor with
+    grad of sum(E) when requested, block neighbours)."""
+    if "lkball_ref" not in _LIBS:
+        torch.ops.load_library(LKBALL_REF_LIB)
+        _LIBS["lkball_ref"] = True
+    ops = torch.ops.tmol_lk_ball
+    c = coords.detach().cpu().reshape(-1, 3).clone()
+    if require_gradient:
+        c.requires_grad_(True)
+    wa = [a.cpu() if isinstance(a, torch.Tensor) else a for a in water_args]
+    sa = [a.cpu() if isinstance(a, torch.Tensor) else a for a in score_args]
+    W = ops.gen_pose_waters(c, *wa)
+    sa[-2] = W
+    E, nbr = ops.lk_ball_pose_score(c, *sa)
+    return E, W, c, nbr
 
 
 def reference_pose_scores(coords, args, require_gradient=True):

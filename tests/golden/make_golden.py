@@ -25,6 +25,13 @@ Writes
                      reference elec rotamer op (elec_rotamer_scores) on the
                      rotamer set of rotamers.npz (energies, indices, the
                      gradient of sum(w * E) for seeded w)
+  lkball.npz         the reference LK-ball ops (gen_pose_waters, then
+                     lk_ball_pose_score) on 1ubq and on a seeded synthetic
+                     pose, float32 and float64: waters, the four energies,
+                     the gradient of their sum; plus the reference test
+                     suite's stored 1ubq LK-ball energies
+                     (tmol/tests/data/term_baselines/LKBallEnergyTerm/
+                     test_whole_pose_scoring_10.yaml)
   rotamers.npz       the reference rotamer-score op (ljlk_rotamer_scores) on
                      a seeded rotamer set over a jagged batch of poses: the
                      set itself, the rotamer-pair energies and dispatch
@@ -52,11 +59,13 @@ from tmol_b200.score.elec_energy_term import (  # noqa: E402
     elec_rotamer_score_args,
 )
 from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm, pose_score_args, rotamer_score_args  # noqa: E402
+from tmol_b200.score.lkball_energy_term import LKBallEnergyTerm, score_args, water_gen_args  # noqa: E402
 
 SYN_SIZES = [1, 2, 7, 33, 100]
 SYN_SEEDS = [11, 12, 13, 14, 15]
 ELEC_SIZES = [40, 3, 17, 120]
 ELEC_SEEDS = [31, 32, 33, 34]
+LKB_SYN = ([60], [44], 20.0)  # sizes, seeds, extra chi sd
 ROT_SIZES = [12, 30, 1, 45]
 ROT_SEEDS = [21, 22, 23, 24]
 ROT_SET = dict(max_rots=4, mutate_fraction=0.25, seed=5, skip_fraction=0.1)
@@ -130,6 +139,33 @@ def main(ref_root):
             f"{tag}_neighbors": nbr.numpy(),
             f"{tag}_block_pair": Eb.detach().numpy(),
         })
+    lterm = LKBallEnergyTerm()
+    with open(
+        os.path.join(ref_root, "tmol/tests/data/term_baselines/LKBallEnergyTerm/test_whole_pose_scoring_10.yaml")
+    ) as f:
+        lgold = yaml.safe_load(f)
+    lout = {"ubq_tmol_test_energies": numpy.array([lgold[f"term{t}"]["pose0"] for t in range(4)], numpy.float64)}
+    lsyn = synthetic_pose_stack(LKB_SYN[0], LKB_SYN[1], extra_chi_sd=LKB_SYN[2])
+    for tag, lps in (("ubq", build_pose_stack([topo], [xyz])), ("syn", lsyn)):
+        for dt, dn in ((torch.float32, "f32"), (torch.float64, "f64")):
+            wa = water_gen_args(lps, lterm)
+            sa = score_args(lps, lterm, None)
+            if dt == torch.float64:
+                wa = [a.to(dt) if isinstance(a, torch.Tensor) and a.is_floating_point() else a for a in wa]
+                sa = [a.to(dt) if isinstance(a, torch.Tensor) and a.is_floating_point() else a for a in sa]
+            E, W, c, _ = O.reference_lkball(lps.coords.flatten(0, 1).to(dt), wa, sa)
+            E.sum().backward()
+            lout[f"{tag}_{dn}_energies"] = E.detach().numpy()
+            lout[f"{tag}_{dn}_waters"] = W.detach().numpy()
+            lout[f"{tag}_{dn}_grad"] = c.grad.numpy()
+    numpy.savez_compressed(
+        os.path.join(HERE, "lkball.npz"),
+        syn_sizes=numpy.array(LKB_SYN[0]),
+        syn_seeds=numpy.array(LKB_SYN[1]),
+        syn_chi_sd=numpy.array(LKB_SYN[2]),
+        **lout,
+    )
+
     ps = synthetic_pose_stack(ROT_SIZES, ROT_SEEDS)
     rs = synthetic_rotamer_set(ps, **ROT_SET)
     E, c, idx = O.reference_elec_rotamer_scores(rs.coords, elec_rotamer_score_args(ps, rs, eterm))
