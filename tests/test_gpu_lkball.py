@@ -1,0 +1,190 @@
+"""GPU parity of the LK-ball term (tmol's gen_pose_waters and
+lk_ball_pose_score) through the C ABI.
+
+- against the reference ops' outputs committed in tests/golden/lkball.npz
+  (1ubq and a synthetic pose, float32 and float64): waters, the four
+  energies (1e-5 relative / 1e-3 kcal/mol in float32) and the gradient
+  through the waters (1e-4 of its largest component);
+- against the C oracle on seeded multi-pose batches, float64 to 1e-9;
+- block-pair energies (upper triangle, summing to the whole-pose ones) and
+  their adjoint; float64 gradcheck of both ops;
+- plan kinds: a water plan and a score plan serve their own entry points.
+"""
+
+import numpy
+import pytest
+import torch
+
+from oracle import oracle as O
+from tests.conftest import load_golden
+from tmol_b200 import native
+from tmol_b200.pose.synthetic import synthetic_pose_stack
+from tmol_b200.score.lkball_energy_term import LKBallEnergyTerm, score_args, water_gen_args
+from tmol_b200.score.lkball_op import LKBallPlan, gen_pose_waters, lk_ball_pose_score
+
+pytestmark = pytest.mark.gpu
+DEV = torch.device("cuda:0")
+
+
+@pytest.fixture(scope="module")
+def lterm():
+    return LKBallEnergyTerm()
+
+
+def to_dev(args, dtype):
+    out = []
+    for a in args:
+        if isinstance(a, torch.Tensor):
+            a = a.to(DEV)
+            if a.is_floating_point():
+                a = a.to(dtype)
+        out.append(a)
+    return out
+
+
+def static_args(ps, lterm, dtype):
+    wa = to_dev(water_gen_args(ps, lterm), dtype)
+    sa = to_dev(score_args(ps, lterm, None)[:-2], dtype)
+    return wa, sa
+
+
+def gpu_run(ps, lterm, dtype, block_pair=False):
+    """(waters, energies, d(sum E)/dcoords through the waters, neighbours)"""
+    wa, sa = static_args(ps, lterm, dtype)
+    coords = ps.coords.flatten(0, 1).to(DEV, dtype).requires_grad_(True)
+    W = gen_pose_waters(coords, *wa)
+    E, nbr = lk_ball_pose_score(coords, *sa, W, block_pair)
+    E.sum().backward()
+    return W.detach(), E.detach(), coords.grad, nbr
+
+
+def oracle_run(ps, lterm, f64):
+    dt = torch.float64 if f64 else torch.float32
+    oc = O.OracleCall(ps.coords.flatten(0, 1).to(dt), score_args(ps, lterm, None), f64=f64, term="lkball",
+                      lkb_water_args=water_gen_args(ps, lterm))
+    W = oc.lkb_waters()
+    E, dx, nbr = oc.lkb_scores(W, weights=numpy.ones((4, ps.n_poses)))
+    return W, E, dx, nbr
+
+
+def E_close(E, ref, rtol=1e-5, atol=1e-3):
+    numpy.testing.assert_allclose(E, ref, rtol=rtol, atol=atol)
+
+
+def g_close(g, ref, rtol=1e-4):
+    numpy.testing.assert_allclose(g, ref, rtol=rtol, atol=rtol * numpy.abs(ref).max())
+
+
+def W_close(W, ref, atol):
+    assert numpy.array_equal(numpy.isnan(W), numpy.isnan(ref))
+    numpy.testing.assert_allclose(W[~numpy.isnan(W)], ref[~numpy.isnan(ref)], rtol=0, atol=atol)
+
+
+def fixture_cases(ubq_pose_stack):
+    g = load_golden("lkball.npz")
+    syn = synthetic_pose_stack(list(g["syn_sizes"]), list(g["syn_seeds"]), extra_chi_sd=float(g["syn_chi_sd"]))
+    return g, [("ubq", ubq_pose_stack), ("syn", syn)]
+
+
+@pytest.mark.parametrize("f64", [False, True])
+def test_matches_reference_fixture(ubq_pose_stack, lterm, f64):
+    g, cases = fixture_cases(ubq_pose_stack)
+    dn = "f64" if f64 else "f32"
+    for tag, ps in cases:
+        W, E, dx, _ = gpu_run(ps, lterm, torch.float64 if f64 else torch.float32)
+        W_close(W.cpu().numpy(), g[f"{tag}_{dn}_waters"], 1e-9 if f64 else 1e-4)
+        if f64:
+            E_close(E.cpu().numpy(), g[f"{tag}_{dn}_energies"], rtol=1e-10, atol=1e-10)
+            g_close(dx.cpu().numpy(), g[f"{tag}_{dn}_grad"], rtol=1e-9)
+        else:
+            E_close(E.cpu().numpy(), g[f"{tag}_{dn}_energies"])
+            g_close(dx.cpu().numpy(), g[f"{tag}_{dn}_grad"])
+
+
+def test_ubq_reproduces_stored_energies(ubq_pose_stack, lterm):
+    g = load_golden("lkball.npz")
+    _, E, _, _ = gpu_run(ubq_pose_stack, lterm, torch.float32)
+    E_close(E[:, 0].cpu().numpy(), g["ubq_tmol_test_energies"])
+
+
+@pytest.mark.parametrize("f64", [False, True])
+def test_batches_match_oracle(lterm, f64):
+    dt = torch.float64 if f64 else torch.float32
+    for sizes, seeds in (([40, 3, 75, 1, 22], [5, 6, 7, 8, 9]), ([120, 64], [11, 12])):
+        ps = synthetic_pose_stack(sizes, seeds, extra_chi_sd=25.0)
+        W, E, dx, nbr = gpu_run(ps, lterm, dt)
+        Wo, Eo, dxo, nbro = oracle_run(ps, lterm, f64)
+        assert numpy.array_equal(nbr.cpu().numpy(), nbro)
+        if f64:
+            W_close(W.cpu().numpy(), Wo, 1e-9)
+            E_close(E.cpu().numpy(), Eo, rtol=1e-9, atol=1e-9)
+            g_close(dx.cpu().numpy(), dxo, rtol=1e-9)
+        else:
+            W_close(W.cpu().numpy(), Wo, 1e-4)
+            E_close(E.cpu().numpy(), Eo)
+            g_close(dx.cpu().numpy(), dxo)
+
+
+def test_block_pair_energies_and_adjoint(lterm):
+    ps = synthetic_pose_stack([50, 17, 33], [21, 22, 23], extra_chi_sd=20.0)
+    dt = torch.float64
+    wa, sa = static_args(ps, lterm, dt)
+    coords = ps.coords.flatten(0, 1).to(DEV, dt)
+    plan = LKBallPlan(coords, water_static=wa, score_static=sa)
+    W = plan.waters(coords)
+    E, nbr = plan.forward(coords, W)
+    Ebp, nbr2 = plan.forward(coords, W, block_pair=True)
+    assert torch.equal(nbr, nbr2)
+    E_close(Ebp.sum(dim=(2, 3)).cpu().numpy(), E.cpu().numpy(), rtol=1e-12, atol=1e-12)
+    B = ps.max_n_blocks
+    lower = torch.tril(torch.ones(B, B, dtype=torch.bool, device=DEV), diagonal=-1)
+    assert not Ebp[:, :, lower].any()
+    # block-pair weights that are constant per pose give the whole-pose adjoint
+    w = torch.rand(4, ps.n_poses, device=DEV, dtype=dt)
+    dx0, dw0 = plan.backward(coords, W, w)
+    dx1, dw1 = plan.backward(coords, W, w[:, :, None, None].expand(4, ps.n_poses, B, B), block_pair=True)
+    numpy.testing.assert_allclose(dx1.cpu().numpy(), dx0.cpu().numpy(), rtol=1e-10, atol=1e-10)
+    numpy.testing.assert_allclose(dw1.cpu().numpy(), dw0.cpu().numpy(), rtol=1e-10, atol=1e-10)
+
+
+def test_gradcheck(lterm):
+    ps = synthetic_pose_stack([9, 6], [31, 32], extra_chi_sd=30.0)
+    wa, sa = static_args(ps, lterm, torch.float64)
+    coords = ps.coords.flatten(0, 1).to(DEV, torch.float64).requires_grad_(True)
+
+    def whole(c):
+        return lk_ball_pose_score(c, *sa, gen_pose_waters(c, *wa), False)[0]
+
+    def pairs(c):
+        return lk_ball_pose_score(c, *sa, gen_pose_waters(c, *wa), True)[0]
+
+    assert torch.autograd.gradcheck(whole, (coords,), eps=1e-6, atol=1e-6, nondet_tol=1e-10)
+    assert torch.autograd.gradcheck(pairs, (coords,), eps=1e-6, atol=1e-6, nondet_tol=1e-10)
+
+
+def test_plan_parts(ubq_pose_stack, lterm):
+    wa, sa = static_args(ubq_pose_stack, lterm, torch.float32)
+    coords = ubq_pose_stack.coords.flatten(0, 1).to(DEV)
+    water_plan = LKBallPlan(coords, water_static=wa)
+    score_plan = LKBallPlan(coords, score_static=sa)
+    W = water_plan.waters(coords)
+    with pytest.raises(native.NativeError):
+        water_plan.forward(coords, W)
+    with pytest.raises(native.NativeError):
+        score_plan.waters(coords)
+    E, _ = score_plan.forward(coords, W)
+    both = LKBallPlan(coords, water_static=wa, score_static=sa)
+    E2, _ = both.forward(coords, both.waters(coords))
+    E_close(E2.cpu().numpy(), E.cpu().numpy(), rtol=1e-6, atol=1e-6)
+    # an LK-ball plan is not an LJ/LK plan
+    with pytest.raises(native.NativeError):
+        native.call("tmol_b200_ljlk_forward", both.ptr, coords.data_ptr(), 0, E.data_ptr(), None, None)
+
+
+def test_short_poses_with_padding(lterm):
+    ps = synthetic_pose_stack([1, 4], [41, 42])
+    W, E, dx, nbr = gpu_run(ps, lterm, torch.float64)
+    Wo, Eo, dxo, nbro = oracle_run(ps, lterm, True)
+    W_close(W.cpu().numpy(), Wo, 1e-9)
+    E_close(E.cpu().numpy(), Eo, rtol=1e-9, atol=1e-9)
+    assert numpy.array_equal(nbr.cpu().numpy(), nbro)

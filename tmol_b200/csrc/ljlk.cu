@@ -38,6 +38,7 @@
 
 #include "../../include/tmol_b200_elec.h"
 #include "../../include/tmol_b200_ljlk.h"
+#include "../../include/tmol_b200_lkball.h"
 #include "../../include/tmol_b200_pose.h"
 #include "../../include/tmol_b200_screen.h"
 #include "bondsep.cuh"
@@ -56,9 +57,11 @@ constexpr int MAX_WARPS = 8;
 // elec (fa_elec).  Both share the neighbour detection, count-pair tables,
 // staging and screening; they differ in the per-atom record (atom type and
 // heavy flag, or partial charge) and the pair potential.
-enum TermKind : int { kTermLJLK = 0, kTermElec = 1 };
+enum TermKind : int { kTermLJLK = 0, kTermElec = 1, kTermLKBall = 2 };
 
-__host__ __device__ constexpr int n_terms(int term) { return term == kTermElec ? 1 : 3; }
+__host__ __device__ constexpr int n_terms(int term) {
+  return term == kTermElec ? 1 : (term == kTermLKBall ? 4 : 3);
+}
 
 enum StatusBits : int {
   kStIndex = 1,
@@ -1709,6 +1712,8 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
     atomicAdd(&s.counts[lane], w.counts[lane]);
 }
 
+#include "lkball.cuh"
+
 // Sub-spheres of every block for the screen's features: atoms [0, 4) (the
 // backbone N, CA, C, O of an amino acid) and atoms [4, n) (the rest; the
 // first part again when n <= 4), each as centroid + largest centroid
@@ -1869,6 +1874,16 @@ struct tmol_b200_ljlk_plan {
   void* bt_q = nullptr;    // elec: partial charges [nbt * A] reals
   void* elec_k = nullptr;  // elec: ElecK constants [N_ELEC_K] reals
   unsigned char elec_k_host[N_ELEC_K * sizeof(double)];
+  // LK-ball plans: water sites [N * 4], per block type polar / occluder
+  // atom lists and per-atom parameters [nbt * A * 9] reals
+  void* lkb_sites = nullptr;
+  int* lkb_pol = nullptr;
+  int* lkb_npol = nullptr;
+  int* lkb_occ = nullptr;
+  int* lkb_nocc = nullptr;
+  int lkb_maxpol = 0, lkb_maxocc = 0;
+  void* lkb_par = nullptr;
+  double lkb_water_dist = 0;
   tmol_b200_ljlk_inputs dims;  // sizes only; pointers are not kept
   int P, B, nbt, A, C, ntiles, T;
   int64_t N;
@@ -1957,7 +1972,8 @@ void free_plan(tmol_b200_ljlk_plan* pl) {
                   pl->counters,  pl->counts,     pl->sub_spheres, pl->rot_bt,
                   pl->rot_off,   pl->rot_block,  pl->rot_pose,    pl->nrb,
                   pl->rob,       pl->rot_spheres, pl->row_pairs,  pl->row_items,
-                  pl->bt_q,      pl->elec_k};
+                  pl->bt_q,      pl->elec_k,      pl->lkb_sites,   pl->lkb_pol,
+                  pl->lkb_npol,  pl->lkb_occ,     pl->lkb_nocc,    pl->lkb_par};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t e : pl->prof_events) cudaEventDestroy(e);
@@ -2045,6 +2061,13 @@ ScoreArgs<Real> score_args(tmol_b200_ljlk_plan* pl, const void* coords) {
     s.g.max_dis = gp[4];
     s.bt_q = (const Real*)pl->bt_q;
     s.elec_k = (const Real*)pl->elec_k;
+  } else if (pl->term == kTermLKBall) {
+    // LK-ball global parameters: hbond, OH-donor, H distances, water
+    // distance, max_dis
+    s.g.max_dis = gp[4];
+    s.g.lj_hbond_dis = gp[0];
+    s.g.lj_hbond_OH_donor_dis = gp[1];
+    s.g.lj_hbond_hdis = gp[2];
   } else {
     s.g.max_dis = gp[0];
     s.g.lj_dlin_sigma_factor = gp[1];
@@ -2237,6 +2260,88 @@ int rotamer_score_impl(tmol_b200_ljlk_plan* pl, const void* coords, const int32_
   return TMOL_B200_OK;
 }
 
+template <typename Real>
+LkbArgs<Real> lkb_args(tmol_b200_ljlk_plan* pl) {
+  LkbArgs<Real> k = {};
+  k.sites = (const LkbSite<Real>*)pl->lkb_sites;
+  k.n_sites = pl->N * LKB_NW;
+  k.pol = pl->lkb_pol;
+  k.npol = pl->lkb_npol;
+  k.occ = pl->lkb_occ;
+  k.nocc = pl->lkb_nocc;
+  k.maxpol = pl->lkb_maxpol;
+  k.maxocc = pl->lkb_maxocc;
+  k.par = (const Real*)pl->lkb_par;
+  const Real* gp = (const Real*)pl->global_params;
+  k.hbond_dis = gp[0];
+  k.hbond_oh = gp[1];
+  k.hbond_h = gp[2];
+  k.water_dist = (Real)pl->lkb_water_dist;
+  k.max_dis = gp[4];
+  return k;
+}
+
+template <typename Real>
+int lkb_waters_impl(tmol_b200_ljlk_plan* pl, const void* coords, void* waters, cudaStream_t st) {
+  LkbArgs<Real> k = lkb_args<Real>(pl);
+  k.waters_out = (Real*)waters;
+  if (k.n_sites == 0) return TMOL_B200_OK;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((k.n_sites + 255) / 256, (int64_t)pl->n_sm * 16));
+  lkb_waters_kernel<Real><<<grid, 256, 0, st>>>(k, (const Real*)coords);
+  CK(cudaGetLastError());
+  return TMOL_B200_OK;
+}
+
+template <typename Real>
+int lkb_waters_backward_impl(tmol_b200_ljlk_plan* pl, const void* coords, const void* dwaters, void* dcoords,
+                             cudaStream_t st) {
+  LkbArgs<Real> k = lkb_args<Real>(pl);
+  k.dwaters = (const Real*)dwaters;
+  if (k.n_sites == 0) return TMOL_B200_OK;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((k.n_sites + 255) / 256, (int64_t)pl->n_sm * 16));
+  lkb_waters_backward_kernel<Real><<<grid, 256, 0, st>>>(k, (const Real*)coords, (Real*)dcoords);
+  CK(cudaGetLastError());
+  return TMOL_B200_OK;
+}
+
+template <typename Real, bool GRAD, bool BLOCK_PAIR>
+int lkb_score_impl(tmol_b200_ljlk_plan* pl, const void* coords, const void* waters, void* energies, int32_t* nbr,
+                   const void* dTdV, void* dcoords, void* dwaters, cudaStream_t st) {
+  ScoreArgs<Real> s = score_args<Real>(pl, coords);
+  LkbArgs<Real> k = lkb_args<Real>(pl);
+  k.water_dist = ((const Real*)pl->global_params)[3];  // the score op's own copy
+  k.waters = (const Real*)waters;
+  k.dwaters_out = (Real*)dwaters;
+  s.energies = (Real*)energies;
+  s.nbr = nbr;
+  s.dTdV = (const Real*)dTdV;
+  s.dcoords = (Real*)dcoords;
+  const size_t PBB = (size_t)pl->P * pl->B * pl->B;
+  if (energies) CK(cudaMemsetAsync(energies, 0, (BLOCK_PAIR ? PBB : (size_t)pl->P) * 4 * sizeof(Real), st));
+  if (nbr) CK(cudaMemsetAsync(nbr, 0, PBB * sizeof(int32_t), st));
+  if (dcoords) CK(cudaMemsetAsync(dcoords, 0, (size_t)pl->N * 3 * sizeof(Real), st));
+  if (dwaters) CK(cudaMemsetAsync(dwaters, 0, (size_t)pl->N * LKB_NW * 3 * sizeof(Real), st));
+  const int n_blocks = pl->P * pl->B;
+  const int grid_s = std::max(1, std::min((n_blocks + 7) / 8, pl->n_sm * 16));
+  spheres_kernel<Real><<<grid_s, 256, 0, st>>>(s);
+  CK(cudaGetLastError());
+  CK(cudaMemsetAsync(pl->counters, 0, sizeof(int), st));
+  if (pl->n_work == 0) return TMOL_B200_OK;
+  const int warps = pl->launch.warps_per_cta;
+  const int R = pl->launch.rows_per_item;
+  const int n_tickets = (pl->n_work + R - 1) / R;
+  const int grid = std::max(1, std::min((n_tickets + warps - 1) / warps, pl->n_sm * pl->launch.ctas_per_sm));
+  const bool prof = pl->profiling && 2 * (size_t)pl->prof_n + 1 < pl->prof_events.size();
+  if (prof) CK(cudaEventRecord(pl->prof_events[2 * pl->prof_n], st));
+  lkb_score_kernel<Real, GRAD, BLOCK_PAIR><<<grid, 32 * warps, 0, st>>>(s, k, R);
+  CK(cudaGetLastError());
+  if (prof) {
+    CK(cudaEventRecord(pl->prof_events[2 * pl->prof_n + 1], st));
+    ++pl->prof_n;
+  }
+  return TMOL_B200_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -2265,12 +2370,118 @@ struct ElecExtra {
   const int32_t* inter_repr_pd;    // [nbt, A, A]
 };
 
+// LK-ball plan tables: each block type's polar and occluder atoms (the
+// reference's per-tile lists, lk_ball_pose_score.impl.hh:560-640, flattened
+// to one list per block type), their nine parameters per atom, and every
+// water site of the PoseStack (lkb_sites_kernel).
+template <typename Real>
+int build_lkball(tmol_b200_ljlk_plan* pl, const tmol_b200_lkball_inputs* k, const std::vector<int>& h_nat,
+                 cudaStream_t st) {
+  const int nbt = pl->nbt, A = pl->A, NT = k->max_n_tiles;
+  const bool waters = k->bt_all_bonds != nullptr, scoring = k->bt_tile_pol_occ_inds != nullptr;
+  const size_t ntile = scoring ? (size_t)nbt * NT : 0;
+  std::vector<int> npol(ntile), nocc(ntile), inds(ntile * TILE);
+  std::vector<Real> tpar(ntile * TILE * LKB_NPAR);
+  Real wg[4] = {0, 0, 0, 0};
+  if (ntile > 0) {
+    CK(cudaMemcpyAsync(npol.data(), k->bt_tile_n_polar_atoms, sizeof(int) * ntile, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(nocc.data(), k->bt_tile_n_occluder_atoms, sizeof(int) * ntile, cudaMemcpyDeviceToHost,
+                       st));
+    CK(cudaMemcpyAsync(inds.data(), k->bt_tile_pol_occ_inds, sizeof(int) * ntile * TILE, cudaMemcpyDeviceToHost,
+                       st));
+    CK(cudaMemcpyAsync(tpar.data(), k->bt_tile_lk_ball_params, sizeof(Real) * tpar.size(),
+                       cudaMemcpyDeviceToHost, st));
+  }
+  if (waters && k->water_gen_global_params)
+    CK(cudaMemcpyAsync(wg, k->water_gen_global_params, sizeof(wg), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  std::vector<std::vector<int>> pol(nbt), occ(nbt);
+  std::vector<Real> par((size_t)std::max(nbt * A, 1) * LKB_NPAR, Real(0));
+  for (int bt = 0; scoring && bt < nbt; ++bt)
+    for (int t = 0; t < NT; ++t) {
+      const size_t tb = (size_t)bt * NT + t;
+      if (npol[tb] < 0 || nocc[tb] < npol[tb] || nocc[tb] > TILE) return TMOL_B200_ERR_INDEX_RANGE;
+      for (int q = 0; q < nocc[tb]; ++q) {
+        const int i = inds[tb * TILE + q];
+        const int a = t * TILE + i;
+        if (i < 0 || i >= TILE || a >= h_nat[bt] || a >= A) return TMOL_B200_ERR_INDEX_RANGE;
+        if (q < npol[tb]) pol[bt].push_back(a);
+        occ[bt].push_back(a);
+        std::copy_n(&tpar[(tb * TILE + q) * LKB_NPAR], LKB_NPAR, &par[((size_t)bt * A + a) * LKB_NPAR]);
+      }
+    }
+  int maxpol = 1, maxocc = 1;
+  for (int bt = 0; bt < nbt; ++bt) {
+    maxpol = std::max(maxpol, (int)pol[bt].size());
+    maxocc = std::max(maxocc, (int)occ[bt].size());
+  }
+  std::vector<int> hpol((size_t)std::max(nbt, 1) * maxpol, 0), hocc((size_t)std::max(nbt, 1) * maxocc, 0);
+  std::vector<int> hnpol(std::max(nbt, 1), 0), hnocc(std::max(nbt, 1), 0);
+  for (int bt = 0; bt < nbt; ++bt) {
+    hnpol[bt] = (int)pol[bt].size();
+    hnocc[bt] = (int)occ[bt].size();
+    std::copy(pol[bt].begin(), pol[bt].end(), &hpol[(size_t)bt * maxpol]);
+    std::copy(occ[bt].begin(), occ[bt].end(), &hocc[(size_t)bt * maxocc]);
+  }
+  pl->lkb_maxpol = maxpol;
+  pl->lkb_maxocc = maxocc;
+  pl->lkb_water_dist = (double)wg[0];
+  if (scoring) {
+    CK(dalloc(pl, &pl->lkb_pol, hpol.size()));
+    CK(dalloc(pl, &pl->lkb_occ, hocc.size()));
+    CK(dalloc(pl, &pl->lkb_npol, hnpol.size()));
+    CK(dalloc(pl, &pl->lkb_nocc, hnocc.size()));
+    CK(dalloc(pl, (Real**)&pl->lkb_par, par.size()));
+    CK(cudaMemcpyAsync(pl->lkb_pol, hpol.data(), sizeof(int) * hpol.size(), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(pl->lkb_occ, hocc.data(), sizeof(int) * hocc.size(), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(pl->lkb_npol, hnpol.data(), sizeof(int) * hnpol.size(), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(pl->lkb_nocc, hnocc.data(), sizeof(int) * hnocc.size(), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(pl->lkb_par, par.data(), sizeof(Real) * par.size(), cudaMemcpyHostToDevice, st));
+  }
+  if (!waters) return TMOL_B200_OK;
+  const int64_t n_sites = pl->N * LKB_NW;
+  CK(dalloc(pl, (LkbSite<Real>**)&pl->lkb_sites, (size_t)n_sites));
+  CK(cudaMemsetAsync(pl->lkb_sites, 0, sizeof(LkbSite<Real>) * std::max<int64_t>(n_sites, 1), st));
+  const int64_t PB = (int64_t)pl->P * pl->B;
+  if (PB > 0 && nbt > 0) {
+    LkbTables t;
+    t.irc = k->inter_residue_connections;
+    t.all_bonds = k->bt_all_bonds;
+    t.ranges = k->bt_atom_all_bond_ranges;
+    t.NB = k->max_n_all_bonds;
+    t.NT = NT;
+    t.tile_n_donH = k->bt_tile_n_donH;
+    t.tile_n_acc = k->bt_tile_n_acc;
+    t.tile_donH = k->bt_tile_donH_inds;
+    t.tile_donH_hvy = k->bt_tile_donH_hvy_inds;
+    t.tile_which = k->bt_tile_which_donH_for_hvy;
+    t.tile_acc = k->bt_tile_acc_inds;
+    t.tile_hyb = k->bt_tile_hybridization;
+    t.tile_nH = k->bt_tile_acc_n_attached_H;
+    t.is_h = k->bt_atom_is_hydrogen;
+    t.bt_conn_atom = k->bt_conn_atom;
+    const int g = std::max(1, std::min<int>((int)((PB + 127) / 128), pl->n_sm * 8));
+    lkb_sites_kernel<Real><<<g, 128, 0, st>>>(
+        pl->blk_bt, pl->blk_off, pl->bt_n_atoms, pl->P, pl->B, pl->C, A, t, (const Real*)k->sp2_water_tors,
+        k->n_sp2_tors, (const Real*)k->sp3_water_tors, k->n_sp3_tors, (const Real*)k->ring_water_tors,
+        k->n_ring_tors, wg[1], wg[2], wg[3], (LkbSite<Real>*)pl->lkb_sites, pl->counters + 1);
+    CK(cudaGetLastError());
+  }
+  return TMOL_B200_OK;
+}
+
 int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
                 const tmol_b200_ljlk_launch* launch, void* stream, bool rotamers,
                 tmol_b200_ljlk_plan** plan_out, const ElecExtra* elec = nullptr,
-                const tmol_b200_pose_connectivity* conn = nullptr) {
+                const tmol_b200_pose_connectivity* conn = nullptr,
+                const tmol_b200_lkball_inputs* lkb = nullptr) {
   if (!in || !plan_out) return TMOL_B200_ERR_INVALID_ARGUMENT;
-  const int term = elec ? kTermElec : kTermLJLK;
+  const int term = elec ? kTermElec : (lkb ? kTermLKBall : kTermLJLK);
+  // an LK-ball plan serves water generation (its bond and hbond tables
+  // given), scoring (its polar / occluder tables given), or both
+  const bool lkb_waters = lkb && lkb->bt_all_bonds;
+  const bool scoring = !lkb || lkb->bt_tile_pol_occ_inds;
+  if (lkb && !lkb_waters && !scoring) return TMOL_B200_ERR_INVALID_ARGUMENT;
   *plan_out = nullptr;
   if (real_bytes != 4 && real_bytes != 8) return TMOL_B200_ERR_DTYPE;
   const int P = in->n_poses, B = in->max_n_blocks, nbt = in->n_block_types;
@@ -2291,7 +2502,7 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
   if (conn && (conn->n_poses != P || conn->max_n_blocks != B || conn->n_block_types != nbt ||
                conn->max_n_conn != C))
     return TMOL_B200_ERR_SHAPE;
-  if (P * B > 0) {
+  if (P * B > 0 && scoring) {
     if (conn) {
       for (const void* r : conn_req)
         if (!r) return TMOL_B200_ERR_INVALID_ARGUMENT;
@@ -2302,8 +2513,29 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
   }
   const void* req[] = {in->rot_coord_offset, in->first_rot_block_type, in->block_ind_for_rot,
                        in->pose_ind_for_rot, in->block_type_ind_for_rot, in->rot_offset_for_block,
-                       in->bt_n_atoms, in->bt_n_conn, in->bt_conn_atom, in->bt_path_distance,
-                       in->bt_is_ligand_fragment, in->global_params};
+                       in->bt_n_atoms, in->bt_n_conn, in->bt_conn_atom,
+                       scoring ? in->bt_path_distance : in->bt_n_atoms,
+                       lkb ? in->bt_n_atoms : in->bt_is_ligand_fragment,
+                       scoring ? in->global_params : in->bt_n_atoms};
+  if (lkb && lkb->max_n_tiles * TILE < A) return TMOL_B200_ERR_SHAPE;
+  if (lkb_waters && P * B > 0 && nbt > 0) {
+    const void* lreq[] = {lkb->inter_residue_connections, lkb->bt_atom_all_bond_ranges, lkb->bt_tile_n_donH,
+                          lkb->bt_tile_n_acc, lkb->bt_tile_donH_inds, lkb->bt_tile_donH_hvy_inds,
+                          lkb->bt_tile_which_donH_for_hvy, lkb->bt_tile_acc_inds, lkb->bt_tile_hybridization,
+                          lkb->bt_tile_acc_n_attached_H, lkb->bt_atom_is_hydrogen, lkb->water_gen_global_params};
+    for (const void* r : lreq)
+      if (!r) return TMOL_B200_ERR_INVALID_ARGUMENT;
+    if (lkb->max_n_all_bonds < 0 || lkb->n_sp2_tors < 0 || lkb->n_sp3_tors < 0 || lkb->n_ring_tors < 0)
+      return TMOL_B200_ERR_SHAPE;
+    if ((lkb->n_sp2_tors && !lkb->sp2_water_tors) || (lkb->n_sp3_tors && !lkb->sp3_water_tors) ||
+        (lkb->n_ring_tors && !lkb->ring_water_tors))
+      return TMOL_B200_ERR_INVALID_ARGUMENT;
+  }
+  if (lkb && scoring && nbt > 0) {
+    const void* lreq[] = {lkb->bt_tile_n_polar_atoms, lkb->bt_tile_n_occluder_atoms, lkb->bt_tile_lk_ball_params};
+    for (const void* r : lreq)
+      if (!r) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  }
   const void* req_ljlk[] = {in->bt_n_heavy_atoms_in_tile, in->bt_heavy_atoms_in_tile, in->bt_atom_types,
                             in->type_params};
   const void* req_elec[] = {elec ? elec->partial_charge : nullptr, elec ? elec->inter_repr_pd : nullptr};
@@ -2313,12 +2545,12 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
     if (term == kTermLJLK) {
       for (const void* r : req_ljlk)
         if (!r) return TMOL_B200_ERR_INVALID_ARGUMENT;
-    } else {
+    } else if (term == kTermElec) {
       for (const void* r : req_elec)
         if (!r) return TMOL_B200_ERR_INVALID_ARGUMENT;
     }
   }
-  if (!in->global_params) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  if (scoring && !in->global_params) return TMOL_B200_ERR_INVALID_ARGUMENT;
 
   cudaStream_t st = (cudaStream_t)stream;
   auto* pl = new tmol_b200_ljlk_plan();
@@ -2381,10 +2613,14 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
   PCK(cudaMemsetAsync(pl->bt_flags, 0, sizeof(int) * std::max<int64_t>((int64_t)nbt * A, 1), st));
   PCK(cudaMemcpyAsync(pl->bt_n_atoms, in->bt_n_atoms, sizeof(int) * nbt, cudaMemcpyDeviceToDevice, st));
   PCK(cudaMemcpyAsync(pl->bt_n_conn, in->bt_n_conn, sizeof(int) * nbt, cudaMemcpyDeviceToDevice, st));
-  PCK(cudaMemcpyAsync(pl->bt_is_ligand, in->bt_is_ligand_fragment, sizeof(int) * nbt,
-                      cudaMemcpyDeviceToDevice, st));
-  PCK(cudaMemcpyAsync(pl->global_params, in->global_params, 5 * real_bytes,
-                      cudaMemcpyDeviceToHost, st));
+  if (term == kTermLKBall)
+    // LK-ball's inter-block count pair has no ligand rule
+    PCK(cudaMemsetAsync(pl->bt_is_ligand, 0, sizeof(int) * std::max(nbt, 1), st));
+  else
+    PCK(cudaMemcpyAsync(pl->bt_is_ligand, in->bt_is_ligand_fragment, sizeof(int) * nbt,
+                        cudaMemcpyDeviceToDevice, st));
+  if (scoring)
+    PCK(cudaMemcpyAsync(pl->global_params, in->global_params, 5 * real_bytes, cudaMemcpyDeviceToHost, st));
 
   PlanBuildArgs a;
   a.in = *in;
@@ -2442,7 +2678,9 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
     plan_heavy_kernel<<<gh, 256, 0, st>>>(a);
     PCK(cudaGetLastError());
   }
-  if (PB > 0 && conn) {
+  if (PB > 0 && !scoring) {
+    // water generation only: no count-pair tables
+  } else if (PB > 0 && conn) {
     int gc = std::max(1, std::min<int>((int)((PB + 127) / 128), pl->n_sm * 16));
     plan_count_pair_conn_kernel<<<gc, 128, 0, st>>>(a);
     PCK(cudaGetLastError());
@@ -2500,7 +2738,7 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
   if (pl->ntp > 0)
     PCK(cudaMemcpyAsync(pl->compact_types, compact.data(), sizeof(int) * pl->ntp,
                         cudaMemcpyHostToDevice, st));
-  if (nbt > 0) {
+  if (nbt > 0 && scoring) {
     int gb = std::max(1, std::min(((nbt * A) + 255) / 256, pl->n_sm * 8));
     plan_block_types_kernel<<<gb, 256, 0, st>>>(a, pl->type_map, pl->bt_tf);
     PCK(cudaGetLastError());
@@ -2523,6 +2761,13 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
     PCK(cudaMemcpyAsync(pl->elec_k, pl->elec_k_host, (size_t)N_ELEC_K * real_bytes, cudaMemcpyHostToDevice,
                         st));
   }
+  if (term == kTermLKBall) {
+    rc = real_bytes == 4 ? build_lkball<float>(pl, lkb, h_nat, st) : build_lkball<double>(pl, lkb, h_nat, st);
+    if (rc != TMOL_B200_OK) {
+      free_plan(pl);
+      return rc;
+    }
+  }
   if (pl->ntp > 0) {
     int gt = std::max(1, std::min((int)((ntp2 + 127) / 128), pl->n_sm * 8));
     if (real_bytes == 4)
@@ -2542,7 +2787,7 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
     free_plan(pl);
     return rc;
   }
-  rc = rotamers ? TMOL_B200_OK : build_work(pl, st);
+  rc = (rotamers || !scoring) ? TMOL_B200_OK : build_work(pl, st);
   if (rc != TMOL_B200_OK) {
     free_plan(pl);
     return rc;
@@ -2586,6 +2831,42 @@ tmol_b200_ljlk_inputs shared_inputs(const tmol_b200_elec_inputs* e) {
   in.global_params = e->global_params;
   in.max_dis = e->max_dis;
   return in;
+}
+
+int create_lkball_plan(const tmol_b200_lkball_inputs* k, int real_bytes, const tmol_b200_ljlk_launch* launch,
+                       void* stream, tmol_b200_ljlk_plan** plan_out) {
+  if (!k || !plan_out) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  tmol_b200_ljlk_inputs in = {};
+  in.n_atoms = k->n_atoms;
+  in.n_poses = k->n_poses;
+  in.max_n_blocks = k->max_n_blocks;
+  in.n_rots = k->n_rots;
+  in.n_block_types = k->n_block_types;
+  in.max_n_block_atoms = k->max_n_block_atoms;
+  in.max_n_conn = k->max_n_conn;
+  in.max_n_tiles = k->max_n_tiles;
+  in.n_atom_types = 0;
+  in.rot_coord_offset = k->rot_coord_offset;
+  in.pose_ind_for_atom = k->pose_ind_for_atom;
+  in.first_rot_for_block = k->first_rot_for_block;
+  in.first_rot_block_type = k->first_rot_block_type;
+  in.block_ind_for_rot = k->block_ind_for_rot;
+  in.pose_ind_for_rot = k->pose_ind_for_rot;
+  in.block_type_ind_for_rot = k->block_type_ind_for_rot;
+  in.n_rots_for_pose = k->n_rots_for_pose;
+  in.rot_offset_for_pose = k->rot_offset_for_pose;
+  in.n_rots_for_block = k->n_rots_for_block;
+  in.rot_offset_for_block = k->rot_offset_for_block;
+  in.max_n_rots_per_pose = k->max_n_rots_per_pose;
+  in.min_bondsep = k->min_bondsep;
+  in.inter_block_bondsep = k->inter_block_bondsep;
+  in.bt_n_atoms = k->bt_n_atoms;
+  in.bt_n_conn = k->bt_n_conn;
+  in.bt_conn_atom = k->bt_conn_atom;
+  in.bt_path_distance = k->bt_path_distance;
+  in.global_params = k->global_params;
+  in.max_dis = k->max_dis;
+  return create_plan(&in, real_bytes, launch, stream, false, plan_out, nullptr, nullptr, k);
 }
 
 int create_elec_plan(const tmol_b200_elec_inputs* e, int real_bytes, const tmol_b200_ljlk_launch* launch,
@@ -2954,6 +3235,70 @@ int tmol_b200_elec_rotamer_backward(tmol_b200_elec_plan* plan, const void* coord
                                     const int32_t* items, int64_t n_items, int64_t n_pairs,
                                     const void* dTdV, void* dcoords, void* stream) {
   return rotamer_backward(plan, kTermElec, coords, items, n_items, n_pairs, dTdV, dcoords, stream);
+}
+
+// LK-ball entry points (include/tmol_b200_lkball.h)
+
+int tmol_b200_lkball_plan_create(const tmol_b200_lkball_inputs* inputs, int real_bytes,
+                                 const tmol_b200_ljlk_launch* launch, void* stream,
+                                 tmol_b200_lkball_plan** plan_out) {
+  return create_lkball_plan(inputs, real_bytes, launch, stream, plan_out);
+}
+
+int tmol_b200_lkball_plan_destroy(tmol_b200_lkball_plan* plan) {
+  if (!plan || plan->term != kTermLKBall) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  free_plan(plan);
+  return TMOL_B200_OK;
+}
+
+int tmol_b200_lkball_waters(tmol_b200_lkball_plan* plan, const void* coords, void* waters, void* stream) {
+  if (!plan || plan->term != kTermLKBall || !plan->lkb_sites) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  if (plan->N > 0 && (!coords || !waters)) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  return plan->real_bytes == 4 ? lkb_waters_impl<float>(plan, coords, waters, st)
+                               : lkb_waters_impl<double>(plan, coords, waters, st);
+}
+
+int tmol_b200_lkball_waters_backward(tmol_b200_lkball_plan* plan, const void* coords, const void* dwaters,
+                                     void* dcoords, void* stream) {
+  if (!plan || plan->term != kTermLKBall || !plan->lkb_sites) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  if (plan->N > 0 && (!coords || !dwaters || !dcoords)) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  return plan->real_bytes == 4 ? lkb_waters_backward_impl<float>(plan, coords, dwaters, dcoords, st)
+                               : lkb_waters_backward_impl<double>(plan, coords, dwaters, dcoords, st);
+}
+
+int tmol_b200_lkball_forward(tmol_b200_lkball_plan* plan, const void* coords, const void* waters,
+                             int block_pair, void* energies, int32_t* block_neighbors, void* stream) {
+  if (!plan || plan->term != kTermLKBall || !plan->lkb_pol || !energies) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  if (plan->N > 0 && (!coords || !waters)) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->real_bytes == 4)
+    return block_pair ? lkb_score_impl<float, false, true>(plan, coords, waters, energies, block_neighbors,
+                                                           nullptr, nullptr, nullptr, st)
+                      : lkb_score_impl<float, false, false>(plan, coords, waters, energies, block_neighbors,
+                                                            nullptr, nullptr, nullptr, st);
+  return block_pair ? lkb_score_impl<double, false, true>(plan, coords, waters, energies, block_neighbors,
+                                                          nullptr, nullptr, nullptr, st)
+                    : lkb_score_impl<double, false, false>(plan, coords, waters, energies, block_neighbors,
+                                                           nullptr, nullptr, nullptr, st);
+}
+
+int tmol_b200_lkball_backward(tmol_b200_lkball_plan* plan, const void* coords, const void* waters,
+                              int block_pair, const void* dTdV, void* dcoords, void* dwaters,
+                              void* stream) {
+  if (!plan || plan->term != kTermLKBall || !plan->lkb_pol || !dTdV) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  if (plan->N > 0 && (!coords || !waters || !dcoords || !dwaters)) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->real_bytes == 4)
+    return block_pair ? lkb_score_impl<float, true, true>(plan, coords, waters, nullptr, nullptr, dTdV, dcoords,
+                                                          dwaters, st)
+                      : lkb_score_impl<float, true, false>(plan, coords, waters, nullptr, nullptr, dTdV, dcoords,
+                                                           dwaters, st);
+  return block_pair ? lkb_score_impl<double, true, true>(plan, coords, waters, nullptr, nullptr, dTdV, dcoords,
+                                                         dwaters, st)
+                    : lkb_score_impl<double, true, false>(plan, coords, waters, nullptr, nullptr, dTdV, dcoords,
+                                                          dwaters, st);
 }
 
 int64_t tmol_b200_ljlk_plan_device_bytes(const tmol_b200_ljlk_plan* plan) {

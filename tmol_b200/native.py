@@ -1,6 +1,6 @@
 """ctypes binding of the C ABI in ``include/tmol_b200_ljlk.h``,
-``include/tmol_b200_elec.h``, ``include/tmol_b200_pose.h`` and
-``include/tmol_b200_screen.h``.
+``include/tmol_b200_elec.h``, ``include/tmol_b200_lkball.h``,
+``include/tmol_b200_pose.h`` and ``include/tmol_b200_screen.h``.
 
 The shared library is built in-tree (``tmol_b200/lib``) by
 ``tmol_b200.build``.  There is no fallback: importing this module without the
@@ -93,6 +93,32 @@ class ElecInputs(ctypes.Structure):
         ("global_params", ctypes.c_void_p),
         ("max_dis", ctypes.c_double),
     ]
+
+
+class LKBallInputs(ctypes.Structure):
+    """``tmol_b200_lkball_inputs``."""
+
+    _fields_ = (
+        [("n_atoms", ctypes.c_int64)]
+        + [(n, ctypes.c_int32) for n in ("n_poses", "max_n_blocks", "n_rots", "n_block_types", "max_n_block_atoms",
+                                         "max_n_conn", "max_n_tiles", "max_n_all_bonds")]
+        + [(n, ctypes.c_void_p) for n in (
+            "rot_coord_offset", "pose_ind_for_atom", "first_rot_for_block", "first_rot_block_type",
+            "block_ind_for_rot", "pose_ind_for_rot", "block_type_ind_for_rot", "n_rots_for_pose",
+            "rot_offset_for_pose", "n_rots_for_block", "rot_offset_for_block")]
+        + [("max_n_rots_per_pose", ctypes.c_int32)]
+        + [(n, ctypes.c_void_p) for n in (
+            "inter_residue_connections", "min_bondsep", "inter_block_bondsep", "bt_n_atoms", "bt_n_conn",
+            "bt_conn_atom", "bt_n_all_bonds", "bt_all_bonds", "bt_atom_all_bond_ranges", "bt_tile_n_donH",
+            "bt_tile_n_acc", "bt_tile_donH_inds", "bt_tile_donH_hvy_inds", "bt_tile_which_donH_for_hvy",
+            "bt_tile_acc_inds", "bt_tile_hybridization", "bt_tile_acc_n_attached_H", "bt_atom_is_hydrogen",
+            "water_gen_global_params", "sp2_water_tors", "sp3_water_tors", "ring_water_tors")]
+        + [(n, ctypes.c_int32) for n in ("n_sp2_tors", "n_sp3_tors", "n_ring_tors")]
+        + [(n, ctypes.c_void_p) for n in (
+            "bt_tile_n_polar_atoms", "bt_tile_n_occluder_atoms", "bt_tile_pol_occ_inds", "bt_tile_lk_ball_params",
+            "bt_path_distance", "global_params")]
+        + [("max_dis", ctypes.c_double)]
+    )
 
 
 class PoseConnectivity(ctypes.Structure):
@@ -209,6 +235,16 @@ SIGNATURES = {
     "tmol_b200_elec_rotamer_fill": (ctypes.c_int, [_V, _V, _V, _V]),
     "tmol_b200_elec_rotamer_forward": (ctypes.c_int, [_V, _V, _V, _I64, _I64, _V, _V]),
     "tmol_b200_elec_rotamer_backward": (ctypes.c_int, [_V, _V, _V, _I64, _I64, _V, _V, _V]),
+    # LK-ball (include/tmol_b200_lkball.h)
+    "tmol_b200_lkball_plan_create": (
+        ctypes.c_int,
+        [ctypes.POINTER(LKBallInputs), ctypes.c_int, ctypes.POINTER(Launch), _V, ctypes.POINTER(ctypes.c_void_p)],
+    ),
+    "tmol_b200_lkball_plan_destroy": (ctypes.c_int, [_V]),
+    "tmol_b200_lkball_waters": (ctypes.c_int, [_V, _V, _V, _V]),
+    "tmol_b200_lkball_waters_backward": (ctypes.c_int, [_V, _V, _V, _V, _V]),
+    "tmol_b200_lkball_forward": (ctypes.c_int, [_V, _V, _V, ctypes.c_int, _V, _V, _V]),
+    "tmol_b200_lkball_backward": (ctypes.c_int, [_V, _V, _V, ctypes.c_int, _V, _V, _V, _V]),
     # PoseStack construction (include/tmol_b200_pose.h)
     "tmol_b200_pose_bondsep": (ctypes.c_int, [ctypes.POINTER(PoseConnectivity), _V, _V, _V, _V]),
     "tmol_b200_apsp_stacked": (ctypes.c_int, [_V, _I32, _I32, _I32, _V]),

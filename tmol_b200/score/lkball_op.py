@@ -1,0 +1,280 @@
+"""The LK-ball ops on B200, with tmol's argument lists and outputs.
+
+``gen_pose_waters(coords, <32 static arguments>)`` takes exactly the
+arguments of ``torch.ops.tmol_lk_ball.gen_pose_waters``
+(``tmol/score/lk_ball/potentials/compiled.ops.cpp:25-64``) and returns the
+waters ``[n_atoms, 4, 3]`` (NaN in unused slots); gradients flow back to
+``coords`` through the water-building adjoint.
+
+``lk_ball_pose_score(coords, <25 static arguments>, water_coords,
+output_block_pair_energies)`` is ``torch.ops.tmol_lk_ball.lk_ball_pose_score``
+(``compiled.ops.cpp:370-600, 843-907``): ``(scores, block_neighbors)``,
+scores ``[4, P]`` (lk_ball_iso, lk_ball, lk_bridge, lk_bridge_uncpl) or
+``[4, P, B, B]``; gradients flow to ``coords`` and ``water_coords``.
+
+Each op builds its plan (include/tmol_b200_lkball.h) once per set of static
+tensors and caches it as the LJ/LK op's is.  All tensors must be on one CUDA
+device; there is no CPU path.
+"""
+
+import ctypes
+
+import torch
+
+from .. import native
+from .ljlk_op import LJLKPlan, get_plan
+
+N_WATER_STATIC = 32  # gen_pose_waters' arguments after coords
+N_SCORE_STATIC = 27  # lk_ball_pose_score's after coords (water_coords and the output-mode flag included)
+MAX_N_WATER = 4
+
+
+class LKBallPlan(LJLKPlan):
+    """Owns one ``tmol_b200_lkball_plan``.  ``water_static`` (gen_pose_waters'
+    32 arguments after coords) enables water generation, ``score_static``
+    (lk_ball_pose_score's first 25 arguments after coords) scoring; either
+    may be None."""
+
+    N_TERMS = 4  # lk_ball_iso, lk_ball, lk_bridge, lk_bridge_uncpl
+    ABI = "tmol_b200_lkball"
+    NAME = "LK-ball"
+
+    def __init__(self, coords_like, water_static=None, score_static=None, launch=None):
+        if water_static is None and score_static is None:
+            raise ValueError("an LK-ball plan needs the water-generation or the scoring arguments")
+        device = self._set_device(coords_like)
+        s = native.LKBallInputs()
+        keep = []
+
+        def put(name, t, real=False):
+            if not isinstance(t, torch.Tensor):
+                raise TypeError(f"{name} must be a tensor")
+            if t.device != device:
+                raise RuntimeError(f"{name} is on {t.device}, coordinates on {device}")
+            t = t.to(self.dtype if real else torch.int32).contiguous()
+            keep.append(t)
+            setattr(s, name, t.data_ptr())
+            return t
+
+        common = water_static[:12] if water_static is not None else score_static[:12]
+        names = ("rot_coord_offset", "pose_ind_for_atom", "first_rot_for_block", "first_rot_block_type",
+                 "block_ind_for_rot", "pose_ind_for_rot", "block_type_ind_for_rot", "n_rots_for_pose",
+                 "rot_offset_for_pose", "n_rots_for_block", "rot_offset_for_block")
+        for name, t in zip(names, common[:11]):
+            put(name, t)
+        s.max_n_rots_per_pose = int(common[11])
+        P, B = common[2].shape
+        if water_static is not None:
+            if len(water_static) != N_WATER_STATIC:
+                raise TypeError(f"gen_pose_waters takes coords + {N_WATER_STATIC} arguments")
+            (irc, bt_n_atoms, bt_n_conn, bt_conn_atom, bt_n_all_bonds, all_bonds, ranges, t_ndonH, t_nacc,
+             t_donH, t_donH_hvy, t_which, t_acc, t_hyb, t_nH, is_h, wg_gp, tors_sp2, tors_sp3,
+             tors_ring) = water_static[12:]
+            for name, t in (("inter_residue_connections", irc), ("bt_n_all_bonds", bt_n_all_bonds),
+                            ("bt_all_bonds", all_bonds), ("bt_atom_all_bond_ranges", ranges),
+                            ("bt_tile_n_donH", t_ndonH), ("bt_tile_n_acc", t_nacc), ("bt_tile_donH_inds", t_donH),
+                            ("bt_tile_donH_hvy_inds", t_donH_hvy), ("bt_tile_which_donH_for_hvy", t_which),
+                            ("bt_tile_acc_inds", t_acc), ("bt_tile_hybridization", t_hyb),
+                            ("bt_tile_acc_n_attached_H", t_nH), ("bt_atom_is_hydrogen", is_h)):
+                put(name, t)
+            if wg_gp.numel() != 4:
+                raise ValueError("the water-generation global parameters must hold 4 values")
+            put("water_gen_global_params", wg_gp, real=True)
+            for name, t in (("sp2", tors_sp2), ("sp3", tors_sp3), ("ring", tors_ring)):
+                if t.numel():
+                    put(f"{name}_water_tors", t.reshape(-1), real=True)
+                setattr(s, f"n_{name}_tors", t.numel())
+            s.max_n_all_bonds = all_bonds.shape[1]
+            s.max_n_tiles = t_ndonH.shape[1]
+            A = is_h.shape[1]
+        if score_static is not None:
+            if len(score_static) != N_SCORE_STATIC - 2:
+                raise TypeError(f"lk_ball_pose_score takes coords + {N_SCORE_STATIC} arguments")
+            (irc, min_bondsep, ibb, bt_n_atoms, bt_n_conn, bt_conn_atom, t_npol, t_nocc, t_polocc, t_params,
+             path_distance, gp, max_dis) = score_static[12:]
+            for name, t in (("inter_residue_connections", irc), ("min_bondsep", min_bondsep),
+                            ("inter_block_bondsep", ibb), ("bt_tile_n_polar_atoms", t_npol),
+                            ("bt_tile_n_occluder_atoms", t_nocc), ("bt_tile_pol_occ_inds", t_polocc),
+                            ("bt_path_distance", path_distance)):
+                put(name, t)
+            C = bt_conn_atom.shape[1]
+            if tuple(ibb.shape) != (P, B, B, C, C) or tuple(min_bondsep.shape) != (P, B, B):
+                raise ValueError("bond separation tensors do not match the PoseStack's shape")
+            if t_params.shape[-1] != 9:
+                raise ValueError("LK-ball atom parameters must be [n_block_types, n_tiles, 32, 9]")
+            if gp.numel() != 5:
+                raise ValueError("the scoring global parameters must hold 5 values")
+            put("bt_tile_lk_ball_params", t_params, real=True)
+            put("global_params", gp, real=True)
+            s.max_dis = float(max_dis)
+            s.max_n_tiles = t_npol.shape[1]
+            A = path_distance.shape[1]
+        put("bt_n_atoms", bt_n_atoms)
+        put("bt_n_conn", bt_n_conn)
+        put("bt_conn_atom", bt_conn_atom)
+        s.n_poses = P
+        s.max_n_blocks = B
+        s.n_rots = common[0].shape[0]
+        s.n_block_types = bt_n_atoms.shape[0]
+        s.max_n_block_atoms = A
+        s.max_n_conn = bt_conn_atom.shape[1]
+        self.n_poses, self.max_n_blocks = P, B
+        self.n_atoms = common[1].shape[0]
+        s.n_atoms = self.n_atoms
+        self.launch = native.Launch(*(launch or (0, 0, 0, 0)))
+        self.rotamers = False
+        ptr = ctypes.c_void_p()
+        real_bytes = 4 if self.dtype == torch.float32 else 8
+        with torch.cuda.device(self.device):
+            native.call(
+                "tmol_b200_lkball_plan_create", ctypes.byref(s), real_bytes, ctypes.byref(self.launch),
+                self._stream(), ctypes.byref(ptr),
+            )
+        self.ptr = ptr
+        del keep
+
+    def waters(self, coords, out=None):
+        """Waters [n_atoms, 4, 3] at ``coords``."""
+        self._check_coords(coords)
+        coords = coords.contiguous()
+        if out is None:
+            out = torch.empty((self.n_atoms, MAX_N_WATER, 3), dtype=self.dtype, device=self.device)
+        native.call("tmol_b200_lkball_waters", self.ptr, ctypes.c_void_p(coords.data_ptr()),
+                    ctypes.c_void_p(out.data_ptr()), self._stream())
+        return out
+
+    def waters_backward(self, coords, dwaters, dcoords=None):
+        """dcoords (+)= the adjoint of dL/dwaters (zeros first when
+        ``dcoords`` is None)."""
+        self._check_coords(coords)
+        coords = coords.contiguous()
+        dwaters = dwaters.to(self.dtype).contiguous()
+        if dcoords is None:
+            dcoords = torch.zeros_like(coords)
+        native.call("tmol_b200_lkball_waters_backward", self.ptr, ctypes.c_void_p(coords.data_ptr()),
+                    ctypes.c_void_p(dwaters.data_ptr()), ctypes.c_void_p(dcoords.data_ptr()), self._stream())
+        return dcoords
+
+    def _check_waters(self, waters):
+        if waters.device != self.device or waters.dtype != self.dtype:
+            raise RuntimeError("waters do not match the plan's device and dtype")
+        if tuple(waters.shape) != (self.n_atoms, MAX_N_WATER, 3):
+            raise ValueError(f"waters must be [{self.n_atoms}, {MAX_N_WATER}, 3], got {tuple(waters.shape)}")
+
+    def forward(self, coords, waters, block_pair=False, want_neighbors=True, energies=None):
+        self._check_coords(coords)
+        self._check_waters(waters)
+        coords, waters = coords.contiguous(), waters.contiguous()
+        P, B = self.n_poses, self.max_n_blocks
+        shape = (self.N_TERMS, P, B, B) if block_pair else (self.N_TERMS, P)
+        if energies is None:
+            energies = torch.empty(shape, dtype=self.dtype, device=self.device)
+        nbr = torch.empty((P, B, B), dtype=torch.int32, device=self.device) if want_neighbors else None
+        native.call(
+            "tmol_b200_lkball_forward", self.ptr, ctypes.c_void_p(coords.data_ptr()),
+            ctypes.c_void_p(waters.data_ptr()), int(block_pair), ctypes.c_void_p(energies.data_ptr()),
+            ctypes.c_void_p(nbr.data_ptr() if nbr is not None else 0), self._stream(),
+        )
+        return energies, nbr
+
+    def backward(self, coords, waters, dTdV, block_pair=False, dcoords=None, dwaters=None):
+        """(dL/dcoords directly, dL/dwaters) from dL/dE."""
+        self._check_coords(coords)
+        self._check_waters(waters)
+        coords, waters = coords.contiguous(), waters.contiguous()
+        dTdV = dTdV.to(self.dtype).contiguous()
+        if dcoords is None:
+            dcoords = torch.empty_like(coords)
+        if dwaters is None:
+            dwaters = torch.empty_like(waters)
+        native.call(
+            "tmol_b200_lkball_backward", self.ptr, ctypes.c_void_p(coords.data_ptr()),
+            ctypes.c_void_p(waters.data_ptr()), int(block_pair), ctypes.c_void_p(dTdV.data_ptr()),
+            ctypes.c_void_p(dcoords.data_ptr()), ctypes.c_void_p(dwaters.data_ptr()), self._stream(),
+        )
+        return dcoords, dwaters
+
+    def energy_and_gradient(self, *a, **k):
+        raise NotImplementedError("LK-ball scoring runs forward, then backward")
+
+    def last_counts(self):
+        raise NotImplementedError("LK-ball scoring keeps no work counters")
+
+    def set_skip_mask(self, mask):
+        raise NotImplementedError("the learned block-pair screen serves LJ/LK plans")
+
+    def screen_candidates(self, coords, capacity, out=None):
+        raise NotImplementedError("the learned block-pair screen serves LJ/LK plans")
+
+    def rotamer_dispatch(self, coords):
+        raise NotImplementedError("LK-ball rotamer scoring is not built")
+
+
+class LKBallWaterPlan(LKBallPlan):
+    def __init__(self, coords_like, static_args, launch=None, rotamers=False):
+        if rotamers:
+            raise ValueError("water plans have no rotamer mode")
+        super().__init__(coords_like, water_static=static_args, launch=launch)
+
+
+class LKBallScorePlan(LKBallPlan):
+    def __init__(self, coords_like, static_args, launch=None, rotamers=False):
+        if rotamers:
+            raise NotImplementedError("LK-ball rotamer scoring is not built")
+        super().__init__(coords_like, score_static=static_args, launch=launch)
+
+
+class _WaterFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, coords, plan):
+        ctx.plan = plan
+        ctx.save_for_backward(coords)
+        return plan.waters(coords)
+
+    @staticmethod
+    def backward(ctx, dW):
+        (coords,) = ctx.saved_tensors
+        if dW is None:
+            return None, None
+        return ctx.plan.waters_backward(coords, dW), None
+
+
+class _LKBallScoreFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, coords, waters, plan, block_pair, want_neighbors):
+        E, nbr = plan.forward(coords, waters, block_pair, want_neighbors)
+        ctx.plan = plan
+        ctx.block_pair = block_pair
+        ctx.save_for_backward(coords, waters)
+        if nbr is None:
+            nbr = torch.empty((0,), dtype=torch.int32, device=coords.device)
+        ctx.mark_non_differentiable(nbr)
+        return E, nbr
+
+    @staticmethod
+    def backward(ctx, dE, _dnbr):
+        coords, waters = ctx.saved_tensors
+        if dE is None:
+            return None, None, None, None, None
+        dx, dw = ctx.plan.backward(coords, waters, dE, ctx.block_pair)
+        return dx, dw, None, None, None
+
+
+def gen_pose_waters(coords, *args):
+    """Drop-in for ``torch.ops.tmol_lk_ball.gen_pose_waters``."""
+    if len(args) != N_WATER_STATIC:
+        raise TypeError(f"gen_pose_waters takes coords + {N_WATER_STATIC} arguments, got {1 + len(args)}")
+    flat = coords.reshape(-1, 3)
+    plan = get_plan(flat, args, plan_class=LKBallWaterPlan)
+    return _WaterFn.apply(flat, plan)
+
+
+def lk_ball_pose_score(coords, *args, return_block_neighbors=True):
+    """Drop-in for ``torch.ops.tmol_lk_ball.lk_ball_pose_score``."""
+    if len(args) != N_SCORE_STATIC:
+        raise TypeError(f"lk_ball_pose_score takes coords + {N_SCORE_STATIC} arguments, got {1 + len(args)}")
+    static, waters, block_pair = args[:-2], args[-2], bool(args[-1])
+    flat = coords.reshape(-1, 3)
+    plan = get_plan(flat, static, plan_class=LKBallScorePlan)
+    E, nbr = _LKBallScoreFn.apply(flat, waters, plan, block_pair, return_block_neighbors)
+    return E, (nbr if return_block_neighbors else None)
