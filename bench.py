@@ -57,6 +57,7 @@ ROT_RES = 150
 ROT_SET = dict(max_rots=31, mutate_fraction=0.25, seed=9)
 ROT_METRIC = "LJ+LK rotamer-pair energies/s (16 poses x 150 residues, 1-31 rotamers per block, 1 B200)"
 ELEC_METRIC = "elec energy+grad poses/s (64x150-residue batch, 1 B200)"
+LKBALL_METRIC = "LK-ball energy+grad poses/s (64x150-residue batch, waters included, 1 B200)"
 BONDSEP_METRIC = "inter-block bond separation poses/s (256-pose uneven batch, dense [P,B,B,C,C] + min, 1 B200)"
 
 # Algorithmic FLOPs per unit (E + dE), counted on the restatement's most
@@ -69,6 +70,17 @@ F_LK = 111  # each heavy-atom pair among those (both LK directions)
 # distance and unit vector 12, eps 14, deps 10, E 4, dE 8, weights 2,
 # energy sum 1, gradient on both atoms 9, charge product 1
 F_ELEC = 61
+# LK-ball, energy and gradient in one pass (counted on the restatement,
+# the isotropic term on its 2-4.5 A branch): each polar / occluder pair in
+# reach (bond separation > 3, inside max_dis, polar atom with waters):
+# distance 9, sigma 1, isotropic LK and its derivative 38, desolvation
+# fraction over 4 waters with its adjoint 139, combination and adjoint onto
+# both atoms and the polar waters 64, energy sums 4.
+F_LKB_PAIR = 255
+# ...and when the occluder is a donor or acceptor, the water-bridge term
+# over 4 x 4 water pairs with its adjoint onto both atoms' waters (481) and
+# its share of the combination (180)
+F_LKB_BRIDGE = 661
 
 
 def workload_sizes(name, rank):
@@ -76,7 +88,7 @@ def workload_sizes(name, rank):
 
     from tmol_b200.pose.synthetic import log_uniform_sizes
 
-    if name in ("uniform64x150", "elec64x150"):
+    if name in ("uniform64x150", "elec64x150", "lkball64x150"):
         return [N_RES] * N_POSES, [rank * N_POSES + k for k in range(N_POSES)]
     rng = numpy.random.default_rng(UNEVEN_SEED + 1000 * rank)
     sizes = log_uniform_sizes(rng, UNEVEN_POSES, 20, 1000)
@@ -105,6 +117,11 @@ def rotamer_workload(rank, device, sizes=None, seeds=None):
 def workload_label(name):
     if name == "elec64x150":
         return f"{N_POSES} poses x {N_RES} residues, fa_elec energy + gradient"
+    if name == "lkball64x150":
+        return (
+            f"{N_POSES} poses x {N_RES} residues, lk_ball_iso + lk_ball + lk_bridge + lk_bridge_uncpl "
+            "energies + gradient through the waters"
+        )
     if name == "uniform64x150":
         return f"{N_POSES} poses x {N_RES} residues, energy + gradient, weights {list(TERM_WEIGHTS)}"
     return (
@@ -252,10 +269,10 @@ def cpu_reference_sample(ps, term, reps=3):
     return kind, best
 
 
-def _ref_worker(conn, sizes, seeds, elec=False):
+def _ref_worker(conn, sizes, seeds, term="ljlk"):
     """One single-threaded process of the reference arm: builds its share of
     the poses (same sizes and seeds as the GPU arm) and scores it on demand
-    (LJ/LK, or elec with `elec`)."""
+    (`term`: "ljlk", "elec" or "lkball")."""
     import torch
 
     torch.set_num_threads(1)
@@ -264,7 +281,30 @@ def _ref_worker(conn, sizes, seeds, elec=False):
 
     ps = synthetic_pose_stack(sizes, seeds)
     coords = ps.coords.flatten(0, 1).clone()
-    if elec:
+    if term == "lkball":
+        import numpy
+
+        from tmol_b200.score.lkball_energy_term import LKBallEnergyTerm, score_args, water_gen_args
+
+        lt = LKBallEnergyTerm()
+        wa, sa = water_gen_args(ps, lt), score_args(ps, lt, None)
+        ref = O.reference_lkball_available()
+        oc = None if ref else O.OracleCall(coords, sa, term="lkball", lkb_water_args=wa)
+        ones = numpy.ones((4, ps.n_poses))
+        conn.send("ready")
+        while True:
+            msg = conn.recv()
+            if msg is None:
+                break
+            t0 = time.perf_counter()
+            if ref:
+                E, _, c, _ = O.reference_lkball(coords, wa, sa)
+                E.sum().backward()
+            else:
+                oc.lkb_scores(oc.lkb_waters(), weights=ones)
+            conn.send(time.perf_counter() - t0)
+        return
+    if term == "elec":
         from tmol_b200.score.elec_energy_term import ElecEnergyTerm, elec_pose_score_args
 
         args = elec_pose_score_args(ps, ElecEnergyTerm())
@@ -334,6 +374,8 @@ def run_reference(args, world, rank):
     if args.workload == "bondsep256":
         return run_reference_bondsep(args)
     elec = args.workload == "elec64x150"
+    lkball = args.workload == "lkball64x150"
+    term = "elec" if elec else ("lkball" if lkball else "ljlk")
     sizes, seeds = workload_sizes(args.workload, 0)
     n_poses = len(sizes)
     n_proc = min(os.cpu_count() or 1, n_poses)
@@ -349,7 +391,7 @@ def run_reference(args, world, rank):
         parent, child = ctx.Pipe()
         pr = ctx.Process(
             target=_ref_worker,
-            args=(child, [sizes[k] for k in share], [seeds[k] for k in share], elec),
+            args=(child, [sizes[k] for k in share], [seeds[k] for k in share], term),
         )
         pr.start()
         workers.append((pr, parent))
@@ -374,11 +416,13 @@ def run_reference(args, world, rank):
     value = n_poses * args.steps / t
     if elec:
         kind = "reference" if O.reference_elec_available() else "port"
+    elif lkball:
+        kind = "reference" if O.reference_lkball_available() else "port"
     else:
         kind = "reference" if O.reference_available() else "port"
     line = {
         "impl": "reference",
-        "metric": ELEC_METRIC if elec else METRIC,
+        "metric": ELEC_METRIC if elec else (LKBALL_METRIC if lkball else METRIC),
         "value": value,
         "unit": "poses/s",
         "n_gpus": args.gpus,
@@ -1007,6 +1051,272 @@ def run_elec(args, world, rank, local):
     return 0
 
 
+def lkball_plan_for(ps, coords):
+    """An LK-ball plan of the batch (both parts: waters and scoring)."""
+    import torch
+
+    from tmol_b200.score.lkball_energy_term import LKBallEnergyTerm, score_args, water_gen_args
+    from tmol_b200.score.lkball_op import LKBallPlan
+
+    dev, dt = coords.device, coords.dtype
+    lt = LKBallEnergyTerm()
+
+    def on(args):
+        out = []
+        for a in args:
+            if isinstance(a, torch.Tensor):
+                a = a.to(dev)
+                if a.is_floating_point():
+                    a = a.to(dt)
+            out.append(a)
+        return out
+
+    return LKBallPlan(coords, water_static=on(water_gen_args(ps, lt)), score_static=on(score_args(ps, lt, None)[:-2]))
+
+
+def measure_lkball(plan, coords, flush, steps):
+    """LK-ball energy + gradient on the batch (waters, one scoring pass, the
+    waters' adjoint): graph-replayed step time (L2 flushed before each), the
+    scoring kernel's average launch time and its FP32 figures."""
+    import torch
+
+    P = plan.n_poses
+    w = torch.ones((4, P), device=coords.device, dtype=coords.dtype)
+    E = torch.empty((4, P), device=coords.device, dtype=coords.dtype)
+    dx = torch.empty_like(coords)
+
+    def step():
+        plan.energy_and_gradient(coords, w, E, dx)
+
+    step()
+    plan.rebalance()
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    counts = plan.last_counts()
+    ms = time_replays(step, steps, flush) / steps
+    plan.profile(True)
+    for _ in range(steps):
+        flush.zero_()
+        step()
+    kern_ms, n_launch = plan.profile_read()
+    plan.profile(False)
+    kern = kern_ms / max(n_launch, 1)
+    flops = counts["pairs_evaluated"] * F_LKB_PAIR + counts["bridged_pairs"] * F_LKB_BRIDGE
+    return {
+        "ms_per_step": ms,
+        "poses_per_s": P / (ms / 1e3),
+        "kernel_ms": kern,
+        "flops_per_launch": flops,
+        "achieved_tflops": flops / (kern * 1e-3) / 1e12,
+        "work_per_step": {k: counts[k] for k in ("block_pairs", "polar_occluder_pairs", "pairs_evaluated",
+                                                 "bridged_pairs")},
+    }, step
+
+
+def cpu_lkball_sample(ps, reps=3):
+    """tmol's CPU LK-ball ops (oracle/_ref/lk_ball, else the C restatement)
+    on the whole batch: waters, energies, gradient; single thread, best of
+    `reps`."""
+    import numpy
+    import torch
+
+    from oracle import oracle as O
+    from tmol_b200.score.lkball_energy_term import LKBallEnergyTerm, score_args, water_gen_args
+
+    torch.set_num_threads(1)
+    lt = LKBallEnergyTerm()
+    wa, sa = water_gen_args(ps, lt), score_args(ps, lt, None)
+    coords = ps.coords.flatten(0, 1)
+    if O.reference_lkball_available():
+        kind = "reference"
+
+        def run():
+            E, _, _, _ = O.reference_lkball(coords, wa, sa)
+            E.sum().backward()
+
+    else:
+        kind = "port"
+        oc = O.OracleCall(coords, sa, term="lkball", lkb_water_args=wa)
+        ones = numpy.ones((4, ps.n_poses))
+
+        def run():
+            oc.lkb_scores(oc.lkb_waters(), weights=ones)
+
+    run()
+    best = float("inf")
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        run()
+        best = min(best, time.perf_counter() - t0)
+    return kind, best
+
+
+def run_lkball(args, world, rank, local):
+    """The LK-ball term on the uniform batch: waters, the four energies per
+    pose and the gradient of their sum through the waters, one call per
+    step (4 kernels and the sphere pass), replayed as a CUDA graph."""
+    import torch
+
+    from tmol_b200 import native
+    from tmol_b200.score.lkball_op import gen_pose_waters, lk_ball_pose_score
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    sizes, seeds = workload_sizes("lkball64x150", rank)
+    ps = workload(rank, "lkball64x150", device=dev)
+    coords = ps.coords.flatten(0, 1).to(dev).contiguous()
+    plan = lkball_plan_for(ps, coords)
+    P = ps.n_poses
+    flush = torch.empty(L2_FLUSH_BYTES // 4, device=dev, dtype=torch.float32)
+    m, step = measure_lkball(plan, coords, flush, max(args.warmup, 3))
+    if args.launch:
+        launch = tuple(int(v) for v in args.launch.split(","))
+        plan.set_launch(*launch)
+        step()
+        plan.rebalance()
+    else:
+        from tmol_b200.tune import autotune
+
+        launch, _ = autotune(plan, step, use_cache=False)
+    m, step = measure_lkball(plan, coords, flush, max(args.warmup, 3))
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        step()
+        torch.cuda.synchronize()
+        with torch.cuda.graph(g, stream=s):
+            step()
+    torch.cuda.current_stream().wait_stream(s)
+    for _ in range(max(args.warmup, 3)):
+        g.replay()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record()
+            g.replay()
+            ev[k][1].record()
+        torch.cuda.synchronize()
+    barrier(world)
+    ms_max = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), world)
+    poses_total = sum_over_ranks(P * args.steps, world)
+    value = poses_total / (ms_max / 1e3)
+    m, _ = measure_lkball(plan, coords, flush, args.steps)
+
+    # end to end through the drop-in ops, as tmol's LK-ball term calls them:
+    # pinned coordinates in, gen_pose_waters, lk_ball_pose_score, backward
+    # through both, energies and gradient out
+    from tmol_b200.score.lkball_energy_term import LKBallEnergyTerm, score_args, water_gen_args
+
+    lt = LKBallEnergyTerm()
+    wa = [a.to(dev) if isinstance(a, torch.Tensor) else a for a in water_gen_args(ps, lt)]
+    sa = [a.to(dev) if isinstance(a, torch.Tensor) else a for a in score_args(ps, lt, None)[:-2]]
+    del ps
+    h_coords = coords.cpu().pin_memory()
+    h_E = torch.empty((4, P), pin_memory=True)
+    h_g = torch.empty(coords.shape, pin_memory=True)
+
+    def e2e_step():
+        d_in = h_coords.to(dev, non_blocking=True).requires_grad_(True)
+        W = gen_pose_waters(d_in, *wa)
+        E, _ = lk_ball_pose_score(d_in, *sa, W, False, return_block_neighbors=False)
+        E.sum().backward()
+        h_E.copy_(E.detach(), non_blocking=True)
+        h_g.copy_(d_in.grad, non_blocking=True)
+
+    for _ in range(max(args.warmup, 3)):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier(world)
+    for k in range(args.steps):
+        flush.zero_()
+        e2e_ev[k][0].record()
+        e2e_step()
+        e2e_ev[k][1].record()
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in e2e_ev), world)
+
+    fp32_peak = native.measure_fp32_peak_tflops(torch.cuda.current_stream().cuda_stream)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from tmol_b200.pose.synthetic import synthetic_pose_stack
+
+        n_sample = 8
+        kind, t = cpu_lkball_sample(synthetic_pose_stack(sizes[:n_sample], seeds[:n_sample]))
+        cpu = {
+            "value": n_sample / t,
+            "unit": "poses/s",
+            "cores": 1,
+            "kind": kind,
+            "sample": f"{n_sample} of the {len(sizes)} {N_RES}-residue poses, waters + energies + gradient, "
+            "best of 3, one thread",
+        }
+    if rank == 0:
+        line = {
+            "metric": LKBALL_METRIC,
+            "value": value,
+            "unit": "poses/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded proteins, ideal geometry)",
+            "config": {
+                "workload": workload_label("lkball64x150"),
+                "poses_per_gpu": P,
+                "atoms_per_gpu": int(coords.shape[0]),
+                "l2": "flushed (256 MiB write) before every timed step",
+                "launch": "CUDA graph replay: 4 kernels per step (waters, block spheres, scoring with its "
+                "adjoint, waters adjoint) and 5 memsets",
+                "launch_shape": dict(
+                    zip(("items_per_ticket", "warps_per_cta", "ctas_per_sm", "candidates_per_item"), launch)
+                ),
+                "parallelism": f"weak, {world} independent batch(es)",
+            },
+            "work_per_step": m["work_per_step"],
+            "gpu_launches": 4 * args.steps,
+            "clocks": clk.summary(),
+            "roofline": {
+                "bound": "fp32",
+                "achieved": m["achieved_tflops"],
+                "peak": fp32_peak,
+                "unit": "TFLOP/s",
+                "frac": m["achieved_tflops"] / fp32_peak,
+                "traffic": None,
+                "kernel": "lkb_score_kernel<float, GRAD> (neighbour test + polar/occluder energies and adjoint)",
+                "kernel_ms": m["kernel_ms"],
+                "flops_per_launch": m["flops_per_launch"],
+                "peak_source": "measured: FMA-loop probe over all SMs in this run (tmol_b200_measure_fp32_peak)",
+            },
+            "e2e": {
+                "value": poses_total / (e2e_ms / 1e3),
+                "unit": "poses/s",
+                "h2d_bytes_per_step": coords.numel() * 4,
+                "d2h_bytes_per_step": (4 * P + coords.numel()) * 4,
+                "path": "gen_pose_waters + lk_ball_pose_score drop-ins, autograd backward",
+            },
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    del g
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
 def _bondsep_port_worker(conn, sizes, seeds):
     """One single-threaded process of the bond-separation CPU arm: the C
     restatement of the reference route (connection-point matrix, shortest
@@ -1521,7 +1831,7 @@ def main():
     ap.add_argument(
         "--workload",
         default="uniform64x150",
-        choices=["uniform64x150", "uneven256", "rotamers16x150", "elec64x150", "bondsep256"],
+        choices=["uniform64x150", "uneven256", "rotamers16x150", "elec64x150", "lkball64x150", "bondsep256"],
     )
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-screen", action="store_true", help="skip the learned-screen measurement")
@@ -1542,6 +1852,8 @@ def main():
         return run_rotamers(args, world, rank, local)
     if args.workload == "elec64x150":
         return run_elec(args, world, rank, local)
+    if args.workload == "lkball64x150":
+        return run_lkball(args, world, rank, local)
     if args.workload == "bondsep256":
         return run_bondsep(args, world, rank, local)
     return run_b200(args, world, rank, local)

@@ -129,6 +129,16 @@ int tmol_b200_lkball_backward(tmol_b200_lkball_plan* plan, const void* coords, c
                               int block_pair, const void* dTdV, void* dcoords, void* dwaters,
                               void* stream);
 
+/* Whole-pose energies and gradient in one call (a plan with both parts):
+ * the waters, the four energies [4, P] (overwritten) and dcoords [n_atoms,
+ * 3] (overwritten) = d(sum_t,p weights[t, p] * E[t, p]) / dcoords through
+ * the waters, weights [4, P].  Equivalent to gen_pose_waters forward,
+ * lk_ball_pose_score forward and backward, and gen_pose_waters backward
+ * (lk_ball_energy_term.py:240-300 composes them so), with the waters and
+ * their adjoint kept in the plan's scratch and one scoring pass. */
+int tmol_b200_lkball_energy_and_gradient(tmol_b200_lkball_plan* plan, const void* coords, const void* weights,
+                                         void* energies, void* dcoords, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

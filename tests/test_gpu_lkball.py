@@ -58,12 +58,12 @@ def gpu_run(ps, lterm, dtype, block_pair=False):
     return W.detach(), E.detach(), coords.grad, nbr
 
 
-def oracle_run(ps, lterm, f64):
+def oracle_run(ps, lterm, f64, weights=None):
     dt = torch.float64 if f64 else torch.float32
     oc = O.OracleCall(ps.coords.flatten(0, 1).to(dt), score_args(ps, lterm, None), f64=f64, term="lkball",
                       lkb_water_args=water_gen_args(ps, lterm))
     W = oc.lkb_waters()
-    E, dx, nbr = oc.lkb_scores(W, weights=numpy.ones((4, ps.n_poses)))
+    E, dx, nbr = oc.lkb_scores(W, weights=numpy.ones((4, ps.n_poses)) if weights is None else weights)
     return W, E, dx, nbr
 
 
@@ -145,6 +145,31 @@ def test_block_pair_energies_and_adjoint(lterm):
     dx1, dw1 = plan.backward(coords, W, w[:, :, None, None].expand(4, ps.n_poses, B, B), block_pair=True)
     numpy.testing.assert_allclose(dx1.cpu().numpy(), dx0.cpu().numpy(), rtol=1e-10, atol=1e-10)
     numpy.testing.assert_allclose(dw1.cpu().numpy(), dw0.cpu().numpy(), rtol=1e-10, atol=1e-10)
+
+
+@pytest.mark.parametrize("f64", [False, True])
+def test_energy_and_gradient_in_one_call(lterm, f64):
+    dt = torch.float64 if f64 else torch.float32
+    ps = synthetic_pose_stack([60, 25, 44], [51, 52, 53], extra_chi_sd=20.0)
+    wa, sa = static_args(ps, lterm, dt)
+    coords = ps.coords.flatten(0, 1).to(DEV, dt)
+    plan = LKBallPlan(coords, water_static=wa, score_static=sa)
+    w = torch.rand(4, ps.n_poses, dtype=torch.float64, generator=torch.Generator().manual_seed(3))
+    for _ in range(2):  # the plan's scratch is reused
+        E, dx = plan.energy_and_gradient(coords, w.to(DEV, dt))
+    _, Eo, dxo, _ = oracle_run(ps, lterm, f64, weights=w.numpy())
+    if f64:
+        E_close(E.cpu().numpy(), Eo, rtol=1e-9, atol=1e-9)
+        g_close(dx.cpu().numpy(), dxo, rtol=1e-9)
+    else:
+        E_close(E.cpu().numpy(), Eo)
+        g_close(dx.cpu().numpy(), dxo)
+    c = plan.last_counts()
+    assert 0 < c["bridged_pairs"] <= c["pairs_evaluated"] <= c["polar_occluder_pairs"]
+    assert c["block_pairs"] > 0
+    # a water-only plan has no one-call path
+    with pytest.raises(native.NativeError):
+        LKBallPlan(coords, water_static=wa).energy_and_gradient(coords, w.to(DEV, dt))
 
 
 def test_gradcheck(lterm):

@@ -1884,6 +1884,8 @@ struct tmol_b200_ljlk_plan {
   int lkb_maxpol = 0, lkb_maxocc = 0;
   void* lkb_par = nullptr;
   double lkb_water_dist = 0;
+  void* lkb_waters = nullptr;   // [N, 4, 3] scratch of the one-call energy + gradient
+  void* lkb_dwaters = nullptr;
   tmol_b200_ljlk_inputs dims;  // sizes only; pointers are not kept
   int P, B, nbt, A, C, ntiles, T;
   int64_t N;
@@ -1973,7 +1975,8 @@ void free_plan(tmol_b200_ljlk_plan* pl) {
                   pl->rot_off,   pl->rot_block,  pl->rot_pose,    pl->nrb,
                   pl->rob,       pl->rot_spheres, pl->row_pairs,  pl->row_items,
                   pl->bt_q,      pl->elec_k,      pl->lkb_sites,   pl->lkb_pol,
-                  pl->lkb_npol,  pl->lkb_occ,     pl->lkb_nocc,    pl->lkb_par};
+                  pl->lkb_npol,  pl->lkb_occ,     pl->lkb_nocc,    pl->lkb_par,
+                  pl->lkb_waters, pl->lkb_dwaters};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t e : pl->prof_events) cudaEventDestroy(e);
@@ -2321,6 +2324,7 @@ int lkb_score_impl(tmol_b200_ljlk_plan* pl, const void* coords, const void* wate
   if (nbr) CK(cudaMemsetAsync(nbr, 0, PBB * sizeof(int32_t), st));
   if (dcoords) CK(cudaMemsetAsync(dcoords, 0, (size_t)pl->N * 3 * sizeof(Real), st));
   if (dwaters) CK(cudaMemsetAsync(dwaters, 0, (size_t)pl->N * LKB_NW * 3 * sizeof(Real), st));
+  CK(cudaMemsetAsync(pl->counts, 0, N_COUNTS * sizeof(unsigned long long), st));
   const int n_blocks = pl->P * pl->B;
   const int grid_s = std::max(1, std::min((n_blocks + 7) / 8, pl->n_sm * 16));
   spheres_kernel<Real><<<grid_s, 256, 0, st>>>(s);
@@ -2440,6 +2444,10 @@ int build_lkball(tmol_b200_ljlk_plan* pl, const tmol_b200_lkball_inputs* k, cons
   }
   if (!waters) return TMOL_B200_OK;
   const int64_t n_sites = pl->N * LKB_NW;
+  if (scoring) {
+    CK(dalloc(pl, (Real**)&pl->lkb_waters, (size_t)n_sites * 3));
+    CK(dalloc(pl, (Real**)&pl->lkb_dwaters, (size_t)n_sites * 3));
+  }
   CK(dalloc(pl, (LkbSite<Real>**)&pl->lkb_sites, (size_t)n_sites));
   CK(cudaMemsetAsync(pl->lkb_sites, 0, sizeof(LkbSite<Real>) * std::max<int64_t>(n_sites, 1), st));
   const int64_t PB = (int64_t)pl->P * pl->B;
@@ -3282,6 +3290,28 @@ int tmol_b200_lkball_forward(tmol_b200_lkball_plan* plan, const void* coords, co
                                                           nullptr, nullptr, nullptr, st)
                     : lkb_score_impl<double, false, false>(plan, coords, waters, energies, block_neighbors,
                                                            nullptr, nullptr, nullptr, st);
+}
+
+int tmol_b200_lkball_energy_and_gradient(tmol_b200_lkball_plan* plan, const void* coords, const void* weights,
+                                         void* energies, void* dcoords, void* stream) {
+  if (!plan || plan->term != kTermLKBall || !plan->lkb_pol || !plan->lkb_sites || !weights || !energies ||
+      !dcoords)
+    return TMOL_B200_ERR_INVALID_ARGUMENT;
+  if (plan->N > 0 && !coords) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc;
+  if (plan->real_bytes == 4) {
+    if ((rc = lkb_waters_impl<float>(plan, coords, plan->lkb_waters, st))) return rc;
+    if ((rc = lkb_score_impl<float, true, false>(plan, coords, plan->lkb_waters, energies, nullptr, weights,
+                                                 dcoords, plan->lkb_dwaters, st)))
+      return rc;
+    return lkb_waters_backward_impl<float>(plan, coords, plan->lkb_dwaters, dcoords, st);
+  }
+  if ((rc = lkb_waters_impl<double>(plan, coords, plan->lkb_waters, st))) return rc;
+  if ((rc = lkb_score_impl<double, true, false>(plan, coords, plan->lkb_waters, energies, nullptr, weights,
+                                                dcoords, plan->lkb_dwaters, st)))
+    return rc;
+  return lkb_waters_backward_impl<double>(plan, coords, plan->lkb_dwaters, dcoords, st);
 }
 
 int tmol_b200_lkball_backward(tmol_b200_lkball_plan* plan, const void* coords, const void* waters,

@@ -568,17 +568,19 @@ __device__ inline void lkb_lk_pair(Real dist, int sep, Real sigma, Real ri, Real
 }
 
 // lk_ball_score (lk_ball.hh:335-500) for polar I against occluder J: E[4]
-// and, with GRAD, the adjoint of g . E onto I, J, WI, WJ (added)
+// and, with GRAD, the adjoint of g . E onto I, J, WI, WJ (added).  Returns
+// 0 when the pair is out of reach (bond separation, distance, no water),
+// 1 when evaluated, 2 when evaluated with the water-bridge term.
 template <typename Real, bool GRAD>
-__device__ inline void lkb_pair(const Real* I, const Real* J, const Real* WI, const Real* WJ, int sep,
+__device__ inline int lkb_pair(const Real* I, const Real* J, const Real* WI, const Real* WJ, int sep,
                                 const LkbParams<Real>& pi, const LkbParams<Real>& pj, const LkbArgs<Real>& k,
                                 Real* E, const Real* g, Real* gI, Real* gJ, Real* gWI, Real* gWJ) {
   E[0] = E[1] = E[2] = E[3] = 0;
-  if (sep <= 3) return;
+  if (sep <= 3) return 0;
   const Real dv[3] = {I[0] - J[0], I[1] - J[1], I[2] - J[2]};
   const Real dist = lkb_sqrt(lkb_dot(dv, dv));
-  if (dist >= k.max_dis) return;
-  if (isnan(WI[0])) return;
+  if (dist >= k.max_dis) return 0;
+  if (isnan(WI[0])) return 0;
   const Real sigma = lkb_sigma(pi, pj, k);
   Real iso, diso;
   lkb_lk_pair(dist, sep, sigma, pi.lj_radius, pi.lk_dgfree, pi.lk_lambda, pj.lk_volume, k.max_dis,
@@ -587,7 +589,8 @@ __device__ inline void lkb_pair(const Real* I, const Real* J, const Real* WI, co
   const Real fdes = lkb_fraction<Real, GRAD>(WI, J, pj.lj_radius, fdJ, fdWI);
   Real bdI[3] = {0, 0, 0}, bdJ[3] = {0, 0, 0}, bdWI[LKB_NW * 3], bdWJ[LKB_NW * 3];
   Real fov = 0;
-  if (pj.is_donor != 0 || pj.is_acceptor != 0) {
+  const bool bridged = pj.is_donor != 0 || pj.is_acceptor != 0;
+  if (bridged) {
     fov = lkb_bridge<Real, GRAD>(I, J, WI, WJ, k.water_dist, bdI, bdJ, bdWI, bdWJ);
   } else if (GRAD) {
     for (int i = 0; i < LKB_NW * 3; ++i) bdWI[i] = bdWJ[i] = 0;
@@ -596,7 +599,7 @@ __device__ inline void lkb_pair(const Real* I, const Real* J, const Real* WI, co
   E[1] = iso * fdes;
   E[2] = iso * fov;
   E[3] = fov / 2;
-  if (!GRAD) return;
+  if (!GRAD) return bridged ? 2 : 1;
   Real u[3] = {0, 0, 0};
   if (dist != Real(0))
     for (int i = 0; i < 3; ++i) u[i] = dv[i] / dist;
@@ -609,6 +612,7 @@ __device__ inline void lkb_pair(const Real* I, const Real* J, const Real* WI, co
     gWI[i] += g[1] * iso * fdWI[i] + g[2] * iso * bdWI[i] + g[3] * bdWI[i] / 2;
     gWJ[i] += g[2] * iso * bdWJ[i] + g[3] * bdWJ[i] / 2;
   }
+  return bridged ? 2 : 1;
 }
 
 // ---------------------------------------------------------------------------
@@ -652,6 +656,9 @@ template <typename Real, bool GRAD, bool BLOCK_PAIR>
 __global__ void __launch_bounds__(256) lkb_score_kernel(ScoreArgs<Real> s, LkbArgs<Real> k, int items_per_ticket) {
   const int lane = threadIdx.x & 31;
   const int64_t stride = (int64_t)s.P * s.B * s.B;
+  // work counters: block pairs, polar / occluder pairs, bridged pairs,
+  // pairs evaluated
+  unsigned long long n_bp = 0, n_pairs = 0, n_bridge = 0, n_eval = 0;
   for (;;) {
     int t = 0;
     if (lane == 0) t = atomicAdd(s.ticket, 1);
@@ -660,11 +667,15 @@ __global__ void __launch_bounds__(256) lkb_score_kernel(ScoreArgs<Real> s, LkbAr
     if (it0 >= s.n_work) break;
     const int it1 = min(it0 + items_per_ticket, s.n_work);
     for (int item = it0; item < it1; ++item) {
+      const long long t_item = clock64();
       const int4 wi = s.work[item];
       const int p = wi.x, b1 = wi.y, cand0 = wi.z, cand1 = wi.w;
       const int i1 = p * s.B + b1;
       const int bt1 = s.blk_bt[i1];
-      if (bt1 < 0) continue;
+      if (bt1 < 0) {
+        if (s.item_cost && lane == 0) s.item_cost[item] = 0;
+        continue;
+      }
       const int off1 = s.blk_off[i1];
       const Real* sph1 = s.spheres + 4 * (int64_t)i1;
       const Real c1x = sph1[0], c1y = sph1[1], c1z = sph1[2], rad1 = sph1[3];
@@ -724,6 +735,8 @@ __global__ void __launch_bounds__(256) lkb_score_kernel(ScoreArgs<Real> s, LkbAr
           const int npol2 = k.npol[bt2], nocc2 = k.nocc[bt2];
           const int n01 = npol1 * (intra ? nocc1 : nocc2);
           const int total = intra ? n01 : n01 + nocc1 * npol2;
+          n_bp += 1;
+          n_pairs += total;
           for (int idx = lane; idx < total; idx += 32) {
             int ap, ao, btp, bto, offp, offo, sep;
             if (idx < n01) {
@@ -765,7 +778,9 @@ __global__ void __launch_bounds__(256) lkb_score_kernel(ScoreArgs<Real> s, LkbAr
             Real e[4], gI[3] = {0, 0, 0}, gJ[3] = {0, 0, 0}, gWI[LKB_NW * 3], gWJ[LKB_NW * 3];
             if (GRAD)
               for (int q = 0; q < LKB_NW * 3; ++q) gWI[q] = gWJ[q] = 0;
-            lkb_pair<Real, GRAD>(I, J, WI, WJ, sep, pp, po, k, e, w, gI, gJ, gWI, gWJ);
+            const int how = lkb_pair<Real, GRAD>(I, J, WI, WJ, sep, pp, po, k, e, w, gI, gJ, gWI, gWJ);
+            n_eval += how > 0;
+            n_bridge += how == 2;
             for (int q = 0; q < 4; ++q) e4[q] += e[q];
             if (GRAD) {
               for (int q = 0; q < 3; ++q) {
@@ -789,11 +804,30 @@ __global__ void __launch_bounds__(256) lkb_score_kernel(ScoreArgs<Real> s, LkbAr
           }
         }
       }
-      if (!BLOCK_PAIR && !GRAD)
+      // whole-pose energies (also in the adjoint when asked for: one pass
+      // for energy and gradient)
+      if (!BLOCK_PAIR && s.energies)
         for (int q = 0; q < 4; ++q) {
           const Real v = warp_sum(acc[q]);
           if (lane == 0 && v != Real(0)) atomicAdd(&s.energies[(int64_t)q * s.P + p], v);
         }
+      // the item's cost, for ordering the work longest-first
+      if (s.item_cost && lane == 0) s.item_cost[item] = (int)min((clock64() - t_item) >> 4, (long long)0x7fffffff);
+    }
+  }
+  if (s.counts) {
+    // n_bp is the same on every lane; the pair counts are per lane
+    const unsigned long long a = n_eval, b = n_bridge;
+    unsigned long long sa = a, sb = b;
+    for (int o = 16; o > 0; o >>= 1) {
+      sa += __shfl_xor_sync(0xffffffffu, sa, o);
+      sb += __shfl_xor_sync(0xffffffffu, sb, o);
+    }
+    if (lane == 0) {
+      if (n_bp) atomicAdd(&s.counts[0], n_bp);
+      if (n_pairs) atomicAdd(&s.counts[1], n_pairs);
+      if (sb) atomicAdd(&s.counts[2], sb);
+      if (sa) atomicAdd(&s.counts[3], sa);
     }
   }
 }

@@ -245,6 +245,7 @@ SIGNATURES = {
     "tmol_b200_lkball_waters_backward": (ctypes.c_int, [_V, _V, _V, _V, _V]),
     "tmol_b200_lkball_forward": (ctypes.c_int, [_V, _V, _V, ctypes.c_int, _V, _V, _V]),
     "tmol_b200_lkball_backward": (ctypes.c_int, [_V, _V, _V, ctypes.c_int, _V, _V, _V, _V]),
+    "tmol_b200_lkball_energy_and_gradient": (ctypes.c_int, [_V, _V, _V, _V, _V, _V]),
     # PoseStack construction (include/tmol_b200_pose.h)
     "tmol_b200_pose_bondsep": (ctypes.c_int, [ctypes.POINTER(PoseConnectivity), _V, _V, _V, _V]),
     "tmol_b200_apsp_stacked": (ctypes.c_int, [_V, _I32, _I32, _I32, _V]),

@@ -194,11 +194,7 @@ class LKBallPlan(LJLKPlan):
         )
         return dcoords, dwaters
 
-    def energy_and_gradient(self, *a, **k):
-        raise NotImplementedError("LK-ball scoring runs forward, then backward")
-
-    def last_counts(self):
-        raise NotImplementedError("LK-ball scoring keeps no work counters")
+    COUNT_NAMES = ("block_pairs", "polar_occluder_pairs", "bridged_pairs", "pairs_evaluated", "unused")
 
     def set_skip_mask(self, mask):
         raise NotImplementedError("the learned block-pair screen serves LJ/LK plans")
