@@ -1881,6 +1881,7 @@ struct tmol_b200_ljlk_plan {
   int* lkb_npol = nullptr;
   int* lkb_occ = nullptr;
   int* lkb_nocc = nullptr;
+  int* lkb_nbocc = nullptr;
   int lkb_maxpol = 0, lkb_maxocc = 0;
   void* lkb_par = nullptr;
   double lkb_water_dist = 0;
@@ -1976,7 +1977,7 @@ void free_plan(tmol_b200_ljlk_plan* pl) {
                   pl->rob,       pl->rot_spheres, pl->row_pairs,  pl->row_items,
                   pl->bt_q,      pl->elec_k,      pl->lkb_sites,   pl->lkb_pol,
                   pl->lkb_npol,  pl->lkb_occ,     pl->lkb_nocc,    pl->lkb_par,
-                  pl->lkb_waters, pl->lkb_dwaters};
+                  pl->lkb_waters, pl->lkb_dwaters, pl->lkb_nbocc};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t e : pl->prof_events) cudaEventDestroy(e);
@@ -2272,6 +2273,7 @@ LkbArgs<Real> lkb_args(tmol_b200_ljlk_plan* pl) {
   k.npol = pl->lkb_npol;
   k.occ = pl->lkb_occ;
   k.nocc = pl->lkb_nocc;
+  k.nbocc = pl->lkb_nbocc;
   k.maxpol = pl->lkb_maxpol;
   k.maxocc = pl->lkb_maxocc;
   k.par = (const Real*)pl->lkb_par;
@@ -2414,6 +2416,17 @@ int build_lkball(tmol_b200_ljlk_plan* pl, const tmol_b200_lkball_inputs* k, cons
         std::copy_n(&tpar[(tb * TILE + q) * LKB_NPAR], LKB_NPAR, &par[((size_t)bt * A + a) * LKB_NPAR]);
       }
     }
+  // occluders that are donors or acceptors (parameters 4 and 7) first: the
+  // scoring kernel queues their pairs apart (the water-bridge term)
+  std::vector<int> hnbocc(std::max(nbt, 1), 0);
+  for (int bt = 0; bt < nbt; ++bt) {
+    auto bridges = [&](int a) {
+      const Real* q = &par[((size_t)bt * A + a) * LKB_NPAR];
+      return q[4] != Real(0) || q[7] != Real(0);
+    };
+    std::stable_partition(occ[bt].begin(), occ[bt].end(), bridges);
+    for (int a : occ[bt]) hnbocc[bt] += bridges(a) ? 1 : 0;
+  }
   int maxpol = 1, maxocc = 1;
   for (int bt = 0; bt < nbt; ++bt) {
     maxpol = std::max(maxpol, (int)pol[bt].size());
@@ -2435,6 +2448,8 @@ int build_lkball(tmol_b200_ljlk_plan* pl, const tmol_b200_lkball_inputs* k, cons
     CK(dalloc(pl, &pl->lkb_occ, hocc.size()));
     CK(dalloc(pl, &pl->lkb_npol, hnpol.size()));
     CK(dalloc(pl, &pl->lkb_nocc, hnocc.size()));
+    CK(dalloc(pl, &pl->lkb_nbocc, hnbocc.size()));
+    CK(cudaMemcpyAsync(pl->lkb_nbocc, hnbocc.data(), sizeof(int) * hnbocc.size(), cudaMemcpyHostToDevice, st));
     CK(dalloc(pl, (Real**)&pl->lkb_par, par.size()));
     CK(cudaMemcpyAsync(pl->lkb_pol, hpol.data(), sizeof(int) * hpol.size(), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(pl->lkb_occ, hocc.data(), sizeof(int) * hocc.size(), cudaMemcpyHostToDevice, st));

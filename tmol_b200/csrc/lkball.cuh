@@ -37,8 +37,9 @@ struct LkbArgs {
   Real* dwaters_out;    // adjoint out
   const int* pol;       // [nbt][maxpol] polar atoms of each block type
   const int* npol;      // [nbt]
-  const int* occ;       // [nbt][maxocc] heavy atoms (polar ones included)
+  const int* occ;       // [nbt][maxocc] heavy atoms (polar ones included), donors / acceptors first
   const int* nocc;
+  const int* nbocc;     // [nbt] leading occluders that are donors or acceptors (the bridge term)
   int maxpol, maxocc;
   const Real* par;      // [nbt][A][9]
   Real water_dist, hbond_dis, hbond_oh, hbond_h, max_dis;
@@ -652,13 +653,67 @@ __device__ __forceinline__ LkbParams<Real> lkb_params(const LkbArgs<Real>& k, in
   return r;
 }
 
+// Pairs in reach wait in two per-warp queues, those whose occluder bridges
+// (donor or acceptor: the 4 x 4 water-pair term) and the rest, and are
+// evaluated 32 at a time with every lane busy on the same branch.
+constexpr int LKB_Q = 64;
+
+struct LkbQueue {
+  int rp[LKB_Q], ro[LKB_Q], pi[LKB_Q], oi[LKB_Q];  // coordinate rows; (bt * A + atom) of the polar / occluder
+  uint8_t sep[LKB_Q];
+};
+
+// Evaluates entries [0, n) of q (one per lane): energies into e4, the
+// adjoint of w . E into dcoords / dwaters.
+template <typename Real, bool GRAD>
+__device__ __forceinline__ void lkb_drain(const ScoreArgs<Real>& s, const LkbArgs<Real>& k, const LkbQueue& q,
+                                          int n, int lane, const Real* w, Real* e4) {
+  if (lane >= n) return;
+  const int64_t rp = q.rp[lane], ro = q.ro[lane];
+  const int pidx = q.pi[lane], oidx = q.oi[lane], sep = q.sep[lane];
+  Real I[3], J[3], WI[LKB_NW * 3], WJ[LKB_NW * 3];
+  lkb_load3(s.coords, rp, I);
+  lkb_load3(s.coords, ro, J);
+#pragma unroll
+  for (int c = 0; c < LKB_NW * 3; ++c) {
+    WI[c] = k.waters[rp * LKB_NW * 3 + c];
+    WJ[c] = k.waters[ro * LKB_NW * 3 + c];
+  }
+  const LkbParams<Real> pp = lkb_params(k, s.A, pidx / s.A, pidx % s.A);
+  const LkbParams<Real> po = lkb_params(k, s.A, oidx / s.A, oidx % s.A);
+  Real e[4], gI[3] = {0, 0, 0}, gJ[3] = {0, 0, 0}, gWI[LKB_NW * 3], gWJ[LKB_NW * 3];
+  if (GRAD)
+#pragma unroll
+    for (int c = 0; c < LKB_NW * 3; ++c) gWI[c] = gWJ[c] = 0;
+  lkb_pair<Real, GRAD>(I, J, WI, WJ, sep, pp, po, k, e, w, gI, gJ, gWI, gWJ);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) e4[c] += e[c];
+  if (GRAD) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      if (gI[c] != Real(0)) atomicAdd(&s.dcoords[3 * rp + c], gI[c]);
+      if (gJ[c] != Real(0)) atomicAdd(&s.dcoords[3 * ro + c], gJ[c]);
+    }
+#pragma unroll
+    for (int c = 0; c < LKB_NW * 3; ++c) {
+      if (gWI[c] != Real(0)) atomicAdd(&k.dwaters_out[rp * LKB_NW * 3 + c], gWI[c]);
+      if (gWJ[c] != Real(0)) atomicAdd(&k.dwaters_out[ro * LKB_NW * 3 + c], gWJ[c]);
+    }
+  }
+}
+
 template <typename Real, bool GRAD, bool BLOCK_PAIR>
 __global__ void __launch_bounds__(256) lkb_score_kernel(ScoreArgs<Real> s, LkbArgs<Real> k, int items_per_ticket) {
-  const int lane = threadIdx.x & 31;
+  __shared__ LkbQueue queues[8][2];  // [warp][plain, bridged]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  LkbQueue* const qs = queues[warp];
+  const unsigned lt_mask = (1u << lane) - 1u;
   const int64_t stride = (int64_t)s.P * s.B * s.B;
+  const Real reach2 = k.max_dis * k.max_dis;
   // work counters: block pairs, polar / occluder pairs, bridged pairs,
-  // pairs evaluated
+  // pairs evaluated (warp-uniform)
   unsigned long long n_bp = 0, n_pairs = 0, n_bridge = 0, n_eval = 0;
+  int nq[2] = {0, 0};
   for (;;) {
     int t = 0;
     if (lane == 0) t = atomicAdd(s.ticket, 1);
@@ -706,7 +761,39 @@ __global__ void __launch_bounds__(256) lkb_score_kernel(ScoreArgs<Real> s, LkbAr
       if (GRAD && !BLOCK_PAIR)
         for (int q = 0; q < 4; ++q) w[q] = s.dTdV[(int64_t)q * s.P + p];
       Real acc[4] = {0, 0, 0, 0};
-      const int npol1 = k.npol[bt1], nocc1 = k.nocc[bt1];
+      const int npol1 = k.npol[bt1], nocc1 = k.nocc[bt1], nbr1 = k.nbocc[bt1];
+      // evaluates full queues (or, with `all`, everything queued) and
+      // shifts what is left to the front
+      auto pump = [&](bool all, Real* e4) {
+        for (;;) {
+          int which, n;
+          if (nq[0] >= 32) {
+            which = 0, n = 32;
+          } else if (nq[1] >= 32) {
+            which = 1, n = 32;
+          } else if (all && nq[0] > 0) {
+            which = 0, n = nq[0];
+          } else if (all && nq[1] > 0) {
+            which = 1, n = nq[1];
+          } else {
+            break;
+          }
+          LkbQueue& q = qs[which];
+          __syncwarp();
+          lkb_drain<Real, GRAD>(s, k, q, n, lane, w, e4);
+          const int rest = nq[which] - n;
+          int a = 0, b = 0, c = 0, d = 0, e = 0;
+          if (lane < rest) {
+            a = q.rp[n + lane], b = q.ro[n + lane], c = q.pi[n + lane], d = q.oi[n + lane], e = q.sep[n + lane];
+          }
+          __syncwarp();
+          if (lane < rest) {
+            q.rp[lane] = a, q.ro[lane] = b, q.pi[lane] = c, q.oi[lane] = d, q.sep[lane] = (uint8_t)e;
+          }
+          __syncwarp();
+          nq[which] = rest;
+        }
+      };
       for (int bi = 0; bi < n_batches; ++bi) {
         unsigned mask = __shfl_sync(0xffffffffu, my_mask, bi);
         while (mask) {
@@ -732,78 +819,89 @@ __global__ void __launch_bounds__(256) lkb_score_kernel(ScoreArgs<Real> s, LkbAr
           if (GRAD && BLOCK_PAIR)
             for (int q = 0; q < 4; ++q) w[q] = s.dTdV[(int64_t)q * stride + pair_o];
           Real e4[4] = {0, 0, 0, 0};
-          const int npol2 = k.npol[bt2], nocc2 = k.nocc[bt2];
-          const int n01 = npol1 * (intra ? nocc1 : nocc2);
+          const int npol2 = k.npol[bt2], nocc2 = k.nocc[bt2], nbr2 = k.nbocc[bt2];
+          const int no = intra ? nocc1 : nocc2;
+          const int n01 = npol1 * no;
           const int total = intra ? n01 : n01 + nocc1 * npol2;
           n_bp += 1;
           n_pairs += total;
-          for (int idx = lane; idx < total; idx += 32) {
-            int ap, ao, btp, bto, offp, offo, sep;
-            if (idx < n01) {
-              const int no = intra ? nocc1 : nocc2;
-              const int x = idx / no, y = idx - x * no;
-              btp = bt1;
-              bto = intra ? bt1 : bt2;
-              ap = k.pol[(int64_t)btp * k.maxpol + x];
-              ao = k.occ[(int64_t)bto * k.maxocc + y];
-              offp = off1;
-              offo = intra ? off1 : off2;
-              if (intra) {
-                if (ap == ao) continue;
-                sep = s.bt_pd[((int64_t)bt1 * s.A + ap) * s.A + ao];
+          // filter: bond separation, distance, waters; queue what is in reach
+          for (int base = 0; base < total; base += 32) {
+            const int idx = base + lane;
+            bool in_reach = false, bridged = false;
+            int rp = 0, ro = 0, pidx = 0, oidx = 0, sep = 0;
+            if (idx < total) {
+              int ap, ao, btp, bto, offp, offo, y;
+              if (idx < n01) {
+                const int x = idx / no;
+                y = idx - x * no;
+                btp = bt1;
+                bto = intra ? bt1 : bt2;
+                ap = k.pol[(int64_t)btp * k.maxpol + x];
+                ao = k.occ[(int64_t)bto * k.maxocc + y];
+                offp = off1;
+                offo = intra ? off1 : off2;
+                if (intra)
+                  sep = ap == ao ? 0 : s.bt_pd[((int64_t)bt1 * s.A + ap) * s.A + ao];
+                else
+                  sep = striking ? lkb_inter_sep(s, bt1, bt2, nc1, nc2, seps, ap, ao) : 6;
+                bridged = y < (intra ? nbr1 : nbr2);
               } else {
-                sep = striking ? lkb_inter_sep(s, bt1, bt2, nc1, nc2, seps, ap, ao) : 6;
+                const int j = idx - n01;
+                const int x = j / nocc1;
+                y = j - x * nocc1;
+                btp = bt2;
+                bto = bt1;
+                ap = k.pol[(int64_t)btp * k.maxpol + x];
+                ao = k.occ[(int64_t)bto * k.maxocc + y];
+                offp = off2;
+                offo = off1;
+                sep = striking ? lkb_inter_sep(s, bt1, bt2, nc1, nc2, seps, ao, ap) : 6;
+                bridged = y < nbr1;
               }
-            } else {
-              const int j = idx - n01;
-              const int x = j / nocc1, y = j - x * nocc1;
-              btp = bt2;
-              bto = bt1;
-              ap = k.pol[(int64_t)btp * k.maxpol + x];
-              ao = k.occ[(int64_t)bto * k.maxocc + y];
-              offp = off2;
-              offo = off1;
-              sep = striking ? lkb_inter_sep(s, bt1, bt2, nc1, nc2, seps, ao, ap) : 6;
-            }
-            const int64_t rp = (int64_t)offp + ap, ro = (int64_t)offo + ao;
-            Real I[3], J[3], WI[LKB_NW * 3], WJ[LKB_NW * 3];
-            lkb_load3(s.coords, rp, I);
-            lkb_load3(s.coords, ro, J);
-#pragma unroll
-            for (int q = 0; q < LKB_NW * 3; ++q) {
-              WI[q] = k.waters[rp * LKB_NW * 3 + q];
-              WJ[q] = k.waters[ro * LKB_NW * 3 + q];
-            }
-            const LkbParams<Real> pp = lkb_params(k, s.A, btp, ap), po = lkb_params(k, s.A, bto, ao);
-            Real e[4], gI[3] = {0, 0, 0}, gJ[3] = {0, 0, 0}, gWI[LKB_NW * 3], gWJ[LKB_NW * 3];
-            if (GRAD)
-              for (int q = 0; q < LKB_NW * 3; ++q) gWI[q] = gWJ[q] = 0;
-            const int how = lkb_pair<Real, GRAD>(I, J, WI, WJ, sep, pp, po, k, e, w, gI, gJ, gWI, gWJ);
-            n_eval += how > 0;
-            n_bridge += how == 2;
-            for (int q = 0; q < 4; ++q) e4[q] += e[q];
-            if (GRAD) {
-              for (int q = 0; q < 3; ++q) {
-                if (gI[q] != Real(0)) atomicAdd(&s.dcoords[3 * rp + q], gI[q]);
-                if (gJ[q] != Real(0)) atomicAdd(&s.dcoords[3 * ro + q], gJ[q]);
-              }
-              for (int q = 0; q < LKB_NW * 3; ++q) {
-                if (gWI[q] != Real(0)) atomicAdd(&k.dwaters_out[rp * LKB_NW * 3 + q], gWI[q]);
-                if (gWJ[q] != Real(0)) atomicAdd(&k.dwaters_out[ro * LKB_NW * 3 + q], gWJ[q]);
+              if (sep > 3) {
+                rp = offp + ap;
+                ro = offo + ao;
+                Real I[3], J[3];
+                lkb_load3(s.coords, rp, I);
+                lkb_load3(s.coords, ro, J);
+                const Real dv[3] = {I[0] - J[0], I[1] - J[1], I[2] - J[2]};
+                const Real dist = lkb_sqrt(lkb_dot(dv, dv));
+                in_reach = dist < k.max_dis && !isnan(k.waters[(int64_t)rp * LKB_NW * 3]);
+                pidx = btp * s.A + ap;
+                oidx = bto * s.A + ao;
               }
             }
+            const unsigned m1 = __ballot_sync(0xffffffffu, in_reach && bridged);
+            const unsigned m0 = __ballot_sync(0xffffffffu, in_reach && !bridged);
+            if (in_reach) {
+              const int which = bridged ? 1 : 0;
+              LkbQueue& q = qs[which];
+              const int pos = nq[which] + __popc((bridged ? m1 : m0) & lt_mask);
+              q.rp[pos] = rp;
+              q.ro[pos] = ro;
+              q.pi[pos] = pidx;
+              q.oi[pos] = oidx;
+              q.sep[pos] = (uint8_t)(sep > 255 ? 255 : sep);
+            }
+            nq[0] += __popc(m0);
+            nq[1] += __popc(m1);
+            n_eval += __popc(m0 | m1);
+            n_bridge += __popc(m1);
+            pump(false, BLOCK_PAIR ? e4 : acc);
           }
+          (void)reach2;
           if (BLOCK_PAIR) {
+            pump(true, e4);
             if (!GRAD)
               for (int q = 0; q < 4; ++q) {
                 const Real v = warp_sum(e4[q]);
                 if (lane == 0) s.energies[(int64_t)q * stride + pair_o] = v;
               }
-          } else {
-            for (int q = 0; q < 4; ++q) acc[q] += e4[q];
           }
         }
       }
+      if (!BLOCK_PAIR) pump(true, acc);
       // whole-pose energies (also in the adjoint when asked for: one pass
       // for energy and gradient)
       if (!BLOCK_PAIR && s.energies)
@@ -815,19 +913,10 @@ __global__ void __launch_bounds__(256) lkb_score_kernel(ScoreArgs<Real> s, LkbAr
       if (s.item_cost && lane == 0) s.item_cost[item] = (int)min((clock64() - t_item) >> 4, (long long)0x7fffffff);
     }
   }
-  if (s.counts) {
-    // n_bp is the same on every lane; the pair counts are per lane
-    const unsigned long long a = n_eval, b = n_bridge;
-    unsigned long long sa = a, sb = b;
-    for (int o = 16; o > 0; o >>= 1) {
-      sa += __shfl_xor_sync(0xffffffffu, sa, o);
-      sb += __shfl_xor_sync(0xffffffffu, sb, o);
-    }
-    if (lane == 0) {
-      if (n_bp) atomicAdd(&s.counts[0], n_bp);
-      if (n_pairs) atomicAdd(&s.counts[1], n_pairs);
-      if (sb) atomicAdd(&s.counts[2], sb);
-      if (sa) atomicAdd(&s.counts[3], sa);
-    }
+  if (s.counts && lane == 0) {
+    if (n_bp) atomicAdd(&s.counts[0], n_bp);
+    if (n_pairs) atomicAdd(&s.counts[1], n_pairs);
+    if (n_bridge) atomicAdd(&s.counts[2], n_bridge);
+    if (n_eval) atomicAdd(&s.counts[3], n_eval);
   }
 }
