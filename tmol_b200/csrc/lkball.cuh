@@ -468,7 +468,9 @@ __device__ inline Real lkb_bridge(const Real* I, const Real* J, const Real* WI, 
   Real wsum = 0;
   if (GRAD)
     for (int i = 0; i < LKB_NW * 3; ++i) dWI[i] = dWJ[i] = 0;
+#pragma unroll 1
   for (int a = 0; a < LKB_NW; ++a)
+#pragma unroll
     for (int c = 0; c < LKB_NW; ++c) {
       const Real dl[3] = {WI[3 * a] - WJ[3 * c], WI[3 * a + 1] - WJ[3 * c + 1], WI[3 * a + 2] - WJ[3 * c + 2]};
       const Real d2 = lkb_dot(dl, dl) - gap;
@@ -517,9 +519,8 @@ __device__ inline Real lkb_bridge(const Real* I, const Real* J, const Real* WI, 
   return ofrac * afrac;
 }
 
-template <typename Real>
-__device__ __forceinline__ Real lkb_sigma(const LkbParams<Real>& i, const LkbParams<Real>& j,
-                                          const LkbArgs<Real>& k) {
+template <typename Real, typename K>
+__device__ __forceinline__ Real lkb_sigma(const LkbParams<Real>& i, const LkbParams<Real>& j, const K& k) {
   const bool di = i.is_donor != 0, dj = j.is_donor != 0, ai = i.is_acceptor != 0, aj = j.is_acceptor != 0;
   if ((di && aj) || (dj && ai)) {
     if ((di && i.is_hydroxyl != 0) || (dj && j.is_hydroxyl != 0)) return k.hbond_oh;
@@ -572,9 +573,9 @@ __device__ inline void lkb_lk_pair(Real dist, int sep, Real sigma, Real ri, Real
 // and, with GRAD, the adjoint of g . E onto I, J, WI, WJ (added).  Returns
 // 0 when the pair is out of reach (bond separation, distance, no water),
 // 1 when evaluated, 2 when evaluated with the water-bridge term.
-template <typename Real, bool GRAD>
+template <typename Real, bool GRAD, typename K>
 __device__ inline int lkb_pair(const Real* I, const Real* J, const Real* WI, const Real* WJ, int sep,
-                                const LkbParams<Real>& pi, const LkbParams<Real>& pj, const LkbArgs<Real>& k,
+                                const LkbParams<Real>& pi, const LkbParams<Real>& pj, const K& k,
                                 Real* E, const Real* g, Real* gI, Real* gJ, Real* gWI, Real* gWJ) {
   E[0] = E[1] = E[2] = E[3] = 0;
   if (sep <= 3) return 0;
@@ -637,8 +638,8 @@ __device__ __forceinline__ int lkb_inter_sep(const ScoreArgs<Real>& s, int bt1, 
   return sep;
 }
 
-template <typename Real>
-__device__ __forceinline__ LkbParams<Real> lkb_params(const LkbArgs<Real>& k, int A, int bt, int atom) {
+template <typename Real, typename K>
+__device__ __forceinline__ LkbParams<Real> lkb_params(const K& k, int A, int bt, int atom) {
   const Real* q = k.par + ((int64_t)bt * A + atom) * LKB_NPAR;
   LkbParams<Real> r;
   r.lj_radius = q[0];
@@ -663,47 +664,75 @@ struct LkbQueue {
   uint8_t sep[LKB_Q];
 };
 
-// Evaluates entries [0, n) of q (one per lane): energies into e4, the
-// adjoint of w . E into dcoords / dwaters.
+// What evaluating a queued pair needs (a compact by-value context).
+template <typename Real>
+struct LkbEval {
+  const Real* coords;
+  const Real* waters;
+  const Real* par;
+  Real* dcoords;
+  Real* dwaters;
+  int A;
+  Real water_dist, hbond_dis, hbond_oh, hbond_h, max_dis;
+};
+
+template <typename Real>
+struct Lkb4 {
+  Real v[4];
+};
+
+// Evaluates entry `lane` of q when lane < n: returns its four energies and,
+// with GRAD, adds the adjoint of w . E to dcoords / dwaters.
+// inlined: an out-of-line copy (smaller code) measured 34% slower, its
+// calling convention spilling the kernel's state
+#ifndef TMOL_B200_LKB_DRAIN_ATTR
+#define TMOL_B200_LKB_DRAIN_ATTR __forceinline__
+#endif
+// two 256-thread CTAs per SM (128 registers): measured faster than one
+// (182 registers) and than three (80 registers, spilling)
+#ifndef TMOL_B200_LKB_MIN_CTAS
+#define TMOL_B200_LKB_MIN_CTAS 2
+#endif
+
 template <typename Real, bool GRAD>
-__device__ __forceinline__ void lkb_drain(const ScoreArgs<Real>& s, const LkbArgs<Real>& k, const LkbQueue& q,
-                                          int n, int lane, const Real* w, Real* e4) {
-  if (lane >= n) return;
+__device__ TMOL_B200_LKB_DRAIN_ATTR Lkb4<Real> lkb_drain(const LkbEval<Real> ev, const LkbQueue& q, int n, int lane,
+                                             const Lkb4<Real> w) {
+  Lkb4<Real> out = {{0, 0, 0, 0}};
+  if (lane >= n) return out;
   const int64_t rp = q.rp[lane], ro = q.ro[lane];
   const int pidx = q.pi[lane], oidx = q.oi[lane], sep = q.sep[lane];
   Real I[3], J[3], WI[LKB_NW * 3], WJ[LKB_NW * 3];
-  lkb_load3(s.coords, rp, I);
-  lkb_load3(s.coords, ro, J);
+  lkb_load3(ev.coords, rp, I);
+  lkb_load3(ev.coords, ro, J);
 #pragma unroll
   for (int c = 0; c < LKB_NW * 3; ++c) {
-    WI[c] = k.waters[rp * LKB_NW * 3 + c];
-    WJ[c] = k.waters[ro * LKB_NW * 3 + c];
+    WI[c] = ev.waters[rp * LKB_NW * 3 + c];
+    WJ[c] = ev.waters[ro * LKB_NW * 3 + c];
   }
-  const LkbParams<Real> pp = lkb_params(k, s.A, pidx / s.A, pidx % s.A);
-  const LkbParams<Real> po = lkb_params(k, s.A, oidx / s.A, oidx % s.A);
-  Real e[4], gI[3] = {0, 0, 0}, gJ[3] = {0, 0, 0}, gWI[LKB_NW * 3], gWJ[LKB_NW * 3];
+  const LkbParams<Real> pp = lkb_params<Real>(ev, 0, 0, pidx);  // row bt * A + atom
+  const LkbParams<Real> po = lkb_params<Real>(ev, 0, 0, oidx);
+  Real gI[3] = {0, 0, 0}, gJ[3] = {0, 0, 0}, gWI[LKB_NW * 3], gWJ[LKB_NW * 3];
   if (GRAD)
 #pragma unroll
     for (int c = 0; c < LKB_NW * 3; ++c) gWI[c] = gWJ[c] = 0;
-  lkb_pair<Real, GRAD>(I, J, WI, WJ, sep, pp, po, k, e, w, gI, gJ, gWI, gWJ);
-#pragma unroll
-  for (int c = 0; c < 4; ++c) e4[c] += e[c];
+  lkb_pair<Real, GRAD>(I, J, WI, WJ, sep, pp, po, ev, out.v, w.v, gI, gJ, gWI, gWJ);
   if (GRAD) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      if (gI[c] != Real(0)) atomicAdd(&s.dcoords[3 * rp + c], gI[c]);
-      if (gJ[c] != Real(0)) atomicAdd(&s.dcoords[3 * ro + c], gJ[c]);
+      if (gI[c] != Real(0)) atomicAdd(&ev.dcoords[3 * rp + c], gI[c]);
+      if (gJ[c] != Real(0)) atomicAdd(&ev.dcoords[3 * ro + c], gJ[c]);
     }
 #pragma unroll
     for (int c = 0; c < LKB_NW * 3; ++c) {
-      if (gWI[c] != Real(0)) atomicAdd(&k.dwaters_out[rp * LKB_NW * 3 + c], gWI[c]);
-      if (gWJ[c] != Real(0)) atomicAdd(&k.dwaters_out[ro * LKB_NW * 3 + c], gWJ[c]);
+      if (gWI[c] != Real(0)) atomicAdd(&ev.dwaters[rp * LKB_NW * 3 + c], gWI[c]);
+      if (gWJ[c] != Real(0)) atomicAdd(&ev.dwaters[ro * LKB_NW * 3 + c], gWJ[c]);
     }
   }
+  return out;
 }
 
 template <typename Real, bool GRAD, bool BLOCK_PAIR>
-__global__ void __launch_bounds__(256) lkb_score_kernel(ScoreArgs<Real> s, LkbArgs<Real> k, int items_per_ticket) {
+__global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS) lkb_score_kernel(ScoreArgs<Real> s, LkbArgs<Real> k, int items_per_ticket) {
   __shared__ LkbQueue queues[8][2];  // [warp][plain, bridged]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   LkbQueue* const qs = queues[warp];
@@ -714,6 +743,18 @@ __global__ void __launch_bounds__(256) lkb_score_kernel(ScoreArgs<Real> s, LkbAr
   // pairs evaluated (warp-uniform)
   unsigned long long n_bp = 0, n_pairs = 0, n_bridge = 0, n_eval = 0;
   int nq[2] = {0, 0};
+  LkbEval<Real> ev;
+  ev.coords = s.coords;
+  ev.waters = k.waters;
+  ev.par = k.par;
+  ev.dcoords = s.dcoords;
+  ev.dwaters = k.dwaters_out;
+  ev.A = s.A;
+  ev.water_dist = k.water_dist;
+  ev.hbond_dis = k.hbond_dis;
+  ev.hbond_oh = k.hbond_oh;
+  ev.hbond_h = k.hbond_h;
+  ev.max_dis = k.max_dis;
   for (;;) {
     int t = 0;
     if (lane == 0) t = atomicAdd(s.ticket, 1);
@@ -757,11 +798,12 @@ __global__ void __launch_bounds__(256) lkb_score_kernel(ScoreArgs<Real> s, LkbAr
       const int ncp = s.cp_count[i1];
       const int cp_b2 = lane < ncp ? s.cp_b2[i1 * CP_CAP + lane] : -1;
       const int cp_min = lane < ncp ? s.cp_minsep[i1 * CP_CAP + lane] : 6;
-      Real w[4] = {0, 0, 0, 0};
+      Lkb4<Real> w = {{0, 0, 0, 0}};
       if (GRAD && !BLOCK_PAIR)
-        for (int q = 0; q < 4; ++q) w[q] = s.dTdV[(int64_t)q * s.P + p];
+        for (int q = 0; q < 4; ++q) w.v[q] = s.dTdV[(int64_t)q * s.P + p];
       Real acc[4] = {0, 0, 0, 0};
       const int npol1 = k.npol[bt1], nocc1 = k.nocc[bt1], nbr1 = k.nbocc[bt1];
+      const float inv_nocc1 = nocc1 > 0 ? 1.0f / float(nocc1) : 0.0f;
       // evaluates full queues (or, with `all`, everything queued) and
       // shifts what is left to the front
       auto pump = [&](bool all, Real* e4) {
@@ -780,7 +822,8 @@ __global__ void __launch_bounds__(256) lkb_score_kernel(ScoreArgs<Real> s, LkbAr
           }
           LkbQueue& q = qs[which];
           __syncwarp();
-          lkb_drain<Real, GRAD>(s, k, q, n, lane, w, e4);
+          const Lkb4<Real> got = lkb_drain<Real, GRAD>(ev, q, n, lane, w);
+          for (int c = 0; c < 4; ++c) e4[c] += got.v[c];
           const int rest = nq[which] - n;
           int a = 0, b = 0, c = 0, d = 0, e = 0;
           if (lane < rest) {
@@ -817,12 +860,13 @@ __global__ void __launch_bounds__(256) lkb_score_kernel(ScoreArgs<Real> s, LkbAr
           const int nc1 = striking ? s.bt_n_conn[bt1] : 0, nc2 = striking ? s.bt_n_conn[bt2] : 0;
           const int64_t pair_o = (int64_t)i1 * s.B + b2;
           if (GRAD && BLOCK_PAIR)
-            for (int q = 0; q < 4; ++q) w[q] = s.dTdV[(int64_t)q * stride + pair_o];
+            for (int q = 0; q < 4; ++q) w.v[q] = s.dTdV[(int64_t)q * stride + pair_o];
           Real e4[4] = {0, 0, 0, 0};
           const int npol2 = k.npol[bt2], nocc2 = k.nocc[bt2], nbr2 = k.nbocc[bt2];
           const int no = intra ? nocc1 : nocc2;
           const int n01 = npol1 * no;
           const int total = intra ? n01 : n01 + nocc1 * npol2;
+          const float inv_no = no > 0 ? 1.0f / float(no) : 0.0f;
           n_bp += 1;
           n_pairs += total;
           // filter: bond separation, distance, waters; queue what is in reach
@@ -833,7 +877,9 @@ __global__ void __launch_bounds__(256) lkb_score_kernel(ScoreArgs<Real> s, LkbAr
             if (idx < total) {
               int ap, ao, btp, bto, offp, offo, y;
               if (idx < n01) {
-                const int x = idx / no;
+                // idx / no in float: exact for these sizes (idx < 2^16,
+                // no <= 256: the error is far below 0.5 / no)
+                const int x = (int)((float(idx) + 0.5f) * inv_no);
                 y = idx - x * no;
                 btp = bt1;
                 bto = intra ? bt1 : bt2;
@@ -848,7 +894,7 @@ __global__ void __launch_bounds__(256) lkb_score_kernel(ScoreArgs<Real> s, LkbAr
                 bridged = y < (intra ? nbr1 : nbr2);
               } else {
                 const int j = idx - n01;
-                const int x = j / nocc1;
+                const int x = (int)((float(j) + 0.5f) * inv_nocc1);
                 y = j - x * nocc1;
                 btp = bt2;
                 bto = bt1;
