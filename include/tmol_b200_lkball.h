@@ -30,7 +30,7 @@ extern "C" {
 
 typedef struct tmol_b200_ljlk_plan tmol_b200_lkball_plan;
 
-/* The static arguments of both ops (compiled.ops.cpp:28-64, 530-600):
+/* The static arguments of both ops (compiled.ops.cpp:27-64, 363-398):
  *   P = n_poses, B = max_n_blocks, nbt = n_block_types,
  *   A = max_n_block_atoms, C = max_n_conn, NT = max_n_tiles (ceil(A/32)),
  *   NB = max_n_all_bonds. */
@@ -89,9 +89,9 @@ typedef struct {
 } tmol_b200_lkball_inputs;
 
 /* Replaces the per-call setup of both dispatches (gen_pose_waters.impl.hh:
- * 30-100, lk_ball_pose_score.impl.hh:385-560): validates the tables and
+ * 35-130, lk_ball_pose_score.impl.hh:362-470): validates the tables and
  * resolves every water's building atoms (acceptor bases across block
- * connections, identification.hh:27-160) once.
+ * connections, tmol/score/hbond/identification.hh:26-168) once.
  *
  * A plan serves water generation when bt_all_bonds is given (with the other
  * water-generation tables), scoring when bt_tile_pol_occ_inds is given
@@ -105,23 +105,24 @@ int tmol_b200_lkball_plan_create(const tmol_b200_lkball_inputs* inputs, int real
 int tmol_b200_lkball_plan_destroy(tmol_b200_lkball_plan* plan);
 
 /* gen_pose_waters forward (GeneratePoseWaters::forward,
- * gen_pose_waters.impl.hh:30-250): waters [n_atoms, 4, 3], overwritten. */
+ * gen_pose_waters.impl.hh:35-230): waters [n_atoms, 4, 3], overwritten. */
 int tmol_b200_lkball_waters(tmol_b200_lkball_plan* plan, const void* coords, void* waters, void* stream);
 
-/* gen_pose_waters backward (GeneratePoseWaters::backward): dcoords
+/* gen_pose_waters backward (GeneratePoseWaters::backward,
+ * gen_pose_waters.impl.hh:231-440): dcoords
  * [n_atoms, 3] += the adjoint of dL/dwaters [n_atoms, 4, 3] (accumulated,
  * not overwritten). */
 int tmol_b200_lkball_waters_backward(tmol_b200_lkball_plan* plan, const void* coords,
                                      const void* dwaters, void* dcoords, void* stream);
 
 /* lk_ball_pose_score forward (LKBallPoseScoreDispatch::forward,
- * lk_ball_pose_score.impl.hh:385-700): energies [4, P] (block_pair == 0)
+ * lk_ball_pose_score.impl.hh:362-681): energies [4, P] (block_pair == 0)
  * or [4, P, B, B], overwritten; block_neighbors [P, B, B] or NULL. */
 int tmol_b200_lkball_forward(tmol_b200_lkball_plan* plan, const void* coords, const void* waters,
                              int block_pair, void* energies, int32_t* block_neighbors, void* stream);
 
 /* lk_ball_pose_score backward as a recompute adjoint (the reference's
- * block-pair backward, lk_ball_pose_score.impl.hh:1040-1400): with
+ * backward, lk_ball_pose_score.impl.hh:682-1004): with
  * dTdV [4, P] or [4, P, B, B], dcoords [n_atoms, 3] and dwaters
  * [n_atoms, 4, 3] are overwritten with the gradients of sum dTdV * E with
  * respect to the coordinates (directly) and the waters. */

@@ -1,6 +1,6 @@
 // LK-ball on B200: water sites, water building and its adjoint, and the
 // four-term polar / occluder pair potential (tmol/score/lk_ball/potentials:
-// water.hh, lk_ball.hh; acceptor bases hbond/identification.hh:27-160).
+// water.hh, lk_ball.hh; acceptor bases tmol/score/hbond/identification.hh:26-168).
 // Included by ljlk.cu inside namespace tmol_b200, after ScoreArgs and the
 // LJ/LK kernels, whose plan (neighbour detection, count-pair tables, work
 // items) the LK-ball kernels share.
@@ -103,7 +103,7 @@ __device__ __forceinline__ void lkb_range(const LkbTables& t, int A, LkbAtom x, 
   hi = r[1] > t.NB ? t.NB : r[1];
 }
 
-// acceptor bases (identification.hh:35-148); false when the water frame
+// acceptor bases (identification.hh:32-150); false when the water frame
 // is undefined
 __device__ inline bool lkb_bases(const LkbTables& t, const int* blk_bt, int p, int B, int C, int A, LkbAtom a,
                                  int hyb, LkbAtom& b, LkbAtom& b0) {
@@ -169,7 +169,9 @@ __device__ __forceinline__ int lkb_row(const int* blk_off, int p, int B, LkbAtom
   return blk_off[p * B + x.block] + x.atom;
 }
 
-// One thread per block: its water sites (gen_pose_waters.impl.hh:140-200).
+// One thread per block: its water sites, the donor and acceptor waters the
+// reference builds per rotamer (gen_pose_waters.impl.hh:112-175; water.hh:
+// 332-445).
 template <typename Real>
 __global__ void lkb_sites_kernel(const int* blk_bt, const int* blk_off, const int* bt_n_atoms, int P, int B, int C,
                                  int A, LkbTables t,

@@ -2,13 +2,13 @@
 
 ``gen_pose_waters(coords, <32 static arguments>)`` takes exactly the
 arguments of ``torch.ops.tmol_lk_ball.gen_pose_waters``
-(``tmol/score/lk_ball/potentials/compiled.ops.cpp:25-64``) and returns the
+(``tmol/score/lk_ball/potentials/compiled.ops.cpp:25-360``) and returns the
 waters ``[n_atoms, 4, 3]`` (NaN in unused slots); gradients flow back to
 ``coords`` through the water-building adjoint.
 
 ``lk_ball_pose_score(coords, <25 static arguments>, water_coords,
 output_block_pair_energies)`` is ``torch.ops.tmol_lk_ball.lk_ball_pose_score``
-(``compiled.ops.cpp:370-600, 843-907``): ``(scores, block_neighbors)``,
+(``compiled.ops.cpp:361-603, 843-907``): ``(scores, block_neighbors)``,
 scores ``[4, P]`` (lk_ball_iso, lk_ball, lk_bridge, lk_bridge_uncpl) or
 ``[4, P, B, B]``; gradients flow to ``coords`` and ``water_coords``.
 
