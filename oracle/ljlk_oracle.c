@@ -1236,6 +1236,12 @@ static bcat_t lkb_bonded(const oracle_inputs_t* in, const lkb_inputs_t* k, int p
   }
   r.block = t[0];
   r.bt = in->first_rot_block_type[(size_t)p * in->B + t[0]];
+  if (r.bt < 0) {
+    /* a partner block without a rotamer (a rotamer set may leave blocks
+     * out): the bond does not resolve */
+    r.block = r.atom = -1;
+    return r;
+  }
   r.atom = in->bt_conn_atom[(size_t)r.bt * in->C + t[1]];
   return r;
 }
@@ -1409,10 +1415,21 @@ typedef struct {
   real tor, ang;
 } lkb_site_t;
 
-/* the site of water slot `w` of pose-atom (p, b, atom), or kind 0 */
-static void lkb_sites_for_block(const oracle_inputs_t* in, const lkb_inputs_t* k, int p, int b,
-                                lkb_site_t* sites /* [n_atoms][4] */) {
-  int bt = in->first_rot_block_type[(size_t)p * in->B + b];
+/* the coordinate row of x for waters built on rotamer `rot` (block b at
+ * offset off): its own block from the rotamer's coordinates, other blocks
+ * from their first rotamer's (water.hh:318-327) */
+static size_t lkb_row(const oracle_inputs_t* in, int p, int b, size_t off, bcat_t x) {
+  return x.block == b ? off + x.atom : lkb_atom_row(in, p, x);
+}
+
+/* the site of water slot `w` of each atom of rotamer `rot`, or kind 0
+ * (gen_pose_waters.impl.hh:112-175, per rotamer as the reference runs it;
+ * in the pose op each block's one rotamer) */
+static void lkb_sites_for_rot(const oracle_inputs_t* in, const lkb_inputs_t* k, int rot,
+                              lkb_site_t* sites /* [n_atoms][4] */) {
+  int bt = in->block_type_ind_for_rot[rot];
+  int p = in->pose_ind_for_rot[rot], b = in->block_ind_for_rot[rot];
+  size_t off = in->rot_coord_offset[rot];
   int n = in->bt_n_atoms[bt];
   for (int i = 0; i < n * LKB_NW; ++i) sites[i].kind = 0;
   for (int t = 0; t < k->NT; ++t) {
@@ -1424,8 +1441,8 @@ static void lkb_sites_for_block(const oracle_inputs_t* in, const lkb_inputs_t* k
       bcat_t dh = {b, bt, D}, hh = {b, bt, H};
       lkb_site_t* s = &sites[D * LKB_NW + which];
       s->kind = 1;
-      s->rowA = lkb_atom_row(in, p, dh);
-      s->rowB = lkb_atom_row(in, p, hh);
+      s->rowA = lkb_row(in, p, b, off, dh);
+      s->rowB = lkb_row(in, p, b, off, hh);
     }
     for (int q = 0; q < k->tile_n_acc[tb]; ++q) {
       int Aat = t * TILE + k->tile_acc_inds[tb * TILE + q];
@@ -1441,9 +1458,9 @@ static void lkb_sites_for_block(const oracle_inputs_t* in, const lkb_inputs_t* k
         lkb_site_t* s = &sites[Aat * LKB_NW + w + nH];
         s->kind = 2;
         s->hyb = hyb;
-        s->rowA = lkb_atom_row(in, p, A);
-        s->rowB = lkb_atom_row(in, p, Bb);
-        s->rowB0 = lkb_atom_row(in, p, B0);
+        s->rowA = lkb_row(in, p, b, off, A);
+        s->rowB = lkb_row(in, p, b, off, Bb);
+        s->rowB0 = lkb_row(in, p, b, off, B0);
         s->tor = tors[w];
         s->ang = ang;
       }
@@ -1475,20 +1492,18 @@ int oracle_lkb_waters(const oracle_inputs_t* in, const lkb_inputs_t* k, real* W)
   for (size_t i = 0; i < (size_t)in->n_atoms * LKB_NW * 3; ++i) W[i] = (real)NAN;
   lkb_site_t* sites = (lkb_site_t*)malloc(sizeof(lkb_site_t) * (size_t)in->A * LKB_NW);
   if (!sites) return 2;
-  for (int p = 0; p < in->P; ++p)
-    for (int b = 0; b < in->B; ++b) {
-      int bt = in->first_rot_block_type[(size_t)p * in->B + b];
-      if (bt < 0) continue;
-      lkb_sites_for_block(in, k, p, b, sites);
-      int rot = in->rot_offset_for_block[(size_t)p * in->B + b];
-      size_t off = in->rot_coord_offset[rot];
-      for (int a = 0; a < in->bt_n_atoms[bt]; ++a)
-        for (int w = 0; w < LKB_NW; ++w) {
-          frame_t f;
-          if (sites[a * LKB_NW + w].kind)
-            lkb_site_water(in, k, &sites[a * LKB_NW + w], W + ((off + a) * LKB_NW + w) * 3, &f);
-        }
-    }
+  for (int rot = 0; rot < in->n_rots; ++rot) {
+    int bt = in->block_type_ind_for_rot[rot];
+    if (bt < 0) continue;
+    lkb_sites_for_rot(in, k, rot, sites);
+    size_t off = in->rot_coord_offset[rot];
+    for (int a = 0; a < in->bt_n_atoms[bt]; ++a)
+      for (int w = 0; w < LKB_NW; ++w) {
+        frame_t f;
+        if (sites[a * LKB_NW + w].kind)
+          lkb_site_water(in, k, &sites[a * LKB_NW + w], W + ((off + a) * LKB_NW + w) * 3, &f);
+      }
+  }
   free(sites);
   return 0;
 }
@@ -1676,19 +1691,150 @@ static int lkb_lists(const oracle_inputs_t* in, const lkb_inputs_t* k, int bt, i
   return no;
 }
 
+/* scratch for the polar / occluder lists of the two sides of a pair */
+typedef struct {
+  int *pol1, *occ1, *pol2, *occ2;
+  const real **ppar1, **opar1, **ppar2, **opar2;
+  void* mem;
+} lkb_lists_t;
+
+static int lkb_lists_alloc(lkb_lists_t* L, int A) {
+  int* ib = (int*)malloc(sizeof(int) * 4 * (size_t)(A + 1));
+  const real** pb = (const real**)malloc(sizeof(real*) * 4 * (size_t)(A + 1));
+  if (!ib || !pb) {
+    free(ib);
+    free((void*)pb);
+    return 0;
+  }
+  L->pol1 = ib, L->occ1 = ib + (A + 1), L->pol2 = ib + 2 * (A + 1), L->occ2 = ib + 3 * (A + 1);
+  L->ppar1 = pb, L->opar1 = pb + (A + 1), L->ppar2 = pb + 2 * (A + 1), L->opar2 = pb + 3 * (A + 1);
+  L->mem = pb;
+  return 1;
+}
+
+static void lkb_lists_free(lkb_lists_t* L) {
+  free(L->pol1);
+  free(L->mem);
+}
+
+/* Every polar / occluder pair of the rotamer pair in c (one side's polars
+ * against the other side's occluders, both ways; within one rotamer,
+ * ordered pairs of distinct atoms; lk_ball.hh:1270-1360): energies added
+ * to e4[4]; with g4, the adjoint of g4 . E added to dx (directly) and gW
+ * (the waters). */
+static void lkb_eval_ctx(const oracle_inputs_t* in, const lkb_inputs_t* k, const real* W, const pair_ctx_t* c,
+                         lkb_lists_t* L, const real* g4, real* e4, real* dx, real* gW) {
+  const int same = c->rot1 == c->rot2;
+  int np1, np2;
+  int no1 = lkb_lists(in, k, c->bt1, L->pol1, L->occ1, &np1, L->ppar1, L->opar1);
+  int no2 = lkb_lists(in, k, c->bt2, L->pol2, L->occ2, &np2, L->ppar2, L->opar2);
+  for (int side = 0; side < 2; ++side) {
+    if (same && side == 1) break;
+    const int* pol = side ? L->pol2 : L->pol1;
+    const real** ppar = side ? L->ppar2 : L->ppar1;
+    int npol = side ? np2 : np1;
+    const int* occ = same ? L->occ1 : (side ? L->occ1 : L->occ2);
+    const real** opar = same ? L->opar1 : (side ? L->opar1 : L->opar2);
+    int nocc = same ? no1 : (side ? no1 : no2);
+    size_t offp = side ? c->off2 : c->off1, offo = same ? c->off1 : (side ? c->off1 : c->off2);
+    for (int x = 0; x < npol; ++x)
+      for (int y = 0; y < nocc; ++y) {
+        int ap = pol[x], ao = occ[y];
+        if (same && ap == ao) continue;
+        int sep;
+        if (same)
+          sep = in->bt_path_distance[((size_t)c->bt1 * in->A + ap) * in->A + ao];
+        else
+          sep = side ? inter_separation(in, c, ao, ap) : inter_separation(in, c, ap, ao);
+        size_t rp = offp + ap, ro = offo + ao;
+        real I[3], J[3], e[4];
+        v3_load(in->coords, rp, I);
+        v3_load(in->coords, ro, J);
+        lkb_params_t pi, pj;
+        memcpy(&pi, ppar[x], sizeof(pi));
+        memcpy(&pj, opar[y], sizeof(pj));
+        real gI[3] = {0, 0, 0}, gJ[3] = {0, 0, 0}, gWI[LKB_NW * 3] = {0}, gWJ[LKB_NW * 3] = {0};
+        lkb_pair(I, J, W + rp * LKB_NW * 3, W + ro * LKB_NW * 3, sep, &pi, &pj, k, e, g4, gI, gJ, gWI, gWJ);
+        for (int t = 0; t < 4; ++t) e4[t] += e[t];
+        if (g4) {
+          for (int i = 0; i < 3; ++i) {
+            dx[3 * rp + i] += gI[i];
+            dx[3 * ro + i] += gJ[i];
+          }
+          for (int i = 0; i < LKB_NW * 3; ++i) {
+            gW[rp * LKB_NW * 3 + i] += gWI[i];
+            gW[ro * LKB_NW * 3 + i] += gWJ[i];
+          }
+        }
+      }
+  }
+}
+
+/* The waters' adjoint onto the atoms that place them: dx += d(waters)/dx^T
+ * gW (water.hh:412-600), every rotamer's waters. */
+static int lkb_waters_adjoint(const oracle_inputs_t* in, const lkb_inputs_t* k, const real* gW, real* dx) {
+  lkb_site_t* sites = (lkb_site_t*)malloc(sizeof(lkb_site_t) * (size_t)(in->A + 1) * LKB_NW);
+  if (!sites) return 2;
+  for (int rot = 0; rot < in->n_rots; ++rot) {
+    int bt = in->block_type_ind_for_rot[rot];
+    if (bt < 0) continue;
+    lkb_sites_for_rot(in, k, rot, sites);
+    size_t off = in->rot_coord_offset[rot];
+    for (int a = 0; a < in->bt_n_atoms[bt]; ++a)
+      for (int w = 0; w < LKB_NW; ++w) {
+        const lkb_site_t* s = &sites[a * LKB_NW + w];
+        if (!s->kind) continue;
+        const real* g = gW + ((off + a) * LKB_NW + w) * 3;
+        if (g[0] == 0 && g[1] == 0 && g[2] == 0) continue;
+        real Av[3], Bv[3];
+        v3_load(in->coords, s->rowA, Av);
+        v3_load(in->coords, s->rowB, Bv);
+        if (s->kind == 1) {
+          real h[3] = {Bv[0] - Av[0], Bv[1] - Av[1], Bv[2] - Av[2]};
+          real nh = rsqrt_(v3_dot(h, h));
+          real n[3] = {h[0] / nh, h[1] / nh, h[2] / nh};
+          real gn[3] = {k->water_dist * g[0], k->water_dist * g[1], k->water_dist * g[2]};
+          real sdot = v3_dot(n, gn);
+          for (int i = 0; i < 3; ++i) {
+            real gh = (gn[i] - n[i] * sdot) / nh;
+            dx[3 * s->rowA + i] += g[i] - gh;
+            dx[3 * s->rowB + i] += gh;
+          }
+          continue;
+        }
+        real B0v[3], Bm[3];
+        v3_load(in->coords, s->rowB0, B0v);
+        for (int i = 0; i < 3; ++i) Bm[i] = s->hyb == 3 ? (Bv[i] + B0v[i]) / 2 : Bv[i];
+        frame_t f;
+        lkb_frame(Av, Bm, B0v, k->water_dist, s->ang, s->tor, &f);
+        real gA[3] = {0, 0, 0}, gB[3] = {0, 0, 0}, gC[3] = {0, 0, 0};
+        lkb_build_vjp(&f, g, gA, gB, gC);
+        for (int i = 0; i < 3; ++i) {
+          dx[3 * s->rowA + i] += gA[i];
+          if (s->hyb == 3) {
+            dx[3 * s->rowB + i] += gB[i] / 2;
+            dx[3 * s->rowB0 + i] += gB[i] / 2;
+          } else {
+            dx[3 * s->rowB + i] += gB[i];
+          }
+          dx[3 * s->rowB0 + i] += gC[i];
+        }
+      }
+  }
+  free(sites);
+  return 0;
+}
+
 /* lk_ball_pose_score, whole-pose: E [4][P]; with wts [4][P] the gradient of
  * sum_t wts[t][p] E[t][p] w.r.t. the coordinates (through the waters) goes
  * to dx [n_atoms][3]; nbr [P][B][B] gets the block-neighbour matrix. */
 int oracle_lkb_pose_scores(const oracle_inputs_t* in, const lkb_inputs_t* k, const real* W, real* E,
                            const real* wts, real* dx, int32_t* nbr) {
-  const int P = in->P, B = in->B, A = in->A;
+  const int P = in->P, B = in->B;
   real* spheres = (real*)malloc(sizeof(real) * 4 * ((size_t)P * B + 1));
-  int* pol1 = (int*)malloc(sizeof(int) * 4 * (size_t)(A + 1));
-  const real** par1 = (const real**)malloc(sizeof(real*) * 4 * (size_t)(A + 1));
   real* gW = dx ? (real*)calloc((size_t)in->n_atoms * LKB_NW * 3 + 1, sizeof(real)) : NULL;
-  if (!spheres || !pol1 || !par1 || (dx && !gW)) return 2;
-  int *occ1 = pol1 + (A + 1), *pol2 = pol1 + 2 * (A + 1), *occ2 = pol1 + 3 * (A + 1);
-  const real **opar1 = par1 + (A + 1), **ppar2 = par1 + 2 * (A + 1), **opar2 = par1 + 3 * (A + 1);
+  lkb_lists_t L;
+  if (!spheres || (dx && !gW) || !lkb_lists_alloc(&L, in->A)) return 2;
   compute_spheres(in, spheres);
   detect_neighbors(in, spheres, nbr);
   for (size_t i = 0; i < (size_t)4 * P; ++i) E[i] = 0;
@@ -1700,114 +1846,61 @@ int oracle_lkb_pose_scores(const oracle_inputs_t* in, const lkb_inputs_t* k, con
         if (!nbr[((size_t)p * B + b1) * B + b2]) continue;
         pair_ctx_t c;
         if (!setup_pair(in, p, b1, b2, &c)) continue;
-        int np1, np2;
-        int no1 = lkb_lists(in, k, c.bt1, pol1, occ1, &np1, par1, opar1);
-        int no2 = lkb_lists(in, k, c.bt2, pol2, occ2, &np2, ppar2, opar2);
-        real g4[4];
-        const real* gp = NULL;
-        if (dx) {
+        real g4[4], e4[4] = {0, 0, 0, 0};
+        if (dx)
           for (int t = 0; t < 4; ++t) g4[t] = wts[(size_t)t * P + p];
-          gp = g4;
-        }
-        /* (polar of side s, occluder of the other side) */
-        for (int side = 0; side < 2; ++side) {
-          if (b1 == b2 && side == 1) break;
-          const int* pol = side ? pol2 : pol1;
-          const real** ppar = side ? ppar2 : par1;
-          int npol = side ? np2 : np1;
-          const int* occ = (b1 == b2) ? occ1 : (side ? occ1 : occ2);
-          const real** opar = (b1 == b2) ? opar1 : (side ? opar1 : opar2);
-          int nocc = (b1 == b2) ? no1 : (side ? no1 : no2);
-          int offp = side ? c.off2 : c.off1, offo = (b1 == b2) ? c.off1 : (side ? c.off1 : c.off2);
-          for (int x = 0; x < npol; ++x)
-            for (int y = 0; y < nocc; ++y) {
-              int ap = pol[x], ao = occ[y];
-              if (b1 == b2 && ap == ao) continue;
-              int sep;
-              if (b1 == b2)
-                sep = in->bt_path_distance[((size_t)c.bt1 * A + ap) * A + ao];
-              else
-                sep = side ? inter_separation(in, &c, ao, ap) : inter_separation(in, &c, ap, ao);
-              size_t rp = (size_t)offp + ap, ro = (size_t)offo + ao;
-              real I[3], J[3], e[4];
-              v3_load(in->coords, rp, I);
-              v3_load(in->coords, ro, J);
-              lkb_params_t pi, pj;
-              memcpy(&pi, ppar[x], sizeof(pi));
-              memcpy(&pj, opar[y], sizeof(pj));
-              real gI[3] = {0, 0, 0}, gJ[3] = {0, 0, 0}, gWI[LKB_NW * 3] = {0}, gWJ[LKB_NW * 3] = {0};
-              lkb_pair(I, J, W + rp * LKB_NW * 3, W + ro * LKB_NW * 3, sep, &pi, &pj, k, e, gp, gI, gJ, gWI,
-                       gWJ);
-              for (int t = 0; t < 4; ++t) E[(size_t)t * P + p] += e[t];
-              if (dx) {
-                for (int i = 0; i < 3; ++i) {
-                  dx[3 * rp + i] += gI[i];
-                  dx[3 * ro + i] += gJ[i];
-                }
-                for (int i = 0; i < LKB_NW * 3; ++i) {
-                  gW[rp * LKB_NW * 3 + i] += gWI[i];
-                  gW[ro * LKB_NW * 3 + i] += gWJ[i];
-                }
-              }
-            }
-        }
+        lkb_eval_ctx(in, k, W, &c, &L, dx ? g4 : NULL, e4, dx, gW);
+        for (int t = 0; t < 4; ++t) E[(size_t)t * P + p] += e4[t];
       }
-  if (dx) {
-    /* the waters' adjoint onto the atoms that place them (water.hh:412-600) */
-    lkb_site_t* sites = (lkb_site_t*)malloc(sizeof(lkb_site_t) * (size_t)A * LKB_NW);
-    for (int p = 0; p < P && sites; ++p)
-      for (int b = 0; b < B; ++b) {
-        int bt = in->first_rot_block_type[(size_t)p * B + b];
-        if (bt < 0) continue;
-        lkb_sites_for_block(in, k, p, b, sites);
-        int rot = in->rot_offset_for_block[(size_t)p * B + b];
-        size_t off = in->rot_coord_offset[rot];
-        for (int a = 0; a < in->bt_n_atoms[bt]; ++a)
-          for (int w = 0; w < LKB_NW; ++w) {
-            const lkb_site_t* s = &sites[a * LKB_NW + w];
-            if (!s->kind) continue;
-            const real* g = gW + ((off + a) * LKB_NW + w) * 3;
-            if (g[0] == 0 && g[1] == 0 && g[2] == 0) continue;
-            real Av[3], Bv[3];
-            v3_load(in->coords, s->rowA, Av);
-            v3_load(in->coords, s->rowB, Bv);
-            if (s->kind == 1) {
-              real h[3] = {Bv[0] - Av[0], Bv[1] - Av[1], Bv[2] - Av[2]};
-              real nh = rsqrt_(v3_dot(h, h));
-              real n[3] = {h[0] / nh, h[1] / nh, h[2] / nh};
-              real gn[3] = {k->water_dist * g[0], k->water_dist * g[1], k->water_dist * g[2]};
-              real sdot = v3_dot(n, gn);
-              for (int i = 0; i < 3; ++i) {
-                real gh = (gn[i] - n[i] * sdot) / nh;
-                dx[3 * s->rowA + i] += g[i] - gh;
-                dx[3 * s->rowB + i] += gh;
-              }
-              continue;
+  int rc = dx ? lkb_waters_adjoint(in, k, gW, dx) : 0;
+  free(spheres);
+  lkb_lists_free(&L);
+  free(gW);
+  return rc;
+}
+
+/* lk_ball_rotamer_score (LKBallRotamerScoreDispatch, lk_ball_pose_score.impl.hh:
+ * 1005-1380): the four energies E [4][n] of the n rotamer pairs that
+ * oracle_ljlk_rotamer_count dispatched (nbr as it returned), in its order,
+ * with their (pose, rot1, rot2) in idx [3][n]; with dTdV [4][n], dx
+ * [n_atoms][3] gets the gradient of sum dTdV * E through the waters. */
+int oracle_lkb_rotamer_scores(const oracle_inputs_t* in, const lkb_inputs_t* k, const real* W,
+                              const int32_t* nbr, int64_t n, real* E, int32_t* idx, const real* dTdV, real* dx) {
+  const int P = in->P, B = in->B;
+  real* gW = dx ? (real*)calloc((size_t)in->n_atoms * LKB_NW * 3 + 1, sizeof(real)) : NULL;
+  lkb_lists_t L;
+  if ((dx && !gW) || !lkb_lists_alloc(&L, in->A)) return 2;
+  if (dx)
+    for (size_t i = 0; i < (size_t)in->n_atoms * 3; ++i) dx[i] = 0;
+  int64_t q = 0;
+  for (int p = 0; p < P; ++p)
+    for (int b1 = 0; b1 < B; ++b1)
+      for (int b2 = b1; b2 < B; ++b2) {
+        if (!nbr[((size_t)p * B + b1) * B + b2]) continue;
+        int n1 = in->n_rots_for_block[p * B + b1], n2 = in->n_rots_for_block[p * B + b2];
+        int o1 = in->rot_offset_for_block[p * B + b1], o2 = in->rot_offset_for_block[p * B + b2];
+        if (o1 < 0 || o2 < 0) continue;
+        for (int i = 0; i < n1; ++i)
+          for (int j = 0; j < (b1 == b2 ? 1 : n2); ++j) {
+            int r1 = o1 + i, r2 = b1 == b2 ? o1 + i : o2 + j;
+            if (q >= n) return 3;
+            idx[q] = p;
+            idx[n + q] = r1;
+            idx[2 * n + q] = r2;
+            real e4[4] = {0, 0, 0, 0}, g4[4];
+            pair_ctx_t c;
+            if (setup_rot_pair(in, p, b1, b2, r1, r2, &c)) {
+              if (dx)
+                for (int t = 0; t < 4; ++t) g4[t] = dTdV[(size_t)t * n + q];
+              lkb_eval_ctx(in, k, W, &c, &L, dx ? g4 : NULL, e4, dx, gW);
             }
-            real B0v[3], Bm[3];
-            v3_load(in->coords, s->rowB0, B0v);
-            for (int i = 0; i < 3; ++i) Bm[i] = s->hyb == 3 ? (Bv[i] + B0v[i]) / 2 : Bv[i];
-            frame_t f;
-            lkb_frame(Av, Bm, B0v, k->water_dist, s->ang, s->tor, &f);
-            real gA[3] = {0, 0, 0}, gB[3] = {0, 0, 0}, gC[3] = {0, 0, 0};
-            lkb_build_vjp(&f, g, gA, gB, gC);
-            for (int i = 0; i < 3; ++i) {
-              dx[3 * s->rowA + i] += gA[i];
-              if (s->hyb == 3) {
-                dx[3 * s->rowB + i] += gB[i] / 2;
-                dx[3 * s->rowB0 + i] += gB[i] / 2;
-              } else {
-                dx[3 * s->rowB + i] += gB[i];
-              }
-              dx[3 * s->rowB0 + i] += gC[i];
-            }
+            for (int t = 0; t < 4; ++t) E[(size_t)t * n + q] = e4[t];
+            ++q;
           }
       }
-    free(sites);
-  }
-  free(spheres);
-  free(pol1);
-  free(par1);
+  int rc = q == n ? 0 : 3;
+  if (!rc && dx) rc = lkb_waters_adjoint(in, k, gW, dx);
+  lkb_lists_free(&L);
   free(gW);
-  return 0;
+  return rc;
 }

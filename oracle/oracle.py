@@ -274,6 +274,31 @@ class OracleCall:
         assert rc == 0
         return E, dx, nbr
 
+    def lkb_rotamer_scores(self, W, dTdV=None):
+        """lk_ball_rotamer_score on a rotamer set: (E [4, n], indices [3, n]
+        (pose, rot1, rot2), block neighbours [P, B, B], and with dTdV
+        [4, n] the gradient of sum dTdV * E through the waters [N, 3])."""
+        lib = _lib(self.f64)
+        nbr = numpy.zeros((self.P, self.B, self.B), dtype=numpy.int32)
+        n = lib.oracle_ljlk_rotamer_count(ctypes.byref(self.s), self._ptr(nbr))
+        assert n >= 0
+        E = numpy.zeros((4, n), dtype=self.np_real)
+        idx = numpy.zeros((3, n), dtype=numpy.int32)
+        W = numpy.ascontiguousarray(W, dtype=self.np_real)
+        dx = None
+        wp = ctypes.c_void_p(0)
+        if dTdV is not None:
+            w = numpy.ascontiguousarray(numpy.asarray(dTdV, dtype=self.np_real).reshape(4, n))
+            self.keep.append(w)
+            wp = self._ptr(w)
+            dx = numpy.zeros((self.N, 3), dtype=self.np_real)
+        rc = lib.oracle_lkb_rotamer_scores(
+            ctypes.byref(self.s), ctypes.byref(self.k), self._ptr(W), self._ptr(nbr), ctypes.c_int64(n),
+            self._ptr(E), self._ptr(idx), wp, self._ptr(dx) if dx is not None else ctypes.c_void_p(0),
+        )
+        assert rc == 0
+        return E, idx, nbr, dx
+
     def _ptr(self, a):
         return a.ctypes.data_as(ctypes.c_void_p)
 
@@ -460,6 +485,24 @@ def reference_lkball(coords, water_args, score_args, require_gradient=True):
     sa[-2] = W
     E, nbr = ops.lk_ball_pose_score(c, *sa)
     return E, W, c, nbr
+
+
+def reference_lkball_rotamers(coords, water_args, score_args):
+    """The reference CPU LK-ball rotamer op on a rotamer set: waters from
+    gen_pose_waters on the rotamers' coordinates, then lk_ball_rotamer_score;
+    returns (E [4, n], dispatch indices [3, n], waters, coords tensor that
+    requires grad)."""
+    if "lkball_ref" not in _LIBS:
+        torch.ops.load_library(LKBALL_REF_LIB)
+        _LIBS["lkball_ref"] = True
+    ops = torch.ops.tmol_lk_ball
+    c = coords.detach().cpu().reshape(-1, 3).clone().requires_grad_(True)
+    wa = [a.cpu() if isinstance(a, torch.Tensor) else a for a in water_args]
+    sa = [a.cpu() if isinstance(a, torch.Tensor) else a for a in score_args]
+    W = ops.gen_pose_waters(c, *wa)
+    sa[-2] = W
+    E, idx = ops.lk_ball_rotamer_score(c, *sa)
+    return E, idx, W, c
 
 
 def reference_pose_scores(coords, args, require_gradient=True):

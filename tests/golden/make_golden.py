@@ -32,6 +32,13 @@ Writes
                      suite's stored 1ubq LK-ball energies
                      (tmol/tests/data/term_baselines/LKBallEnergyTerm/
                      test_whole_pose_scoring_10.yaml)
+  lkball_rotamers.npz  the reference LK-ball rotamer op (gen_pose_waters on the
+                     rotamers' coordinates, then lk_ball_rotamer_score) on
+                     the rotamer set of rotamers.npz, float32 and float64:
+                     waters, rotamer-pair energies, dispatch indices and the
+                     gradient of sum(w * E) for seeded w
+                     (``make_golden.py <tmol root> lkball_rotamers`` writes
+                     this file alone)
   rotamers.npz       the reference rotamer-score op (ljlk_rotamer_scores) on
                      a seeded rotamer set over a jagged batch of poses: the
                      set itself, the rotamer-pair energies and dispatch
@@ -59,7 +66,12 @@ from tmol_b200.score.elec_energy_term import (  # noqa: E402
     elec_rotamer_score_args,
 )
 from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm, pose_score_args, rotamer_score_args  # noqa: E402
-from tmol_b200.score.lkball_energy_term import LKBallEnergyTerm, score_args, water_gen_args  # noqa: E402
+from tmol_b200.score.lkball_energy_term import (  # noqa: E402
+    LKBallEnergyTerm,
+    rotamer_score_args as lkball_rotamer_score_args,
+    score_args,
+    water_gen_args,
+)
 
 SYN_SIZES = [1, 2, 7, 33, 100]
 SYN_SEEDS = [11, 12, 13, 14, 15]
@@ -197,8 +209,39 @@ def main(ref_root):
         weights=w.numpy(),
         ref_grad=c.grad.numpy(),
     )
-    print("wrote fixtures to", HERE)
+
+
+def lkball_rotamers():
+    """lkball_rotamers.npz (the rotamer set is rebuilt from its seeds, as
+    rotamers.npz stores it)."""
+    ps = synthetic_pose_stack(ROT_SIZES, ROT_SEEDS)
+    rs = synthetic_rotamer_set(ps, **ROT_SET)
+    lterm = LKBallEnergyTerm()
+    out = {}
+    for dt, dn in ((torch.float32, "f32"), (torch.float64, "f64")):
+        wa = water_gen_args(ps, lterm, rs)
+        sa = lkball_rotamer_score_args(ps, rs, lterm, None)
+        wa = [a.to(dt) if isinstance(a, torch.Tensor) and a.is_floating_point() else a for a in wa]
+        sa = [a.to(dt) if isinstance(a, torch.Tensor) and a.is_floating_point() else a for a in sa]
+        E, idx, W, c = O.reference_lkball_rotamers(rs.coords.to(dt), wa, sa)
+        w = torch.tensor(numpy.random.default_rng(11).normal(size=tuple(E.shape)), dtype=dt)
+        (E * w).sum().backward()
+        out.update({
+            f"{dn}_energies": E.detach().numpy(),
+            f"{dn}_waters": W.detach().numpy(),
+            f"{dn}_weights": w.numpy(),
+            f"{dn}_grad": c.grad.numpy(),
+        })
+        out["indices"] = idx.numpy()
+    numpy.savez_compressed(os.path.join(HERE, "lkball_rotamers.npz"), **out)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    only = sys.argv[2] if len(sys.argv) > 2 else None
+    if only == "lkball_rotamers":
+        lkball_rotamers()
+    else:
+        main(root)
+        lkball_rotamers()
+    print("wrote fixtures to", HERE)

@@ -7,7 +7,10 @@
   (fixture: the reference's outputs, tests/golden/lkball.npz);
 - the oracle's waters, four energies and gradient (through the waters)
   against the reference's, float64 to 1e-10, float32 to 1e-5 relative, on
-  1ubq and a synthetic pose; live against the compiled op when present.
+  1ubq and a synthetic pose; live against the compiled op when present;
+- the rotamer op (waters on a rotamer set, lk_ball_rotamer_score): dispatch
+  indices exact, energies, waters and the gradient of a weighted sum against
+  the fixture (tests/golden/lkball_rotamers.npz) and the live op.
 """
 
 import numpy
@@ -71,3 +74,62 @@ def test_oracle_matches_live_reference():
         numpy.testing.assert_allclose(Eo, E.detach().numpy(), rtol=1e-10, atol=1e-10)
         numpy.testing.assert_allclose(dx, c.grad.numpy(), rtol=1e-9, atol=1e-9 * numpy.abs(dx).max())
         assert numpy.array_equal(nbro, nbr.numpy())
+
+
+def rotamer_case():
+    from tests.test_rotamer_oracle import fixture_case
+
+    _, ps, rs = fixture_case()
+    return ps, rs
+
+
+def oracle_rotamers(ps, rs, f64, weights=None):
+    from tmol_b200.score.lkball_energy_term import rotamer_score_args
+
+    lt = LKBallEnergyTerm()
+    dt = torch.float64 if f64 else torch.float32
+    oc = O.OracleCall(rs.coords.to(dt), rotamer_score_args(ps, rs, lt, None), f64=f64, term="lkball",
+                      lkb_water_args=water_gen_args(ps, lt, rs))
+    W = oc.lkb_waters()
+    E, idx, nbr, dx = oc.lkb_rotamer_scores(W, dTdV=weights)
+    return W, E, idx, dx
+
+
+@pytest.mark.parametrize("f64", [False, True])
+def test_rotamer_oracle_matches_reference_fixture(f64):
+    """lk_ball_rotamer_score on the rotamer set of rotamers.npz (some blocks
+    without rotamers, some rotamers of another residue type)."""
+    g = load_golden("lkball_rotamers.npz")
+    ps, rs = rotamer_case()
+    dn = "f64" if f64 else "f32"
+    tol = 1e-10 if f64 else 1e-5
+    W, E, idx, dx = oracle_rotamers(ps, rs, f64, weights=g[f"{dn}_weights"])
+    assert numpy.array_equal(idx, g["indices"])
+    Wr = g[f"{dn}_waters"]
+    assert numpy.array_equal(numpy.isnan(W), numpy.isnan(Wr))
+    numpy.testing.assert_allclose(W[~numpy.isnan(W)], Wr[~numpy.isnan(Wr)], rtol=0, atol=10 * tol if f64 else 2e-4)
+    numpy.testing.assert_allclose(E, g[f"{dn}_energies"], rtol=tol, atol=tol if f64 else 1e-3)
+    gr = g[f"{dn}_grad"]
+    numpy.testing.assert_allclose(dx, gr, rtol=10 * tol, atol=10 * tol * numpy.abs(gr).max())
+
+
+@pytest.mark.skipif(not O.reference_lkball_available(), reason="compiled reference LK-ball op not built")
+def test_rotamer_oracle_matches_live_reference():
+    from tmol_b200.pose.rotamers import synthetic_rotamer_set
+    from tmol_b200.score.lkball_energy_term import rotamer_score_args
+
+    lt = LKBallEnergyTerm()
+    for seed in (8, 9):
+        ps = synthetic_pose_stack([25, 14], [seed, seed + 1], extra_chi_sd=20.0)
+        rs = synthetic_rotamer_set(ps, max_rots=3, mutate_fraction=0.3, seed=seed, skip_fraction=0.2)
+        wa = [a.double() if isinstance(a, torch.Tensor) and a.is_floating_point() else a
+              for a in water_gen_args(ps, lt, rs)]
+        sa = [a.double() if isinstance(a, torch.Tensor) and a.is_floating_point() else a
+              for a in rotamer_score_args(ps, rs, lt, None)]
+        E, idx, _, c = O.reference_lkball_rotamers(rs.coords.double(), wa, sa)
+        w = numpy.random.default_rng(seed).normal(size=tuple(E.shape))
+        (E * torch.tensor(w)).sum().backward()
+        _, Eo, idxo, dx = oracle_rotamers(ps, rs, True, weights=w)
+        assert numpy.array_equal(idxo, idx.numpy())
+        numpy.testing.assert_allclose(Eo, E.detach().numpy(), rtol=1e-10, atol=1e-10)
+        numpy.testing.assert_allclose(dx, c.grad.numpy(), rtol=1e-9, atol=1e-9 * numpy.abs(dx).max())

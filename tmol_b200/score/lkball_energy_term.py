@@ -88,13 +88,40 @@ def _common(pose_stack):
     ]
 
 
-def water_gen_args(pose_stack, term):
+def _rotamer_common(rotamer_set):
+    """A rotamer set's indexing, as tmol's TermRotamerScoringModule passes
+    it (tmol/score/common/scoring_module.py:133-170)."""
+
+    def i32(t):
+        return t if isinstance(t, int) else t.to(torch.int32)
+
+    rs = rotamer_set
+    return [
+        i32(rs.coord_offset_for_rot),
+        i32(rs.pose_ind_for_atom),
+        i32(rs.rot_offset_for_block),
+        i32(rs.first_rot_block_type),
+        i32(rs.block_ind_for_rot),
+        i32(rs.pose_for_rot),
+        i32(rs.block_type_ind_for_rot),
+        i32(rs.n_rots_for_pose),
+        i32(rs.rot_offset_for_pose),
+        i32(rs.n_rots_for_block),
+        i32(rs.rot_offset_for_block),
+        int(rs.max_n_rots_per_pose),
+    ]
+
+
+def water_gen_args(pose_stack, term, rotamer_set=None):
     """gen_pose_waters' argument list minus the coordinates
-    (tmol lk_ball_energy_term.py:245-270, compiled.ops.cpp:28-64)."""
+    (tmol lk_ball_energy_term.py:245-270, compiled.ops.cpp:28-64); with a
+    rotamer set, its indexing in front, as tmol's rotamer scoring calls the
+    op on the rotamers' coordinates (lk_ball_energy_term.py:300-336)."""
     pbt = pose_stack.packed_block_types
     t = packed_lkball_tables(pbt)
     gp, tors = term.water_gen_global_params(pbt, pose_stack.device)
-    return _common(pose_stack) + [
+    common = _common(pose_stack) if rotamer_set is None else _rotamer_common(rotamer_set)
+    return common + [
         pose_stack.inter_residue_connections,
         pbt.n_atoms,
         pbt.n_conn,
@@ -114,6 +141,14 @@ def water_gen_args(pose_stack, term):
         gp,
         *tors,
     ]
+
+
+def rotamer_score_args(pose_stack, rotamer_set, term, water_coords):
+    """lk_ball_rotamer_score's argument list minus the coordinates
+    (lk_ball_energy_term.py:338-358, compiled.ops.cpp:909-976): the rotamer
+    set's indexing, the pose's LK-ball tables, the rotamers' waters and
+    ``output_block_pair_energies=True``."""
+    return _rotamer_common(rotamer_set) + score_args(pose_stack, term, water_coords, True)[12:]
 
 
 def score_args(pose_stack, term, water_coords, block_pair=False):
