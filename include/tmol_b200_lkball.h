@@ -140,6 +140,31 @@ int tmol_b200_lkball_backward(tmol_b200_lkball_plan* plan, const void* coords, c
 int tmol_b200_lkball_energy_and_gradient(tmol_b200_lkball_plan* plan, const void* coords, const void* weights,
                                          void* energies, void* dcoords, void* stream);
 
+/* The rotamer op, lk_ball_rotamer_score (LKBallRotamerScoreDispatch,
+ * lk_ball_pose_score.impl.hh:1005-1380; compiled.ops.cpp:604-842): a plan
+ * over a rotamer set (the inputs' indexing is the set's, n_rots its
+ * rotamers, coordinates and waters its atoms).  Water generation on such a
+ * plan builds every rotamer's waters (gen_pose_waters on the rotamers'
+ * coordinates, as tmol's rotamer scoring calls it), with atoms of other
+ * blocks from those blocks' first rotamers.  count / fill give the
+ * dispatched rotamer pairs (pose, rot1, rot2) and work items as
+ * tmol_b200_ljlk_rotamer_count / _fill do (count synchronises the stream);
+ * forward writes energies [4, n_pairs]; backward overwrites dcoords
+ * [n_atoms, 3] and dwaters [n_atoms, 4, 3] with the gradients of
+ * sum dTdV * E, dTdV [4, n_pairs]. */
+int tmol_b200_lkball_rotamer_plan_create(const tmol_b200_lkball_inputs* inputs, int real_bytes,
+                                         const tmol_b200_ljlk_launch* launch, void* stream,
+                                         tmol_b200_lkball_plan** plan_out);
+int tmol_b200_lkball_rotamer_count(tmol_b200_lkball_plan* plan, const void* coords, int64_t* n_pairs,
+                                   int64_t* n_items, void* stream);
+int tmol_b200_lkball_rotamer_fill(tmol_b200_lkball_plan* plan, int32_t* indices, int32_t* items, void* stream);
+int tmol_b200_lkball_rotamer_forward(tmol_b200_lkball_plan* plan, const void* coords, const void* waters,
+                                     const int32_t* items, int64_t n_items, int64_t n_pairs, void* energies,
+                                     void* stream);
+int tmol_b200_lkball_rotamer_backward(tmol_b200_lkball_plan* plan, const void* coords, const void* waters,
+                                      const int32_t* items, int64_t n_items, int64_t n_pairs, const void* dTdV,
+                                      void* dcoords, void* dwaters, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -8,7 +8,10 @@ lk_ball_pose_score) through the C ABI.
 - against the C oracle on seeded multi-pose batches, float64 to 1e-9;
 - block-pair energies (upper triangle, summing to the whole-pose ones) and
   their adjoint; float64 gradcheck of both ops;
-- plan kinds: a water plan and a score plan serve their own entry points.
+- plan kinds: a water plan and a score plan serve their own entry points;
+- the rotamer op (waters on a rotamer set, lk_ball_rotamer_score): dispatch
+  exact, energies and the gradient of a weighted sum against the reference
+  fixture (tests/golden/lkball_rotamers.npz) and the oracle; gradcheck.
 """
 
 import numpy
@@ -213,3 +216,72 @@ def test_short_poses_with_padding(lterm):
     W_close(W.cpu().numpy(), Wo, 1e-9)
     E_close(E.cpu().numpy(), Eo, rtol=1e-9, atol=1e-9)
     assert numpy.array_equal(nbr.cpu().numpy(), nbro)
+
+
+def gpu_rotamers(ps, rs, lterm, dtype, weights=None):
+    """(waters, energies [4, n], indices, gradient of sum(weights * E))"""
+    from tmol_b200.score.lkball_energy_term import rotamer_score_args
+    from tmol_b200.score.lkball_op import lk_ball_rotamer_score
+
+    wa = to_dev(water_gen_args(ps, lterm, rs), dtype)
+    sa = to_dev(rotamer_score_args(ps, rs, lterm, None)[:-2], dtype)
+    coords = rs.coords.to(DEV, dtype).requires_grad_(True)
+    W = gen_pose_waters(coords, *wa)
+    E, idx = lk_ball_rotamer_score(coords, *sa, W, True)
+    if weights is not None:
+        (E * torch.as_tensor(weights, device=DEV, dtype=dtype)).sum().backward()
+    return W.detach(), E.detach(), idx, coords.grad
+
+
+@pytest.mark.parametrize("f64", [False, True])
+def test_rotamers_match_reference_fixture(lterm, f64):
+    """lk_ball_rotamer_score on the rotamer set of rotamers.npz against the
+    reference op's outputs (tests/golden/lkball_rotamers.npz)."""
+    from tests.test_rotamer_oracle import fixture_case
+
+    g = load_golden("lkball_rotamers.npz")
+    _, ps, rs = fixture_case()
+    dn = "f64" if f64 else "f32"
+    W, E, idx, dx = gpu_rotamers(ps, rs, lterm, torch.float64 if f64 else torch.float32, g[f"{dn}_weights"])
+    assert numpy.array_equal(idx.cpu().numpy(), g["indices"])
+    W_close(W.cpu().numpy(), g[f"{dn}_waters"], 1e-9 if f64 else 2e-4)
+    if f64:
+        E_close(E.cpu().numpy(), g[f"{dn}_energies"], rtol=1e-10, atol=1e-10)
+        g_close(dx.cpu().numpy(), g[f"{dn}_grad"], rtol=1e-9)
+    else:
+        E_close(E.cpu().numpy(), g[f"{dn}_energies"])
+        g_close(dx.cpu().numpy(), g[f"{dn}_grad"])
+
+
+def test_rotamers_match_oracle(lterm):
+    from tests.test_lkball_oracle import oracle_rotamers
+    from tmol_b200.pose.rotamers import synthetic_rotamer_set
+
+    for seed in (13, 14):
+        ps = synthetic_pose_stack([70, 22, 5], [seed, seed + 1, seed + 2], extra_chi_sd=20.0)
+        rs = synthetic_rotamer_set(ps, max_rots=5, mutate_fraction=0.3, seed=seed, skip_fraction=0.2)
+        _, Eo, idxo, _ = oracle_rotamers(ps, rs, True)
+        w = numpy.random.default_rng(seed).normal(size=Eo.shape)
+        Wo, Eo, idxo, dxo = oracle_rotamers(ps, rs, True, weights=w)
+        W, E, idx, dx = gpu_rotamers(ps, rs, lterm, torch.float64, w)
+        assert numpy.array_equal(idx.cpu().numpy(), idxo)
+        W_close(W.cpu().numpy(), Wo, 1e-9)
+        E_close(E.cpu().numpy(), Eo, rtol=1e-9, atol=1e-9)
+        g_close(dx.cpu().numpy(), dxo, rtol=1e-9)
+
+
+def test_rotamer_gradcheck(lterm):
+    from tmol_b200.pose.rotamers import synthetic_rotamer_set
+    from tmol_b200.score.lkball_energy_term import rotamer_score_args
+    from tmol_b200.score.lkball_op import lk_ball_rotamer_score
+
+    ps = synthetic_pose_stack([7, 4], [33, 34], extra_chi_sd=30.0)
+    rs = synthetic_rotamer_set(ps, max_rots=2, mutate_fraction=0.3, seed=3)
+    wa = to_dev(water_gen_args(ps, lterm, rs), torch.float64)
+    sa = to_dev(rotamer_score_args(ps, rs, lterm, None)[:-2], torch.float64)
+    coords = rs.coords.to(DEV, torch.float64).requires_grad_(True)
+
+    def f(c):
+        return lk_ball_rotamer_score(c, *sa, gen_pose_waters(c, *wa), True)[0]
+
+    assert torch.autograd.gradcheck(f, (coords,), eps=1e-6, atol=1e-6, nondet_tol=1e-10)

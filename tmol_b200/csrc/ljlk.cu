@@ -2348,6 +2348,38 @@ int lkb_score_impl(tmol_b200_ljlk_plan* pl, const void* coords, const void* wate
   return TMOL_B200_OK;
 }
 
+template <typename Real, bool GRAD>
+int lkb_rotamer_score_impl(tmol_b200_ljlk_plan* pl, const void* coords, const void* waters, const int32_t* items,
+                           int64_t n_items, int64_t n_pairs, void* energies, const void* dTdV, void* dcoords,
+                           void* dwaters, cudaStream_t st) {
+  ScoreArgs<Real> s = score_args<Real>(pl, coords);
+  LkbArgs<Real> k = lkb_args<Real>(pl);
+  k.water_dist = ((const Real*)pl->global_params)[3];
+  k.waters = (const Real*)waters;
+  k.dwaters_out = (Real*)dwaters;
+  RotArgs ra = rot_args(pl);
+  ra.items = (int4*)items;
+  ra.n_items = n_items;
+  ra.n_pairs = n_pairs;
+  s.energies = (Real*)energies;
+  s.dTdV = (const Real*)dTdV;
+  s.dcoords = (Real*)dcoords;
+  s.nbr = nullptr;
+  s.counts = pl->counts;
+  CK(cudaMemsetAsync(pl->counts, 0, N_COUNTS * sizeof(unsigned long long), st));
+  if (energies) CK(cudaMemsetAsync(energies, 0, (size_t)4 * n_pairs * sizeof(Real), st));
+  if (dcoords) CK(cudaMemsetAsync(dcoords, 0, (size_t)pl->N * 3 * sizeof(Real), st));
+  if (dwaters) CK(cudaMemsetAsync(dwaters, 0, (size_t)pl->N * LKB_NW * 3 * sizeof(Real), st));
+  if (n_items == 0) return TMOL_B200_OK;
+  CK(cudaMemsetAsync(pl->counters, 0, sizeof(int), st));
+  const int warps = pl->launch.warps_per_cta;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n_items + warps - 1) / warps,
+                                                               (int64_t)pl->n_sm * pl->launch.ctas_per_sm));
+  lkb_rotamer_kernel<Real, GRAD><<<grid, 32 * warps, 0, st>>>(s, k, ra);
+  CK(cudaGetLastError());
+  return TMOL_B200_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -2466,7 +2498,18 @@ int build_lkball(tmol_b200_ljlk_plan* pl, const tmol_b200_lkball_inputs* k, cons
   CK(dalloc(pl, (LkbSite<Real>**)&pl->lkb_sites, (size_t)n_sites));
   CK(cudaMemsetAsync(pl->lkb_sites, 0, sizeof(LkbSite<Real>) * std::max<int64_t>(n_sites, 1), st));
   const int64_t PB = (int64_t)pl->P * pl->B;
-  if (PB > 0 && nbt > 0) {
+  if (PB > 0 && nbt > 0 && k->n_rots > 0) {
+    LkbRots rs;
+    rs.rot_coord_offset = k->rot_coord_offset;
+    rs.pose_ind_for_rot = k->pose_ind_for_rot;
+    rs.block_ind_for_rot = k->block_ind_for_rot;
+    rs.block_type_ind_for_rot = k->block_type_ind_for_rot;
+    rs.first_rot_for_block = k->first_rot_for_block;
+    rs.first_rot_block_type = k->first_rot_block_type;
+    rs.bt_n_atoms = pl->bt_n_atoms;
+    rs.R = k->n_rots;
+    rs.nbt = nbt;
+    rs.N = pl->N;
     LkbTables t;
     t.irc = k->inter_residue_connections;
     t.all_bonds = k->bt_all_bonds;
@@ -2483,9 +2526,9 @@ int build_lkball(tmol_b200_ljlk_plan* pl, const tmol_b200_lkball_inputs* k, cons
     t.tile_nH = k->bt_tile_acc_n_attached_H;
     t.is_h = k->bt_atom_is_hydrogen;
     t.bt_conn_atom = k->bt_conn_atom;
-    const int g = std::max(1, std::min<int>((int)((PB + 127) / 128), pl->n_sm * 8));
+    const int g = std::max(1, std::min<int>((k->n_rots + 127) / 128, pl->n_sm * 8));
     lkb_sites_kernel<Real><<<g, 128, 0, st>>>(
-        pl->blk_bt, pl->blk_off, pl->bt_n_atoms, pl->P, pl->B, pl->C, A, t, (const Real*)k->sp2_water_tors,
+        rs, pl->P, pl->B, pl->C, A, t, (const Real*)k->sp2_water_tors,
         k->n_sp2_tors, (const Real*)k->sp3_water_tors, k->n_sp3_tors, (const Real*)k->ring_water_tors,
         k->n_ring_tors, wg[1], wg[2], wg[3], (LkbSite<Real>*)pl->lkb_sites, pl->counters + 1);
     CK(cudaGetLastError());
@@ -2542,7 +2585,8 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
                        scoring ? in->global_params : in->bt_n_atoms};
   if (lkb && lkb->max_n_tiles * TILE < A) return TMOL_B200_ERR_SHAPE;
   if (lkb_waters && P * B > 0 && nbt > 0) {
-    const void* lreq[] = {lkb->inter_residue_connections, lkb->bt_atom_all_bond_ranges, lkb->bt_tile_n_donH,
+    const void* lreq[] = {lkb->inter_residue_connections, lkb->first_rot_for_block, lkb->bt_atom_all_bond_ranges,
+                          lkb->bt_tile_n_donH,
                           lkb->bt_tile_n_acc, lkb->bt_tile_donH_inds, lkb->bt_tile_donH_hvy_inds,
                           lkb->bt_tile_which_donH_for_hvy, lkb->bt_tile_acc_inds, lkb->bt_tile_hybridization,
                           lkb->bt_tile_acc_n_attached_H, lkb->bt_atom_is_hydrogen, lkb->water_gen_global_params};
@@ -2857,7 +2901,7 @@ tmol_b200_ljlk_inputs shared_inputs(const tmol_b200_elec_inputs* e) {
 }
 
 int create_lkball_plan(const tmol_b200_lkball_inputs* k, int real_bytes, const tmol_b200_ljlk_launch* launch,
-                       void* stream, tmol_b200_ljlk_plan** plan_out) {
+                       void* stream, bool rotamers, tmol_b200_ljlk_plan** plan_out) {
   if (!k || !plan_out) return TMOL_B200_ERR_INVALID_ARGUMENT;
   tmol_b200_ljlk_inputs in = {};
   in.n_atoms = k->n_atoms;
@@ -2889,7 +2933,7 @@ int create_lkball_plan(const tmol_b200_lkball_inputs* k, int real_bytes, const t
   in.bt_path_distance = k->bt_path_distance;
   in.global_params = k->global_params;
   in.max_dis = k->max_dis;
-  return create_plan(&in, real_bytes, launch, stream, false, plan_out, nullptr, nullptr, k);
+  return create_plan(&in, real_bytes, launch, stream, rotamers, plan_out, nullptr, nullptr, k);
 }
 
 int create_elec_plan(const tmol_b200_elec_inputs* e, int real_bytes, const tmol_b200_ljlk_launch* launch,
@@ -3265,7 +3309,54 @@ int tmol_b200_elec_rotamer_backward(tmol_b200_elec_plan* plan, const void* coord
 int tmol_b200_lkball_plan_create(const tmol_b200_lkball_inputs* inputs, int real_bytes,
                                  const tmol_b200_ljlk_launch* launch, void* stream,
                                  tmol_b200_lkball_plan** plan_out) {
-  return create_lkball_plan(inputs, real_bytes, launch, stream, plan_out);
+  return create_lkball_plan(inputs, real_bytes, launch, stream, false, plan_out);
+}
+
+int tmol_b200_lkball_rotamer_plan_create(const tmol_b200_lkball_inputs* inputs, int real_bytes,
+                                         const tmol_b200_ljlk_launch* launch, void* stream,
+                                         tmol_b200_lkball_plan** plan_out) {
+  return create_lkball_plan(inputs, real_bytes, launch, stream, true, plan_out);
+}
+
+int tmol_b200_lkball_rotamer_count(tmol_b200_lkball_plan* plan, const void* coords, int64_t* n_pairs,
+                                   int64_t* n_items, void* stream) {
+  if (!plan || !plan->lkb_pol) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  return rotamer_count(plan, kTermLKBall, coords, n_pairs, n_items, stream);
+}
+
+int tmol_b200_lkball_rotamer_fill(tmol_b200_lkball_plan* plan, int32_t* indices, int32_t* items, void* stream) {
+  if (!plan || !plan->lkb_pol) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  return rotamer_fill(plan, kTermLKBall, indices, items, stream);
+}
+
+int tmol_b200_lkball_rotamer_forward(tmol_b200_lkball_plan* plan, const void* coords, const void* waters,
+                                     const int32_t* items, int64_t n_items, int64_t n_pairs, void* energies,
+                                     void* stream) {
+  if (!rotamer_plan_of(plan, kTermLKBall) || !plan->lkb_pol || !energies || n_items < 0 || n_pairs < 0 ||
+      (n_items > 0 && !items) || (plan->N > 0 && (!coords || !waters)))
+    return TMOL_B200_ERR_INVALID_ARGUMENT;
+  if (n_items >= ((int64_t)1 << 31) || n_pairs >= ((int64_t)1 << 31)) return TMOL_B200_ERR_CAPACITY;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->real_bytes == 4)
+    return lkb_rotamer_score_impl<float, false>(plan, coords, waters, items, n_items, n_pairs, energies, nullptr,
+                                                nullptr, nullptr, st);
+  return lkb_rotamer_score_impl<double, false>(plan, coords, waters, items, n_items, n_pairs, energies, nullptr,
+                                               nullptr, nullptr, st);
+}
+
+int tmol_b200_lkball_rotamer_backward(tmol_b200_lkball_plan* plan, const void* coords, const void* waters,
+                                      const int32_t* items, int64_t n_items, int64_t n_pairs, const void* dTdV,
+                                      void* dcoords, void* dwaters, void* stream) {
+  if (!rotamer_plan_of(plan, kTermLKBall) || !plan->lkb_pol || !dTdV || !dcoords || !dwaters || n_items < 0 ||
+      n_pairs < 0 || (n_items > 0 && !items) || (plan->N > 0 && (!coords || !waters)))
+    return TMOL_B200_ERR_INVALID_ARGUMENT;
+  if (n_items >= ((int64_t)1 << 31) || n_pairs >= ((int64_t)1 << 31)) return TMOL_B200_ERR_CAPACITY;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->real_bytes == 4)
+    return lkb_rotamer_score_impl<float, true>(plan, coords, waters, items, n_items, n_pairs, nullptr, dTdV,
+                                               dcoords, dwaters, st);
+  return lkb_rotamer_score_impl<double, true>(plan, coords, waters, items, n_items, n_pairs, nullptr, dTdV,
+                                              dcoords, dwaters, st);
 }
 
 int tmol_b200_lkball_plan_destroy(tmol_b200_lkball_plan* plan) {

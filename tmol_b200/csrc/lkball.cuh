@@ -165,25 +165,51 @@ __device__ inline bool lkb_bases(const LkbTables& t, const int* blk_bt, int p, i
   return b.atom >= 0 && !lkb_same(b0, b);
 }
 
-__device__ __forceinline__ int lkb_row(const int* blk_off, int p, int B, LkbAtom x) {
-  return blk_off[p * B + x.block] + x.atom;
+// The rotamer-set indexing the sites are built from (the op's own
+// arguments, read at plan time): waters are built per rotamer, with atoms of
+// other blocks taken from those blocks' first rotamers (water.hh:318-327).
+struct LkbRots {
+  const int32_t* rot_coord_offset;      // [R]
+  const int32_t* pose_ind_for_rot;      // [R]
+  const int32_t* block_ind_for_rot;     // [R]
+  const int32_t* block_type_ind_for_rot;// [R]
+  const int32_t* first_rot_for_block;   // [P][B]
+  const int32_t* first_rot_block_type;  // [P][B]
+  const int32_t* bt_n_atoms;            // [nbt]
+  int R, nbt;
+  int64_t N;
+};
+
+// x's coordinate row for waters of rotamer (p, b, off); -1 if unresolved
+__device__ __forceinline__ int64_t lkb_row(const LkbRots& r, int p, int B, int b, int off, LkbAtom x) {
+  if (x.block == b) return (int64_t)off + x.atom;
+  const int fr = r.first_rot_for_block[p * B + x.block];
+  if (fr < 0 || fr >= r.R) return -1;
+  return (int64_t)r.rot_coord_offset[fr] + x.atom;
 }
 
-// One thread per block: its water sites, the donor and acceptor waters the
-// reference builds per rotamer (gen_pose_waters.impl.hh:112-175; water.hh:
-// 332-445).
+// One thread per rotamer: its water sites, the donor and acceptor waters
+// the reference builds per rotamer (gen_pose_waters.impl.hh:112-175;
+// water.hh:332-445).  In the pose op every block has one rotamer.
 template <typename Real>
-__global__ void lkb_sites_kernel(const int* blk_bt, const int* blk_off, const int* bt_n_atoms, int P, int B, int C,
-                                 int A, LkbTables t,
+__global__ void lkb_sites_kernel(LkbRots rs, int P, int B, int C, int A, LkbTables t,
                                  const Real* tors_sp2, int n_sp2, const Real* tors_sp3, int n_sp3,
                                  const Real* tors_ring, int n_ring, Real ang_sp2, Real ang_sp3, Real ang_ring,
                                  LkbSite<Real>* sites, int* status) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P * B; i += gridDim.x * blockDim.x) {
-    const int p = i / B, b = i - p * B;
-    const int bt = blk_bt[i];
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rs.R; r += gridDim.x * blockDim.x) {
+    const int bt = rs.block_type_ind_for_rot[r];
     if (bt < 0) continue;
-    const int off = blk_off[i];
-    const int n = bt_n_atoms[bt];
+    const int p = rs.pose_ind_for_rot[r], b = rs.block_ind_for_rot[r];
+    const int off = rs.rot_coord_offset[r];
+    if (bt >= rs.nbt || p < 0 || p >= P || b < 0 || b >= B || off < 0) {
+      atomicOr(status, kStIndex);
+      continue;
+    }
+    const int n = rs.bt_n_atoms[bt];
+    if ((int64_t)off + n > rs.N) {
+      atomicOr(status, kStIndex);
+      continue;
+    }
     for (int tt = 0; tt < t.NT; ++tt) {
       const int64_t tb = (int64_t)bt * t.NT + tt;
       for (int q = 0; q < t.tile_n_donH[tb]; ++q) {
@@ -211,8 +237,10 @@ __global__ void lkb_sites_kernel(const int* blk_bt, const int* blk_off, const in
           continue;
         }
         LkbAtom x = {b, bt, a}, bb, b0;
-        if (!lkb_bases(t, blk_bt, p, B, C, A, x, hyb, bb, b0)) continue;
-        if (bb.atom >= bt_n_atoms[bb.bt] || b0.atom >= bt_n_atoms[b0.bt]) {
+        if (!lkb_bases(t, rs.first_rot_block_type, p, B, C, A, x, hyb, bb, b0)) continue;
+        const int64_t rb = lkb_row(rs, p, B, b, off, bb), rb0 = lkb_row(rs, p, B, b, off, b0);
+        if (bb.atom >= rs.bt_n_atoms[bb.bt] || b0.atom >= rs.bt_n_atoms[b0.bt] || rb < 0 || rb0 < 0 ||
+            rb >= rs.N || rb0 >= rs.N) {
           atomicOr(status, kStIndex);
           continue;
         }
@@ -223,8 +251,8 @@ __global__ void lkb_sites_kernel(const int* blk_bt, const int* blk_off, const in
           LkbSite<Real> s;
           s.kind = kLkbDonor + hyb;
           s.rowA = off + a;
-          s.rowB = lkb_row(blk_off, p, B, bb);
-          s.rowB0 = lkb_row(blk_off, p, B, b0);
+          s.rowB = (int)rb;
+          s.rowB0 = (int)rb0;
           s.tor = tors[w];
           s.ang = ang;
           sites[(int64_t)(off + a) * LKB_NW + w + nh] = s;
@@ -733,18 +761,167 @@ __device__ TMOL_B200_LKB_DRAIN_ATTR Lkb4<Real> lkb_drain(const LkbEval<Real> ev,
   return out;
 }
 
-template <typename Real, bool GRAD, bool BLOCK_PAIR>
-__global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS) lkb_score_kernel(ScoreArgs<Real> s, LkbArgs<Real> k, int items_per_ticket) {
-  __shared__ LkbQueue queues[8][2];  // [warp][plain, bridged]
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  LkbQueue* const qs = queues[warp];
-  const unsigned lt_mask = (1u << lane) - 1u;
-  const int64_t stride = (int64_t)s.P * s.B * s.B;
-  const Real reach2 = k.max_dis * k.max_dis;
-  // work counters: block pairs, polar / occluder pairs, bridged pairs,
-  // pairs evaluated (warp-uniform)
-  unsigned long long n_bp = 0, n_pairs = 0, n_bridge = 0, n_eval = 0;
-  int nq[2] = {0, 0};
+// Per-warp queue state: the two queues (plain, bridged) in shared memory,
+// their fill (warp-uniform) and the work counters.
+template <typename Real>
+struct LkbWarp {
+  LkbQueue* qs;
+  int nq[2];
+  int lane;
+  unsigned lt_mask;
+  unsigned long long n_bp, n_pairs, n_bridge, n_eval;
+};
+
+// Evaluates full queues (or, with `all`, everything queued) under the
+// weights w, adding energies to e4, and shifts what is left to the front.
+template <typename Real, bool GRAD>
+__device__ __forceinline__ void lkb_pump(const LkbEval<Real>& ev, LkbWarp<Real>& q, bool all, const Lkb4<Real>& w,
+                                         Real* e4) {
+  for (;;) {
+    int which, n;
+    if (q.nq[0] >= 32) {
+      which = 0, n = 32;
+    } else if (q.nq[1] >= 32) {
+      which = 1, n = 32;
+    } else if (all && q.nq[0] > 0) {
+      which = 0, n = q.nq[0];
+    } else if (all && q.nq[1] > 0) {
+      which = 1, n = q.nq[1];
+    } else {
+      break;
+    }
+    LkbQueue& Q = q.qs[which];
+    const int lane = q.lane;
+    __syncwarp();
+    const Lkb4<Real> got = lkb_drain<Real, GRAD>(ev, Q, n, lane, w);
+    for (int c = 0; c < 4; ++c) e4[c] += got.v[c];
+    const int rest = q.nq[which] - n;
+    int a = 0, b = 0, c = 0, d = 0, e = 0;
+    if (lane < rest) a = Q.rp[n + lane], b = Q.ro[n + lane], c = Q.pi[n + lane], d = Q.oi[n + lane], e = Q.sep[n + lane];
+    __syncwarp();
+    if (lane < rest) Q.rp[lane] = a, Q.ro[lane] = b, Q.pi[lane] = c, Q.oi[lane] = d, Q.sep[lane] = (uint8_t)e;
+    __syncwarp();
+    q.nq[which] = rest;
+  }
+}
+
+// One side of a pair of blocks (or rotamers): block type, first coordinate
+// row, polar / occluder counts.
+struct LkbSide {
+  int bt, off, npol, nocc, nbr;
+};
+
+template <typename Real>
+__device__ __forceinline__ LkbSide lkb_side(const LkbArgs<Real>& k, int bt, int off) {
+  return LkbSide{bt, off, k.npol[bt], k.nocc[bt], k.nbocc[bt]};
+}
+
+// Every polar / occluder pair of sides 1 and 2 (intra: ordered pairs of
+// distinct atoms of side 1; else both directions): filtered on bond
+// separation (intra: the block type's path distances; inter: through the
+// connections when `striking`), distance and the polar atom's waters, and
+// queued; full queues are evaluated under w into e4.
+template <typename Real, bool GRAD>
+__device__ __forceinline__ void lkb_enqueue_pairs(const ScoreArgs<Real>& s, const LkbArgs<Real>& k,
+                                                  const LkbEval<Real>& ev, LkbWarp<Real>& q, const LkbSide& a,
+                                                  const LkbSide& b, bool intra, bool striking, int nc1, int nc2,
+                                                  const uint8_t* seps, const Lkb4<Real>& w, Real* e4) {
+  const int lane = q.lane;
+  const int no = intra ? a.nocc : b.nocc;
+  const int n01 = a.npol * no;
+  const int total = intra ? n01 : n01 + a.nocc * b.npol;
+  // idx / no in float: exact for these sizes (idx < 2^16, no <= 256: the
+  // error is far below 0.5 / no)
+  const float inv_no = no > 0 ? 1.0f / float(no) : 0.0f;
+  const float inv_nocc1 = a.nocc > 0 ? 1.0f / float(a.nocc) : 0.0f;
+  q.n_bp += 1;
+  q.n_pairs += total;
+  for (int base = 0; base < total; base += 32) {
+    const int idx = base + lane;
+    bool in_reach = false, bridged = false;
+    int rp = 0, ro = 0, pidx = 0, oidx = 0, sep = 0;
+    if (idx < total) {
+      int ap, ao, btp, bto, offp, offo, y;
+      if (idx < n01) {
+        const int x = (int)((float(idx) + 0.5f) * inv_no);
+        y = idx - x * no;
+        btp = a.bt;
+        bto = intra ? a.bt : b.bt;
+        ap = k.pol[(int64_t)btp * k.maxpol + x];
+        ao = k.occ[(int64_t)bto * k.maxocc + y];
+        offp = a.off;
+        offo = intra ? a.off : b.off;
+        if (intra)
+          sep = ap == ao ? 0 : s.bt_pd[((int64_t)a.bt * s.A + ap) * s.A + ao];
+        else
+          sep = striking ? lkb_inter_sep(s, a.bt, b.bt, nc1, nc2, seps, ap, ao) : 6;
+        bridged = y < (intra ? a.nbr : b.nbr);
+      } else {
+        const int j = idx - n01;
+        const int x = (int)((float(j) + 0.5f) * inv_nocc1);
+        y = j - x * a.nocc;
+        btp = b.bt;
+        bto = a.bt;
+        ap = k.pol[(int64_t)btp * k.maxpol + x];
+        ao = k.occ[(int64_t)bto * k.maxocc + y];
+        offp = b.off;
+        offo = a.off;
+        sep = striking ? lkb_inter_sep(s, a.bt, b.bt, nc1, nc2, seps, ao, ap) : 6;
+        bridged = y < a.nbr;
+      }
+      if (sep > 3) {
+        rp = offp + ap;
+        ro = offo + ao;
+        Real I[3], J[3];
+        lkb_load3(s.coords, rp, I);
+        lkb_load3(s.coords, ro, J);
+        const Real dv[3] = {I[0] - J[0], I[1] - J[1], I[2] - J[2]};
+        const Real dist = lkb_sqrt(lkb_dot(dv, dv));
+        in_reach = dist < k.max_dis && !isnan(k.waters[(int64_t)rp * LKB_NW * 3]);
+        pidx = btp * s.A + ap;
+        oidx = bto * s.A + ao;
+      }
+    }
+    const unsigned m1 = __ballot_sync(0xffffffffu, in_reach && bridged);
+    const unsigned m0 = __ballot_sync(0xffffffffu, in_reach && !bridged);
+    if (in_reach) {
+      const int which = bridged ? 1 : 0;
+      LkbQueue& Q = q.qs[which];
+      const int pos = q.nq[which] + __popc((bridged ? m1 : m0) & q.lt_mask);
+      Q.rp[pos] = rp;
+      Q.ro[pos] = ro;
+      Q.pi[pos] = pidx;
+      Q.oi[pos] = oidx;
+      Q.sep[pos] = (uint8_t)(sep > 255 ? 255 : sep);
+    }
+    q.nq[0] += __popc(m0);
+    q.nq[1] += __popc(m1);
+    q.n_eval += __popc(m0 | m1);
+    q.n_bridge += __popc(m1);
+    lkb_pump<Real, GRAD>(ev, q, false, w, e4);
+  }
+}
+
+// The count-pair data of block pair (row i1, block b2): whether any atom
+// pair is within 4 bonds and, if so, the connection-to-connection
+// separations.
+template <typename Real>
+__device__ __forceinline__ bool lkb_striking(const ScoreArgs<Real>& s, int64_t i1, int b2, int cp_b2, int cp_min,
+                                             uint8_t* seps) {
+  const unsigned pm = __ballot_sync(0xffffffffu, cp_b2 == b2);
+  bool striking = false;
+  if (pm) {
+    const int src = __ffs(pm) - 1;
+    striking = __shfl_sync(0xffffffffu, cp_min, src) <= 4;
+    const int64_t e = i1 * CP_CAP + src;
+    if (striking)
+      for (int c = 0; c < 16; ++c) seps[c] = s.cp_seps[e * 16 + c];
+  }
+  return striking;
+}
+
+template <typename Real>
+__device__ __forceinline__ LkbEval<Real> lkb_eval_of(const ScoreArgs<Real>& s, const LkbArgs<Real>& k) {
   LkbEval<Real> ev;
   ev.coords = s.coords;
   ev.waters = k.waters;
@@ -757,6 +934,34 @@ __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS) lkb_score_kernel(
   ev.hbond_oh = k.hbond_oh;
   ev.hbond_h = k.hbond_h;
   ev.max_dis = k.max_dis;
+  return ev;
+}
+
+template <typename Real>
+__device__ __forceinline__ void lkb_flush_counts(const ScoreArgs<Real>& s, const LkbWarp<Real>& q) {
+  if (s.counts && q.lane == 0) {
+    if (q.n_bp) atomicAdd(&s.counts[0], q.n_bp);
+    if (q.n_pairs) atomicAdd(&s.counts[1], q.n_pairs);
+    if (q.n_bridge) atomicAdd(&s.counts[2], q.n_bridge);
+    if (q.n_eval) atomicAdd(&s.counts[3], q.n_eval);
+  }
+}
+
+// The pose op: the plan's work items (pose, b1, candidate blocks b2 >= b1),
+// the neighbour rule as score_kernel applies it, then every polar /
+// occluder pair of each neighbouring block pair.
+template <typename Real, bool GRAD, bool BLOCK_PAIR>
+__global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS) lkb_score_kernel(ScoreArgs<Real> s, LkbArgs<Real> k, int items_per_ticket) {
+  __shared__ LkbQueue queues[MAX_WARPS][2];  // [warp][plain, bridged]
+  LkbWarp<Real> q;
+  q.lane = threadIdx.x & 31;
+  q.qs = queues[threadIdx.x >> 5];
+  q.lt_mask = (1u << q.lane) - 1u;
+  q.nq[0] = q.nq[1] = 0;
+  q.n_bp = q.n_pairs = q.n_bridge = q.n_eval = 0;
+  const int lane = q.lane;
+  const int64_t stride = (int64_t)s.P * s.B * s.B;
+  const LkbEval<Real> ev = lkb_eval_of(s, k);
   for (;;) {
     int t = 0;
     if (lane == 0) t = atomicAdd(s.ticket, 1);
@@ -774,7 +979,6 @@ __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS) lkb_score_kernel(
         if (s.item_cost && lane == 0) s.item_cost[item] = 0;
         continue;
       }
-      const int off1 = s.blk_off[i1];
       const Real* sph1 = s.spheres + 4 * (int64_t)i1;
       const Real c1x = sph1[0], c1y = sph1[1], c1z = sph1[2], rad1 = sph1[3];
       unsigned my_mask = 0;
@@ -802,43 +1006,9 @@ __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS) lkb_score_kernel(
       const int cp_min = lane < ncp ? s.cp_minsep[i1 * CP_CAP + lane] : 6;
       Lkb4<Real> w = {{0, 0, 0, 0}};
       if (GRAD && !BLOCK_PAIR)
-        for (int q = 0; q < 4; ++q) w.v[q] = s.dTdV[(int64_t)q * s.P + p];
+        for (int c = 0; c < 4; ++c) w.v[c] = s.dTdV[(int64_t)c * s.P + p];
       Real acc[4] = {0, 0, 0, 0};
-      const int npol1 = k.npol[bt1], nocc1 = k.nocc[bt1], nbr1 = k.nbocc[bt1];
-      const float inv_nocc1 = nocc1 > 0 ? 1.0f / float(nocc1) : 0.0f;
-      // evaluates full queues (or, with `all`, everything queued) and
-      // shifts what is left to the front
-      auto pump = [&](bool all, Real* e4) {
-        for (;;) {
-          int which, n;
-          if (nq[0] >= 32) {
-            which = 0, n = 32;
-          } else if (nq[1] >= 32) {
-            which = 1, n = 32;
-          } else if (all && nq[0] > 0) {
-            which = 0, n = nq[0];
-          } else if (all && nq[1] > 0) {
-            which = 1, n = nq[1];
-          } else {
-            break;
-          }
-          LkbQueue& q = qs[which];
-          __syncwarp();
-          const Lkb4<Real> got = lkb_drain<Real, GRAD>(ev, q, n, lane, w);
-          for (int c = 0; c < 4; ++c) e4[c] += got.v[c];
-          const int rest = nq[which] - n;
-          int a = 0, b = 0, c = 0, d = 0, e = 0;
-          if (lane < rest) {
-            a = q.rp[n + lane], b = q.ro[n + lane], c = q.pi[n + lane], d = q.oi[n + lane], e = q.sep[n + lane];
-          }
-          __syncwarp();
-          if (lane < rest) {
-            q.rp[lane] = a, q.ro[lane] = b, q.pi[lane] = c, q.oi[lane] = d, q.sep[lane] = (uint8_t)e;
-          }
-          __syncwarp();
-          nq[which] = rest;
-        }
-      };
+      const LkbSide side1 = lkb_side(k, bt1, s.blk_off[i1]);
       for (int bi = 0; bi < n_batches; ++bi) {
         unsigned mask = __shfl_sync(0xffffffffu, my_mask, bi);
         while (mask) {
@@ -846,125 +1016,94 @@ __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS) lkb_score_kernel(
           mask &= mask - 1;
           const int b2 = cand0 + bi * 32 + kk;
           const int i2 = p * s.B + b2;
-          const int bt2 = s.blk_bt[i2];
-          const int off2 = s.blk_off[i2];
           const bool intra = b2 == b1;
-          const unsigned pm = __ballot_sync(0xffffffffu, cp_b2 == b2);
-          bool striking = false;
           uint8_t seps[16];
-          if (pm && !intra) {
-            const int src = __ffs(pm) - 1;
-            striking = __shfl_sync(0xffffffffu, cp_min, src) <= 4;
-            const int64_t e = (int64_t)i1 * CP_CAP + src;
-            if (striking)
-              for (int q = 0; q < 16; ++q) seps[q] = s.cp_seps[e * 16 + q];
-          }
-          const int nc1 = striking ? s.bt_n_conn[bt1] : 0, nc2 = striking ? s.bt_n_conn[bt2] : 0;
+          const bool striking = !intra && lkb_striking(s, i1, b2, cp_b2, cp_min, seps);
+          const LkbSide side2 = lkb_side(k, s.blk_bt[i2], s.blk_off[i2]);
+          const int nc1 = striking ? s.bt_n_conn[bt1] : 0, nc2 = striking ? s.bt_n_conn[side2.bt] : 0;
           const int64_t pair_o = (int64_t)i1 * s.B + b2;
           if (GRAD && BLOCK_PAIR)
-            for (int q = 0; q < 4; ++q) w.v[q] = s.dTdV[(int64_t)q * stride + pair_o];
+            for (int c = 0; c < 4; ++c) w.v[c] = s.dTdV[(int64_t)c * stride + pair_o];
           Real e4[4] = {0, 0, 0, 0};
-          const int npol2 = k.npol[bt2], nocc2 = k.nocc[bt2], nbr2 = k.nbocc[bt2];
-          const int no = intra ? nocc1 : nocc2;
-          const int n01 = npol1 * no;
-          const int total = intra ? n01 : n01 + nocc1 * npol2;
-          const float inv_no = no > 0 ? 1.0f / float(no) : 0.0f;
-          n_bp += 1;
-          n_pairs += total;
-          // filter: bond separation, distance, waters; queue what is in reach
-          for (int base = 0; base < total; base += 32) {
-            const int idx = base + lane;
-            bool in_reach = false, bridged = false;
-            int rp = 0, ro = 0, pidx = 0, oidx = 0, sep = 0;
-            if (idx < total) {
-              int ap, ao, btp, bto, offp, offo, y;
-              if (idx < n01) {
-                // idx / no in float: exact for these sizes (idx < 2^16,
-                // no <= 256: the error is far below 0.5 / no)
-                const int x = (int)((float(idx) + 0.5f) * inv_no);
-                y = idx - x * no;
-                btp = bt1;
-                bto = intra ? bt1 : bt2;
-                ap = k.pol[(int64_t)btp * k.maxpol + x];
-                ao = k.occ[(int64_t)bto * k.maxocc + y];
-                offp = off1;
-                offo = intra ? off1 : off2;
-                if (intra)
-                  sep = ap == ao ? 0 : s.bt_pd[((int64_t)bt1 * s.A + ap) * s.A + ao];
-                else
-                  sep = striking ? lkb_inter_sep(s, bt1, bt2, nc1, nc2, seps, ap, ao) : 6;
-                bridged = y < (intra ? nbr1 : nbr2);
-              } else {
-                const int j = idx - n01;
-                const int x = (int)((float(j) + 0.5f) * inv_nocc1);
-                y = j - x * nocc1;
-                btp = bt2;
-                bto = bt1;
-                ap = k.pol[(int64_t)btp * k.maxpol + x];
-                ao = k.occ[(int64_t)bto * k.maxocc + y];
-                offp = off2;
-                offo = off1;
-                sep = striking ? lkb_inter_sep(s, bt1, bt2, nc1, nc2, seps, ao, ap) : 6;
-                bridged = y < nbr1;
-              }
-              if (sep > 3) {
-                rp = offp + ap;
-                ro = offo + ao;
-                Real I[3], J[3];
-                lkb_load3(s.coords, rp, I);
-                lkb_load3(s.coords, ro, J);
-                const Real dv[3] = {I[0] - J[0], I[1] - J[1], I[2] - J[2]};
-                const Real dist = lkb_sqrt(lkb_dot(dv, dv));
-                in_reach = dist < k.max_dis && !isnan(k.waters[(int64_t)rp * LKB_NW * 3]);
-                pidx = btp * s.A + ap;
-                oidx = bto * s.A + ao;
-              }
-            }
-            const unsigned m1 = __ballot_sync(0xffffffffu, in_reach && bridged);
-            const unsigned m0 = __ballot_sync(0xffffffffu, in_reach && !bridged);
-            if (in_reach) {
-              const int which = bridged ? 1 : 0;
-              LkbQueue& q = qs[which];
-              const int pos = nq[which] + __popc((bridged ? m1 : m0) & lt_mask);
-              q.rp[pos] = rp;
-              q.ro[pos] = ro;
-              q.pi[pos] = pidx;
-              q.oi[pos] = oidx;
-              q.sep[pos] = (uint8_t)(sep > 255 ? 255 : sep);
-            }
-            nq[0] += __popc(m0);
-            nq[1] += __popc(m1);
-            n_eval += __popc(m0 | m1);
-            n_bridge += __popc(m1);
-            pump(false, BLOCK_PAIR ? e4 : acc);
-          }
-          (void)reach2;
+          lkb_enqueue_pairs<Real, GRAD>(s, k, ev, q, side1, side2, intra, striking, nc1, nc2, seps, w,
+                                        BLOCK_PAIR ? e4 : acc);
           if (BLOCK_PAIR) {
-            pump(true, e4);
+            lkb_pump<Real, GRAD>(ev, q, true, w, e4);
             if (!GRAD)
-              for (int q = 0; q < 4; ++q) {
-                const Real v = warp_sum(e4[q]);
-                if (lane == 0) s.energies[(int64_t)q * stride + pair_o] = v;
+              for (int c = 0; c < 4; ++c) {
+                const Real v = warp_sum(e4[c]);
+                if (lane == 0) s.energies[(int64_t)c * stride + pair_o] = v;
               }
           }
         }
       }
-      if (!BLOCK_PAIR) pump(true, acc);
+      if (!BLOCK_PAIR) lkb_pump<Real, GRAD>(ev, q, true, w, acc);
       // whole-pose energies (also in the adjoint when asked for: one pass
       // for energy and gradient)
       if (!BLOCK_PAIR && s.energies)
-        for (int q = 0; q < 4; ++q) {
-          const Real v = warp_sum(acc[q]);
-          if (lane == 0 && v != Real(0)) atomicAdd(&s.energies[(int64_t)q * s.P + p], v);
+        for (int c = 0; c < 4; ++c) {
+          const Real v = warp_sum(acc[c]);
+          if (lane == 0 && v != Real(0)) atomicAdd(&s.energies[(int64_t)c * s.P + p], v);
         }
       // the item's cost, for ordering the work longest-first
       if (s.item_cost && lane == 0) s.item_cost[item] = (int)min((clock64() - t_item) >> 4, (long long)0x7fffffff);
     }
   }
-  if (s.counts && lane == 0) {
-    if (n_bp) atomicAdd(&s.counts[0], n_bp);
-    if (n_pairs) atomicAdd(&s.counts[1], n_pairs);
-    if (n_bridge) atomicAdd(&s.counts[2], n_bridge);
-    if (n_eval) atomicAdd(&s.counts[3], n_eval);
+  lkb_flush_counts(s, q);
+}
+
+// The rotamer op: work items (rot1, first rot2, n rot2, first pair) from
+// the rotamer dispatch; every polar / occluder pair of rot1 against each
+// rot2 (itself on the diagonal), energies per dispatched pair
+// (energies[t * n_pairs + d]), the adjoint under dTdV[t * n_pairs + d].
+template <typename Real, bool GRAD>
+__global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS)
+    lkb_rotamer_kernel(ScoreArgs<Real> s, LkbArgs<Real> k, RotArgs ra) {
+  __shared__ LkbQueue queues[MAX_WARPS][2];
+  LkbWarp<Real> q;
+  q.lane = threadIdx.x & 31;
+  q.qs = queues[threadIdx.x >> 5];
+  q.lt_mask = (1u << q.lane) - 1u;
+  q.nq[0] = q.nq[1] = 0;
+  q.n_bp = q.n_pairs = q.n_bridge = q.n_eval = 0;
+  const int lane = q.lane;
+  const long long np = ra.n_pairs;
+  const LkbEval<Real> ev = lkb_eval_of(s, k);
+  for (;;) {
+    int it = 0;
+    if (lane == 0) it = atomicAdd(s.ticket, 1);
+    it = __shfl_sync(0xffffffffu, it, 0);
+    if (it >= ra.n_items) break;
+    const int4 item = ra.items[it];
+    const int rot1 = item.x, rot2_first = item.y, n_rot2 = item.z;
+    const long long pair_first = item.w;
+    const int p = ra.rot_pose[rot1], b1 = ra.rot_block[rot1];
+    const int64_t i1 = (int64_t)p * s.B + b1;
+    const LkbSide side1 = lkb_side(k, ra.rot_bt[rot1], ra.rot_off[rot1]);
+    const int ncp = s.cp_count[i1];
+    const int cp_b2 = lane < ncp ? s.cp_b2[i1 * CP_CAP + lane] : -1;
+    const int cp_min = lane < ncp ? s.cp_minsep[i1 * CP_CAP + lane] : 6;
+    for (int j = 0; j < n_rot2; ++j) {
+      const int rot2 = rot2_first + j;
+      const long long d = pair_first + j;
+      const int b2 = ra.rot_block[rot2];
+      const bool intra = rot2 == rot1;
+      uint8_t seps[16];
+      const bool striking = b2 != b1 && lkb_striking(s, i1, b2, cp_b2, cp_min, seps);
+      const LkbSide side2 = lkb_side(k, ra.rot_bt[rot2], ra.rot_off[rot2]);
+      const int nc1 = striking ? s.bt_n_conn[side1.bt] : 0, nc2 = striking ? s.bt_n_conn[side2.bt] : 0;
+      Lkb4<Real> w = {{0, 0, 0, 0}};
+      if (GRAD)
+        for (int c = 0; c < 4; ++c) w.v[c] = s.dTdV[(int64_t)c * np + d];
+      Real e4[4] = {0, 0, 0, 0};
+      lkb_enqueue_pairs<Real, GRAD>(s, k, ev, q, side1, side2, intra, striking, nc1, nc2, seps, w, e4);
+      lkb_pump<Real, GRAD>(ev, q, true, w, e4);
+      if (!GRAD)
+        for (int c = 0; c < 4; ++c) {
+          const Real v = warp_sum(e4[c]);
+          if (lane == 0) s.energies[(int64_t)c * np + d] = v;
+        }
+    }
   }
+  lkb_flush_counts(s, q);
 }

@@ -246,6 +246,16 @@ SIGNATURES = {
     "tmol_b200_lkball_forward": (ctypes.c_int, [_V, _V, _V, ctypes.c_int, _V, _V, _V]),
     "tmol_b200_lkball_backward": (ctypes.c_int, [_V, _V, _V, ctypes.c_int, _V, _V, _V, _V]),
     "tmol_b200_lkball_energy_and_gradient": (ctypes.c_int, [_V, _V, _V, _V, _V, _V]),
+    "tmol_b200_lkball_rotamer_plan_create": (
+        ctypes.c_int,
+        [ctypes.POINTER(LKBallInputs), ctypes.c_int, ctypes.POINTER(Launch), _V, ctypes.POINTER(ctypes.c_void_p)],
+    ),
+    "tmol_b200_lkball_rotamer_count": (
+        ctypes.c_int, [_V, _V, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64), _V]
+    ),
+    "tmol_b200_lkball_rotamer_fill": (ctypes.c_int, [_V, _V, _V, _V]),
+    "tmol_b200_lkball_rotamer_forward": (ctypes.c_int, [_V, _V, _V, _V, _I64, _I64, _V, _V]),
+    "tmol_b200_lkball_rotamer_backward": (ctypes.c_int, [_V, _V, _V, _V, _I64, _I64, _V, _V, _V, _V]),
     # PoseStack construction (include/tmol_b200_pose.h)
     "tmol_b200_pose_bondsep": (ctypes.c_int, [ctypes.POINTER(PoseConnectivity), _V, _V, _V, _V]),
     "tmol_b200_apsp_stacked": (ctypes.c_int, [_V, _I32, _I32, _I32, _V]),

@@ -6,6 +6,11 @@ arguments of ``torch.ops.tmol_lk_ball.gen_pose_waters``
 waters ``[n_atoms, 4, 3]`` (NaN in unused slots); gradients flow back to
 ``coords`` through the water-building adjoint.
 
+``lk_ball_rotamer_score(coords, <25 static arguments>, water_coords, True)``
+is ``torch.ops.tmol_lk_ball.lk_ball_rotamer_score`` (``compiled.ops.cpp:604-842,
+909-976``) on a rotamer set, whose waters come from ``gen_pose_waters`` on the
+rotamers' coordinates: ``(scores [4, n], indices [3, n])``.
+
 ``lk_ball_pose_score(coords, <25 static arguments>, water_coords,
 output_block_pair_energies)`` is ``torch.ops.tmol_lk_ball.lk_ball_pose_score``
 (``compiled.ops.cpp:361-603, 843-907``): ``(scores, block_neighbors)``,
@@ -39,7 +44,7 @@ class LKBallPlan(LJLKPlan):
     ABI = "tmol_b200_lkball"
     NAME = "LK-ball"
 
-    def __init__(self, coords_like, water_static=None, score_static=None, launch=None):
+    def __init__(self, coords_like, water_static=None, score_static=None, launch=None, rotamers=False):
         if water_static is None and score_static is None:
             raise ValueError("an LK-ball plan needs the water-generation or the scoring arguments")
         device = self._set_device(coords_like)
@@ -122,13 +127,13 @@ class LKBallPlan(LJLKPlan):
         self.n_atoms = common[1].shape[0]
         s.n_atoms = self.n_atoms
         self.launch = native.Launch(*(launch or (0, 0, 0, 0)))
-        self.rotamers = False
+        self.rotamers = bool(rotamers)
         ptr = ctypes.c_void_p()
         real_bytes = 4 if self.dtype == torch.float32 else 8
         with torch.cuda.device(self.device):
             native.call(
-                "tmol_b200_lkball_plan_create", ctypes.byref(s), real_bytes, ctypes.byref(self.launch),
-                self._stream(), ctypes.byref(ptr),
+                "tmol_b200_lkball_rotamer_plan_create" if rotamers else "tmol_b200_lkball_plan_create",
+                ctypes.byref(s), real_bytes, ctypes.byref(self.launch), self._stream(), ctypes.byref(ptr),
             )
         self.ptr = ptr
         del keep
@@ -202,22 +207,51 @@ class LKBallPlan(LJLKPlan):
     def screen_candidates(self, coords, capacity, out=None):
         raise NotImplementedError("the learned block-pair screen serves LJ/LK plans")
 
-    def rotamer_dispatch(self, coords):
-        raise NotImplementedError("LK-ball rotamer scoring is not built")
+    # rotamer_dispatch (count + fill) is the LJ/LK plan's, on this ABI
+
+    def rotamer_forward(self, coords, items, n_pairs, waters=None):
+        """Energies [4, n_pairs] of the dispatched rotamer pairs."""
+        self._check_coords(coords)
+        self._check_waters(waters)
+        coords, waters = coords.contiguous(), waters.contiguous()
+        energies = torch.empty((self.N_TERMS, n_pairs), dtype=self.dtype, device=self.device)
+        native.call(
+            "tmol_b200_lkball_rotamer_forward", self.ptr, ctypes.c_void_p(coords.data_ptr()),
+            ctypes.c_void_p(waters.data_ptr()), ctypes.c_void_p(items.data_ptr() if items.numel() else 0),
+            items.shape[0], n_pairs, ctypes.c_void_p(energies.data_ptr()), self._stream(),
+        )
+        return energies
+
+    def rotamer_backward(self, coords, items, dTdV, waters=None):
+        """(dL/dcoords directly, dL/dwaters) from dL/dE [4, n_pairs]."""
+        self._check_coords(coords)
+        self._check_waters(waters)
+        coords, waters = coords.contiguous(), waters.contiguous()
+        dTdV = dTdV.to(self.dtype).contiguous()
+        dcoords = torch.empty_like(coords)
+        dwaters = torch.empty_like(waters)
+        native.call(
+            "tmol_b200_lkball_rotamer_backward", self.ptr, ctypes.c_void_p(coords.data_ptr()),
+            ctypes.c_void_p(waters.data_ptr()), ctypes.c_void_p(items.data_ptr() if items.numel() else 0),
+            items.shape[0], dTdV.shape[1], ctypes.c_void_p(dTdV.data_ptr()), ctypes.c_void_p(dcoords.data_ptr()),
+            ctypes.c_void_p(dwaters.data_ptr()), self._stream(),
+        )
+        return dcoords, dwaters
 
 
 class LKBallWaterPlan(LKBallPlan):
+    """Water generation; over a rotamer set (more or fewer rotamers than
+    blocks) the plan is a rotamer plan."""
+
     def __init__(self, coords_like, static_args, launch=None, rotamers=False):
-        if rotamers:
-            raise ValueError("water plans have no rotamer mode")
-        super().__init__(coords_like, water_static=static_args, launch=launch)
+        P, B = static_args[2].shape
+        rotamers = rotamers or static_args[0].shape[0] != P * B
+        super().__init__(coords_like, water_static=static_args, launch=launch, rotamers=rotamers)
 
 
 class LKBallScorePlan(LKBallPlan):
     def __init__(self, coords_like, static_args, launch=None, rotamers=False):
-        if rotamers:
-            raise NotImplementedError("LK-ball rotamer scoring is not built")
-        super().__init__(coords_like, score_static=static_args, launch=launch)
+        super().__init__(coords_like, score_static=static_args, launch=launch, rotamers=rotamers)
 
 
 class _WaterFn(torch.autograd.Function):
@@ -256,6 +290,25 @@ class _LKBallScoreFn(torch.autograd.Function):
         return dx, dw, None, None, None
 
 
+class _LKBallRotamerScoreFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, coords, waters, plan):
+        indices, items = plan.rotamer_dispatch(coords)
+        energies = plan.rotamer_forward(coords, items, indices.shape[1], waters)
+        ctx.plan = plan
+        ctx.save_for_backward(coords, waters, items)
+        ctx.mark_non_differentiable(indices)
+        return energies, indices
+
+    @staticmethod
+    def backward(ctx, dE, _dindices):
+        coords, waters, items = ctx.saved_tensors
+        if dE is None:
+            return None, None, None
+        dx, dw = ctx.plan.rotamer_backward(coords, items, dE, waters)
+        return dx, dw, None
+
+
 def gen_pose_waters(coords, *args):
     """Drop-in for ``torch.ops.tmol_lk_ball.gen_pose_waters``."""
     if len(args) != N_WATER_STATIC:
@@ -274,3 +327,20 @@ def lk_ball_pose_score(coords, *args, return_block_neighbors=True):
     plan = get_plan(flat, static, plan_class=LKBallScorePlan)
     E, nbr = _LKBallScoreFn.apply(flat, waters, plan, block_pair, return_block_neighbors)
     return E, (nbr if return_block_neighbors else None)
+
+
+def lk_ball_rotamer_score(coords, *args):
+    """Drop-in for ``torch.ops.tmol_lk_ball.lk_ball_rotamer_score``: a rotamer
+    set's coordinates, its indexing and the pose's LK-ball tables (25
+    arguments), its waters and ``output_block_pair_energies`` (True, as tmol's
+    rotamer scoring passes it).  Returns ``(scores [4, n], indices [3, n])``
+    for every rotamer pair of neighbouring blocks and every rotamer with
+    itself; gradients flow to ``coords`` and the waters."""
+    if len(args) != N_SCORE_STATIC:
+        raise TypeError(f"lk_ball_rotamer_score takes coords + {N_SCORE_STATIC} arguments, got {1 + len(args)}")
+    static, waters, block_pair = args[:-2], args[-2], args[-1]
+    if not block_pair:
+        raise ValueError("rotamer scoring reports rotamer-pair energies (output_block_pair_energies=True)")
+    flat = coords.reshape(-1, 3)
+    plan = get_plan(flat, static, rotamers=True, plan_class=LKBallScorePlan)
+    return _LKBallRotamerScoreFn.apply(flat, waters, plan)
