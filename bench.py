@@ -58,6 +58,9 @@ ROT_SET = dict(max_rots=31, mutate_fraction=0.25, seed=9)
 ROT_METRIC = "LJ+LK rotamer-pair energies/s (16 poses x 150 residues, 1-31 rotamers per block, 1 B200)"
 ELEC_METRIC = "elec energy+grad poses/s (64x150-residue batch, 1 B200)"
 LKBALL_METRIC = "LK-ball energy+grad poses/s (64x150-residue batch, waters included, 1 B200)"
+LKB_ROT_METRIC = (
+    "LK-ball rotamer-pair energies/s (16 poses x 150 residues, 1-31 rotamers per block, waters included, 1 B200)"
+)
 BONDSEP_METRIC = "inter-block bond separation poses/s (256-pose uneven batch, dense [P,B,B,C,C] + min, 1 B200)"
 
 # Algorithmic FLOPs per unit (E + dE), counted on the restatement's most
@@ -81,6 +84,11 @@ F_LKB_PAIR = 255
 # over 4 x 4 water pairs with its adjoint onto both atoms' waters (481) and
 # its share of the combination (180)
 F_LKB_BRIDGE = 661
+# energies alone (the rotamer op's forward): 112 per evaluated pair
+# (distance 9, sigma 1, isotropic LK 38, desolvation fraction 57, sums 7)
+# and 225 more per bridged pair
+F_LKB_PAIR_E = 112
+F_LKB_BRIDGE_E = 225
 
 
 def workload_sizes(name, rank):
@@ -337,8 +345,9 @@ def _ref_worker(conn, sizes, seeds, term="ljlk"):
         conn.send(time.perf_counter() - t0)
 
 
-def _ref_rot_worker(conn, sizes, seeds):
-    """One single-threaded process of the rotamer reference arm."""
+def _ref_rot_worker(conn, sizes, seeds, term="ljlk"):
+    """One single-threaded process of the rotamer reference arm (`term`:
+    "ljlk", or "lkball": waters on the rotamers, then the rotamer op)."""
     import torch
 
     torch.set_num_threads(1)
@@ -346,6 +355,27 @@ def _ref_rot_worker(conn, sizes, seeds):
     from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm, rotamer_score_args
 
     ps, rs, _, _ = rotamer_workload(0, "cpu", sizes, seeds)
+    if term == "lkball":
+        from tmol_b200.score.lkball_energy_term import LKBallEnergyTerm, water_gen_args
+        from tmol_b200.score.lkball_energy_term import rotamer_score_args as lkb_rotamer_score_args
+
+        lt = LKBallEnergyTerm()
+        wa, sa = water_gen_args(ps, lt, rs), lkb_rotamer_score_args(ps, rs, lt, None)
+        ref = O.reference_lkball_available()
+        oc = None if ref else O.OracleCall(rs.coords, sa, term="lkball", lkb_water_args=wa)
+        conn.send("ready")
+        while True:
+            msg = conn.recv()
+            if msg is None:
+                break
+            t0 = time.perf_counter()
+            if ref:
+                with torch.no_grad():
+                    O.reference_lkball_rotamers(rs.coords, wa, sa)
+            else:
+                oc.lkb_rotamer_scores(oc.lkb_waters())
+            conn.send(time.perf_counter() - t0)
+        return
     args = rotamer_score_args(ps, rs, LJLKEnergyTerm())
     conn.send("ready")
     while True:
@@ -371,6 +401,8 @@ def run_reference(args, world, rank):
         return 0
     if args.workload == "rotamers16x150":
         return run_reference_rotamers(args)
+    if args.workload == "lkball_rotamers16x150":
+        return run_reference_rotamers(args, term="lkball")
     if args.workload == "bondsep256":
         return run_reference_bondsep(args)
     elec = args.workload == "elec64x150"
@@ -448,9 +480,9 @@ def run_reference(args, world, rank):
     return 0
 
 
-def run_reference_rotamers(args):
+def run_reference_rotamers(args, term="ljlk"):
     """tmol's CPU rotamer op, one process per pose (energies of every
-    rotamer pair, as the packer asks for them)."""
+    rotamer pair, as the packer asks for them); LK-ball with its waters."""
     import multiprocessing as mp
 
     from oracle import oracle as O
@@ -463,7 +495,9 @@ def run_reference_rotamers(args):
     workers = []
     for share in shares:
         parent, child = ctx.Pipe()
-        pr = ctx.Process(target=_ref_rot_worker, args=(child, [sizes[k] for k in share], [seeds[k] for k in share]))
+        pr = ctx.Process(
+            target=_ref_rot_worker, args=(child, [sizes[k] for k in share], [seeds[k] for k in share], term)
+        )
         pr.start()
         workers.append((pr, parent))
     for _, c in workers:
@@ -492,10 +526,13 @@ def run_reference_rotamers(args):
     n_pairs = O.OracleCall(rs.coords, rotamer_score_args(ps, rs, LJLKEnergyTerm())).rotamer_scores()[0].shape[1]
     t = sum(times)
     value = n_pairs * args.steps / t
-    kind = "reference" if O.reference_available() else "port"
+    if term == "lkball":
+        kind = "reference" if O.reference_lkball_available() else "port"
+    else:
+        kind = "reference" if O.reference_available() else "port"
     line = {
         "impl": "reference",
-        "metric": ROT_METRIC,
+        "metric": LKB_ROT_METRIC if term == "lkball" else ROT_METRIC,
         "value": value,
         "unit": "rotamer pairs/s",
         "n_gpus": args.gpus,
@@ -507,7 +544,15 @@ def run_reference_rotamers(args):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded proteins and rotamers, ideal geometry)",
-        "config": {"workload": "16 poses x 150 residues, 1-31 rotamers per block, energies", "rotamer_pairs": n_pairs},
+        "config": {
+            "workload": (
+                "16 poses x 150 residues, 1-31 rotamers per block, waters and the four LK-ball energies of every "
+                "rotamer pair"
+                if term == "lkball"
+                else "16 poses x 150 residues, 1-31 rotamers per block, energies of every rotamer pair"
+            ),
+            "rotamer_pairs": n_pairs,
+        },
         "cpu_baseline": {
             "value": value,
             "unit": "rotamer pairs/s",
@@ -648,6 +693,163 @@ def run_rotamers(args, world, rank, local):
                 "frac": achieved / fp32_peak,
                 "traffic": None,
                 "kernel": "rotamer_kernel<float, energies> (+ rotamer spheres), timed as graph replays",
+                "kernel_ms": e_ms,
+                "flops_per_launch": flops,
+                "peak_source": "measured: FMA-loop probe over all SMs in this run (tmol_b200_measure_fp32_peak)",
+            },
+            "e2e": {
+                "value": sum_over_ranks(n_pairs * args.steps, world) / (e2e_ms / 1e3),
+                "unit": "rotamer pairs/s",
+                "h2d_bytes_per_step": coords.numel() * 4,
+                "d2h_bytes_per_step": d2h,
+            },
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+def run_lkball_rotamers(args, world, rank, local):
+    """LK-ball rotamer scoring (tmol's rotamer scoring of the term): per step
+    the waters of every rotamer (gen_pose_waters on the rotamers'
+    coordinates), the dispatch (one host synchronisation to size the
+    output) and the four energies of every rotamer pair of neighbouring
+    blocks (lk_ball_rotamer_score)."""
+    import torch
+
+    from tmol_b200 import native
+    from tmol_b200.score.lkball_energy_term import LKBallEnergyTerm, rotamer_score_args, water_gen_args
+    from tmol_b200.score.lkball_op import LKBallPlan
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    ps, rs, sizes, seeds = rotamer_workload(rank, dev)
+    lt = LKBallEnergyTerm()
+    on = lambda a: [x.to(dev) if isinstance(x, torch.Tensor) else x for x in a]  # noqa: E731
+    wa = on(water_gen_args(ps, lt, rs))
+    sa = on(rotamer_score_args(ps, rs, lt, None)[:-2])
+    coords = rs.coords.contiguous()
+    plan = LKBallPlan(coords, water_static=wa, score_static=sa, rotamers=True, launch=(1, 8, 2, 32))
+    flush = torch.empty(L2_FLUSH_BYTES // 4, device=dev, dtype=torch.float32)
+    W = torch.empty((coords.shape[0], 4, 3), device=dev)
+
+    def op():
+        plan.waters(coords, W)
+        idx, items = plan.rotamer_dispatch(coords)
+        return plan.rotamer_forward(coords, items, idx.shape[1], W), idx, items
+
+    for _ in range(max(args.warmup, 3)):
+        E, idx, items = op()
+    torch.cuda.synchronize()
+    n_pairs = idx.shape[1]
+    counts = plan.last_counts()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record()
+            op()
+            ev[k][1].record()
+        torch.cuda.synchronize()
+    barrier(world)
+    ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), world)
+    value = sum_over_ranks(n_pairs * args.steps, world) / (ms / 1e3)
+    # the scoring kernel alone on a fixed pair list (as a packer reuses it)
+    energies = torch.empty((4, n_pairs), device=dev)
+
+    def energies_only():
+        native.call(
+            "tmol_b200_lkball_rotamer_forward", plan.ptr, ctypes_ptr(coords), ctypes_ptr(W), ctypes_ptr(items),
+            items.shape[0], n_pairs, ctypes_ptr(energies), plan._stream(),
+        )
+
+    e_ms = time_replays(energies_only, args.steps, flush) / args.steps
+    h_coords = coords.cpu().pin_memory()
+    d_in = torch.empty_like(coords)
+    e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    d2h = 0
+    for k in range(args.steps):
+        flush.zero_()
+        e2e_ev[k][0].record()
+        d_in.copy_(h_coords, non_blocking=True)
+        plan.waters(d_in, W)
+        idx2, items2 = plan.rotamer_dispatch(d_in)
+        E2 = plan.rotamer_forward(d_in, items2, idx2.shape[1], W)
+        hE, hI = E2.cpu(), idx2.cpu()
+        d2h = hE.numel() * 4 + hI.numel() * 4
+        e2e_ev[k][1].record()
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in e2e_ev), world)
+    fp32_peak = native.measure_fp32_peak_tflops(torch.cuda.current_stream().cuda_stream)
+    flops = counts["pairs_evaluated"] * F_LKB_PAIR_E + counts["bridged_pairs"] * F_LKB_BRIDGE_E
+    achieved = flops / (e_ms * 1e-3) / 1e12
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        ps0, rs0, _, _ = rotamer_workload(0, "cpu", sizes[:1], seeds[:1])
+        wa0, sa0 = water_gen_args(ps0, lt, rs0), rotamer_score_args(ps0, rs0, lt, None)
+        torch.set_num_threads(1)
+        best = float("inf")
+        for _ in range(2):
+            t0 = time.perf_counter()
+            if O.reference_lkball_available():
+                with torch.no_grad():
+                    E0 = O.reference_lkball_rotamers(rs0.coords, wa0, sa0)[0]
+            else:
+                oc = O.OracleCall(rs0.coords, sa0, term="lkball", lkb_water_args=wa0)
+                E0 = torch.tensor(oc.lkb_rotamer_scores(oc.lkb_waters())[0])
+            best = min(best, time.perf_counter() - t0)
+        cpu = {
+            "value": E0.shape[1] / best,
+            "unit": "rotamer pairs/s",
+            "cores": 1,
+            "kind": "reference" if O.reference_lkball_available() else "port",
+            "sample": "pose 0 of the batch (its waters and all its rotamer pairs), one thread, best of 2",
+        }
+    if rank == 0:
+        line = {
+            "metric": LKB_ROT_METRIC,
+            "value": value,
+            "unit": "rotamer pairs/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded proteins and rotamers, ideal geometry)",
+            "config": {
+                "workload": "16 poses x 150 residues, 1-31 rotamers per block, waters and the four LK-ball "
+                "energies of every rotamer pair",
+                "rotamers": int(rs.n_rotamers_total),
+                "rotamer_pairs": n_pairs,
+                "l2": "flushed (256 MiB write) before every timed step",
+                "parallelism": f"weak, {world} independent batch(es)",
+            },
+            "scoring_only_ms_per_step": e_ms,
+            "work_per_step": counts,
+            # waters, 4 dispatch kernels (rotamer and block spheres, row
+            # counts, scan), the fill, the rotamer spheres and the scoring
+            # kernel
+            "gpu_launches": 8 * args.steps,
+            "clocks": clk.summary(),
+            "roofline": {
+                "bound": "fp32",
+                "achieved": achieved,
+                "peak": fp32_peak,
+                "unit": "TFLOP/s",
+                "frac": achieved / fp32_peak,
+                "traffic": None,
+                "kernel": "lkb_rotamer_kernel<float, energies>, timed as graph replays",
                 "kernel_ms": e_ms,
                 "flops_per_launch": flops,
                 "peak_source": "measured: FMA-loop probe over all SMs in this run (tmol_b200_measure_fp32_peak)",
@@ -1831,7 +2033,10 @@ def main():
     ap.add_argument(
         "--workload",
         default="uniform64x150",
-        choices=["uniform64x150", "uneven256", "rotamers16x150", "elec64x150", "lkball64x150", "bondsep256"],
+        choices=[
+            "uniform64x150", "uneven256", "rotamers16x150", "elec64x150", "lkball64x150", "lkball_rotamers16x150",
+            "bondsep256",
+        ],
     )
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-screen", action="store_true", help="skip the learned-screen measurement")
@@ -1854,6 +2059,8 @@ def main():
         return run_elec(args, world, rank, local)
     if args.workload == "lkball64x150":
         return run_lkball(args, world, rank, local)
+    if args.workload == "lkball_rotamers16x150":
+        return run_lkball_rotamers(args, world, rank, local)
     if args.workload == "bondsep256":
         return run_bondsep(args, world, rank, local)
     return run_b200(args, world, rank, local)

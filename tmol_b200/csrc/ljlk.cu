@@ -2371,11 +2371,16 @@ int lkb_rotamer_score_impl(tmol_b200_ljlk_plan* pl, const void* coords, const vo
   if (dcoords) CK(cudaMemsetAsync(dcoords, 0, (size_t)pl->N * 3 * sizeof(Real), st));
   if (dwaters) CK(cudaMemsetAsync(dwaters, 0, (size_t)pl->N * LKB_NW * 3 * sizeof(Real), st));
   if (n_items == 0) return TMOL_B200_OK;
+  if (pl->R > 0) {
+    const int gr = std::max(1, std::min((pl->R + 7) / 8, pl->n_sm * 16));
+    rot_spheres_kernel<Real><<<gr, 256, 0, st>>>(s, ra, (Real*)pl->rot_spheres);
+    CK(cudaGetLastError());
+  }
   CK(cudaMemsetAsync(pl->counters, 0, sizeof(int), st));
   const int warps = pl->launch.warps_per_cta;
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n_items + warps - 1) / warps,
                                                                (int64_t)pl->n_sm * pl->launch.ctas_per_sm));
-  lkb_rotamer_kernel<Real, GRAD><<<grid, 32 * warps, 0, st>>>(s, k, ra);
+  lkb_rotamer_kernel<Real, GRAD><<<grid, 32 * warps, 0, st>>>(s, k, ra, (const Real*)pl->rot_spheres);
   CK(cudaGetLastError());
   return TMOL_B200_OK;
 }

@@ -691,6 +691,7 @@ constexpr int LKB_Q = 64;
 
 struct LkbQueue {
   int rp[LKB_Q], ro[LKB_Q], pi[LKB_Q], oi[LKB_Q];  // coordinate rows; (bt * A + atom) of the polar / occluder
+  int tag[LKB_Q];  // the output row the pair belongs to (rotamer op: the dispatched pair)
   uint8_t sep[LKB_Q];
 };
 
@@ -772,11 +773,21 @@ struct LkbWarp {
   unsigned long long n_bp, n_pairs, n_bridge, n_eval;
 };
 
+// Where tagged entries' energies go and their weights come from:
+// out[t * n + tag] (rotamer op: energies [4, n_pairs], dTdV [4, n_pairs]).
+template <typename Real>
+struct LkbTagged {
+  Real* energies;
+  const Real* dTdV;
+  int64_t n;
+};
+
 // Evaluates full queues (or, with `all`, everything queued) under the
 // weights w, adding energies to e4, and shifts what is left to the front.
-template <typename Real, bool GRAD>
+// TAGGED: each entry's weights and energies are those of its tag's row.
+template <typename Real, bool GRAD, bool TAGGED = false>
 __device__ __forceinline__ void lkb_pump(const LkbEval<Real>& ev, LkbWarp<Real>& q, bool all, const Lkb4<Real>& w,
-                                         Real* e4) {
+                                         Real* e4, const LkbTagged<Real>& tg = LkbTagged<Real>{}) {
   for (;;) {
     int which, n;
     if (q.nq[0] >= 32) {
@@ -793,13 +804,29 @@ __device__ __forceinline__ void lkb_pump(const LkbEval<Real>& ev, LkbWarp<Real>&
     LkbQueue& Q = q.qs[which];
     const int lane = q.lane;
     __syncwarp();
-    const Lkb4<Real> got = lkb_drain<Real, GRAD>(ev, Q, n, lane, w);
-    for (int c = 0; c < 4; ++c) e4[c] += got.v[c];
+    Lkb4<Real> wl = w;
+    const int tag = TAGGED && lane < n ? Q.tag[lane] : 0;
+    if (TAGGED && GRAD && lane < n)
+      for (int c = 0; c < 4; ++c) wl.v[c] = tg.dTdV[(int64_t)c * tg.n + tag];
+    const Lkb4<Real> got = lkb_drain<Real, GRAD>(ev, Q, n, lane, wl);
+    if (TAGGED) {
+      if (!GRAD && lane < n)
+        for (int c = 0; c < 4; ++c)
+          if (got.v[c] != Real(0)) atomicAdd(&tg.energies[(int64_t)c * tg.n + tag], got.v[c]);
+    } else {
+      for (int c = 0; c < 4; ++c) e4[c] += got.v[c];
+    }
     const int rest = q.nq[which] - n;
-    int a = 0, b = 0, c = 0, d = 0, e = 0;
-    if (lane < rest) a = Q.rp[n + lane], b = Q.ro[n + lane], c = Q.pi[n + lane], d = Q.oi[n + lane], e = Q.sep[n + lane];
+    int a = 0, b = 0, c = 0, d = 0, e = 0, f = 0;
+    if (lane < rest) {
+      a = Q.rp[n + lane], b = Q.ro[n + lane], c = Q.pi[n + lane], d = Q.oi[n + lane], e = Q.sep[n + lane];
+      if (TAGGED) f = Q.tag[n + lane];
+    }
     __syncwarp();
-    if (lane < rest) Q.rp[lane] = a, Q.ro[lane] = b, Q.pi[lane] = c, Q.oi[lane] = d, Q.sep[lane] = (uint8_t)e;
+    if (lane < rest) {
+      Q.rp[lane] = a, Q.ro[lane] = b, Q.pi[lane] = c, Q.oi[lane] = d, Q.sep[lane] = (uint8_t)e;
+      if (TAGGED) Q.tag[lane] = f;
+    }
     __syncwarp();
     q.nq[which] = rest;
   }
@@ -821,11 +848,12 @@ __device__ __forceinline__ LkbSide lkb_side(const LkbArgs<Real>& k, int bt, int 
 // separation (intra: the block type's path distances; inter: through the
 // connections when `striking`), distance and the polar atom's waters, and
 // queued; full queues are evaluated under w into e4.
-template <typename Real, bool GRAD>
+template <typename Real, bool GRAD, bool TAGGED = false>
 __device__ __forceinline__ void lkb_enqueue_pairs(const ScoreArgs<Real>& s, const LkbArgs<Real>& k,
                                                   const LkbEval<Real>& ev, LkbWarp<Real>& q, const LkbSide& a,
                                                   const LkbSide& b, bool intra, bool striking, int nc1, int nc2,
-                                                  const uint8_t* seps, const Lkb4<Real>& w, Real* e4) {
+                                                  const uint8_t* seps, const Lkb4<Real>& w, Real* e4,
+                                                  int tag = 0, const LkbTagged<Real>& tg = LkbTagged<Real>{}) {
   const int lane = q.lane;
   const int no = intra ? a.nocc : b.nocc;
   const int n01 = a.npol * no;
@@ -893,12 +921,13 @@ __device__ __forceinline__ void lkb_enqueue_pairs(const ScoreArgs<Real>& s, cons
       Q.pi[pos] = pidx;
       Q.oi[pos] = oidx;
       Q.sep[pos] = (uint8_t)(sep > 255 ? 255 : sep);
+      if (TAGGED) Q.tag[pos] = tag;
     }
     q.nq[0] += __popc(m0);
     q.nq[1] += __popc(m1);
     q.n_eval += __popc(m0 | m1);
     q.n_bridge += __popc(m1);
-    lkb_pump<Real, GRAD>(ev, q, false, w, e4);
+    lkb_pump<Real, GRAD, TAGGED>(ev, q, false, w, e4, tg);
   }
 }
 
@@ -1055,10 +1084,12 @@ __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS) lkb_score_kernel(
 // The rotamer op: work items (rot1, first rot2, n rot2, first pair) from
 // the rotamer dispatch; every polar / occluder pair of rot1 against each
 // rot2 (itself on the diagonal), energies per dispatched pair
-// (energies[t * n_pairs + d]), the adjoint under dTdV[t * n_pairs + d].
+// (energies[t * n_pairs + d], added by atomics), the adjoint under
+// dTdV[t * n_pairs + d].  Queued pairs carry d, so the queues fill across
+// rotamer pairs and items (a rotamer pair has few pairs in reach).
 template <typename Real, bool GRAD>
 __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS)
-    lkb_rotamer_kernel(ScoreArgs<Real> s, LkbArgs<Real> k, RotArgs ra) {
+    lkb_rotamer_kernel(ScoreArgs<Real> s, LkbArgs<Real> k, RotArgs ra, const Real* rot_spheres) {
   __shared__ LkbQueue queues[MAX_WARPS][2];
   LkbWarp<Real> q;
   q.lane = threadIdx.x & 31;
@@ -1067,8 +1098,13 @@ __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS)
   q.nq[0] = q.nq[1] = 0;
   q.n_bp = q.n_pairs = q.n_bridge = q.n_eval = 0;
   const int lane = q.lane;
-  const long long np = ra.n_pairs;
   const LkbEval<Real> ev = lkb_eval_of(s, k);
+  LkbTagged<Real> tg;
+  tg.energies = s.energies;
+  tg.dTdV = s.dTdV;
+  tg.n = ra.n_pairs;
+  const Lkb4<Real> none = {{0, 0, 0, 0}};
+  Real dummy[4] = {0, 0, 0, 0};
   for (;;) {
     int it = 0;
     if (lane == 0) it = atomicAdd(s.ticket, 1);
@@ -1083,27 +1119,31 @@ __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS)
     const int ncp = s.cp_count[i1];
     const int cp_b2 = lane < ncp ? s.cp_b2[i1 * CP_CAP + lane] : -1;
     const int cp_min = lane < ncp ? s.cp_minsep[i1 * CP_CAP + lane] : 6;
+    // b2 and its count-pair data are the same for every rot2 of the item
+    const int b2 = n_rot2 > 0 ? ra.rot_block[rot2_first] : b1;
+    uint8_t seps[16];
+    const bool striking = b2 != b1 && lkb_striking(s, i1, b2, cp_b2, cp_min, seps);
+    const Real* sp1 = rot_spheres + 4 * (int64_t)rot1;
+    const Real c1x = sp1[0], c1y = sp1[1], c1z = sp1[2], r1 = sp1[3];
     for (int j = 0; j < n_rot2; ++j) {
       const int rot2 = rot2_first + j;
-      const long long d = pair_first + j;
-      const int b2 = ra.rot_block[rot2];
       const bool intra = rot2 == rot1;
-      uint8_t seps[16];
-      const bool striking = b2 != b1 && lkb_striking(s, i1, b2, cp_b2, cp_min, seps);
+      if (!intra) {
+        // no atom pair of two rotamers whose bounding spheres are farther
+        // apart than max_dis (with a margin far above rounding) is in
+        // reach: their energies are zero
+        const Real* sp2 = rot_spheres + 4 * (int64_t)rot2;
+        const Real dx = c1x - sp2[0], dy = c1y - sp2[1], dz = c1z - sp2[2];
+        const Real thr = r1 + sp2[3] + k.max_dis + Real(0.01);
+        if (dx * dx + dy * dy + dz * dz > thr * thr) continue;
+      }
       const LkbSide side2 = lkb_side(k, ra.rot_bt[rot2], ra.rot_off[rot2]);
       const int nc1 = striking ? s.bt_n_conn[side1.bt] : 0, nc2 = striking ? s.bt_n_conn[side2.bt] : 0;
-      Lkb4<Real> w = {{0, 0, 0, 0}};
-      if (GRAD)
-        for (int c = 0; c < 4; ++c) w.v[c] = s.dTdV[(int64_t)c * np + d];
-      Real e4[4] = {0, 0, 0, 0};
-      lkb_enqueue_pairs<Real, GRAD>(s, k, ev, q, side1, side2, intra, striking, nc1, nc2, seps, w, e4);
-      lkb_pump<Real, GRAD>(ev, q, true, w, e4);
-      if (!GRAD)
-        for (int c = 0; c < 4; ++c) {
-          const Real v = warp_sum(e4[c]);
-          if (lane == 0) s.energies[(int64_t)c * np + d] = v;
-        }
+      lkb_enqueue_pairs<Real, GRAD, true>(s, k, ev, q, side1, side2, intra, striking, nc1, nc2, seps, none, dummy,
+                                          (int)(pair_first + j), tg);
     }
   }
+  // entries carry their pair: the queues drain across items, once at the end
+  lkb_pump<Real, GRAD, true>(ev, q, true, none, dummy, tg);
   lkb_flush_counts(s, q);
 }
