@@ -2322,6 +2322,8 @@ int lkb_score_impl(tmol_b200_ljlk_plan* pl, const void* coords, const void* wate
   s.dTdV = (const Real*)dTdV;
   s.dcoords = (Real*)dcoords;
   const size_t PBB = (size_t)pl->P * pl->B * pl->B;
+  // block-pair energies and weights are addressed by an int block-pair index
+  if (BLOCK_PAIR && PBB >= ((size_t)1 << 31)) return TMOL_B200_ERR_CAPACITY;
   if (energies) CK(cudaMemsetAsync(energies, 0, (BLOCK_PAIR ? PBB : (size_t)pl->P) * 4 * sizeof(Real), st));
   if (nbr) CK(cudaMemsetAsync(nbr, 0, PBB * sizeof(int32_t), st));
   if (dcoords) CK(cudaMemsetAsync(dcoords, 0, (size_t)pl->N * 3 * sizeof(Real), st));

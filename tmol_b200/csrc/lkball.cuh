@@ -991,6 +991,12 @@ __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS) lkb_score_kernel(
   const int lane = q.lane;
   const int64_t stride = (int64_t)s.P * s.B * s.B;
   const LkbEval<Real> ev = lkb_eval_of(s, k);
+  // block-pair mode: queued pairs carry their block pair (p * B + b1) * B + b2
+  LkbTagged<Real> tg;
+  tg.energies = s.energies;
+  tg.dTdV = s.dTdV;
+  tg.n = stride;
+  const Lkb4<Real> none = {{0, 0, 0, 0}};
   for (;;) {
     int t = 0;
     if (lane == 0) t = atomicAdd(s.ticket, 1);
@@ -1050,20 +1056,11 @@ __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS) lkb_score_kernel(
           const bool striking = !intra && lkb_striking(s, i1, b2, cp_b2, cp_min, seps);
           const LkbSide side2 = lkb_side(k, s.blk_bt[i2], s.blk_off[i2]);
           const int nc1 = striking ? s.bt_n_conn[bt1] : 0, nc2 = striking ? s.bt_n_conn[side2.bt] : 0;
-          const int64_t pair_o = (int64_t)i1 * s.B + b2;
-          if (GRAD && BLOCK_PAIR)
-            for (int c = 0; c < 4; ++c) w.v[c] = s.dTdV[(int64_t)c * stride + pair_o];
-          Real e4[4] = {0, 0, 0, 0};
-          lkb_enqueue_pairs<Real, GRAD>(s, k, ev, q, side1, side2, intra, striking, nc1, nc2, seps, w,
-                                        BLOCK_PAIR ? e4 : acc);
-          if (BLOCK_PAIR) {
-            lkb_pump<Real, GRAD>(ev, q, true, w, e4);
-            if (!GRAD)
-              for (int c = 0; c < 4; ++c) {
-                const Real v = warp_sum(e4[c]);
-                if (lane == 0) s.energies[(int64_t)c * stride + pair_o] = v;
-              }
-          }
+          if (BLOCK_PAIR)
+            lkb_enqueue_pairs<Real, GRAD, true>(s, k, ev, q, side1, side2, intra, striking, nc1, nc2, seps, none,
+                                                acc, (int)((int64_t)i1 * s.B + b2), tg);
+          else
+            lkb_enqueue_pairs<Real, GRAD>(s, k, ev, q, side1, side2, intra, striking, nc1, nc2, seps, w, acc);
         }
       }
       if (!BLOCK_PAIR) lkb_pump<Real, GRAD>(ev, q, true, w, acc);
@@ -1077,6 +1074,10 @@ __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS) lkb_score_kernel(
       // the item's cost, for ordering the work longest-first
       if (s.item_cost && lane == 0) s.item_cost[item] = (int)min((clock64() - t_item) >> 4, (long long)0x7fffffff);
     }
+  }
+  if (BLOCK_PAIR) {
+    Real dummy[4] = {0, 0, 0, 0};
+    lkb_pump<Real, GRAD, true>(ev, q, true, none, dummy, tg);
   }
   lkb_flush_counts(s, q);
 }
