@@ -618,9 +618,12 @@ def run_rotamers(args, world, rank, local):
         )
 
     e_ms = time_replays(energies_only, args.steps, flush) / args.steps
-    # end to end: host coordinates in, energies and pair indices out
+    # end to end: host coordinates in, energies and pair indices out (into
+    # pinned host buffers sized by the pair count)
     h_coords = coords.cpu().pin_memory()
     d_in = torch.empty_like(coords)
+    h_E = torch.empty((3, n_pairs), pin_memory=True)
+    h_I = torch.empty((3, n_pairs), dtype=torch.int32, pin_memory=True)
     e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     d2h = 0
     for k in range(args.steps):
@@ -629,8 +632,12 @@ def run_rotamers(args, world, rank, local):
         d_in.copy_(h_coords, non_blocking=True)
         idx2, items2 = plan.rotamer_dispatch(d_in)
         E2 = plan.rotamer_forward(d_in, items2, idx2.shape[1])
-        hE, hI = E2.cpu(), idx2.cpu()
-        d2h = hE.numel() * 4 + hI.numel() * 4
+        if idx2.shape[1] != h_E.shape[1]:
+            h_E = torch.empty(tuple(E2.shape), pin_memory=True)
+            h_I = torch.empty(tuple(idx2.shape), dtype=torch.int32, pin_memory=True)
+        h_E.copy_(E2, non_blocking=True)
+        h_I.copy_(idx2, non_blocking=True)
+        d2h = h_E.numel() * 4 + h_I.numel() * 4
         e2e_ev[k][1].record()
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in e2e_ev), world)
@@ -772,6 +779,8 @@ def run_lkball_rotamers(args, world, rank, local):
     e_ms = time_replays(energies_only, args.steps, flush) / args.steps
     h_coords = coords.cpu().pin_memory()
     d_in = torch.empty_like(coords)
+    h_E = torch.empty((4, n_pairs), pin_memory=True)
+    h_I = torch.empty((3, n_pairs), dtype=torch.int32, pin_memory=True)
     e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     d2h = 0
     for k in range(args.steps):
@@ -781,8 +790,12 @@ def run_lkball_rotamers(args, world, rank, local):
         plan.waters(d_in, W)
         idx2, items2 = plan.rotamer_dispatch(d_in)
         E2 = plan.rotamer_forward(d_in, items2, idx2.shape[1], W)
-        hE, hI = E2.cpu(), idx2.cpu()
-        d2h = hE.numel() * 4 + hI.numel() * 4
+        if idx2.shape[1] != h_E.shape[1]:
+            h_E = torch.empty(tuple(E2.shape), pin_memory=True)
+            h_I = torch.empty(tuple(idx2.shape), dtype=torch.int32, pin_memory=True)
+        h_E.copy_(E2, non_blocking=True)
+        h_I.copy_(idx2, non_blocking=True)
+        d2h = h_E.numel() * 4 + h_I.numel() * 4
         e2e_ev[k][1].record()
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in e2e_ev), world)
@@ -1410,9 +1423,10 @@ def run_lkball(args, world, rank, local):
     value = poses_total / (ms_max / 1e3)
     m, _ = measure_lkball(plan, coords, flush, args.steps)
 
-    # end to end through the drop-in ops, as tmol's LK-ball term calls them:
-    # pinned coordinates in, gen_pose_waters, lk_ball_pose_score, backward
-    # through both, energies and gradient out
+    # end to end, pinned coordinates in and energies and gradient out: through
+    # the C entry point (e2e), and through the drop-in ops as tmol's LK-ball
+    # term calls them (gen_pose_waters, lk_ball_pose_score, backward through
+    # both)
     from tmol_b200.score.lkball_energy_term import LKBallEnergyTerm, score_args, water_gen_args
 
     lt = LKBallEnergyTerm()
@@ -1431,19 +1445,36 @@ def run_lkball(args, world, rank, local):
         h_E.copy_(E.detach(), non_blocking=True)
         h_g.copy_(d_in.grad, non_blocking=True)
 
-    for _ in range(max(args.warmup, 3)):
-        e2e_step()
-    torch.cuda.synchronize()
-    e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    barrier(world)
-    for k in range(args.steps):
-        flush.zero_()
-        e2e_ev[k][0].record()
-        e2e_step()
-        e2e_ev[k][1].record()
-    torch.cuda.synchronize()
-    barrier(world)
-    e2e_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in e2e_ev), world)
+    def timed(fn):
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        barrier(world)
+        for k in range(args.steps):
+            flush.zero_()
+            evs[k][0].record()
+            fn()
+            evs[k][1].record()
+        torch.cuda.synchronize()
+        barrier(world)
+        return max_over_ranks(sum(a.elapsed_time(b) for a, b in evs), world)
+
+    # the plan's one-call C entry point with host buffers (pinned coordinates
+    # in; energies and gradient out), as the LJ/LK arm measures it
+    w1 = torch.ones((4, P), device=dev)
+    E1 = torch.empty((4, P), device=dev)
+    dx1 = torch.empty_like(coords)
+    d_in = torch.empty_like(coords)
+
+    def e2e_c_abi():
+        d_in.copy_(h_coords, non_blocking=True)
+        plan.energy_and_gradient(d_in, w1, E1, dx1)
+        h_E.copy_(E1, non_blocking=True)
+        h_g.copy_(dx1, non_blocking=True)
+
+    e2e_ms = timed(e2e_c_abi)
+    dropin_ms = timed(e2e_step)
 
     fp32_peak = native.measure_fp32_peak_tflops(torch.cuda.current_stream().cuda_stream)
     cpu = None
@@ -1506,7 +1537,12 @@ def run_lkball(args, world, rank, local):
                 "unit": "poses/s",
                 "h2d_bytes_per_step": coords.numel() * 4,
                 "d2h_bytes_per_step": (4 * P + coords.numel()) * 4,
-                "path": "gen_pose_waters + lk_ball_pose_score drop-ins, autograd backward",
+                "path": "tmol_b200_lkball_energy_and_gradient (C ABI) with host buffers",
+            },
+            "e2e_dropin_ops": {
+                "value": poses_total / (dropin_ms / 1e3),
+                "unit": "poses/s",
+                "path": "gen_pose_waters + lk_ball_pose_score drop-ins, autograd backward, same host copies",
             },
             "cpu_baseline": cpu,
         }

@@ -285,3 +285,29 @@ def test_rotamer_gradcheck(lterm):
         return lk_ball_rotamer_score(c, *sa, gen_pose_waters(c, *wa), True)[0]
 
     assert torch.autograd.gradcheck(f, (coords,), eps=1e-6, atol=1e-6, nondet_tol=1e-10)
+
+
+@pytest.mark.parametrize("f64", [False, True])
+def test_exotic_blocks_match_oracle(lterm, f64):
+    """Block types of 40 and 45 atoms (two tiles), three connections and
+    ligand fragments."""
+    import os
+    import sys
+
+    sys.path.insert(0, os.path.dirname(__file__))
+    from exotic_blocks import exotic_pose_stack
+
+    dt = torch.float64 if f64 else torch.float32
+    for seed in (4, 5):
+        ps = exotic_pose_stack(seed=seed)
+        W, E, dx, nbr = gpu_run(ps, lterm, dt)
+        Wo, Eo, dxo, nbro = oracle_run(ps, lterm, f64)
+        assert numpy.array_equal(nbr.cpu().numpy(), nbro)
+        if f64:
+            W_close(W.cpu().numpy(), Wo, 1e-9)
+            E_close(E.cpu().numpy(), Eo, rtol=1e-9, atol=1e-9)
+            g_close(dx.cpu().numpy(), dxo, rtol=1e-9)
+        else:
+            W_close(W.cpu().numpy(), Wo, 1e-4)
+            E_close(E.cpu().numpy(), Eo)
+            g_close(dx.cpu().numpy(), dxo)
