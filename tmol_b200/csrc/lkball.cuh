@@ -689,9 +689,10 @@ __device__ __forceinline__ LkbParams<Real> lkb_params(const K& k, int A, int bt,
 // evaluated 32 at a time with every lane busy on the same branch.
 constexpr int LKB_Q = 64;
 
+template <bool TAGGED>
 struct LkbQueue {
   int rp[LKB_Q], ro[LKB_Q], pi[LKB_Q], oi[LKB_Q];  // coordinate rows; (bt * A + atom) of the polar / occluder
-  int tag[LKB_Q];  // the output row the pair belongs to (rotamer op: the dispatched pair)
+  int tag[TAGGED ? LKB_Q : 1];  // the output row each pair belongs to (tagged queues only)
   uint8_t sep[LKB_Q];
 };
 
@@ -725,8 +726,8 @@ struct Lkb4 {
 #define TMOL_B200_LKB_MIN_CTAS 2
 #endif
 
-template <typename Real, bool GRAD>
-__device__ TMOL_B200_LKB_DRAIN_ATTR Lkb4<Real> lkb_drain(const LkbEval<Real> ev, const LkbQueue& q, int n, int lane,
+template <typename Real, bool GRAD, typename Queue>
+__device__ TMOL_B200_LKB_DRAIN_ATTR Lkb4<Real> lkb_drain(const LkbEval<Real> ev, const Queue& q, int n, int lane,
                                              const Lkb4<Real> w) {
   Lkb4<Real> out = {{0, 0, 0, 0}};
   if (lane >= n) return out;
@@ -764,9 +765,9 @@ __device__ TMOL_B200_LKB_DRAIN_ATTR Lkb4<Real> lkb_drain(const LkbEval<Real> ev,
 
 // Per-warp queue state: the two queues (plain, bridged) in shared memory,
 // their fill (warp-uniform) and the work counters.
-template <typename Real>
+template <typename Real, bool TAGGED>
 struct LkbWarp {
-  LkbQueue* qs;
+  LkbQueue<TAGGED>* qs;
   int nq[2];
   int lane;
   unsigned lt_mask;
@@ -785,8 +786,8 @@ struct LkbTagged {
 // Evaluates full queues (or, with `all`, everything queued) under the
 // weights w, adding energies to e4, and shifts what is left to the front.
 // TAGGED: each entry's weights and energies are those of its tag's row.
-template <typename Real, bool GRAD, bool TAGGED = false>
-__device__ __forceinline__ void lkb_pump(const LkbEval<Real>& ev, LkbWarp<Real>& q, bool all, const Lkb4<Real>& w,
+template <typename Real, bool GRAD, bool TAGGED>
+__device__ __forceinline__ void lkb_pump(const LkbEval<Real>& ev, LkbWarp<Real, TAGGED>& q, bool all, const Lkb4<Real>& w,
                                          Real* e4, const LkbTagged<Real>& tg = LkbTagged<Real>{}) {
   for (;;) {
     int which, n;
@@ -801,7 +802,7 @@ __device__ __forceinline__ void lkb_pump(const LkbEval<Real>& ev, LkbWarp<Real>&
     } else {
       break;
     }
-    LkbQueue& Q = q.qs[which];
+    LkbQueue<TAGGED>& Q = q.qs[which];
     const int lane = q.lane;
     __syncwarp();
     Lkb4<Real> wl = w;
@@ -848,9 +849,9 @@ __device__ __forceinline__ LkbSide lkb_side(const LkbArgs<Real>& k, int bt, int 
 // separation (intra: the block type's path distances; inter: through the
 // connections when `striking`), distance and the polar atom's waters, and
 // queued; full queues are evaluated under w into e4.
-template <typename Real, bool GRAD, bool TAGGED = false>
+template <typename Real, bool GRAD, bool TAGGED>
 __device__ __forceinline__ void lkb_enqueue_pairs(const ScoreArgs<Real>& s, const LkbArgs<Real>& k,
-                                                  const LkbEval<Real>& ev, LkbWarp<Real>& q, const LkbSide& a,
+                                                  const LkbEval<Real>& ev, LkbWarp<Real, TAGGED>& q, const LkbSide& a,
                                                   const LkbSide& b, bool intra, bool striking, int nc1, int nc2,
                                                   const uint8_t* seps, const Lkb4<Real>& w, Real* e4,
                                                   int tag = 0, const LkbTagged<Real>& tg = LkbTagged<Real>{}) {
@@ -914,7 +915,7 @@ __device__ __forceinline__ void lkb_enqueue_pairs(const ScoreArgs<Real>& s, cons
     const unsigned m0 = __ballot_sync(0xffffffffu, in_reach && !bridged);
     if (in_reach) {
       const int which = bridged ? 1 : 0;
-      LkbQueue& Q = q.qs[which];
+      LkbQueue<TAGGED>& Q = q.qs[which];
       const int pos = q.nq[which] + __popc((bridged ? m1 : m0) & q.lt_mask);
       Q.rp[pos] = rp;
       Q.ro[pos] = ro;
@@ -966,8 +967,8 @@ __device__ __forceinline__ LkbEval<Real> lkb_eval_of(const ScoreArgs<Real>& s, c
   return ev;
 }
 
-template <typename Real>
-__device__ __forceinline__ void lkb_flush_counts(const ScoreArgs<Real>& s, const LkbWarp<Real>& q) {
+template <typename Real, bool TAGGED>
+__device__ __forceinline__ void lkb_flush_counts(const ScoreArgs<Real>& s, const LkbWarp<Real, TAGGED>& q) {
   if (s.counts && q.lane == 0) {
     if (q.n_bp) atomicAdd(&s.counts[0], q.n_bp);
     if (q.n_pairs) atomicAdd(&s.counts[1], q.n_pairs);
@@ -981,8 +982,10 @@ __device__ __forceinline__ void lkb_flush_counts(const ScoreArgs<Real>& s, const
 // occluder pair of each neighbouring block pair.
 template <typename Real, bool GRAD, bool BLOCK_PAIR>
 __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS) lkb_score_kernel(ScoreArgs<Real> s, LkbArgs<Real> k, int items_per_ticket) {
-  __shared__ LkbQueue queues[MAX_WARPS][2];  // [warp][plain, bridged]
-  LkbWarp<Real> q;
+  // [warp][plain, bridged]; block-pair mode tags queued pairs with their
+  // block pair (p * B + b1) * B + b2
+  __shared__ LkbQueue<BLOCK_PAIR> queues[MAX_WARPS][2];
+  LkbWarp<Real, BLOCK_PAIR> q;
   q.lane = threadIdx.x & 31;
   q.qs = queues[threadIdx.x >> 5];
   q.lt_mask = (1u << q.lane) - 1u;
@@ -991,7 +994,6 @@ __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS) lkb_score_kernel(
   const int lane = q.lane;
   const int64_t stride = (int64_t)s.P * s.B * s.B;
   const LkbEval<Real> ev = lkb_eval_of(s, k);
-  // block-pair mode: queued pairs carry their block pair (p * B + b1) * B + b2
   LkbTagged<Real> tg;
   tg.energies = s.energies;
   tg.dTdV = s.dTdV;
@@ -1056,14 +1058,12 @@ __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS) lkb_score_kernel(
           const bool striking = !intra && lkb_striking(s, i1, b2, cp_b2, cp_min, seps);
           const LkbSide side2 = lkb_side(k, s.blk_bt[i2], s.blk_off[i2]);
           const int nc1 = striking ? s.bt_n_conn[bt1] : 0, nc2 = striking ? s.bt_n_conn[side2.bt] : 0;
-          if (BLOCK_PAIR)
-            lkb_enqueue_pairs<Real, GRAD, true>(s, k, ev, q, side1, side2, intra, striking, nc1, nc2, seps, none,
-                                                acc, (int)((int64_t)i1 * s.B + b2), tg);
-          else
-            lkb_enqueue_pairs<Real, GRAD>(s, k, ev, q, side1, side2, intra, striking, nc1, nc2, seps, w, acc);
+          lkb_enqueue_pairs<Real, GRAD, BLOCK_PAIR>(s, k, ev, q, side1, side2, intra, striking, nc1, nc2, seps,
+                                                    BLOCK_PAIR ? none : w, acc,
+                                                    BLOCK_PAIR ? (int)((int64_t)i1 * s.B + b2) : 0, tg);
         }
       }
-      if (!BLOCK_PAIR) lkb_pump<Real, GRAD>(ev, q, true, w, acc);
+      if (!BLOCK_PAIR) lkb_pump<Real, GRAD, BLOCK_PAIR>(ev, q, true, w, acc, tg);
       // whole-pose energies (also in the adjoint when asked for: one pass
       // for energy and gradient)
       if (!BLOCK_PAIR && s.energies)
@@ -1077,7 +1077,7 @@ __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS) lkb_score_kernel(
   }
   if (BLOCK_PAIR) {
     Real dummy[4] = {0, 0, 0, 0};
-    lkb_pump<Real, GRAD, true>(ev, q, true, none, dummy, tg);
+    lkb_pump<Real, GRAD, BLOCK_PAIR>(ev, q, true, none, dummy, tg);
   }
   lkb_flush_counts(s, q);
 }
@@ -1091,8 +1091,8 @@ __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS) lkb_score_kernel(
 template <typename Real, bool GRAD>
 __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS)
     lkb_rotamer_kernel(ScoreArgs<Real> s, LkbArgs<Real> k, RotArgs ra, const Real* rot_spheres) {
-  __shared__ LkbQueue queues[MAX_WARPS][2];
-  LkbWarp<Real> q;
+  __shared__ LkbQueue<true> queues[MAX_WARPS][2];
+  LkbWarp<Real, true> q;
   q.lane = threadIdx.x & 31;
   q.qs = queues[threadIdx.x >> 5];
   q.lt_mask = (1u << q.lane) - 1u;
