@@ -311,3 +311,28 @@ def test_exotic_blocks_match_oracle(lterm, f64):
             W_close(W.cpu().numpy(), Wo, 1e-4)
             E_close(E.cpu().numpy(), Eo)
             g_close(dx.cpu().numpy(), dxo)
+
+
+def test_rendered_scoring_modules(lterm):
+    """LKBallEnergyTerm's whole-pose, block-pair and rotamer scoring modules
+    (tmol's energy-term surface) score like the ops they wrap."""
+    from tmol_b200.pose.rotamers import synthetic_rotamer_set
+
+    ps = synthetic_pose_stack([30, 12], [61, 62], extra_chi_sd=20.0)
+    W, E, dx, _ = gpu_run(ps, lterm, torch.float32)
+    psd = ps.to(DEV)
+    coords = psd.coords.clone().requires_grad_(True)
+    whole = lterm.render_whole_pose_scoring_module(psd)
+    Em = whole(coords)
+    E_close(Em.detach().cpu().numpy(), E.cpu().numpy(), rtol=1e-6, atol=1e-6)
+    Em.sum().backward()
+    g_close(coords.grad.flatten(0, 1).cpu().numpy(), dx.cpu().numpy(), rtol=1e-5)
+    pairs = lterm.render_block_pair_scoring_module(psd)
+    Eb = pairs(psd.coords)
+    E_close(Eb.sum(dim=(2, 3)).cpu().numpy(), E.cpu().numpy(), rtol=1e-5, atol=1e-5)
+    rs = synthetic_rotamer_set(ps, max_rots=3, mutate_fraction=0.3, seed=7)
+    _, Er, idxr, _ = gpu_rotamers(ps, rs, lterm, torch.float32)
+    rot = lterm.render_rotamer_scoring_module(psd, rs.to(DEV))
+    Em2, idx2 = rot(rs.coords.to(DEV))
+    assert torch.equal(idx2, idxr)
+    E_close(Em2.cpu().numpy(), Er.cpu().numpy(), rtol=1e-6, atol=1e-6)

@@ -43,6 +43,77 @@ class LKBallEnergyTerm:
     def _gp(pbt):
         return pbt.db.ljlk_global_params, pbt.db.lkball_global_params
 
+    # -- the scoring-module surface (tmol energy_term.py:35-147) -----------
+
+    N_WATER_TABLES = 20  # gen_pose_waters' arguments after the 12 indexing ones
+    N_SCORE_TABLES = 13  # lk_ball_pose_score's, before the waters and the output flag
+
+    def get_score_term_attributes(self, pose_stack):
+        """The pose's LK-ball arguments of both ops, built once: the 20
+        water-generation tables, then the 13 scoring ones (tmol passes the
+        PoseStack itself and rebuilds these lists per call,
+        lk_ball_energy_term.py:236-369)."""
+        return water_gen_args(pose_stack, self)[12:] + score_args(pose_stack, self, None)[12:-2]
+
+    @classmethod
+    def _split(cls, args):
+        common = args[:12]
+        wt = args[12 : 12 + cls.N_WATER_TABLES]
+        st = args[12 + cls.N_WATER_TABLES : 12 + cls.N_WATER_TABLES + cls.N_SCORE_TABLES]
+        return common, wt, st, args[12 + cls.N_WATER_TABLES + cls.N_SCORE_TABLES]
+
+    @classmethod
+    def pose_score_lk_ball(cls, coords, *args):
+        """tmol ``LKBallEnergyTerm.pose_score_lk_ball``: the waters, then the
+        pose scores on them; ``(scores, block_neighbors)``."""
+        from .lkball_op import gen_pose_waters, lk_ball_pose_score
+
+        common, wt, st, block_pair = cls._split(args)
+        W = gen_pose_waters(coords, *common, *wt)
+        return lk_ball_pose_score(coords, *common, *st, W, block_pair)
+
+    @classmethod
+    def rotamer_score_lk_ball(cls, coords, *args):
+        """tmol ``LKBallEnergyTerm.rotamer_score_lk_ball``: the waters of every
+        rotamer, then the rotamer-pair scores; ``(scores, indices)``."""
+        from .lkball_op import gen_pose_waters, lk_ball_rotamer_score
+
+        common, wt, st, block_pair = cls._split(args)
+        W = gen_pose_waters(coords, *common, *wt)
+        return lk_ball_rotamer_score(coords, *common, *st, W, block_pair)
+
+    def get_pose_score_term_function(self):
+        return self.pose_score_lk_ball
+
+    def get_rotamer_score_term_function(self):
+        return self.rotamer_score_lk_ball
+
+    def render_whole_pose_scoring_module(self, pose_stack):
+        from .scoring_module import TermWholePoseScoringModule
+
+        return TermWholePoseScoringModule(
+            self.class_name(), pose_stack, self.get_score_term_attributes(pose_stack),
+            self.get_pose_score_term_function(),
+        )
+
+    def render_block_pair_scoring_module(self, pose_stack):
+        from .scoring_module import TermBlockPairScoringModule
+
+        return TermBlockPairScoringModule(
+            self.class_name(), pose_stack, self.get_score_term_attributes(pose_stack),
+            self.get_pose_score_term_function(),
+        )
+
+    def render_rotamer_scoring_module(self, pose_stack, rotamer_set):
+        """tmol ``energy_term.py:132-147``: the rotamer-pair scoring module
+        over ``rotamer_set``."""
+        from .scoring_module import TermRotamerScoringModule
+
+        return TermRotamerScoringModule(
+            self.class_name(), rotamer_set, self.get_score_term_attributes(pose_stack),
+            self.get_rotamer_score_term_function(),
+        )
+
     def water_gen_global_params(self, pbt, device):
         """[1, 4] (water distance, sp2 / sp3 / ring angles) and the three
         torsion lists, float32 as tmol's resolver holds them."""
