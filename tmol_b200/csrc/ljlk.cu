@@ -728,13 +728,19 @@ __device__ __forceinline__ void cnt_add(unsigned long long* c, int k, long long 
   if (lane == 0) c[k] += (unsigned long long)v;
 }
 
+// The pair-evaluation helpers below are out of line by default (one copy
+// each: the kernel's code footprint and register budget stay small).
+#ifndef TMOL_B200_LJLK_OUTLINE
+#define TMOL_B200_LJLK_OUTLINE __noinline__
+#endif
+
 // Dense evaluation of one queue (HEAVY: LJ + LK, else LJ only; elec: the
 // elec energy in .atr); returns the lane's energy sums.  Entries come in
 // screening order, so lanes sharing a1 are mostly contiguous: their a1
 // forces are summed with a segmented shuffle reduction and added once per
 // segment.
 template <typename Real, bool GRAD, bool HEAVY, int TERM = kTermLJLK>
-__device__ __noinline__ E3<Real> eval_queue(EvalCtx<Real> c, Slab<Real>* wp,
+__device__ TMOL_B200_LJLK_OUTLINE E3<Real> eval_queue(EvalCtx<Real> c, Slab<Real>* wp,
                                             int n, int lane) {
   Slab<Real>& w = *wp;
   E3<Real> acc = {0, 0, 0};
@@ -900,7 +906,7 @@ __device__ __forceinline__ void queue_push(uint16_t* queue, bool in, bool hv,
 // intra-block separation table (ljlk_pose_score.impl.hh:115-134; the ligand
 // 3/4 -> 5 rule is already folded into that table and is not applied again).
 template <typename Real, bool GRAD, int TERM = kTermLJLK>
-__device__ __noinline__ E3<Real> intra_tile(EvalCtx<Real> c, Slab<Real>* wp,
+__device__ TMOL_B200_LJLK_OUTLINE E3<Real> intra_tile(EvalCtx<Real> c, Slab<Real>* wp,
                                             int st1, int c1, int lane) {
   Slab<Real>& w = *wp;
   E3<Real> acc = {0, 0, 0};
@@ -943,7 +949,7 @@ __device__ __noinline__ E3<Real> intra_tile(EvalCtx<Real> c, Slab<Real>* wp,
 // step, skipping those farther than r_k + max_dis from every slot block's
 // centroid.  Returns the lane's energy sums.
 template <typename Real, bool GRAD, int TERM = kTermLJLK>
-__device__ __noinline__ E3<Real> screen_slots(EvalCtx<Real> c, Slab<Real>* wp,
+__device__ TMOL_B200_LJLK_OUTLINE E3<Real> screen_slots(EvalCtx<Real> c, Slab<Real>* wp,
                                               int c1, int nc1, int m, int ns,
                                               int lane) {
   Slab<Real>& w = *wp;
