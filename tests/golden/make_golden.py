@@ -39,6 +39,11 @@ Writes
                      gradient of sum(w * E) for seeded w
                      (``make_golden.py <tmol root> lkball_rotamers`` writes
                      this file alone)
+  lkball_block_pair.npz  the reference lk_ball_pose_score in block-pair mode
+                     on the synthetic pose of lkball.npz, float32 and
+                     float64: energies [4, P, B, B] and the gradient of
+                     sum(w * E) for seeded w (``... lkball_block_pair``
+                     writes this file alone)
   rotamers.npz       the reference rotamer-score op (ljlk_rotamer_scores) on
                      a seeded rotamer set over a jagged batch of poses: the
                      set itself, the rotamer-pair energies and dispatch
@@ -236,12 +241,32 @@ def lkball_rotamers():
     numpy.savez_compressed(os.path.join(HERE, "lkball_rotamers.npz"), **out)
 
 
+def lkball_block_pair():
+    """lkball_block_pair.npz"""
+    ps = synthetic_pose_stack(LKB_SYN[0], LKB_SYN[1], extra_chi_sd=LKB_SYN[2])
+    lterm = LKBallEnergyTerm()
+    out = {}
+    for dt, dn in ((torch.float32, "f32"), (torch.float64, "f64")):
+        wa = water_gen_args(ps, lterm)
+        sa = score_args(ps, lterm, None, block_pair=True)
+        wa = [a.to(dt) if isinstance(a, torch.Tensor) and a.is_floating_point() else a for a in wa]
+        sa = [a.to(dt) if isinstance(a, torch.Tensor) and a.is_floating_point() else a for a in sa]
+        E, W, c, nbr = O.reference_lkball(ps.coords.flatten(0, 1).to(dt), wa, sa)
+        w = torch.tensor(numpy.random.default_rng(12).normal(size=tuple(E.shape)), dtype=dt)
+        (E * w).sum().backward()
+        out.update({f"{dn}_energies": E.detach().numpy(), f"{dn}_weights": w.numpy(), f"{dn}_grad": c.grad.numpy()})
+    numpy.savez_compressed(os.path.join(HERE, "lkball_block_pair.npz"), **out)
+
+
 if __name__ == "__main__":
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     only = sys.argv[2] if len(sys.argv) > 2 else None
     if only == "lkball_rotamers":
         lkball_rotamers()
+    elif only == "lkball_block_pair":
+        lkball_block_pair()
     else:
         main(root)
         lkball_rotamers()
+        lkball_block_pair()
     print("wrote fixtures to", HERE)

@@ -7,7 +7,8 @@ lk_ball_pose_score) through the C ABI.
   through the waters (1e-4 of its largest component);
 - against the C oracle on seeded multi-pose batches, float64 to 1e-9;
 - block-pair energies (upper triangle, summing to the whole-pose ones) and
-  their adjoint; float64 gradcheck of both ops;
+  their adjoint, against the reference op (tests/golden/lkball_block_pair.npz);
+  float64 gradcheck of both ops;
 - plan kinds: a water plan and a score plan serve their own entry points;
 - the rotamer op (waters on a rotamer set, lk_ball_rotamer_score): dispatch
   exact, energies and the gradient of a weighted sum against the reference
@@ -336,3 +337,25 @@ def test_rendered_scoring_modules(lterm):
     Em2, idx2 = rot(rs.coords.to(DEV))
     assert torch.equal(idx2, idxr)
     E_close(Em2.cpu().numpy(), Er.cpu().numpy(), rtol=1e-6, atol=1e-6)
+
+
+@pytest.mark.parametrize("f64", [False, True])
+def test_block_pair_matches_reference_fixture(lterm, f64):
+    """Block-pair energies [4, P, B, B] (upper triangle, as the reference
+    writes them) and the gradient of sum(w * E) through the waters against
+    the reference op (tests/golden/lkball_block_pair.npz)."""
+    g = load_golden("lkball_block_pair.npz")
+    lk = load_golden("lkball.npz")
+    ps = synthetic_pose_stack(list(lk["syn_sizes"]), list(lk["syn_seeds"]), extra_chi_sd=float(lk["syn_chi_sd"]))
+    dn = "f64" if f64 else "f32"
+    dt = torch.float64 if f64 else torch.float32
+    wa, sa = static_args(ps, lterm, dt)
+    coords = ps.coords.flatten(0, 1).to(DEV, dt).requires_grad_(True)
+    E, _ = lk_ball_pose_score(coords, *sa, gen_pose_waters(coords, *wa), True)
+    (E * torch.as_tensor(g[f"{dn}_weights"], device=DEV)).sum().backward()
+    if f64:
+        E_close(E.detach().cpu().numpy(), g[f"{dn}_energies"], rtol=1e-10, atol=1e-10)
+        g_close(coords.grad.cpu().numpy(), g[f"{dn}_grad"], rtol=1e-9)
+    else:
+        E_close(E.detach().cpu().numpy(), g[f"{dn}_energies"])
+        g_close(coords.grad.cpu().numpy(), g[f"{dn}_grad"])
