@@ -787,8 +787,8 @@ struct LkbTagged {
 // weights w, adding energies to e4, and shifts what is left to the front.
 // TAGGED: each entry's weights and energies are those of its tag's row.
 template <typename Real, bool GRAD, bool TAGGED>
-__device__ __forceinline__ void lkb_pump(const LkbEval<Real>& ev, LkbWarp<Real, TAGGED>& q, bool all, const Lkb4<Real>& w,
-                                         Real* e4, const LkbTagged<Real>& tg = LkbTagged<Real>{}) {
+__device__ __forceinline__ void lkb_pump(const LkbEval<Real>& ev, LkbWarp<Real, TAGGED>& q, bool all, const Lkb4<Real> w,
+                                         Real* e4, const LkbTagged<Real> tg) {
   for (;;) {
     int which, n;
     if (q.nq[0] >= 32) {
@@ -817,7 +817,7 @@ __device__ __forceinline__ void lkb_pump(const LkbEval<Real>& ev, LkbWarp<Real, 
     } else {
       for (int c = 0; c < 4; ++c) e4[c] += got.v[c];
     }
-    const int rest = q.nq[which] - n;
+    const int rest = (which ? q.nq[1] : q.nq[0]) - n;
     int a = 0, b = 0, c = 0, d = 0, e = 0, f = 0;
     if (lane < rest) {
       a = Q.rp[n + lane], b = Q.ro[n + lane], c = Q.pi[n + lane], d = Q.oi[n + lane], e = Q.sep[n + lane];
@@ -829,7 +829,10 @@ __device__ __forceinline__ void lkb_pump(const LkbEval<Real>& ev, LkbWarp<Real, 
       if (TAGGED) Q.tag[lane] = f;
     }
     __syncwarp();
-    q.nq[which] = rest;
+    if (which)
+      q.nq[1] = rest;
+    else
+      q.nq[0] = rest;
   }
 }
 
@@ -853,8 +856,8 @@ template <typename Real, bool GRAD, bool TAGGED>
 __device__ __forceinline__ void lkb_enqueue_pairs(const ScoreArgs<Real>& s, const LkbArgs<Real>& k,
                                                   const LkbEval<Real>& ev, LkbWarp<Real, TAGGED>& q, const LkbSide& a,
                                                   const LkbSide& b, bool intra, bool striking, int nc1, int nc2,
-                                                  const uint8_t* seps, const Lkb4<Real>& w, Real* e4,
-                                                  int tag = 0, const LkbTagged<Real>& tg = LkbTagged<Real>{}) {
+                                                  const uint8_t* seps, const Lkb4<Real> w, Real* e4, int tag,
+                                                  const LkbTagged<Real> tg) {
   const int lane = q.lane;
   const int no = intra ? a.nocc : b.nocc;
   const int n01 = a.npol * no;
@@ -916,7 +919,7 @@ __device__ __forceinline__ void lkb_enqueue_pairs(const ScoreArgs<Real>& s, cons
     if (in_reach) {
       const int which = bridged ? 1 : 0;
       LkbQueue<TAGGED>& Q = q.qs[which];
-      const int pos = q.nq[which] + __popc((bridged ? m1 : m0) & q.lt_mask);
+      const int pos = (bridged ? q.nq[1] : q.nq[0]) + __popc((bridged ? m1 : m0) & q.lt_mask);
       Q.rp[pos] = rp;
       Q.ro[pos] = ro;
       Q.pi[pos] = pidx;
