@@ -883,6 +883,66 @@ def run_lkball_rotamers(args, world, rank, local):
     return 0
 
 
+def pipelined_e2e_ms(plan, weights, h_coords, flush, steps, world, P, n_terms=3):
+    """Device time (max over ranks) of `steps` energy + gradient steps
+    through the plan's C entry point, each with its host->device copy of
+    the coordinates, an L2 flush and the device->host copy of energies and
+    gradient, double-buffered over a copy-in, a compute and a copy-out
+    stream."""
+    import torch
+
+    dev = h_coords.device if h_coords.is_cuda else torch.device("cuda", torch.cuda.current_device())
+    s_in, s_run, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    d_in = [torch.empty(h_coords.shape, device=dev) for _ in range(2)]
+    E = [torch.empty((n_terms, P), device=dev) for _ in range(2)]
+    dx = [torch.empty(h_coords.shape, device=dev) for _ in range(2)]
+    h_E = [torch.empty((n_terms, P), pin_memory=True) for _ in range(2)]
+    h_g = [torch.empty(h_coords.shape, pin_memory=True) for _ in range(2)]
+    ev = lambda: torch.cuda.Event()  # noqa: E731
+    copied_in = [ev(), ev()]
+    computed = [ev(), ev()]
+    copied_out = [ev(), ev()]
+    for e in copied_in + computed + copied_out:
+        e.record(torch.cuda.current_stream(dev))
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def run(n, timed):
+        cur = torch.cuda.current_stream(dev)
+        if timed:
+            start.record(cur)
+        for s_ in (s_in, s_run, s_out):
+            s_.wait_stream(cur)
+        for k in range(n):
+            b = k & 1
+            with torch.cuda.stream(s_in):
+                s_in.wait_event(computed[b])  # d_in[b] no longer read
+                d_in[b].copy_(h_coords, non_blocking=True)
+                copied_in[b].record(s_in)
+            with torch.cuda.stream(s_run):
+                s_run.wait_event(copied_in[b])
+                s_run.wait_event(copied_out[b])  # E[b], dx[b] copied out
+                flush.zero_()
+                plan.energy_and_gradient(d_in[b], weights, E[b], dx[b])
+                computed[b].record(s_run)
+            with torch.cuda.stream(s_out):
+                s_out.wait_event(computed[b])
+                h_E[b].copy_(E[b], non_blocking=True)
+                h_g[b].copy_(dx[b], non_blocking=True)
+                copied_out[b].record(s_out)
+        for s_ in (s_in, s_run, s_out):
+            cur.wait_stream(s_)
+        if timed:
+            end.record(cur)
+
+    run(3, False)
+    torch.cuda.synchronize()
+    barrier(world)
+    run(steps, True)
+    torch.cuda.synchronize()
+    barrier(world)
+    return max_over_ranks(start.elapsed_time(end), world)
+
+
 def ctypes_ptr(t):
     import ctypes
 
@@ -1194,7 +1254,8 @@ def run_elec(args, world, rank, local):
         e2e_ev[k][1].record()
     torch.cuda.synchronize()
     barrier(world)
-    e2e_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in e2e_ev), world)
+    serial_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in e2e_ev), world)
+    e2e_ms = pipelined_e2e_ms(plan, w, h_coords, flush, args.steps, world, P, n_terms=1)
 
     fp32_peak = native.measure_fp32_peak_tflops(torch.cuda.current_stream().cuda_stream)
     cpu = None
@@ -1254,6 +1315,9 @@ def run_elec(args, world, rank, local):
                 "unit": "poses/s",
                 "h2d_bytes_per_step": coords.numel() * 4,
                 "d2h_bytes_per_step": (P + coords.numel()) * 4,
+                "schedule": "double-buffered over copy-in / compute / copy-out streams; L2 flushed before every "
+                "step's compute, inside the timed region",
+                "serial_value": poses_total / (serial_ms / 1e3),
             },
             "cpu_baseline": cpu,
         }
@@ -1473,7 +1537,8 @@ def run_lkball(args, world, rank, local):
         h_E.copy_(E1, non_blocking=True)
         h_g.copy_(dx1, non_blocking=True)
 
-    e2e_ms = timed(e2e_c_abi)
+    serial_ms = timed(e2e_c_abi)
+    e2e_ms = pipelined_e2e_ms(plan, w1, h_coords, flush, args.steps, world, P, n_terms=4)
     dropin_ms = timed(e2e_step)
 
     fp32_peak = native.measure_fp32_peak_tflops(torch.cuda.current_stream().cuda_stream)
@@ -1538,6 +1603,9 @@ def run_lkball(args, world, rank, local):
                 "h2d_bytes_per_step": coords.numel() * 4,
                 "d2h_bytes_per_step": (4 * P + coords.numel()) * 4,
                 "path": "tmol_b200_lkball_energy_and_gradient (C ABI) with host buffers",
+                "schedule": "double-buffered over copy-in / compute / copy-out streams; L2 flushed before every "
+                "step's compute, inside the timed region",
+                "serial_value": poses_total / (serial_ms / 1e3),
             },
             "e2e_dropin_ops": {
                 "value": poses_total / (dropin_ms / 1e3),
@@ -1965,7 +2033,12 @@ def run_b200(args, world, rank, local):
         e2e_ev[k][1].record()
     torch.cuda.synchronize()
     barrier(world)
-    e2e_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in e2e_ev), world)
+    serial_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in e2e_ev), world)
+    # the same steps double-buffered over three streams, as a host pipeline
+    # runs them: step k+1's coordinates go in and step k-1's results come out
+    # while step k computes; every step still copies its inputs in, flushes
+    # L2 and copies its energies and gradient out inside the timed region
+    e2e_ms = pipelined_e2e_ms(plan, weights, h_coords, flush, args.steps, world, P)
     e2e_value = poses_total / (e2e_ms / 1e3)
     h2d = coords.numel() * 4
     d2h = (3 * P + coords.numel()) * 4
@@ -2046,6 +2119,9 @@ def run_b200(args, world, rank, local):
                 "unit": "poses/s",
                 "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h,
+                "schedule": "double-buffered over copy-in / compute / copy-out streams; L2 flushed before every "
+                "step's compute, inside the timed region",
+                "serial_value": poses_total / (serial_ms / 1e3),
             },
             "cpu_baseline": cpu,
             "screened": screened,
