@@ -63,6 +63,16 @@ def test_status_strings_and_argument_checks():
     assert lib.tmol_b200_elec_plan_destroy(None) == 1
     assert lib.tmol_b200_elec_forward(None, None, 0, None, None, None) == 1
     assert lib.tmol_b200_elec_rotamer_fill(None, None, None, None) == 1
+    # and the LK-ball ones: a plan needs the water or the scoring tables
+    assert lib.tmol_b200_lkball_plan_create(None, 4, None, None, ctypes.byref(out)) == 1
+    k = native.LKBallInputs()
+    assert lib.tmol_b200_lkball_plan_create(ctypes.byref(k), 4, None, None, ctypes.byref(out)) == 1
+    assert lib.tmol_b200_lkball_rotamer_plan_create(ctypes.byref(k), 4, None, None, ctypes.byref(out)) == 1
+    assert lib.tmol_b200_lkball_plan_destroy(None) == 1
+    assert lib.tmol_b200_lkball_waters(None, None, None, None) == 1
+    assert lib.tmol_b200_lkball_forward(None, None, None, 0, None, None, None) == 1
+    assert lib.tmol_b200_lkball_energy_and_gradient(None, None, None, None, None, None) == 1
+    assert lib.tmol_b200_lkball_rotamer_fill(None, None, None, None) == 1
 
 
 def test_op_refuses_cpu_tensors(ubq_pose_stack, term):
