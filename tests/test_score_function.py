@@ -57,3 +57,33 @@ def test_rendered_modules_sum_the_terms():
     pairs = sfxn.render_block_pair_scoring_module(ps)(ps.coords)
     numpy.testing.assert_allclose(pairs.sum(dim=(1, 2)).cpu().numpy(), total.detach().cpu().numpy(), rtol=1e-4,
                                   atol=1e-2)
+
+
+@pytest.mark.gpu
+def test_minimise_the_full_score_function():
+    """The ScoreFunction's module drives the batched L-BFGS: the weighted
+    LJ/LK + elec + LK-ball energy of every pose falls, and its float64
+    gradient (through the LK-ball waters) matches central differences."""
+    from tmol_b200.optimization.minimize import minimize_module
+
+    dev = torch.device("cuda:0")
+    ps = synthetic_pose_stack([18, 9], [81, 82], extra_chi_sd=25.0, device=dev)
+    sfxn = ScoreFunction.from_weights(WEIGHTS, device=dev)
+    whole = sfxn.render_whole_pose_scoring_module(ps)
+    x0 = ps.coords.double()
+    E0 = whole(x0).detach()
+    x, E, g, opt = minimize_module(whole, x0, max_iter=40)
+    assert (E < E0).all()
+    c = x0.clone().requires_grad_(True)
+    whole(c).sum().backward()
+    gen = numpy.random.default_rng(5)
+    real = torch.nonzero(c.grad.abs().sum(-1).flatten() > 0).squeeze(-1).cpu().numpy()
+    h = 1e-5
+    for flat in gen.choice(real, size=12, replace=False):
+        p_, a_ = divmod(int(flat), ps.coords.shape[1])
+        k = int(gen.integers(3))
+        xp, xm = x0.clone(), x0.clone()
+        xp[p_, a_, k] += h
+        xm[p_, a_, k] -= h
+        fd = (whole(xp).sum() - whole(xm).sum()).item() / (2 * h)
+        assert abs(fd - c.grad[p_, a_, k].item()) <= 1e-5 * max(1.0, abs(fd)), (p_, a_, k)

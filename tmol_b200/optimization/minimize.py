@@ -84,6 +84,26 @@ def minimize(pose_stack, term=None, max_iter=200, weights=BETA2016_WEIGHTS, **kw
     return x.reshape(P, A, 3), E, g, opt
 
 
+def minimize_module(module, coords, max_iter=200, **kw):
+    """Minimise any whole-pose scoring module (a term's, or a
+    ScoreFunction's: ``(coords [P, A, 3]) -> [P]`` per-pose energies,
+    differentiable) from coords [P, A, 3]; the gradient comes from autograd
+    through the terms' adjoint kernels.  Returns (coords, E, g, optimiser)."""
+    P, A = coords.shape[0], coords.shape[1]
+
+    def func(x):
+        c = x.detach().reshape(P, A, 3).requires_grad_(True)
+        E = module(c)
+        if E.dim() > 1:
+            E = E.sum(0)
+        (g,) = torch.autograd.grad(E.sum(), c)
+        return E.detach(), g.reshape(P, -1)
+
+    opt = LBFGSArmijo(func, coords.detach().reshape(P, -1), max_iter=max_iter, **kw)
+    x, E, g = opt.run()
+    return x.reshape(P, A, 3), E, g, opt
+
+
 def main():
     from ..pose.synthetic import synthetic_pose_stack
 
