@@ -214,13 +214,20 @@ def dist_setup():
     return world, rank, local
 
 
+def _reduce_device():
+    import torch.distributed as dist
+
+    # NCCL reduces device tensors; gloo (the CPU tests of this logic) host ones
+    return "cuda" if dist.get_backend() == "nccl" else "cpu"
+
+
 def max_over_ranks(x, world):
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_reduce_device())
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return t.item()
 
@@ -231,7 +238,7 @@ def sum_over_ranks(x, world):
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_reduce_device())
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return t.item()
 
