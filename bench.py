@@ -61,6 +61,11 @@ LKBALL_METRIC = "LK-ball energy+grad poses/s (64x150-residue batch, waters inclu
 LKB_ROT_METRIC = (
     "LK-ball rotamer-pair energies/s (16 poses x 150 residues, 1-31 rotamers per block, waters included, 1 B200)"
 )
+SFXN_METRIC = "score function (LJ/LK + elec + LK-ball) energy+grad poses/s (64x150-residue batch, 1 B200)"
+# weights of the eight score types (fa_ljatr, fa_ljrep, fa_lk, fa_elec,
+# lk_ball_iso, lk_ball, lk_bridge, lk_bridge_uncpl), as in tmol's beta-2016
+# style score functions
+SFXN_WEIGHTS = (1.0, 0.55, 1.0, 1.0, -0.38, 0.92, -0.33, -0.33)
 BONDSEP_METRIC = "inter-block bond separation poses/s (256-pose uneven batch, dense [P,B,B,C,C] + min, 1 B200)"
 
 # Algorithmic FLOPs per unit (E + dE), counted on the restatement's most
@@ -96,7 +101,7 @@ def workload_sizes(name, rank):
 
     from tmol_b200.pose.synthetic import log_uniform_sizes
 
-    if name in ("uniform64x150", "elec64x150", "lkball64x150"):
+    if name in ("uniform64x150", "elec64x150", "lkball64x150", "sfxn64x150"):
         return [N_RES] * N_POSES, [rank * N_POSES + k for k in range(N_POSES)]
     rng = numpy.random.default_rng(UNEVEN_SEED + 1000 * rank)
     sizes = log_uniform_sizes(rng, UNEVEN_POSES, 20, 1000)
@@ -125,6 +130,11 @@ def rotamer_workload(rank, device, sizes=None, seeds=None):
 def workload_label(name):
     if name == "elec64x150":
         return f"{N_POSES} poses x {N_RES} residues, fa_elec energy + gradient"
+    if name == "sfxn64x150":
+        return (
+            f"{N_POSES} poses x {N_RES} residues, fa_ljatr + fa_ljrep + fa_lk + fa_elec + the four LK-ball terms, "
+            f"weighted sum and its gradient, weights {list(SFXN_WEIGHTS)}"
+        )
     if name == "lkball64x150":
         return (
             f"{N_POSES} poses x {N_RES} residues, lk_ball_iso + lk_ball + lk_bridge + lk_bridge_uncpl "
@@ -287,7 +297,7 @@ def cpu_reference_sample(ps, term, reps=3):
 def _ref_worker(conn, sizes, seeds, term="ljlk"):
     """One single-threaded process of the reference arm: builds its share of
     the poses (same sizes and seeds as the GPU arm) and scores it on demand
-    (`term`: "ljlk", "elec" or "lkball")."""
+    (`term`: "ljlk", "elec", "lkball" or "sfxn": all three, weighted)."""
     import torch
 
     torch.set_num_threads(1)
@@ -296,6 +306,43 @@ def _ref_worker(conn, sizes, seeds, term="ljlk"):
 
     ps = synthetic_pose_stack(sizes, seeds)
     coords = ps.coords.flatten(0, 1).clone()
+    if term == "sfxn":
+        import numpy
+
+        from tmol_b200.score.elec_energy_term import ElecEnergyTerm, elec_pose_score_args
+        from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm, pose_score_args
+        from tmol_b200.score.lkball_energy_term import LKBallEnergyTerm, score_args, water_gen_args
+
+        lt = LKBallEnergyTerm()
+        la, ea = pose_score_args(ps, LJLKEnergyTerm()), elec_pose_score_args(ps, ElecEnergyTerm())
+        wa, sa = water_gen_args(ps, lt), score_args(ps, lt, None)
+        avail = O.reference_available() and O.reference_elec_available() and O.reference_lkball_available()
+        if avail:
+            O.reference_elec_pose_scores(coords, ea)  # loads the op libraries
+            ljlk_op, elec_op = O.load_reference(), torch.ops.tmol_elec.elec_pose_scores
+        else:
+            ocs = (O.OracleCall(coords, la), O.OracleCall(coords, ea, term="elec"),
+                   O.OracleCall(coords, sa, term="lkball", lkb_water_args=wa))
+        wts = torch.tensor(SFXN_WEIGHTS)
+        conn.send("ready")
+        while True:
+            msg = conn.recv()
+            if msg is None:
+                break
+            t0 = time.perf_counter()
+            if avail:
+                c = coords.clone().requires_grad_(True)
+                E1, _ = ljlk_op(c, *la)
+                E2, _ = elec_op(c, *ea)
+                El, _, cl, _ = O.reference_lkball(coords, wa, sa)
+                ((wts[:3, None] * E1).sum() + (wts[3] * E2).sum()).backward()
+                (wts[4:, None] * El).sum().backward()
+            else:
+                ocs[0].pose_scores(require_gradient=True)
+                ocs[1].pose_scores(require_gradient=True)
+                ocs[2].lkb_scores(ocs[2].lkb_waters(), weights=numpy.ones((4, ps.n_poses)))
+            conn.send(time.perf_counter() - t0)
+        return
     if term == "lkball":
         import numpy
 
@@ -414,7 +461,8 @@ def run_reference(args, world, rank):
         return run_reference_bondsep(args)
     elec = args.workload == "elec64x150"
     lkball = args.workload == "lkball64x150"
-    term = "elec" if elec else ("lkball" if lkball else "ljlk")
+    sfxn = args.workload == "sfxn64x150"
+    term = "elec" if elec else ("lkball" if lkball else ("sfxn" if sfxn else "ljlk"))
     sizes, seeds = workload_sizes(args.workload, 0)
     n_poses = len(sizes)
     n_proc = min(os.cpu_count() or 1, n_poses)
@@ -457,11 +505,14 @@ def run_reference(args, world, rank):
         kind = "reference" if O.reference_elec_available() else "port"
     elif lkball:
         kind = "reference" if O.reference_lkball_available() else "port"
+    elif sfxn:
+        both = O.reference_available() and O.reference_elec_available() and O.reference_lkball_available()
+        kind = "reference" if both else "port"
     else:
         kind = "reference" if O.reference_available() else "port"
     line = {
         "impl": "reference",
-        "metric": ELEC_METRIC if elec else (LKBALL_METRIC if lkball else METRIC),
+        "metric": ELEC_METRIC if elec else (LKBALL_METRIC if lkball else (SFXN_METRIC if sfxn else METRIC)),
         "value": value,
         "unit": "poses/s",
         "n_gpus": args.gpus,
@@ -1630,6 +1681,200 @@ def run_lkball(args, world, rank, local):
     return 0
 
 
+def run_sfxn(args, world, rank, local):
+    """The three terms as one score function on the uniform batch: per step
+    each plan's one-call energy + gradient (LJ/LK, elec, LK-ball with its
+    waters) under the score-type weights, and the summed gradient; replayed
+    as a CUDA graph."""
+    import torch
+
+    from tmol_b200 import native
+    from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm, pose_score_args
+    from tmol_b200.score.ljlk_op import LJLKPlan
+    from tmol_b200.tune import autotune
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    sizes, seeds = workload_sizes("sfxn64x150", rank)
+    ps = workload(rank, "sfxn64x150", device=dev)
+    coords = ps.coords.flatten(0, 1).to(dev).contiguous()
+    P = ps.n_poses
+    plans = [
+        LJLKPlan(coords, pose_score_args(ps, LJLKEnergyTerm(device=dev))[:-1]),
+        elec_plan_for(ps, coords),
+        lkball_plan_for(ps, coords),
+    ]
+    del ps
+    wt = torch.tensor(SFXN_WEIGHTS, device=dev)
+    ws = [wt[0:3, None].expand(3, P).contiguous(), wt[3:4, None].expand(1, P).contiguous(),
+          wt[4:8, None].expand(4, P).contiguous()]
+    Es = [torch.empty((w.shape[0], P), device=dev) for w in ws]
+    dxs = [torch.empty_like(coords) for _ in plans]
+    dx = torch.empty_like(coords)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, device=dev, dtype=torch.float32)
+
+    side = [torch.cuda.Stream(dev) for _ in plans]
+
+    def step(c=coords):
+        # the terms are independent: one stream each (parallel branches in
+        # the captured graph), joined for the gradient sum
+        cur = torch.cuda.current_stream(dev)
+        for sd, plan, w, E, g in zip(side, plans, ws, Es, dxs):
+            sd.wait_stream(cur)
+            with torch.cuda.stream(sd):
+                plan.energy_and_gradient(c, w, E, g)
+        for sd in side:
+            cur.wait_stream(sd)
+        torch.add(dxs[0], dxs[1], out=dx)
+        dx.add_(dxs[2])
+
+    # each term's launch shape autotuned on its own call, work ordered by cost
+    for plan, w, E, g in zip(plans, ws, Es, dxs):
+        autotune(plan, lambda plan=plan, w=w, E=E, g=g: plan.energy_and_gradient(coords, w, E, g), use_cache=False)
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    st = torch.cuda.Stream()
+    st.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(st):
+        step()
+        torch.cuda.synchronize()
+        with torch.cuda.graph(g, stream=st):
+            step()
+    torch.cuda.current_stream().wait_stream(st)
+    for _ in range(max(args.warmup, 3)):
+        g.replay()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record()
+            g.replay()
+            ev[k][1].record()
+        torch.cuda.synchronize()
+    barrier(world)
+    ms_max = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), world)
+    poses_total = sum_over_ranks(P * args.steps, world)
+    value = poses_total / (ms_max / 1e3)
+    # the scoring kernels' own times and the FLOP models' work
+    kern_ms, flops = 0.0, 0.0
+    for i, (plan, w, E, gg) in enumerate(zip(plans, ws, Es, dxs)):
+        plan.profile(True)
+        for _ in range(args.steps):
+            flush.zero_()
+            plan.energy_and_gradient(coords, w, E, gg)
+        ms, n = plan.profile_read()
+        plan.profile(False)
+        kern_ms += ms / max(n, 1)
+        c = plan.last_counts()
+        if i == 0:
+            flops += c["atom_pairs"] * F_PAIR_TEST + c["atom_pairs_in_range"] * F_LJ + c["heavy_pairs_in_range"] * F_LK
+        elif i == 1:
+            flops += c["atom_pairs"] * F_PAIR_TEST + c["atom_pairs_in_range"] * F_ELEC
+        else:
+            flops += c["pairs_evaluated"] * F_LKB_PAIR + c["bridged_pairs"] * F_LKB_BRIDGE
+    # end to end: pinned coordinates in, the weighted totals and the summed
+    # gradient out, step by step
+    h_coords = coords.cpu().pin_memory()
+    h_E = torch.empty((P,), pin_memory=True)
+    h_g = torch.empty(coords.shape, pin_memory=True)
+    d_in = torch.empty_like(coords)
+    total = torch.empty((P,), device=dev)
+    e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier(world)
+    for k in range(args.steps + 2):
+        flush.zero_()
+        if k >= 2:
+            e2e_ev[k - 2][0].record()
+        d_in.copy_(h_coords, non_blocking=True)
+        step(d_in)
+        torch.sum(torch.cat([w * E for w, E in zip(ws, Es)]), dim=0, out=total)
+        h_E.copy_(total, non_blocking=True)
+        h_g.copy_(dx, non_blocking=True)
+        if k >= 2:
+            e2e_ev[k - 2][1].record()
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in e2e_ev), world)
+    fp32_peak = native.measure_fp32_peak_tflops(torch.cuda.current_stream().cuda_stream)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from tmol_b200.pose.synthetic import synthetic_pose_stack
+
+        n_sample = 8
+        ps0 = synthetic_pose_stack(sizes[:n_sample], seeds[:n_sample])
+        k1, t1 = cpu_reference_sample(ps0, LJLKEnergyTerm(), reps=2)
+        k2, t2 = cpu_elec_sample(ps0, reps=2)
+        k3, t3 = cpu_lkball_sample(ps0, reps=2)
+        cpu = {
+            "value": n_sample / (t1 + t2 + t3),
+            "unit": "poses/s",
+            "cores": 1,
+            "kind": "reference" if k1 == k2 == k3 == "reference" else "port",
+            "sample": f"{n_sample} of the {len(sizes)} {N_RES}-residue poses, the three reference ops (LK-ball with "
+            "its waters), energies + gradient, best of 2 each, one thread",
+        }
+    if rank == 0:
+        achieved = flops / (kern_ms * 1e-3) / 1e12
+        line = {
+            "metric": SFXN_METRIC,
+            "value": value,
+            "unit": "poses/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded proteins, ideal geometry)",
+            "config": {
+                "workload": workload_label("sfxn64x150"),
+                "poses_per_gpu": P,
+                "atoms_per_gpu": int(coords.shape[0]),
+                "l2": "flushed (256 MiB write) before every timed step",
+                "launch": "CUDA graph replay: 10 kernels per step (LJ/LK 2, elec 2, LK-ball 4 on three concurrent "
+                "streams, gradient sum 2)",
+                "parallelism": f"weak, {world} independent batch(es)",
+            },
+            "gpu_launches": 10 * args.steps,
+            "clocks": clk.summary(),
+            "roofline": {
+                "bound": "fp32",
+                "achieved": achieved,
+                "peak": fp32_peak,
+                "unit": "TFLOP/s",
+                "frac": achieved / fp32_peak,
+                "traffic": None,
+                "kernel": "the three scoring kernels (score_kernel LJ/LK and elec, lkb_score_kernel), FLOPs and "
+                "times summed",
+                "kernel_ms": kern_ms,
+                "flops_per_launch": flops,
+                "peak_source": "measured: FMA-loop probe over all SMs in this run (tmol_b200_measure_fp32_peak)",
+            },
+            "e2e": {
+                "value": poses_total / (e2e_ms / 1e3),
+                "unit": "poses/s",
+                "h2d_bytes_per_step": coords.numel() * 4,
+                "d2h_bytes_per_step": (P + coords.numel()) * 4,
+                "schedule": "step by step",
+            },
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    del g
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
 def _bondsep_port_worker(conn, sizes, seeds):
     """One single-threaded process of the bond-separation CPU arm: the C
     restatement of the reference route (connection-point matrix, shortest
@@ -2154,7 +2399,7 @@ def main():
         default="uniform64x150",
         choices=[
             "uniform64x150", "uneven256", "rotamers16x150", "elec64x150", "lkball64x150", "lkball_rotamers16x150",
-            "bondsep256",
+            "sfxn64x150", "bondsep256",
         ],
     )
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -2180,6 +2425,8 @@ def main():
         return run_lkball(args, world, rank, local)
     if args.workload == "lkball_rotamers16x150":
         return run_lkball_rotamers(args, world, rank, local)
+    if args.workload == "sfxn64x150":
+        return run_sfxn(args, world, rank, local)
     if args.workload == "bondsep256":
         return run_bondsep(args, world, rank, local)
     return run_b200(args, world, rank, local)
