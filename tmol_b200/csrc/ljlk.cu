@@ -1891,7 +1891,9 @@ struct tmol_b200_ljlk_plan {
   int lkb_maxpol = 0, lkb_maxocc = 0;
   void* lkb_par = nullptr;
   double lkb_water_dist = 0;
-  void* lkb_waters = nullptr;   // [N, 4, 3] scratch of the one-call energy + gradient
+  int* lkb_active = nullptr;    // occupied water sites, ascending
+  int64_t lkb_n_active = 0;
+  void* lkb_waters = nullptr;   // [N, 4, 3] scratch of the one-call energy + gradient (NaN in empty slots)
   void* lkb_dwaters = nullptr;
   tmol_b200_ljlk_inputs dims;  // sizes only; pointers are not kept
   int P, B, nbt, A, C, ntiles, T;
@@ -1983,7 +1985,7 @@ void free_plan(tmol_b200_ljlk_plan* pl) {
                   pl->rob,       pl->rot_spheres, pl->row_pairs,  pl->row_items,
                   pl->bt_q,      pl->elec_k,      pl->lkb_sites,   pl->lkb_pol,
                   pl->lkb_npol,  pl->lkb_occ,     pl->lkb_nocc,    pl->lkb_par,
-                  pl->lkb_waters, pl->lkb_dwaters, pl->lkb_nbocc};
+                  pl->lkb_waters, pl->lkb_dwaters, pl->lkb_nbocc, pl->lkb_active};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t e : pl->prof_events) cudaEventDestroy(e);
@@ -2275,6 +2277,8 @@ LkbArgs<Real> lkb_args(tmol_b200_ljlk_plan* pl) {
   LkbArgs<Real> k = {};
   k.sites = (const LkbSite<Real>*)pl->lkb_sites;
   k.n_sites = pl->N * LKB_NW;
+  k.active = pl->lkb_active;
+  k.n_active = pl->lkb_n_active;
   k.pol = pl->lkb_pol;
   k.npol = pl->lkb_npol;
   k.occ = pl->lkb_occ;
@@ -2292,12 +2296,18 @@ LkbArgs<Real> lkb_args(tmol_b200_ljlk_plan* pl) {
   return k;
 }
 
+// `prefilled`: the empty slots of `waters` already hold NaN (the plan's
+// scratch, filled once)
 template <typename Real>
-int lkb_waters_impl(tmol_b200_ljlk_plan* pl, const void* coords, void* waters, cudaStream_t st) {
+int lkb_waters_impl(tmol_b200_ljlk_plan* pl, const void* coords, void* waters, cudaStream_t st,
+                    bool prefilled = false) {
   LkbArgs<Real> k = lkb_args<Real>(pl);
   k.waters_out = (Real*)waters;
   if (k.n_sites == 0) return TMOL_B200_OK;
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((k.n_sites + 255) / 256, (int64_t)pl->n_sm * 16));
+  // all-ones bytes are a NaN in float and double
+  if (!prefilled) CK(cudaMemsetAsync(waters, 0xff, sizeof(Real) * 3 * (size_t)k.n_sites, st));
+  if (k.n_active == 0) return TMOL_B200_OK;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((k.n_active + 255) / 256, (int64_t)pl->n_sm * 16));
   lkb_waters_kernel<Real><<<grid, 256, 0, st>>>(k, (const Real*)coords);
   CK(cudaGetLastError());
   return TMOL_B200_OK;
@@ -2308,8 +2318,8 @@ int lkb_waters_backward_impl(tmol_b200_ljlk_plan* pl, const void* coords, const 
                              cudaStream_t st) {
   LkbArgs<Real> k = lkb_args<Real>(pl);
   k.dwaters = (const Real*)dwaters;
-  if (k.n_sites == 0) return TMOL_B200_OK;
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((k.n_sites + 255) / 256, (int64_t)pl->n_sm * 16));
+  if (k.n_active == 0) return TMOL_B200_OK;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((k.n_active + 255) / 256, (int64_t)pl->n_sm * 16));
   lkb_waters_backward_kernel<Real><<<grid, 256, 0, st>>>(k, (const Real*)coords, (Real*)dcoords);
   CK(cudaGetLastError());
   return TMOL_B200_OK;
@@ -2504,6 +2514,7 @@ int build_lkball(tmol_b200_ljlk_plan* pl, const tmol_b200_lkball_inputs* k, cons
   }
   if (!waters) return TMOL_B200_OK;
   const int64_t n_sites = pl->N * LKB_NW;
+  if (n_sites >= ((int64_t)1 << 31)) return TMOL_B200_ERR_SHAPE;  // site indices are int
   if (scoring) {
     CK(dalloc(pl, (Real**)&pl->lkb_waters, (size_t)n_sites * 3));
     CK(dalloc(pl, (Real**)&pl->lkb_dwaters, (size_t)n_sites * 3));
@@ -2546,6 +2557,22 @@ int build_lkball(tmol_b200_ljlk_plan* pl, const tmol_b200_lkball_inputs* k, cons
         k->n_ring_tors, wg[1], wg[2], wg[3], (LkbSite<Real>*)pl->lkb_sites, pl->counters + 1);
     CK(cudaGetLastError());
   }
+  // the occupied sites, in ascending order (the per-call kernels visit only
+  // these); the plan's waters scratch holds NaN in the empty slots for good
+  std::vector<LkbSite<Real>> h_sites((size_t)n_sites);
+  if (n_sites > 0)
+    CK(cudaMemcpyAsync(h_sites.data(), pl->lkb_sites, sizeof(LkbSite<Real>) * n_sites, cudaMemcpyDeviceToHost,
+                       st));
+  CK(cudaStreamSynchronize(st));
+  std::vector<int> active;
+  for (int64_t i = 0; i < n_sites; ++i)
+    if (h_sites[i].kind != kLkbNone) active.push_back((int)i);
+  pl->lkb_n_active = (int64_t)active.size();
+  CK(dalloc(pl, &pl->lkb_active, active.size()));
+  if (!active.empty())
+    CK(cudaMemcpyAsync(pl->lkb_active, active.data(), sizeof(int) * active.size(), cudaMemcpyHostToDevice, st));
+  if (scoring && n_sites > 0)
+    CK(cudaMemsetAsync(pl->lkb_waters, 0xff, sizeof(Real) * 3 * (size_t)n_sites, st));
   return TMOL_B200_OK;
 }
 
@@ -3420,13 +3447,13 @@ int tmol_b200_lkball_energy_and_gradient(tmol_b200_lkball_plan* plan, const void
   cudaStream_t st = (cudaStream_t)stream;
   int rc;
   if (plan->real_bytes == 4) {
-    if ((rc = lkb_waters_impl<float>(plan, coords, plan->lkb_waters, st))) return rc;
+    if ((rc = lkb_waters_impl<float>(plan, coords, plan->lkb_waters, st, true))) return rc;
     if ((rc = lkb_score_impl<float, true, false>(plan, coords, plan->lkb_waters, energies, nullptr, weights,
                                                  dcoords, plan->lkb_dwaters, st)))
       return rc;
     return lkb_waters_backward_impl<float>(plan, coords, plan->lkb_dwaters, dcoords, st);
   }
-  if ((rc = lkb_waters_impl<double>(plan, coords, plan->lkb_waters, st))) return rc;
+  if ((rc = lkb_waters_impl<double>(plan, coords, plan->lkb_waters, st, true))) return rc;
   if ((rc = lkb_score_impl<double, true, false>(plan, coords, plan->lkb_waters, energies, nullptr, weights,
                                                 dcoords, plan->lkb_dwaters, st)))
     return rc;

@@ -31,6 +31,8 @@ template <typename Real>
 struct LkbArgs {
   const LkbSite<Real>* sites;  // [n_atoms * 4]
   int64_t n_sites;
+  const int* active;  // the occupied sites (kind != none), ascending
+  int64_t n_active;
   const Real* waters;   // [n_atoms][4][3]
   Real* waters_out;
   const Real* dwaters;  // adjoint in
@@ -349,30 +351,29 @@ __device__ inline void lkb_site_water(const LkbSite<Real>& s, const Real* coords
   for (int i = 0; i < 3; ++i) W[i] = A[i] + f.v[0] * f.e0[i] + f.v[1] * f.e1[i] + f.v[2] * f.e2[i];
 }
 
+// The waters of the occupied sites (the empty slots hold NaN, written
+// beforehand as a byte fill)
 template <typename Real>
 __global__ void lkb_waters_kernel(LkbArgs<Real> k, const Real* coords) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < k.n_sites;
-       i += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < k.n_active;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = k.active[j];
     const LkbSite<Real> s = k.sites[i];
     Real W[3];
-    if (s.kind == kLkbNone) {
-      W[0] = W[1] = W[2] = Real(NAN);
-    } else {
-      lkb_site_water(s, coords, k.water_dist, W);
-    }
+    lkb_site_water(s, coords, k.water_dist, W);
     k.waters_out[3 * i] = W[0];
     k.waters_out[3 * i + 1] = W[1];
     k.waters_out[3 * i + 2] = W[2];
   }
 }
 
-// dcoords += the adjoint of each site's water
+// dcoords += the adjoint of each occupied site's water
 template <typename Real>
 __global__ void lkb_waters_backward_kernel(LkbArgs<Real> k, const Real* coords, Real* dcoords) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < k.n_sites;
-       i += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < k.n_active;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = k.active[j];
     const LkbSite<Real> s = k.sites[i];
-    if (s.kind == kLkbNone) continue;
     const Real g[3] = {k.dwaters[3 * i], k.dwaters[3 * i + 1], k.dwaters[3 * i + 2]};
     if (g[0] == Real(0) && g[1] == Real(0) && g[2] == Real(0)) continue;
     Real A[3], Bv[3];
