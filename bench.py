@@ -919,8 +919,9 @@ def run_lkball_rotamers(args, world, rank, local):
                 "peak": fp32_peak,
                 "unit": "TFLOP/s",
                 "frac": achieved / fp32_peak,
-                "traffic": None,
+                "traffic": load_traffic("lkb_rotamer"),
                 "kernel": "lkb_rotamer_kernel<float, energies>, timed as graph replays",
+                "traffic_source": "ncu capture, profiles/lkb_rotamer_traffic.json",
                 "kernel_ms": e_ms,
                 "flops_per_launch": flops,
                 "peak_source": "measured: FMA-loop probe over all SMs in this run (tmol_b200_measure_fp32_peak)",
@@ -1015,8 +1016,10 @@ def flops_per_step(counts):
     )
 
 
-def load_traffic():
-    path = os.path.join(ROOT, "profiles", "ljlk_score_traffic.json")
+def load_traffic(name="ljlk_score"):
+    """DRAM bytes per launch of a scoring kernel from its committed ncu
+    capture (profiles/<name>_traffic.json), or None."""
+    path = os.path.join(ROOT, "profiles", f"{name}_traffic.json")
     try:
         with open(path) as f:
             d = json.load(f)
@@ -1362,8 +1365,9 @@ def run_elec(args, world, rank, local):
                 "peak": fp32_peak,
                 "unit": "TFLOP/s",
                 "frac": m["achieved_tflops"] / fp32_peak,
-                "traffic": None,
+                "traffic": load_traffic("elec_score"),
                 "kernel": "score_kernel<float, GRAD, elec> (fused neighbour + atom-pair energy and gradient)",
+                "traffic_source": "ncu capture, profiles/elec_score_traffic.json",
                 "kernel_ms": m["kernel_ms"],
                 "flops_per_launch": m["flops_per_launch"],
                 "peak_source": "measured: FMA-loop probe over all SMs in this run (tmol_b200_measure_fp32_peak)",
@@ -1649,8 +1653,9 @@ def run_lkball(args, world, rank, local):
                 "peak": fp32_peak,
                 "unit": "TFLOP/s",
                 "frac": m["achieved_tflops"] / fp32_peak,
-                "traffic": None,
+                "traffic": load_traffic("lkb_score"),
                 "kernel": "lkb_score_kernel<float, GRAD> (neighbour test + polar/occluder energies and adjoint)",
+                "traffic_source": "ncu capture, profiles/lkb_score_traffic.json",
                 "kernel_ms": m["kernel_ms"],
                 "flops_per_launch": m["flops_per_launch"],
                 "peak_source": "measured: FMA-loop probe over all SMs in this run (tmol_b200_measure_fp32_peak)",
