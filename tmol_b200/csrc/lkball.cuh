@@ -1080,8 +1080,8 @@ __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS) lkb_score_kernel(
     }
   }
   if (BLOCK_PAIR) {
-    Real dummy[4] = {0, 0, 0, 0};
-    lkb_pump<Real, GRAD, BLOCK_PAIR>(ev, q, true, none, dummy, tg);
+    Real unused[4] = {0, 0, 0, 0};  // tagged entries add their energies to their rows
+    lkb_pump<Real, GRAD, BLOCK_PAIR>(ev, q, true, none, unused, tg);
   }
   lkb_flush_counts(s, q);
 }
@@ -1109,7 +1109,7 @@ __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS)
   tg.dTdV = s.dTdV;
   tg.n = ra.n_pairs;
   const Lkb4<Real> none = {{0, 0, 0, 0}};
-  Real dummy[4] = {0, 0, 0, 0};
+  Real unused[4] = {0, 0, 0, 0};  // tagged entries add their energies to their rows
   for (;;) {
     int it = 0;
     if (lane == 0) it = atomicAdd(s.ticket, 1);
@@ -1144,11 +1144,11 @@ __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS)
       }
       const LkbSide side2 = lkb_side(k, ra.rot_bt[rot2], ra.rot_off[rot2]);
       const int nc1 = striking ? s.bt_n_conn[side1.bt] : 0, nc2 = striking ? s.bt_n_conn[side2.bt] : 0;
-      lkb_enqueue_pairs<Real, GRAD, true>(s, k, ev, q, side1, side2, intra, striking, nc1, nc2, seps, none, dummy,
+      lkb_enqueue_pairs<Real, GRAD, true>(s, k, ev, q, side1, side2, intra, striking, nc1, nc2, seps, none, unused,
                                           (int)(pair_first + j), tg);
     }
   }
   // entries carry their pair: the queues drain across items, once at the end
-  lkb_pump<Real, GRAD, true>(ev, q, true, none, dummy, tg);
+  lkb_pump<Real, GRAD, true>(ev, q, true, none, unused, tg);
   lkb_flush_counts(s, q);
 }
