@@ -10,6 +10,7 @@ lk_ball_pose_score) through the C ABI.
   their adjoint, against the reference op (tests/golden/lkball_block_pair.npz);
   float64 gradcheck of both ops;
 - plan kinds: a water plan and a score plan serve their own entry points;
+  corrupted polar / occluder and hbond tables are rejected with a status;
 - the rotamer op (waters on a rotamer set, lk_ball_rotamer_score): dispatch
   exact, energies and the gradient of a weighted sum against the reference
   fixture (tests/golden/lkball_rotamers.npz) and the oracle; gradcheck.
@@ -359,3 +360,31 @@ def test_block_pair_matches_reference_fixture(lterm, f64):
     else:
         E_close(E.detach().cpu().numpy(), g[f"{dn}_energies"])
         g_close(coords.grad.cpu().numpy(), g[f"{dn}_grad"])
+
+
+def test_bad_tables_are_rejected(lterm):
+    """Out-of-range entries in the polar / occluder lists or the hbond
+    tables stop plan creation with a status (checked before any use)."""
+    ps = synthetic_pose_stack([12, 5], [91, 92])
+    wa, sa = static_args(ps, lterm, torch.float32)
+    coords = ps.coords.flatten(0, 1).to(DEV)
+    # lk_ball_pose_score's tile_pol_occ_inds (argument 12 + 8): an index past the tile
+    bad = list(sa)
+    t = bad[20].clone()
+    nz = torch.nonzero(bad[19] > 0)[0]  # a tile with occluders
+    t[nz[0], nz[1], 0] = 40
+    bad[20] = t
+    with pytest.raises(native.NativeError) as e:
+        LKBallPlan(coords, score_static=bad)
+    assert e.value.status == 3  # index range
+    # gen_pose_waters' tile_donH_hvy_inds (argument 12 + 10): a heavy atom
+    # past the block, in a block type the poses use (water sites are resolved
+    # for the blocks present)
+    bad = list(wa)
+    t = bad[22].clone()
+    used = [int(b) for b in ps.block_type_ind.flatten() if b >= 0 and bad[19][int(b), 0] > 0]
+    t[used[0], 0, 0] = 999
+    bad[22] = t
+    with pytest.raises(native.NativeError) as e:
+        LKBallPlan(coords, water_static=bad)
+    assert e.value.status == 3
