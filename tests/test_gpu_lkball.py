@@ -388,3 +388,22 @@ def test_bad_tables_are_rejected(lterm):
     with pytest.raises(native.NativeError) as e:
         LKBallPlan(coords, water_static=bad)
     assert e.value.status == 3
+
+
+@pytest.mark.parametrize("f64", [False, True])
+def test_large_ragged_batch_matches_oracle(lterm, f64):
+    """Poses of 700, 30, 250 and 1 residues in one stack (blocks padded to
+    700 per pose)."""
+    dt = torch.float64 if f64 else torch.float32
+    ps = synthetic_pose_stack([700, 30, 250, 1], [101, 102, 103, 104], extra_chi_sd=15.0)
+    W, E, dx, nbr = gpu_run(ps, lterm, dt)
+    Wo, Eo, dxo, nbro = oracle_run(ps, lterm, f64)
+    assert numpy.array_equal(nbr.cpu().numpy(), nbro)
+    if f64:
+        W_close(W.cpu().numpy(), Wo, 1e-9)
+        E_close(E.cpu().numpy(), Eo, rtol=1e-9, atol=1e-9)
+        g_close(dx.cpu().numpy(), dxo, rtol=1e-9)
+    else:
+        W_close(W.cpu().numpy(), Wo, 1e-4)
+        E_close(E.cpu().numpy(), Eo)
+        g_close(dx.cpu().numpy(), dxo)
