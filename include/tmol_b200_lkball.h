@@ -23,6 +23,7 @@
 #include <stdint.h>
 
 #include "tmol_b200_ljlk.h"
+#include "tmol_b200_pose.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -103,6 +104,16 @@ int tmol_b200_lkball_plan_create(const tmol_b200_lkball_inputs* inputs, int real
                                  const tmol_b200_ljlk_launch* launch, void* stream,
                                  tmol_b200_lkball_plan** plan_out);
 int tmol_b200_lkball_plan_destroy(tmol_b200_lkball_plan* plan);
+
+/* The same plan built from the PoseStack's connectivity
+ * (include/tmol_b200_pose.h) instead of the dense min_bondsep /
+ * inter_block_bondsep tensors, which may then be NULL (the count-pair
+ * tables come straight from the connectivity, as for the LJ/LK and elec
+ * plans); `rotamers` selects a rotamer plan. */
+int tmol_b200_lkball_plan_create_from_connectivity(const tmol_b200_lkball_inputs* inputs,
+                                                   const tmol_b200_pose_connectivity* conn, int real_bytes,
+                                                   const tmol_b200_ljlk_launch* launch, void* stream, int rotamers,
+                                                   tmol_b200_lkball_plan** plan_out);
 
 /* gen_pose_waters forward (GeneratePoseWaters::forward,
  * gen_pose_waters.impl.hh:35-230): waters [n_atoms, 4, 3], overwritten. */

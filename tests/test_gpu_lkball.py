@@ -407,3 +407,44 @@ def test_large_ragged_batch_matches_oracle(lterm, f64):
         W_close(W.cpu().numpy(), Wo, 1e-4)
         E_close(E.cpu().numpy(), Eo)
         g_close(dx.cpu().numpy(), dxo)
+
+
+def test_plans_from_connectivity_score_like_dense_plans(lterm, ubq_pose_stack):
+    """A plan built from the PoseStack's connectivity (no min_bondsep /
+    inter_block_bondsep tensors) scores like one built from them."""
+    from tmol_b200.pose.rotamers import synthetic_rotamer_set
+    from tmol_b200.score.lkball_energy_term import rotamer_score_args
+
+    for ps in (ubq_pose_stack, synthetic_pose_stack([60, 25], [111, 112], extra_chi_sd=20.0)):
+        psd = ps.to(DEV)
+        wa, sa = static_args(ps, lterm, torch.float32)
+        coords = psd.coords.flatten(0, 1).contiguous()
+        dense = LKBallPlan(coords, water_static=wa, score_static=sa)
+        sparse_sa = [None if i in (13, 14) else a for i, a in enumerate(sa)]
+        sparse = LKBallPlan(coords, water_static=wa, score_static=sparse_sa, connectivity=psd)
+        W = dense.waters(coords)
+        assert torch.equal(torch.isnan(sparse.waters(coords)), torch.isnan(W))
+        for bp in (False, True):
+            E0, n0 = dense.forward(coords, W, block_pair=bp)
+            E1, n1 = sparse.forward(coords, W, block_pair=bp)
+            E_close(E1.cpu().numpy(), E0.cpu().numpy(), rtol=1e-6, atol=1e-6)
+            assert torch.equal(n0, n1)
+        w = torch.rand(4, ps.n_poses, device=DEV)
+        E0, g0 = dense.energy_and_gradient(coords, w)
+        E1, g1 = sparse.energy_and_gradient(coords, w)
+        g_close(g1.cpu().numpy(), g0.cpu().numpy(), rtol=1e-5)
+    # a rotamer plan
+    ps = synthetic_pose_stack([40, 20], [113, 114])
+    rs = synthetic_rotamer_set(ps, max_rots=3, mutate_fraction=0.3, seed=9)
+    wa = to_dev(water_gen_args(ps, lterm, rs), torch.float32)
+    sa = to_dev(rotamer_score_args(ps, rs, lterm, None)[:-2], torch.float32)
+    rc = rs.coords.to(DEV)
+    dense = LKBallPlan(rc, water_static=wa, score_static=sa, rotamers=True)
+    sparse = LKBallPlan(rc, water_static=wa, score_static=[None if i in (13, 14) else a for i, a in enumerate(sa)],
+                        rotamers=True, connectivity=ps.to(DEV))
+    W = dense.waters(rc)
+    i0, it0 = dense.rotamer_dispatch(rc)
+    i1, it1 = sparse.rotamer_dispatch(rc)
+    assert torch.equal(i0, i1)
+    E_close(sparse.rotamer_forward(rc, it1, i1.shape[1], W).cpu().numpy(),
+            dense.rotamer_forward(rc, it0, i0.shape[1], W).cpu().numpy(), rtol=1e-6, atol=1e-6)

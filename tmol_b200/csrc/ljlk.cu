@@ -2941,7 +2941,8 @@ tmol_b200_ljlk_inputs shared_inputs(const tmol_b200_elec_inputs* e) {
 }
 
 int create_lkball_plan(const tmol_b200_lkball_inputs* k, int real_bytes, const tmol_b200_ljlk_launch* launch,
-                       void* stream, bool rotamers, tmol_b200_ljlk_plan** plan_out) {
+                       void* stream, bool rotamers, tmol_b200_ljlk_plan** plan_out,
+                       const tmol_b200_pose_connectivity* conn = nullptr) {
   if (!k || !plan_out) return TMOL_B200_ERR_INVALID_ARGUMENT;
   tmol_b200_ljlk_inputs in = {};
   in.n_atoms = k->n_atoms;
@@ -2973,7 +2974,7 @@ int create_lkball_plan(const tmol_b200_lkball_inputs* k, int real_bytes, const t
   in.bt_path_distance = k->bt_path_distance;
   in.global_params = k->global_params;
   in.max_dis = k->max_dis;
-  return create_plan(&in, real_bytes, launch, stream, rotamers, plan_out, nullptr, nullptr, k);
+  return create_plan(&in, real_bytes, launch, stream, rotamers, plan_out, nullptr, conn, k);
 }
 
 int create_elec_plan(const tmol_b200_elec_inputs* e, int real_bytes, const tmol_b200_ljlk_launch* launch,
@@ -3350,6 +3351,14 @@ int tmol_b200_lkball_plan_create(const tmol_b200_lkball_inputs* inputs, int real
                                  const tmol_b200_ljlk_launch* launch, void* stream,
                                  tmol_b200_lkball_plan** plan_out) {
   return create_lkball_plan(inputs, real_bytes, launch, stream, false, plan_out);
+}
+
+int tmol_b200_lkball_plan_create_from_connectivity(const tmol_b200_lkball_inputs* inputs,
+                                                   const tmol_b200_pose_connectivity* conn, int real_bytes,
+                                                   const tmol_b200_ljlk_launch* launch, void* stream, int rotamers,
+                                                   tmol_b200_lkball_plan** plan_out) {
+  if (!conn) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  return create_lkball_plan(inputs, real_bytes, launch, stream, rotamers != 0, plan_out, conn);
 }
 
 int tmol_b200_lkball_rotamer_plan_create(const tmol_b200_lkball_inputs* inputs, int real_bytes,

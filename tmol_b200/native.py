@@ -246,6 +246,13 @@ SIGNATURES = {
     "tmol_b200_lkball_forward": (ctypes.c_int, [_V, _V, _V, ctypes.c_int, _V, _V, _V]),
     "tmol_b200_lkball_backward": (ctypes.c_int, [_V, _V, _V, ctypes.c_int, _V, _V, _V, _V]),
     "tmol_b200_lkball_energy_and_gradient": (ctypes.c_int, [_V, _V, _V, _V, _V, _V]),
+    "tmol_b200_lkball_plan_create_from_connectivity": (
+        ctypes.c_int,
+        [
+            ctypes.POINTER(LKBallInputs), ctypes.POINTER(PoseConnectivity), ctypes.c_int, ctypes.POINTER(Launch), _V,
+            ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+        ],
+    ),
     "tmol_b200_lkball_rotamer_plan_create": (
         ctypes.c_int,
         [ctypes.POINTER(LKBallInputs), ctypes.c_int, ctypes.POINTER(Launch), _V, ctypes.POINTER(ctypes.c_void_p)],

@@ -44,7 +44,12 @@ class LKBallPlan(LJLKPlan):
     ABI = "tmol_b200_lkball"
     NAME = "LK-ball"
 
-    def __init__(self, coords_like, water_static=None, score_static=None, launch=None, rotamers=False):
+    def __init__(self, coords_like, water_static=None, score_static=None, launch=None, rotamers=False,
+                 connectivity=None):
+        """With ``connectivity`` (a PoseStack, or the tuple (block_type_ind,
+        inter_residue_connections, bt_n_conn, bt_conn_sep)) the count-pair
+        tables come from it and the scoring arguments' min_bondsep /
+        inter_block_bondsep may be None."""
         if water_static is None and score_static is None:
             raise ValueError("an LK-ball plan needs the water-generation or the scoring arguments")
         device = self._set_device(coords_like)
@@ -101,9 +106,13 @@ class LKBallPlan(LJLKPlan):
                             ("inter_block_bondsep", ibb), ("bt_tile_n_polar_atoms", t_npol),
                             ("bt_tile_n_occluder_atoms", t_nocc), ("bt_tile_pol_occ_inds", t_polocc),
                             ("bt_path_distance", path_distance)):
+                if t is None and connectivity is not None and name in ("min_bondsep", "inter_block_bondsep"):
+                    continue
                 put(name, t)
             C = bt_conn_atom.shape[1]
-            if tuple(ibb.shape) != (P, B, B, C, C) or tuple(min_bondsep.shape) != (P, B, B):
+            if (ibb is not None and tuple(ibb.shape) != (P, B, B, C, C)) or (
+                min_bondsep is not None and tuple(min_bondsep.shape) != (P, B, B)
+            ):
                 raise ValueError("bond separation tensors do not match the PoseStack's shape")
             if t_params.shape[-1] != 9:
                 raise ValueError("LK-ball atom parameters must be [n_block_types, n_tiles, 32, 9]")
@@ -131,10 +140,22 @@ class LKBallPlan(LJLKPlan):
         ptr = ctypes.c_void_p()
         real_bytes = 4 if self.dtype == torch.float32 else 8
         with torch.cuda.device(self.device):
-            native.call(
-                "tmol_b200_lkball_rotamer_plan_create" if rotamers else "tmol_b200_lkball_plan_create",
-                ctypes.byref(s), real_bytes, ctypes.byref(self.launch), self._stream(), ctypes.byref(ptr),
-            )
+            if connectivity is None:
+                native.call(
+                    "tmol_b200_lkball_rotamer_plan_create" if rotamers else "tmol_b200_lkball_plan_create",
+                    ctypes.byref(s), real_bytes, ctypes.byref(self.launch), self._stream(), ctypes.byref(ptr),
+                )
+            else:
+                from ..pose.bondsep import connectivity as conn_struct, pose_connectivity
+
+                cs, conn_keep = (
+                    conn_struct(*connectivity) if isinstance(connectivity, tuple) else pose_connectivity(connectivity)
+                )
+                native.call(
+                    "tmol_b200_lkball_plan_create_from_connectivity", ctypes.byref(s), ctypes.byref(cs), real_bytes,
+                    ctypes.byref(self.launch), self._stream(), int(bool(rotamers)), ctypes.byref(ptr),
+                )
+                del conn_keep
         self.ptr = ptr
         del keep
 
