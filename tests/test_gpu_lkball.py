@@ -5,7 +5,9 @@ lk_ball_pose_score) through the C ABI.
   (1ubq and a synthetic pose, float32 and float64): waters, the four
   energies (1e-5 relative / 1e-3 kcal/mol in float32) and the gradient
   through the waters (1e-4 of its largest component);
-- against the C oracle on seeded multi-pose batches, float64 to 1e-9;
+- against the C oracle on seeded multi-pose batches, float64 to 1e-9, and
+  on the bench's full 64 x 150 batch with size-independent properties
+  (block-pair sums, translation invariance, linearity in the weights);
 - block-pair energies (upper triangle, summing to the whole-pose ones) and
   their adjoint, against the reference op (tests/golden/lkball_block_pair.npz);
   float64 gradcheck of both ops;
@@ -448,3 +450,33 @@ def test_plans_from_connectivity_score_like_dense_plans(lterm, ubq_pose_stack):
     assert torch.equal(i0, i1)
     E_close(sparse.rotamer_forward(rc, it1, i1.shape[1], W).cpu().numpy(),
             dense.rotamer_forward(rc, it0, i0.shape[1], W).cpu().numpy(), rtol=1e-6, atol=1e-6)
+
+
+def test_full_size_batch_properties(lterm):
+    """The bench's batch (64 poses x 150 residues): energies and gradient
+    against the oracle, the forward against the one-call energies,
+    block-pair energies summing to the whole-pose ones, translation
+    invariance, and linearity of the gradient in the weights."""
+    ps = synthetic_pose_stack([150] * 64, list(range(64)))
+    wa, sa = static_args(ps, lterm, torch.float32)
+    coords = ps.coords.flatten(0, 1).to(DEV).contiguous()
+    plan = LKBallPlan(coords, water_static=wa, score_static=sa)
+    W = plan.waters(coords)
+    E, _ = plan.forward(coords, W)
+    ones = torch.ones(4, 64, device=DEV)
+    E1, g1 = plan.energy_and_gradient(coords, ones)
+    E_close(E1.cpu().numpy(), E.cpu().numpy(), rtol=1e-5, atol=1e-4)
+    _, Eo, dxo, _ = oracle_run(ps, lterm, False)
+    E_close(E.cpu().numpy(), Eo)
+    g_close(g1.cpu().numpy(), dxo)
+    Ebp, _ = plan.forward(coords, W, block_pair=True)
+    E_close(Ebp.sum(dim=(2, 3)).cpu().numpy(), E.cpu().numpy(), rtol=1e-5, atol=1e-3)
+    shift = torch.tensor([3.1, -2.2, 5.7], device=DEV)
+    Es, _ = plan.energy_and_gradient(coords + shift, ones)
+    E_close(Es.cpu().numpy(), E1.cpu().numpy(), rtol=1e-4, atol=1e-3)
+    w1 = torch.rand(4, 64, device=DEV, generator=torch.Generator(device=DEV).manual_seed(1))
+    w2 = torch.rand(4, 64, device=DEV, generator=torch.Generator(device=DEV).manual_seed(2))
+    _, ga = plan.energy_and_gradient(coords, w1)
+    _, gb = plan.energy_and_gradient(coords, w2)
+    _, gab = plan.energy_and_gradient(coords, w1 + w2)
+    g_close(gab.cpu().numpy(), (ga + gb).cpu().numpy())
