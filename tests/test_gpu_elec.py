@@ -234,3 +234,28 @@ def test_rendered_modules_and_plan_kinds(ubq_pose_stack, eterm):
         native.call("tmol_b200_elec_forward", lplan.ptr, flat.data_ptr(), 0, E.data_ptr(), None, None)
     with pytest.raises(native.NativeError):
         native.call("tmol_b200_elec_plan_destroy", lplan.ptr)
+
+
+def test_full_size_batch_properties(eterm):
+    """The bench's batch (64 poses x 150 residues): energies and gradient
+    against the oracle, block-pair energies summing to the whole-pose ones,
+    translation invariance, and linearity of the gradient in the weights."""
+    ps = synthetic_pose_stack([150] * 64, list(range(64)))
+    args = elec_pose_score_args(ps, eterm)
+    coords = ps.coords.flatten(0, 1).to(DEV).contiguous()
+    plan = ElecPlan(coords, to_dev(args[:-1]))
+    ones = torch.ones(1, 64, device=DEV)
+    E, g = plan.energy_and_gradient(coords, ones)
+    Eo, dVo, _ = O.OracleCall(ps.coords.flatten(0, 1), args, term="elec").pose_scores(require_gradient=True)
+    E_close(E.cpu().numpy(), Eo[:1])
+    g_close(g.cpu().numpy(), dVo[0])
+    Ebp, _ = plan.forward(coords, block_pair=True)
+    E_close(Ebp.sum(dim=(2, 3)).cpu().numpy(), E.cpu().numpy(), rtol=1e-5, atol=1e-3)
+    Es, _ = plan.energy_and_gradient(coords + torch.tensor([3.1, -2.2, 5.7], device=DEV), ones)
+    E_close(Es.cpu().numpy(), E.cpu().numpy(), rtol=1e-4, atol=1e-3)
+    w1 = torch.rand(1, 64, device=DEV, generator=torch.Generator(device=DEV).manual_seed(1))
+    w2 = torch.rand(1, 64, device=DEV, generator=torch.Generator(device=DEV).manual_seed(2))
+    _, ga = plan.energy_and_gradient(coords, w1)
+    _, gb = plan.energy_and_gradient(coords, w2)
+    _, gab = plan.energy_and_gradient(coords, w1 + w2)
+    g_close(gab.cpu().numpy(), (ga + gb).cpu().numpy())
