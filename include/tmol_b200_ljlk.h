@@ -191,8 +191,15 @@ int64_t tmol_b200_ljlk_plan_device_bytes(const tmol_b200_ljlk_plan* plan);
  * memory: at most 262,144 blocks (n_poses * max_n_blocks), 4 MiB, kept by
  * every GPU that loads the library until the process exits; larger inputs
  * return TMOL_B200_ERR_CAPACITY before any GPU work.  The first call on a
- * device looks up that array's device address (cudaGetSymbolAddress); make
- * the first call on each device before any stream capture.  Every call
+ * device looks up that array's device address (cudaGetSymbolAddress).  With
+ * CUDA's default lazy module loading that lookup is also what loads this
+ * library's device code onto the device, and the load itself takes device
+ * memory: the 4 MiB array plus the kernels' code.  So make the first call on
+ * each device at start-up, before the host's own pool reserves the free
+ * memory and before any stream capture; later calls allocate nothing.  The
+ * looked-up address is kept for the life of the process: do not use this
+ * entry point across a cudaDeviceReset (or any teardown of the device's
+ * primary context), after which that address is no longer valid.  Every call
  * shares the one array and overwrites it, so calls that overlap on the GPU
  * (different streams, or different host threads on one device) race; order
  * them on one stream.  Calls no cudaMalloc, cudaFree or allocating routine. */

@@ -22,20 +22,30 @@ vendored Eigen / moderngpu headers in ``tmol/extern``.  They are compiled in
 place with g++ -O3 through torch's extension builder (no reference build
 system is run); the shared library lands in ``oracle/_ref/``.
 
-Usage: ``python oracle/build_ref.py [/path/to/tmol/checkout]``
+Usage: ``python oracle/build_ref.py [/path/to/tmol/checkout]``.  Without an
+argument the checkout is taken from the ``TMOL_REFERENCE`` environment
+variable, else from a ``reference`` directory beside this repository.
 """
 
 import os
 import sys
 import time
 
-REF_DEFAULT = "/root/reference"
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 LIB_NAME = "tmol_ljlk_ref"
 ELEC_LIB_NAME = "tmol_elec_ref"
 APSP_LIB_NAME = "tmol_apsp_ref"
 LKBALL_LIB_NAME = "tmol_lk_ball_ref"
+
+
+def reference_root():
+    """The tmol checkout the reference ops are compiled from: ``$TMOL_REFERENCE``,
+    else ``reference/`` beside this repository's directory."""
+    env = os.environ.get("TMOL_REFERENCE")
+    if env:
+        return env
+    return os.path.normpath(os.path.join(HERE, "..", "..", "reference"))
 
 
 def lib_path():
@@ -54,9 +64,10 @@ def lk_ball_lib_path():
     return os.path.join(OUT, "lk_ball", LKBALL_LIB_NAME + ".so")
 
 
-def build(ref=REF_DEFAULT, verbose=False):
+def build(ref=None, verbose=False):
     from torch.utils.cpp_extension import load
 
+    ref = ref or reference_root()
     t0 = time.time()
     # each op in its own build directory: both have a compiled.ops.cpp
     for name, sub, srcs, out in (
@@ -92,6 +103,6 @@ def build(ref=REF_DEFAULT, verbose=False):
 
 
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else REF_DEFAULT
+    ref = sys.argv[1] if len(sys.argv) > 1 else reference_root()
     t = build(ref, verbose=True)
     print(f"built {lib_path()}, {elec_lib_path()}, {apsp_lib_path()} and {lk_ball_lib_path()} in {t:.1f}s")

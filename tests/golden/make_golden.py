@@ -259,7 +259,9 @@ def lkball_block_pair():
 
 
 if __name__ == "__main__":
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    from oracle.build_ref import reference_root
+
+    root = sys.argv[1] if len(sys.argv) > 1 else reference_root()
     only = sys.argv[2] if len(sys.argv) > 2 else None
     if only == "lkball_rotamers":
         lkball_rotamers()

@@ -75,3 +75,18 @@ def test_noalloc_neighbors_match_the_scoring_path(term):
         assert rc == 0, native.load().tmol_b200_status_string(rc)
         torch.cuda.synchronize()
         assert numpy.array_equal(out.cpu().numpy(), nbr_ref.cpu().numpy())
+
+        # the promise itself: once the first call has loaded the module, a
+        # call leaves the device's free memory and torch's allocations as
+        # they were (everything it touches is allocated above)
+        free0, _ = torch.cuda.mem_get_info(dev)
+        torch_bytes0 = torch.cuda.memory_allocated(dev)
+        rc = _noalloc(
+            coords, args[3].contiguous(), args[0].contiguous(), args[14].contiguous(),
+            P, B, float(args[24]), out, stream,
+        )
+        torch.cuda.synchronize()
+        assert rc == 0
+        assert torch.cuda.mem_get_info(dev)[0] == free0
+        assert torch.cuda.memory_allocated(dev) == torch_bytes0
+        assert numpy.array_equal(out.cpu().numpy(), nbr_ref.cpu().numpy())

@@ -2596,8 +2596,13 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
   if (P < 0 || B < 0 || nbt < 0 || A < 0 || C < 0 || T < 0 || in->n_atoms < 0)
     return TMOL_B200_ERR_SHAPE;
   if (C > MAX_CONN || B >= 65536) return TMOL_B200_ERR_SHAPE;
-  if (rotamers ? in->n_rots < 0 : in->n_rots != P * B) return TMOL_B200_ERR_SHAPE;
-  if (rotamers && P * B > 0 && !in->n_rots_for_block) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  // block slots, formed in 64 bits; the kernels index blocks (and their
+  // count-pair rows, 16 entries each) in 32-bit ints, so the product is
+  // capped far below where those indices could wrap
+  const int64_t n_slots = (int64_t)P * B;
+  if (n_slots > ((int64_t)1 << 26)) return TMOL_B200_ERR_SHAPE;
+  if (rotamers ? in->n_rots < 0 : (int64_t)in->n_rots != n_slots) return TMOL_B200_ERR_SHAPE;
+  if (rotamers && n_slots > 0 && !in->n_rots_for_block) return TMOL_B200_ERR_INVALID_ARGUMENT;
   if (nt * TILE < A) return TMOL_B200_ERR_SHAPE;
   if (in->n_atoms >= ((int64_t)1 << 31)) return TMOL_B200_ERR_SHAPE;
   // with the pose's connectivity, the dense bond-separation tensors are not
@@ -2608,7 +2613,7 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
   if (conn && (conn->n_poses != P || conn->max_n_blocks != B || conn->n_block_types != nbt ||
                conn->max_n_conn != C))
     return TMOL_B200_ERR_SHAPE;
-  if (P * B > 0 && scoring) {
+  if (n_slots > 0 && scoring) {
     if (conn) {
       for (const void* r : conn_req)
         if (!r) return TMOL_B200_ERR_INVALID_ARGUMENT;
@@ -2624,7 +2629,7 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
                        lkb ? in->bt_n_atoms : in->bt_is_ligand_fragment,
                        scoring ? in->global_params : in->bt_n_atoms};
   if (lkb && lkb->max_n_tiles * TILE < A) return TMOL_B200_ERR_SHAPE;
-  if (lkb_waters && P * B > 0 && nbt > 0) {
+  if (lkb_waters && n_slots > 0 && nbt > 0) {
     const void* lreq[] = {lkb->inter_residue_connections, lkb->first_rot_for_block, lkb->bt_atom_all_bond_ranges,
                           lkb->bt_tile_n_donH,
                           lkb->bt_tile_n_acc, lkb->bt_tile_donH_inds, lkb->bt_tile_donH_hvy_inds,
@@ -2646,7 +2651,7 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
   const void* req_ljlk[] = {in->bt_n_heavy_atoms_in_tile, in->bt_heavy_atoms_in_tile, in->bt_atom_types,
                             in->type_params};
   const void* req_elec[] = {elec ? elec->partial_charge : nullptr, elec ? elec->inter_repr_pd : nullptr};
-  if (P * B > 0 && nbt > 0) {
+  if (n_slots > 0 && nbt > 0) {
     for (const void* r : req)
       if (!r) return TMOL_B200_ERR_INVALID_ARGUMENT;
     if (term == kTermLJLK) {

@@ -33,6 +33,10 @@ static __device__ __align__(256) float g_noalloc_spheres[kMaxBlocks * 4];
 
 // Device address of g_noalloc_spheres, looked up once per device: in host
 // code the array's name is a host-side stand-in, not a device address.
+// Under CUDA's lazy module loading, the first lookup on a device also loads
+// this module there, which takes device memory (the array and the code):
+// callers make their first call at start-up.  The cached address is only
+// valid while the device's primary context lives (no cudaDeviceReset).
 float* g_scratch_addr[kMaxDevices] = {};
 std::mutex g_scratch_mutex;
 
