@@ -74,3 +74,36 @@ def exotic_pose_stack(seed=0):
         xyz = 0.6 * xyz + rng.normal(scale=0.3, size=xyz.shape)
         coords.append(xyz)
     return build_pose_stack(topos, coords, pbt=pbt)
+
+
+def degenerate_pose_stack(seed=3):
+    """Three poses with the degenerate cases the scoring path must define:
+    a block type with no atoms (its sphere's centroid is 0/0 = NaN, so it
+    is nobody's neighbour, not even its own) inside pose 0, a pose of a
+    single block (pose 1), and an ordinary pose (pose 2)."""
+    from tmol_b200.chem.restypes import ResidueType
+    from tmol_b200.pose.synthetic import synthetic_topologies_and_coords
+
+    rts = ResidueTypeSet.get_default()
+    db = ChemicalDatabase.get_default()
+    empty = ResidueType(
+        name="EMPTY", base_name="EMPTY", atoms=[], bonds=[], connections=[], icoors=[], chis=[], aliases=[],
+        is_polymer=False, is_ligand_fragment=True,
+    )
+    pbt = PackedBlockTypes(db, list(rts.types.values()) + [empty])
+    topos, coords = synthetic_topologies_and_coords([20, 1, 8], [seed, seed + 1, seed + 2], pbt=pbt)
+    names = list(topos[0].block_type_names)
+    shift = lambda b: b if b < 6 else b + 1  # noqa: E731
+    topos[0] = PoseTopology(
+        names[:6] + ["EMPTY"] + names[6:], [(shift(a), ca, shift(b), cb) for a, ca, b, cb in topos[0].bonds]
+    )
+    return build_pose_stack(topos, coords, pbt=pbt)
+
+
+def with_nan_atom(ps, pose=2, block=3, atom=1, dim=1):
+    """The stack's coordinates with one atom coordinate set to NaN: its
+    block's sphere is NaN, so the block drops out of neighbour detection and
+    scores nothing, while the rest of the pose scores as before."""
+    c = ps.coords.clone()
+    c[pose, int(ps.block_coord_offset[pose, block]) + atom, dim] = float("nan")
+    return c

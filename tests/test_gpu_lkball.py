@@ -4,10 +4,14 @@ lk_ball_pose_score) through the C ABI.
 - against the reference ops' outputs committed in tests/golden/lkball.npz
   (1ubq and a synthetic pose, float32 and float64): waters, the four
   energies (1e-5 relative / 1e-3 kcal/mol in float32) and the gradient
-  through the waters (1e-4 of its largest component);
-- against the C oracle on seeded multi-pose batches, float64 to 1e-9, and
-  on the bench's full 64 x 150 batch with size-independent properties
-  (block-pair sums, translation invariance, linearity in the weights);
+  through the waters per component (tests/tolerances.py; float32 against
+  the stored float32 output: the doubled band);
+- against the C oracle on seeded multi-pose batches: float32 runs against
+  the oracle in float64 (per component, 1e-4 relative + 1e-3 kcal/mol/A;
+  the neighbour matrix against the float32 oracle, bit-exact), float64 to
+  1e-9; and on the bench's full 64 x 150 batch with size-independent
+  properties (block-pair sums, translation invariance, linearity in the
+  weights);
 - block-pair energies (upper triangle, summing to the whole-pose ones) and
   their adjoint, against the reference op (tests/golden/lkball_block_pair.npz);
   float64 gradcheck of both ops;
@@ -28,6 +32,7 @@ from tmol_b200 import native
 from tmol_b200.pose.synthetic import synthetic_pose_stack
 from tmol_b200.score.lkball_energy_term import LKBallEnergyTerm, score_args, water_gen_args
 from tmol_b200.score.lkball_op import LKBallPlan, gen_pose_waters, lk_ball_pose_score
+from tolerances import E_close, g_close, g_close_f32
 
 pytestmark = pytest.mark.gpu
 DEV = torch.device("cuda:0")
@@ -65,7 +70,7 @@ def gpu_run(ps, lterm, dtype, block_pair=False):
     return W.detach(), E.detach(), coords.grad, nbr
 
 
-def oracle_run(ps, lterm, f64, weights=None):
+def _oracle(ps, lterm, f64, weights=None):
     dt = torch.float64 if f64 else torch.float32
     oc = O.OracleCall(ps.coords.flatten(0, 1).to(dt), score_args(ps, lterm, None), f64=f64, term="lkball",
                       lkb_water_args=water_gen_args(ps, lterm))
@@ -74,12 +79,15 @@ def oracle_run(ps, lterm, f64, weights=None):
     return W, E, dx, nbr
 
 
-def E_close(E, ref, rtol=1e-5, atol=1e-3):
-    numpy.testing.assert_allclose(E, ref, rtol=rtol, atol=atol)
-
-
-def g_close(g, ref, rtol=1e-4):
-    numpy.testing.assert_allclose(g, ref, rtol=rtol, atol=rtol * numpy.abs(ref).max())
+def oracle_run(ps, lterm, f64, weights=None):
+    """The oracle's (waters, energies, gradient, neighbours), the values from
+    the oracle in float64.  For a float32 GPU run (f64 False) the neighbour
+    matrix comes from the float32 oracle: the rule's float32 rounding
+    decides borderline block pairs."""
+    W, E, dx, nbr = _oracle(ps, lterm, True, weights)
+    if not f64:
+        nbr = _oracle(ps, lterm, False, weights)[3]
+    return W, E, dx, nbr
 
 
 def W_close(W, ref, atol):
@@ -105,7 +113,7 @@ def test_matches_reference_fixture(ubq_pose_stack, lterm, f64):
             g_close(dx.cpu().numpy(), g[f"{tag}_{dn}_grad"], rtol=1e-9)
         else:
             E_close(E.cpu().numpy(), g[f"{tag}_{dn}_energies"])
-            g_close(dx.cpu().numpy(), g[f"{tag}_{dn}_grad"])
+            g_close_f32(dx.cpu().numpy(), g[f"{tag}_{dn}_grad"])
 
 
 def test_ubq_reproduces_stored_energies(ubq_pose_stack, lterm):
@@ -254,7 +262,7 @@ def test_rotamers_match_reference_fixture(lterm, f64):
         g_close(dx.cpu().numpy(), g[f"{dn}_grad"], rtol=1e-9)
     else:
         E_close(E.cpu().numpy(), g[f"{dn}_energies"])
-        g_close(dx.cpu().numpy(), g[f"{dn}_grad"])
+        g_close_f32(dx.cpu().numpy(), g[f"{dn}_grad"])
 
 
 def test_rotamers_match_oracle(lterm):
@@ -330,7 +338,7 @@ def test_rendered_scoring_modules(lterm):
     Em = whole(coords)
     E_close(Em.detach().cpu().numpy(), E.cpu().numpy(), rtol=1e-6, atol=1e-6)
     Em.sum().backward()
-    g_close(coords.grad.flatten(0, 1).cpu().numpy(), dx.cpu().numpy(), rtol=1e-5)
+    g_close_f32(coords.grad.flatten(0, 1).cpu().numpy(), dx.cpu().numpy())
     pairs = lterm.render_block_pair_scoring_module(psd)
     Eb = pairs(psd.coords)
     E_close(Eb.sum(dim=(2, 3)).cpu().numpy(), E.cpu().numpy(), rtol=1e-5, atol=1e-5)
@@ -361,7 +369,7 @@ def test_block_pair_matches_reference_fixture(lterm, f64):
         g_close(coords.grad.cpu().numpy(), g[f"{dn}_grad"], rtol=1e-9)
     else:
         E_close(E.detach().cpu().numpy(), g[f"{dn}_energies"])
-        g_close(coords.grad.cpu().numpy(), g[f"{dn}_grad"])
+        g_close_f32(coords.grad.cpu().numpy(), g[f"{dn}_grad"])
 
 
 def test_bad_tables_are_rejected(lterm):
@@ -434,7 +442,7 @@ def test_plans_from_connectivity_score_like_dense_plans(lterm, ubq_pose_stack):
         w = torch.rand(4, ps.n_poses, device=DEV)
         E0, g0 = dense.energy_and_gradient(coords, w)
         E1, g1 = sparse.energy_and_gradient(coords, w)
-        g_close(g1.cpu().numpy(), g0.cpu().numpy(), rtol=1e-5)
+        g_close_f32(g1.cpu().numpy(), g0.cpu().numpy())
     # a rotamer plan
     ps = synthetic_pose_stack([40, 20], [113, 114])
     rs = synthetic_rotamer_set(ps, max_rots=3, mutate_fraction=0.3, seed=9)
@@ -479,4 +487,4 @@ def test_full_size_batch_properties(lterm):
     _, ga = plan.energy_and_gradient(coords, w1)
     _, gb = plan.energy_and_gradient(coords, w2)
     _, gab = plan.energy_and_gradient(coords, w1 + w2)
-    g_close(gab.cpu().numpy(), (ga + gb).cpu().numpy())
+    g_close_f32(gab.cpu().numpy(), (ga + gb).cpu().numpy())

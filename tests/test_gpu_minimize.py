@@ -25,16 +25,31 @@ def test_lbfgs_lowers_every_pose_energy():
 
 
 def test_adjoint_against_finite_differences_float64():
+    """Every one of 1000 random atoms x 3 components, none exempt:
+    |g - fd| <= 1e-4 |g| + 1e-6 + |fd(h) - fd(h/2)|.  The last term is the
+    difference quotient's own error, measured per component: on a smooth
+    stretch central differences err by O(h^2) and the two quotients agree
+    to ~1e-7; within h of a region boundary of the potentials (the LJ
+    linear extension, the spline knots, where the second derivative jumps)
+    the quotient errs by O(h) and the two quotients differ by as much."""
     ps = synthetic_pose_stack([300] * 32, list(range(32)), device=DEV, extra_chi_sd=30.0)
     term = LJLKEnergyTerm(device=DEV)
     static = [a.double() if isinstance(a, torch.Tensor) and a.is_floating_point() else a
               for a in pose_score_args(ps, term)[:-1]]
     coords = ps.coords.flatten(0, 1).double().contiguous()
     plan = LJLKPlan(coords, static)
-    fd, g = finite_difference_check(plan, coords, ps.pose_ind_for_atom, BETA2016_WEIGHTS, n_atoms=1000, h=1e-3)
+    h = 1e-3
+    fd, g = finite_difference_check(plan, coords, ps.pose_ind_for_atom, BETA2016_WEIGHTS, n_atoms=1000, h=h)
+    fd2, g2 = finite_difference_check(plan, coords, ps.pose_ind_for_atom, BETA2016_WEIGHTS, n_atoms=1000, h=h / 2)
+    assert numpy.array_equal(g, g2)  # the same atoms
+    fd_err = numpy.abs(fd - fd2)
     err = numpy.abs(fd - g)
-    # central differences are exact to O(h^2 f''') on smooth regions; a kink
-    # of the second derivative at a region boundary costs O(h)
-    tol = 1e-3 * numpy.maximum(numpy.abs(g), 1.0)
-    assert (err <= tol).mean() > 0.995, (err.max(), numpy.sort(err.ravel())[-5:])
+    tol = 1e-4 * numpy.abs(g) + 1e-6 + fd_err
+    smooth = fd_err < 1e-5
+    print(
+        f"[fd] {err.size} components: max |fd - g| {err.max():.3e}; on the {int(smooth.sum())} smooth ones "
+        f"max rel {(err[smooth] / numpy.maximum(numpy.abs(g[smooth]), 1e-12)).max():.3e}; "
+        f"{int((~smooth).sum())} within h of a region boundary"
+    )
+    assert (err <= tol).all(), (err[err > tol], g[err > tol], fd_err[err > tol])
     assert numpy.median(err) < 1e-5

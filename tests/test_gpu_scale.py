@@ -1,19 +1,23 @@
-"""Full-size checks on the GPU.  At these sizes the oracle scores a sample
-of poses (poses never interact, so each pose's energy is a property of that
-pose alone); the rest are size-independent properties of the path:
+"""Size-independent properties of the path on the uneven 256-pose batch
+(every pose of it is checked against the oracle in test_gpu_fullsize.py):
 linearity of the gradient in the term weights, block-pair energies summing
 to whole-pose energies, energy-only forward agreeing with the fused
-energy + gradient pass, and translation invariance.  Tolerances as in
-test_gpu_parity.py."""
+energy + gradient pass, the autograd adjoint agreeing with the fused pass,
+and translation invariance.  GPU results compared with each other use the
+float32-vs-float32 band of tests/tolerances.py, per component.  Translation
+is the exception: poses sit up to 6000 A from the origin, where a float32
+coordinate is only good to 2.4e-4 A, so moving a pose changes its pair
+distances by that much and steep clash gradients by ~1e-4 relative; that
+test bounds the change by 1e-4 of the largest component."""
 
 import numpy
 import pytest
 import torch
 
-from oracle import oracle as O
 from tmol_b200.pose.synthetic import log_uniform_sizes, synthetic_pose_stack
 from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm, pose_score_args
 from tmol_b200.score.ljlk_op import LJLKPlan
+from tolerances import E_close, g_close_f32
 
 pytestmark = pytest.mark.gpu
 DEV = torch.device("cuda:0")
@@ -37,18 +41,6 @@ def uneven_plan():
     return plan, coords, sizes, seeds, ps.pose_ind_for_atom
 
 
-def test_uneven_batch_against_oracle_on_sampled_poses(uneven_plan):
-    plan, coords, sizes, seeds, _ = uneven_plan
-    E, nbr = plan.forward(coords, want_neighbors=False)
-    E = E.cpu().numpy()
-    term = LJLKEnergyTerm()
-    pick = [int(k) for k in numpy.random.default_rng(11).choice(len(sizes), 8, replace=False)]
-    pick.append(int(numpy.argmax(sizes)))
-    sub = synthetic_pose_stack([sizes[k] for k in pick], [seeds[k] for k in pick])
-    Eo, _, _ = O.OracleCall(sub.coords.flatten(0, 1), pose_score_args(sub, term)).pose_scores()
-    numpy.testing.assert_allclose(E[:, pick], Eo, rtol=1e-5, atol=1e-3)
-
-
 def test_gradient_is_linear_in_the_weights(uneven_plan):
     plan, coords, sizes, _, _ = uneven_plan
     P = len(sizes)
@@ -58,9 +50,8 @@ def test_gradient_is_linear_in_the_weights(uneven_plan):
     E1, g1 = plan.energy_and_gradient(coords, w1)
     E2, g2 = plan.energy_and_gradient(coords, w2)
     E3, g3 = plan.energy_and_gradient(coords, w1 + w2)
-    torch.testing.assert_close(E1, E2, rtol=1e-5, atol=1e-3)
-    scale = g3.abs().max().item()
-    torch.testing.assert_close(g3, g1 + g2, rtol=1e-4, atol=1e-4 * scale)
+    E_close(E1.cpu().numpy(), E2.cpu().numpy())
+    g_close_f32(g3.cpu().numpy(), (g1 + g2).cpu().numpy(), what="gradient linearity in the weights")
 
 
 def test_energy_only_forward_matches_fused_pass(uneven_plan):
@@ -80,8 +71,7 @@ def test_autograd_backward_matches_fused_gradient(uneven_plan):
     E, _ = pose_scores_with_plan(c, plan)
     (w * E).sum().backward()
     _, g = plan.energy_and_gradient(coords, w)
-    scale = g.abs().max().item()
-    torch.testing.assert_close(c.grad, g, rtol=1e-4, atol=1e-4 * scale)
+    g_close_f32(c.grad.cpu().numpy(), g.cpu().numpy(), what="autograd adjoint vs fused pass")
 
 
 def test_translation_invariance(uneven_plan):

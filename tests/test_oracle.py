@@ -174,3 +174,54 @@ def test_exotic_blocks_oracle_matches_reference(term):
     assert numpy.array_equal(E.detach().numpy(), Eo)
     assert numpy.array_equal(dVo.sum(0), c.grad.numpy())
     assert numpy.array_equal(nbr.numpy(), nbro)
+
+
+def _degenerate_cases():
+    from exotic_blocks import degenerate_pose_stack, with_nan_atom
+
+    ps = degenerate_pose_stack()
+    return ps, [("zero-atom block, one-block pose", ps.coords), ("NaN coordinate", with_nan_atom(ps))]
+
+
+@pytest.mark.skipif(not O.reference_available(), reason="reference op not built")
+def test_degenerate_inputs_bit_exact_with_reference(term):
+    """A block type without atoms, a one-block pose and a NaN coordinate:
+    the oracle defines what the GPU must return, and it is the reference's
+    result bit for bit (the NaN block and the empty block are no block's
+    neighbours; every energy and gradient stays finite)."""
+    ps, cases = _degenerate_cases()
+    args = pose_score_args(ps, term)
+    for what, coords in cases:
+        flat = coords.flatten(0, 1)
+        E, dV, nbr = O.OracleCall(flat, args).pose_scores(require_gradient=True)
+        Er, c, nbrr = O.reference_pose_scores(flat, args)
+        Er.sum().backward()
+        assert numpy.array_equal(E, Er.detach().numpy()), what
+        assert numpy.array_equal(nbr, nbrr.numpy()), what
+        assert numpy.array_equal(dV.sum(0), c.grad.numpy()), what
+        assert numpy.isfinite(E).all() and numpy.isfinite(dV).all(), what
+    # the NaN block has no neighbours and its atoms no gradient
+    E, dV, nbr = O.OracleCall(cases[1][1].flatten(0, 1), args).pose_scores(require_gradient=True)
+    assert nbr[2, 3].sum() == 0 and nbr[2, :, 3].sum() == 0
+    assert nbr[0, 6].sum() == 0 and nbr[0, :, 6].sum() == 0  # the empty block
+
+
+@pytest.mark.skipif(not O.reference_available(), reason="reference op not built")
+def test_soft_repulsion_bit_exact_with_reference(synthetic_pose_stack_golden):
+    """tmol's soft_rep option (lj_dlin_sigma_factor 0.91 instead of 0.6,
+    tmol/score/ljlk/ljlk_energy_term.py:44-46,150-156)."""
+    from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm
+
+    ps = synthetic_pose_stack_golden
+    soft, hard = LJLKEnergyTerm(), LJLKEnergyTerm()
+    soft.set_options({"soft_rep": True})
+    assert float(soft.global_params[0, 1]) == pytest.approx(0.91)
+    flat = ps.coords.flatten(0, 1)
+    args = pose_score_args(ps, soft)
+    E, dV, nbr = O.OracleCall(flat, args).pose_scores(require_gradient=True)
+    Er, c, nbrr = O.reference_pose_scores(flat, args)
+    Er.sum().backward()
+    assert numpy.array_equal(E, Er.detach().numpy())
+    assert numpy.array_equal(dV.sum(0), c.grad.numpy())
+    Eh, _, _ = O.OracleCall(flat, pose_score_args(ps, hard)).pose_scores()
+    assert (E[1] < Eh[1]).any()  # a softer wall
