@@ -49,6 +49,7 @@ METRIC = "LJ+LK energy+grad poses/s (64x150-residue batch, 1 B200)"
 UNEVEN_POSES = 256
 UNEVEN_SEED = 2
 PERTURB_SD = 0.05
+UNEVEN_REPLAYS = 100  # graph replays of the uneven batch's sub-record
 L2_FLUSH_BYTES = 256 << 20
 # the rotamer workload: 16 poses x 150 residues, every block with 1..31
 # rotamers (the native one first; chis resampled, a quarter mutated)
@@ -2171,23 +2172,29 @@ def run_reference_bondsep(args):
     return 0
 
 
-def run_b200(args, world, rank, local):
+def measure_pose_batch(args, workload_name, world, rank, local, steps, extras=True):
+    """One LJ/LK pose workload on this rank's GPU: the timed graph replays,
+    the scoring kernel's own time and roofline, the end-to-end figures and
+    (rank 0) the CPU baseline.  Returns the JSON line's dict on rank 0."""
     import torch
 
     from tmol_b200 import native
     from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm, pose_score_args
-    from tmol_b200.score.ljlk_op import LJLKPlan
+    from tmol_b200.score.ljlk_op import LJLKPlan, clear_plan_cache, ljlk_pose_scores
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     term = LJLKEnergyTerm()
-    sizes_seeds = workload_sizes(args.workload, rank)
-    ps = workload(rank, args.workload, device=dev)
-    static = [a.to(dev) if isinstance(a, torch.Tensor) else a for a in pose_score_args(ps, term)[:-1]]
+    sizes_seeds = workload_sizes(workload_name, rank)
+    ps = workload(rank, workload_name, device=dev)
+    full_args = [a.to(dev) if isinstance(a, torch.Tensor) else a for a in pose_score_args(ps, term)]
+    static = full_args[:-1]
     coords = ps.coords.flatten(0, 1).to(dev).contiguous()
     plan = LJLKPlan(coords, static)
-    plan64 = None if args.no_screen else LJLKPlan(coords.double(), static)
-    eplan = None if args.no_elec else elec_plan_for(ps, coords)
+    with_screen = extras and not args.no_screen
+    with_elec = extras and not args.no_elec
+    plan64 = LJLKPlan(coords.double(), static) if with_screen else None
+    eplan = elec_plan_for(ps, coords) if with_elec else None
     bt_names = [bt.name for bt in ps.packed_block_types.active_block_types]
     del static
     P = ps.n_poses
@@ -2198,7 +2205,7 @@ def run_b200(args, world, rank, local):
     energies = torch.empty((3, P), device=dev)
     dcoords = torch.empty_like(coords)
     flush = torch.empty(L2_FLUSH_BYTES // 4, device=dev, dtype=torch.float32)
-    perturb = args.workload == "uneven256"
+    perturb = workload_name == "uneven256"
     base = coords.clone()
     noise = torch.empty_like(coords)
 
@@ -2240,11 +2247,11 @@ def run_b200(args, world, rank, local):
     torch.cuda.synchronize()
 
     # timed region: K graph replays, L2 flushed before each (outside the events)
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     barrier(world)
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
-        for k in range(args.steps):
+        for k in range(steps):
             flush.zero_()
             ev[k][0].record()
             g.replay()
@@ -2253,13 +2260,13 @@ def run_b200(args, world, rank, local):
     barrier(world)
     ms = sum(a.elapsed_time(b) for a, b in ev)
     ms_max = max_over_ranks(ms, world)
-    poses_total = sum_over_ranks(P * args.steps, world)
+    poses_total = sum_over_ranks(P * steps, world)
     value = poses_total / (ms_max / 1e3)
 
     # kernel-level timing of the scoring kernel (direct launches, events
     # recorded by the library around each launch on the launching stream)
     plan.profile(True)
-    for _ in range(args.steps):
+    for _ in range(steps):
         flush.zero_()
         step()
     kern_ms, n_launch = plan.profile_read()
@@ -2272,7 +2279,7 @@ def run_b200(args, world, rank, local):
     h_E = torch.empty((3, P), pin_memory=True)
     h_g = torch.empty(coords.shape, pin_memory=True)
     d_in = torch.empty_like(coords)
-    e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     for _ in range(2):
         d_in.copy_(h_coords, non_blocking=True)
         plan.energy_and_gradient(d_in, weights, energies, dcoords)
@@ -2280,7 +2287,7 @@ def run_b200(args, world, rank, local):
         h_g.copy_(dcoords, non_blocking=True)
     torch.cuda.synchronize()
     barrier(world)
-    for k in range(args.steps):
+    for k in range(steps):
         flush.zero_()
         e2e_ev[k][0].record()
         d_in.copy_(h_coords, non_blocking=True)
@@ -2295,15 +2302,45 @@ def run_b200(args, world, rank, local):
     # runs them: step k+1's coordinates go in and step k-1's results come out
     # while step k computes; every step still copies its inputs in, flushes
     # L2 and copies its energies and gradient out inside the timed region
-    e2e_ms = pipelined_e2e_ms(plan, weights, h_coords, flush, args.steps, world, P)
+    e2e_ms = pipelined_e2e_ms(plan, weights, h_coords, flush, steps, world, P)
     e2e_value = poses_total / (e2e_ms / 1e3)
     h2d = coords.numel() * 4
     d2h = (3 * P + coords.numel()) * 4
 
+    # end to end through tmol's drop-in op, as a tmol caller runs it: the
+    # 27-argument ljlk_pose_scores on coordinates copied in from pinned host
+    # memory, backward() of the weighted energies through the autograd
+    # function, energies and gradient copied back, step by step
+    dropin_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    w_col = weights[:, :1].contiguous()
+
+    def dropin_step():
+        c = d_in.copy_(h_coords, non_blocking=True).requires_grad_(True)
+        E, _ = ljlk_pose_scores(c, *full_args)
+        (E * w_col).sum().backward()
+        h_E.copy_(E.detach(), non_blocking=True)
+        h_g.copy_(c.grad, non_blocking=True)
+        c.grad = None
+        c.requires_grad_(False)
+
+    for _ in range(3):
+        dropin_step()
+    torch.cuda.synchronize()
+    barrier(world)
+    for k in range(steps):
+        flush.zero_()
+        dropin_ev[k][0].record()
+        dropin_step()
+        dropin_ev[k][1].record()
+    torch.cuda.synchronize()
+    barrier(world)
+    dropin_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in dropin_ev), world)
+    clear_plan_cache()
+
     screened = None
-    if not args.no_screen:
+    if with_screen:
         screened = measure_screen(
-            plan, plan64, coords, weights, step, flush, args.steps, bt_names, ms_max / args.steps
+            plan, plan64, coords, weights, step, flush, steps, bt_names, ms_max / steps
         )
         del plan64
 
@@ -2313,7 +2350,7 @@ def run_b200(args, world, rank, local):
         # the elec term on the same batch and launch shape (its own workload
         # line: --workload elec64x150)
         eplan.set_launch(*launch_shape)
-        elec, _ = measure_elec(eplan, coords, flush, args.steps)
+        elec, _ = measure_elec(eplan, coords, flush, steps)
         elec["roofline_frac"] = elec["achieved_tflops"] / fp32_peak
         elec["metric"] = ELEC_METRIC
         del eplan
@@ -2322,28 +2359,29 @@ def run_b200(args, world, rank, local):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_for(args.workload, sizes_seeds, counts["atom_pairs"])
+        cpu = cpu_baseline_for(workload_name, sizes_seeds, counts["atom_pairs"])
 
+    line = None
     if rank == 0:
         peaks = measured_peaks()
         traffic = load_traffic()
         line = {
-            "metric": METRIC if args.workload == "uniform64x150" else METRIC.replace(
+            "metric": METRIC if workload_name == "uniform64x150" else METRIC.replace(
                 "64x150-residue batch", "256-pose uneven batch"
             ),
             "value": value,
             "unit": "poses/s",
             "n_gpus": world,
-            "steps": args.steps,
+            "steps": steps,
             "warmup": args.warmup,
-            "ms_per_step": ms_max / args.steps,
+            "ms_per_step": ms_max / steps,
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic (seeded proteins, ideal geometry)",
             "config": {
-                "workload": workload_label(args.workload),
+                "workload": workload_label(workload_name),
                 "poses_per_gpu": P,
                 "residues_per_gpu": n_residues,
                 "atoms_per_gpu": int(coords.shape[0]),
@@ -2354,9 +2392,9 @@ def run_b200(args, world, rank, local):
                 ),
                 "parallelism": f"weak, {world} independent batch(es)",
             },
-            "atom_pairs_per_s": counts["atom_pairs"] * args.steps * world / (ms_max / 1e3),
+            "atom_pairs_per_s": counts["atom_pairs"] * steps * world / (ms_max / 1e3),
             "work_per_step": counts,
-            "gpu_launches": 2 * args.steps,
+            "gpu_launches": 2 * steps,
             "clocks": clk.summary(),
             "roofline": {
                 "bound": "fp32",
@@ -2364,7 +2402,7 @@ def run_b200(args, world, rank, local):
                 "peak": fp32_peak,
                 "unit": "TFLOP/s",
                 "frac": achieved / fp32_peak,
-                "traffic": traffic if args.workload == "uniform64x150" else None,
+                "traffic": traffic if workload_name == "uniform64x150" else None,
                 "kernel": "score_kernel<float, GRAD> (fused neighbour + atom-pair energy and gradient)",
                 "kernel_ms": kern_avg_ms,
                 "flops_per_launch": flops,
@@ -2379,13 +2417,138 @@ def run_b200(args, world, rank, local):
                 "schedule": "double-buffered over copy-in / compute / copy-out streams; L2 flushed before every "
                 "step's compute, inside the timed region",
                 "serial_value": poses_total / (serial_ms / 1e3),
+                "dropin_value": poses_total / (dropin_ms / 1e3),
+                "dropin_schedule": "tmol's drop-in op ljlk_pose_scores (27 arguments) + backward() through its "
+                "autograd function, coordinates in from pinned host memory, energies and gradient out, step by "
+                "step, L2 flushed before each step inside the timed region",
             },
             "cpu_baseline": cpu,
             "screened": screened,
             "elec": elec,
         }
-        print(json.dumps(line), flush=True)
     del g
+    return line
+
+
+def sub_record(line):
+    """The parts of a workload's line that a sub-record keeps."""
+    keep = ("metric", "value", "unit", "steps", "ms_per_step", "config", "atom_pairs_per_s", "work_per_step",
+            "clocks", "roofline", "e2e", "cpu_baseline")
+    return {k: line[k] for k in keep if k in line}
+
+
+def measure_lbfgs(local, n_poses=32, n_res=300, iters=200):
+    """The minimisation scenario: 32 poses x 300 residues with chis + N(0,
+    30 deg), 200 iterations of the batched L-BFGS on Cartesian coordinates,
+    every energy + gradient one fused pass of the scoring kernel."""
+    import torch
+
+    from tmol_b200.optimization.lbfgs import LBFGSArmijo
+    from tmol_b200.optimization.minimize import BETA2016_WEIGHTS, make_func
+    from tmol_b200.pose.synthetic import synthetic_pose_stack
+    from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm, pose_score_args
+    from tmol_b200.score.ljlk_op import LJLKPlan
+
+    dev = torch.device("cuda", local)
+    ps = synthetic_pose_stack([n_res] * n_poses, list(range(n_poses)), device=dev, extra_chi_sd=30.0)
+    term = LJLKEnergyTerm(device=dev)
+    coords = ps.coords.flatten(0, 1).contiguous()
+    plan = LJLKPlan(coords, pose_score_args(ps, term)[:-1])
+    P, A = ps.n_poses, ps.max_n_pose_atoms
+    func = make_func(plan, BETA2016_WEIGHTS, P, A)
+    x0 = ps.coords.reshape(P, -1)
+    E0, _ = func(x0)
+    LBFGSArmijo(func, x0, max_iter=3).run()  # warm-up
+    opt = LBFGSArmijo(func, x0, max_iter=iters)
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    wall0 = time.perf_counter()
+    t0.record()
+    x, E, gr = opt.run()
+    t1.record()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    ms = t0.elapsed_time(t1)
+    return {
+        "scenario": f"{n_poses} poses x {n_res} residues, chis + N(0, 30 deg), beta2016 LJ/LK weights, "
+        f"batched L-BFGS (Armijo) on Cartesian coordinates, {iters} iterations at most",
+        "iterations": len(opt.history) - 1,
+        "evaluations": opt.n_evals,
+        "ms_total": ms,
+        "wall_s": wall,
+        "ms_per_evaluation": ms / max(opt.n_evals, 1),
+        "energy_before_mean": float(E0.mean()),
+        "energy_after_mean": float(E.mean()),
+        "poses_whose_energy_fell": int((E < E0).sum()),
+        "max_abs_grad_after": float(gr.abs().max()),
+    }
+
+
+def measure_screen_eval(local, reps=20):
+    """The learned block-pair screen on its held-out batch (16 poses x 1000
+    residues, chis + N(0, 20 deg)): skipped fraction, per-pose |dE| in
+    float64, and the energy + gradient step against the plain kernel, with
+    the screen rebuilt every step and with the mask reused; beside it the
+    exact zero-energy mask, the most any block-pair screen could skip (its
+    speedup is the ceiling of the method on this kernel)."""
+    import numpy
+    import torch
+
+    from tmol_b200.chem.restypes import default_packed_block_types
+    from tmol_b200.score.ljlk_energy_term import LJLKEnergyTerm
+    from tmol_b200.screen.mlp import ScreenMLP
+    from tmol_b200.screen.screen import TRAINED_WEIGHTS
+    from tmol_b200.screen.train import evaluate
+
+    dev = torch.device("cuda", local)
+    term = LJLKEnergyTerm(device=dev)
+    names = [bt.name for bt in default_packed_block_types(dev).active_block_types]
+    mlp, thr = ScreenMLP.load(TRAINED_WEIGHTS, dev, names)
+    gap_thr = float(numpy.load(TRAINED_WEIGHTS, allow_pickle=False)["gap_threshold"])
+    sizes, seeds = [1000] * 16, [30_000_000 + k for k in range(16)]
+    res = evaluate(mlp, thr, gap_thr, sizes, seeds, 20.0, term, dev, reps, log=lambda m: None)
+    lr, ceil = res["learned"], res["exact_zero_mask"]
+    return {
+        "workload": "16 held-out poses x 1000 residues, chis + N(0, 20 deg), energy + gradient, L2 flushed",
+        "plain_ms": res["plain_ms"],
+        "candidates": res["candidates"],
+        "skipped_fraction": lr["skipped_fraction_of_candidates"],
+        "max_abs_dE_per_pose_f64": lr["max_abs_dE_f64_total"],
+        "budget_kcal_per_mol": 0.01,
+        "speedup_with_update": lr.get("speedup_with_update"),
+        "speedup_mask_reused": lr["speedup_kernel_only"],
+        "update_ms": lr.get("update_ms"),
+        "ceiling": {
+            "what": "exact zero-energy mask (every candidate whose block-pair energy is zero skipped; no update "
+            "cost counted): the most a block-pair screen can save on this kernel",
+            "skipped_fraction": ceil["skipped_fraction_of_candidates"],
+            "speedup": ceil["speedup_kernel_only"],
+        },
+        "sphere_gap_rule": {
+            "skipped_fraction": res["sphere_gap_rule"]["skipped_fraction_of_candidates"],
+            "speedup_mask_reused": res["sphere_gap_rule"]["speedup_kernel_only"],
+        },
+    }
+
+
+def run_b200(args, world, rank, local):
+    import torch
+
+    line = measure_pose_batch(args, args.workload, world, rank, local, args.steps)
+    # the other configurations of the path, as sub-records of the default
+    # line (one GPU): the uneven batch through 100 perturbed graph replays,
+    # the L-BFGS scenario, and the learned screen against its ceiling
+    if args.workload == "uniform64x150" and world == 1 and not args.no_extras:
+        torch.cuda.empty_cache()
+        uneven = measure_pose_batch(args, "uneven256", world, rank, local, UNEVEN_REPLAYS, extras=False)
+        line["uneven256"] = sub_record(uneven)
+        torch.cuda.empty_cache()
+        line["lbfgs"] = measure_lbfgs(local)
+        torch.cuda.empty_cache()
+        if not args.no_screen:
+            line["screen_eval"] = measure_screen_eval(local)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
 
@@ -2410,6 +2573,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-screen", action="store_true", help="skip the learned-screen measurement")
     ap.add_argument("--no-elec", action="store_true", help="skip the elec summary of the default line")
+    ap.add_argument(
+        "--no-extras", action="store_true",
+        help="skip the default line's sub-records (uneven batch, L-BFGS, screen evaluation)",
+    )
     ap.add_argument(
         "--launch",
         default="",
