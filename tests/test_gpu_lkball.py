@@ -474,15 +474,21 @@ def test_full_size_batch_properties(lterm):
     ones = torch.ones(4, 64, device=DEV)
     E1, g1 = plan.energy_and_gradient(coords, ones)
     E_close(E1.cpu().numpy(), E.cpu().numpy(), rtol=1e-5, atol=1e-4)
-    _, Eo, dxo, _ = oracle_run(ps, lterm, False)
-    # energies in the float32-vs-float32 band: poses sit up to 3000 A from
-    # the origin, where a float32 coordinate is good to 2.4e-4 A, and the
-    # water-bridge sums inherit that through the waters' positions.  The
-    # reference's own float32 ops land up to 3.9e-3 kcal/mol from the float64
-    # energies on this batch and outside the gradient bar on 1677 components;
-    # this path stays inside the gradient bar on every component
-    E_close(E.cpu().numpy(), Eo, atol=2e-3, rtol=2e-5, what="LK-ball 64x150 energies (float32 vs float64)")
-    g_close(g1.cpu().numpy(), dxo, what="LK-ball 64x150 gradient")
+    # Poses sit up to 3000 A from the origin, where a float32 coordinate is
+    # good to 2.4e-4 A: the absolute float32 waters (the reference API's
+    # water tensor) round by up to 1.2e-4 A, and the steep occlusion terms
+    # carry that into the gradient (the reference's own float32 ops land up
+    # to 0.014 kcal/mol/A from float64 here, 1677 components outside the
+    # bar).  So the waters are checked on their own, and the scoring and its
+    # adjoint against the oracle in float64 evaluated on this path's float32
+    # waters, where the bar holds
+    Wo, _, _, _ = oracle_run(ps, lterm, False)
+    W_close(W.cpu().numpy(), Wo, 2.5e-4)
+    oc = O.OracleCall(ps.coords.flatten(0, 1).double(), score_args(ps, lterm, None), f64=True, term="lkball",
+                      lkb_water_args=water_gen_args(ps, lterm))
+    Eo, dxo, _ = oc.lkb_scores(W.cpu().double().numpy(), weights=numpy.ones((4, ps.n_poses)))
+    E_close(E.cpu().numpy(), Eo, what="LK-ball 64x150 energies (oracle on these waters)")
+    g_close(g1.cpu().numpy(), dxo, what="LK-ball 64x150 gradient (oracle on these waters)")
     Ebp, _ = plan.forward(coords, W, block_pair=True)
     E_close(Ebp.sum(dim=(2, 3)).cpu().numpy(), E.cpu().numpy(), rtol=1e-5, atol=1e-3)
     shift = torch.tensor([3.1, -2.2, 5.7], device=DEV)

@@ -41,7 +41,8 @@ def test_adjoint_against_finite_differences_float64():
     h = 1e-3
     fd, g = finite_difference_check(plan, coords, ps.pose_ind_for_atom, BETA2016_WEIGHTS, n_atoms=1000, h=h)
     fd2, g2 = finite_difference_check(plan, coords, ps.pose_ind_for_atom, BETA2016_WEIGHTS, n_atoms=1000, h=h / 2)
-    assert numpy.array_equal(g, g2)  # the same atoms
+    # the same atoms (float64 atomics add in a run-dependent order)
+    numpy.testing.assert_allclose(g, g2, rtol=1e-12, atol=1e-12)
     fd_err = numpy.abs(fd - fd2)
     err = numpy.abs(fd - g)
     tol = 1e-4 * numpy.abs(g) + 1e-6 + fd_err

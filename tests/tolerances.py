@@ -15,13 +15,19 @@ atom, and on these synthetic poses (hard clashes: per-atom contributions of
 loses up to ~1e-3 kcal/mol/A whichever order it is taken in.  The
 reference's own float32 op, measured against its float64 result on eight
 150-residue poses (oracle/ljlk_oracle.c is bit-exact with it), has a largest
-error of 1.4e-3 kcal/mol/A and no component outside this band; the scoring
-kernels sum in a different order (per-atom partial sums in shared memory,
-then one global atomic per atom and work item), not a less accurate one.
+error of 1.4e-3 kcal/mol/A and no component outside this band.  The scoring
+kernels sum in another order (per-atom partial sums in shared memory, then
+one global atomic per atom and work item).
 
 Comparing two float32 results of the same sums (the reference op's stored
 float32 output, or the GPU path against itself) doubles both terms, since
 each side carries its own rounding (g_close_f32).
+
+Rotamer-set gradients (the packer's ops) sum several times more
+contributions per coordinate (a rotamer meets every rotamer of each
+neighbouring block), and the reference's own float32 rotamer op lands up to
+3.5e-3 kcal/mol/A from its float64 result on the test sets: they are held to
+the float32-vs-float32 band (g_close_rotamers).
 
 float64 paths are held to 1e-9 relative + 1e-9 absolute.
 """
@@ -80,4 +86,9 @@ def g_close(g, ref, rtol=G_RTOL, floor=None, what="gradient"):
 
 def g_close_f32(g, ref, what="gradient (float32 vs float32)"):
     """Two float32 results of the same sums: each side's band, added."""
+    g_close(g, ref, rtol=2 * G_RTOL, floor=2 * G_FLOOR, what=what)
+
+
+def g_close_rotamers(g, ref, what="rotamer-set gradient"):
+    """Rotamer-set gradients against the float64 oracle: the doubled band."""
     g_close(g, ref, rtol=2 * G_RTOL, floor=2 * G_FLOOR, what=what)
