@@ -537,12 +537,15 @@ __global__ void spheres_kernel(ScoreArgs<Real> s) {
 // (LJ + LK) pairs from the back.  Both sides live in one atom array (side 0
 // at [0, TILE), side 1 at [TILE, TILE + M1)), each atom one 16-byte record
 // (x, y, z, type) so that a pair costs two vector loads; an entry packs
-// a1 (5 bits) | j in the atom array (7 bits) | count-pair-weight-0.2 flag
-// (bit 12).
+// a (5 bits: a side-0 atom) | k (7 bits: an index into the atom array) |
+// count-pair-weight-0.2 flag (bit 12).  Entries come in runs that share k:
+// screening emits each side-1 atom's pairs together, the intra-tile pass
+// each row's.  One screening chunk (32 side-1 atoms x 32 rows) emits at
+// most 1024 entries, so a queue of QCAP >= 1024 takes any chunk whole.
 
 constexpr int M1 = 64;
 constexpr int MAX_SLOTS = 8;
-constexpr int QCAP = 512;
+constexpr int QCAP = 1024;
 constexpr int kTfHeavy = 256;
 
 enum SlotKind : int {
@@ -752,6 +755,7 @@ __device__ TMOL_B200_LJLK_OUTLINE E3<Real> eval_queue(EvalCtx<Real> c, Slab<Real
     int i = base + lane;
     bool act = i < n;
     int e = act ? (int)w.queue[HEAVY ? QCAP - 1 - i : i] : 0;
+    // j: the entry's k (runs of equal k are consecutive), a1: its a
     int a1 = e & 31, j = (e >> 5) & 127;
     Real wcp = (e >> 12) & 1 ? Real(0.2) : Real(1);
     Real fx = 0, fy = 0, fz = 0;
@@ -779,6 +783,8 @@ __device__ TMOL_B200_LJLK_OUTLINE E3<Real> eval_queue(EvalCtx<Real> c, Slab<Real
       const AtomRec<Real> p1 = w.at[a1];
       const AtomRec<Real> p2 = w.at[j];
       int t1 = p1.tf & 0xff, t2 = p2.tf & 0xff;
+      // the table row of k's type: the entries of one step mostly share it
+      // (LJ records are symmetric, an LK record's two directions sum alike)
       Real dx = p1.x - p2.x;
       Real dy = p1.y - p2.y;
       Real dz = p1.z - p2.z;
@@ -787,7 +793,7 @@ __device__ TMOL_B200_LJLK_OUTLINE E3<Real> eval_queue(EvalCtx<Real> c, Slab<Real
       // which never use inv_d, and add no force
       const Real inv_d = inv_sqrt(d2);
       const Real d = d2 > Real(0) ? d2 * inv_d : Real(0);
-      int tp = t1 * c.ntp + t2;
+      int tp = t2 * c.ntp + t1;
       LJRecord<Real> lr = c.ljtab[tp];
       Real atr, rep, datr, drep;
       lj_eval<Real, GRAD>(d, inv_d, lr, dmax, atr, rep, datr, drep);
@@ -809,10 +815,10 @@ __device__ TMOL_B200_LJLK_OUTLINE E3<Real> eval_queue(EvalCtx<Real> c, Slab<Real
       }
     }
     if (GRAD) {
-      // segments: maximal runs of lanes with equal a1; a run only merges
-      // lanes before the next segment head, so a1 values that recur later
-      // in the warp form separate segments
-      int key = act ? a1 : -1 - lane;
+      // segments: maximal runs of lanes with equal j (the entry's k); a
+      // run only merges lanes before the next segment head, so j values that
+      // recur later in the warp form separate segments
+      int key = act ? j : -1 - lane;
       int kprev = __shfl_up_sync(0xffffffffu, key, 1);
       bool head = lane == 0 || kprev != key;
       unsigned heads = __ballot_sync(0xffffffffu, head);
@@ -830,35 +836,20 @@ __device__ TMOL_B200_LJLK_OUTLINE E3<Real> eval_queue(EvalCtx<Real> c, Slab<Real
           sz += tz;
         }
       }
-      // segment heads and j targets: a lane whose address no other lane of
-      // this step touches adds without an atomic; lanes sharing an address
-      // (a1 recurring in two segments, j in two rows' entries) use atomics
+      // segment heads and a targets add with shared-memory atomics: the
+      // same j can head two segments and the same a1 sit in two runs'
+      // entries of one step (cheaper than finding the unique targets)
       const bool add0 = act && head;
-      const unsigned me = 1u << lane;
-      const unsigned p0 = __match_any_sync(0xffffffffu, add0 ? a1 : -1 - lane);
-      const unsigned p1 = __match_any_sync(0xffffffffu, act ? j : -1 - lane);
       if (add0) {
-        if (p0 == me) {
-          w.gx[a1] += sx;
-          w.gy[a1] += sy;
-          w.gz[a1] += sz;
-        } else {
-          atomicAdd(&w.gx[a1], sx);
-          atomicAdd(&w.gy[a1], sy);
-          atomicAdd(&w.gz[a1], sz);
-        }
+        atomicAdd(&w.gx[j], -sx);
+        atomicAdd(&w.gy[j], -sy);
+        atomicAdd(&w.gz[j], -sz);
       }
       __syncwarp();
       if (act) {
-        if (p1 == me) {
-          w.gx[j] -= fx;
-          w.gy[j] -= fy;
-          w.gz[j] -= fz;
-        } else {
-          atomicAdd(&w.gx[j], -fx);
-          atomicAdd(&w.gy[j], -fy);
-          atomicAdd(&w.gz[j], -fz);
-        }
+        atomicAdd(&w.gx[a1], fx);
+        atomicAdd(&w.gy[a1], fy);
+        atomicAdd(&w.gz[a1], fz);
       }
       __syncwarp();  // the next step's adds may touch the same atoms
     }
@@ -931,7 +922,8 @@ __device__ TMOL_B200_LJLK_OUTLINE E3<Real> intra_tile(EvalCtx<Real> c, Slab<Real
         hv = TERM == kTermLJLK && in && (p1.tf & p2.tf & kTfHeavy);
       }
     }
-    queue_push(w.queue, in, hv, a1 | (a2 << 5) | (wbit << 12), lane, nl, nh);
+    // the row a1 is the entry's k (a row's entries are consecutive)
+    queue_push(w.queue, in, hv, a2 | (a1 << 5) | (wbit << 12), lane, nl, nh);
     a1 += qq;
     a2 += rr;
     if (a2 >= c1) {
@@ -967,6 +959,8 @@ __device__ TMOL_B200_LJLK_OUTLINE E3<Real> screen_slots(EvalCtx<Real> c, Slab<Re
     }
   }
   const unsigned rows = __ballot_sync(0xffffffffu, act0);
+  const unsigned heavy_rows =
+      TERM == kTermLJLK ? __ballot_sync(0xffffffffu, lane < c1 && (w.at[lane].tf & kTfHeavy)) : 0u;
   int nl = 0, nh = 0;
   for (int cbase = 0; cbase < m; cbase += 32) {
     const int j = cbase + lane;
@@ -1025,6 +1019,9 @@ __device__ TMOL_B200_LJLK_OUTLINE E3<Real> screen_slots(EvalCtx<Real> c, Slab<Re
       }
     }
     const unsigned live = valid ? rows & ~excl : 0u;
+    // distance tests of this lane's atom against every active row, as a
+    // row mask (no per-pair ballots)
+    unsigned inm = 0;
     for (unsigned rm = rows; rm; rm &= rm - 1) {
       const int a1 = __ffs(rm) - 1;
       const AtomRec<Real> pa = w.at[a1];
@@ -1032,12 +1029,38 @@ __device__ TMOL_B200_LJLK_OUTLINE E3<Real> screen_slots(EvalCtx<Real> c, Slab<Re
       const Real dy = pa.y - yj;
       const Real dz = pa.z - zj;
       const Real d2 = dx * dx + dy * dy + dz * dz;
-      const bool in = ((live >> a1) & 1u) && d2 < maxd2;
-      const bool hv = TERM == kTermLJLK && in && (heavy_j & pa.tf);
-      const int wbit = (w02 >> a1) & 1u;
-      queue_push(w.queue, in, hv, a1 | ((TILE + j) << 5) | (wbit << 12), lane, nl, nh);
-      if (nl + nh > QCAP - 32) drain_queue<Real, GRAD, TERM>(c, wp, nl, nh, lane, acc);
+      inm |= (d2 < maxd2 ? 1u : 0u) << a1;
     }
+    inm &= live;
+    const unsigned hm = heavy_j ? inm & heavy_rows : 0u;
+    const unsigned lm = inm & ~hm;
+    // each lane's entries go out together (a run of equal k), at offsets
+    // from a warp scan of the counts (LJ-only low half-word, heavy high)
+    const int cnt = __popc(lm) | (__popc(hm) << 16);
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const int tot = __shfl_sync(0xffffffffu, incl, 31);
+    const int tl = tot & 0xffff, th = tot >> 16;
+    if (tl + th == 0) continue;
+    if (nl + nh + tl + th > QCAP) drain_queue<Real, GRAD, TERM>(c, wp, nl, nh, lane, acc);
+    const int before = incl - cnt;
+    int ql = nl + (before & 0xffff);
+    int qh = nh + (before >> 16);
+    const int kbits = (TILE + j) << 5;
+    for (unsigned b = lm; b; b &= b - 1) {
+      const int a1 = __ffs(b) - 1;
+      w.queue[ql++] = (uint16_t)(a1 | kbits | (int)(((w02 >> a1) & 1u) << 12));
+    }
+    for (unsigned b = hm; b; b &= b - 1) {
+      const int a1 = __ffs(b) - 1;
+      w.queue[QCAP - 1 - qh++] = (uint16_t)(a1 | kbits | (int)(((w02 >> a1) & 1u) << 12));
+    }
+    nl += tl;
+    nh += th;
   }
   drain_queue<Real, GRAD, TERM>(c, wp, nl, nh, lane, acc);
   return acc;
