@@ -2469,9 +2469,38 @@ def measure_lbfgs(local, n_poses=32, n_res=300, iters=200):
     torch.cuda.synchronize()
     wall = time.perf_counter() - wall0
     ms = t0.elapsed_time(t1)
+    # tmol's route: run_min over a CartesianSfxnNetwork of the score function
+    # with LBFGS_Armijo (tmol's interface and steps), every evaluation the
+    # drop-in op's forward and its autograd adjoint
+    from tmol_b200.optimization.minimizers import run_min
+    from tmol_b200.optimization.sfxn_modules import CartesianSfxnNetwork
+    from tmol_b200.score.score_function import ScoreFunction
+
+    sfxn = ScoreFunction.from_weights({"fa_ljatr": 1.0, "fa_ljrep": 0.55, "fa_lk": 1.0}, device=dev)
+    net = CartesianSfxnNetwork(sfxn, ps)
+    run_min(CartesianSfxnNetwork(sfxn, ps), optimizer_kwargs=dict(max_iter=3))  # warm-up
+    torch.cuda.synchronize()
+    t2, t3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t2.record()
+    out, topt = run_min(net, optimizer_kwargs=dict(max_iter=iters))
+    t3.record()
+    torch.cuda.synchronize()
+    tms = t2.elapsed_time(t3)
+    E_t = topt.energy_history[-1]
+    tmol_route = {
+        "what": "tmol's route: run_min over CartesianSfxnNetwork(ScoreFunction beta2016 LJ/LK) with "
+        "LBFGS_Armijo (tmol's interface and steps), each evaluation the drop-in op + autograd adjoint",
+        "iterations": len(topt.energy_history) - 1,
+        "evaluations": topt.n_evals,
+        "ms_total": tms,
+        "ms_per_evaluation": tms / max(topt.n_evals, 1),
+        "energy_after_mean": float(E_t.mean()),
+        "poses_whose_energy_fell": int((E_t < topt.energy_history[0]).sum()),
+    }
     return {
         "scenario": f"{n_poses} poses x {n_res} residues, chis + N(0, 30 deg), beta2016 LJ/LK weights, "
         f"batched L-BFGS (Armijo) on Cartesian coordinates, {iters} iterations at most",
+        "tmol_lbfgs_armijo": tmol_route,
         "iterations": len(opt.history) - 1,
         "evaluations": opt.n_evals,
         "ms_total": ms,
