@@ -483,7 +483,8 @@ def test_full_size_batch_properties(lterm):
     # adjoint against the oracle in float64 evaluated on this path's float32
     # waters, where the bar holds
     Wo, _, _, _ = oracle_run(ps, lterm, False)
-    W_close(W.cpu().numpy(), Wo, 2.5e-4)
+    # a few float32 roundings at the waters' magnitude (2.4e-4 A at 3000 A)
+    W_close(W.cpu().numpy(), Wo, 4 * float(numpy.spacing(numpy.float32(numpy.nanmax(numpy.abs(Wo))))))
     oc = O.OracleCall(ps.coords.flatten(0, 1).double(), score_args(ps, lterm, None), f64=True, term="lkball",
                       lkb_water_args=water_gen_args(ps, lterm))
     Eo, dxo, _ = oc.lkb_scores(W.cpu().double().numpy(), weights=numpy.ones((4, ps.n_poses)))

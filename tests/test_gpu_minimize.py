@@ -26,12 +26,15 @@ def test_lbfgs_lowers_every_pose_energy():
 
 def test_adjoint_against_finite_differences_float64():
     """Every one of 1000 random atoms x 3 components, none exempt:
-    |g - fd| <= 1e-4 |g| + 1e-6 + |fd(h) - fd(h/2)|.  The last term is the
-    difference quotient's own error, measured per component: on a smooth
-    stretch central differences err by O(h^2) and the two quotients agree
-    to ~1e-7; within h of a region boundary of the potentials (the LJ
-    linear extension, the spline knots, where the second derivative jumps)
-    the quotient errs by O(h) and the two quotients differ by as much."""
+    |g - fd| <= 1e-4 |g| + 1e-6 + 2 |fd(h) - fd(h/2)|.  The last term bounds
+    the difference quotient's own error, measured per component: a quotient
+    converging at order p >= 1 errs by at most |fd(h) - fd(h/2)| / (1 - 2^-p)
+    <= 2 |fd(h) - fd(h/2)|.  On a smooth stretch central differences err by
+    O(h^2) and the two quotients agree to ~1e-7; near a region boundary of
+    the potentials (the LJ linear extension, the spline knots, where the
+    second derivative jumps) or on a hard clash (third derivatives of 1e4
+    and more) the quotient errs by up to ~0.04 at h = 1e-3 and converges to
+    the analytic value as h shrinks."""
     ps = synthetic_pose_stack([300] * 32, list(range(32)), device=DEV, extra_chi_sd=30.0)
     term = LJLKEnergyTerm(device=DEV)
     static = [a.double() if isinstance(a, torch.Tensor) and a.is_floating_point() else a
@@ -45,7 +48,7 @@ def test_adjoint_against_finite_differences_float64():
     numpy.testing.assert_allclose(g, g2, rtol=1e-12, atol=1e-12)
     fd_err = numpy.abs(fd - fd2)
     err = numpy.abs(fd - g)
-    tol = 1e-4 * numpy.abs(g) + 1e-6 + fd_err
+    tol = 1e-4 * numpy.abs(g) + 1e-6 + 2 * fd_err
     smooth = fd_err < 1e-5
     print(
         f"[fd] {err.size} components: max |fd - g| {err.max():.3e}; on the {int(smooth.sum())} smooth ones "
