@@ -50,6 +50,7 @@ UNEVEN_POSES = 256
 UNEVEN_SEED = 2
 PERTURB_SD = 0.05
 UNEVEN_REPLAYS = 100  # graph replays of the uneven batch's sub-record
+LAUNCH_FIELDS = ("items_per_ticket", "warps_per_cta", "ctas_per_sm", "candidates_per_item", "slots_per_group")
 L2_FLUSH_BYTES = 256 << 20
 # the rotamer workload: 16 poses x 150 residues, every block with 1..31
 # rotamers (the native one first; chis resampled, a quarter mutated)
@@ -1353,7 +1354,7 @@ def run_elec(args, world, rank, local):
                 "l2": "flushed (256 MiB write) before every timed step",
                 "launch": "CUDA graph replay: 2 kernels per step",
                 "launch_shape": dict(
-                    zip(("items_per_ticket", "warps_per_cta", "ctas_per_sm", "candidates_per_item"), launch)
+                    zip(LAUNCH_FIELDS, launch)
                 ),
                 "parallelism": f"weak, {world} independent batch(es)",
             },
@@ -1641,7 +1642,7 @@ def run_lkball(args, world, rank, local):
                 "launch": "CUDA graph replay: 4 kernels per step (waters, block spheres, scoring with its "
                 "adjoint, waters adjoint) and 5 memsets",
                 "launch_shape": dict(
-                    zip(("items_per_ticket", "warps_per_cta", "ctas_per_sm", "candidates_per_item"), launch)
+                    zip(LAUNCH_FIELDS, launch)
                 ),
                 "parallelism": f"weak, {world} independent batch(es)",
             },
@@ -2388,7 +2389,7 @@ def measure_pose_batch(args, workload_name, world, rank, local, steps, extras=Tr
                 "l2": "flushed (256 MiB write) before every timed step",
                 "launch": "CUDA graph replay: 2 kernels per step" + (" + perturbation" if perturb else ""),
                 "launch_shape": dict(
-                    zip(("items_per_ticket", "warps_per_cta", "ctas_per_sm", "candidates_per_item"), launch_shape)
+                    zip(LAUNCH_FIELDS, launch_shape)
                 ),
                 "parallelism": f"weak, {world} independent batch(es)",
             },
@@ -2609,7 +2610,7 @@ def main():
     ap.add_argument(
         "--launch",
         default="",
-        help="fixed launch shape items_per_ticket,warps_per_cta,ctas_per_sm,candidates_per_item "
+        help="fixed launch shape items_per_ticket,warps_per_cta,ctas_per_sm,candidates_per_item[,slots_per_group] "
         "(default: autotune)",
     )
     args = ap.parse_args()

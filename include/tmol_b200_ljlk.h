@@ -89,12 +89,16 @@ typedef struct {
  *   rows_per_item        work items a warp takes per atomic ticket
  *   warps_per_cta        warps per CTA (at most 8); every warp works alone
  *   ctas_per_sm          resident CTAs per SM of the persistent grid
- *   candidates_per_item  candidate blocks b2 per work item (at most 1024) */
+ *   candidates_per_item  candidate blocks b2 per work item (at most 1024)
+ *   slots_per_group      neighbouring blocks whose atoms share one pass of
+ *                        the warp's 32 lanes (1-8, default 8): how many
+ *                        block pairs a warp screens at once */
 typedef struct {
   int32_t rows_per_item;
   int32_t warps_per_cta;
   int32_t ctas_per_sm;
   int32_t candidates_per_item;
+  int32_t slots_per_group;
 } tmol_b200_ljlk_launch;
 
 typedef struct tmol_b200_ljlk_plan tmol_b200_ljlk_plan;

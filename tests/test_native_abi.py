@@ -83,3 +83,20 @@ def test_op_refuses_cpu_tensors(ubq_pose_stack, term):
     args = pose_score_args(ubq_pose_stack, term)
     with pytest.raises(RuntimeError, match="CUDA"):
         ljlk_pose_scores(ubq_pose_stack.coords.flatten(0, 1), *args)
+
+
+def test_autotuner_block_size_summary():
+    """The autotuner's cache key summarises the PoseStack's blocks: real
+    blocks per pose, mean atoms per block, the share of blocks per size bin."""
+    import types
+
+    import torch
+
+    from tmol_b200.tune import SIZE_BINS, block_size_summary
+
+    bt = torch.tensor([[0, 1, 2, -1], [2, 2, -1, -1]])
+    n_atoms = torch.tensor([7, 20, 40])
+    per_pose, mean, hist = block_size_summary(types.SimpleNamespace(block_sizes=(bt, n_atoms), n_poses=2))
+    assert per_pose == 2.5 and abs(mean - (7 + 20 + 40 + 40 + 40) / 5) < 1e-5
+    assert len(hist) == len(SIZE_BINS) + 1 and abs(sum(hist) - 1) < 1e-6
+    assert abs(hist[0] - 0.2) < 1e-6 and abs(hist[2] - 0.2) < 1e-6 and abs(hist[-1] - 0.6) < 1e-6

@@ -30,6 +30,7 @@
 // row) and are flushed to global memory once per block pair (b2) or row (b1).
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cstdint>
@@ -453,6 +454,7 @@ struct ScoreArgs {
   // pair (never honoured for b1 == b2 or count-pair partners)
   const uint32_t* skip;
   int skip_words;  // 32-bit words per row
+  int max_slots;   // neighbouring blocks packed per screening group
   // elec plans: partial charge per block-type atom [nbt * A] and the
   // potential's per-unit-charge constants (ElecK layout)
   const Real* bt_q;
@@ -1138,7 +1140,7 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
   __syncwarp();
   const bool want_E = !GRAD || s.energies != nullptr;
   const int64_t stride = (int64_t)s.P * s.B * s.B;
-  const int max_slots = BLOCK_PAIR ? 1 : MAX_SLOTS;
+  const int max_slots = BLOCK_PAIR ? 1 : s.max_slots;
   const Real reach_atoms = s.g.max_dis;
 
   for (;;) {
@@ -2020,6 +2022,8 @@ void default_launch(tmol_b200_ljlk_launch& l) {
   if (l.warps_per_cta <= 0) l.warps_per_cta = 8;
   if (l.ctas_per_sm <= 0) l.ctas_per_sm = 2;
   if (l.candidates_per_item <= 0) l.candidates_per_item = 64;
+  if (l.slots_per_group <= 0) l.slots_per_group = MAX_SLOTS;
+  l.slots_per_group = std::min(l.slots_per_group, MAX_SLOTS);
   l.rows_per_item = std::min(l.rows_per_item, MAX_ROWS_PER_ITEM);
   l.warps_per_cta = std::min(l.warps_per_cta, MAX_WARPS);
   l.candidates_per_item = std::min(l.candidates_per_item, 32 * 32);
@@ -2122,6 +2126,7 @@ ScoreArgs<Real> score_args(tmol_b200_ljlk_plan* pl, const void* coords) {
   s.counts = pl->counts;
   s.skip = pl->skip;
   s.skip_words = pl->skip_words;
+  s.max_slots = pl->launch.slots_per_group > 0 ? pl->launch.slots_per_group : MAX_SLOTS;
   return s;
 }
 
@@ -3100,15 +3105,29 @@ int rotamer_backward(tmol_b200_ljlk_plan* plan, int term, const void* coords, co
 
 extern "C" {
 
+namespace {
+// An NVTX range around an entry point's work (named by the entry point), so
+// that the scoring calls show up in Nsight Systems timelines; without a tool
+// attached a push/pop costs a few nanoseconds.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
+}  // namespace
+
 int tmol_b200_ljlk_plan_create(const tmol_b200_ljlk_inputs* in, int real_bytes,
                                const tmol_b200_ljlk_launch* launch,
                                void* stream, tmol_b200_ljlk_plan** plan_out) {
+  NvtxRange nvtx_range("tmol_b200_ljlk_plan_create");
   return create_plan(in, real_bytes, launch, stream, false, plan_out);
 }
 
 int tmol_b200_ljlk_rotamer_plan_create(const tmol_b200_ljlk_inputs* in, int real_bytes,
                                        const tmol_b200_ljlk_launch* launch,
                                        void* stream, tmol_b200_ljlk_plan** plan_out) {
+  NvtxRange nvtx_range("tmol_b200_ljlk_rotamer_plan_create");
   return create_plan(in, real_bytes, launch, stream, true, plan_out);
 }
 
@@ -3116,6 +3135,7 @@ int tmol_b200_ljlk_plan_create_from_connectivity(const tmol_b200_ljlk_inputs* in
                                                  const tmol_b200_pose_connectivity* conn, int real_bytes,
                                                  const tmol_b200_ljlk_launch* launch, void* stream,
                                                  int rotamers, tmol_b200_ljlk_plan** plan_out) {
+  NvtxRange nvtx_range("tmol_b200_ljlk_plan_create_from_connectivity");
   if (!conn) return TMOL_B200_ERR_INVALID_ARGUMENT;
   return create_plan(in, real_bytes, launch, stream, rotamers != 0, plan_out, nullptr, conn);
 }
@@ -3124,6 +3144,7 @@ int tmol_b200_elec_plan_create_from_connectivity(const tmol_b200_elec_inputs* in
                                                  const tmol_b200_pose_connectivity* conn, int real_bytes,
                                                  const tmol_b200_ljlk_launch* launch, void* stream,
                                                  int rotamers, tmol_b200_elec_plan** plan_out) {
+  NvtxRange nvtx_range("tmol_b200_elec_plan_create_from_connectivity");
   if (!conn) return TMOL_B200_ERR_INVALID_ARGUMENT;
   return create_elec_plan(in, real_bytes, launch, stream, rotamers != 0, plan_out, conn);
 }
@@ -3147,12 +3168,14 @@ int tmol_b200_ljlk_plan_set_launch(tmol_b200_ljlk_plan* plan,
 int tmol_b200_ljlk_forward(tmol_b200_ljlk_plan* plan, const void* coords,
                            int block_pair, void* energies,
                            int32_t* block_neighbors, void* stream) {
+  NvtxRange nvtx_range("tmol_b200_ljlk_forward");
   return pose_forward(plan, kTermLJLK, coords, block_pair, energies, block_neighbors, stream);
 }
 
 int tmol_b200_ljlk_backward(tmol_b200_ljlk_plan* plan, const void* coords,
                             int block_pair, const void* dTdV, void* dcoords,
                             void* stream) {
+  NvtxRange nvtx_range("tmol_b200_ljlk_backward");
   return pose_backward(plan, kTermLJLK, coords, block_pair, dTdV, dcoords, stream);
 }
 
@@ -3160,6 +3183,7 @@ int tmol_b200_ljlk_energy_and_gradient(tmol_b200_ljlk_plan* plan,
                                        const void* coords, const void* weights,
                                        void* energies, void* dcoords,
                                        void* stream) {
+  NvtxRange nvtx_range("tmol_b200_ljlk_energy_and_gradient");
   return pose_energy_and_gradient(plan, kTermLJLK, coords, weights, energies, dcoords, stream);
 }
 
@@ -3229,6 +3253,7 @@ int tmol_b200_measure_fp32_peak(void* stream, double* tflops) {
 }
 
 int tmol_b200_ljlk_plan_rebalance(tmol_b200_ljlk_plan* plan, void* stream) {
+  NvtxRange nvtx_range("tmol_b200_ljlk_plan_rebalance");
   if (!plan) return TMOL_B200_ERR_INVALID_ARGUMENT;
   int n = plan->n_work;
   if (n == 0) return TMOL_B200_OK;
@@ -3269,6 +3294,7 @@ int tmol_b200_ljlk_screen_candidates(tmol_b200_ljlk_plan* plan,
                                      int32_t* pair_row, int32_t* pair_b2,
                                      int32_t* pair_bt, float* features,
                                      int32_t* count, void* stream) {
+  NvtxRange nvtx_range("tmol_b200_ljlk_screen_candidates");
   if (!plan || !count || capacity < 0 || (!coords && plan->N > 0))
     return TMOL_B200_ERR_INVALID_ARGUMENT;
   if (capacity > 0 && (!pair_row || !pair_b2 || !pair_bt || !features))
@@ -3294,23 +3320,27 @@ int tmol_b200_ljlk_screen_candidates(tmol_b200_ljlk_plan* plan,
 
 int tmol_b200_ljlk_rotamer_count(tmol_b200_ljlk_plan* plan, const void* coords,
                                   int64_t* n_pairs, int64_t* n_items, void* stream) {
+  NvtxRange nvtx_range("tmol_b200_ljlk_rotamer_count");
   return rotamer_count(plan, kTermLJLK, coords, n_pairs, n_items, stream);
 }
 
 int tmol_b200_ljlk_rotamer_fill(tmol_b200_ljlk_plan* plan, int32_t* indices, int32_t* items,
                                 void* stream) {
+  NvtxRange nvtx_range("tmol_b200_ljlk_rotamer_fill");
   return rotamer_fill(plan, kTermLJLK, indices, items, stream);
 }
 
 int tmol_b200_ljlk_rotamer_forward(tmol_b200_ljlk_plan* plan, const void* coords,
                                     const int32_t* items, int64_t n_items, int64_t n_pairs,
                                     void* energies, void* stream) {
+  NvtxRange nvtx_range("tmol_b200_ljlk_rotamer_forward");
   return rotamer_forward(plan, kTermLJLK, coords, items, n_items, n_pairs, energies, stream);
 }
 
 int tmol_b200_ljlk_rotamer_backward(tmol_b200_ljlk_plan* plan, const void* coords,
                                      const int32_t* items, int64_t n_items, int64_t n_pairs,
                                      const void* dTdV, void* dcoords, void* stream) {
+  NvtxRange nvtx_range("tmol_b200_ljlk_rotamer_backward");
   return rotamer_backward(plan, kTermLJLK, coords, items, n_items, n_pairs, dTdV, dcoords, stream);
 }
 
@@ -3320,12 +3350,14 @@ int tmol_b200_ljlk_rotamer_backward(tmol_b200_ljlk_plan* plan, const void* coord
 int tmol_b200_elec_plan_create(const tmol_b200_elec_inputs* in, int real_bytes,
                                const tmol_b200_ljlk_launch* launch, void* stream,
                                tmol_b200_elec_plan** plan_out) {
+  NvtxRange nvtx_range("tmol_b200_elec_plan_create");
   return create_elec_plan(in, real_bytes, launch, stream, false, plan_out);
 }
 
 int tmol_b200_elec_rotamer_plan_create(const tmol_b200_elec_inputs* in, int real_bytes,
                                        const tmol_b200_ljlk_launch* launch, void* stream,
                                        tmol_b200_elec_plan** plan_out) {
+  NvtxRange nvtx_range("tmol_b200_elec_rotamer_plan_create");
   return create_elec_plan(in, real_bytes, launch, stream, true, plan_out);
 }
 
@@ -3337,39 +3369,46 @@ int tmol_b200_elec_plan_destroy(tmol_b200_elec_plan* plan) {
 
 int tmol_b200_elec_forward(tmol_b200_elec_plan* plan, const void* coords, int block_pair,
                            void* energies, int32_t* block_neighbors, void* stream) {
+  NvtxRange nvtx_range("tmol_b200_elec_forward");
   return pose_forward(plan, kTermElec, coords, block_pair, energies, block_neighbors, stream);
 }
 
 int tmol_b200_elec_backward(tmol_b200_elec_plan* plan, const void* coords, int block_pair,
                             const void* dTdV, void* dcoords, void* stream) {
+  NvtxRange nvtx_range("tmol_b200_elec_backward");
   return pose_backward(plan, kTermElec, coords, block_pair, dTdV, dcoords, stream);
 }
 
 int tmol_b200_elec_energy_and_gradient(tmol_b200_elec_plan* plan, const void* coords,
                                        const void* weights, void* energies, void* dcoords,
                                        void* stream) {
+  NvtxRange nvtx_range("tmol_b200_elec_energy_and_gradient");
   return pose_energy_and_gradient(plan, kTermElec, coords, weights, energies, dcoords, stream);
 }
 
 int tmol_b200_elec_rotamer_count(tmol_b200_elec_plan* plan, const void* coords,
                                  int64_t* n_pairs, int64_t* n_items, void* stream) {
+  NvtxRange nvtx_range("tmol_b200_elec_rotamer_count");
   return rotamer_count(plan, kTermElec, coords, n_pairs, n_items, stream);
 }
 
 int tmol_b200_elec_rotamer_fill(tmol_b200_elec_plan* plan, int32_t* indices, int32_t* items,
                                 void* stream) {
+  NvtxRange nvtx_range("tmol_b200_elec_rotamer_fill");
   return rotamer_fill(plan, kTermElec, indices, items, stream);
 }
 
 int tmol_b200_elec_rotamer_forward(tmol_b200_elec_plan* plan, const void* coords,
                                    const int32_t* items, int64_t n_items, int64_t n_pairs,
                                    void* energies, void* stream) {
+  NvtxRange nvtx_range("tmol_b200_elec_rotamer_forward");
   return rotamer_forward(plan, kTermElec, coords, items, n_items, n_pairs, energies, stream);
 }
 
 int tmol_b200_elec_rotamer_backward(tmol_b200_elec_plan* plan, const void* coords,
                                     const int32_t* items, int64_t n_items, int64_t n_pairs,
                                     const void* dTdV, void* dcoords, void* stream) {
+  NvtxRange nvtx_range("tmol_b200_elec_rotamer_backward");
   return rotamer_backward(plan, kTermElec, coords, items, n_items, n_pairs, dTdV, dcoords, stream);
 }
 
@@ -3378,6 +3417,7 @@ int tmol_b200_elec_rotamer_backward(tmol_b200_elec_plan* plan, const void* coord
 int tmol_b200_lkball_plan_create(const tmol_b200_lkball_inputs* inputs, int real_bytes,
                                  const tmol_b200_ljlk_launch* launch, void* stream,
                                  tmol_b200_lkball_plan** plan_out) {
+  NvtxRange nvtx_range("tmol_b200_lkball_plan_create");
   return create_lkball_plan(inputs, real_bytes, launch, stream, false, plan_out);
 }
 
@@ -3385,6 +3425,7 @@ int tmol_b200_lkball_plan_create_from_connectivity(const tmol_b200_lkball_inputs
                                                    const tmol_b200_pose_connectivity* conn, int real_bytes,
                                                    const tmol_b200_ljlk_launch* launch, void* stream, int rotamers,
                                                    tmol_b200_lkball_plan** plan_out) {
+  NvtxRange nvtx_range("tmol_b200_lkball_plan_create_from_connectivity");
   if (!conn) return TMOL_B200_ERR_INVALID_ARGUMENT;
   return create_lkball_plan(inputs, real_bytes, launch, stream, rotamers != 0, plan_out, conn);
 }
@@ -3392,16 +3433,19 @@ int tmol_b200_lkball_plan_create_from_connectivity(const tmol_b200_lkball_inputs
 int tmol_b200_lkball_rotamer_plan_create(const tmol_b200_lkball_inputs* inputs, int real_bytes,
                                          const tmol_b200_ljlk_launch* launch, void* stream,
                                          tmol_b200_lkball_plan** plan_out) {
+  NvtxRange nvtx_range("tmol_b200_lkball_rotamer_plan_create");
   return create_lkball_plan(inputs, real_bytes, launch, stream, true, plan_out);
 }
 
 int tmol_b200_lkball_rotamer_count(tmol_b200_lkball_plan* plan, const void* coords, int64_t* n_pairs,
                                    int64_t* n_items, void* stream) {
+  NvtxRange nvtx_range("tmol_b200_lkball_rotamer_count");
   if (!plan || !plan->lkb_pol) return TMOL_B200_ERR_INVALID_ARGUMENT;
   return rotamer_count(plan, kTermLKBall, coords, n_pairs, n_items, stream);
 }
 
 int tmol_b200_lkball_rotamer_fill(tmol_b200_lkball_plan* plan, int32_t* indices, int32_t* items, void* stream) {
+  NvtxRange nvtx_range("tmol_b200_lkball_rotamer_fill");
   if (!plan || !plan->lkb_pol) return TMOL_B200_ERR_INVALID_ARGUMENT;
   return rotamer_fill(plan, kTermLKBall, indices, items, stream);
 }
@@ -3409,6 +3453,7 @@ int tmol_b200_lkball_rotamer_fill(tmol_b200_lkball_plan* plan, int32_t* indices,
 int tmol_b200_lkball_rotamer_forward(tmol_b200_lkball_plan* plan, const void* coords, const void* waters,
                                      const int32_t* items, int64_t n_items, int64_t n_pairs, void* energies,
                                      void* stream) {
+  NvtxRange nvtx_range("tmol_b200_lkball_rotamer_forward");
   if (!rotamer_plan_of(plan, kTermLKBall) || !plan->lkb_pol || !energies || n_items < 0 || n_pairs < 0 ||
       (n_items > 0 && !items) || (plan->N > 0 && (!coords || !waters)))
     return TMOL_B200_ERR_INVALID_ARGUMENT;
@@ -3424,6 +3469,7 @@ int tmol_b200_lkball_rotamer_forward(tmol_b200_lkball_plan* plan, const void* co
 int tmol_b200_lkball_rotamer_backward(tmol_b200_lkball_plan* plan, const void* coords, const void* waters,
                                       const int32_t* items, int64_t n_items, int64_t n_pairs, const void* dTdV,
                                       void* dcoords, void* dwaters, void* stream) {
+  NvtxRange nvtx_range("tmol_b200_lkball_rotamer_backward");
   if (!rotamer_plan_of(plan, kTermLKBall) || !plan->lkb_pol || !dTdV || !dcoords || !dwaters || n_items < 0 ||
       n_pairs < 0 || (n_items > 0 && !items) || (plan->N > 0 && (!coords || !waters)))
     return TMOL_B200_ERR_INVALID_ARGUMENT;
@@ -3443,6 +3489,7 @@ int tmol_b200_lkball_plan_destroy(tmol_b200_lkball_plan* plan) {
 }
 
 int tmol_b200_lkball_waters(tmol_b200_lkball_plan* plan, const void* coords, void* waters, void* stream) {
+  NvtxRange nvtx_range("tmol_b200_lkball_waters");
   if (!plan || plan->term != kTermLKBall || !plan->lkb_sites) return TMOL_B200_ERR_INVALID_ARGUMENT;
   if (plan->N > 0 && (!coords || !waters)) return TMOL_B200_ERR_INVALID_ARGUMENT;
   cudaStream_t st = (cudaStream_t)stream;
@@ -3452,6 +3499,7 @@ int tmol_b200_lkball_waters(tmol_b200_lkball_plan* plan, const void* coords, voi
 
 int tmol_b200_lkball_waters_backward(tmol_b200_lkball_plan* plan, const void* coords, const void* dwaters,
                                      void* dcoords, void* stream) {
+  NvtxRange nvtx_range("tmol_b200_lkball_waters_backward");
   if (!plan || plan->term != kTermLKBall || !plan->lkb_sites) return TMOL_B200_ERR_INVALID_ARGUMENT;
   if (plan->N > 0 && (!coords || !dwaters || !dcoords)) return TMOL_B200_ERR_INVALID_ARGUMENT;
   cudaStream_t st = (cudaStream_t)stream;
@@ -3461,6 +3509,7 @@ int tmol_b200_lkball_waters_backward(tmol_b200_lkball_plan* plan, const void* co
 
 int tmol_b200_lkball_forward(tmol_b200_lkball_plan* plan, const void* coords, const void* waters,
                              int block_pair, void* energies, int32_t* block_neighbors, void* stream) {
+  NvtxRange nvtx_range("tmol_b200_lkball_forward");
   if (!plan || plan->term != kTermLKBall || !plan->lkb_pol || !energies) return TMOL_B200_ERR_INVALID_ARGUMENT;
   if (plan->N > 0 && (!coords || !waters)) return TMOL_B200_ERR_INVALID_ARGUMENT;
   cudaStream_t st = (cudaStream_t)stream;
@@ -3477,6 +3526,7 @@ int tmol_b200_lkball_forward(tmol_b200_lkball_plan* plan, const void* coords, co
 
 int tmol_b200_lkball_energy_and_gradient(tmol_b200_lkball_plan* plan, const void* coords, const void* weights,
                                          void* energies, void* dcoords, void* stream) {
+  NvtxRange nvtx_range("tmol_b200_lkball_energy_and_gradient");
   if (!plan || plan->term != kTermLKBall || !plan->lkb_pol || !plan->lkb_sites || !weights || !energies ||
       !dcoords)
     return TMOL_B200_ERR_INVALID_ARGUMENT;
@@ -3500,6 +3550,7 @@ int tmol_b200_lkball_energy_and_gradient(tmol_b200_lkball_plan* plan, const void
 int tmol_b200_lkball_backward(tmol_b200_lkball_plan* plan, const void* coords, const void* waters,
                               int block_pair, const void* dTdV, void* dcoords, void* dwaters,
                               void* stream) {
+  NvtxRange nvtx_range("tmol_b200_lkball_backward");
   if (!plan || plan->term != kTermLKBall || !plan->lkb_pol || !dTdV) return TMOL_B200_ERR_INVALID_ARGUMENT;
   if (plan->N > 0 && (!coords || !waters || !dcoords || !dwaters)) return TMOL_B200_ERR_INVALID_ARGUMENT;
   cudaStream_t st = (cudaStream_t)stream;

@@ -144,6 +144,7 @@ class Launch(ctypes.Structure):
         ("warps_per_cta", ctypes.c_int32),
         ("ctas_per_sm", ctypes.c_int32),
         ("candidates_per_item", ctypes.c_int32),
+        ("slots_per_group", ctypes.c_int32),
     ]
 
 

@@ -57,6 +57,7 @@ class ElecPlan(LJLKPlan):
             max_dis,
         ) = static_args
         device = self._set_device(coords_like)
+        self.block_sizes = (first_rot_block_type, bt_n_atoms)  # for the autotuner's signature
         ints = dict(
             rot_coord_offset=rot_coord_offset,
             pose_ind_for_atom=pose_ind_for_atom,

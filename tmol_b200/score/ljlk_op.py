@@ -61,6 +61,7 @@ class LJLKPlan:
             max_dis,
         ) = static_args
         device = self._set_device(coords_like)
+        self.block_sizes = (first_rot_block_type, bt_n_atoms)  # for the autotuner's signature
         ints = dict(
             rot_coord_offset=rot_coord_offset,
             pose_ind_for_atom=pose_ind_for_atom,
@@ -195,14 +196,16 @@ class LJLKPlan:
                 pass
             self.ptr = None
 
-    def set_launch(self, rows_per_item=0, warps_per_cta=0, ctas_per_sm=0, candidates_per_item=0):
+    def set_launch(self, rows_per_item=0, warps_per_cta=0, ctas_per_sm=0, candidates_per_item=0,
+                   slots_per_group=0):
         """Launch shape (0 = default); see tmol_b200_ljlk_launch."""
-        self.launch = native.Launch(rows_per_item, warps_per_cta, ctas_per_sm, candidates_per_item)
+        self.launch = native.Launch(rows_per_item, warps_per_cta, ctas_per_sm, candidates_per_item,
+                                    slots_per_group)
         native.call("tmol_b200_ljlk_plan_set_launch", self.ptr, ctypes.byref(self.launch))
 
     def launch_tuple(self):
         l = self.launch
-        return (l.rows_per_item, l.warps_per_cta, l.ctas_per_sm, l.candidates_per_item)
+        return (l.rows_per_item, l.warps_per_cta, l.ctas_per_sm, l.candidates_per_item, l.slots_per_group)
 
     def rebalance(self):
         """Order the work items longest-first by their cost in the last call."""

@@ -74,6 +74,8 @@ class LKBallPlan(LJLKPlan):
             put(name, t)
         s.max_n_rots_per_pose = int(common[11])
         P, B = common[2].shape
+        bt_sizes = (water_static if water_static is not None else score_static)[13 if water_static is not None else 15]
+        self.block_sizes = (common[3], bt_sizes)  # for the autotuner's signature
         if water_static is not None:
             if len(water_static) != N_WATER_STATIC:
                 raise TypeError(f"gen_pose_waters takes coords + {N_WATER_STATIC} arguments")

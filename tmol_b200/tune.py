@@ -1,12 +1,16 @@
 """Autotuner for the scoring kernel's launch shape and work order.
 
-The tunables are the fields of ``tmol_b200_ljlk_launch`` (work items per
-ticket, warps per CTA, CTAs per SM, candidate blocks per work item) and the
-order of the work items (longest-first by measured cost, see
-``LJLKPlan.rebalance``).  Each candidate shape is timed with the library's
-CUDA events around the scoring kernel; the winner is cached in a JSON file
-keyed by GPU name and a signature of the workload (poses, rows, mean block
-size), so a later plan for a similar PoseStack starts from it.
+The tunables are the fields of ``tmol_b200_ljlk_launch``: work items per
+ticket, warps per CTA, CTAs per SM, candidate blocks per work item (how a
+row's block pairs are partitioned into work items) and neighbouring blocks
+per screening group (how many block pairs share one pass of a warp's 32
+lanes: the kernel's "threads per block pair"); and the order of the work
+items (longest-first by measured cost, see ``LJLKPlan.rebalance``).  Each
+candidate shape is timed with the library's CUDA events around the scoring
+kernel; the winner is cached in a JSON file keyed by GPU name and a
+signature of the workload (poses, block slots, real blocks per pose and
+the histogram of atoms per block), so a later plan for a similar PoseStack
+starts from it.
 
 Cache file: ``$TMOL_B200_TUNE_CACHE`` or ``~/.cache/tmol_b200/launch.json``.
 """
@@ -22,7 +26,11 @@ DEFAULT_GRID = {
     "warps_per_cta": (4, 8),
     "ctas_per_sm": (2, 3, 4),
     "candidates_per_item": (32, 64, 128),
+    "slots_per_group": (4, 8),
 }
+
+# atoms per block: histogram bin edges of the signature
+SIZE_BINS = (8, 16, 24, 32)
 
 
 def _cache_path():
@@ -31,10 +39,33 @@ def _cache_path():
     )
 
 
-def signature(plan, mean_block_atoms):
+def block_size_summary(plan):
+    """(real blocks per pose, mean atoms per block, fraction of blocks per
+    SIZE_BINS bin) of the plan's PoseStack, from its block types."""
+    block_type, bt_n_atoms = plan.block_sizes
+    bt = block_type.reshape(-1).to(torch.int64)
+    real = bt >= 0
+    n = bt_n_atoms.to(torch.int64)[bt.clamp(min=0)][real].float()
+    if n.numel() == 0:
+        return 0.0, 0.0, (0.0,) * (len(SIZE_BINS) + 1)
+    edges = torch.tensor(SIZE_BINS, dtype=n.dtype, device=n.device)
+    bins = torch.bucketize(n, edges, right=False)
+    hist = torch.bincount(bins, minlength=len(SIZE_BINS) + 1).float() / n.numel()
+    return float(n.numel()) / plan.n_poses, float(n.mean()), tuple(float(h) for h in hist.cpu())
+
+
+def signature(plan):
+    """The cache key: GPU, term, dtype, poses and block slots, and the
+    block-size summary (real blocks per pose to the nearest 10, mean atoms
+    per block to the nearest atom, the size histogram to the nearest 5 %)."""
     name = torch.cuda.get_device_name(plan.device)
     term = getattr(plan, "NAME", "LJ/LK")
-    return f"{name}|{term}|P={plan.n_poses}|B={plan.max_n_blocks}|atoms/block={mean_block_atoms:.0f}|{plan.dtype}"
+    per_pose, mean_atoms, hist = block_size_summary(plan)
+    h = ",".join(f"{round(20 * x) * 5}" for x in hist)
+    return (
+        f"{name}|{term}|{plan.dtype}|P={plan.n_poses}|B={plan.max_n_blocks}|"
+        f"blocks/pose={10 * round(per_pose / 10)}|atoms/block={mean_atoms:.0f}|sizes%={h}"
+    )
 
 
 def _load_cache():
@@ -66,11 +97,11 @@ def time_kernel(plan, run, reps=5):
     return ms / max(n, 1)
 
 
-def autotune(plan, run, grid=None, reps=5, mean_block_atoms=16.0, use_cache=True, verbose=False):
+def autotune(plan, run, grid=None, reps=5, use_cache=True, verbose=False):
     """Pick the fastest launch shape for `run` (a closure making one scoring
     call on `plan`), leave it set, rebalance the work order, and return
     (shape, milliseconds)."""
-    key = signature(plan, mean_block_atoms)
+    key = signature(plan)
     cache = _load_cache() if use_cache else {}
     if key in cache:
         shape = tuple(cache[key]["shape"])
