@@ -744,19 +744,24 @@ __device__ __forceinline__ void cnt_add(unsigned long long* c, int k, long long 
 // screening order, so lanes sharing a1 are mostly contiguous: their a1
 // forces are summed with a segmented shuffle reduction and added once per
 // segment.
-template <typename Real, bool GRAD, bool HEAVY, int TERM = kTermLJLK>
+template <typename Real, bool GRAD, int TERM = kTermLJLK>
 __device__ TMOL_B200_LJLK_OUTLINE E3<Real> eval_queue(EvalCtx<Real> c, Slab<Real>* wp,
-                                            int n, int lane) {
+                                            int nl, int nh, int lane) {
   Slab<Real>& w = *wp;
   E3<Real> acc = {0, 0, 0};
   const Real dmax = c.max_dis;
   const Real far_dmin = c.max_dis - Real(1.5);
+  const Real far_first = far_dmin > Real(4.5) ? far_dmin : Real(4.5);
   ElecK<Real> K;
   if (TERM == kTermElec) K = load_elec_k(c.elec_k);
+  // one pass over the LJ-only entries, then the heavy-atom ones: only the
+  // step holding both has lanes on different paths
+  const int n = nl + nh;
   for (int base = 0; base < n; base += 32) {
     int i = base + lane;
     bool act = i < n;
-    int e = act ? (int)w.queue[HEAVY ? QCAP - 1 - i : i] : 0;
+    const bool heavy = TERM == kTermLJLK && i >= nl;
+    int e = act ? (int)w.queue[heavy ? QCAP - 1 - (i - nl) : i] : 0;
     // j: the entry's k (runs of equal k are consecutive), a1: its a
     int a1 = e & 31, j = (e >> 5) & 127;
     Real wcp = (e >> 12) & 1 ? Real(0.2) : Real(1);
@@ -802,10 +807,9 @@ __device__ TMOL_B200_LJLK_OUTLINE E3<Real> eval_queue(EvalCtx<Real> c, Slab<Real
       acc.atr += wcp * atr;
       acc.rep += wcp * rep;
       Real dE = c.wt0 * datr + c.wt1 * drep;
-      if (HEAVY) {
-        LKRecord<Real> kr = c.lktab[tp];
+      if (heavy) {
         Real lk, dlk;
-        lk_eval<Real, GRAD>(d, inv_d, kr, far_dmin, dmax, lk, dlk);
+        lk_eval<Real, GRAD>(d, inv_d, c.lktab + tp, far_dmin, far_first, dmax, lk, dlk);
         acc.lk += wcp * lk;
         dE += c.wt2 * dlk;
       }
@@ -866,16 +870,11 @@ __device__ __forceinline__ void drain_queue(const EvalCtx<Real>& c,
   __syncwarp();
   cnt_add(wp->counts, 3, nl + nh, lane);
   cnt_add(wp->counts, 4, nh, lane);
-  if (TERM == kTermLJLK && nh) {
-    E3<Real> e = eval_queue<Real, GRAD, true>(c, wp, nh, lane);
+  if (nl + nh) {
+    E3<Real> e = eval_queue<Real, GRAD, TERM>(c, wp, nl, nh, lane);
     acc.atr += e.atr;
     acc.rep += e.rep;
     acc.lk += e.lk;
-  }
-  if (nl) {
-    E3<Real> e = eval_queue<Real, GRAD, false, TERM>(c, wp, nl, lane);
-    acc.atr += e.atr;
-    acc.rep += e.rep;
   }
   __syncwarp();
   nl = 0;

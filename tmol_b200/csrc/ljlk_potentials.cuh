@@ -350,14 +350,22 @@ struct LJRecord {  // 8 values
 };
 
 template <typename Real>
-struct LKRecord {  // 16 values (13 used)
+struct alignas(4 * sizeof(Real)) LKRecord {  // 16 values (13 used), four groups of four
   Real close_dmin, close_dmax;
   Real flat_V;                // both directions at d_min
+  Real pad0;
   Real cmax_V, cmax_dV;       // both directions at close_dmax
   Real fmin_V, fmin_dV;       // both directions at far_dmin
   Real c_i, r_i, il2_i;       // i desolvated by j: c * exp(-(d-r)^2 * il2) / d^2
+  Real pad1;
   Real c_j, r_j, il2_j;       // j desolvated by i
-  Real pad0, pad1, pad2;
+  Real pad2;
+};
+
+// A group of four table values, read with one vector load.
+template <typename Real>
+struct alignas(4 * sizeof(Real)) Quad {
+  Real a, b, c, d;
 };
 
 template <typename Real>
@@ -436,37 +444,58 @@ __device__ __forceinline__ void lj_eval(Real d, Real inv, const LJRecord<Real>& 
   }
 }
 
-// Unweighted LK (both directions) and, with DERIV, its distance
-// derivative; inv_d = 1 / d.
+// The fade-out cubic of LK beyond far_dmin from its knot value and slope.
 template <typename Real, bool DERIV>
-__device__ __forceinline__ void lk_eval(Real d, Real inv_d, const LKRecord<Real>& r,
-                                        Real far_dmin, Real far_dmax, Real& V,
+__device__ __forceinline__ void lk_far(Real d, Real fmin_V, Real fmin_dV, Real far_dmin, Real far_dmax,
+                                       Real& V, Real& dV) {
+  Real h = far_dmax - far_dmin;
+  Real t = (d - far_dmin) / h;
+  Real p0 = fmin_V, dp0 = fmin_dV * h;
+  V = p0 + t * (dp0 + t * (-2 * dp0 - 3 * p0 + t * (dp0 + 2 * p0)));
+  if (DERIV) dV = (dp0 + t * (-4 * dp0 - 6 * p0 + t * (3 * dp0 + 6 * p0))) / h;
+}
+
+// Unweighted LK (both directions) and, with DERIV, its distance
+// derivative; inv_d = 1 / d.  The regions are tested in the order flat,
+// close cubic, Gaussians, fade-out; beyond far_first = max(far_dmin, 4.5 A)
+// only the fade-out can apply (every close cubic ends by sqrt(405 / 20) =
+// 4.5 A), so that, the most populated region, is tested first.  Only the
+// group of four record values a region needs is read.
+template <typename Real, bool DERIV>
+__device__ __forceinline__ void lk_eval(Real d, Real inv_d, const LKRecord<Real>* rp,
+                                        Real far_dmin, Real far_first, Real far_dmax, Real& V,
                                         Real& dV) {
+  const Quad<Real>* q = reinterpret_cast<const Quad<Real>*>(rp);
   dV = 0;
-  if (d < r.close_dmin) {
-    V = r.flat_V;
-  } else if (d < r.close_dmax) {
-    Real h = r.close_dmax - r.close_dmin;
-    Real t = (d - r.close_dmin) / h;
-    Real p0 = r.flat_V, p1 = r.cmax_V, dp1 = r.cmax_dV * h;
+  if (d >= far_first) {
+    const Quad<Real> k = q[1];  // cmax_V, cmax_dV, fmin_V, fmin_dV
+    lk_far<Real, DERIV>(d, k.c, k.d, far_dmin, far_dmax, V, dV);
+    return;
+  }
+  const Quad<Real> b = q[0];  // close_dmin, close_dmax, flat_V
+  if (d < b.a) {
+    V = b.c;
+  } else if (d < b.b) {
+    const Quad<Real> k = q[1];
+    Real h = b.b - b.a;
+    Real t = (d - b.a) / h;
+    Real p0 = b.c, p1 = k.a, dp1 = k.b * h;
     V = p0 + t * (t * (-dp1 - 3 * p0 + 3 * p1 + t * (dp1 + 2 * p0 - 2 * p1)));
     if (DERIV) dV = (t * (-2 * dp1 - 6 * p0 + 6 * p1 + t * (3 * dp1 + 6 * p0 - 6 * p1))) / h;
   } else if (d < far_dmin) {
+    const Quad<Real> gi = q[2], gj = q[3];  // (c, r, il2) of each direction
     Real inv_d2 = inv_d * inv_d;
-    Real xi = d - r.r_i, xj = d - r.r_j;
-    Real ei = r.c_i * exp(-xi * xi * r.il2_i);
-    Real ej = r.c_j * exp(-xj * xj * r.il2_j);
+    Real xi = d - gi.b, xj = d - gj.b;
+    Real ei = gi.a * exp(-xi * xi * gi.c);
+    Real ej = gj.a * exp(-xj * xj * gj.c);
     V = (ei + ej) * inv_d2;
     if (DERIV) {
-      dV = inv_d2 * (ei * (Real(-2) * inv_d - Real(2) * xi * r.il2_i) +
-                     ej * (Real(-2) * inv_d - Real(2) * xj * r.il2_j));
+      dV = inv_d2 * (ei * (Real(-2) * inv_d - Real(2) * xi * gi.c) +
+                     ej * (Real(-2) * inv_d - Real(2) * xj * gj.c));
     }
   } else {
-    Real h = far_dmax - far_dmin;
-    Real t = (d - far_dmin) / h;
-    Real p0 = r.fmin_V, dp0 = r.fmin_dV * h;
-    V = p0 + t * (dp0 + t * (-2 * dp0 - 3 * p0 + t * (dp0 + 2 * p0)));
-    if (DERIV) dV = (dp0 + t * (-4 * dp0 - 6 * p0 + t * (3 * dp0 + 6 * p0))) / h;
+    const Quad<Real> k = q[1];
+    lk_far<Real, DERIV>(d, k.c, k.d, far_dmin, far_dmax, V, dV);
   }
 }
 
