@@ -547,6 +547,10 @@ __global__ void spheres_kernel(ScoreArgs<Real> s) {
 
 constexpr int M1 = 64;
 constexpr int MAX_SLOTS = 8;
+// copies of the side-0 force accumulators: lane l adds an entry's force on
+// its side-0 atom into copy l % A_COPIES, so that at most four lanes of a
+// step can meet at one address (shared atomics serialise on a conflict)
+constexpr int A_COPIES = 8;
 constexpr int QCAP = 1024;
 constexpr int kTfHeavy = 256;
 
@@ -573,6 +577,7 @@ template <typename Real>
 struct Slab {
   AtomRec<Real> at[N_ATOMS];            // side 0, then side 1
   Real gx[N_ATOMS], gy[N_ATOMS], gz[N_ATOMS];  // gradient accumulators
+  Real ga[A_COPIES][3][TILE];  // side-0 forces of entries' a atoms, by copy
   uint32_t cpd0[TILE];  // bond separation to each connection atom, a byte each
   uint32_t cpd1[M1];
   int gidx1[M1];  // global atom index
@@ -638,6 +643,12 @@ __device__ __forceinline__ void stage_side0(const ScoreArgs<Real>& s,
     w.gy[lane] = 0;
     w.gz[lane] = 0;
   }
+#pragma unroll
+  for (int k = 0; k < A_COPIES; ++k) {
+    w.ga[k][0][lane] = 0;
+    w.ga[k][1][lane] = 0;
+    w.ga[k][2][lane] = 0;
+  }
 }
 
 // Append the atoms of [start, start + cnt) of block (bt, off) that can reach
@@ -692,6 +703,12 @@ __device__ __forceinline__ void flush_side0(const ScoreArgs<Real>& s,
   if (lane < cnt) {
     Real* d = s.dcoords + 3 * ((int64_t)off + start + lane);
     Real gx = w.gx[lane], gy = w.gy[lane], gz = w.gz[lane];
+#pragma unroll
+    for (int k = 0; k < A_COPIES; ++k) {
+      gx += w.ga[k][0][lane];
+      gy += w.ga[k][1][lane];
+      gz += w.ga[k][2][lane];
+    }
     if (gx != 0) atomicAdd(d + 0, gx);
     if (gy != 0) atomicAdd(d + 1, gy);
     if (gz != 0) atomicAdd(d + 2, gz);
@@ -853,9 +870,10 @@ __device__ TMOL_B200_LJLK_OUTLINE E3<Real> eval_queue(EvalCtx<Real> c, Slab<Real
       }
       __syncwarp();
       if (act) {
-        atomicAdd(&w.gx[a1], fx);
-        atomicAdd(&w.gy[a1], fy);
-        atomicAdd(&w.gz[a1], fz);
+        Real(*ga)[TILE] = w.ga[lane & (A_COPIES - 1)];
+        atomicAdd(&ga[0][a1], fx);
+        atomicAdd(&ga[1][a1], fy);
+        atomicAdd(&ga[2][a1], fz);
       }
       __syncwarp();  // the next step's adds may touch the same atoms
     }
