@@ -176,6 +176,22 @@ __global__ void plan_blocks_kernel(PlanBuildArgs a) {
 
 // Rotamer plan: per rotamer, its pose, block, block type and coordinates
 // must be in range and the rotamer must lie in its block's range.
+// One record per block slot for the scoring kernel's row and neighbour
+// loads: {block type or -1, first atom, atom count, connections | ligand
+// flag << 8}, from the validated block tables.
+__global__ void plan_block_info_kernel(int64_t n, const int* blk_bt, const int* blk_off, const int* bt_n_atoms,
+                                       const int* bt_n_conn, const int* bt_is_ligand, int4* out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int bt = blk_bt[i];
+    int4 r = make_int4(bt, blk_off[i], 0, 0);
+    if (bt >= 0) {
+      r.z = bt_n_atoms[bt];
+      r.w = (bt_n_conn[bt] & 0xff) | ((bt_is_ligand[bt] ? 1 : 0) << 8);
+    }
+    out[i] = r;
+  }
+}
+
 __global__ void plan_rotamers_kernel(PlanBuildArgs a) {
   const tmol_b200_ljlk_inputs& in = a.in;
   const int P = in.n_poses, B = in.max_n_blocks;
@@ -419,8 +435,17 @@ __global__ void plan_count_pair_conn_kernel(PlanBuildArgs a) {
 // per-call kernels
 
 template <typename Real>
+struct AtomRec;
+
+template <typename Real>
 struct ScoreArgs {
   const Real* coords;
+  // pose plans of the LJ/LK and elec terms: per block {block type, first
+  // atom, atom count, connections | ligand << 8} and every atom as a
+  // staged record (coordinates with its type or charge), written by the
+  // sphere kernel each call; null elsewhere (the staging then gathers)
+  const int4* blk_info;
+  AtomRec<Real>* packed;
   const int* blk_bt;
   const int* blk_off;
   const int* pose_last;
@@ -520,12 +545,17 @@ __device__ __forceinline__ void warp_sphere(const Real* coords, const int* bt_n_
 }
 
 template <typename Real>
+__device__ __forceinline__ void pack_block(const ScoreArgs<Real>& s, int bt, int off, int lane);
+
+template <typename Real>
 __global__ void spheres_kernel(ScoreArgs<Real> s) {
   const int lane = threadIdx.x & 31;
   const int n_blocks = s.P * s.B;
   const int warps = (gridDim.x * blockDim.x) >> 5;
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n_blocks; i += warps)
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n_blocks; i += warps) {
     warp_sphere(s.coords, s.bt_n_atoms, s.blk_bt[i], s.blk_off[i], lane, s.spheres + 4 * (int64_t)i);
+    if (s.packed) pack_block(s, s.blk_bt[i], s.blk_off[i], lane);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -572,6 +602,27 @@ struct alignas(16) AtomRec {
 };
 
 constexpr int N_ATOMS = TILE + M1;
+
+// Writes block (bt, off)'s atoms as staged records: coordinates and the
+// block-type atom's compact type | heavy flag (LJ/LK) or partial charge
+// (elec), so that staging a block costs one vector load per atom.
+template <typename Real>
+__device__ __forceinline__ void pack_block(const ScoreArgs<Real>& s, int bt, int off, int lane) {
+  if (bt < 0) return;
+  const int n = s.bt_n_atoms[bt];
+  for (int k = lane; k < n; k += 32) {
+    const Real* c = s.coords + 3 * ((int64_t)off + k);
+    AtomRec<Real> a;
+    a.x = c[0];
+    a.y = c[1];
+    a.z = c[2];
+    if (s.bt_q)
+      a.q = s.bt_q[(int64_t)bt * s.A + k];
+    else
+      a.tf = s.bt_tf[(int64_t)bt * s.A + k];
+    s.packed[(int64_t)off + k] = a;
+  }
+}
 
 template <typename Real>
 struct Slab {
@@ -628,15 +679,19 @@ __device__ __forceinline__ void stage_side0(const ScoreArgs<Real>& s,
                                             int lane) {
   if (lane < cnt) {
     int at = start + lane;
-    const Real* c = s.coords + 3 * ((int64_t)off + at);
     AtomRec<Real> a;
-    a.x = c[0];
-    a.y = c[1];
-    a.z = c[2];
-    if (TERM == kTermElec)
-      a.q = s.bt_q[(int64_t)bt * s.A + at];
-    else
-      a.tf = s.bt_tf[(int64_t)bt * s.A + at];
+    if (s.packed) {
+      a = s.packed[(int64_t)off + at];
+    } else {
+      const Real* c = s.coords + 3 * ((int64_t)off + at);
+      a.x = c[0];
+      a.y = c[1];
+      a.z = c[2];
+      if (TERM == kTermElec)
+        a.q = s.bt_q[(int64_t)bt * s.A + at];
+      else
+        a.tf = s.bt_tf[(int64_t)bt * s.A + at];
+    }
     w.at[lane] = a;
     w.cpd0[lane] = load_cpd(s, bt, nconn, at);
     w.gx[lane] = 0;
@@ -654,36 +709,41 @@ __device__ __forceinline__ void stage_side0(const ScoreArgs<Real>& s,
 // Append the atoms of [start, start + cnt) of block (bt, off) that can reach
 // block b1 to side 1 at j0: an atom farther than r1 + max_dis from b1's
 // centroid is farther than max_dis from every b1 atom, and every term is zero
-// there.  Returns the number of atoms kept.
+// there.  Returns the number of atoms kept; with `heavy`, also the number of
+// heavy atoms among all cnt (a work counter).
 template <typename Real, int TERM = kTermLJLK>
 __device__ __forceinline__ int stage_side1(const ScoreArgs<Real>& s,
                                            Slab<Real>& w, int j0, int slot,
                                            int bt, int off, int start,
                                            int cnt, int nconn, Real cx,
                                            Real cy, Real cz, Real reach2,
-                                           int lane) {
+                                           int lane, int* heavy = nullptr) {
   bool keep = false;
-  Real x = 0, y = 0, z = 0;
+  AtomRec<Real> a;
+  a.x = a.y = a.z = Real(0);
+  a.tf = 0;
   int at = start + lane;
   if (lane < cnt) {
-    const Real* c = s.coords + 3 * ((int64_t)off + at);
-    x = c[0];
-    y = c[1];
-    z = c[2];
-    Real dx = x - cx, dy = y - cy, dz = z - cz;
+    if (s.packed) {
+      a = s.packed[(int64_t)off + at];
+    } else {
+      const Real* c = s.coords + 3 * ((int64_t)off + at);
+      a.x = c[0];
+      a.y = c[1];
+      a.z = c[2];
+      if (TERM == kTermElec)
+        a.q = s.bt_q[(int64_t)bt * s.A + at];
+      else
+        a.tf = s.bt_tf[(int64_t)bt * s.A + at];
+    }
+    Real dx = a.x - cx, dy = a.y - cy, dz = a.z - cz;
     keep = dx * dx + dy * dy + dz * dz < reach2;
   }
+  if (heavy)
+    *heavy = TERM == kTermLJLK ? __popc(__ballot_sync(0xffffffffu, lane < cnt && (a.tf & kTfHeavy))) : 0;
   unsigned km = __ballot_sync(0xffffffffu, keep);
   if (keep) {
     int j = j0 + __popc(km & ((1u << lane) - 1));
-    AtomRec<Real> a;
-    a.x = x;
-    a.y = y;
-    a.z = z;
-    if (TERM == kTermElec)
-      a.q = s.bt_q[(int64_t)bt * s.A + at];
-    else
-      a.tf = s.bt_tf[(int64_t)bt * s.A + at];
     w.at[TILE + j] = a;
     w.cpd1[j] = load_cpd(s, bt, nconn, at);
     w.gidx1[j] = off + at;
@@ -1175,12 +1235,22 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
       r.b1 = wi.y;
       int cand0 = wi.z, cand1 = wi.w;
       r.i1 = r.p * s.B + r.b1;
-      r.bt1 = s.blk_bt[r.i1];
-      if (r.bt1 < 0) continue;
-      r.off1 = s.blk_off[r.i1];
-      r.n1 = s.bt_n_atoms[r.bt1];
-      r.nc1 = s.bt_n_conn[r.bt1];
-      r.lig1 = s.bt_is_ligand[r.bt1];
+      if (s.blk_info) {
+        const int4 bi1 = s.blk_info[r.i1];
+        r.bt1 = bi1.x;
+        if (r.bt1 < 0) continue;
+        r.off1 = bi1.y;
+        r.n1 = bi1.z;
+        r.nc1 = bi1.w & 0xff;
+        r.lig1 = bi1.w >> 8;
+      } else {
+        r.bt1 = s.blk_bt[r.i1];
+        if (r.bt1 < 0) continue;
+        r.off1 = s.blk_off[r.i1];
+        r.n1 = s.bt_n_atoms[r.bt1];
+        r.nc1 = s.bt_n_conn[r.bt1];
+        r.lig1 = s.bt_is_ligand[r.bt1];
+      }
       E3<Real> acc = {0, 0, 0};
       EvalCtx<Real> ec;
       if (TERM == kTermElec)
@@ -1199,8 +1269,8 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
           ec.wt2 = s.dTdV[2 * s.P + r.p];
         }
       }
-      const Real* sph1 = s.spheres + 4 * (int64_t)r.i1;
-      const Real c1x = sph1[0], c1y = sph1[1], c1z = sph1[2], rad1 = sph1[3];
+      const Quad<Real> sph1 = reinterpret_cast<const Quad<Real>*>(s.spheres)[r.i1];
+      const Real c1x = sph1.a, c1y = sph1.b, c1z = sph1.c, rad1 = sph1.d;
       const Real reach1 = rad1 + reach_atoms;
       const Real reach1_2 = reach1 * reach1 * Real(1.0001);
 
@@ -1221,12 +1291,12 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
         if (b2 < cand1) {
           int i2 = r.p * s.B + b2;
           if (s.blk_bt[i2] >= 0) {
-            const Real* s2 = s.spheres + 4 * (int64_t)i2;
-            Real dx = sub_rn(c1x, s2[0]);
-            Real dy = sub_rn(c1y, s2[1]);
-            Real dz = sub_rn(c1z, s2[2]);
+            const Quad<Real> s2 = reinterpret_cast<const Quad<Real>*>(s.spheres)[i2];
+            Real dx = sub_rn(c1x, s2.a);
+            Real dy = sub_rn(c1y, s2.b);
+            Real dz = sub_rn(c1z, s2.c);
             Real d2 = add_rn(add_rn(mul_rn(dx, dx), mul_rn(dy, dy)), mul_rn(dz, dz));
-            Real thr = add_rn(add_rn(rad1, s2[3]), s.reach);
+            Real thr = add_rn(add_rn(rad1, s2.d), s.reach);
             hit = d2 < mul_rn(thr, thr);
           }
           if (s.nbr) s.nbr[(int64_t)r.i1 * s.B + b2] = hit ? 1 : 0;
@@ -1317,20 +1387,31 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
                   w.slot_sph[0][2] = c1z;
                   w.slot_sph[0][3] = rad1;
                 }
-                int h2 = TERM == kTermLJLK ? __popc(__ballot_sync(0xffffffffu,
-                                                                  lane < c2 && (s.bt_tf[(int64_t)r.bt1 * s.A + st2 + lane] & kTfHeavy)))
-                                           : 0;
+                int h2 = 0;
+                m = stage_side1<Real, TERM>(s, w, 0, 0, r.bt1, r.off1, st2, c2, 0, c1x, c1y, c1z, reach1_2, lane,
+                                            &h2);
                 cnt_add(w.counts, 2, (long long)h1 * h2, lane);
-                m = stage_side1<Real, TERM>(s, w, 0, 0, r.bt1, r.off1, st2, c2, 0, c1x, c1y, c1z, reach1_2, lane);
                 ns = 1;
                 score_group<Real, GRAD, BLOCK_PAIR, TERM>(s, w, ec, r, m, ns, lane, acc, pair_o, want_E);
               }
               continue;
             }
             int i2 = r.p * s.B + bb2;
-            int bt2 = s.blk_bt[i2];
-            int off2 = s.blk_off[i2];
-            int n2 = s.bt_n_atoms[bt2];
+            int bt2, off2, n2, nc2_all, lig2;
+            if (s.blk_info) {
+              const int4 bi2 = s.blk_info[i2];
+              bt2 = bi2.x;
+              off2 = bi2.y;
+              n2 = bi2.z;
+              nc2_all = bi2.w & 0xff;
+              lig2 = bi2.w >> 8;
+            } else {
+              bt2 = s.blk_bt[i2];
+              off2 = s.blk_off[i2];
+              n2 = s.bt_n_atoms[bt2];
+              nc2_all = s.bt_n_conn[bt2];
+              lig2 = s.bt_is_ligand[bt2];
+            }
             int nt2 = (n2 + TILE - 1) / TILE;
             unsigned pm = __ballot_sync(0xffffffffu, rp.b2 == bb2);
             int kind = kSlotFar, nc2 = 0, e = 0;
@@ -1340,8 +1421,8 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
               e = __shfl_sync(0xffffffffu, rp.entry, src);
               kind = msep <= 4 ? kSlotStriking : kSlotFar;
             }
-            if (kind == kSlotStriking) nc2 = s.bt_n_conn[bt2];
-            int lig = r.lig1 && s.bt_is_ligand[bt2];
+            if (kind == kSlotStriking) nc2 = nc2_all;
+            int lig = r.lig1 && lig2;
             const Real* s2 = s.spheres + 4 * (int64_t)i2;
             if (ti == 0) {
               cnt_add(w.counts, 0, 1, lane);
@@ -1349,10 +1430,6 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
             }
             for (int tj = 0; tj < nt2; ++tj) {
               int st2 = tj * TILE, c2 = min(TILE, n2 - st2);
-              int h2 = TERM == kTermLJLK ? __popc(__ballot_sync(0xffffffffu,
-                                                                lane < c2 && (s.bt_tf[(int64_t)bt2 * s.A + st2 + lane] & kTfHeavy)))
-                                         : 0;
-              cnt_add(w.counts, 2, (long long)h1 * h2, lane);
               if (m + c2 > M1 || ns == max_slots)
                 score_group<Real, GRAD, BLOCK_PAIR, TERM>(s, w, ec, r, m, ns, lane, acc, pair_o, want_E);
               if (lane == 0) {
@@ -1362,7 +1439,10 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
               }
               if (lane < 4) w.slot_sph[ns][lane] = s2[lane];
               if (kind == kSlotStriking && lane < 16) w.seps[ns][lane] = s.cp_seps[(int64_t)e * 16 + lane];
-              int kept = stage_side1<Real, TERM>(s, w, m, ns, bt2, off2, st2, c2, nc2, c1x, c1y, c1z, reach1_2, lane);
+              int h2 = 0;
+              int kept = stage_side1<Real, TERM>(s, w, m, ns, bt2, off2, st2, c2, nc2, c1x, c1y, c1z, reach1_2, lane,
+                                                 &h2);
+              cnt_add(w.counts, 2, (long long)h1 * h2, lane);
               if (kept > 0) {
                 m += kept;
                 ns += 1;
@@ -1943,6 +2023,8 @@ struct tmol_b200_ljlk_plan {
   double reach;
   int* blk_bt = nullptr;
   int* blk_off = nullptr;
+  int4* blk_info = nullptr;  // pose plans of LJ/LK and elec: {bt, off, n_atoms, n_conn | ligand << 8}
+  void* packed = nullptr;    // and their atoms as staged records [n_atoms], rewritten every call
   int* pose_last = nullptr;
   uint16_t* bt_tf = nullptr;
   int* type_map = nullptr;
@@ -2027,7 +2109,8 @@ void free_plan(tmol_b200_ljlk_plan* pl) {
                   pl->rob,       pl->rot_spheres, pl->row_pairs,  pl->row_items,
                   pl->bt_q,      pl->elec_k,      pl->lkb_sites,   pl->lkb_pol,
                   pl->lkb_npol,  pl->lkb_occ,     pl->lkb_nocc,    pl->lkb_par,
-                  pl->lkb_waters, pl->lkb_dwaters, pl->lkb_nbocc, pl->lkb_active};
+                  pl->lkb_waters, pl->lkb_dwaters, pl->lkb_nbocc, pl->lkb_active,
+                  pl->blk_info,  pl->packed};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t e : pl->prof_events) cudaEventDestroy(e);
@@ -2096,6 +2179,8 @@ ScoreArgs<Real> score_args(tmol_b200_ljlk_plan* pl, const void* coords) {
   s.coords = (const Real*)coords;
   s.blk_bt = pl->blk_bt;
   s.blk_off = pl->blk_off;
+  s.blk_info = pl->blk_info;
+  s.packed = (AtomRec<Real>*)pl->packed;
   s.pose_last = pl->pose_last;
   s.bt_tf = pl->bt_tf;
   s.ljtab = (const LJRecord<Real>*)pl->ljtab;
@@ -2754,6 +2839,11 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
   PCK(dalloc(pl, &pl->cp_minsep, PB * CP_CAP));
   PCK(dalloc(pl, &pl->cp_seps, PB * CP_CAP * 16));
   PCK(dalloc(pl, (unsigned char**)&pl->spheres, PB * 4 * real_bytes));
+  if (!rotamers && term != kTermLKBall) {
+    PCK(dalloc(pl, &pl->blk_info, PB));
+    PCK(dalloc(pl, (unsigned char**)&pl->packed,
+               std::max<int64_t>(in->n_atoms, 1) * (real_bytes == 4 ? sizeof(AtomRec<float>) : sizeof(AtomRec<double>))));
+  }
   if (real_bytes == 4) PCK(dalloc(pl, &pl->sub_spheres, PB * 8));
   PCK(dalloc(pl, &pl->counters, 4));
   PCK(dalloc(pl, &pl->counts, N_COUNTS));
@@ -2829,6 +2919,11 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
   if (PB > 0) {
     plan_blocks_kernel<<<g, 256, 0, st>>>(a);
     PCK(cudaGetLastError());
+    if (pl->blk_info) {
+      plan_block_info_kernel<<<g, 256, 0, st>>>(PB, pl->blk_bt, pl->blk_off, pl->bt_n_atoms, pl->bt_n_conn,
+                                                pl->bt_is_ligand, pl->blk_info);
+      PCK(cudaGetLastError());
+    }
   }
   if (nbt > 0 && term == kTermLJLK) {
     int gh = std::max(1, std::min(((nbt * nt * TILE) + 255) / 256, pl->n_sm * 8));
