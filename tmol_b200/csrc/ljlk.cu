@@ -829,6 +829,7 @@ __device__ TMOL_B200_LJLK_OUTLINE E3<Real> eval_queue(EvalCtx<Real> c, Slab<Real
   const Real dmax = c.max_dis;
   const Real far_dmin = c.max_dis - Real(1.5);
   const Real far_first = far_dmin > Real(4.5) ? far_dmin : Real(4.5);
+  const Real inv_hf = Real(1) / (dmax - far_dmin);
   ElecK<Real> K;
   if (TERM == kTermElec) K = load_elec_k(c.elec_k);
   // one pass over the LJ-only entries, then the heavy-atom ones: only the
@@ -880,13 +881,13 @@ __device__ TMOL_B200_LJLK_OUTLINE E3<Real> eval_queue(EvalCtx<Real> c, Slab<Real
       int tp = t2 * c.ntp + t1;
       LJRecord<Real> lr = c.ljtab[tp];
       Real atr, rep, datr, drep;
-      lj_eval<Real, GRAD>(d, inv_d, lr, dmax, atr, rep, datr, drep);
+      lj_eval<Real, GRAD>(d, inv_d, lr, atr, rep, datr, drep);
       acc.atr += wcp * atr;
       acc.rep += wcp * rep;
       Real dE = c.wt0 * datr + c.wt1 * drep;
       if (heavy) {
         Real lk, dlk;
-        lk_eval<Real, GRAD>(d, inv_d, c.lktab + tp, far_dmin, far_first, dmax, lk, dlk);
+        lk_eval<Real, GRAD>(d, inv_d, c.lktab + tp, far_dmin, far_first, inv_hf, lk, dlk);
         acc.lk += wcp * lk;
         dE += c.wt2 * dlk;
       }

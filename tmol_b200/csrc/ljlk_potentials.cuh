@@ -343,19 +343,21 @@ namespace tmol_b200 {
 // cubic is evaluated for the pair.
 
 template <typename Real>
-struct LJRecord {  // 8 values
+struct alignas(4 * sizeof(Real)) LJRecord {  // 8 values, two groups of four
   Real sigma, eps, d_lin, dmin;
-  Real lin_V, lin_dV;  // 12-6 value and slope at d_lin
-  Real spl_V, spl_dV;  // 12-6 value and slope at dmin (start of the fade)
+  Real inv_h;   // 1 / (max_dis - dmin), the fade-out interval
+  Real spl_V;   // 12-6 value at dmin (start of the fade)
+  Real spl_dp;  // 12-6 slope at dmin times the fade-out interval
+  Real pad;
 };
 
 template <typename Real>
 struct alignas(4 * sizeof(Real)) LKRecord {  // 16 values (13 used), four groups of four
   Real close_dmin, close_dmax;
   Real flat_V;                // both directions at d_min
-  Real pad0;
-  Real cmax_V, cmax_dV;       // both directions at close_dmax
-  Real fmin_V, fmin_dV;       // both directions at far_dmin
+  Real inv_hc;                // 1 / (close_dmax - close_dmin)
+  Real cmax_V, cmax_dp;       // both directions at close_dmax; slope times the close interval
+  Real fmin_V, fmin_dp;       // both directions at far_dmin; slope times the fade-out interval
   Real c_i, r_i, il2_i;       // i desolvated by j: c * exp(-(d-r)^2 * il2) / d^2
   Real pad1;
   Real c_j, r_j, il2_j;       // j desolvated by i
@@ -379,8 +381,14 @@ __device__ __forceinline__ void build_records(const AtomParams<Real>& i,
   lj.eps = q.eps;
   lj.d_lin = q.d_lin;
   lj.dmin = q.dmin;
-  vdw_V_dV(q.d_lin, q.sigma, q.eps, lj.lin_V, lj.lin_dV);
-  vdw_V_dV(q.dmin, q.sigma, q.eps, lj.spl_V, lj.spl_dV);
+  {
+    Real spl_dV;
+    vdw_V_dV(q.dmin, q.sigma, q.eps, lj.spl_V, spl_dV);
+    const Real h = g.max_dis - q.dmin;
+    lj.inv_h = Real(1) / h;
+    lj.spl_dp = spl_dV * h;
+    lj.pad = Real(0);
+  }
 
   bool cc = (i.flags & kCarbonLK) && (j.flags & kCarbonLK);
   LKKnots<Real> k = lk_knots(q.sigma, cc, g.max_dis);
@@ -392,11 +400,12 @@ __device__ __forceinline__ void build_records(const AtomParams<Real>& i,
   desolv_V_dV(k.close_dmax, i.lj_radius, i.lk_dgfree, i.lk_lambda, j.lk_volume, v1, d1);
   desolv_V_dV(k.close_dmax, j.lj_radius, j.lk_dgfree, j.lk_lambda, i.lk_volume, v2, d2);
   lk.cmax_V = v1 + v2;
-  lk.cmax_dV = d1 + d2;
+  lk.inv_hc = Real(1) / (k.close_dmax - k.close_dmin);
+  lk.cmax_dp = (d1 + d2) * (k.close_dmax - k.close_dmin);
   desolv_V_dV(k.far_dmin, i.lj_radius, i.lk_dgfree, i.lk_lambda, j.lk_volume, v1, d1);
   desolv_V_dV(k.far_dmin, j.lj_radius, j.lk_dgfree, j.lk_lambda, i.lk_volume, v2, d2);
   lk.fmin_V = v1 + v2;
-  lk.fmin_dV = d1 + d2;
+  lk.fmin_dp = (d1 + d2) * (k.far_dmax - k.far_dmin);
   const Real pi_pow1p5 = Real(5.56832799683f);
   lk.c_i = -j.lk_volume * i.lk_dgfree / (Real(2) * pi_pow1p5 * i.lk_lambda);
   lk.r_i = i.lj_radius;
@@ -404,19 +413,23 @@ __device__ __forceinline__ void build_records(const AtomParams<Real>& i,
   lk.c_j = -i.lk_volume * j.lk_dgfree / (Real(2) * pi_pow1p5 * j.lk_lambda);
   lk.r_j = j.lj_radius;
   lk.il2_j = Real(1) / (j.lk_lambda * j.lk_lambda);
-  lk.pad0 = lk.pad1 = lk.pad2 = Real(0);
+  lk.pad1 = lk.pad2 = Real(0);
 }
 
 // Unweighted LJ (atr, rep) and, with DERIV, their distance derivatives;
-// inv = 1 / d.
+// inv = 1 / d.  The fade-out cubic runs on t = (d - dmin) / (max_dis - dmin)
+// with the record's stored reciprocal and pre-scaled slope; the linear
+// extension's knot value and slope (clashes only) are the 12-6 form's at
+// d_lin, computed here.
 template <typename Real, bool DERIV>
 __device__ __forceinline__ void lj_eval(Real d, Real inv, const LJRecord<Real>& r,
-                                        Real dmax, Real& atr, Real& rep,
-                                        Real& datr, Real& drep) {
+                                        Real& atr, Real& rep, Real& datr, Real& drep) {
   Real lj, dlj = 0;
   if (d < r.d_lin) {
-    lj = r.lin_V + r.lin_dV * (d - r.d_lin);
-    dlj = r.lin_dV;
+    Real lin_V, lin_dV;
+    vdw_V_dV(r.d_lin, r.sigma, r.eps, lin_V, lin_dV);
+    lj = lin_V + lin_dV * (d - r.d_lin);
+    dlj = lin_dV;
   } else if (d < r.dmin) {
     Real sd = r.sigma * inv;
     Real sd2 = sd * sd;
@@ -425,11 +438,10 @@ __device__ __forceinline__ void lj_eval(Real d, Real inv, const LJRecord<Real>& 
     lj = r.eps * (sd12 - Real(2) * sd6);
     if (DERIV) dlj = r.eps * (Real(12) * (sd6 - sd12)) * inv;
   } else {
-    Real h = dmax - r.dmin;
-    Real t = (d - r.dmin) / h;
-    Real p0 = r.spl_V, dp0 = r.spl_dV * h;
+    Real t = (d - r.dmin) * r.inv_h;
+    Real p0 = r.spl_V, dp0 = r.spl_dp;
     lj = p0 + t * (dp0 + t * (-2 * dp0 - 3 * p0 + t * (dp0 + 2 * p0)));
-    if (DERIV) dlj = (dp0 + t * (-4 * dp0 - 6 * p0 + t * (3 * dp0 + 6 * p0))) / h;
+    if (DERIV) dlj = (dp0 + t * (-4 * dp0 - 6 * p0 + t * (3 * dp0 + 6 * p0))) * r.inv_h;
   }
   if (d < r.sigma) {
     atr = -r.eps;
@@ -446,13 +458,12 @@ __device__ __forceinline__ void lj_eval(Real d, Real inv, const LJRecord<Real>& 
 
 // The fade-out cubic of LK beyond far_dmin from its knot value and slope.
 template <typename Real, bool DERIV>
-__device__ __forceinline__ void lk_far(Real d, Real fmin_V, Real fmin_dV, Real far_dmin, Real far_dmax,
+__device__ __forceinline__ void lk_far(Real d, Real fmin_V, Real fmin_dp, Real far_dmin, Real inv_hf,
                                        Real& V, Real& dV) {
-  Real h = far_dmax - far_dmin;
-  Real t = (d - far_dmin) / h;
-  Real p0 = fmin_V, dp0 = fmin_dV * h;
+  Real t = (d - far_dmin) * inv_hf;
+  Real p0 = fmin_V, dp0 = fmin_dp;
   V = p0 + t * (dp0 + t * (-2 * dp0 - 3 * p0 + t * (dp0 + 2 * p0)));
-  if (DERIV) dV = (dp0 + t * (-4 * dp0 - 6 * p0 + t * (3 * dp0 + 6 * p0))) / h;
+  if (DERIV) dV = (dp0 + t * (-4 * dp0 - 6 * p0 + t * (3 * dp0 + 6 * p0))) * inv_hf;
 }
 
 // Unweighted LK (both directions) and, with DERIV, its distance
@@ -463,25 +474,24 @@ __device__ __forceinline__ void lk_far(Real d, Real fmin_V, Real fmin_dV, Real f
 // group of four record values a region needs is read.
 template <typename Real, bool DERIV>
 __device__ __forceinline__ void lk_eval(Real d, Real inv_d, const LKRecord<Real>* rp,
-                                        Real far_dmin, Real far_first, Real far_dmax, Real& V,
+                                        Real far_dmin, Real far_first, Real inv_hf, Real& V,
                                         Real& dV) {
   const Quad<Real>* q = reinterpret_cast<const Quad<Real>*>(rp);
   dV = 0;
   if (d >= far_first) {
-    const Quad<Real> k = q[1];  // cmax_V, cmax_dV, fmin_V, fmin_dV
-    lk_far<Real, DERIV>(d, k.c, k.d, far_dmin, far_dmax, V, dV);
+    const Quad<Real> k = q[1];  // cmax_V, cmax_dp, fmin_V, fmin_dp
+    lk_far<Real, DERIV>(d, k.c, k.d, far_dmin, inv_hf, V, dV);
     return;
   }
-  const Quad<Real> b = q[0];  // close_dmin, close_dmax, flat_V
+  const Quad<Real> b = q[0];  // close_dmin, close_dmax, flat_V, 1 / close interval
   if (d < b.a) {
     V = b.c;
   } else if (d < b.b) {
     const Quad<Real> k = q[1];
-    Real h = b.b - b.a;
-    Real t = (d - b.a) / h;
-    Real p0 = b.c, p1 = k.a, dp1 = k.b * h;
+    Real t = (d - b.a) * b.d;
+    Real p0 = b.c, p1 = k.a, dp1 = k.b;
     V = p0 + t * (t * (-dp1 - 3 * p0 + 3 * p1 + t * (dp1 + 2 * p0 - 2 * p1)));
-    if (DERIV) dV = (t * (-2 * dp1 - 6 * p0 + 6 * p1 + t * (3 * dp1 + 6 * p0 - 6 * p1))) / h;
+    if (DERIV) dV = (t * (-2 * dp1 - 6 * p0 + 6 * p1 + t * (3 * dp1 + 6 * p0 - 6 * p1))) * b.d;
   } else if (d < far_dmin) {
     const Quad<Real> gi = q[2], gj = q[3];  // (c, r, il2) of each direction
     Real inv_d2 = inv_d * inv_d;
@@ -495,7 +505,7 @@ __device__ __forceinline__ void lk_eval(Real d, Real inv_d, const LKRecord<Real>
     }
   } else {
     const Quad<Real> k = q[1];
-    lk_far<Real, DERIV>(d, k.c, k.d, far_dmin, far_dmax, V, dV);
+    lk_far<Real, DERIV>(d, k.c, k.d, far_dmin, inv_hf, V, dV);
   }
 }
 
