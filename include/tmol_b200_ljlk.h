@@ -153,8 +153,16 @@ int tmol_b200_ljlk_energy_and_gradient(tmol_b200_ljlk_plan* plan,
                                        void* energies, void* dcoords,
                                        void* stream);
 
-/* Work counters of the last forward / energy_and_gradient call, the units of
- * the throughput and roofline figures (synchronises the stream):
+/* Work counting, off by default: while enabled, the whole-pose LJ/LK and
+ * elec scoring calls run a kernel instantiation that also counts its work
+ * (slower: the counters take registers and instructions in its item loop).
+ * The LK-ball and rotamer kernels always count.  No counterpart in the
+ * reference. */
+int tmol_b200_ljlk_plan_set_counting(tmol_b200_ljlk_plan* plan, int enable);
+
+/* Work counters of the last forward / energy_and_gradient call (all zero
+ * when that call ran with counting off), the units of the throughput and
+ * roofline figures (synchronises the stream):
  *   counts[0] neighbouring block pairs (incl. each block with itself)
  *   counts[1] atom pairs they hold (inter: n1 * n2, intra: n (n - 1) / 2)
  *   counts[2] heavy-atom pairs they hold (same rule)

@@ -230,3 +230,35 @@ def test_degenerate_inputs_against_oracle(term):
     nan_block = slice(int(ps.block_coord_offset[2, 3]), int(ps.block_coord_offset[2, 4]))
     assert (c.grad.reshape(ps.n_poses, -1, 3)[2, nan_block] == 0).all()
     clear_plan_cache()
+
+
+def test_work_counters_against_oracle(term):
+    """Work counting is off by default (every counter reads zero); the
+    counting kernel's block-pair, atom-pair and heavy-pair counts equal the
+    oracle's over the same neighbour list, and its results equal those of
+    the kernel without counters."""
+    from tmol_b200.pose.synthetic import synthetic_pose_stack
+
+    sizes = [150, 150, 37, 5, 80]
+    ps = synthetic_pose_stack(sizes, [300 + k for k in range(len(sizes))])
+    args = pose_score_args(ps, term)
+    gargs = [a.to(DEV) if isinstance(a, torch.Tensor) else a for a in args]
+    coords = ps.coords.flatten(0, 1).to(DEV)
+    plan = LJLKPlan(coords, gargs[:-1])
+    w = torch.tensor([1.0, 0.55, 1.0], device=DEV)[:, None].expand(3, len(sizes)).contiguous()
+    E0, g0 = (t.clone() for t in plan.energy_and_gradient(coords, w))
+    assert all(v == 0 for v in plan.last_counts().values())
+    plan.set_counting(True)
+    E1, g1 = (t.clone() for t in plan.energy_and_gradient(coords, w))
+    counts = plan.last_counts()
+    _, nbr = plan.forward(coords)
+    fwd_counts = plan.last_counts()
+    plan.set_counting(False)
+    nbr = nbr.cpu().numpy()
+    ap, hp = oracle64(ps, args).count_pairs(nbr)
+    n_block_pairs = int(sum(numpy.triu(nbr[p] != 0).sum() for p in range(len(sizes))))
+    for c in (counts, fwd_counts):
+        assert (c["block_pairs"], c["atom_pairs"], c["heavy_pairs"]) == (n_block_pairs, ap, hp), c
+        assert 0 < c["heavy_pairs_in_range"] <= c["atom_pairs_in_range"] <= c["atom_pairs"], c
+    E_close(E1.cpu().numpy(), E0.cpu().numpy(), what="energies, counting kernel")
+    g_close_f32(g1.cpu().numpy(), g0.cpu().numpy(), what="gradient, counting kernel")

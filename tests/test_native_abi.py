@@ -54,6 +54,7 @@ def test_status_strings_and_argument_checks():
     assert lib.tmol_b200_ljlk_plan_destroy(None) == 1
     assert lib.tmol_b200_ljlk_forward(None, None, 0, None, None, None) == 1
     assert lib.tmol_b200_ljlk_plan_device_bytes(None) == -1
+    assert lib.tmol_b200_ljlk_plan_set_counting(None, 1) == 1
     # the elec entry points check their arguments the same way
     assert lib.tmol_b200_elec_plan_create(None, 4, None, None, ctypes.byref(out)) == 1
     e = native.ElecInputs()

@@ -942,13 +942,15 @@ __device__ TMOL_B200_LJLK_OUTLINE E3<Real> eval_queue(EvalCtx<Real> c, Slab<Real
   return acc;
 }
 
-template <typename Real, bool GRAD, int TERM = kTermLJLK>
+template <typename Real, bool GRAD, int TERM = kTermLJLK, bool COUNT = true>
 __device__ __forceinline__ void drain_queue(const EvalCtx<Real>& c,
                                             Slab<Real>* wp, int& nl, int& nh,
                                             int lane, E3<Real>& acc) {
   __syncwarp();
-  cnt_add(wp->counts, 3, nl + nh, lane);
-  cnt_add(wp->counts, 4, nh, lane);
+  if (COUNT) {
+    cnt_add(wp->counts, 3, nl + nh, lane);
+    cnt_add(wp->counts, 4, nh, lane);
+  }
   if (nl + nh) {
     E3<Real> e = eval_queue<Real, GRAD, TERM>(c, wp, nl, nh, lane);
     acc.atr += e.atr;
@@ -976,7 +978,7 @@ __device__ __forceinline__ void queue_push(uint16_t* queue, bool in, bool hv,
 // Pairs inside the side-0 tile of c1 atoms (a1 < a2), weights from the
 // intra-block separation table (ljlk_pose_score.impl.hh:115-134; the ligand
 // 3/4 -> 5 rule is already folded into that table and is not applied again).
-template <typename Real, bool GRAD, int TERM = kTermLJLK>
+template <typename Real, bool GRAD, int TERM = kTermLJLK, bool COUNT = true>
 __device__ TMOL_B200_LJLK_OUTLINE E3<Real> intra_tile(EvalCtx<Real> c, Slab<Real>* wp,
                                             int st1, int c1, int lane) {
   Slab<Real>& w = *wp;
@@ -1011,7 +1013,7 @@ __device__ TMOL_B200_LJLK_OUTLINE E3<Real> intra_tile(EvalCtx<Real> c, Slab<Real
       a1 += 1;
     }
   }
-  drain_queue<Real, GRAD, TERM>(c, wp, nl, nh, lane, acc);
+  drain_queue<Real, GRAD, TERM, COUNT>(c, wp, nl, nh, lane, acc);
   return acc;
 }
 
@@ -1020,7 +1022,7 @@ __device__ TMOL_B200_LJLK_OUTLINE E3<Real> intra_tile(EvalCtx<Real> c, Slab<Real
 // walk the packed atoms (32 per chunk); side-0 atoms are broadcast one per
 // step, skipping those farther than r_k + max_dis from every slot block's
 // centroid.  Returns the lane's energy sums.
-template <typename Real, bool GRAD, int TERM = kTermLJLK>
+template <typename Real, bool GRAD, int TERM = kTermLJLK, bool COUNT = true>
 __device__ TMOL_B200_LJLK_OUTLINE E3<Real> screen_slots(EvalCtx<Real> c, Slab<Real>* wp,
                                               int c1, int nc1, int m, int ns,
                                               int lane) {
@@ -1126,7 +1128,7 @@ __device__ TMOL_B200_LJLK_OUTLINE E3<Real> screen_slots(EvalCtx<Real> c, Slab<Re
     const int tot = __shfl_sync(0xffffffffu, incl, 31);
     const int tl = tot & 0xffff, th = tot >> 16;
     if (tl + th == 0) continue;
-    if (nl + nh + tl + th > QCAP) drain_queue<Real, GRAD, TERM>(c, wp, nl, nh, lane, acc);
+    if (nl + nh + tl + th > QCAP) drain_queue<Real, GRAD, TERM, COUNT>(c, wp, nl, nh, lane, acc);
     const int before = incl - cnt;
     int ql = nl + (before & 0xffff);
     int qh = nh + (before >> 16);
@@ -1142,7 +1144,7 @@ __device__ TMOL_B200_LJLK_OUTLINE E3<Real> screen_slots(EvalCtx<Real> c, Slab<Re
     nl += tl;
     nh += th;
   }
-  drain_queue<Real, GRAD, TERM>(c, wp, nl, nh, lane, acc);
+  drain_queue<Real, GRAD, TERM, COUNT>(c, wp, nl, nh, lane, acc);
   return acc;
 }
 
@@ -1172,7 +1174,7 @@ __device__ __forceinline__ void add_pair_energies(Real* out, int64_t stride, int
 }
 
 // Scores the staged slots against side 0 and flushes their gradients.
-template <typename Real, bool GRAD, bool BLOCK_PAIR, int TERM>
+template <typename Real, bool GRAD, bool BLOCK_PAIR, int TERM, bool COUNT>
 __device__ __forceinline__ void score_group(const ScoreArgs<Real>& s,
                                             Slab<Real>& w, const EvalCtx<Real>& c,
                                             const RowInfo& r, int& m, int& ns,
@@ -1180,7 +1182,7 @@ __device__ __forceinline__ void score_group(const ScoreArgs<Real>& s,
                                             int64_t pair_o, bool want_E) {
   __syncwarp();
   if (m > 0) {
-    E3<Real> e = screen_slots<Real, GRAD, TERM>(c, &w, r.c1, r.nc1, m, ns, lane);
+    E3<Real> e = screen_slots<Real, GRAD, TERM, COUNT>(c, &w, r.c1, r.nc1, m, ns, lane);
     if (GRAD) flush_side1(s, w, m, lane);
     if (BLOCK_PAIR) {
       if (want_E) add_pair_energies<Real, TERM>(s.energies, (int64_t)s.P * s.B * s.B, pair_o, e, lane);
@@ -1208,7 +1210,7 @@ __device__ __forceinline__ void score_group(const ScoreArgs<Real>& s,
 #define TMOL_B200_FLOAT_MIN_CTAS 2
 #endif
 
-template <typename Real, bool GRAD, bool BLOCK_PAIR, int TERM>
+template <typename Real, bool GRAD, bool BLOCK_PAIR, int TERM, bool COUNT>
 __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_CTAS : 1)
     score_kernel(ScoreArgs<Real> s, int items_per_ticket) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1340,7 +1342,7 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
         stage_side0<Real, TERM>(s, w, r.bt1, r.off1, r.st1, r.c1, r.nc1, lane);
         ec.pd = s.bt_pd + ((int64_t)r.bt1 * s.A + r.st1) * s.A;
         __syncwarp();
-        int h1 = TERM == kTermLJLK
+        int h1 = COUNT && TERM == kTermLJLK
                      ? __popc(__ballot_sync(0xffffffffu, lane < r.c1 && (w.at[lane].tf & kTfHeavy)))
                      : 0;
         int m = 0, ns = 0;
@@ -1353,7 +1355,7 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
             int bb2 = cand0 + bi * 32 + k;
             if (bb2 == r.b1) {
               // b1 with itself: this tile with itself, then with b1's later tiles
-              score_group<Real, GRAD, BLOCK_PAIR, TERM>(s, w, ec, r, m, ns, lane, acc, pair_o, want_E);
+              score_group<Real, GRAD, BLOCK_PAIR, TERM, COUNT>(s, w, ec, r, m, ns, lane, acc, pair_o, want_E);
               pair_o = (int64_t)r.i1 * s.B + r.b1;
               if (BLOCK_PAIR && GRAD) {
                 ec.wt0 = s.dTdV[pair_o];
@@ -1362,13 +1364,15 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
                   ec.wt2 = s.dTdV[2 * stride + pair_o];
                 }
               }
-              if (ti == 0) {
-                cnt_add(w.counts, 0, 1, lane);
-                cnt_add(w.counts, 1, (long long)r.n1 * (r.n1 - 1) / 2, lane);
+              if (COUNT) {
+                if (ti == 0) {
+                  cnt_add(w.counts, 0, 1, lane);
+                  cnt_add(w.counts, 1, (long long)r.n1 * (r.n1 - 1) / 2, lane);
+                }
+                cnt_add(w.counts, 2, (long long)h1 * (h1 - 1) / 2, lane);
               }
-              cnt_add(w.counts, 2, (long long)h1 * (h1 - 1) / 2, lane);
               {
-                E3<Real> e = intra_tile<Real, GRAD, TERM>(ec, &w, r.st1, r.c1, lane);
+                E3<Real> e = intra_tile<Real, GRAD, TERM, COUNT>(ec, &w, r.st1, r.c1, lane);
                 if (BLOCK_PAIR) {
                   if (want_E) add_pair_energies<Real, TERM>(s.energies, stride, pair_o, e, lane);
                 } else {
@@ -1390,10 +1394,10 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
                 }
                 int h2 = 0;
                 m = stage_side1<Real, TERM>(s, w, 0, 0, r.bt1, r.off1, st2, c2, 0, c1x, c1y, c1z, reach1_2, lane,
-                                            &h2);
-                cnt_add(w.counts, 2, (long long)h1 * h2, lane);
+                                            COUNT ? &h2 : nullptr);
+                if (COUNT) cnt_add(w.counts, 2, (long long)h1 * h2, lane);
                 ns = 1;
-                score_group<Real, GRAD, BLOCK_PAIR, TERM>(s, w, ec, r, m, ns, lane, acc, pair_o, want_E);
+                score_group<Real, GRAD, BLOCK_PAIR, TERM, COUNT>(s, w, ec, r, m, ns, lane, acc, pair_o, want_E);
               }
               continue;
             }
@@ -1425,14 +1429,14 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
             if (kind == kSlotStriking) nc2 = nc2_all;
             int lig = r.lig1 && lig2;
             const Real* s2 = s.spheres + 4 * (int64_t)i2;
-            if (ti == 0) {
+            if (COUNT && ti == 0) {
               cnt_add(w.counts, 0, 1, lane);
               cnt_add(w.counts, 1, (long long)r.n1 * n2, lane);
             }
             for (int tj = 0; tj < nt2; ++tj) {
               int st2 = tj * TILE, c2 = min(TILE, n2 - st2);
               if (m + c2 > M1 || ns == max_slots)
-                score_group<Real, GRAD, BLOCK_PAIR, TERM>(s, w, ec, r, m, ns, lane, acc, pair_o, want_E);
+                score_group<Real, GRAD, BLOCK_PAIR, TERM, COUNT>(s, w, ec, r, m, ns, lane, acc, pair_o, want_E);
               if (lane == 0) {
                 w.slot_kind[ns] = kind;
                 w.slot_nc[ns] = nc2;
@@ -1442,8 +1446,8 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
               if (kind == kSlotStriking && lane < 16) w.seps[ns][lane] = s.cp_seps[(int64_t)e * 16 + lane];
               int h2 = 0;
               int kept = stage_side1<Real, TERM>(s, w, m, ns, bt2, off2, st2, c2, nc2, c1x, c1y, c1z, reach1_2, lane,
-                                                 &h2);
-              cnt_add(w.counts, 2, (long long)h1 * h2, lane);
+                                                 COUNT ? &h2 : nullptr);
+              if (COUNT) cnt_add(w.counts, 2, (long long)h1 * h2, lane);
               if (kept > 0) {
                 m += kept;
                 ns += 1;
@@ -1461,7 +1465,7 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
             }
           }
         }
-        score_group<Real, GRAD, BLOCK_PAIR, TERM>(s, w, ec, r, m, ns, lane, acc, pair_o, want_E);
+        score_group<Real, GRAD, BLOCK_PAIR, TERM, COUNT>(s, w, ec, r, m, ns, lane, acc, pair_o, want_E);
         if (GRAD) flush_side0(s, w, r.off1, r.st1, r.c1, lane);
         __syncwarp();
       }
@@ -1480,7 +1484,7 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
     }
   }
   __syncwarp();
-  if (s.counts && lane < N_COUNTS && w.counts[lane])
+  if (COUNT && s.counts && lane < N_COUNTS && w.counts[lane])
     atomicAdd(&s.counts[lane], w.counts[lane]);
 }
 
@@ -2049,6 +2053,7 @@ struct tmol_b200_ljlk_plan {
   void* spheres = nullptr;
   int* counters = nullptr;  // [0] ticket, [1] status
   unsigned long long* counts = nullptr;  // [N_COUNTS] of the last forward
+  bool counting = false;  // whole-pose LJ/LK and elec kernels fill `counts`
   unsigned char global_params[5 * sizeof(double)];
   // kernel timing: event pairs around each scoring-kernel launch
   bool profiling = false;
@@ -2134,9 +2139,16 @@ template <typename Real, int TERM>
 cudaError_t set_smem_limits_term() {
   const int smem = (int)(MAX_WARPS * sizeof(Slab<Real>));
   const void* kernels[] = {
-      (const void*)score_kernel<Real, false, false, TERM>, (const void*)score_kernel<Real, false, true, TERM>,
-      (const void*)score_kernel<Real, true, false, TERM>,  (const void*)score_kernel<Real, true, true, TERM>,
-      (const void*)rotamer_kernel<Real, false, TERM>,      (const void*)rotamer_kernel<Real, true, TERM>};
+      (const void*)score_kernel<Real, false, false, TERM, false>,
+      (const void*)score_kernel<Real, false, true, TERM, false>,
+      (const void*)score_kernel<Real, true, false, TERM, false>,
+      (const void*)score_kernel<Real, true, true, TERM, false>,
+      (const void*)score_kernel<Real, false, false, TERM, true>,
+      (const void*)score_kernel<Real, false, true, TERM, true>,
+      (const void*)score_kernel<Real, true, false, TERM, true>,
+      (const void*)score_kernel<Real, true, true, TERM, true>,
+      (const void*)rotamer_kernel<Real, false, TERM>,
+      (const void*)rotamer_kernel<Real, true, TERM>};
   for (const void* k : kernels) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
@@ -2244,8 +2256,13 @@ int launch_score(tmol_b200_ljlk_plan* pl, ScoreArgs<Real> s, cudaStream_t st) {
   if (pl->n_work == 0) return TMOL_B200_OK;
   int warps = pl->launch.warps_per_cta;
   size_t smem = warps * sizeof(Slab<Real>);
-  auto kern = pl->term == kTermElec ? score_kernel<Real, GRAD, BLOCK_PAIR, kTermElec>
-                                    : score_kernel<Real, GRAD, BLOCK_PAIR, kTermLJLK>;
+  // the work counters cost registers and instructions in the item loop:
+  // they are compiled into a separate instantiation, used on request
+  auto kern = pl->term == kTermElec
+                  ? (pl->counting ? score_kernel<Real, GRAD, BLOCK_PAIR, kTermElec, true>
+                                  : score_kernel<Real, GRAD, BLOCK_PAIR, kTermElec, false>)
+                  : (pl->counting ? score_kernel<Real, GRAD, BLOCK_PAIR, kTermLJLK, true>
+                                  : score_kernel<Real, GRAD, BLOCK_PAIR, kTermLJLK, false>);
   int R = pl->launch.rows_per_item;
   int n_tickets = (pl->n_work + R - 1) / R;
   int grid = std::max(1, std::min((n_tickets + warps - 1) / warps, pl->n_sm * pl->launch.ctas_per_sm));
@@ -3298,6 +3315,12 @@ int tmol_b200_ljlk_energy_and_gradient(tmol_b200_ljlk_plan* plan,
                                        void* stream) {
   NvtxRange nvtx_range("tmol_b200_ljlk_energy_and_gradient");
   return pose_energy_and_gradient(plan, kTermLJLK, coords, weights, energies, dcoords, stream);
+}
+
+int tmol_b200_ljlk_plan_set_counting(tmol_b200_ljlk_plan* plan, int enable) {
+  if (!plan) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  plan->counting = enable != 0;
+  return TMOL_B200_OK;
 }
 
 int tmol_b200_ljlk_last_counts(tmol_b200_ljlk_plan* plan, void* stream,

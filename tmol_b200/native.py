@@ -178,6 +178,7 @@ SIGNATURES = {
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
     ),
+    "tmol_b200_ljlk_plan_set_counting": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "tmol_b200_ljlk_last_counts": (
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)],

@@ -287,8 +287,14 @@ class LJLKPlan:
 
     COUNT_NAMES = ("block_pairs", "atom_pairs", "heavy_pairs", "atom_pairs_in_range", "heavy_pairs_in_range")
 
+    def set_counting(self, enable=True):
+        """Work counting for the following calls (off by default: the counting
+        kernel is slower).  LK-ball and rotamer plans always count."""
+        native.call("tmol_b200_ljlk_plan_set_counting", self.ptr, int(bool(enable)))
+
     def last_counts(self):
-        """Work counters of the last forward / energy_and_gradient call."""
+        """Work counters of the last forward / energy_and_gradient call (all
+        zero when it ran with counting off)."""
         arr = (ctypes.c_int64 * 5)()
         native.call("tmol_b200_ljlk_last_counts", self.ptr, self._stream(), arr)
         return dict(zip(self.COUNT_NAMES, list(arr)))

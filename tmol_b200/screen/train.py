@@ -238,8 +238,10 @@ def evaluate(mlp, threshold, gap_threshold, sizes, seeds, chi_sd, term, device, 
     plan.set_skip_mask(None)
     cand, n, e, label = block_pair_labels(plan, coords, 64 * P * B)
     E0, g0 = (t.clone() for t in plan.energy_and_gradient(coords, weights))
+    plan.set_counting(True)
     E0b, _ = plan.energy_and_gradient(coords, weights)
     counts0 = plan.last_counts()
+    plan.set_counting(False)
     E64_0, g64_0 = (t.clone() for t in plan64.energy_and_gradient(coords64, w64))
     rows = cand["row"][:n].long()
     b2 = cand["b2"][:n].long()
@@ -264,8 +266,10 @@ def evaluate(mlp, threshold, gap_threshold, sizes, seeds, chi_sd, term, device, 
         plan64.set_skip_mask(mask)
         if update is not None:
             update()
+        plan.set_counting(True)
         E1, g1 = plan.energy_and_gradient(coords, weights)
         counts = plan.last_counts()
+        plan.set_counting(False)
         E64_1, g64_1 = plan64.energy_and_gradient(coords64, w64)
         d64 = E64_1 - E64_0
         tot64 = (d64 * w64).sum(0)
