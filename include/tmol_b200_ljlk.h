@@ -91,7 +91,7 @@ typedef struct {
  *   ctas_per_sm          resident CTAs per SM of the persistent grid
  *   candidates_per_item  candidate blocks b2 per work item (at most 1024)
  *   slots_per_group      neighbouring blocks whose atoms share one pass of
- *                        the warp's 32 lanes (1-8, default 8): how many
+ *                        the warp's 32 lanes (1-12, default 12): how many
  *                        block pairs a warp screens at once */
 typedef struct {
   int32_t rows_per_item;

@@ -575,8 +575,8 @@ __global__ void spheres_kernel(ScoreArgs<Real> s) {
 // each row's.  One screening chunk (32 side-1 atoms x 32 rows) emits at
 // most 1024 entries, so a queue of QCAP >= 1024 takes any chunk whole.
 
-constexpr int M1 = 64;
-constexpr int MAX_SLOTS = 8;
+constexpr int M1 = 96;
+constexpr int MAX_SLOTS = 12;
 // copies of the side-0 force accumulators: lane l adds an entry's force on
 // its side-0 atom into copy l % A_COPIES, so that at most four lanes of a
 // step can meet at one address (shared atomics serialise on a conflict)
@@ -868,8 +868,9 @@ __device__ TMOL_B200_LJLK_OUTLINE E3<Real> eval_queue(EvalCtx<Real> c, Slab<Real
       const AtomRec<Real> p1 = w.at[a1];
       const AtomRec<Real> p2 = w.at[j];
       int t1 = p1.tf & 0xff, t2 = p2.tf & 0xff;
-      // the table row of k's type: the entries of one step mostly share it
-      // (LJ records are symmetric, an LK record's two directions sum alike)
+      // records are symmetric in the two types (LJ by construction, LK as
+      // sums of both directions), so only the upper triangle is read (lower
+      // type first): half the tables' footprint in L1
       Real dx = p1.x - p2.x;
       Real dy = p1.y - p2.y;
       Real dz = p1.z - p2.z;
@@ -878,10 +879,9 @@ __device__ TMOL_B200_LJLK_OUTLINE E3<Real> eval_queue(EvalCtx<Real> c, Slab<Real
       // which never use inv_d, and add no force
       const Real inv_d = inv_sqrt(d2);
       const Real d = d2 > Real(0) ? d2 * inv_d : Real(0);
-      int tp = t2 * c.ntp + t1;
-      LJRecord<Real> lr = c.ljtab[tp];
+      int tp = t1 < t2 ? t1 * c.ntp + t2 : t2 * c.ntp + t1;
       Real atr, rep, datr, drep;
-      lj_eval<Real, GRAD>(d, inv_d, lr, atr, rep, datr, drep);
+      lj_eval<Real, GRAD>(d, inv_d, c.ljtab + tp, atr, rep, datr, drep);
       acc.atr += wcp * atr;
       acc.rep += wcp * rep;
       Real dE = c.wt0 * datr + c.wt1 * drep;

@@ -420,32 +420,36 @@ __device__ __forceinline__ void build_records(const AtomParams<Real>& i,
 // inv = 1 / d.  The fade-out cubic runs on t = (d - dmin) / (max_dis - dmin)
 // with the record's stored reciprocal and pre-scaled slope; the linear
 // extension's knot value and slope (clashes only) are the 12-6 form's at
-// d_lin, computed here.
+// d_lin, computed here.  The record's second group of four is read only in
+// the fade-out region.
 template <typename Real, bool DERIV>
-__device__ __forceinline__ void lj_eval(Real d, Real inv, const LJRecord<Real>& r,
+__device__ __forceinline__ void lj_eval(Real d, Real inv, const LJRecord<Real>* rp,
                                         Real& atr, Real& rep, Real& datr, Real& drep) {
+  const Quad<Real>* q = reinterpret_cast<const Quad<Real>*>(rp);
+  const Quad<Real> r = q[0];  // sigma, eps, d_lin, dmin
   Real lj, dlj = 0;
-  if (d < r.d_lin) {
+  if (d < r.c) {
     Real lin_V, lin_dV;
-    vdw_V_dV(r.d_lin, r.sigma, r.eps, lin_V, lin_dV);
-    lj = lin_V + lin_dV * (d - r.d_lin);
+    vdw_V_dV(r.c, r.a, r.b, lin_V, lin_dV);
+    lj = lin_V + lin_dV * (d - r.c);
     dlj = lin_dV;
-  } else if (d < r.dmin) {
-    Real sd = r.sigma * inv;
+  } else if (d < r.d) {
+    Real sd = r.a * inv;
     Real sd2 = sd * sd;
     Real sd6 = sd2 * sd2 * sd2;
     Real sd12 = sd6 * sd6;
-    lj = r.eps * (sd12 - Real(2) * sd6);
-    if (DERIV) dlj = r.eps * (Real(12) * (sd6 - sd12)) * inv;
+    lj = r.b * (sd12 - Real(2) * sd6);
+    if (DERIV) dlj = r.b * (Real(12) * (sd6 - sd12)) * inv;
   } else {
-    Real t = (d - r.dmin) * r.inv_h;
-    Real p0 = r.spl_V, dp0 = r.spl_dp;
+    const Quad<Real> f = q[1];  // 1 / interval, value, interval-scaled slope
+    Real t = (d - r.d) * f.a;
+    Real p0 = f.b, dp0 = f.c;
     lj = p0 + t * (dp0 + t * (-2 * dp0 - 3 * p0 + t * (dp0 + 2 * p0)));
-    if (DERIV) dlj = (dp0 + t * (-4 * dp0 - 6 * p0 + t * (3 * dp0 + 6 * p0))) * r.inv_h;
+    if (DERIV) dlj = (dp0 + t * (-4 * dp0 - 6 * p0 + t * (3 * dp0 + 6 * p0))) * f.a;
   }
-  if (d < r.sigma) {
-    atr = -r.eps;
-    rep = lj + r.eps;
+  if (d < r.a) {
+    atr = -r.b;
+    rep = lj + r.b;
     datr = 0;
     drep = dlj;
   } else {

@@ -26,7 +26,7 @@ DEFAULT_GRID = {
     "warps_per_cta": (4, 8),
     "ctas_per_sm": (2, 3, 4),
     "candidates_per_item": (32, 64, 128),
-    "slots_per_group": (4, 8),
+    "slots_per_group": (8, 12),
 }
 
 # atoms per block: histogram bin edges of the signature
