@@ -1190,8 +1190,7 @@ def measure_elec(plan, coords, flush, steps):
     def step():
         plan.energy_and_gradient(coords, w, E, dx)
 
-    step()
-    plan.rebalance()
+    plan.balance(step)
     for _ in range(3):
         step()
     torch.cuda.synchronize()
@@ -1271,8 +1270,7 @@ def run_elec(args, world, rank, local):
     if args.launch:
         launch = tuple(int(v) for v in args.launch.split(","))
         plan.set_launch(*launch)
-        step()
-        plan.rebalance()
+        plan.balance(step)
     else:
         from tmol_b200.tune import autotune
 
@@ -1441,8 +1439,7 @@ def measure_lkball(plan, coords, flush, steps):
     def step():
         plan.energy_and_gradient(coords, w, E, dx)
 
-    step()
-    plan.rebalance()
+    plan.balance(step)
     for _ in range(3):
         step()
     torch.cuda.synchronize()
@@ -1526,8 +1523,7 @@ def run_lkball(args, world, rank, local):
     if args.launch:
         launch = tuple(int(v) for v in args.launch.split(","))
         plan.set_launch(*launch)
-        step()
-        plan.rebalance()
+        plan.balance(step)
     else:
         from tmol_b200.tune import autotune
 
@@ -2236,8 +2232,7 @@ def measure_pose_batch(args, workload_name, world, rank, local, steps, extras=Tr
     if args.launch:
         launch_shape = tuple(int(v) for v in args.launch.split(","))
         plan.set_launch(*launch_shape)
-        step()
-        plan.rebalance()
+        plan.balance(step)
     else:
         launch_shape, _ = autotune(plan, step, use_cache=False)
     for _ in range(max(args.warmup, 3)):

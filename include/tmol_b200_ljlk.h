@@ -116,7 +116,14 @@ int tmol_b200_ljlk_plan_destroy(tmol_b200_ljlk_plan* plan);
 /* Reorders the plan's work items longest-first by the cost each item took
  * in the last scoring call (synchronises the stream).  Coordinates change
  * little between calls in minimisation or trajectory replay, so the order
- * keeps the tail of the next launches short. */
+ * keeps the tail of the next launches short.  An item costlier than half a
+ * warp's share of the call is first split over the halves of its candidate
+ * range (up to half again as many items as the plan started with); the
+ * kernels read the item count from plan memory, so a CUDA graph captured
+ * before a rebalance stays valid (one captured before set_launch does
+ * not).  Items that ran in the tail of the measured call look cheaper than
+ * they are beside other heavy items: a second call and rebalance measure
+ * them again in longest-first order. */
 int tmol_b200_ljlk_plan_rebalance(tmol_b200_ljlk_plan* plan, void* stream);
 
 /* Changes the launch shape of an existing plan (autotuning). */

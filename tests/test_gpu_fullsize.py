@@ -104,8 +104,7 @@ def test_uneven_bench_batch_every_pose_perturbed():
     wt = torch.tensor(w, device=DEV, dtype=torch.float32)
     # the benchmark's replayed step: coordinates + N(0, 0.05 A), after the
     # work items were re-ordered by their measured cost
-    plan.energy_and_gradient(base, wt)
-    plan.rebalance()
+    plan.balance(lambda: plan.energy_and_gradient(base, wt))
     gen = torch.Generator(device=DEV).manual_seed(17)
     moved = (base + torch.randn(base.shape, device=DEV, generator=gen) * PERTURB_SD).contiguous()
     E, g = plan.energy_and_gradient(moved, wt)

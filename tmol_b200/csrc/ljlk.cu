@@ -467,7 +467,6 @@ struct ScoreArgs {
   Real reach;
   const int4* work;
   int* item_cost;  // measured cost of each work item (clock cycles / 16)
-  int n_work;
   int P, B, A, C;
   Real* energies;
   int32_t* nbr;
@@ -1223,13 +1222,14 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
   const int max_slots = BLOCK_PAIR ? 1 : s.max_slots;
   const Real reach_atoms = s.g.max_dis;
 
+  const int n_work = s.ticket[2];
   for (;;) {
     int t = 0;
     if (lane == 0) t = atomicAdd(s.ticket, 1);
     t = __shfl_sync(0xffffffffu, t, 0);
     int it0 = t * items_per_ticket;
-    if (it0 >= s.n_work) break;
-    int it1 = min(it0 + items_per_ticket, s.n_work);
+    if (it0 >= n_work) break;
+    int it1 = min(it0 + items_per_ticket, n_work);
     for (int item = it0; item < it1; ++item) {
       long long t_item = clock64();
       int4 wi = s.work[item];
@@ -2050,8 +2050,9 @@ struct tmol_b200_ljlk_plan {
   int4* work = nullptr;
   int* item_cost = nullptr;
   int n_work = 0;
+  int work_cap = 0;  // capacity of work / item_cost
   void* spheres = nullptr;
-  int* counters = nullptr;  // [0] ticket, [1] status
+  int* counters = nullptr;  // [0] ticket, [1] status, [2] work items
   unsigned long long* counts = nullptr;  // [N_COUNTS] of the last forward
   bool counting = false;  // whole-pose LJ/LK and elec kernels fill `counts`
   unsigned char global_params[5 * sizeof(double)];
@@ -2176,12 +2177,17 @@ int build_work(tmol_b200_ljlk_plan* pl, cudaStream_t st) {
   pl->work = nullptr;
   pl->item_cost = nullptr;
   pl->n_work = (int)work.size();
-  CK(cudaMalloc((void**)&pl->work, std::max<size_t>(work.size(), 1) * sizeof(int4)));
-  CK(cudaMalloc((void**)&pl->item_cost, std::max<size_t>(work.size(), 1) * sizeof(int)));
-  CK(cudaMemsetAsync(pl->item_cost, 0, std::max<size_t>(work.size(), 1) * sizeof(int), st));
+  // room for the items plan_rebalance splits off the heaviest ones
+  pl->work_cap = pl->n_work + pl->n_work / 2 + 64;
+  CK(cudaMalloc((void**)&pl->work, (size_t)pl->work_cap * sizeof(int4)));
+  CK(cudaMalloc((void**)&pl->item_cost, (size_t)pl->work_cap * sizeof(int)));
+  CK(cudaMemsetAsync(pl->item_cost, 0, (size_t)pl->work_cap * sizeof(int), st));
   if (!work.empty())
     CK(cudaMemcpyAsync(pl->work, work.data(), work.size() * sizeof(int4),
                        cudaMemcpyHostToDevice, st));
+  // the kernels read the item count from here, so that a graph captured
+  // before a rebalance still walks every item
+  CK(cudaMemcpyAsync(pl->counters + 2, &pl->n_work, sizeof(int), cudaMemcpyHostToDevice, st));
   CK(cudaStreamSynchronize(st));
   return TMOL_B200_OK;
 }
@@ -2232,7 +2238,6 @@ ScoreArgs<Real> score_args(tmol_b200_ljlk_plan* pl, const void* coords) {
   s.reach = (Real)pl->reach;
   s.work = pl->work;
   s.item_cost = pl->item_cost;
-  s.n_work = pl->n_work;
   s.P = pl->P;
   s.B = pl->B;
   s.A = pl->A;
@@ -3062,7 +3067,7 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
     free_plan(pl);
     return rc;
   }
-  pl->device_bytes += (int64_t)std::max(pl->n_work, 1) * (sizeof(int4) + sizeof(int));
+  pl->device_bytes += (int64_t)pl->work_cap * (sizeof(int4) + sizeof(int));
 #undef PCK
   *plan_out = pl;
   return TMOL_B200_OK;
@@ -3399,6 +3404,28 @@ int tmol_b200_ljlk_plan_rebalance(tmol_b200_ljlk_plan* plan, void* stream) {
   CK(cudaMemcpyAsync(work.data(), plan->work, sizeof(int4) * n, cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(cost.data(), plan->item_cost, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  // An item costlier than half a warp's share of the whole call would end
+  // after every other warp: it is split into two items over the halves of
+  // its candidate range (each estimated at half the cost, measured in the
+  // next call), until it is cheap enough, holds one candidate, or the
+  // buffers are full.
+  long long total = 0;
+  for (int c : cost) total += c;
+  const long long warps =
+      std::max(1LL, (long long)plan->n_sm * plan->launch.ctas_per_sm * plan->launch.warps_per_cta);
+  const long long limit = std::max(1LL, total / warps / 2);
+  for (size_t i = 0; i < work.size(); ++i) {
+    while (cost[i] > limit && work[i].w - work[i].z > 1 && (int)work.size() < plan->work_cap) {
+      int4 hi = work[i];
+      const int mid = (work[i].z + work[i].w) / 2;
+      hi.z = mid;
+      work[i].w = mid;
+      cost[i] /= 2;
+      work.push_back(hi);
+      cost.push_back(cost[i]);
+    }
+  }
+  n = (int)work.size();
   std::vector<int> order(n);
   for (int i = 0; i < n; ++i) order[i] = i;
   // longest items first, so that the last items any warp takes are short
@@ -3409,8 +3436,10 @@ int tmol_b200_ljlk_plan_rebalance(tmol_b200_ljlk_plan* plan, void* stream) {
     sorted[i] = work[order[i]];
     sorted_cost[i] = cost[order[i]];
   }
+  plan->n_work = n;
   CK(cudaMemcpyAsync(plan->work, sorted.data(), sizeof(int4) * n, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(plan->item_cost, sorted_cost.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(plan->counters + 2, &plan->n_work, sizeof(int), cudaMemcpyHostToDevice, st));
   CK(cudaStreamSynchronize(st));
   return TMOL_B200_OK;
 }

@@ -1003,13 +1003,14 @@ __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS) lkb_score_kernel(
   tg.dTdV = s.dTdV;
   tg.n = stride;
   const Lkb4<Real> none = {{0, 0, 0, 0}};
+  const int n_work = s.ticket[2];  // the plan's item count (a rebalance may split items)
   for (;;) {
     int t = 0;
     if (lane == 0) t = atomicAdd(s.ticket, 1);
     t = __shfl_sync(0xffffffffu, t, 0);
     const int it0 = t * items_per_ticket;
-    if (it0 >= s.n_work) break;
-    const int it1 = min(it0 + items_per_ticket, s.n_work);
+    if (it0 >= n_work) break;
+    const int it1 = min(it0 + items_per_ticket, n_work);
     for (int item = it0; item < it1; ++item) {
       const long long t_item = clock64();
       const int4 wi = s.work[item];

@@ -211,6 +211,17 @@ class LJLKPlan:
         """Order the work items longest-first by their cost in the last call."""
         native.call("tmol_b200_ljlk_plan_rebalance", self.ptr, self._stream())
 
+    def balance(self, run, passes=2):
+        """Runs `run()` (one scoring call on this plan) and orders the work
+        items longest-first by their measured costs, `passes` times.  An item
+        that ran in the tail of a call, with its SM nearly to itself, measures
+        several times cheaper than it runs beside other heavy items; measured
+        again in longest-first order, every heavy item runs as it will in the
+        calls that follow."""
+        for _ in range(passes):
+            run()
+            self.rebalance()
+
     def device_bytes(self):
         return native.load().tmol_b200_ljlk_plan_device_bytes(self.ptr)
 

@@ -106,15 +106,13 @@ def autotune(plan, run, grid=None, reps=5, use_cache=True, verbose=False):
     if key in cache:
         shape = tuple(cache[key]["shape"])
         plan.set_launch(*shape)
-        run()
-        plan.rebalance()
+        plan.balance(run)
         return shape, time_kernel(plan, run, reps)
     grid = grid or DEFAULT_GRID
     results = []
     for shape in itertools.product(*(grid[k] for k in DEFAULT_GRID)):
         plan.set_launch(*shape)
-        run()
-        plan.rebalance()
+        plan.balance(run)
         run()
         ms = time_kernel(plan, run, reps)
         results.append((ms, shape))
@@ -123,8 +121,7 @@ def autotune(plan, run, grid=None, reps=5, use_cache=True, verbose=False):
     results.sort()
     ms, shape = results[0]
     plan.set_launch(*shape)
-    run()
-    plan.rebalance()
+    plan.balance(run)
     if use_cache:
         cache[key] = {"shape": list(shape), "ms": ms}
         _store_cache(cache)
