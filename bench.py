@@ -2463,6 +2463,7 @@ def measure_lbfgs(local, n_poses=32, n_res=300, iters=200):
     P, A = ps.n_poses, ps.max_n_pose_atoms
     func = make_func(plan, BETA2016_WEIGHTS, P, A)
     x0 = ps.coords.reshape(P, -1)
+    plan.balance(lambda: func(x0))
     E0, _ = func(x0)
     LBFGSArmijo(func, x0, max_iter=3).run()  # warm-up
     opt = LBFGSArmijo(func, x0, max_iter=iters)

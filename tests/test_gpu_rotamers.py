@@ -112,7 +112,9 @@ def test_gradcheck_float64():
     def f(x):
         return ljlk_rotamer_scores(x, *args)[0]
 
-    assert torch.autograd.gradcheck(f, (c,), eps=1e-6, atol=1e-5, rtol=1e-3)
+    # the adjoint sums float64 forces with atomics, whose order (and the drop-in
+    # plan's work order, rebalanced after its first calls) varies between calls
+    assert torch.autograd.gradcheck(f, (c,), eps=1e-6, atol=1e-5, rtol=1e-3, nondet_tol=1e-10)
 
 
 def test_rendered_module_and_plan_kinds():

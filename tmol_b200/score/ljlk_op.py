@@ -31,6 +31,9 @@ class LJLKPlan:
     N_TERMS = 3  # fa_ljatr, fa_ljrep, fa_lk
     ABI = "tmol_b200_ljlk"  # prefix of the scoring entry points
     NAME = "LJ/LK"
+    # scoring calls after which the work items are reordered by their
+    # measured cost (rebalance); the drop-in ops' plans set 2
+    auto_balance = 0
 
     def __init__(self, coords_like, static_args, launch=None, rotamers=False, connectivity=None):
         (
@@ -211,6 +214,12 @@ class LJLKPlan:
         """Order the work items longest-first by their cost in the last call."""
         native.call("tmol_b200_ljlk_plan_rebalance", self.ptr, self._stream())
 
+    def _after_call(self):
+        # the reorder synchronises the stream: never inside a graph capture
+        if self.auto_balance > 0 and not torch.cuda.is_current_stream_capturing():
+            self.auto_balance -= 1
+            self.rebalance()
+
     def balance(self, run, passes=2):
         """Runs `run()` (one scoring call on this plan) and orders the work
         items longest-first by their measured costs, `passes` times.  An item
@@ -254,6 +263,7 @@ class LJLKPlan:
             ctypes.c_void_p(nbr.data_ptr() if nbr is not None else 0),
             self._stream(),
         )
+        self._after_call()
         return energies, nbr
 
     def backward(self, coords, dTdV, block_pair=False, dcoords=None):
@@ -271,6 +281,7 @@ class LJLKPlan:
             ctypes.c_void_p(dcoords.data_ptr()),
             self._stream(),
         )
+        self._after_call()
         return dcoords
 
     def energy_and_gradient(self, coords, weights, energies=None, dcoords=None):
@@ -294,6 +305,7 @@ class LJLKPlan:
             ctypes.c_void_p(dcoords.data_ptr()),
             self._stream(),
         )
+        self._after_call()
         return energies, dcoords
 
     COUNT_NAMES = ("block_pairs", "atom_pairs", "heavy_pairs", "atom_pairs_in_range", "heavy_pairs_in_range")
@@ -465,6 +477,9 @@ def get_plan(coords, static, rotamers=False, plan_class=None):
         _PLAN_CACHE.move_to_end(key)
         return entry[0]
     plan = plan_class(coords, static, rotamers=rotamers)
+    # the drop-in ops run without a tuning step: their plans order the work
+    # items by measured cost after each of their first two calls
+    plan.auto_balance = 2
     # the static tensors are held so that their addresses cannot be reused
     # by other tensors while the key is cached
     _PLAN_CACHE[key] = (plan, [t for t in static if isinstance(t, torch.Tensor)])

@@ -203,6 +203,7 @@ class LKBallPlan(LJLKPlan):
             ctypes.c_void_p(waters.data_ptr()), int(block_pair), ctypes.c_void_p(energies.data_ptr()),
             ctypes.c_void_p(nbr.data_ptr() if nbr is not None else 0), self._stream(),
         )
+        self._after_call()
         return energies, nbr
 
     def backward(self, coords, waters, dTdV, block_pair=False, dcoords=None, dwaters=None):
@@ -220,6 +221,7 @@ class LKBallPlan(LJLKPlan):
             ctypes.c_void_p(waters.data_ptr()), int(block_pair), ctypes.c_void_p(dTdV.data_ptr()),
             ctypes.c_void_p(dcoords.data_ptr()), ctypes.c_void_p(dwaters.data_ptr()), self._stream(),
         )
+        self._after_call()
         return dcoords, dwaters
 
     COUNT_NAMES = ("block_pairs", "polar_occluder_pairs", "bridged_pairs", "pairs_evaluated", "unused")
