@@ -99,6 +99,15 @@ int tmol_b200_elec_forward(tmol_b200_elec_plan* plan, const void* coords, int bl
 int tmol_b200_elec_backward(tmol_b200_elec_plan* plan, const void* coords, int block_pair,
                             const void* dTdV, void* dcoords, void* stream);
 
+/* The elec pose op's autograd pair with a speculative gradient, as
+ * tmol_b200_ljlk_forward_speculative / _backward_speculative (no
+ * counterpart in the reference). */
+int tmol_b200_elec_forward_speculative(tmol_b200_elec_plan* plan, const void* coords,
+                                       void* energies, int32_t* block_neighbors, void* stream);
+int tmol_b200_elec_backward_speculative(tmol_b200_elec_plan* plan, const void* coords,
+                                        const void* dTdV, void* dcoords, int speculated,
+                                        void* stream);
+
 /* Energies [1, P] and weights[0, pose] * dE/dcoords in one pass. */
 int tmol_b200_elec_energy_and_gradient(tmol_b200_elec_plan* plan, const void* coords,
                                        const void* weights, void* energies, void* dcoords,

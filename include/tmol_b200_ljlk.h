@@ -149,6 +149,25 @@ int tmol_b200_ljlk_backward(tmol_b200_ljlk_plan* plan, const void* coords,
                             int block_pair, const void* dTdV, void* dcoords,
                             void* stream);
 
+/* The drop-in op's autograd pair with a speculative gradient (no counterpart
+ * in the reference, whose backward always recomputes).  Whole-pose mode only.
+ * forward_speculative returns what tmol_b200_ljlk_forward returns; once the
+ * plan has seen a backward_speculative call, the same fused pass also takes
+ * the gradient with that call's dTdV and keeps it in the plan.
+ * backward_speculative writes sum_t dTdV_t * dE_t/dcoords into dcoords:
+ * when `speculated` is nonzero (the caller's last forward_speculative on
+ * this plan was the forward of these coordinates) and dTdV equals the
+ * weights that forward used, the kept gradient is copied on the device and
+ * the scoring launch does no work; otherwise the gradient is recomputed.
+ * Minimisation, which calls forward then backward with the same weights
+ * every step, pays one scoring pass per step instead of two.  The calls
+ * keep state in the plan: make them in order on one stream. */
+int tmol_b200_ljlk_forward_speculative(tmol_b200_ljlk_plan* plan, const void* coords,
+                                       void* energies, int32_t* block_neighbors, void* stream);
+int tmol_b200_ljlk_backward_speculative(tmol_b200_ljlk_plan* plan, const void* coords,
+                                        const void* dTdV, void* dcoords, int speculated,
+                                        void* stream);
+
 /* Energies and weighted gradient in one pass, the work of the reference's
  * whole-pose forward when coords require grad (ljlk_pose_score.impl.hh:
  * 953-1119) followed by its elementwise backward (compiled.ops.cpp:164-173):

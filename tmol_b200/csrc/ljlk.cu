@@ -440,6 +440,9 @@ struct AtomRec;
 template <typename Real>
 struct ScoreArgs {
   const Real* coords;
+  // when set and nonzero, the launch has nothing to do: the gradient was
+  // taken from a speculative pass (pose_backward_speculative)
+  const int* done;
   // pose plans of the LJ/LK and elec terms: per block {block type, first
   // atom, atom count, connections | ligand << 8} and every atom as a
   // staged record (coordinates with its type or charge), written by the
@@ -1212,6 +1215,7 @@ __device__ __forceinline__ void score_group(const ScoreArgs<Real>& s,
 template <typename Real, bool GRAD, bool BLOCK_PAIR, int TERM, bool COUNT>
 __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_CTAS : 1)
     score_kernel(ScoreArgs<Real> s, int items_per_ticket) {
+  if (s.done && *s.done) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   Slab<Real>& w = reinterpret_cast<Slab<Real>*>(smem_raw)[warp];
@@ -2055,6 +2059,16 @@ struct tmol_b200_ljlk_plan {
   int* counters = nullptr;  // [0] ticket, [1] status, [2] work items
   unsigned long long* counts = nullptr;  // [N_COUNTS] of the last forward
   bool counting = false;  // whole-pose LJ/LK and elec kernels fill `counts`
+  // speculative gradient of the pose ops: the weights of the last
+  // backward (for the next speculative forward), the weights the last
+  // speculative forward used and the gradient it took with them, and the
+  // device flag a backward sets when its weights match those
+  void* spec_next = nullptr;  // [n_terms, P]
+  void* spec_used = nullptr;  // [n_terms, P]
+  void* spec_g = nullptr;     // [N, 3]
+  int* spec_flag = nullptr;
+  bool spec_ready = false;  // spec_next holds a backward's weights
+  bool spec_taken = false;  // the last speculative forward took a gradient
   unsigned char global_params[5 * sizeof(double)];
   // kernel timing: event pairs around each scoring-kernel launch
   bool profiling = false;
@@ -2117,7 +2131,8 @@ void free_plan(tmol_b200_ljlk_plan* pl) {
                   pl->bt_q,      pl->elec_k,      pl->lkb_sites,   pl->lkb_pol,
                   pl->lkb_npol,  pl->lkb_occ,     pl->lkb_nocc,    pl->lkb_par,
                   pl->lkb_waters, pl->lkb_dwaters, pl->lkb_nbocc, pl->lkb_active,
-                  pl->blk_info,  pl->packed};
+                  pl->blk_info,  pl->packed,      pl->spec_next,   pl->spec_used, pl->spec_g,
+                  pl->spec_flag};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t e : pl->prof_events) cudaEventDestroy(e);
@@ -2321,6 +2336,82 @@ int energy_and_gradient_impl(tmol_b200_ljlk_plan* pl, const void* coords,
   CK(cudaMemsetAsync(energies, 0, (size_t)n_terms(pl->term) * pl->P * sizeof(Real), st));
   CK(cudaMemsetAsync(pl->counts, 0, N_COUNTS * sizeof(unsigned long long), st));
   return launch_score<Real, true, false>(pl, s, st);
+}
+
+// Sets *flag to 1 when a[0, n) and b[0, n) are equal element by element
+// (one block).
+template <typename Real>
+__global__ void __launch_bounds__(1024) spec_match_kernel(const Real* a, const Real* b, int n, int* flag) {
+  int differ = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) differ |= !(a[i] == b[i]);
+  differ = __syncthreads_or(differ);
+  if (threadIdx.x == 0) *flag = differ ? 0 : 1;
+}
+
+// dst[0, n) = src[0, n) when *flag is set.
+template <typename Real>
+__global__ void spec_copy_kernel(const int* flag, const Real* src, Real* dst, int64_t n) {
+  if (!*flag) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] = src[i];
+}
+
+// The pose op's forward that also takes the gradient with the weights of
+// the last backward (kept in the plan), in one fused pass: an autograd
+// backward that follows with the same weights then needs no second pass.
+template <typename Real>
+int forward_speculative_impl(tmol_b200_ljlk_plan* pl, const void* coords, void* energies, int32_t* nbr,
+                             cudaStream_t st) {
+  pl->spec_taken = false;
+  if (!pl->spec_ready) return forward_impl<Real>(pl, coords, 0, energies, nbr, st);
+  pl->spec_taken = true;
+  const size_t w_bytes = (size_t)n_terms(pl->term) * pl->P * sizeof(Real);
+  if (w_bytes) CK(cudaMemcpyAsync(pl->spec_used, pl->spec_next, w_bytes, cudaMemcpyDeviceToDevice, st));
+  ScoreArgs<Real> s = score_args<Real>(pl, coords);
+  s.energies = (Real*)energies;
+  s.nbr = nbr;
+  s.dTdV = (const Real*)pl->spec_used;
+  s.dcoords = (Real*)pl->spec_g;
+  CK(cudaMemsetAsync(energies, 0, (size_t)n_terms(pl->term) * pl->P * sizeof(Real), st));
+  if (nbr) CK(cudaMemsetAsync(nbr, 0, (size_t)pl->P * pl->B * pl->B * sizeof(int32_t), st));
+  CK(cudaMemsetAsync(pl->spec_g, 0, (size_t)pl->N * 3 * sizeof(Real), st));
+  CK(cudaMemsetAsync(pl->counts, 0, N_COUNTS * sizeof(unsigned long long), st));
+  return launch_score<Real, true, false>(pl, s, st);
+}
+
+// The pose op's backward: when `speculated` (the plan's last speculative
+// forward was the forward of these coordinates, and took a gradient) and
+// dTdV equals the weights that forward used, the gradient is that pass's
+// (copied on the device; the scoring launch exits at once); otherwise it
+// is recomputed.  Either way dTdV becomes the weights of the next
+// speculative forward.  No host synchronisation.
+template <typename Real>
+int backward_speculative_impl(tmol_b200_ljlk_plan* pl, const void* coords, const void* dTdV, void* dcoords,
+                              int speculated, cudaStream_t st) {
+  const int n_w = n_terms(pl->term) * pl->P;
+  const int64_t n_g = (int64_t)pl->N * 3;
+  if (speculated && pl->spec_taken && n_w > 0) {
+    spec_match_kernel<Real><<<1, 1024, 0, st>>>((const Real*)dTdV, (const Real*)pl->spec_used, n_w, pl->spec_flag);
+    CK(cudaGetLastError());
+  } else {
+    CK(cudaMemsetAsync(pl->spec_flag, 0, sizeof(int), st));
+  }
+  CK(cudaMemsetAsync(dcoords, 0, (size_t)n_g * sizeof(Real), st));
+  if (n_g > 0) {
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n_g + 255) / 256, (int64_t)pl->n_sm * 8));
+    spec_copy_kernel<Real><<<grid, 256, 0, st>>>(pl->spec_flag, (const Real*)pl->spec_g, (Real*)dcoords, n_g);
+    CK(cudaGetLastError());
+  }
+  ScoreArgs<Real> s = score_args<Real>(pl, coords);
+  s.dTdV = (const Real*)dTdV;
+  s.dcoords = (Real*)dcoords;
+  s.counts = nullptr;
+  s.done = pl->spec_flag;
+  const int rc = launch_score<Real, true, false>(pl, s, st);
+  if (rc != TMOL_B200_OK) return rc;
+  if (n_w > 0) CK(cudaMemcpyAsync(pl->spec_next, dTdV, (size_t)n_w * sizeof(Real), cudaMemcpyDeviceToDevice, st));
+  pl->spec_ready = true;
+  return TMOL_B200_OK;
 }
 
 RotArgs rot_args(tmol_b200_ljlk_plan* pl) {
@@ -2866,6 +2957,10 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
     PCK(dalloc(pl, &pl->blk_info, PB));
     PCK(dalloc(pl, (unsigned char**)&pl->packed,
                std::max<int64_t>(in->n_atoms, 1) * (real_bytes == 4 ? sizeof(AtomRec<float>) : sizeof(AtomRec<double>))));
+    PCK(dalloc(pl, (unsigned char**)&pl->spec_next, (size_t)n_terms(term) * std::max(P, 1) * real_bytes));
+    PCK(dalloc(pl, (unsigned char**)&pl->spec_used, (size_t)n_terms(term) * std::max(P, 1) * real_bytes));
+    PCK(dalloc(pl, (unsigned char**)&pl->spec_g, (size_t)std::max<int64_t>(in->n_atoms, 1) * 3 * real_bytes));
+    PCK(dalloc(pl, &pl->spec_flag, 1));
   }
   if (real_bytes == 4) PCK(dalloc(pl, &pl->sub_spheres, PB * 8));
   PCK(dalloc(pl, &pl->counters, 4));
@@ -3182,6 +3277,24 @@ int pose_backward(tmol_b200_ljlk_plan* plan, int term, const void* coords, int b
   return backward_impl<double>(plan, coords, block_pair, dTdV, dcoords, st);
 }
 
+int pose_forward_speculative(tmol_b200_ljlk_plan* plan, int term, const void* coords, void* energies,
+                             int32_t* block_neighbors, void* stream) {
+  if (!pose_plan_of(plan, term) || !plan->spec_g || !energies || (!coords && plan->N > 0))
+    return TMOL_B200_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->real_bytes == 4) return forward_speculative_impl<float>(plan, coords, energies, block_neighbors, st);
+  return forward_speculative_impl<double>(plan, coords, energies, block_neighbors, st);
+}
+
+int pose_backward_speculative(tmol_b200_ljlk_plan* plan, int term, const void* coords, const void* dTdV,
+                              void* dcoords, int speculated, void* stream) {
+  if (!pose_plan_of(plan, term) || !plan->spec_g || !dTdV || !dcoords || (!coords && plan->N > 0))
+    return TMOL_B200_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->real_bytes == 4) return backward_speculative_impl<float>(plan, coords, dTdV, dcoords, speculated, st);
+  return backward_speculative_impl<double>(plan, coords, dTdV, dcoords, speculated, st);
+}
+
 int pose_energy_and_gradient(tmol_b200_ljlk_plan* plan, int term, const void* coords, const void* weights,
                              void* energies, void* dcoords, void* stream) {
   if (!pose_plan_of(plan, term) || !weights || !energies || !dcoords || (!coords && plan->N > 0))
@@ -3312,6 +3425,19 @@ int tmol_b200_ljlk_backward(tmol_b200_ljlk_plan* plan, const void* coords,
                             void* stream) {
   NvtxRange nvtx_range("tmol_b200_ljlk_backward");
   return pose_backward(plan, kTermLJLK, coords, block_pair, dTdV, dcoords, stream);
+}
+
+int tmol_b200_ljlk_forward_speculative(tmol_b200_ljlk_plan* plan, const void* coords,
+                                       void* energies, int32_t* block_neighbors, void* stream) {
+  NvtxRange nvtx_range("tmol_b200_ljlk_forward_speculative");
+  return pose_forward_speculative(plan, kTermLJLK, coords, energies, block_neighbors, stream);
+}
+
+int tmol_b200_ljlk_backward_speculative(tmol_b200_ljlk_plan* plan, const void* coords,
+                                        const void* dTdV, void* dcoords, int speculated,
+                                        void* stream) {
+  NvtxRange nvtx_range("tmol_b200_ljlk_backward_speculative");
+  return pose_backward_speculative(plan, kTermLJLK, coords, dTdV, dcoords, speculated, stream);
 }
 
 int tmol_b200_ljlk_energy_and_gradient(tmol_b200_ljlk_plan* plan,
@@ -3542,6 +3668,19 @@ int tmol_b200_elec_backward(tmol_b200_elec_plan* plan, const void* coords, int b
                             const void* dTdV, void* dcoords, void* stream) {
   NvtxRange nvtx_range("tmol_b200_elec_backward");
   return pose_backward(plan, kTermElec, coords, block_pair, dTdV, dcoords, stream);
+}
+
+int tmol_b200_elec_forward_speculative(tmol_b200_elec_plan* plan, const void* coords,
+                                       void* energies, int32_t* block_neighbors, void* stream) {
+  NvtxRange nvtx_range("tmol_b200_elec_forward_speculative");
+  return pose_forward_speculative(plan, kTermElec, coords, energies, block_neighbors, stream);
+}
+
+int tmol_b200_elec_backward_speculative(tmol_b200_elec_plan* plan, const void* coords,
+                                        const void* dTdV, void* dcoords, int speculated,
+                                        void* stream) {
+  NvtxRange nvtx_range("tmol_b200_elec_backward_speculative");
+  return pose_backward_speculative(plan, kTermElec, coords, dTdV, dcoords, speculated, stream);
 }
 
 int tmol_b200_elec_energy_and_gradient(tmol_b200_elec_plan* plan, const void* coords,

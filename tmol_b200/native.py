@@ -174,6 +174,14 @@ SIGNATURES = {
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
     ),
+    "tmol_b200_ljlk_forward_speculative": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    ),
+    "tmol_b200_ljlk_backward_speculative": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p],
+    ),
     "tmol_b200_ljlk_energy_and_gradient": (
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
@@ -231,6 +239,8 @@ SIGNATURES = {
     "tmol_b200_elec_forward": (ctypes.c_int, [_V, _V, ctypes.c_int, _V, _V, _V]),
     "tmol_b200_elec_backward": (ctypes.c_int, [_V, _V, ctypes.c_int, _V, _V, _V]),
     "tmol_b200_elec_energy_and_gradient": (ctypes.c_int, [_V, _V, _V, _V, _V, _V]),
+    "tmol_b200_elec_forward_speculative": (ctypes.c_int, [_V, _V, _V, _V, _V]),
+    "tmol_b200_elec_backward_speculative": (ctypes.c_int, [_V, _V, _V, _V, ctypes.c_int, _V]),
     "tmol_b200_elec_rotamer_count": (
         ctypes.c_int, [_V, _V, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64), _V]
     ),

@@ -34,6 +34,9 @@ class LJLKPlan:
     # scoring calls after which the work items are reordered by their
     # measured cost (rebalance); the drop-in ops' plans set 2
     auto_balance = 0
+    # whole-pose autograd through forward_speculative / backward_speculative
+    SPECULATIVE = True
+    spec_gen = 0  # count of speculative forwards on this plan
 
     def __init__(self, coords_like, static_args, launch=None, rotamers=False, connectivity=None):
         (
@@ -284,6 +287,50 @@ class LJLKPlan:
         self._after_call()
         return dcoords
 
+    def forward_speculative(self, coords, want_neighbors=True):
+        """Whole-pose energies (and neighbour matrix) for an autograd forward
+        whose backward will follow: once the plan has seen a
+        backward_speculative call, the same pass also takes the gradient with
+        that call's weights and keeps it.  Returns (energies, nbr, gen), gen
+        identifying this forward for backward_speculative."""
+        self._check_coords(coords)
+        coords = coords.contiguous()
+        P, B = self.n_poses, self.max_n_blocks
+        energies = torch.empty((self.N_TERMS, P), dtype=self.dtype, device=self.device)
+        nbr = torch.empty((P, B, B), dtype=torch.int32, device=self.device) if want_neighbors else None
+        native.call(
+            f"{self.ABI}_forward_speculative",
+            self.ptr,
+            ctypes.c_void_p(coords.data_ptr()),
+            ctypes.c_void_p(energies.data_ptr()),
+            ctypes.c_void_p(nbr.data_ptr() if nbr is not None else 0),
+            self._stream(),
+        )
+        self.spec_gen += 1
+        self._after_call()
+        return energies, nbr, self.spec_gen
+
+    def backward_speculative(self, coords, dTdV, gen):
+        """sum_t dTdV_t * dE_t/dcoords for the forward `gen` returned: the
+        gradient that forward kept when it is still the plan's latest and
+        its weights equal dTdV (decided on the device), else a recomputed
+        one."""
+        self._check_coords(coords)
+        coords = coords.contiguous()
+        dTdV = dTdV.to(self.dtype).contiguous()
+        dcoords = torch.empty_like(coords)
+        native.call(
+            f"{self.ABI}_backward_speculative",
+            self.ptr,
+            ctypes.c_void_p(coords.data_ptr()),
+            ctypes.c_void_p(dTdV.data_ptr()),
+            ctypes.c_void_p(dcoords.data_ptr()),
+            int(gen is not None and gen == self.spec_gen),
+            self._stream(),
+        )
+        self._after_call()
+        return dcoords
+
     def energy_and_gradient(self, coords, weights, energies=None, dcoords=None):
         """Energies [n_terms, P] and sum_t weights[t, pose] * dE_t/dcoords in
         one pass."""
@@ -435,9 +482,19 @@ class LJLKPlan:
 
 
 class _ScoreFn(torch.autograd.Function):
+    """Whole-pose calls whose coordinates need a gradient go through the
+    speculative pair: from the second call on, the forward's fused pass also
+    takes the gradient with the previous backward's weights, and a backward
+    with the same weights reuses it (one scoring pass per forward + backward
+    instead of two)."""
+
     @staticmethod
     def forward(ctx, coords, plan, block_pair, want_neighbors):
-        E, nbr = plan.forward(coords, block_pair, want_neighbors)
+        ctx.spec_gen = None
+        if not block_pair and plan.SPECULATIVE and ctx.needs_input_grad[0]:
+            E, nbr, ctx.spec_gen = plan.forward_speculative(coords, want_neighbors)
+        else:
+            E, nbr = plan.forward(coords, block_pair, want_neighbors)
         ctx.plan = plan
         ctx.block_pair = block_pair
         ctx.save_for_backward(coords)
@@ -451,7 +508,10 @@ class _ScoreFn(torch.autograd.Function):
         (coords,) = ctx.saved_tensors
         if dE is None:
             return None, None, None, None
-        dx = ctx.plan.backward(coords, dE, ctx.block_pair)
+        if ctx.block_pair or not ctx.plan.SPECULATIVE:
+            dx = ctx.plan.backward(coords, dE, ctx.block_pair)
+        else:
+            dx = ctx.plan.backward_speculative(coords, dE, ctx.spec_gen)
         return dx, None, None, None
 
 

@@ -42,6 +42,7 @@ class LKBallPlan(LJLKPlan):
 
     N_TERMS = 4  # lk_ball_iso, lk_ball, lk_bridge, lk_bridge_uncpl
     ABI = "tmol_b200_lkball"
+    SPECULATIVE = False  # its ops have their own autograd functions
     NAME = "LK-ball"
 
     def __init__(self, coords_like, water_static=None, score_static=None, launch=None, rotamers=False,
