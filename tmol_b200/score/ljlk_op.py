@@ -491,7 +491,13 @@ class _ScoreFn(torch.autograd.Function):
     @staticmethod
     def forward(ctx, coords, plan, block_pair, want_neighbors):
         ctx.spec_gen = None
-        if not block_pair and plan.SPECULATIVE and ctx.needs_input_grad[0]:
+        # not inside a graph capture: the choice between a kept and a fresh
+        # gradient uses host-side state of the plan at call time
+        ctx.speculate = (
+            not block_pair and plan.SPECULATIVE and ctx.needs_input_grad[0]
+            and coords.is_cuda and not torch.cuda.is_current_stream_capturing()
+        )
+        if ctx.speculate:
             E, nbr, ctx.spec_gen = plan.forward_speculative(coords, want_neighbors)
         else:
             E, nbr = plan.forward(coords, block_pair, want_neighbors)
@@ -508,7 +514,7 @@ class _ScoreFn(torch.autograd.Function):
         (coords,) = ctx.saved_tensors
         if dE is None:
             return None, None, None, None
-        if ctx.block_pair or not ctx.plan.SPECULATIVE:
+        if not ctx.speculate or torch.cuda.is_current_stream_capturing():
             dx = ctx.plan.backward(coords, dE, ctx.block_pair)
         else:
             dx = ctx.plan.backward_speculative(coords, dE, ctx.spec_gen)
