@@ -87,8 +87,12 @@ typedef struct {
 /* Launch shape of the scoring kernel; zeros select the built-in defaults.
  * A work item is (pose, block b1, a range of later blocks b2 >= b1).
  *   rows_per_item        work items a warp takes per atomic ticket
- *   warps_per_cta        warps per CTA (at most 8); every warp works alone
+ *   warps_per_cta        warps per CTA (at most 16; 8 for float64 plans and
+ *                        the rotamer and LK-ball kernels); every warp works
+ *                        alone
  *   ctas_per_sm          resident CTAs per SM of the persistent grid
+ *                        (defaults: 16 x 1 for float pose plans of LJ/LK
+ *                        and elec, else 8 x 2)
  *   candidates_per_item  candidate blocks b2 per work item (at most 1024)
  *   slots_per_group      neighbouring blocks whose atoms share one pass of
  *                        the warp's 32 lanes (1-12, default 12): how many

@@ -52,7 +52,7 @@ constexpr int TILE = 32;
 constexpr int MAX_CONN = 4;
 constexpr int CP_CAP = 16;
 constexpr int MAX_ROWS_PER_ITEM = 64;
-constexpr int MAX_WARPS = 8;
+constexpr int MAX_WARPS = 16;
 
 // The energy term a plan scores: LJ + LK (fa_ljatr, fa_ljrep, fa_lk) or
 // elec (fa_elec).  Both share the neighbour detection, count-pair tables,
@@ -1212,8 +1212,10 @@ __device__ __forceinline__ void score_group(const ScoreArgs<Real>& s,
 #define TMOL_B200_FLOAT_MIN_CTAS 2
 #endif
 
+// float: up to 16 warps per CTA (one CTA of 16 warps per SM measured best),
+// 128 registers; double: up to 8 warps
 template <typename Real, bool GRAD, bool BLOCK_PAIR, int TERM, bool COUNT>
-__global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_CTAS : 1)
+__global__ void __launch_bounds__(sizeof(Real) == 4 ? 512 : 256, 1)
     score_kernel(ScoreArgs<Real> s, int items_per_ticket) {
   if (s.done && *s.done) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -2153,7 +2155,7 @@ void default_launch(tmol_b200_ljlk_launch& l) {
 
 template <typename Real, int TERM>
 cudaError_t set_smem_limits_term() {
-  const int smem = (int)(MAX_WARPS * sizeof(Slab<Real>));
+  const int smem = (int)std::min<size_t>(MAX_WARPS * sizeof(Slab<Real>), 227 * 1024);
   const void* kernels[] = {
       (const void*)score_kernel<Real, false, false, TERM, false>,
       (const void*)score_kernel<Real, false, true, TERM, false>,
@@ -2275,6 +2277,7 @@ int launch_score(tmol_b200_ljlk_plan* pl, ScoreArgs<Real> s, cudaStream_t st) {
   CK(cudaMemsetAsync(pl->counters, 0, sizeof(int), st));
   if (pl->n_work == 0) return TMOL_B200_OK;
   int warps = pl->launch.warps_per_cta;
+  if (sizeof(Real) == 8) warps = std::min(warps, 8);  // the float64 kernel: at most 256 threads
   size_t smem = warps * sizeof(Slab<Real>);
   // the work counters cost registers and instructions in the item loop:
   // they are compiled into a separate instantiation, used on request
@@ -2504,7 +2507,7 @@ int rotamer_score_impl(tmol_b200_ljlk_plan* pl, const void* coords, const int32_
     CK(cudaGetLastError());
   }
   CK(cudaMemsetAsync(pl->counters, 0, sizeof(int), st));
-  const int warps = pl->launch.warps_per_cta;
+  const int warps = std::min(pl->launch.warps_per_cta, 8);  // a kernel of at most 256 threads
   const size_t smem = warps * sizeof(Slab<Real>);
   int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n_items + warps - 1) / warps,
                                                          (int64_t)pl->n_sm * pl->launch.ctas_per_sm));
@@ -2595,7 +2598,7 @@ int lkb_score_impl(tmol_b200_ljlk_plan* pl, const void* coords, const void* wate
   CK(cudaGetLastError());
   CK(cudaMemsetAsync(pl->counters, 0, sizeof(int), st));
   if (pl->n_work == 0) return TMOL_B200_OK;
-  const int warps = pl->launch.warps_per_cta;
+  const int warps = std::min(pl->launch.warps_per_cta, 8);  // a kernel of at most 256 threads
   const int R = pl->launch.rows_per_item;
   const int n_tickets = (pl->n_work + R - 1) / R;
   const int grid = std::max(1, std::min((n_tickets + warps - 1) / warps, pl->n_sm * pl->launch.ctas_per_sm));
@@ -2639,7 +2642,7 @@ int lkb_rotamer_score_impl(tmol_b200_ljlk_plan* pl, const void* coords, const vo
     CK(cudaGetLastError());
   }
   CK(cudaMemsetAsync(pl->counters, 0, sizeof(int), st));
-  const int warps = pl->launch.warps_per_cta;
+  const int warps = std::min(pl->launch.warps_per_cta, 8);  // a kernel of at most 256 threads
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n_items + warps - 1) / warps,
                                                                (int64_t)pl->n_sm * pl->launch.ctas_per_sm));
   lkb_rotamer_kernel<Real, GRAD><<<grid, 32 * warps, 0, st>>>(s, k, ra, (const Real*)pl->rot_spheres);
@@ -2923,6 +2926,13 @@ int create_plan(const tmol_b200_ljlk_inputs* in, int real_bytes,
   pl->N = in->n_atoms;
   pl->reach = in->max_dis;
   pl->launch = launch ? *launch : tmol_b200_ljlk_launch{0, 0, 0, 0};
+  // float pose plans of LJ/LK and elec: one CTA of 16 warps per SM unless
+  // the caller chose
+  if (real_bytes == 4 && !rotamers && term != kTermLKBall && pl->launch.warps_per_cta <= 0 &&
+      pl->launch.ctas_per_sm <= 0) {
+    pl->launch.warps_per_cta = 16;
+    pl->launch.ctas_per_sm = 1;
+  }
   default_launch(pl->launch);
   int dev = 0;
   int rc = TMOL_B200_OK;

@@ -23,11 +23,22 @@ import torch
 
 DEFAULT_GRID = {
     "rows_per_item": (1, 2),
-    "warps_per_cta": (4, 8),
-    "ctas_per_sm": (2, 3, 4),
+    # (warps per CTA, CTAs per SM): 16 warps per SM, the register limit at
+    # 128 registers a thread (the LK-ball and rotamer kernels take at most
+    # 8 warps per CTA)
+    "cta_shape": ((4, 4), (8, 2), (16, 1)),
     "candidates_per_item": (32, 64, 128),
     "slots_per_group": (8, 12),
 }
+
+
+def launch_shapes(grid):
+    """(items per ticket, warps per CTA, CTAs per SM, candidates per item,
+    slots per group) of every grid point."""
+    for rows, (warps, ctas), cands, slots in itertools.product(
+        grid["rows_per_item"], grid["cta_shape"], grid["candidates_per_item"], grid["slots_per_group"]
+    ):
+        yield (rows, warps, ctas, cands, slots)
 
 # atoms per block: histogram bin edges of the signature
 SIZE_BINS = (8, 16, 24, 32)
@@ -110,7 +121,7 @@ def autotune(plan, run, grid=None, reps=5, use_cache=True, verbose=False):
         return shape, time_kernel(plan, run, reps)
     grid = grid or DEFAULT_GRID
     results = []
-    for shape in itertools.product(*(grid[k] for k in DEFAULT_GRID)):
+    for shape in launch_shapes(grid):
         plan.set_launch(*shape)
         plan.balance(run)
         run()
