@@ -141,6 +141,17 @@ int tmol_b200_lkball_backward(tmol_b200_lkball_plan* plan, const void* coords, c
                               int block_pair, const void* dTdV, void* dcoords, void* dwaters,
                               void* stream);
 
+/* lk_ball_pose_score's forward / backward pair with a speculative gradient
+ * (whole-pose mode; no counterpart in the reference, whose backward always
+ * recomputes): as tmol_b200_ljlk_forward_speculative /
+ * _backward_speculative, the kept gradient being both the coordinates'
+ * direct part and the waters' part. */
+int tmol_b200_lkball_forward_speculative(tmol_b200_lkball_plan* plan, const void* coords, const void* waters,
+                                         void* energies, int32_t* block_neighbors, void* stream);
+int tmol_b200_lkball_backward_speculative(tmol_b200_lkball_plan* plan, const void* coords, const void* waters,
+                                          const void* dTdV, void* dcoords, void* dwaters, int speculated,
+                                          void* stream);
+
 /* Whole-pose energies and gradient in one call (a plan with both parts):
  * the waters, the four energies [4, P] (overwritten) and dcoords [n_atoms,
  * 3] (overwritten) = d(sum_t,p weights[t, p] * E[t, p]) / dcoords through

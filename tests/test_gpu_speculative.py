@@ -123,3 +123,40 @@ def test_elec_dropin_speculates_correctly():
         E_close(E.detach().cpu().numpy(), E0.cpu().numpy(), what="elec energies")
         g_close_f32(c.grad.cpu().numpy(), g0.cpu().numpy(), what="elec gradient")
     clear_plan_cache()
+
+
+def test_lkball_dropin_speculates_correctly():
+    """gen_pose_waters + lk_ball_pose_score with autograd, call after call:
+    the gradient through the waters equals the plan's one-call energy and
+    gradient, with repeated weights (the speculation's hits), changed
+    weights and moved coordinates."""
+    from tmol_b200.score.lkball_energy_term import LKBallEnergyTerm, score_args, water_gen_args
+    from tmol_b200.score.lkball_op import LKBallPlan, gen_pose_waters, lk_ball_pose_score
+
+    lt = LKBallEnergyTerm()
+    ps = synthetic_pose_stack([70, 30, 45], [61, 62, 63], extra_chi_sd=20.0)
+
+    def dev(args):
+        return [a.to(DEV) if isinstance(a, torch.Tensor) else a for a in args]
+
+    wa, sa = dev(water_gen_args(ps, lt)), dev(score_args(ps, lt, None)[:-2])
+    coords = ps.coords.flatten(0, 1).to(DEV)
+    moved = coords + 0.05 * torch.randn(coords.shape, device=DEV, generator=torch.Generator(device=DEV).manual_seed(9))
+    w1 = torch.tensor([1.0, 0.9, 0.8, 0.7], device=DEV)[:, None].expand(4, ps.n_poses).contiguous()
+    w2 = torch.rand((4, ps.n_poses), device=DEV, generator=torch.Generator(device=DEV).manual_seed(10))
+    ref = {}
+    for name, x in (("start", coords), ("moved", moved)):
+        for wn, w in (("w1", w1), ("w2", w2)):
+            E, g = LKBallPlan(x, water_static=wa, score_static=sa).energy_and_gradient(x, w)
+            ref[name, wn] = (E.cpu().numpy(), g.cpu().numpy())
+    clear_plan_cache()
+    for name, wn in [("start", "w1")] * 3 + [("moved", "w1"), ("moved", "w2"), ("start", "w2"), ("start", "w1")]:
+        x = coords if name == "start" else moved
+        w = w1 if wn == "w1" else w2
+        c = x.clone().requires_grad_(True)
+        W = gen_pose_waters(c, *wa)
+        E, _ = lk_ball_pose_score(c, *sa, W, False)
+        (E * w).sum().backward()
+        E_close(E.detach().cpu().numpy(), ref[name, wn][0], what=f"LK-ball energies, {name} {wn}")
+        g_close_f32(c.grad.cpu().numpy(), ref[name, wn][1], what=f"LK-ball gradient, {name} {wn}")
+    clear_plan_cache()

@@ -2068,6 +2068,7 @@ struct tmol_b200_ljlk_plan {
   void* spec_next = nullptr;  // [n_terms, P]
   void* spec_used = nullptr;  // [n_terms, P]
   void* spec_g = nullptr;     // [N, 3]
+  void* spec_dw = nullptr;    // LK-ball: [N, 4, 3], the waters' gradient
   int* spec_flag = nullptr;
   bool spec_ready = false;  // spec_next holds a backward's weights
   bool spec_taken = false;  // the last speculative forward took a gradient
@@ -2134,7 +2135,7 @@ void free_plan(tmol_b200_ljlk_plan* pl) {
                   pl->lkb_npol,  pl->lkb_occ,     pl->lkb_nocc,    pl->lkb_par,
                   pl->lkb_waters, pl->lkb_dwaters, pl->lkb_nbocc, pl->lkb_active,
                   pl->blk_info,  pl->packed,      pl->spec_next,   pl->spec_used, pl->spec_g,
-                  pl->spec_flag};
+                  pl->spec_dw,   pl->spec_flag};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t e : pl->prof_events) cudaEventDestroy(e);
@@ -2574,8 +2575,9 @@ int lkb_waters_backward_impl(tmol_b200_ljlk_plan* pl, const void* coords, const 
 
 template <typename Real, bool GRAD, bool BLOCK_PAIR>
 int lkb_score_impl(tmol_b200_ljlk_plan* pl, const void* coords, const void* waters, void* energies, int32_t* nbr,
-                   const void* dTdV, void* dcoords, void* dwaters, cudaStream_t st) {
+                   const void* dTdV, void* dcoords, void* dwaters, cudaStream_t st, const int* done = nullptr) {
   ScoreArgs<Real> s = score_args<Real>(pl, coords);
+  s.done = done;
   LkbArgs<Real> k = lkb_args<Real>(pl);
   k.water_dist = ((const Real*)pl->global_params)[3];  // the score op's own copy
   k.waters = (const Real*)waters;
@@ -2610,6 +2612,50 @@ int lkb_score_impl(tmol_b200_ljlk_plan* pl, const void* coords, const void* wate
     CK(cudaEventRecord(pl->prof_events[2 * pl->prof_n + 1], st));
     ++pl->prof_n;
   }
+  return TMOL_B200_OK;
+}
+
+// LK-ball's score op with a speculative gradient, as
+// forward_speculative_impl / backward_speculative_impl: the kept gradient
+// is the coordinates' direct part and the waters' part.
+template <typename Real>
+int lkb_forward_speculative_impl(tmol_b200_ljlk_plan* pl, const void* coords, const void* waters, void* energies,
+                                 int32_t* nbr, cudaStream_t st) {
+  pl->spec_taken = false;
+  if (!pl->spec_ready)
+    return lkb_score_impl<Real, false, false>(pl, coords, waters, energies, nbr, nullptr, nullptr, nullptr, st);
+  pl->spec_taken = true;
+  const size_t w_bytes = (size_t)4 * pl->P * sizeof(Real);
+  if (w_bytes) CK(cudaMemcpyAsync(pl->spec_used, pl->spec_next, w_bytes, cudaMemcpyDeviceToDevice, st));
+  return lkb_score_impl<Real, true, false>(pl, coords, waters, energies, nbr, pl->spec_used, pl->spec_g,
+                                           pl->spec_dw, st);
+}
+
+template <typename Real>
+int lkb_backward_speculative_impl(tmol_b200_ljlk_plan* pl, const void* coords, const void* waters,
+                                  const void* dTdV, void* dcoords, void* dwaters, int speculated,
+                                  cudaStream_t st) {
+  const int n_w = 4 * pl->P;
+  if (speculated && pl->spec_taken && n_w > 0) {
+    spec_match_kernel<Real><<<1, 1024, 0, st>>>((const Real*)dTdV, (const Real*)pl->spec_used, n_w, pl->spec_flag);
+    CK(cudaGetLastError());
+  } else {
+    CK(cudaMemsetAsync(pl->spec_flag, 0, sizeof(int), st));
+  }
+  // zeroes the outputs; its scoring launch does no work when the flag is set
+  const int rc = lkb_score_impl<Real, true, false>(pl, coords, waters, nullptr, nullptr, dTdV, dcoords, dwaters,
+                                                   st, pl->spec_flag);
+  if (rc != TMOL_B200_OK) return rc;
+  const int64_t n_g = (int64_t)pl->N * 3, n_dw = (int64_t)pl->N * LKB_NW * 3;
+  if (n_g > 0) {
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n_dw + 255) / 256, (int64_t)pl->n_sm * 8));
+    spec_copy_kernel<Real><<<grid, 256, 0, st>>>(pl->spec_flag, (const Real*)pl->spec_g, (Real*)dcoords, n_g);
+    CK(cudaGetLastError());
+    spec_copy_kernel<Real><<<grid, 256, 0, st>>>(pl->spec_flag, (const Real*)pl->spec_dw, (Real*)dwaters, n_dw);
+    CK(cudaGetLastError());
+  }
+  if (n_w > 0) CK(cudaMemcpyAsync(pl->spec_next, dTdV, (size_t)n_w * sizeof(Real), cudaMemcpyDeviceToDevice, st));
+  pl->spec_ready = true;
   return TMOL_B200_OK;
 }
 
@@ -2758,6 +2804,14 @@ int build_lkball(tmol_b200_ljlk_plan* pl, const tmol_b200_lkball_inputs* k, cons
     CK(cudaMemcpyAsync(pl->lkb_npol, hnpol.data(), sizeof(int) * hnpol.size(), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(pl->lkb_nocc, hnocc.data(), sizeof(int) * hnocc.size(), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(pl->lkb_par, par.data(), sizeof(Real) * par.size(), cudaMemcpyHostToDevice, st));
+  }
+  if (scoring && !pl->rotamers) {
+    // the score op's speculative gradient (lkb_backward_speculative)
+    CK(dalloc(pl, (Real**)&pl->spec_next, (size_t)4 * std::max(pl->P, 1)));
+    CK(dalloc(pl, (Real**)&pl->spec_used, (size_t)4 * std::max(pl->P, 1)));
+    CK(dalloc(pl, (Real**)&pl->spec_g, (size_t)std::max<int64_t>(pl->N, 1) * 3));
+    CK(dalloc(pl, (Real**)&pl->spec_dw, (size_t)std::max<int64_t>(pl->N, 1) * LKB_NW * 3));
+    CK(dalloc(pl, &pl->spec_flag, 1));
   }
   if (!waters) return TMOL_B200_OK;
   const int64_t n_sites = pl->N * LKB_NW;
@@ -3836,6 +3890,31 @@ int tmol_b200_lkball_forward(tmol_b200_lkball_plan* plan, const void* coords, co
                                                           nullptr, nullptr, nullptr, st)
                     : lkb_score_impl<double, false, false>(plan, coords, waters, energies, block_neighbors,
                                                            nullptr, nullptr, nullptr, st);
+}
+
+int tmol_b200_lkball_forward_speculative(tmol_b200_lkball_plan* plan, const void* coords, const void* waters,
+                                         void* energies, int32_t* block_neighbors, void* stream) {
+  NvtxRange nvtx_range("tmol_b200_lkball_forward_speculative");
+  if (!plan || plan->term != kTermLKBall || plan->rotamers || !plan->lkb_pol || !plan->spec_g || !energies)
+    return TMOL_B200_ERR_INVALID_ARGUMENT;
+  if (plan->N > 0 && (!coords || !waters)) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->real_bytes == 4)
+    return lkb_forward_speculative_impl<float>(plan, coords, waters, energies, block_neighbors, st);
+  return lkb_forward_speculative_impl<double>(plan, coords, waters, energies, block_neighbors, st);
+}
+
+int tmol_b200_lkball_backward_speculative(tmol_b200_lkball_plan* plan, const void* coords, const void* waters,
+                                          const void* dTdV, void* dcoords, void* dwaters, int speculated,
+                                          void* stream) {
+  NvtxRange nvtx_range("tmol_b200_lkball_backward_speculative");
+  if (!plan || plan->term != kTermLKBall || plan->rotamers || !plan->lkb_pol || !plan->spec_g || !dTdV)
+    return TMOL_B200_ERR_INVALID_ARGUMENT;
+  if (plan->N > 0 && (!coords || !waters || !dcoords || !dwaters)) return TMOL_B200_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->real_bytes == 4)
+    return lkb_backward_speculative_impl<float>(plan, coords, waters, dTdV, dcoords, dwaters, speculated, st);
+  return lkb_backward_speculative_impl<double>(plan, coords, waters, dTdV, dcoords, dwaters, speculated, st);
 }
 
 int tmol_b200_lkball_energy_and_gradient(tmol_b200_lkball_plan* plan, const void* coords, const void* weights,

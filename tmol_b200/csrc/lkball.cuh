@@ -689,6 +689,8 @@ __device__ __forceinline__ LkbParams<Real> lkb_params(const K& k, int A, int bt,
 // (donor or acceptor: the 4 x 4 water-pair term) and the rest, and are
 // evaluated 32 at a time with every lane busy on the same branch.
 constexpr int LKB_Q = 64;
+// warps per CTA of the LK-ball kernels (launches clamp to it)
+constexpr int LKB_MAX_WARPS = 8;
 
 template <bool TAGGED>
 struct LkbQueue {
@@ -986,9 +988,10 @@ __device__ __forceinline__ void lkb_flush_counts(const ScoreArgs<Real>& s, const
 // occluder pair of each neighbouring block pair.
 template <typename Real, bool GRAD, bool BLOCK_PAIR>
 __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS) lkb_score_kernel(ScoreArgs<Real> s, LkbArgs<Real> k, int items_per_ticket) {
+  if (s.done && *s.done) return;  // a speculative gradient was taken
   // [warp][plain, bridged]; block-pair mode tags queued pairs with their
   // block pair (p * B + b1) * B + b2
-  __shared__ LkbQueue<BLOCK_PAIR> queues[MAX_WARPS][2];
+  __shared__ LkbQueue<BLOCK_PAIR> queues[LKB_MAX_WARPS][2];
   LkbWarp<Real, BLOCK_PAIR> q;
   q.lane = threadIdx.x & 31;
   q.qs = queues[threadIdx.x >> 5];
@@ -1096,7 +1099,7 @@ __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS) lkb_score_kernel(
 template <typename Real, bool GRAD>
 __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS)
     lkb_rotamer_kernel(ScoreArgs<Real> s, LkbArgs<Real> k, RotArgs ra, const Real* rot_spheres) {
-  __shared__ LkbQueue<true> queues[MAX_WARPS][2];
+  __shared__ LkbQueue<true> queues[LKB_MAX_WARPS][2];
   LkbWarp<Real, true> q;
   q.lane = threadIdx.x & 31;
   q.qs = queues[threadIdx.x >> 5];

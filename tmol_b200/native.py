@@ -257,6 +257,8 @@ SIGNATURES = {
     "tmol_b200_lkball_waters_backward": (ctypes.c_int, [_V, _V, _V, _V, _V]),
     "tmol_b200_lkball_forward": (ctypes.c_int, [_V, _V, _V, ctypes.c_int, _V, _V, _V]),
     "tmol_b200_lkball_backward": (ctypes.c_int, [_V, _V, _V, ctypes.c_int, _V, _V, _V, _V]),
+    "tmol_b200_lkball_forward_speculative": (ctypes.c_int, [_V, _V, _V, _V, _V, _V]),
+    "tmol_b200_lkball_backward_speculative": (ctypes.c_int, [_V, _V, _V, _V, _V, _V, ctypes.c_int, _V]),
     "tmol_b200_lkball_energy_and_gradient": (ctypes.c_int, [_V, _V, _V, _V, _V, _V]),
     "tmol_b200_lkball_plan_create_from_connectivity": (
         ctypes.c_int,

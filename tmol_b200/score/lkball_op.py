@@ -42,7 +42,9 @@ class LKBallPlan(LJLKPlan):
 
     N_TERMS = 4  # lk_ball_iso, lk_ball, lk_bridge, lk_bridge_uncpl
     ABI = "tmol_b200_lkball"
-    SPECULATIVE = False  # its ops have their own autograd functions
+    # the score op's own autograd function uses the speculative pair below
+    # (LJLKPlan's _ScoreFn is not used for LK-ball)
+    SPECULATIVE = False
     NAME = "LK-ball"
 
     def __init__(self, coords_like, water_static=None, score_static=None, launch=None, rotamers=False,
@@ -225,6 +227,46 @@ class LKBallPlan(LJLKPlan):
         self._after_call()
         return dcoords, dwaters
 
+    def forward_speculative(self, coords, waters, want_neighbors=True):
+        """Whole-pose energies (and neighbour matrix) for an autograd forward
+        whose backward will follow: once the plan has seen a
+        backward_speculative call, the same pass also takes the gradients
+        (coordinates directly, and waters) with that call's weights and keeps
+        them.  Returns (energies, nbr, gen)."""
+        self._check_coords(coords)
+        self._check_waters(waters)
+        coords, waters = coords.contiguous(), waters.contiguous()
+        P, B = self.n_poses, self.max_n_blocks
+        energies = torch.empty((self.N_TERMS, P), dtype=self.dtype, device=self.device)
+        nbr = torch.empty((P, B, B), dtype=torch.int32, device=self.device) if want_neighbors else None
+        native.call(
+            "tmol_b200_lkball_forward_speculative", self.ptr, ctypes.c_void_p(coords.data_ptr()),
+            ctypes.c_void_p(waters.data_ptr()), ctypes.c_void_p(energies.data_ptr()),
+            ctypes.c_void_p(nbr.data_ptr() if nbr is not None else 0), self._stream(),
+        )
+        self.spec_gen += 1
+        self._after_call()
+        return energies, nbr, self.spec_gen
+
+    def backward_speculative(self, coords, waters, dTdV, gen):
+        """(dL/dcoords directly, dL/dwaters) for the forward `gen` returned:
+        that forward's kept gradients when it is still the plan's latest and
+        its weights equal dTdV (decided on the device), else recomputed."""
+        self._check_coords(coords)
+        self._check_waters(waters)
+        coords, waters = coords.contiguous(), waters.contiguous()
+        dTdV = dTdV.to(self.dtype).contiguous()
+        dcoords = torch.empty_like(coords)
+        dwaters = torch.empty_like(waters)
+        native.call(
+            "tmol_b200_lkball_backward_speculative", self.ptr, ctypes.c_void_p(coords.data_ptr()),
+            ctypes.c_void_p(waters.data_ptr()), ctypes.c_void_p(dTdV.data_ptr()),
+            ctypes.c_void_p(dcoords.data_ptr()), ctypes.c_void_p(dwaters.data_ptr()),
+            int(gen is not None and gen == self.spec_gen), self._stream(),
+        )
+        self._after_call()
+        return dcoords, dwaters
+
     COUNT_NAMES = ("block_pairs", "polar_occluder_pairs", "bridged_pairs", "pairs_evaluated", "unused")
 
     def set_skip_mask(self, mask):
@@ -296,9 +338,21 @@ class _WaterFn(torch.autograd.Function):
 
 
 class _LKBallScoreFn(torch.autograd.Function):
+    """Whole-pose calls that need a gradient go through the speculative pair
+    (one scoring pass per forward + backward from the second call on, as
+    the LJ/LK op)."""
+
     @staticmethod
     def forward(ctx, coords, waters, plan, block_pair, want_neighbors):
-        E, nbr = plan.forward(coords, waters, block_pair, want_neighbors)
+        ctx.spec_gen = None
+        ctx.speculate = (
+            not block_pair and (ctx.needs_input_grad[0] or ctx.needs_input_grad[1])
+            and coords.is_cuda and not torch.cuda.is_current_stream_capturing()
+        )
+        if ctx.speculate:
+            E, nbr, ctx.spec_gen = plan.forward_speculative(coords, waters, want_neighbors)
+        else:
+            E, nbr = plan.forward(coords, waters, block_pair, want_neighbors)
         ctx.plan = plan
         ctx.block_pair = block_pair
         ctx.save_for_backward(coords, waters)
@@ -312,7 +366,10 @@ class _LKBallScoreFn(torch.autograd.Function):
         coords, waters = ctx.saved_tensors
         if dE is None:
             return None, None, None, None, None
-        dx, dw = ctx.plan.backward(coords, waters, dE, ctx.block_pair)
+        if not ctx.speculate or torch.cuda.is_current_stream_capturing():
+            dx, dw = ctx.plan.backward(coords, waters, dE, ctx.block_pair)
+        else:
+            dx, dw = ctx.plan.backward_speculative(coords, waters, dE, ctx.spec_gen)
         return dx, dw, None, None, None
 
 
