@@ -2432,7 +2432,8 @@ def measure_pose_batch(args, workload_name, world, rank, local, steps, extras=Tr
                 "serial_value": poses_total / (serial_ms / 1e3),
                 "dropin_value": poses_total / (dropin_ms / 1e3),
                 "dropin_schedule": "tmol's drop-in op ljlk_pose_scores (27 arguments) + backward() through its "
-                "autograd function, coordinates in from pinned host memory, energies and gradient out, step by "
+                "autograd function (speculative gradient: one fused scoring pass per forward + backward once "
+                "the weights repeat), coordinates in from pinned host memory, energies and gradient out, step by "
                 "step, L2 flushed before each step inside the timed region",
             },
             "cpu_baseline": cpu,
