@@ -551,6 +551,7 @@ __device__ __forceinline__ void pack_block(const ScoreArgs<Real>& s, int bt, int
 
 template <typename Real>
 __global__ void spheres_kernel(ScoreArgs<Real> s) {
+  if (s.done && *s.done) return;  // the scoring launch that follows does no work
   const int lane = threadIdx.x & 31;
   const int n_blocks = s.P * s.B;
   const int warps = (gridDim.x * blockDim.x) >> 5;
