@@ -183,10 +183,10 @@ int tmol_b200_ljlk_energy_and_gradient(tmol_b200_ljlk_plan* plan,
                                        void* energies, void* dcoords,
                                        void* stream);
 
-/* Work counting, off by default: while enabled, the whole-pose LJ/LK and
- * elec scoring calls run a kernel instantiation that also counts its work
- * (slower: the counters take registers and instructions in its item loop).
- * The LK-ball and rotamer kernels always count.  No counterpart in the
+/* Work counting, off by default: while enabled, the LJ/LK, elec and
+ * LK-ball pose scoring calls run a kernel instantiation that also counts
+ * its work (slower: the counters take registers and instructions in its
+ * item loop).  The rotamer kernels always count.  No counterpart in the
  * reference. */
 int tmol_b200_ljlk_plan_set_counting(tmol_b200_ljlk_plan* plan, int enable);
 

@@ -170,6 +170,7 @@ def test_energy_and_gradient_in_one_call(lterm, f64):
     coords = ps.coords.flatten(0, 1).to(DEV, dt)
     plan = LKBallPlan(coords, water_static=wa, score_static=sa)
     w = torch.rand(4, ps.n_poses, dtype=torch.float64, generator=torch.Generator().manual_seed(3))
+    plan.set_counting(True)
     for _ in range(2):  # the plan's scratch is reused
         E, dx = plan.energy_and_gradient(coords, w.to(DEV, dt))
     _, Eo, dxo, _ = oracle_run(ps, lterm, f64, weights=w.numpy())

@@ -2607,7 +2607,10 @@ int lkb_score_impl(tmol_b200_ljlk_plan* pl, const void* coords, const void* wate
   const int grid = std::max(1, std::min((n_tickets + warps - 1) / warps, pl->n_sm * pl->launch.ctas_per_sm));
   const bool prof = pl->profiling && 2 * (size_t)pl->prof_n + 1 < pl->prof_events.size();
   if (prof) CK(cudaEventRecord(pl->prof_events[2 * pl->prof_n], st));
-  lkb_score_kernel<Real, GRAD, BLOCK_PAIR><<<grid, 32 * warps, 0, st>>>(s, k, R);
+  if (pl->counting)
+    lkb_score_kernel<Real, GRAD, BLOCK_PAIR, true><<<grid, 32 * warps, 0, st>>>(s, k, R);
+  else
+    lkb_score_kernel<Real, GRAD, BLOCK_PAIR, false><<<grid, 32 * warps, 0, st>>>(s, k, R);
   CK(cudaGetLastError());
   if (prof) {
     CK(cudaEventRecord(pl->prof_events[2 * pl->prof_n + 1], st));

@@ -855,7 +855,7 @@ __device__ __forceinline__ LkbSide lkb_side(const LkbArgs<Real>& k, int bt, int 
 // separation (intra: the block type's path distances; inter: through the
 // connections when `striking`), distance and the polar atom's waters, and
 // queued; full queues are evaluated under w into e4.
-template <typename Real, bool GRAD, bool TAGGED>
+template <typename Real, bool GRAD, bool TAGGED, bool COUNT = true>
 __device__ __forceinline__ void lkb_enqueue_pairs(const ScoreArgs<Real>& s, const LkbArgs<Real>& k,
                                                   const LkbEval<Real>& ev, LkbWarp<Real, TAGGED>& q, const LkbSide& a,
                                                   const LkbSide& b, bool intra, bool striking, int nc1, int nc2,
@@ -869,8 +869,10 @@ __device__ __forceinline__ void lkb_enqueue_pairs(const ScoreArgs<Real>& s, cons
   // error is far below 0.5 / no)
   const float inv_no = no > 0 ? 1.0f / float(no) : 0.0f;
   const float inv_nocc1 = a.nocc > 0 ? 1.0f / float(a.nocc) : 0.0f;
-  q.n_bp += 1;
-  q.n_pairs += total;
+  if (COUNT) {
+    q.n_bp += 1;
+    q.n_pairs += total;
+  }
   for (int base = 0; base < total; base += 32) {
     const int idx = base + lane;
     bool in_reach = false, bridged = false;
@@ -932,8 +934,10 @@ __device__ __forceinline__ void lkb_enqueue_pairs(const ScoreArgs<Real>& s, cons
     }
     q.nq[0] += __popc(m0);
     q.nq[1] += __popc(m1);
-    q.n_eval += __popc(m0 | m1);
-    q.n_bridge += __popc(m1);
+    if (COUNT) {
+      q.n_eval += __popc(m0 | m1);
+      q.n_bridge += __popc(m1);
+    }
     lkb_pump<Real, GRAD, TAGGED>(ev, q, false, w, e4, tg);
   }
 }
@@ -986,7 +990,9 @@ __device__ __forceinline__ void lkb_flush_counts(const ScoreArgs<Real>& s, const
 // The pose op: the plan's work items (pose, b1, candidate blocks b2 >= b1),
 // the neighbour rule as score_kernel applies it, then every polar /
 // occluder pair of each neighbouring block pair.
-template <typename Real, bool GRAD, bool BLOCK_PAIR>
+// COUNT: the work counters (registers and instructions in the pair loop),
+// compiled into a separate instantiation used on request
+template <typename Real, bool GRAD, bool BLOCK_PAIR, bool COUNT>
 __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS) lkb_score_kernel(ScoreArgs<Real> s, LkbArgs<Real> k, int items_per_ticket) {
   if (s.done && *s.done) return;  // a speculative gradient was taken
   // [warp][plain, bridged]; block-pair mode tags queued pairs with their
@@ -1066,7 +1072,7 @@ __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS) lkb_score_kernel(
           const bool striking = !intra && lkb_striking(s, i1, b2, cp_b2, cp_min, seps);
           const LkbSide side2 = lkb_side(k, s.blk_bt[i2], s.blk_off[i2]);
           const int nc1 = striking ? s.bt_n_conn[bt1] : 0, nc2 = striking ? s.bt_n_conn[side2.bt] : 0;
-          lkb_enqueue_pairs<Real, GRAD, BLOCK_PAIR>(s, k, ev, q, side1, side2, intra, striking, nc1, nc2, seps,
+          lkb_enqueue_pairs<Real, GRAD, BLOCK_PAIR, COUNT>(s, k, ev, q, side1, side2, intra, striking, nc1, nc2, seps,
                                                     BLOCK_PAIR ? none : w, acc,
                                                     BLOCK_PAIR ? (int)((int64_t)i1 * s.B + b2) : 0, tg);
         }
