@@ -654,7 +654,7 @@ def run_rotamers(args, world, rank, local):
         E, idx, items = op()
     torch.cuda.synchronize()
     n_pairs = idx.shape[1]
-    counts = plan.last_counts()
+    counts = counted_work(plan, op)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     barrier(world)
     torch.cuda.synchronize()
@@ -813,7 +813,7 @@ def run_lkball_rotamers(args, world, rank, local):
         E, idx, items = op()
     torch.cuda.synchronize()
     n_pairs = idx.shape[1]
-    counts = plan.last_counts()
+    counts = counted_work(plan, op)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     barrier(world)
     torch.cuda.synchronize()

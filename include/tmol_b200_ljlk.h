@@ -184,10 +184,9 @@ int tmol_b200_ljlk_energy_and_gradient(tmol_b200_ljlk_plan* plan,
                                        void* stream);
 
 /* Work counting, off by default: while enabled, the LJ/LK, elec and
- * LK-ball pose scoring calls run a kernel instantiation that also counts
- * its work (slower: the counters take registers and instructions in its
- * item loop).  The rotamer kernels always count.  No counterpart in the
- * reference. */
+ * LK-ball scoring calls (pose and rotamer ops) run a kernel instantiation
+ * that also counts its work (slower: the counters take registers and
+ * instructions in its item loop).  No counterpart in the reference. */
 int tmol_b200_ljlk_plan_set_counting(tmol_b200_ljlk_plan* plan, int enable);
 
 /* Work counters of the last forward / energy_and_gradient call (all zero

@@ -1701,7 +1701,7 @@ __global__ void rot_row_fill_kernel(ScoreArgs<Real> s, RotArgs ra) {
 // group), or against itself on the diagonal.  Energies go to the item's
 // pairs (energies[t * n_pairs + d]; the warp owns them), the adjoint
 // weights come from dTdV[t * n_pairs + d].
-template <typename Real, bool GRAD, int TERM>
+template <typename Real, bool GRAD, int TERM, bool COUNT>
 __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_CTAS : 1)
     rotamer_kernel(ScoreArgs<Real> s, RotArgs ra, const Real* rs) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1777,12 +1777,14 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
         E3<Real> e = {0, 0, 0};
         if (ti == 0) {
           const long long n2a = diag ? 0 : s.bt_n_atoms[ra.rot_bt[rot2_first + k]];
-          cnt_add(w.counts, 0, 1, lane);
-          cnt_add(w.counts, 1, diag ? (long long)r.n1 * (r.n1 - 1) / 2 : (long long)r.n1 * n2a, lane);
+          if (COUNT) {
+            cnt_add(w.counts, 0, 1, lane);
+            cnt_add(w.counts, 1, diag ? (long long)r.n1 * (r.n1 - 1) / 2 : (long long)r.n1 * n2a, lane);
+          }
         }
         if (diag) {
           // this tile with itself, then with the rotamer's later tiles
-          E3<Real> t = intra_tile<Real, GRAD, TERM>(ec, &w, r.st1, r.c1, lane);
+          E3<Real> t = intra_tile<Real, GRAD, TERM, COUNT>(ec, &w, r.st1, r.c1, lane);
           e.atr += t.atr;
           e.rep += t.rep;
           e.lk += t.lk;
@@ -1800,7 +1802,7 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
             const int m = stage_side1<Real, TERM>(s, w, 0, 0, r.bt1, r.off1, st2, c2, 0, c1x, c1y, c1z, reach1_2, lane);
             __syncwarp();
             if (m > 0) {
-              E3<Real> g = screen_slots<Real, GRAD, TERM>(ec, &w, r.c1, r.nc1, m, 1, lane);
+              E3<Real> g = screen_slots<Real, GRAD, TERM, COUNT>(ec, &w, r.c1, r.nc1, m, 1, lane);
               if (GRAD) flush_side1(s, w, m, lane);
               e.atr += g.atr;
               e.rep += g.rep;
@@ -1832,7 +1834,7 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
             const int m = stage_side1<Real, TERM>(s, w, 0, 0, bt2, off2, st2, c2, nc2, c1x, c1y, c1z, reach1_2, lane);
             __syncwarp();
             if (m > 0) {
-              E3<Real> g = screen_slots<Real, GRAD, TERM>(ec, &w, r.c1, r.nc1, m, 1, lane);
+              E3<Real> g = screen_slots<Real, GRAD, TERM, COUNT>(ec, &w, r.c1, r.nc1, m, 1, lane);
               if (GRAD) flush_side1(s, w, m, lane);
               e.atr += g.atr;
               e.rep += g.rep;
@@ -1848,7 +1850,7 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? TMOL_B200_FLOAT_MIN_C
     }
   }
   __syncwarp();
-  if (s.counts && lane < N_COUNTS && w.counts[lane])
+  if (COUNT && s.counts && lane < N_COUNTS && w.counts[lane])
     atomicAdd(&s.counts[lane], w.counts[lane]);
 }
 
@@ -2167,8 +2169,10 @@ cudaError_t set_smem_limits_term() {
       (const void*)score_kernel<Real, false, true, TERM, true>,
       (const void*)score_kernel<Real, true, false, TERM, true>,
       (const void*)score_kernel<Real, true, true, TERM, true>,
-      (const void*)rotamer_kernel<Real, false, TERM>,
-      (const void*)rotamer_kernel<Real, true, TERM>};
+      (const void*)rotamer_kernel<Real, false, TERM, false>,
+      (const void*)rotamer_kernel<Real, true, TERM, false>,
+      (const void*)rotamer_kernel<Real, false, TERM, true>,
+      (const void*)rotamer_kernel<Real, true, TERM, true>};
   for (const void* k : kernels) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
@@ -2513,10 +2517,10 @@ int rotamer_score_impl(tmol_b200_ljlk_plan* pl, const void* coords, const int32_
   const size_t smem = warps * sizeof(Slab<Real>);
   int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n_items + warps - 1) / warps,
                                                          (int64_t)pl->n_sm * pl->launch.ctas_per_sm));
-  if (pl->term == kTermElec)
-    rotamer_kernel<Real, GRAD, kTermElec><<<grid, 32 * warps, smem, st>>>(s, ra, (const Real*)pl->rot_spheres);
-  else
-    rotamer_kernel<Real, GRAD, kTermLJLK><<<grid, 32 * warps, smem, st>>>(s, ra, (const Real*)pl->rot_spheres);
+  auto kern = pl->term == kTermElec
+                  ? (pl->counting ? rotamer_kernel<Real, GRAD, kTermElec, true> : rotamer_kernel<Real, GRAD, kTermElec, false>)
+                  : (pl->counting ? rotamer_kernel<Real, GRAD, kTermLJLK, true> : rotamer_kernel<Real, GRAD, kTermLJLK, false>);
+  kern<<<grid, 32 * warps, smem, st>>>(s, ra, (const Real*)pl->rot_spheres);
   CK(cudaGetLastError());
   return TMOL_B200_OK;
 }
@@ -2695,7 +2699,10 @@ int lkb_rotamer_score_impl(tmol_b200_ljlk_plan* pl, const void* coords, const vo
   const int warps = std::min(pl->launch.warps_per_cta, 8);  // a kernel of at most 256 threads
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n_items + warps - 1) / warps,
                                                                (int64_t)pl->n_sm * pl->launch.ctas_per_sm));
-  lkb_rotamer_kernel<Real, GRAD><<<grid, 32 * warps, 0, st>>>(s, k, ra, (const Real*)pl->rot_spheres);
+  if (pl->counting)
+    lkb_rotamer_kernel<Real, GRAD, true><<<grid, 32 * warps, 0, st>>>(s, k, ra, (const Real*)pl->rot_spheres);
+  else
+    lkb_rotamer_kernel<Real, GRAD, false><<<grid, 32 * warps, 0, st>>>(s, k, ra, (const Real*)pl->rot_spheres);
   CK(cudaGetLastError());
   return TMOL_B200_OK;
 }

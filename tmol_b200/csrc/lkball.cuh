@@ -1102,7 +1102,7 @@ __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS) lkb_score_kernel(
 // (energies[t * n_pairs + d], added by atomics), the adjoint under
 // dTdV[t * n_pairs + d].  Queued pairs carry d, so the queues fill across
 // rotamer pairs and items (a rotamer pair has few pairs in reach).
-template <typename Real, bool GRAD>
+template <typename Real, bool GRAD, bool COUNT>
 __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS)
     lkb_rotamer_kernel(ScoreArgs<Real> s, LkbArgs<Real> k, RotArgs ra, const Real* rot_spheres) {
   __shared__ LkbQueue<true> queues[LKB_MAX_WARPS][2];
@@ -1154,7 +1154,7 @@ __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS)
       }
       const LkbSide side2 = lkb_side(k, ra.rot_bt[rot2], ra.rot_off[rot2]);
       const int nc1 = striking ? s.bt_n_conn[side1.bt] : 0, nc2 = striking ? s.bt_n_conn[side2.bt] : 0;
-      lkb_enqueue_pairs<Real, GRAD, true>(s, k, ev, q, side1, side2, intra, striking, nc1, nc2, seps, none, unused,
+      lkb_enqueue_pairs<Real, GRAD, true, COUNT>(s, k, ev, q, side1, side2, intra, striking, nc1, nc2, seps, none, unused,
                                           (int)(pair_first + j), tg);
     }
   }

@@ -359,7 +359,7 @@ class LJLKPlan:
 
     def set_counting(self, enable=True):
         """Work counting for the following calls (off by default: the counting
-        kernel is slower).  Rotamer plans always count."""
+        kernel is slower)."""
         native.call("tmol_b200_ljlk_plan_set_counting", self.ptr, int(bool(enable)))
 
     def last_counts(self):
