@@ -118,7 +118,9 @@ int tmol_b200_ljlk_plan_create(const tmol_b200_ljlk_inputs* inputs,
 int tmol_b200_ljlk_plan_destroy(tmol_b200_ljlk_plan* plan);
 
 /* Reorders the plan's work items longest-first by the cost each item took
- * in the last scoring call (synchronises the stream).  Coordinates change
+ * in the last scoring call made with counting on (the counting kernels time
+ * each item; see tmol_b200_ljlk_plan_set_counting) (synchronises the
+ * stream).  Coordinates change
  * little between calls in minimisation or trajectory replay, so the order
  * keeps the tail of the next launches short.  An item costlier than half a
  * warp's share of the call is first split over the halves of its candidate

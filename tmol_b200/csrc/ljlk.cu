@@ -1238,7 +1238,8 @@ __global__ void __launch_bounds__(sizeof(Real) == 4 ? 512 : 256, 1)
     if (it0 >= n_work) break;
     int it1 = min(it0 + items_per_ticket, n_work);
     for (int item = it0; item < it1; ++item) {
-      long long t_item = clock64();
+      // item costs for plan_rebalance: measured by the counting instantiation
+      const long long t_item = COUNT ? clock64() : 0;
       int4 wi = s.work[item];
       RowInfo r;
       r.p = wi.x;
@@ -1325,7 +1326,7 @@ __global__ void __launch_bounds__(sizeof(Real) == 4 ? 512 : 256, 1)
       }
       bool any = __any_sync(0xffffffffu, my_mask != 0);
       if (!any) {
-        if (s.item_cost && lane == 0)
+        if (COUNT && s.item_cost && lane == 0)
           s.item_cost[item] = (int)min((clock64() - t_item) >> 4, (long long)0x7fffffff);
         continue;
       }
@@ -1486,7 +1487,7 @@ __global__ void __launch_bounds__(sizeof(Real) == 4 ? 512 : 256, 1)
           if (v2 != Real(0)) atomicAdd(&s.energies[2 * s.P + r.p], v2);
         }
       }
-      if (s.item_cost && lane == 0)
+      if (COUNT && s.item_cost && lane == 0)
         s.item_cost[item] = (int)min((clock64() - t_item) >> 4, (long long)0x7fffffff);
     }
   }

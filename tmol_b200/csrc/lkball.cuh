@@ -1021,7 +1021,7 @@ __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS) lkb_score_kernel(
     if (it0 >= n_work) break;
     const int it1 = min(it0 + items_per_ticket, n_work);
     for (int item = it0; item < it1; ++item) {
-      const long long t_item = clock64();
+      const long long t_item = COUNT ? clock64() : 0;  // item costs: the counting instantiation
       const int4 wi = s.work[item];
       const int p = wi.x, b1 = wi.y, cand0 = wi.z, cand1 = wi.w;
       const int i1 = p * s.B + b1;
@@ -1086,7 +1086,8 @@ __global__ void __launch_bounds__(256, TMOL_B200_LKB_MIN_CTAS) lkb_score_kernel(
           if (lane == 0 && v != Real(0)) atomicAdd(&s.energies[(int64_t)c * s.P + p], v);
         }
       // the item's cost, for ordering the work longest-first
-      if (s.item_cost && lane == 0) s.item_cost[item] = (int)min((clock64() - t_item) >> 4, (long long)0x7fffffff);
+      if (COUNT && s.item_cost && lane == 0)
+        s.item_cost[item] = (int)min((clock64() - t_item) >> 4, (long long)0x7fffffff);
     }
   }
   if (BLOCK_PAIR) {

@@ -214,7 +214,8 @@ class LJLKPlan:
         return (l.rows_per_item, l.warps_per_cta, l.ctas_per_sm, l.candidates_per_item, l.slots_per_group)
 
     def rebalance(self):
-        """Order the work items longest-first by their cost in the last call."""
+        """Order the work items longest-first by their cost in the last call
+        made with counting on (the counting kernels time each item)."""
         native.call("tmol_b200_ljlk_plan_rebalance", self.ptr, self._stream())
 
     def _after_call(self):
@@ -222,6 +223,8 @@ class LJLKPlan:
         if self.auto_balance > 0 and not torch.cuda.is_current_stream_capturing():
             self.auto_balance -= 1
             self.rebalance()
+            if self.auto_balance == 0:
+                self.set_counting(False)
 
     def balance(self, run, passes=2):
         """Runs `run()` (one scoring call on this plan) and orders the work
@@ -230,9 +233,11 @@ class LJLKPlan:
         several times cheaper than it runs beside other heavy items; measured
         again in longest-first order, every heavy item runs as it will in the
         calls that follow."""
+        self.set_counting(True)  # the counting kernels time each item
         for _ in range(passes):
             run()
             self.rebalance()
+        self.set_counting(False)
 
     def device_bytes(self):
         return native.load().tmol_b200_ljlk_plan_device_bytes(self.ptr)
@@ -544,8 +549,11 @@ def get_plan(coords, static, rotamers=False, plan_class=None):
         return entry[0]
     plan = plan_class(coords, static, rotamers=rotamers)
     # the drop-in ops run without a tuning step: their plans order the work
-    # items by measured cost after each of their first two calls
-    plan.auto_balance = 2
+    # items by measured cost after each of their first two calls (made with
+    # the counting kernels, which time each item)
+    if not rotamers:
+        plan.auto_balance = 2
+        plan.set_counting(True)
     # the static tensors are held so that their addresses cannot be reused
     # by other tensors while the key is cached
     _PLAN_CACHE[key] = (plan, [t for t in static if isinstance(t, torch.Tensor)])
