@@ -443,6 +443,9 @@ struct ScoreArgs {
   // when set and nonzero, the launch has nothing to do: the gradient was
   // taken from a speculative pass (pose_backward_speculative)
   const int* done;
+  // reals of dcoords and of energies the sphere pass zeroes first (the
+  // one-call energy and gradient: no separate memsets in its step)
+  int64_t zero_dcoords, zero_energies;
   // pose plans of the LJ/LK and elec terms: per block {block type, first
   // atom, atom count, connections | ligand << 8} and every atom as a
   // staged record (coordinates with its type or charge), written by the
@@ -552,6 +555,10 @@ __device__ __forceinline__ void pack_block(const ScoreArgs<Real>& s, int bt, int
 template <typename Real>
 __global__ void spheres_kernel(ScoreArgs<Real> s) {
   if (s.done && *s.done) return;  // the scoring launch that follows does no work
+  const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t n_threads = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = tid; i < s.zero_dcoords; i += n_threads) s.dcoords[i] = Real(0);
+  for (int64_t i = tid; i < s.zero_energies; i += n_threads) s.energies[i] = Real(0);
   const int lane = threadIdx.x & 31;
   const int n_blocks = s.P * s.B;
   const int warps = (gridDim.x * blockDim.x) >> 5;
@@ -2342,8 +2349,9 @@ int energy_and_gradient_impl(tmol_b200_ljlk_plan* pl, const void* coords,
   s.dTdV = (const Real*)weights;
   s.dcoords = (Real*)dcoords;
   s.energies = (Real*)energies;
-  CK(cudaMemsetAsync(dcoords, 0, (size_t)pl->N * 3 * sizeof(Real), st));
-  CK(cudaMemsetAsync(energies, 0, (size_t)n_terms(pl->term) * pl->P * sizeof(Real), st));
+  // the sphere pass zeroes the outputs before the scoring launch adds to them
+  s.zero_dcoords = (int64_t)pl->N * 3;
+  s.zero_energies = (int64_t)n_terms(pl->term) * pl->P;
   CK(cudaMemsetAsync(pl->counts, 0, N_COUNTS * sizeof(unsigned long long), st));
   return launch_score<Real, true, false>(pl, s, st);
 }
