@@ -50,6 +50,12 @@ namespace tmol_b200 {
 
 constexpr int TILE = 32;
 constexpr int MAX_CONN = 4;
+// Work counters (units of the throughput and roofline figures):
+//   [0] block pairs, [1] atom pairs (inter n1*n2, intra n(n-1)/2),
+//   [2] heavy-atom pairs (same rule), [3] atom pairs inside max_dis with a
+//   non-zero count-pair weight, [4] heavy-atom pairs among those.
+// Per warp they are warp-uniform.
+constexpr int N_COUNTS = 5;
 constexpr int CP_CAP = 16;
 constexpr int MAX_ROWS_PER_ITEM = 64;
 constexpr int MAX_WARPS = 16;
@@ -559,6 +565,8 @@ __global__ void spheres_kernel(ScoreArgs<Real> s) {
   const int64_t n_threads = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = tid; i < s.zero_dcoords; i += n_threads) s.dcoords[i] = Real(0);
   for (int64_t i = tid; i < s.zero_energies; i += n_threads) s.energies[i] = Real(0);
+  if (s.zero_energies && s.counts && tid < N_COUNTS) s.counts[tid] = 0;
+  if (tid == 0 && s.ticket) *s.ticket = 0;  // the scoring launch's work ticket
   const int lane = threadIdx.x & 31;
   const int n_blocks = s.P * s.B;
   const int warps = (gridDim.x * blockDim.x) >> 5;
@@ -656,12 +664,6 @@ struct RowInfo {
   int st1, c1;  // tile of b1 in side 0
 };
 
-// Per-warp work counters (units of the throughput and roofline figures):
-//   [0] block pairs, [1] atom pairs (inter n1*n2, intra n(n-1)/2),
-//   [2] heavy-atom pairs (same rule), [3] atom pairs inside max_dis with a
-//   non-zero count-pair weight, [4] heavy-atom pairs among those.
-// All are warp-uniform.
-constexpr int N_COUNTS = 5;
 
 
 template <typename Real>
@@ -2286,9 +2288,8 @@ int launch_score(tmol_b200_ljlk_plan* pl, ScoreArgs<Real> s, cudaStream_t st) {
   int n_blocks = pl->P * pl->B;
   int threads = 256;
   int grid_s = std::max(1, std::min((n_blocks + 7) / 8, pl->n_sm * 16));
-  spheres_kernel<Real><<<grid_s, threads, 0, st>>>(s);
+  spheres_kernel<Real><<<grid_s, threads, 0, st>>>(s);  // also resets the work ticket
   CK(cudaGetLastError());
-  CK(cudaMemsetAsync(pl->counters, 0, sizeof(int), st));
   if (pl->n_work == 0) return TMOL_B200_OK;
   int warps = pl->launch.warps_per_cta;
   if (sizeof(Real) == 8) warps = std::min(warps, 8);  // the float64 kernel: at most 256 threads
@@ -2351,8 +2352,7 @@ int energy_and_gradient_impl(tmol_b200_ljlk_plan* pl, const void* coords,
   s.energies = (Real*)energies;
   // the sphere pass zeroes the outputs before the scoring launch adds to them
   s.zero_dcoords = (int64_t)pl->N * 3;
-  s.zero_energies = (int64_t)n_terms(pl->term) * pl->P;
-  CK(cudaMemsetAsync(pl->counts, 0, N_COUNTS * sizeof(unsigned long long), st));
+  s.zero_energies = (int64_t)n_terms(pl->term) * pl->P;  // and the work counters
   return launch_score<Real, true, false>(pl, s, st);
 }
 
