@@ -449,9 +449,12 @@ struct ScoreArgs {
   // when set and nonzero, the launch has nothing to do: the gradient was
   // taken from a speculative pass (pose_backward_speculative)
   const int* done;
-  // reals of dcoords and of energies the sphere pass zeroes first (the
-  // one-call energy and gradient: no separate memsets in its step)
-  int64_t zero_dcoords, zero_energies;
+  // what the sphere pass zeroes before the scoring launch adds to it (no
+  // separate memsets in a step): reals of dcoords, of energies and of
+  // zero_aux (LK-ball: the waters' gradient), and the work counters
+  int64_t zero_dcoords, zero_energies, zero_aux_n;
+  Real* zero_aux;
+  int zero_counts;
   // pose plans of the LJ/LK and elec terms: per block {block type, first
   // atom, atom count, connections | ligand << 8} and every atom as a
   // staged record (coordinates with its type or charge), written by the
@@ -565,7 +568,8 @@ __global__ void spheres_kernel(ScoreArgs<Real> s) {
   const int64_t n_threads = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = tid; i < s.zero_dcoords; i += n_threads) s.dcoords[i] = Real(0);
   for (int64_t i = tid; i < s.zero_energies; i += n_threads) s.energies[i] = Real(0);
-  if (s.zero_energies && s.counts && tid < N_COUNTS) s.counts[tid] = 0;
+  for (int64_t i = tid; i < s.zero_aux_n; i += n_threads) s.zero_aux[i] = Real(0);
+  if (s.zero_counts && s.counts && tid < N_COUNTS) s.counts[tid] = 0;
   if (tid == 0 && s.ticket) *s.ticket = 0;  // the scoring launch's work ticket
   const int lane = threadIdx.x & 31;
   const int n_blocks = s.P * s.B;
@@ -2323,9 +2327,12 @@ int forward_impl(tmol_b200_ljlk_plan* pl, const void* coords, int block_pair,
   s.nbr = nbr;
   const size_t nt = n_terms(pl->term);
   size_t n_e = block_pair ? nt * pl->P * pl->B * pl->B : nt * pl->P;
-  CK(cudaMemsetAsync(energies, 0, n_e * sizeof(Real), st));
+  if (block_pair)
+    CK(cudaMemsetAsync(energies, 0, n_e * sizeof(Real), st));
+  else
+    s.zero_energies = (int64_t)n_e;  // by the sphere pass
   if (nbr) CK(cudaMemsetAsync(nbr, 0, (size_t)pl->P * pl->B * pl->B * sizeof(int32_t), st));
-  CK(cudaMemsetAsync(pl->counts, 0, N_COUNTS * sizeof(unsigned long long), st));
+  s.zero_counts = 1;
   if (block_pair) return launch_score<Real, false, true>(pl, s, st);
   return launch_score<Real, false, false>(pl, s, st);
 }
@@ -2337,7 +2344,7 @@ int backward_impl(tmol_b200_ljlk_plan* pl, const void* coords, int block_pair,
   s.dTdV = (const Real*)dTdV;
   s.dcoords = (Real*)dcoords;
   s.counts = nullptr;
-  CK(cudaMemsetAsync(dcoords, 0, (size_t)pl->N * 3 * sizeof(Real), st));
+  s.zero_dcoords = (int64_t)pl->N * 3;  // by the sphere pass
   if (block_pair) return launch_score<Real, true, true>(pl, s, st);
   return launch_score<Real, true, false>(pl, s, st);
 }
@@ -2352,7 +2359,8 @@ int energy_and_gradient_impl(tmol_b200_ljlk_plan* pl, const void* coords,
   s.energies = (Real*)energies;
   // the sphere pass zeroes the outputs before the scoring launch adds to them
   s.zero_dcoords = (int64_t)pl->N * 3;
-  s.zero_energies = (int64_t)n_terms(pl->term) * pl->P;  // and the work counters
+  s.zero_energies = (int64_t)n_terms(pl->term) * pl->P;
+  s.zero_counts = 1;
   return launch_score<Real, true, false>(pl, s, st);
 }
 
@@ -2390,10 +2398,11 @@ int forward_speculative_impl(tmol_b200_ljlk_plan* pl, const void* coords, void* 
   s.nbr = nbr;
   s.dTdV = (const Real*)pl->spec_used;
   s.dcoords = (Real*)pl->spec_g;
-  CK(cudaMemsetAsync(energies, 0, (size_t)n_terms(pl->term) * pl->P * sizeof(Real), st));
   if (nbr) CK(cudaMemsetAsync(nbr, 0, (size_t)pl->P * pl->B * pl->B * sizeof(int32_t), st));
-  CK(cudaMemsetAsync(pl->spec_g, 0, (size_t)pl->N * 3 * sizeof(Real), st));
-  CK(cudaMemsetAsync(pl->counts, 0, N_COUNTS * sizeof(unsigned long long), st));
+  // energies, the kept gradient and the counters: by the sphere pass
+  s.zero_energies = (int64_t)n_terms(pl->term) * pl->P;
+  s.zero_dcoords = (int64_t)pl->N * 3;
+  s.zero_counts = 1;
   return launch_score<Real, true, false>(pl, s, st);
 }
 
@@ -2414,7 +2423,8 @@ int backward_speculative_impl(tmol_b200_ljlk_plan* pl, const void* coords, const
   } else {
     CK(cudaMemsetAsync(pl->spec_flag, 0, sizeof(int), st));
   }
-  CK(cudaMemsetAsync(dcoords, 0, (size_t)n_g * sizeof(Real), st));
+  // a hit copies the kept gradient whole; a miss zeroes dcoords in the
+  // sphere pass (which a hit skips) before the scoring launch
   if (n_g > 0) {
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n_g + 255) / 256, (int64_t)pl->n_sm * 8));
     spec_copy_kernel<Real><<<grid, 256, 0, st>>>(pl->spec_flag, (const Real*)pl->spec_g, (Real*)dcoords, n_g);
@@ -2425,6 +2435,7 @@ int backward_speculative_impl(tmol_b200_ljlk_plan* pl, const void* coords, const
   s.dcoords = (Real*)dcoords;
   s.counts = nullptr;
   s.done = pl->spec_flag;
+  s.zero_dcoords = n_g;
   const int rc = launch_score<Real, true, false>(pl, s, st);
   if (rc != TMOL_B200_OK) return rc;
   if (n_w > 0) CK(cudaMemcpyAsync(pl->spec_next, dTdV, (size_t)n_w * sizeof(Real), cudaMemcpyDeviceToDevice, st));
@@ -2603,16 +2614,22 @@ int lkb_score_impl(tmol_b200_ljlk_plan* pl, const void* coords, const void* wate
   const size_t PBB = (size_t)pl->P * pl->B * pl->B;
   // block-pair energies and weights are addressed by an int block-pair index
   if (BLOCK_PAIR && PBB >= ((size_t)1 << 31)) return TMOL_B200_ERR_CAPACITY;
-  if (energies) CK(cudaMemsetAsync(energies, 0, (BLOCK_PAIR ? PBB : (size_t)pl->P) * 4 * sizeof(Real), st));
+  if (energies && BLOCK_PAIR) CK(cudaMemsetAsync(energies, 0, PBB * 4 * sizeof(Real), st));
   if (nbr) CK(cudaMemsetAsync(nbr, 0, PBB * sizeof(int32_t), st));
-  if (dcoords) CK(cudaMemsetAsync(dcoords, 0, (size_t)pl->N * 3 * sizeof(Real), st));
-  if (dwaters) CK(cudaMemsetAsync(dwaters, 0, (size_t)pl->N * LKB_NW * 3 * sizeof(Real), st));
-  CK(cudaMemsetAsync(pl->counts, 0, N_COUNTS * sizeof(unsigned long long), st));
+  // the whole-pose energies, the gradients, the counters and the work
+  // ticket: by the sphere pass (which a taken speculative gradient skips:
+  // its outputs are then copied whole)
+  if (energies && !BLOCK_PAIR) s.zero_energies = (int64_t)pl->P * 4;
+  if (dcoords) s.zero_dcoords = (int64_t)pl->N * 3;
+  if (dwaters) {
+    s.zero_aux = (Real*)dwaters;
+    s.zero_aux_n = (int64_t)pl->N * LKB_NW * 3;
+  }
+  s.zero_counts = 1;
   const int n_blocks = pl->P * pl->B;
   const int grid_s = std::max(1, std::min((n_blocks + 7) / 8, pl->n_sm * 16));
   spheres_kernel<Real><<<grid_s, 256, 0, st>>>(s);
   CK(cudaGetLastError());
-  CK(cudaMemsetAsync(pl->counters, 0, sizeof(int), st));
   if (pl->n_work == 0) return TMOL_B200_OK;
   const int warps = std::min(pl->launch.warps_per_cta, 8);  // a kernel of at most 256 threads
   const int R = pl->launch.rows_per_item;
